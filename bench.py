@@ -1,0 +1,465 @@
+#!/usr/bin/env python
+"""Time-to-solve benchmark of the CST assembly -> Dirichlet -> Jacobi-PCG path on B200.
+
+A step is one full pass of the path over one synthetic plate: stiffness pattern, assembly,
+Dirichlet elimination, Jacobi setup and PCG to rtol 1e-10 on the FP64 TRUE residual
+(||b - A x|| / ||b||). The default workload is the 2M-DOF quarter plate (O-grid n_r = 565 x
+n_theta = 1766, 2,000,244 DOFs, ~28M nonzeros; E = 1, nu = 0.3, plane stress, t = 1,
+traction (1, 0) on x = 10, u_x = 0 on x = 0, u_y = 0 on y = 0).
+
+  value  DOFs solved per second with the mesh, loads and BCs already in HBM (CUDA events on
+         the work stream), summed over all GPUs (independent replicas, weak scaling).
+  e2e    the same through the C ABI with pinned HOST buffers: every step uploads the mesh,
+         loads and BCs and downloads the displacements (wall clock around the step).
+
+One JSON line on rank 0. `--impl reference` times the reference's own CPU path (compiled from
+its sources into oracle/_ref) on this host's cores instead, on bounded samples.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import importlib
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+WORKLOADS = {
+    # name: (n_r, n_theta, description)
+    "plate2m": (565, 1766, "quarter plate [0,10]^2 minus r<1, O-grid n_r=565 x n_theta=1766"),
+    "plate1m": (400, 1250, "quarter plate [0,10]^2 minus r<1, O-grid n_r=400 x n_theta=1250"),
+    "plate40x80": (40, 80, "quarter plate [0,10]^2 minus r<1, O-grid n_r=40 x n_theta=80"),
+}
+
+# FP64 Jacobi-PCG iterations to the reference's own stopping rule (recursive residual < 1e-10,
+# solver.cpp:80-82) on each workload, measured with this library's FP64 solver (same
+# recurrence; the GPU-vs-reference parity tests hold the count to 2 %). The CPU baseline and
+# the reference arm time a bounded number of the reference's iterations and scale to this.
+REF_RULE_ITERS = {"plate2m": None, "plate1m": 13812, "plate40x80": 897}
+
+METRIC = ("time-to-solve @rtol 1e-10 (FP64 true residual), 2M-DOF plate, as DOFs solved per "
+          "second")
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="plate2m", choices=sorted(WORKLOADS))
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--cpu-sample-iters", type=int, default=150)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    a = ap.parse_args()
+    a.warmup = max(a.warmup, 3)
+    return a
+
+
+# ---- distributed plumbing (replicas: barrier + max over ranks only) -------------------------
+
+class Dist:
+    def __init__(self):
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+
+    def init(self, backend: str):
+        if self.world > 1:
+            import torch.distributed as dist
+            dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=300))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, v: float, device=None) -> float:
+        if not self.pg:
+            return v
+        import torch
+        t = torch.tensor([v], dtype=torch.float64, device=device)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+def timed_region(step, k: int, w: int, dist: Dist, start_timer, stop_timer, sync) -> float:
+    """W untimed steps, then K steps bracketed by barrier + sync on both sides; returns the
+    max over ranks of the elapsed seconds (the timer pair may be CUDA events or a clock)."""
+    for _ in range(w):
+        step()
+    sync()
+    dist.barrier()
+    sync()
+    t = start_timer()
+    for _ in range(k):
+        step()
+    el = stop_timer(t)
+    sync()
+    dist.barrier()
+    return el
+
+
+# ---- clocks -----------------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ["clocks.sm", "clocks.max.sm", "power.draw", "clocks_event_reasons.hw_slowdown",
+              "clocks_event_reasons.hw_thermal_slowdown", "clocks_event_reasons.sw_thermal_slowdown",
+              "clocks_event_reasons.sw_power_cap"]
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={','.join(self.FIELDS)}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.device)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        return parse_clock_csv(out)
+
+
+def parse_clock_csv(text: str) -> dict:
+    """Median SM clock, max clock and the throttle reasons seen (ClockSampler.FIELDS order)."""
+    sm, mx, reasons = [], None, set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    for line in text.strip().splitlines():
+        f = [x.strip() for x in line.split(",")]
+        if len(f) < 7:
+            continue
+        try:
+            sm.append(float(f[0]))
+            mx = float(f[1])
+        except ValueError:
+            continue
+        for name, v in zip(names, f[3:7]):
+            if v.lower().startswith("active"):
+                reasons.add(name)
+    return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+            "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---- helpers ------------------------------------------------------------------------------------
+
+def measured_peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(name: str):
+    """DRAM bytes per launch from the committed ncu summary of the SpMV kernel, if present."""
+    p = os.path.join(REPO, "profiles", name)
+    if not os.path.exists(p):
+        return None
+    m = re.search(r"dram_bytes_per_launch_full_size:\s*([0-9.eE+]+)", open(p).read())
+    return float(m.group(1)) if m else None
+
+
+def make_inputs(pkg, workload):
+    n_r, n_t, _ = WORKLOADS[workload]
+    mesh = pkg.plate.quarter_plate(n_r, n_t)
+    D = pkg.constitutive_matrix(1.0, 0.3)
+    dofs, vals = pkg.plate.symmetry_dirichlet(mesh)
+    return mesh, D, dofs, vals
+
+
+# ---- CPU baseline: the reference's serial core on a bounded sample ---------------------------------
+
+def cpu_sample(mesh, dofs, vals, sample_iters: int):
+    """Times the reference's CPU path (oracle/_ref) on this plate: full pattern + assembly +
+    loads + BCs, then `sample_iters` PCG iterations. Falls back to the oracle restatement."""
+    import oracle
+    if oracle.RefCore.available():
+        R = oracle.RefCore()
+        t0 = time.perf_counter()
+        m = R.mesh_from_arrays(mesh.xy, mesh.triangles, mesh.boundary_edges)
+        K = R.pattern(m)
+        R.assemble(m, R.constitutive_matrix(1.0, 0.3), 1.0, K)
+        f = np.zeros(mesh.num_dofs)
+        R.add_traction(m, "right", 1.0, 1.0, 0.0, f)
+        R.apply_dirichlet(K, dofs, vals, f)
+        t1 = time.perf_counter()
+        _, st = R.pcg(K, f, 1e-10, sample_iters)
+        t2 = time.perf_counter()
+        R.free_csr(K)
+        R.free_mesh(m)
+        return {"kind": "reference", "setup_s": t1 - t0, "solve_s": t2 - t1,
+                "iters": st["iterations"], "per_iter_s": st["t_solve"] / max(st["iterations"], 1)}
+    O = oracle.Oracle()
+    t0 = time.perf_counter()
+    rp, cols = O.build_stiffness_pattern(mesh.num_nodes, mesh.triangles)
+    kv = O.assemble_stiffness(mesh.xy, mesh.triangles, O.constitutive_matrix(1.0, 0.3), 1.0, rp, cols)
+    f = np.zeros(mesh.num_dofs)
+    O.add_traction(mesh.xy, mesh.triangles, mesh.boundary_edges["right"], 1.0, 1.0, 0.0, f)
+    O.apply_dirichlet(rp, cols, kv, dofs, vals, f)
+    t1 = time.perf_counter()
+    _, st = O.pcg_jacobi(rp, cols, kv, f, 1e-10, sample_iters)
+    t2 = time.perf_counter()
+    return {"kind": "port", "setup_s": t1 - t0, "solve_s": t2 - t1, "iters": st["iterations"],
+            "per_iter_s": (t2 - t1) / max(st["iterations"], 1)}
+
+
+def cpu_baseline_entry(s, n_dofs, iters_full, sample_iters):
+    t = s["setup_s"] + s["per_iter_s"] * iters_full
+    return {"value": n_dofs / t, "unit": "DOF/s", "cores": 1, "kind": s["kind"],
+            "time_to_solve_s": t,
+            "sample": (f"full pattern+assembly+loads+BCs ({s['setup_s']:.2f} s) + {s['iters']} of "
+                       f"{iters_full} PCG iterations ({s['per_iter_s'] * 1e3:.2f} ms each, the "
+                       f"reference's recursive-residual rule), extrapolated; single-threaded "
+                       f"reference serial core, host has {os.cpu_count()} cores")}
+
+
+# ---- the reference arm ----------------------------------------------------------------------------
+
+def run_reference(a, dist: Dist):
+    if dist.rank != 0:
+        return 0
+    pkg = importlib.import_module("mpi-cst-fem-solver_b200.plate")
+    n_r, n_t, desc = WORKLOADS[a.workload]
+    mesh = pkg.quarter_plate(n_r, n_t)
+    dofs, vals = pkg.symmetry_dirichlet(mesh)
+    iters_full = REF_RULE_ITERS.get(a.workload)
+    if iters_full is None:
+        print(json.dumps({"impl": "reference", "unavailable": f"no iteration count recorded for {a.workload}"}))
+        return 0
+    sample_iters = max(10, a.cpu_sample_iters // 3)
+    samples = []
+    for i in range(a.warmup + a.steps):
+        s = cpu_sample(mesh, dofs, vals, sample_iters)
+        if i >= a.warmup:
+            samples.append(s)
+    per_it = statistics.median(s["per_iter_s"] for s in samples)
+    setup = statistics.median(s["setup_s"] for s in samples)
+    t = setup + per_it * iters_full
+    value = mesh.num_dofs / t
+    cb = cpu_baseline_entry({"kind": samples[0]["kind"], "setup_s": setup, "per_iter_s": per_it,
+                             "iters": sample_iters}, mesh.num_dofs, iters_full, sample_iters)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "DOF/s", "n_gpus": a.gpus,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{a.workload}: {desc}, {mesh.num_dofs} DOFs",
+                       "step": "reference serial core: pattern + assembly + loads + BCs + Jacobi-PCG "
+                               "(rtol 1e-10, its recursive-residual rule), bounded sample extrapolated"},
+            "cpu_baseline": cb, "time_to_solve_s": t,
+            "e2e": {"value": value, "unit": "DOF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ---- our arm --------------------------------------------------------------------------------------
+
+def run_ours(a, dist: Dist):
+    import torch
+    pkg = importlib.import_module("mpi-cst-fem-solver_b200")
+    dev = dist.local_rank if a.gpus > 1 else 0
+    torch.cuda.set_device(dev)
+    dist.init("nccl")
+    L = pkg.native.load(build_if_missing=False)
+    mesh, D, dofs, vals = make_inputs(pkg, a.workload)
+    n_r, n_t, desc = WORKLOADS[a.workload]
+    n = mesh.num_dofs
+
+    stream = torch.cuda.Stream(device=dev)
+    ctx = pkg.Context(dev)
+    ctx.set_stream(stream)
+    # loads on the host (bc.cpp:190-253) once; the step starts from them
+    ctx.set_mesh(mesh)
+    b0 = np.zeros(n)
+    pkg.add_traction(ctx, mesh.boundary_edges["right"], 1.0, 1.0, 0.0, b0)
+
+    # device-resident inputs
+    d_xy = torch.from_numpy(mesh.xy).to(dev)
+    d_tri = torch.from_numpy(mesh.triangles).to(dev)
+    d_dofs = torch.from_numpy(dofs).to(dev)
+    d_vals = torch.from_numpy(vals).to(dev)
+    d_b0 = torch.from_numpy(b0).to(dev)
+    d_b = torch.empty_like(d_b0)
+    d_x = torch.empty_like(d_b0)
+    dmesh = pkg.plate.Mesh(xy=d_xy, triangles=d_tri, boundary_edges=mesh.boundary_edges)
+    torch.cuda.synchronize()
+    opts = pkg.SolverOptions(rtol=1e-10, max_iter=200000, precision=a.precision, true_residual_stop=True)
+    last = {}
+
+    def step():
+        with torch.cuda.stream(stream):
+            K = pkg.build_stiffness_pattern(dmesh, ctx=ctx)
+            pkg.assemble_stiffness(dmesh, D, 1.0, K)
+            d_b.copy_(d_b0)
+            pkg.apply_dirichlet((d_dofs, d_vals), K, d_b)
+            s = pkg.CgJacobiSolver(opts)
+            s.setup(K)
+            last["st"] = s.solve(d_b, d_x)
+            last["K"] = K
+
+    def ev_start():
+        e = torch.cuda.Event(enable_timing=True)
+        e.record(stream)
+        return e
+
+    def ev_stop(e0):
+        e1 = torch.cuda.Event(enable_timing=True)
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) * 1e-3
+
+    sync = torch.cuda.synchronize
+    clocks = ClockSampler(dev)
+    for _ in range(a.warmup):
+        step()
+    sync()
+    l0 = L.cstg_kernel_launches()
+    clocks.start()
+    el = timed_region(step, a.steps, 0, dist, ev_start, ev_stop, sync)
+    clk = clocks.stop()
+    launches = L.cstg_kernel_launches() - l0
+    el_max = dist.max(el, device=f"cuda:{dev}")
+    st = last["st"]
+    if not st.converged or not st.true_rel_residual < 1e-10:
+        raise RuntimeError(f"solve did not reach the FP64 true residual 1e-10: {st.message}, "
+                           f"true {st.true_rel_residual:.3e}")
+    t_step = el_max / a.steps
+    value = a.gpus * n / t_step
+
+    # reference-rule iterations (for the CPU extrapolation and the parity report)
+    with torch.cuda.stream(stream):
+        s_ref = pkg.CgJacobiSolver(pkg.SolverOptions(rtol=1e-10, max_iter=200000))
+        s_ref.setup(last["K"])
+        st_ref = s_ref.solve(d_b, torch.empty_like(d_x))
+    sync()
+
+    # dominant kernel: the 2x2-block SpMV, timed alone (CUDA events, back-to-back launches)
+    K = last["K"]
+    N = mesh.num_nodes
+    nnz = K.nnz()
+    nb = nnz // 4
+    xs = torch.randn(n, dtype=torch.float64, device=dev)
+    ys = torch.empty_like(xs)
+    reps = 100
+    with torch.cuda.stream(stream):
+        for _ in range(20):
+            K.multiply(xs, ys)
+        e0 = ev_start()
+        for _ in range(reps):
+            K.multiply(xs, ys)
+        spmv_s = ev_stop(e0) / reps
+    spmv_bytes = nnz * 8 + nb * 4 + (N + 1) * 4 + n * 8 + n * 8
+    peak, peak_kind = measured_peaks()
+    achieved = spmv_bytes / spmv_s / 1e9
+    traffic = profile_traffic("spmv_block_fp64_plate2m.md") if a.workload == "plate2m" else None
+    iter_bytes = spmv_bytes + n * (5 * 8 + 2 * 8) + n * (2 * 8 + 2 * 8)
+    iter_s = st.solve_seconds / max(st.iterations, 1)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "DOF/s", "n_gpus": a.gpus, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if a.precision == "fp64" else "f32+f64", "data": "synthetic",
+        "config": {"workload": f"{a.workload}: {desc}, {n} DOFs, {nnz} nnz, E=1 nu=0.3 plane stress t=1, "
+                               "traction (1,0) on x=10, u_x=0 on x=0, u_y=0 on y=0",
+                   "step": "pattern + assembly + Dirichlet + Jacobi setup + PCG to rtol 1e-10 on the "
+                           "FP64 true residual (residual replacement)",
+                   "precision": a.precision, "dofs": n, "nnz": nnz,
+                   "l2": f"inputs larger than L2 (matrix values {nnz * 8 / 1e6:.0f} MB)",
+                   "parallelism": f"replicas x{a.gpus}"},
+        "time_to_solve_s": t_step, "iterations": st.iterations, "refinements": st.refinements,
+        "true_rel_residual": st.true_rel_residual, "solve_s": st.solve_seconds,
+        "reference_rule_iterations": st_ref.iterations, "reference_rule_solve_s": st_ref.solve_seconds,
+        "pcg_iteration_gbs": iter_bytes / iter_s / 1e9,
+        "roofline": {"bound": "hbm", "kernel": "k_spmv_block<PCG=false> (FP64 2x2-block SpMV)",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs, burst copy)",
+                     "traffic": traffic, "algorithmic_bytes": spmv_bytes, "launch_us": spmv_s * 1e6},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+    }
+
+    # e2e: through the C ABI with pinned host buffers
+    if not a.no_e2e:
+        def pinned(arr):
+            t = torch.empty(arr.shape, dtype={np.float64: torch.float64, np.int32: torch.int32}[arr.dtype.type],
+                            pin_memory=True)
+            v = t.numpy()
+            v[...] = arr
+            return v
+        hmesh = pkg.plate.Mesh(xy=pinned(mesh.xy), triangles=pinned(mesh.triangles),
+                               boundary_edges=mesh.boundary_edges)
+        h_dofs, h_vals, h_b0 = pinned(dofs), pinned(vals), pinned(b0)
+        h_b = pinned(b0)
+        h_x = pinned(np.zeros(n))
+        ectx = pkg.Context(dev)
+
+        def e2e_step():
+            K2 = pkg.build_stiffness_pattern(hmesh, ctx=ectx)
+            pkg.assemble_stiffness(hmesh, D, 1.0, K2)
+            np.copyto(h_b, h_b0)
+            pkg.apply_dirichlet((h_dofs, h_vals), K2, h_b)
+            s2 = pkg.CgJacobiSolver(opts)
+            s2.setup(K2)
+            last["e2e"] = s2.solve(h_b, h_x)
+
+        def wall_start():
+            return time.perf_counter()
+
+        def wall_stop(t0):
+            return time.perf_counter() - t0
+
+        el2 = timed_region(e2e_step, a.steps, a.warmup, dist, wall_start, wall_stop, sync)
+        el2 = dist.max(el2, device=f"cuda:{dev}")
+        h2d = mesh.xy.nbytes + mesh.triangles.nbytes + dofs.nbytes + vals.nbytes + 2 * b0.nbytes
+        d2h = b0.nbytes + h_x.nbytes
+        line["e2e"] = {"value": a.gpus * n / (el2 / a.steps), "unit": "DOF/s", "h2d_bytes_per_step": int(h2d),
+                       "d2h_bytes_per_step": int(d2h), "ms_per_step": el2 / a.steps * 1e3,
+                       "path": "C ABI, host pinned buffers (cstg_set_mesh .. cstg_pcg_solve)"}
+        ectx.close()
+
+    if dist.rank == 0 and not a.no_cpu_baseline and a.gpus == 1:
+        iters_full = st_ref.iterations
+        s = cpu_sample(mesh, dofs, vals, a.cpu_sample_iters)
+        line["cpu_baseline"] = cpu_baseline_entry(s, n, iters_full, a.cpu_sample_iters)
+    ctx.close()
+    if dist.rank == 0:
+        print(json.dumps(line))
+    dist.close()
+    return 0
+
+
+def main():
+    a = parse()
+    dist = Dist()
+    if a.impl == "reference":
+        return run_reference(a, dist)
+    return run_ours(a, dist)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,170 @@
+/*
+ * cstfem_b200.h -- C ABI of the B200 (sm_100a) CST assembly / Dirichlet / Jacobi-PCG path.
+ *
+ * Drop-in for the serial core of FreddyJuka/mpi-cst-fem-solver (cstfem_core). The call shapes
+ * are the reference's: build_stiffness_pattern -> assemble_stiffness -> apply_dirichlet ->
+ * CgJacobiSolver::setup / solve (pcg_jacobi), on the reference's row-owner CSR layout
+ * (row_ptr int32[n+1], cols int32[nnz] sorted per row, vals double[nnz]; DOF 2*node+component;
+ * one 2x2 block per pair of nodes sharing a triangle). Only plain pointers and sizes cross
+ * the boundary.
+ *
+ * Conventions
+ *  - Every call returns a status code (CSTG_OK = 0). Where the reference throws an exception
+ *    the call returns the matching CSTG_ERR_* code and cstg_last_error() gives the message.
+ *    Solver non-convergence is not an error (the reference reports it in SolverStats):
+ *    cstg_pcg_solve returns CSTG_OK with stats.converged = 0 and stats.status set.
+ *  - Functions without a suffix take HOST pointers and copy through pinned staging buffers;
+ *    the *_device variants take device pointers on the context's device (no copies).
+ *  - A context owns all the device memory it uses; buffers grow and are reused, so repeated
+ *    calls of the same size allocate nothing. A context is used by one host thread at a
+ *    time; work is ordered on the context's stream (cstg_set_stream).
+ *  - The context keeps the mesh, the pattern and the matrix between calls, like the
+ *    reference's Mesh / CsrMatrix objects live between the driver's phases.
+ */
+#ifndef CSTFEM_B200_H
+#define CSTFEM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------------------------- */
+#define CSTG_OK 0
+#define CSTG_ERR_INVALID_ARGUMENT 1   /* bad sizes / pointers / DOF out of range            */
+#define CSTG_ERR_CUDA 2               /* a CUDA runtime call failed                           */
+#define CSTG_ERR_NONPOSITIVE_DIAGONAL 3 /* solver.cpp:139-140, bc.cpp:151-153                  */
+#define CSTG_ERR_PATTERN 4            /* entry missing from the pattern, assembly.cpp:67-69   */
+#define CSTG_ERR_DIRICHLET_CONFLICT 5 /* same DOF with two values, bc.cpp:107-116             */
+#define CSTG_ERR_STATE 6              /* call order (e.g. solve before setup, solver.cpp:151) */
+#define CSTG_ERR_MESH 7               /* node index out of range, node neighbourhood too big  */
+#define CSTG_ERR_TIMEOUT 8            /* a bounded device wait gave up                        */
+#define CSTG_ERR_UNSUPPORTED 9        /* option not available for this matrix kind            */
+
+/* stats.status values (how the iteration ended) */
+#define CSTG_SOLVE_CONVERGED 0        /* recursive residual < rtol (solver.cpp:80-87)         */
+#define CSTG_SOLVE_ZERO_RHS 1         /* ||b|| = 0, x = 0 (solver.cpp:44-49)                  */
+#define CSTG_SOLVE_BREAKDOWN 2        /* p'Ap <= 0 (solver.cpp:65-71)                          */
+#define CSTG_SOLVE_MAX_ITER 3         /* max_iter reached (solver.cpp:100-104)                */
+#define CSTG_SOLVE_TIMEOUT 4          /* a device barrier gave up; result not usable          */
+
+/* precision / method of cstg_pcg_solve */
+#define CSTG_PRECISION_FP64 0         /* plain FP64 Jacobi-PCG, the reference's arithmetic     */
+#define CSTG_PRECISION_MIXED 1        /* FP32 SpMV + preconditioner, FP64 scalars/accumulation,
+                                         FP64 true-residual replacement (iterative refinement) */
+
+typedef struct cstg_ctx cstg_ctx;
+
+/* ≙ cstfem::SolverOptions (include/cstfem/solver.hpp:93-97) plus the B200 additions. */
+typedef struct {
+  double rtol;              /* default 1e-10                                               */
+  int max_iter;             /* default 20000                                               */
+  int record_history;       /* fill `history` (max_iter + 1 doubles) with ||r_k||/||b||     */
+  int precision;            /* CSTG_PRECISION_*                                            */
+  int true_residual_stop;   /* 1: converge only when the FP64 true residual ||b-Ax||/||b||
+                               < rtol (residual replacement + restart when the recursive
+                               residual converged first); 0: the reference's rule
+                               (recursive residual, solver.cpp:80-82)                      */
+  int max_refinements;      /* cap on replacements/restarts when true_residual_stop (16)   */
+  int check_interval;       /* iterations per device graph between host checks (0: auto)  */
+  int reserved[4];
+} cstg_solver_options;
+
+/* ≙ cstfem::SolverStats (include/cstfem/solver.hpp:99-107) plus counters. */
+typedef struct {
+  int iterations;           /* CG iterations (all restarts together)                        */
+  int converged;            /* 1 when the stopping rule was met                             */
+  int status;               /* CSTG_SOLVE_*                                                 */
+  int refinements;          /* FP64 residual replacements / restarts performed             */
+  double rel_residual;      /* recursive ||r_k|| / ||b|| at exit                            */
+  double true_rel_residual; /* ||b - A x|| / ||b|| recomputed in FP64 at exit               */
+  double solve_seconds;     /* device time of the solve (CUDA events)                       */
+  long long spmv_calls;     /* SpMV launches (iterations + true residuals)                  */
+  char message[256];        /* SolverStats::message                                         */
+  char warning[256];        /* SolverStats::warning (true residual > 10 rtol)               */
+} cstg_stats;
+
+/* ---- context --------------------------------------------------------------------------- */
+/* No reference counterpart (the reference keeps its state in caller objects). */
+cstg_ctx* cstg_create(int device, int* status);
+void cstg_destroy(cstg_ctx* ctx);
+const char* cstg_last_error(const cstg_ctx* ctx);
+int cstg_set_stream(cstg_ctx* ctx, void* cuda_stream); /* NULL: the context's own stream */
+void cstg_default_options(cstg_solver_options* opt);
+int cstg_version(void);
+/* Kernel launches issued by this library in this process so far (every kernel node of a
+ * replayed CUDA graph counts). Benchmarks read it around a timed region. */
+long long cstg_kernel_launches(void);
+
+/* ---- mesh -------------------------------------------------------------------------------
+ * ≙ cstfem::Mesh (include/cstfem/mesh.hpp:19-30): xy = 2 doubles per node, tri = 3 int32 per
+ * triangle, counter-clockwise, 0-based (read_gmsh reorients, mesh_io.cpp:281-289).        */
+int cstg_set_mesh(cstg_ctx* ctx, int n_nodes, const double* xy, int n_tri, const int32_t* tri);
+int cstg_set_mesh_device(cstg_ctx* ctx, int n_nodes, const double* d_xy, int n_tri,
+                         const int32_t* d_tri);
+
+/* ---- build_stiffness_pattern (include/cstfem/assembly.hpp:15, src/assembly.cpp:9-42) -----
+ * Builds the CSR pattern and the element slot map on the device. nnz_out may be NULL. */
+int cstg_build_pattern(cstg_ctx* ctx, int64_t* nnz_out);
+
+/* ---- assemble_stiffness (include/cstfem/assembly.hpp:22, src/assembly.cpp:54-74) ---------
+ * Zeroes the values and adds every triangle's Ke = t |A| B^T D B (element.cpp:37-55),
+ * bit-identical to the reference (same FP64 operations, same per-entry summation order).
+ * D is the 3x3 row-major constitutive matrix (constitutive_matrix, element.cpp:7-15). */
+int cstg_assemble(cstg_ctx* ctx, const double D[9], double thickness);
+
+/* ---- CSR access ----------------------------------------------------------------------------
+ * cstg_get_csr copies the current matrix (pattern + values) to host arrays sized by
+ * cstg_matrix_size; any pointer may be NULL. cstg_set_csr replaces the matrix by a caller's
+ * CSR (≙ passing any CsrMatrix to CgJacobiSolver::setup, solver.hpp:134); such a matrix has no
+ * mesh pattern and uses the scalar-CSR SpMV. */
+int cstg_matrix_size(cstg_ctx* ctx, int* n_rows, int64_t* nnz);
+int cstg_get_csr(cstg_ctx* ctx, int32_t* row_ptr, int32_t* cols, double* vals);
+int cstg_set_csr(cstg_ctx* ctx, int n_rows, const int32_t* row_ptr, const int32_t* cols,
+                 const double* vals);
+
+/* ---- apply_dirichlet (include/cstfem/bc.hpp:53, src/bc.cpp:137-166) -----------------------
+ * dofs/values: prescribed DOFs (any order; a DOF repeated with the same value is allowed,
+ * with different values -> CSTG_ERR_DIRICHLET_CONFLICT, DirichletDofs::add bc.cpp:107-116).
+ * Symmetric elimination in place on the context's matrix and on b (n_rows doubles).    */
+int cstg_apply_dirichlet(cstg_ctx* ctx, int n_fixed, const int32_t* dofs, const double* values,
+                         double* b_inout);
+int cstg_apply_dirichlet_device(cstg_ctx* ctx, int n_fixed, const int32_t* d_dofs,
+                                const double* d_values, double* d_b_inout);
+
+/* ---- LinearOperator::apply / CsrMatrix::multiply (solver.hpp:60-64, csr.cpp:19-26) ------
+ * cstg_multiply returns when y is on the host; cstg_multiply_device only enqueues the SpMV on
+ * the context's stream (the caller orders / synchronises). */
+int cstg_multiply(cstg_ctx* ctx, const double* x, double* y);
+int cstg_multiply_device(cstg_ctx* ctx, const double* d_x, double* d_y);
+
+/* ---- CgJacobiSolver::setup (solver.hpp:134, solver.cpp:133-148) ----------------------------
+ * inv_diag = 1 / K_ii; CSTG_ERR_NONPOSITIVE_DIAGONAL names the first such row. */
+int cstg_pcg_setup(cstg_ctx* ctx);
+
+/* ---- CgJacobiSolver::solve / pcg_jacobi (solver.hpp:115-118,135; solver.cpp:35-131) ------
+ * Jacobi-PCG from x = 0 on the current matrix. opt NULL = defaults. history: NULL or
+ * max_iter + 1 doubles (host for cstg_pcg_solve, device for the _device variant). */
+int cstg_pcg_solve(cstg_ctx* ctx, const double* b, double* x, const cstg_solver_options* opt,
+                   cstg_stats* stats, double* history);
+int cstg_pcg_solve_device(cstg_ctx* ctx, const double* d_b, double* d_x,
+                          const cstg_solver_options* opt, cstg_stats* stats, double* d_history);
+
+/* ---- compute_element_stresses (postprocess.cpp:35-60, element.cpp:57-81) ------------------
+ * u: 2 doubles per node. out: 8 arrays of n_tri doubles, in this order:
+ * sxx, syy, txy, von_mises, szz, cx, cy, area. */
+int cstg_element_stresses(cstg_ctx* ctx, const double* u, double E, double nu, int plane_strain,
+                          double* out);
+
+/* ---- add_traction (bc.hpp:74-75, bc.cpp:190-253) -----------------------------------------
+ * Host C++: consistent nodal forces of a constant traction (tx, ty) on line edges
+ * (n_edges x 2 node pairs), 2-point Gauss, times thickness, added to f (2 per node). Uses the
+ * mesh given to cstg_set_mesh (host copy). Bit-identical to the reference. */
+int cstg_add_traction(cstg_ctx* ctx, int n_edges, const int32_t* edges, double thickness,
+                      double tx, double ty, double* f);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CSTFEM_B200_H */

@@ -1,0 +1,899 @@
+// C-ABI layer (include/cstfem_b200.h): the context, argument checks, device buffers, error
+// reporting with the reference's messages, and the host side of the PCG driver (chunks of
+// iterations captured once in a CUDA graph, a host check of the device state between
+// chunks).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/cstfem_b200.h"
+#include "common.cuh"
+#include "kernels.h"
+
+using namespace cstg;
+
+namespace {
+
+constexpr int kErrNone = 0x7f7f7f7f;  // memset(0x7f) sentinel of the device error word
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace
+
+struct cstg_ctx {
+  int device = 0;
+  cudaStream_t own = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::string err;
+  unsigned long long generation = 0;  // bumped whenever a device buffer moves
+
+  // pinned host staging: error word + state snapshot
+  int* h_err = nullptr;
+  PcgState* h_state = nullptr;
+
+  // mesh
+  int n_nodes = 0, n_tri = 0;
+  bool has_mesh = false, host_mesh = false;
+  std::vector<double> h_xy;
+  std::vector<int32_t> h_tri;
+  std::vector<int> h_ne_ptr, h_ne;  // host incidence for add_traction (built lazily)
+  DevBuf xy, tri;
+
+  // incidence + pattern
+  DevBuf cnt, cursor, ne_ptr, ne, scan_tmp, deg, node_ptr, bnbr, slot;
+  DevBuf row_ptr, cols, vals;
+  int kind = 0;  // 0 none, 1 mesh block pattern, 2 caller CSR
+  int n_rows = 0;
+  long long nnz = 0;
+  int csr_sub = 8;
+  bool has_values = false, setup_done = false;
+
+  // Dirichlet
+  DevBuf fixed, ubar, dofs, dvals;
+
+  // solver
+  DevBuf b_in, x, r, p, Ap, inv_diag, partials, state, err_word, hist, vec_in, vec_out, stress;
+  cudaGraphExec_t graph = nullptr;
+  unsigned long long graph_gen = ~0ull;
+  int graph_chunk = 0, graph_hist = -1, graph_kind = -1, graph_n = -1;
+};
+
+namespace {
+
+int fail(cstg_ctx* c, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (c) c->err = buf;
+  return code;
+}
+
+#define CK(call)                                                                           \
+  do {                                                                                     \
+    const cudaError_t e_ = (call);                                                         \
+    if (e_ != cudaSuccess)                                                                 \
+      return fail(ctx, CSTG_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_));            \
+  } while (0)
+
+template <class T>
+T* buf_ptr(DevBuf& b) {
+  return static_cast<T*>(b.p);
+}
+
+// Grow-only device buffer. Returns 0 or an error code.
+int ensure(cstg_ctx* ctx, DevBuf& b, size_t bytes) {
+  bytes = std::max<size_t>(bytes, 256);
+  if (b.bytes >= bytes) return CSTG_OK;
+  if (b.p) {
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaFree(b.p));
+    b.p = nullptr;
+    b.bytes = 0;
+  }
+  CK(cudaMalloc(&b.p, bytes));
+  b.bytes = bytes;
+  ctx->generation++;
+  return CSTG_OK;
+}
+
+#define ENSURE(buf, bytes)                          \
+  do {                                              \
+    const int rc_ = ensure(ctx, (buf), (bytes));    \
+    if (rc_) return rc_;                            \
+  } while (0)
+
+void free_buf(DevBuf& b) {
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.bytes = 0;
+}
+
+int begin(cstg_ctx* ctx) {
+  if (!ctx) return CSTG_ERR_INVALID_ARGUMENT;
+  ctx->err.clear();
+  CK(cudaSetDevice(ctx->device));
+  return CSTG_OK;
+}
+
+#define BEGIN(ctx)                 \
+  do {                             \
+    const int rb_ = begin(ctx);    \
+    if (rb_) return rb_;           \
+  } while (0)
+
+int reset_err(cstg_ctx* ctx) {
+  CK(cudaMemsetAsync(ctx->err_word.p, 0x7f, sizeof(int) * kErrSlots, ctx->stream));
+  return CSTG_OK;
+}
+
+// Copies the error word to the host and waits for the stream.
+int read_err(cstg_ctx* ctx) {
+  CK(cudaMemcpyAsync(ctx->h_err, ctx->err_word.p, sizeof(int) * kErrSlots, cudaMemcpyDeviceToHost,
+                     ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return CSTG_OK;
+}
+
+#define RESET_ERR()                     \
+  do {                                  \
+    const int r_ = reset_err(ctx);      \
+    if (r_) return r_;                  \
+  } while (0)
+#define READ_ERR()                      \
+  do {                                  \
+    const int r_ = read_err(ctx);       \
+    if (r_) return r_;                  \
+  } while (0)
+
+// constitutive_matrix (element.cpp:7-15), host side, same operations.
+void constitutive(double E, double nu, int plane_strain, double D[9]) {
+  if (!plane_strain) {
+    const double c = E / (1.0 - nu * nu);
+    const double v[9] = {c, c * nu, 0.0, c * nu, c, 0.0, 0.0, 0.0, c * (1.0 - nu) / 2.0};
+    std::memcpy(D, v, sizeof v);
+  } else {
+    const double c = E / ((1.0 + nu) * (1.0 - 2.0 * nu));
+    const double v[9] = {c * (1.0 - nu), c * nu, 0.0, c * nu, c * (1.0 - nu), 0.0,
+                         0.0, 0.0, c * (1.0 - 2.0 * nu) / 2.0};
+    std::memcpy(D, v, sizeof v);
+  }
+}
+
+BlockMatrix block_view(cstg_ctx* ctx) {
+  BlockMatrix m;
+  m.n_nodes = ctx->n_nodes;
+  m.node_ptr = buf_ptr<int>(ctx->node_ptr);
+  m.bnbr = buf_ptr<int>(ctx->bnbr);
+  m.vals = buf_ptr<double>(ctx->vals);
+  return m;
+}
+
+CsrMatrixDev csr_view(cstg_ctx* ctx) {
+  CsrMatrixDev m;
+  m.n_rows = ctx->n_rows;
+  m.row_ptr = buf_ptr<int>(ctx->row_ptr);
+  m.cols = buf_ptr<int>(ctx->cols);
+  m.vals = buf_ptr<double>(ctx->vals);
+  m.sub = ctx->csr_sub;
+  return m;
+}
+
+int spmv(cstg_ctx* ctx, const double* x, double* y) {
+  if (ctx->kind == 1) {
+    const BlockMatrix bm = block_view(ctx);
+    CK(launch_spmv(&bm, nullptr, x, y, ctx->stream));
+  } else {
+    const CsrMatrixDev cm = csr_view(ctx);
+    CK(launch_spmv(nullptr, &cm, x, y, ctx->stream));
+  }
+  return CSTG_OK;
+}
+
+void g_fmt(char* out, size_t n, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(out, n, fmt, ap);
+  va_end(ap);
+}
+
+}  // namespace
+
+extern "C" {
+
+int cstg_version(void) { return 1; }
+
+long long cstg_kernel_launches(void) { return launches_total(); }
+
+void cstg_default_options(cstg_solver_options* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof *o);
+  o->rtol = 1e-10;
+  o->max_iter = 20000;
+  o->precision = CSTG_PRECISION_FP64;
+  o->true_residual_stop = 0;
+  o->max_refinements = 16;
+  o->check_interval = 0;
+}
+
+cstg_ctx* cstg_create(int device, int* status) {
+  auto set = [&](int s) {
+    if (status) *status = s;
+  };
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+    set(CSTG_ERR_CUDA);
+    return nullptr;
+  }
+  if (cudaSetDevice(device) != cudaSuccess) {
+    set(CSTG_ERR_CUDA);
+    return nullptr;
+  }
+  auto* ctx = new cstg_ctx;
+  ctx->device = device;
+  bool ok = cudaStreamCreateWithFlags(&ctx->own, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaEventCreate(&ctx->ev0) == cudaSuccess && cudaEventCreate(&ctx->ev1) == cudaSuccess &&
+            cudaMallocHost(&ctx->h_err, sizeof(int) * kErrSlots) == cudaSuccess &&
+            cudaMallocHost(&ctx->h_state, sizeof(PcgState)) == cudaSuccess;
+  ctx->stream = ctx->own;
+  ok = ok && ensure(ctx, ctx->err_word, sizeof(int) * kErrSlots) == 0 &&
+       ensure(ctx, ctx->state, sizeof(PcgState)) == 0 &&
+       ensure(ctx, ctx->partials, sizeof(double) * 4 * kReduceBlocks) == 0 &&
+       cudaMemsetAsync(ctx->state.p, 0, sizeof(PcgState), ctx->stream) == cudaSuccess &&
+       cudaStreamSynchronize(ctx->stream) == cudaSuccess;
+  if (!ok) {
+    cstg_destroy(ctx);
+    set(CSTG_ERR_CUDA);
+    return nullptr;
+  }
+  set(CSTG_OK);
+  return ctx;
+}
+
+void cstg_destroy(cstg_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->graph) cudaGraphExecDestroy(ctx->graph);
+  DevBuf* all[] = {&ctx->xy,      &ctx->tri,    &ctx->cnt,      &ctx->cursor,   &ctx->ne_ptr,
+                   &ctx->ne,      &ctx->scan_tmp, &ctx->deg,    &ctx->node_ptr, &ctx->bnbr,
+                   &ctx->slot,    &ctx->row_ptr, &ctx->cols,    &ctx->vals,     &ctx->fixed,
+                   &ctx->ubar,    &ctx->dofs,   &ctx->dvals,    &ctx->b_in,     &ctx->x,
+                   &ctx->r,       &ctx->p,      &ctx->Ap,       &ctx->inv_diag, &ctx->partials,
+                   &ctx->state,   &ctx->err_word, &ctx->hist,   &ctx->vec_in,   &ctx->vec_out,
+                   &ctx->stress};
+  for (DevBuf* b : all) free_buf(*b);
+  if (ctx->h_err) cudaFreeHost(ctx->h_err);
+  if (ctx->h_state) cudaFreeHost(ctx->h_state);
+  if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+  if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  if (ctx->own) cudaStreamDestroy(ctx->own);
+  delete ctx;
+}
+
+const char* cstg_last_error(const cstg_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int cstg_set_stream(cstg_ctx* ctx, void* s) {
+  BEGIN(ctx);
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->stream = s ? static_cast<cudaStream_t>(s) : ctx->own;
+  return CSTG_OK;
+}
+
+// ---- mesh --------------------------------------------------------------------------------
+
+static int set_mesh_common(cstg_ctx* ctx, int n_nodes, int n_tri) {
+  if (n_nodes < 0 || n_tri < 0)
+    return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "set_mesh: negative size (%d nodes, %d triangles)",
+                n_nodes, n_tri);
+  if ((long long)n_nodes * 2 > INT_MAX - 1)
+    return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "set_mesh: %d nodes exceed the int32 DOF range",
+                n_nodes);
+  ENSURE(ctx->xy, sizeof(double) * 2 * (size_t)n_nodes);
+  ENSURE(ctx->tri, sizeof(int) * 3 * (size_t)n_tri);
+  ctx->n_nodes = n_nodes;
+  ctx->n_tri = n_tri;
+  ctx->has_mesh = true;
+  ctx->kind = 0;
+  ctx->has_values = ctx->setup_done = false;
+  ctx->h_ne_ptr.clear();
+  ctx->h_ne.clear();
+  return CSTG_OK;
+}
+
+int cstg_set_mesh(cstg_ctx* ctx, int n_nodes, const double* xy, int n_tri, const int32_t* tri) {
+  BEGIN(ctx);
+  if ((n_nodes > 0 && !xy) || (n_tri > 0 && !tri))
+    return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "set_mesh: null array");
+  const int rc = set_mesh_common(ctx, n_nodes, n_tri);
+  if (rc) return rc;
+  ctx->h_xy.assign(xy, xy + 2 * (size_t)n_nodes);
+  ctx->h_tri.assign(tri, tri + 3 * (size_t)n_tri);
+  ctx->host_mesh = true;
+  if (n_nodes)
+    CK(cudaMemcpyAsync(ctx->xy.p, xy, sizeof(double) * 2 * (size_t)n_nodes, cudaMemcpyHostToDevice,
+                       ctx->stream));
+  if (n_tri)
+    CK(cudaMemcpyAsync(ctx->tri.p, tri, sizeof(int) * 3 * (size_t)n_tri, cudaMemcpyHostToDevice,
+                       ctx->stream));
+  return CSTG_OK;
+}
+
+int cstg_set_mesh_device(cstg_ctx* ctx, int n_nodes, const double* d_xy, int n_tri,
+                         const int32_t* d_tri) {
+  BEGIN(ctx);
+  if ((n_nodes > 0 && !d_xy) || (n_tri > 0 && !d_tri))
+    return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "set_mesh_device: null array");
+  const int rc = set_mesh_common(ctx, n_nodes, n_tri);
+  if (rc) return rc;
+  ctx->host_mesh = false;
+  ctx->h_xy.clear();
+  ctx->h_tri.clear();
+  if (n_nodes)
+    CK(cudaMemcpyAsync(ctx->xy.p, d_xy, sizeof(double) * 2 * (size_t)n_nodes,
+                       cudaMemcpyDeviceToDevice, ctx->stream));
+  if (n_tri)
+    CK(cudaMemcpyAsync(ctx->tri.p, d_tri, sizeof(int) * 3 * (size_t)n_tri,
+                       cudaMemcpyDeviceToDevice, ctx->stream));
+  return CSTG_OK;
+}
+
+// ---- build_stiffness_pattern ----------------------------------------------------------------
+
+int cstg_build_pattern(cstg_ctx* ctx, int64_t* nnz_out) {
+  BEGIN(ctx);
+  if (!ctx->has_mesh) return fail(ctx, CSTG_ERR_STATE, "build_pattern: no mesh (call cstg_set_mesh)");
+  const int N = ctx->n_nodes, E = ctx->n_tri;
+  ENSURE(ctx->cnt, sizeof(int) * (size_t)N);
+  ENSURE(ctx->cursor, sizeof(int) * (size_t)N);
+  ENSURE(ctx->ne_ptr, sizeof(int) * ((size_t)N + 1));
+  ENSURE(ctx->ne, sizeof(int) * 3 * (size_t)E);
+  ENSURE(ctx->scan_tmp, sizeof(int) * (size_t)scan_tmp_ints(std::max(N, 1)));
+  ENSURE(ctx->deg, sizeof(int) * (size_t)N);
+  ENSURE(ctx->node_ptr, sizeof(int) * ((size_t)N + 1));
+  MeshDev m;
+  m.n_nodes = N;
+  m.n_tri = E;
+  m.xy = buf_ptr<double>(ctx->xy);
+  m.tri = buf_ptr<int>(ctx->tri);
+  RESET_ERR();
+  int* err = buf_ptr<int>(ctx->err_word);
+  CK(launch_incidence(m, buf_ptr<int>(ctx->cnt), buf_ptr<int>(ctx->cursor), buf_ptr<int>(ctx->ne_ptr),
+                      buf_ptr<int>(ctx->ne), buf_ptr<int>(ctx->scan_tmp), err, ctx->stream));
+  CK(launch_pattern_count(m, buf_ptr<int>(ctx->ne_ptr), buf_ptr<int>(ctx->ne), buf_ptr<int>(ctx->deg),
+                          buf_ptr<int>(ctx->node_ptr), buf_ptr<int>(ctx->scan_tmp), err, ctx->stream));
+  CK(cudaMemcpyAsync(&ctx->h_err[kErrSlots - 1], buf_ptr<int>(ctx->node_ptr) + N, sizeof(int),
+                     cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->h_err, ctx->err_word.p, sizeof(int) * (kErrSlots - 1),
+                     cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (ctx->h_err[kErrMesh] != kErrNone)
+    return fail(ctx, CSTG_ERR_MESH, "build_pattern: triangle %d has a node index outside [0, %d)",
+                ctx->h_err[kErrMesh], N);
+  if (ctx->h_err[kErrNeighbours] != kErrNone)
+    return fail(ctx, CSTG_ERR_MESH, "build_pattern: node %d has more than %d neighbours",
+                ctx->h_err[kErrNeighbours], kMaxNeighbours - 1);
+  const long long nb = (unsigned)ctx->h_err[kErrSlots - 1];
+  if (4 * nb > INT_MAX)
+    return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "build_pattern: nnz = %lld exceeds the int32 range",
+                4 * nb);
+  ENSURE(ctx->bnbr, sizeof(int) * (size_t)nb);
+  ENSURE(ctx->slot, sizeof(int) * 9 * (size_t)E);
+  ENSURE(ctx->row_ptr, sizeof(int) * (2 * (size_t)N + 1));
+  ENSURE(ctx->cols, sizeof(int) * 4 * (size_t)nb);
+  ENSURE(ctx->vals, sizeof(double) * 4 * (size_t)nb);
+  if (N)
+    CK(launch_pattern_fill(m, buf_ptr<int>(ctx->ne_ptr), buf_ptr<int>(ctx->ne),
+                           buf_ptr<int>(ctx->node_ptr), buf_ptr<int>(ctx->bnbr), buf_ptr<int>(ctx->slot),
+                           buf_ptr<int>(ctx->row_ptr), buf_ptr<int>(ctx->cols), ctx->stream));
+  else
+    CK(cudaMemsetAsync(ctx->row_ptr.p, 0, sizeof(int), ctx->stream));
+  ctx->kind = 1;
+  ctx->n_rows = 2 * N;
+  ctx->nnz = 4 * nb;
+  ctx->has_values = ctx->setup_done = false;
+  if (nnz_out) *nnz_out = ctx->nnz;
+  return CSTG_OK;
+}
+
+// ---- assemble_stiffness ---------------------------------------------------------------------
+
+int cstg_assemble(cstg_ctx* ctx, const double D[9], double thickness) {
+  BEGIN(ctx);
+  if (!D) return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "assemble: null D");
+  if (ctx->kind != 1)
+    return fail(ctx, CSTG_ERR_STATE, "assemble: no mesh pattern (call cstg_build_pattern)");
+  MeshDev m;
+  m.n_nodes = ctx->n_nodes;
+  m.n_tri = ctx->n_tri;
+  m.xy = buf_ptr<double>(ctx->xy);
+  m.tri = buf_ptr<int>(ctx->tri);
+  Mat3 d;
+  std::memcpy(d.v, D, sizeof d.v);
+  if (ctx->n_nodes)
+    CK(launch_assemble(m, buf_ptr<int>(ctx->ne_ptr), buf_ptr<int>(ctx->ne), buf_ptr<int>(ctx->slot),
+                       buf_ptr<int>(ctx->node_ptr), d, thickness, buf_ptr<double>(ctx->vals),
+                       ctx->stream));
+  ctx->has_values = true;
+  ctx->setup_done = false;
+  return CSTG_OK;
+}
+
+// ---- CSR access -------------------------------------------------------------------------------
+
+int cstg_matrix_size(cstg_ctx* ctx, int* n_rows, int64_t* nnz) {
+  BEGIN(ctx);
+  if (!ctx->kind) return fail(ctx, CSTG_ERR_STATE, "matrix_size: no matrix");
+  if (n_rows) *n_rows = ctx->n_rows;
+  if (nnz) *nnz = ctx->nnz;
+  return CSTG_OK;
+}
+
+int cstg_get_csr(cstg_ctx* ctx, int32_t* row_ptr, int32_t* cols, double* vals) {
+  BEGIN(ctx);
+  if (!ctx->kind) return fail(ctx, CSTG_ERR_STATE, "get_csr: no matrix");
+  if (row_ptr)
+    CK(cudaMemcpyAsync(row_ptr, ctx->row_ptr.p, sizeof(int) * ((size_t)ctx->n_rows + 1),
+                       cudaMemcpyDeviceToHost, ctx->stream));
+  if (cols && ctx->nnz)
+    CK(cudaMemcpyAsync(cols, ctx->cols.p, sizeof(int) * (size_t)ctx->nnz, cudaMemcpyDeviceToHost,
+                       ctx->stream));
+  if (vals && ctx->nnz) {
+    if (!ctx->has_values) return fail(ctx, CSTG_ERR_STATE, "get_csr: values not assembled");
+    CK(cudaMemcpyAsync(vals, ctx->vals.p, sizeof(double) * (size_t)ctx->nnz, cudaMemcpyDeviceToHost,
+                       ctx->stream));
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  return CSTG_OK;
+}
+
+int cstg_set_csr(cstg_ctx* ctx, int n, const int32_t* row_ptr, const int32_t* cols,
+                 const double* vals) {
+  BEGIN(ctx);
+  if (n < 0 || !row_ptr || (n > 0 && (!cols || !vals)))
+    return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "set_csr: bad arguments");
+  if (row_ptr[0] != 0) return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "set_csr: row_ptr[0] != 0");
+  for (int i = 0; i < n; ++i)
+    if (row_ptr[i + 1] < row_ptr[i])
+      return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "set_csr: row_ptr decreases at row %d", i);
+  const long long nnz = row_ptr[n];
+  for (long long k = 0; k < nnz; ++k)
+    if (cols[k] < 0 || cols[k] >= n)
+      return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "set_csr: column %d out of range at entry %lld",
+                  cols[k], k);
+  ENSURE(ctx->row_ptr, sizeof(int) * ((size_t)n + 1));
+  ENSURE(ctx->cols, sizeof(int) * (size_t)nnz);
+  ENSURE(ctx->vals, sizeof(double) * (size_t)nnz);
+  CK(cudaMemcpyAsync(ctx->row_ptr.p, row_ptr, sizeof(int) * ((size_t)n + 1), cudaMemcpyHostToDevice,
+                     ctx->stream));
+  if (nnz) {
+    CK(cudaMemcpyAsync(ctx->cols.p, cols, sizeof(int) * (size_t)nnz, cudaMemcpyHostToDevice,
+                       ctx->stream));
+    CK(cudaMemcpyAsync(ctx->vals.p, vals, sizeof(double) * (size_t)nnz, cudaMemcpyHostToDevice,
+                       ctx->stream));
+  }
+  const double avg = n ? (double)nnz / n : 1.0;
+  int sub = 1;
+  while (sub < 32 && sub < avg) sub <<= 1;
+  ctx->csr_sub = sub;
+  ctx->kind = 2;
+  ctx->n_rows = n;
+  ctx->nnz = nnz;
+  ctx->has_values = true;
+  ctx->setup_done = false;
+  CK(cudaStreamSynchronize(ctx->stream));
+  return CSTG_OK;
+}
+
+// ---- apply_dirichlet -------------------------------------------------------------------------
+
+int cstg_apply_dirichlet_device(cstg_ctx* ctx, int n_fixed, const int32_t* d_dofs,
+                                const double* d_values, double* d_b) {
+  BEGIN(ctx);
+  if (!ctx->kind || !ctx->has_values)
+    return fail(ctx, CSTG_ERR_STATE, "apply_dirichlet: no assembled matrix");
+  if (n_fixed < 0 || (n_fixed > 0 && (!d_dofs || !d_values)) || (ctx->n_rows > 0 && !d_b))
+    return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "apply_dirichlet: bad arguments");
+  const int n = ctx->n_rows;
+  ENSURE(ctx->fixed, (size_t)n);
+  ENSURE(ctx->ubar, sizeof(double) * (size_t)n);
+  int* err = buf_ptr<int>(ctx->err_word);
+  RESET_ERR();
+  CK(launch_dirichlet(n, nullptr, nullptr, nullptr, n_fixed, d_dofs, d_values,
+                      buf_ptr<unsigned char>(ctx->fixed), buf_ptr<double>(ctx->ubar), nullptr, err,
+                      ctx->stream, false));
+  READ_ERR();
+  if (ctx->h_err[kErrRange] != kErrNone) {
+    int dof = 0;
+    CK(cudaMemcpy(&dof, d_dofs + ctx->h_err[kErrRange], sizeof(int), cudaMemcpyDeviceToHost));
+    return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "apply_dirichlet: DOF %d out of range", dof);
+  }
+  if (ctx->h_err[kErrConflict] != kErrNone) {
+    const int dof = ctx->h_err[kErrConflict];
+    return fail(ctx, CSTG_ERR_DIRICHLET_CONFLICT,
+                "conflicting Dirichlet values for node %d (0-based) component %s", dof / 2,
+                dof % 2 == 0 ? "ux" : "uy");
+  }
+  CK(launch_dirichlet(n, buf_ptr<int>(ctx->row_ptr), buf_ptr<int>(ctx->cols),
+                      buf_ptr<double>(ctx->vals), n_fixed, d_dofs, d_values,
+                      buf_ptr<unsigned char>(ctx->fixed), buf_ptr<double>(ctx->ubar), d_b, err,
+                      ctx->stream, true));
+  ctx->setup_done = false;
+  READ_ERR();
+  if (ctx->h_err[kErrDiag] != kErrNone)
+    return fail(ctx, CSTG_ERR_NONPOSITIVE_DIAGONAL,
+                "apply_dirichlet: non-positive diagonal at DOF %d", ctx->h_err[kErrDiag]);
+  return CSTG_OK;
+}
+
+int cstg_apply_dirichlet(cstg_ctx* ctx, int n_fixed, const int32_t* dofs, const double* values,
+                         double* b) {
+  BEGIN(ctx);
+  if (!ctx->kind) return fail(ctx, CSTG_ERR_STATE, "apply_dirichlet: no assembled matrix");
+  if (n_fixed < 0 || (n_fixed > 0 && (!dofs || !values)) || (ctx->n_rows > 0 && !b))
+    return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "apply_dirichlet: bad arguments");
+  const size_t n = (size_t)ctx->n_rows;
+  ENSURE(ctx->dofs, sizeof(int) * (size_t)n_fixed);
+  ENSURE(ctx->dvals, sizeof(double) * (size_t)n_fixed);
+  ENSURE(ctx->b_in, sizeof(double) * n);
+  if (n_fixed) {
+    CK(cudaMemcpyAsync(ctx->dofs.p, dofs, sizeof(int) * (size_t)n_fixed, cudaMemcpyHostToDevice,
+                       ctx->stream));
+    CK(cudaMemcpyAsync(ctx->dvals.p, values, sizeof(double) * (size_t)n_fixed,
+                       cudaMemcpyHostToDevice, ctx->stream));
+  }
+  if (n) CK(cudaMemcpyAsync(ctx->b_in.p, b, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
+  const int rc = cstg_apply_dirichlet_device(ctx, n_fixed, buf_ptr<int>(ctx->dofs),
+                                             buf_ptr<double>(ctx->dvals), buf_ptr<double>(ctx->b_in));
+  if (rc) {
+    if (rc == CSTG_ERR_INVALID_ARGUMENT && ctx->err.find("out of range") != std::string::npos) {
+      // report the DOF value from the host array
+      for (int q = 0; q < n_fixed; ++q)
+        if (dofs[q] < 0 || dofs[q] >= (int)n)
+          return fail(ctx, rc, "apply_dirichlet: DOF %d out of range", dofs[q]);
+    }
+    return rc;
+  }
+  if (n) CK(cudaMemcpyAsync(b, ctx->b_in.p, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return CSTG_OK;
+}
+
+// ---- multiply -----------------------------------------------------------------------------------
+
+int cstg_multiply_device(cstg_ctx* ctx, const double* d_x, double* d_y) {
+  BEGIN(ctx);
+  if (!ctx->kind || !ctx->has_values) return fail(ctx, CSTG_ERR_STATE, "multiply: no matrix");
+  if (ctx->n_rows && (!d_x || !d_y))
+    return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "multiply: null vector");
+  return spmv(ctx, d_x, d_y);  // asynchronous: ordered on the context's stream
+}
+
+int cstg_multiply(cstg_ctx* ctx, const double* x, double* y) {
+  BEGIN(ctx);
+  if (!ctx->kind || !ctx->has_values) return fail(ctx, CSTG_ERR_STATE, "multiply: no matrix");
+  const size_t n = (size_t)ctx->n_rows;
+  if (n && (!x || !y)) return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "multiply: null vector");
+  ENSURE(ctx->vec_in, sizeof(double) * n);
+  ENSURE(ctx->vec_out, sizeof(double) * n);
+  if (n) CK(cudaMemcpyAsync(ctx->vec_in.p, x, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
+  const int rc = spmv(ctx, buf_ptr<double>(ctx->vec_in), buf_ptr<double>(ctx->vec_out));
+  if (rc) return rc;
+  if (n) CK(cudaMemcpyAsync(y, ctx->vec_out.p, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return CSTG_OK;
+}
+
+// ---- CgJacobiSolver::setup ----------------------------------------------------------------------
+
+int cstg_pcg_setup(cstg_ctx* ctx) {
+  BEGIN(ctx);
+  if (!ctx->kind || !ctx->has_values) return fail(ctx, CSTG_ERR_STATE, "pcg_setup: no matrix");
+  const int n = ctx->n_rows;
+  ENSURE(ctx->inv_diag, sizeof(double) * (size_t)n);
+  RESET_ERR();
+  if (n)
+    CK(launch_inv_diag(n, buf_ptr<int>(ctx->row_ptr), buf_ptr<int>(ctx->cols), buf_ptr<double>(ctx->vals),
+                       buf_ptr<double>(ctx->inv_diag), buf_ptr<int>(ctx->err_word), ctx->stream));
+  READ_ERR();
+  if (ctx->h_err[kErrDiag] != kErrNone) {
+    ctx->setup_done = false;
+    return fail(ctx, CSTG_ERR_NONPOSITIVE_DIAGONAL, "cg_jacobi: non-positive diagonal at row %d",
+                ctx->h_err[kErrDiag]);
+  }
+  ctx->setup_done = true;
+  return CSTG_OK;
+}
+
+// ---- CgJacobiSolver::solve / pcg_jacobi ------------------------------------------------------------
+
+static int snapshot(cstg_ctx* ctx) {
+  CK(cudaMemcpyAsync(ctx->h_state, ctx->state.p, sizeof(PcgState), cudaMemcpyDeviceToHost,
+                     ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return CSTG_OK;
+}
+
+static int run_solve(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg_solver_options& o,
+                     cstg_stats* stats, double* d_hist, bool hist_host) {
+  const int n = ctx->n_rows;
+  ENSURE(ctx->x, sizeof(double) * (size_t)n);
+  ENSURE(ctx->r, sizeof(double) * (size_t)n);
+  ENSURE(ctx->p, sizeof(double) * (size_t)n);
+  ENSURE(ctx->Ap, sizeof(double) * (size_t)n);
+  const bool hist = o.record_history != 0;
+  if (hist) ENSURE(ctx->hist, sizeof(double) * ((size_t)o.max_iter + 1));
+
+  PcgBuffers w;
+  w.n = n;
+  w.x = buf_ptr<double>(ctx->x);
+  w.r = buf_ptr<double>(ctx->r);
+  w.p = buf_ptr<double>(ctx->p);
+  w.Ap = buf_ptr<double>(ctx->Ap);
+  w.inv_diag = buf_ptr<double>(ctx->inv_diag);
+  w.b = d_b;
+  w.partials = buf_ptr<double>(ctx->partials);
+  w.history = hist ? buf_ptr<double>(ctx->hist) : nullptr;
+  w.st = buf_ptr<PcgState>(ctx->state);
+  w.err = buf_ptr<int>(ctx->err_word);
+  const BlockMatrix bm = block_view(ctx);
+  const CsrMatrixDev cm = csr_view(ctx);
+  const BlockMatrix* pbm = ctx->kind == 1 ? &bm : nullptr;
+  const CsrMatrixDev* pcm = ctx->kind == 1 ? nullptr : &cm;
+
+  const int chunk = o.check_interval > 0 ? o.check_interval : 50;
+  // (Re)capture the chunk graph when a buffer or the shape changed.
+  if (!ctx->graph || ctx->graph_gen != ctx->generation || ctx->graph_chunk != chunk ||
+      ctx->graph_hist != (hist ? 1 : 0) || ctx->graph_kind != ctx->kind || ctx->graph_n != n) {
+    if (ctx->graph) {
+      cudaGraphExecDestroy(ctx->graph);
+      ctx->graph = nullptr;
+    }
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < chunk; ++k) launch_pcg_iteration(w, pbm, pcm, ctx->stream);
+    CK(cudaStreamEndCapture(ctx->stream, &g));
+    count_launches(-3LL * chunk);  // captured, not run: counted per graph launch below
+    const cudaError_t ie = cudaGraphInstantiate(&ctx->graph, g, 0);
+    cudaGraphDestroy(g);
+    CK(ie);
+    ctx->graph_gen = ctx->generation;
+    ctx->graph_chunk = chunk;
+    ctx->graph_hist = hist ? 1 : 0;
+    ctx->graph_kind = ctx->kind;
+    ctx->graph_n = n;
+  }
+
+  CK(cudaEventRecord(ctx->ev0, ctx->stream));
+  CK(launch_pcg_init(w, o.rtol, o.max_iter, hist, ctx->stream));
+  long long spmv_calls = 0;
+  int rc = snapshot(ctx);
+  if (rc) return rc;
+  const long long max_chunks = (long long)o.max_iter / chunk + 2 + (long long)o.max_refinements * 4;
+  long long chunks = 0;
+  bool true_done = false;
+  while (ctx->h_state->done != CSTG_SOLVE_ZERO_RHS + 1) {
+    while (ctx->h_state->done == 0) {
+      if (++chunks > max_chunks)
+        return fail(ctx, CSTG_ERR_TIMEOUT, "pcg_solve: the device state did not finish after %lld chunks",
+                    chunks);
+      const int it0 = ctx->h_state->iter;
+      CK(cudaGraphLaunch(ctx->graph, ctx->stream));
+      count_launches(3LL * chunk);
+      rc = snapshot(ctx);
+      if (rc) return rc;
+      spmv_calls += ctx->h_state->iter - it0 + (ctx->h_state->done == CSTG_SOLVE_BREAKDOWN + 1);
+    }
+    // true residual (solver.cpp:117-122); with true_residual_stop it may re-open the solve
+    rc = spmv(ctx, w.x, w.Ap);
+    if (rc) return rc;
+    ++spmv_calls;
+    CK(launch_true_residual(w, o.true_residual_stop != 0, o.max_refinements, ctx->stream));
+    rc = snapshot(ctx);
+    if (rc) return rc;
+    true_done = true;
+    if (ctx->h_state->done != 0) break;
+  }
+  CK(cudaEventRecord(ctx->ev1, ctx->stream));
+  if (n) CK(cudaMemcpyAsync(d_x, w.x, sizeof(double) * (size_t)n, cudaMemcpyDeviceToDevice, ctx->stream));
+  const PcgState s = *ctx->h_state;
+  if (hist && d_hist) {
+    const int cnt = s.done == CSTG_SOLVE_ZERO_RHS + 1 ? 1 : s.iter + 1;
+    CK(cudaMemcpyAsync(d_hist, w.history, sizeof(double) * (size_t)cnt,
+                       hist_host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, ctx->stream));
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+
+  if (stats) {
+    std::memset(stats, 0, sizeof *stats);
+    stats->iterations = s.iter;
+    stats->status = s.done - 1;
+    stats->converged = (s.done == CSTG_SOLVE_CONVERGED + 1 || s.done == CSTG_SOLVE_ZERO_RHS + 1);
+    stats->refinements = s.replace_count;
+    stats->rel_residual = s.rel;
+    stats->true_rel_residual = true_done ? s.true_rel : 0.0;
+    stats->solve_seconds = ms * 1e-3;
+    stats->spmv_calls = spmv_calls;
+    switch (s.done - 1) {
+      case CSTG_SOLVE_ZERO_RHS:
+        g_fmt(stats->message, sizeof stats->message, "zero right-hand side, x = 0");
+        break;
+      case CSTG_SOLVE_CONVERGED:
+        g_fmt(stats->message, sizeof stats->message, "converged in %d iterations, relative residual %g",
+              s.iter, s.rel);
+        break;
+      case CSTG_SOLVE_BREAKDOWN:
+        g_fmt(stats->message, sizeof stats->message,
+              "CG breakdown at iteration %d: p'Ap = %g (matrix not SPD?)", s.iter + 1, s.pAp);
+        break;
+      default:
+        g_fmt(stats->message, sizeof stats->message,
+              "NOT converged: reached max_iter = %d, relative residual %g (rtol %g)", o.max_iter, s.rel,
+              o.rtol);
+        break;
+    }
+    if (stats->converged && s.done != CSTG_SOLVE_ZERO_RHS + 1 && stats->true_rel_residual > 10.0 * o.rtol)
+      g_fmt(stats->warning, sizeof stats->warning,
+            "WARNING: CG recursive residual converged (%g) but the true residual ||b - Ax|| / ||b|| = %g "
+            "exceeds 10 * rtol = %g",
+            s.rel, stats->true_rel_residual, 10.0 * o.rtol);
+  }
+  return CSTG_OK;
+}
+
+static int check_solve_args(cstg_ctx* ctx, const cstg_solver_options* opt, cstg_solver_options& o) {
+  if (opt)
+    o = *opt;
+  else
+    cstg_default_options(&o);
+  if (!ctx->setup_done)
+    return fail(ctx, CSTG_ERR_STATE, "cg_jacobi: solve() called before setup()");
+  if (!(o.rtol >= 0.0) || o.max_iter < 0 || o.max_refinements < 0 || o.check_interval < 0)
+    return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "pcg_solve: bad options");
+  if (o.precision != CSTG_PRECISION_FP64)
+    return fail(ctx, CSTG_ERR_UNSUPPORTED, "pcg_solve: precision %d not available", o.precision);
+  return CSTG_OK;
+}
+
+int cstg_pcg_solve_device(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg_solver_options* opt,
+                          cstg_stats* stats, double* d_history) {
+  BEGIN(ctx);
+  cstg_solver_options o;
+  int rc = check_solve_args(ctx, opt, o);
+  if (rc) return rc;
+  if (ctx->n_rows && (!d_b || !d_x)) return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "pcg_solve: null vector");
+  return run_solve(ctx, d_b, d_x, o, stats, d_history, false);
+}
+
+int cstg_pcg_solve(cstg_ctx* ctx, const double* b, double* x, const cstg_solver_options* opt,
+                   cstg_stats* stats, double* history) {
+  BEGIN(ctx);
+  cstg_solver_options o;
+  int rc = check_solve_args(ctx, opt, o);
+  if (rc) return rc;
+  const size_t n = (size_t)ctx->n_rows;
+  if (n && (!b || !x)) return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "pcg_solve: null vector");
+  ENSURE(ctx->b_in, sizeof(double) * n);
+  ENSURE(ctx->vec_out, sizeof(double) * n);
+  if (n) CK(cudaMemcpyAsync(ctx->b_in.p, b, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
+  rc = run_solve(ctx, buf_ptr<double>(ctx->b_in), buf_ptr<double>(ctx->vec_out), o, stats, history, true);
+  if (rc) return rc;
+  if (n) CK(cudaMemcpyAsync(x, ctx->vec_out.p, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return CSTG_OK;
+}
+
+// ---- compute_element_stresses -----------------------------------------------------------------
+
+int cstg_element_stresses(cstg_ctx* ctx, const double* u, double E, double nu, int plane_strain,
+                          double* out) {
+  BEGIN(ctx);
+  if (!ctx->has_mesh) return fail(ctx, CSTG_ERR_STATE, "element_stresses: no mesh");
+  if ((ctx->n_nodes && !u) || (ctx->n_tri && !out))
+    return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "element_stresses: null array");
+  const size_t nd = 2 * (size_t)ctx->n_nodes, ne = (size_t)ctx->n_tri;
+  ENSURE(ctx->vec_in, sizeof(double) * nd);
+  ENSURE(ctx->stress, sizeof(double) * 8 * ne);
+  if (nd) CK(cudaMemcpyAsync(ctx->vec_in.p, u, sizeof(double) * nd, cudaMemcpyHostToDevice, ctx->stream));
+  Mat3 D;
+  constitutive(E, nu, plane_strain, D.v);
+  MeshDev m;
+  m.n_nodes = ctx->n_nodes;
+  m.n_tri = ctx->n_tri;
+  m.xy = buf_ptr<double>(ctx->xy);
+  m.tri = buf_ptr<int>(ctx->tri);
+  CK(launch_element_stresses(m, buf_ptr<double>(ctx->vec_in), D, nu, plane_strain,
+                             buf_ptr<double>(ctx->stress), ctx->stream));
+  if (ne)
+    CK(cudaMemcpyAsync(out, ctx->stress.p, sizeof(double) * 8 * ne, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return CSTG_OK;
+}
+
+// ---- add_traction (host) -------------------------------------------------------------------------
+
+int cstg_add_traction(cstg_ctx* ctx, int n_edges, const int32_t* edges, double thickness, double tx,
+                      double ty, double* f) {
+  if (!ctx) return CSTG_ERR_INVALID_ARGUMENT;
+  ctx->err.clear();
+  if (!ctx->host_mesh)
+    return fail(ctx, CSTG_ERR_STATE, "add_traction: needs the host mesh of cstg_set_mesh");
+  if (n_edges < 0 || (n_edges > 0 && (!edges || !f)))
+    return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "add_traction: bad arguments");
+  const int N = ctx->n_nodes, E = ctx->n_tri;
+  const int32_t* tri = ctx->h_tri.data();
+  const double* xy = ctx->h_xy.data();
+  if (ctx->h_ne_ptr.empty()) {  // host node -> triangle incidence, built once per mesh
+    ctx->h_ne_ptr.assign((size_t)N + 1, 0);
+    for (long i = 0; i < 3L * E; ++i) {
+      if (tri[i] < 0 || tri[i] >= N) {
+        ctx->h_ne_ptr.clear();
+        return fail(ctx, CSTG_ERR_MESH, "add_traction: triangle %ld has a node out of range", i / 3);
+      }
+      ctx->h_ne_ptr[tri[i] + 1]++;
+    }
+    for (int v = 0; v < N; ++v) ctx->h_ne_ptr[v + 1] += ctx->h_ne_ptr[v];
+    ctx->h_ne.assign((size_t)3 * E, 0);
+    std::vector<int> cur(ctx->h_ne_ptr.begin(), ctx->h_ne_ptr.end() - 1);
+    for (int e = 0; e < E; ++e)
+      for (int c = 0; c < 3; ++c) ctx->h_ne[cur[tri[3 * e + c]]++] = e;
+  }
+  const double g = 1.0 / std::sqrt(3.0);
+  const double xi[2] = {-g, g};
+  for (int q = 0; q < n_edges; ++q) {
+    const int a = edges[2 * q], b = edges[2 * q + 1];
+    if (a < 0 || a >= N || b < 0 || b >= N)
+      return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "add_traction: edge %d has a node out of range", q);
+    // triangles holding edge {a, b} as one of their three edges (bc.cpp:198-210)
+    int count = 0, c = -1;
+    for (int k = ctx->h_ne_ptr[a]; k < ctx->h_ne_ptr[a + 1]; ++k) {
+      const int e = ctx->h_ne[k];
+      const int32_t* t = tri + 3 * (size_t)e;
+      for (int s = 0; s < 3; ++s) {
+        const int u = t[s], v = t[(s + 1) % 3];
+        if ((u == a && v == b) || (u == b && v == a)) {
+          ++count;
+          c = t[(s + 2) % 3];
+        }
+      }
+    }
+    if (count != 1)
+      return fail(ctx, CSTG_ERR_MESH, "traction edge (%d, %d) is adjacent to %d triangles (expected 1)",
+                  a, b, count);
+    const double xa = xy[2 * a], ya = xy[2 * a + 1];
+    const double xb = xy[2 * b], yb = xy[2 * b + 1];
+    const double len = std::hypot(xb - xa, yb - ya);
+    double nx = (yb - ya) / len, ny = -(xb - xa) / len;
+    if (nx * (xy[2 * c] - xa) + ny * (xy[2 * c + 1] - ya) > 0.0) {
+      nx = -nx;
+      ny = -ny;
+    }
+    (void)nx;
+    (void)ny;
+    for (double s : xi) {
+      const double Na = 0.5 * (1.0 - s), Nb = 0.5 * (1.0 + s);
+      const double w = thickness * 0.5 * len;
+      f[2 * a] += w * Na * tx;
+      f[2 * a + 1] += w * Na * ty;
+      f[2 * b] += w * Nb * tx;
+      f[2 * b + 1] += w * Nb * ty;
+    }
+  }
+  return CSTG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,127 @@
+// Internal launcher declarations shared by the C-ABI layer and the kernel files.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace cstg {
+
+// Slots of the device error word (each holds the smallest offending index, INT_MAX if none).
+enum ErrSlot {
+  kErrMesh = 0,        // triangle with a node index out of range
+  kErrNeighbours = 1,  // node whose neighbourhood exceeds kMaxNeighbours
+  kErrRange = 2,       // Dirichlet entry with a DOF out of range
+  kErrConflict = 3,    // Dirichlet DOF given two different values
+  kErrDiag = 4,        // non-positive diagonal (Dirichlet row or Jacobi setup)
+  kErrTimeout = 5,     // bounded device wait gave up
+  kErrSlots = 8
+};
+
+struct Mat3 {  // 3x3 row-major constitutive matrix, passed by value to kernels
+  double v[9];
+};
+
+struct MeshDev {
+  int n_nodes = 0, n_tri = 0;
+  const double* xy = nullptr;
+  const int* tri = nullptr;
+};
+
+// Matrix views for the SpMV paths.
+struct BlockMatrix {  // 2x2 node-block CSR (mesh pattern)
+  int n_nodes = 0;
+  const int* node_ptr = nullptr;
+  const int* bnbr = nullptr;
+  const double* vals = nullptr;  // reference CSR order (node n's 2 rows contiguous)
+  const float* vals32 = nullptr; // same layout, FP32 (mixed precision)
+};
+
+struct CsrMatrixDev {  // generic scalar CSR (caller-supplied matrix)
+  int n_rows = 0;
+  const int* row_ptr = nullptr;
+  const int* cols = nullptr;
+  const double* vals = nullptr;
+  const float* vals32 = nullptr;
+  int sub = 8;  // lanes per row
+};
+
+// Solver state in device memory (scalars of the CG recurrence). 128-byte aligned.
+struct alignas(128) PcgState {
+  double rz;       // r'z of the current iterate
+  double alpha, beta;
+  double bnorm;    // ||b||
+  double rel;      // recursive ||r|| / ||b||
+  double pAp;
+  double true_rel; // ||b - A x|| / ||b||
+  double rtol;
+  double rr;       // r'r of the current iterate
+  double rmax;     // residual norm at the last reliable update (mixed precision)
+  int iter;        // completed CG iterations
+  int done;        // 0 running, else CSTG_SOLVE_* + 1
+  int max_iter;
+  int hist_on;
+  int restart_pending;
+  int replace_count;
+  unsigned int ticket[8];  // last-block tickets, one per kernel kind
+};
+
+// Process-wide count of kernel launches issued by this library (graph launches count every
+// kernel node they run).
+void count_launches(long long k);
+long long launches_total();
+
+// mesh_kernels.cu
+cudaError_t scan_exclusive(const int* in, int n, int* out, int* tmp, cudaStream_t s);
+int scan_tmp_ints(int n);
+cudaError_t launch_incidence(const MeshDev& m, int* cnt, int* cursor, int* ne_ptr, int* ne,
+                             int* scan_tmp, int* err, cudaStream_t s);
+cudaError_t launch_pattern_count(const MeshDev& m, const int* ne_ptr, const int* ne, int* deg,
+                                 int* node_ptr, int* scan_tmp, int* err, cudaStream_t s);
+cudaError_t launch_pattern_fill(const MeshDev& m, const int* ne_ptr, const int* ne,
+                                const int* node_ptr, int* bnbr, int* slot, int* row_ptr,
+                                int* cols, cudaStream_t s);
+cudaError_t launch_assemble(const MeshDev& m, const int* ne_ptr, const int* ne, const int* slot,
+                            const int* node_ptr, const Mat3& D, double t, double* vals,
+                            cudaStream_t s);
+cudaError_t launch_dirichlet(int n_rows, const int* row_ptr, const int* cols, double* vals,
+                             int n_fixed, const int* dofs, const double* values,
+                             unsigned char* fixed, double* ubar, double* b, int* err,
+                             cudaStream_t s, bool apply);
+cudaError_t launch_inv_diag(int n_rows, const int* row_ptr, const int* cols, const double* vals,
+                            double* inv_diag, int* err, cudaStream_t s);
+cudaError_t launch_element_stresses(const MeshDev& m, const double* u, const Mat3& D, double nu,
+                                    int plane_strain, double* out, cudaStream_t s);
+
+// pcg_kernels.cu
+struct PcgBuffers {
+  int n = 0;  // rows
+  double* x = nullptr;
+  double* r = nullptr;
+  double* p = nullptr;
+  double* Ap = nullptr;
+  const double* inv_diag = nullptr;
+  const double* b = nullptr;
+  double* partials = nullptr;  // 4 * kReduceBlocks doubles
+  double* history = nullptr;   // max_iter + 1 or null
+  PcgState* st = nullptr;
+  int* err = nullptr;
+  // mixed precision work vectors
+  float* p32 = nullptr;
+  float* Ap32 = nullptr;
+  float* inv_diag32 = nullptr;
+};
+
+cudaError_t launch_pcg_init(const PcgBuffers& w, double rtol, int max_iter, bool hist,
+                            cudaStream_t s);
+// One CG iteration: SpMV + p'Ap, x/r update + norms, p update.
+cudaError_t launch_pcg_iteration(const PcgBuffers& w, const BlockMatrix* bm,
+                                 const CsrMatrixDev* cm, cudaStream_t s);
+// y = A x (plain SpMV).
+cudaError_t launch_spmv(const BlockMatrix* bm, const CsrMatrixDev* cm, const double* x, double* y,
+                        cudaStream_t s);
+// True residual: r_true = b - A x into w.Ap (A x must already be in w.Ap), ||.|| -> st->true_rel.
+// With `restart`, also r = r_true, p = D^-1 r, rz, and done = 0 when the iteration may go on.
+cudaError_t launch_true_residual(const PcgBuffers& w, bool restart, int max_replacements,
+                                 cudaStream_t s);
+
+}  // namespace cstg
