@@ -164,6 +164,28 @@ int cstg_element_stresses(cstg_ctx* ctx, const double* u, double E, double nu, i
 int cstg_add_traction(cstg_ctx* ctx, int n_edges, const int32_t* edges, double thickness,
                       double tx, double ty, double* f);
 
+/* ---- Jacobi-PCG without allocating ----------------------------------------------------------
+ * No counterpart in the reference. For callers that cannot allocate device memory where they
+ * solve: applications with a fixed device-memory budget whose pool allocator forbids foreign
+ * cudaMalloc calls after start-up, plugin hosts calling from a callback where cudaMalloc /
+ * cudaFree would synchronise the device and stall other work, real-time loops that must not
+ * block in the driver's allocator. CgJacobiSolver setup + solve (FP64, the same kernels and
+ * arithmetic as cstg_pcg_solve on a caller CSR) on the caller's device CSR (d_row_ptr[n+1],
+ * d_cols, d_vals), right-hand side d_b and solution d_x, on the calling thread's current
+ * device and `stream` (NULL: the legacy default stream); returns when the solve has ended.
+ * Every work vector lives in one static device array of the library sized for at most
+ * CSTG_STATIC_MAX_ROWS rows (2.02 MiB on every GPU that loads the library, held until the
+ * process exits); larger systems are rejected with CSTG_ERR_INVALID_ARGUMENT. The first call
+ * on a device looks up the array's device address (cudaGetSymbolAddress): make that first
+ * call before any stream capture. All calls share the array and it keeps the last call's
+ * contents (each call resets the state it needs): calls that overlap on a GPU race, so
+ * serialise them. Needs precision CSTG_PRECISION_FP64 and record_history 0. Errors return a
+ * status code with the text in stats->message. */
+#define CSTG_STATIC_MAX_ROWS 65536
+int cstg_pcg_solve_static(int n_rows, const int32_t* d_row_ptr, const int32_t* d_cols,
+                          const double* d_vals, const double* d_b, double* d_x,
+                          const cstg_solver_options* opt, cstg_stats* stats, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

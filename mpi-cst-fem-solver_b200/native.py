@@ -86,7 +86,11 @@ _SIGS = {
                                         _vp]),
     "cstg_element_stresses": (C.c_int, [_vp, _vp, C.c_double, C.c_double, C.c_int, _vp]),
     "cstg_add_traction": (C.c_int, [_vp, C.c_int, _vp, C.c_double, C.c_double, C.c_double, _vp]),
+    "cstg_pcg_solve_static": (C.c_int, [C.c_int, _vp, _vp, _vp, _vp, _vp, C.POINTER(SolverOptions),
+                                        C.POINTER(Stats), _vp]),
 }
+
+STATIC_MAX_ROWS = 65536  # CSTG_STATIC_MAX_ROWS
 
 _lock = threading.Lock()
 _lib = None
