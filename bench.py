@@ -65,6 +65,10 @@ def parse():
     ap.add_argument("--cpu-sample-iters", type=int, default=150)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--only", choices=["spmv", "solve"], default=None,
+                    help="profiling modes: `spmv` runs --reps SpMV launches on the assembled plate, "
+                         "`solve` one full step; both print one JSON line")
+    ap.add_argument("--reps", type=int, default=20)
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)
     return a
@@ -334,6 +338,27 @@ def run_ours(a, dist: Dist):
         return e0.elapsed_time(e1) * 1e-3
 
     sync = torch.cuda.synchronize
+    if a.only:
+        out = {"mode": a.only, "workload": a.workload}
+        if a.only == "solve":
+            step()
+            sync()
+            out.update(iterations=last["st"].iterations, solve_s=last["st"].solve_seconds)
+        else:  # the assembled, eliminated matrix and `reps` plain SpMV launches, nothing else
+            with torch.cuda.stream(stream):
+                K = pkg.build_stiffness_pattern(dmesh, ctx=ctx)
+                pkg.assemble_stiffness(dmesh, D, 1.0, K)
+                d_b.copy_(d_b0)
+                pkg.apply_dirichlet((d_dofs, d_vals), K, d_b)
+                xs = torch.randn(n, dtype=torch.float64, device=dev)
+                ys = torch.empty_like(xs)
+                e0 = ev_start()
+                for _ in range(a.reps):
+                    K.multiply(xs, ys)
+                out["spmv_us"] = ev_stop(e0) / a.reps * 1e6
+        print(json.dumps(out))
+        ctx.close()
+        return 0
     clocks = ClockSampler(dev)
     for _ in range(a.warmup):
         step()

@@ -15,6 +15,8 @@
  *    cstg_pcg_solve returns CSTG_OK with stats.converged = 0 and stats.status set.
  *  - Functions without a suffix take HOST pointers and copy through pinned staging buffers;
  *    the *_device variants take device pointers on the context's device (no copies).
+ *    Device vectors of doubles must be 16-byte aligned (cudaMalloc / torch allocations are);
+ *    misaligned ones are rejected with CSTG_ERR_INVALID_ARGUMENT.
  *  - A context owns all the device memory it uses; buffers grow and are reused, so repeated
  *    calls of the same size allocate nothing. A context is used by one host thread at a
  *    time; work is ordered on the context's stream (cstg_set_stream).
@@ -174,7 +176,7 @@ int cstg_add_traction(cstg_ctx* ctx, int n_edges, const int32_t* edges, double t
  * d_cols, d_vals), right-hand side d_b and solution d_x, on the calling thread's current
  * device and `stream` (NULL: the legacy default stream); returns when the solve has ended.
  * Every work vector lives in one static device array of the library sized for at most
- * CSTG_STATIC_MAX_ROWS rows (2.02 MiB on every GPU that loads the library, held until the
+ * CSTG_STATIC_MAX_ROWS rows (2.06 MiB on every GPU that loads the library, held until the
  * process exits); larger systems are rejected with CSTG_ERR_INVALID_ARGUMENT. The first call
  * on a device looks up the array's device address (cudaGetSymbolAddress): make that first
  * call before any stream capture. All calls share the array and it keeps the last call's

@@ -202,6 +202,9 @@ int spmv(cstg_ctx* ctx, const double* x, double* y) {
   return CSTG_OK;
 }
 
+// The vector kernels load 16-byte pairs; caller device vectors must allow that.
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
 void g_fmt(char* out, size_t n, const char* fmt, ...) {
   va_list ap;
   va_start(ap, fmt);
@@ -250,7 +253,7 @@ cstg_ctx* cstg_create(int device, int* status) {
   ctx->stream = ctx->own;
   ok = ok && ensure(ctx, ctx->err_word, sizeof(int) * kErrSlots) == 0 &&
        ensure(ctx, ctx->state, sizeof(PcgState)) == 0 &&
-       ensure(ctx, ctx->partials, sizeof(double) * 4 * kReduceBlocks) == 0 &&
+       ensure(ctx, ctx->partials, sizeof(double) * 4 * kMaxGrid) == 0 &&
        cudaMemsetAsync(ctx->state.p, 0, sizeof(PcgState), ctx->stream) == cudaSuccess &&
        cudaStreamSynchronize(ctx->stream) == cudaSuccess;
   if (!ok) {
@@ -578,6 +581,8 @@ int cstg_multiply_device(cstg_ctx* ctx, const double* d_x, double* d_y) {
   if (!ctx->kind || !ctx->has_values) return fail(ctx, CSTG_ERR_STATE, "multiply: no matrix");
   if (ctx->n_rows && (!d_x || !d_y))
     return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "multiply: null vector");
+  if (!aligned16(d_x) || !aligned16(d_y))
+    return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "multiply: device vectors must be 16-byte aligned");
   return spmv(ctx, d_x, d_y);  // asynchronous: ordered on the context's stream
 }
 
@@ -776,6 +781,8 @@ int cstg_pcg_solve_device(cstg_ctx* ctx, const double* d_b, double* d_x, const c
   int rc = check_solve_args(ctx, opt, o);
   if (rc) return rc;
   if (ctx->n_rows && (!d_b || !d_x)) return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "pcg_solve: null vector");
+  if (!aligned16(d_b) || !aligned16(d_x))
+    return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "pcg_solve: device vectors must be 16-byte aligned");
   return run_solve(ctx, d_b, d_x, o, stats, d_history, false);
 }
 

@@ -13,7 +13,9 @@ namespace cstg {
 constexpr int kSMs = 148;
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
-constexpr int kReduceBlocks = kSMs * 4;  // blocks of the vector / SpMV kernels
+// Largest grid of the reduction kernels (their partial-sum buffers hold 4 x kMaxGrid doubles).
+// The actual grid is one full wave: SMs x resident blocks per SM (occupancy calculator).
+constexpr int kMaxGrid = 2048;
 
 // Largest node neighbourhood (self included) the pattern builder accepts.
 constexpr int kMaxNeighbours = 64;

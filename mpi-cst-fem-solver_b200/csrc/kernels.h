@@ -101,7 +101,7 @@ struct PcgBuffers {
   double* Ap = nullptr;
   const double* inv_diag = nullptr;
   const double* b = nullptr;
-  double* partials = nullptr;  // 4 * kReduceBlocks doubles
+  double* partials = nullptr;  // 4 * kMaxGrid doubles
   double* history = nullptr;   // max_iter + 1 or null
   PcgState* st = nullptr;
   int* err = nullptr;

@@ -11,7 +11,7 @@
 // its matrix, right-hand side and solution.
 //
 // The array holds at most CSTG_STATIC_MAX_ROWS rows (65,536: 4 vectors of 512 KiB plus
-// about 19 KiB of partial sums and state, 2.02 MiB in all). Every GPU that loads the library
+// about 65 KiB of partial sums and state, 2.06 MiB in all). Every GPU that loads the library
 // holds it until the process exits. All calls in the process share it, so two calls whose
 // work overlaps on a GPU (other threads, other streams) race and corrupt each other's
 // results; callers serialise them.
@@ -33,7 +33,7 @@ namespace {
 
 constexpr size_t kStateBytes = 256;                                // PcgState
 constexpr size_t kErrBytes = 256;                                  // error word (int[8])
-constexpr size_t kPartialBytes = sizeof(double) * 4 * kReduceBlocks;  // 18,944 B
+constexpr size_t kPartialBytes = sizeof(double) * 4 * kMaxGrid;  // 64 KiB
 constexpr size_t kVecBytes = sizeof(double) * (size_t)CSTG_STATIC_MAX_ROWS;
 constexpr size_t kScratchBytes = kStateBytes + kErrBytes + kPartialBytes + 4 * kVecBytes;
 static_assert(sizeof(PcgState) <= kStateBytes, "state slot too small");
@@ -96,6 +96,9 @@ extern "C" int cstg_pcg_solve_static(int n_rows, const int32_t* d_row_ptr, const
                     CSTG_STATIC_MAX_ROWS);
   if (n_rows > 0 && (!d_row_ptr || !d_cols || !d_vals || !d_b || !d_x))
     return fail_msg(stats, CSTG_ERR_INVALID_ARGUMENT, "pcg_solve_static: null array");
+  if (((reinterpret_cast<uintptr_t>(d_b) | reinterpret_cast<uintptr_t>(d_x)) & 15u) != 0)
+    return fail_msg(stats, CSTG_ERR_INVALID_ARGUMENT,
+                    "pcg_solve_static: b and x must be 16-byte aligned device vectors");
   if (o.precision != CSTG_PRECISION_FP64 || o.record_history || !(o.rtol >= 0.0) || o.max_iter < 0 ||
       o.max_refinements < 0 || o.check_interval < 0)
     return fail_msg(stats, CSTG_ERR_UNSUPPORTED,
