@@ -53,8 +53,11 @@ extern "C" {
 
 /* precision / method of cstg_pcg_solve */
 #define CSTG_PRECISION_FP64 0         /* plain FP64 Jacobi-PCG, the reference's arithmetic     */
-#define CSTG_PRECISION_MIXED 1        /* FP32 SpMV + preconditioner, FP64 scalars/accumulation,
-                                         FP64 true-residual replacement (iterative refinement) */
+#define CSTG_PRECISION_MIXED 1        /* FP32 SpMV matrix (difference form) with FP64
+                                         accumulation, FP64 vectors and scalars, FP64
+                                         true-residual replacement (reliable updates); the
+                                         solve stops on the FP64 true residual. Mesh pattern
+                                         matrices only. */
 
 typedef struct cstg_ctx cstg_ctx;
 
@@ -140,6 +143,11 @@ int cstg_apply_dirichlet_device(cstg_ctx* ctx, int n_fixed, const int32_t* d_dof
  * the context's stream (the caller orders / synchronises). */
 int cstg_multiply(cstg_ctx* ctx, const double* x, double* y);
 int cstg_multiply_device(cstg_ctx* ctx, const double* d_x, double* d_y);
+/* The SpMV of the mixed-precision solver (no reference counterpart): y = K x with K's
+ * off-diagonal 2x2 blocks stored in FP32 in difference form, (K x)_n = sum_{m != n} K_nm (x_m -
+ * x_n) + S_n x_n, S_n the FP64 row-block sum; FP64 x and y, FP64 accumulation. Needs the mesh
+ * pattern and cstg_pcg_setup; enqueued on the context's stream. */
+int cstg_multiply_mixed_device(cstg_ctx* ctx, const double* d_x, double* d_y);
 
 /* ---- CgJacobiSolver::setup (solver.hpp:134, solver.cpp:133-148) ----------------------------
  * inv_diag = 1 / K_ii; CSTG_ERR_NONPOSITIVE_DIAGONAL names the first such row. */

@@ -22,6 +22,9 @@ using namespace cstg;
 namespace {
 
 constexpr int kErrNone = 0x7f7f7f7f;  // memset(0x7f) sentinel of the device error word
+// Mixed precision: a reliable update replaces the FP32 recursive residual by the FP64 one when
+// it has dropped by this factor since the last update (~one replacement per decade).
+constexpr double kReliableDelta = 0.1;
 
 struct DevBuf {
   void* p = nullptr;
@@ -64,9 +67,13 @@ struct cstg_ctx {
 
   // solver
   DevBuf b_in, x, r, p, Ap, inv_diag, partials, state, err_word, hist, vec_in, vec_out, stress;
+  // mixed precision: FP32 difference-form operator and FP32 work vectors
+  DevBuf val32, nbr32, S32;
+  bool mixed_ready = false;
   cudaGraphExec_t graph = nullptr;
   unsigned long long graph_gen = ~0ull;
-  int graph_chunk = 0, graph_hist = -1, graph_kind = -1, graph_n = -1;
+  int graph_chunk = 0, graph_hist = -1, graph_kind = -1, graph_n = -1, graph_prec = -1, graph_refs = -1;
+  const double* graph_b = nullptr;
 };
 
 namespace {
@@ -276,7 +283,7 @@ void cstg_destroy(cstg_ctx* ctx) {
                    &ctx->ubar,    &ctx->dofs,   &ctx->dvals,    &ctx->b_in,     &ctx->x,
                    &ctx->r,       &ctx->p,      &ctx->Ap,       &ctx->inv_diag, &ctx->partials,
                    &ctx->state,   &ctx->err_word, &ctx->hist,   &ctx->vec_in,   &ctx->vec_out,
-                   &ctx->stress};
+                   &ctx->stress,    &ctx->val32,  &ctx->nbr32,    &ctx->S32};
   for (DevBuf* b : all) free_buf(*b);
   if (ctx->h_err) cudaFreeHost(ctx->h_err);
   if (ctx->h_state) cudaFreeHost(ctx->h_state);
@@ -619,6 +626,7 @@ int cstg_pcg_setup(cstg_ctx* ctx) {
                 ctx->h_err[kErrDiag]);
   }
   ctx->setup_done = true;
+  ctx->mixed_ready = false;  // the FP32 operator is rebuilt from this matrix on first use
   return CSTG_OK;
 }
 
@@ -628,6 +636,45 @@ static int snapshot(cstg_ctx* ctx) {
   CK(cudaMemcpyAsync(ctx->h_state, ctx->state.p, sizeof(PcgState), cudaMemcpyDeviceToHost,
                      ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
+  return CSTG_OK;
+}
+
+// The FP32 difference-form operator of the current matrix (built once per setup).
+static int ensure_mixed(cstg_ctx* ctx) {
+  const int N = ctx->n_nodes;
+  const size_t noff = (size_t)(ctx->nnz / 4) - (size_t)N;
+  ENSURE(ctx->val32, sizeof(float4) * noff);
+  ENSURE(ctx->nbr32, sizeof(int) * noff);
+  ENSURE(ctx->S32, sizeof(double2) * 2 * (size_t)N);
+  if (!ctx->mixed_ready) {
+    CK(launch_make_mixed(N, buf_ptr<int>(ctx->node_ptr), buf_ptr<int>(ctx->bnbr), buf_ptr<double>(ctx->vals),
+                         buf_ptr<float4>(ctx->val32), buf_ptr<int>(ctx->nbr32), buf_ptr<double2>(ctx->S32),
+                         ctx->stream));
+    ctx->mixed_ready = true;
+  }
+  return CSTG_OK;
+}
+
+static MixedMatrix mixed_view(cstg_ctx* ctx) {
+  MixedMatrix mm;
+  mm.n_nodes = ctx->n_nodes;
+  mm.node_ptr = buf_ptr<int>(ctx->node_ptr);
+  mm.nbr32 = buf_ptr<int>(ctx->nbr32);
+  mm.val32 = buf_ptr<float4>(ctx->val32);
+  mm.S64 = buf_ptr<double2>(ctx->S32);
+  return mm;
+}
+
+int cstg_multiply_mixed_device(cstg_ctx* ctx, const double* d_x, double* d_y) {
+  BEGIN(ctx);
+  if (ctx->kind != 1 || !ctx->setup_done)
+    return fail(ctx, CSTG_ERR_STATE, "multiply_mixed: needs the mesh pattern and cstg_pcg_setup");
+  if (ctx->n_rows && (!d_x || !d_y)) return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "multiply_mixed: null vector");
+  if (!aligned16(d_x) || !aligned16(d_y))
+    return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "multiply_mixed: device vectors must be 16-byte aligned");
+  const int rc = ensure_mixed(ctx);
+  if (rc) return rc;
+  CK(launch_spmv_mixed(mixed_view(ctx), d_x, d_y, ctx->stream));
   return CSTG_OK;
 }
 
@@ -658,19 +705,49 @@ static int run_solve(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg_s
   const BlockMatrix* pbm = ctx->kind == 1 ? &bm : nullptr;
   const CsrMatrixDev* pcm = ctx->kind == 1 ? nullptr : &cm;
 
+  // mixed precision: FP32 difference-form operator built once per matrix (after setup)
+  const bool mixed = o.precision == CSTG_PRECISION_MIXED;
+  MixedBuffers mw;
+  MixedMatrix mm;
+  if (mixed) {
+    const int N = ctx->n_nodes;
+    const int rcm = ensure_mixed(ctx);
+    if (rcm) return rcm;
+    mm = mixed_view(ctx);
+    mw.n_nodes = N;
+    mw.x = w.x;
+    mw.b = d_b;
+    mw.inv_diag = w.inv_diag;
+    mw.r = w.r;
+    mw.p = w.p;
+    mw.Ap = w.Ap;
+    mw.partials = w.partials;
+    mw.history = w.history;
+    mw.st = w.st;
+  }
+  const long long per_iter = mixed ? 4 : 3;
+
   const int chunk = o.check_interval > 0 ? o.check_interval : 50;
-  // (Re)capture the chunk graph when a buffer or the shape changed.
+  // (Re)capture the chunk graph when a buffer, the shape or the method changed. The mixed
+  // graph reads b (reliable updates), so it is also tied to the right-hand-side pointer.
   if (!ctx->graph || ctx->graph_gen != ctx->generation || ctx->graph_chunk != chunk ||
-      ctx->graph_hist != (hist ? 1 : 0) || ctx->graph_kind != ctx->kind || ctx->graph_n != n) {
+      ctx->graph_hist != (hist ? 1 : 0) || ctx->graph_kind != ctx->kind || ctx->graph_n != n ||
+      ctx->graph_prec != o.precision || ctx->graph_refs != o.max_refinements ||
+      (mixed && ctx->graph_b != d_b)) {
     if (ctx->graph) {
       cudaGraphExecDestroy(ctx->graph);
       ctx->graph = nullptr;
     }
     cudaGraph_t g;
     CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-    for (int k = 0; k < chunk; ++k) launch_pcg_iteration(w, pbm, pcm, ctx->stream);
+    for (int k = 0; k < chunk; ++k) {
+      if (mixed)
+        launch_mixed_iteration(mw, mm, bm, o.max_refinements, ctx->stream);
+      else
+        launch_pcg_iteration(w, pbm, pcm, ctx->stream);
+    }
     CK(cudaStreamEndCapture(ctx->stream, &g));
-    count_launches(-3LL * chunk);  // captured, not run: counted per graph launch below
+    count_launches(-per_iter * chunk);  // captured, not run: counted per graph launch below
     const cudaError_t ie = cudaGraphInstantiate(&ctx->graph, g, 0);
     cudaGraphDestroy(g);
     CK(ie);
@@ -679,10 +756,16 @@ static int run_solve(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg_s
     ctx->graph_hist = hist ? 1 : 0;
     ctx->graph_kind = ctx->kind;
     ctx->graph_n = n;
+    ctx->graph_prec = o.precision;
+    ctx->graph_refs = o.max_refinements;
+    ctx->graph_b = d_b;
   }
 
   CK(cudaEventRecord(ctx->ev0, ctx->stream));
-  CK(launch_pcg_init(w, o.rtol, o.max_iter, hist, ctx->stream));
+  if (mixed)
+    CK(launch_mixed_init(mw, o.rtol, o.max_iter, hist, kReliableDelta, ctx->stream));
+  else
+    CK(launch_pcg_init(w, o.rtol, o.max_iter, hist, ctx->stream));
   long long spmv_calls = 0;
   int rc = snapshot(ctx);
   if (rc) return rc;
@@ -696,7 +779,7 @@ static int run_solve(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg_s
                     chunks);
       const int it0 = ctx->h_state->iter;
       CK(cudaGraphLaunch(ctx->graph, ctx->stream));
-      count_launches(3LL * chunk);
+      count_launches(per_iter * chunk);
       rc = snapshot(ctx);
       if (rc) return rc;
       spmv_calls += ctx->h_state->iter - it0 + (ctx->h_state->done == CSTG_SOLVE_BREAKDOWN + 1);
@@ -705,7 +788,8 @@ static int run_solve(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg_s
     rc = spmv(ctx, w.x, w.Ap);
     if (rc) return rc;
     ++spmv_calls;
-    CK(launch_true_residual(w, o.true_residual_stop != 0, o.max_refinements, ctx->stream));
+    // (the mixed method confirms convergence on the FP64 true residual itself)
+    CK(launch_true_residual(w, !mixed && o.true_residual_stop != 0, o.max_refinements, ctx->stream));
     rc = snapshot(ctx);
     if (rc) return rc;
     true_done = true;
@@ -732,14 +816,25 @@ static int run_solve(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg_s
     stats->rel_residual = s.rel;
     stats->true_rel_residual = true_done ? s.true_rel : 0.0;
     stats->solve_seconds = ms * 1e-3;
-    stats->spmv_calls = spmv_calls;
+    stats->spmv_calls = spmv_calls + (o.precision == CSTG_PRECISION_MIXED ? s.replace_count : 0);
     switch (s.done - 1) {
       case CSTG_SOLVE_ZERO_RHS:
         g_fmt(stats->message, sizeof stats->message, "zero right-hand side, x = 0");
         break;
       case CSTG_SOLVE_CONVERGED:
-        g_fmt(stats->message, sizeof stats->message, "converged in %d iterations, relative residual %g",
-              s.iter, s.rel);
+        if (mixed && s.fp64_mode)
+          g_fmt(stats->message, sizeof stats->message,
+                "converged in %d iterations, relative residual %g (FP64 true residual; %d reliable "
+                "updates; FP32 operator to iteration %d, then FP64)",
+                s.iter, s.rel, s.replace_count, s.fp64_switch_iter);
+        else if (mixed)
+          g_fmt(stats->message, sizeof stats->message,
+                "converged in %d iterations, relative residual %g (FP64 true residual; %d reliable "
+                "updates; FP32 operator throughout)",
+                s.iter, s.rel, s.replace_count);
+        else
+          g_fmt(stats->message, sizeof stats->message, "converged in %d iterations, relative residual %g",
+                s.iter, s.rel);
         break;
       case CSTG_SOLVE_BREAKDOWN:
         g_fmt(stats->message, sizeof stats->message,
@@ -769,8 +864,11 @@ static int check_solve_args(cstg_ctx* ctx, const cstg_solver_options* opt, cstg_
     return fail(ctx, CSTG_ERR_STATE, "cg_jacobi: solve() called before setup()");
   if (!(o.rtol >= 0.0) || o.max_iter < 0 || o.max_refinements < 0 || o.check_interval < 0)
     return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "pcg_solve: bad options");
-  if (o.precision != CSTG_PRECISION_FP64)
+  if (o.precision != CSTG_PRECISION_FP64 && o.precision != CSTG_PRECISION_MIXED)
     return fail(ctx, CSTG_ERR_UNSUPPORTED, "pcg_solve: precision %d not available", o.precision);
+  if (o.precision == CSTG_PRECISION_MIXED && ctx->kind != 1)
+    return fail(ctx, CSTG_ERR_UNSUPPORTED,
+                "pcg_solve: mixed precision needs the mesh (2x2-block) pattern of cstg_build_pattern");
   return CSTG_OK;
 }
 

@@ -55,15 +55,58 @@ struct alignas(128) PcgState {
   double true_rel; // ||b - A x|| / ||b||
   double rtol;
   double rr;       // r'r of the current iterate
-  double rmax;     // residual norm at the last reliable update (mixed precision)
+  double rmax;     // largest recursive residual norm since the last reliable update (mixed)
+  double rz_prev;  // r'z before the last update (mixed: beta after a reliable update)
+  double delta;    // reliable-update threshold (mixed)
   int iter;        // completed CG iterations
   int done;        // 0 running, else CSTG_SOLVE_* + 1
   int max_iter;
   int hist_on;
-  int restart_pending;
-  int replace_count;
+  int restart_pending;  // mixed: 1 reliable update due, 2 confirm convergence in FP64
+  int replace_count;    // residual replacements performed
+  int final_checks;     // mixed: FP64 confirmations that failed
+  int last_replace;     // mixed: iteration of the last reliable update
+  int cycle_limit;      // mixed: force a reliable update after this many iterations
+  int fp64_mode;        // mixed: the FP32 operator reached its accuracy floor; SpMV in FP64
+  int fp64_switch_iter; // mixed: iteration of that switch (0: none)
+  double best_true;     // mixed: smallest FP64 true residual seen at a reliable update
   unsigned int ticket[8];  // last-block tickets, one per kernel kind
 };
+static_assert(sizeof(PcgState) <= 256, "PcgState must fit its 256-byte slot");
+
+// Mixed-precision operator: FP32 off-diagonal 2x2 blocks + FP32 row-block sums (difference
+// form, see mixed_kernels.cu). Node n's off-diagonal blocks start at node_ptr[n] - n.
+struct MixedMatrix {
+  int n_nodes = 0;
+  const int* node_ptr = nullptr;
+  const int* nbr32 = nullptr;
+  const float4* val32 = nullptr;
+  const double2* S64 = nullptr;  // row-block sums in FP64: [2n] = (s00, s01), [2n+1] = (s10, s11)
+};
+
+struct MixedBuffers {
+  int n_nodes = 0;
+  double* x = nullptr;            // FP64 vectors (see mixed_kernels.cu for why)
+  const double* b = nullptr;
+  const double* inv_diag = nullptr;
+  double* r = nullptr;
+  double* p = nullptr;
+  double* Ap = nullptr;
+  double* partials = nullptr;
+  double* history = nullptr;
+  PcgState* st = nullptr;
+};
+
+// mixed_kernels.cu
+cudaError_t launch_make_mixed(int N, const int* node_ptr, const int* bnbr, const double* vals,
+                              float4* val32, int* nbr32, double2* S64, cudaStream_t s);
+cudaError_t launch_mixed_init(const MixedBuffers& w, double rtol, int max_iter, bool hist, double delta,
+                              cudaStream_t s);
+// One iteration: FP32 SpMV + p'Ap, update + reliable-update decision, the (usually idle)
+// FP64 replacement, p update.
+cudaError_t launch_mixed_iteration(const MixedBuffers& w, const MixedMatrix& A32, const BlockMatrix& A64,
+                                   int max_final_checks, cudaStream_t s);
+cudaError_t launch_spmv_mixed(const MixedMatrix& A32, const double* x, double* y, cudaStream_t s);
 
 // Process-wide count of kernel launches issued by this library (graph launches count every
 // kernel node they run).

@@ -80,6 +80,7 @@ _SIGS = {
     "cstg_apply_dirichlet_device": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp]),
     "cstg_multiply": (C.c_int, [_vp, _vp, _vp]),
     "cstg_multiply_device": (C.c_int, [_vp, _vp, _vp]),
+    "cstg_multiply_mixed_device": (C.c_int, [_vp, _vp, _vp]),
     "cstg_pcg_setup": (C.c_int, [_vp]),
     "cstg_pcg_solve": (C.c_int, [_vp, _vp, _vp, C.POINTER(SolverOptions), C.POINTER(Stats), _vp]),
     "cstg_pcg_solve_device": (C.c_int, [_vp, _vp, _vp, C.POINTER(SolverOptions), C.POINTER(Stats),

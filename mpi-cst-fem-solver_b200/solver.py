@@ -171,6 +171,17 @@ class GpuCsrMatrix:
         self.ctx.check(self.ctx.L.cstg_multiply(self.ctx.h, _ptr(x), _ptr(y)))
         return y
 
+    def multiply_mixed(self, x, y=None):
+        """y = K x with the mixed-precision SpMV (FP32 difference-form matrix, FP64 vectors and
+        accumulation); torch CUDA float64 tensors; needs the mesh pattern and a solver setup on
+        this matrix. Asynchronous on the context's stream."""
+        import torch
+        if not (_is_device(x) and x.dtype == torch.float64 and x.is_contiguous()):
+            raise CstgError(native.ERR_INVALID_ARGUMENT, "multiply_mixed: x must be a contiguous CUDA float64 tensor")
+        y = torch.empty_like(x) if y is None else y
+        self.ctx.check(self.ctx.L.cstg_multiply_mixed_device(self.ctx.h, _ptr(x), _ptr(y)))
+        return y
+
 
 def build_stiffness_pattern(mesh, ctx: Context | None = None) -> GpuCsrMatrix:
     """Sparsity pattern of K: one 2x2 block per pair of nodes sharing a triangle, self

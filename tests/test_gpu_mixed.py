@@ -1,0 +1,129 @@
+"""Mixed precision (FP32 difference-form SpMV and preconditioner, FP64 accumulation and
+scalars, FP64 true-residual reliable updates) against the reference's FP64 solution.
+
+Bar: converged on the FP64 TRUE residual (< rtol), displacements within relative 1e-8 of the
+reference's serial FP64 CG at rtol 1e-10 (the north star's bar), iterations at most 1.35x the
+FP64 count (the difference form keeps the FP32 penalty small)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+REL_TOL = 1e-8
+
+
+def _rel(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+def _mixed(rtol=1e-10, **kw):
+    import importlib
+    pkg = importlib.import_module("mpi-cst-fem-solver_b200")
+    return pkg.SolverOptions(rtol=rtol, precision="mixed", max_iter=200000, **kw)
+
+
+@pytest.mark.parametrize("name,plane", [("kirsch_L0", "stress"), ("kirsch_L1", "strain")])
+def test_mixed_kirsch_vs_reference(pkg, gpu_lib, golden, name, plane):
+    g = golden(name)
+    mesh = g.mesh(pkg)
+    K = pkg.build_stiffness_pattern(mesh)
+    pkg.assemble_stiffness(mesh, pkg.constitutive_matrix(210e9, 0.3, plane == "strain"), 0.01, K)
+    b = g[f"{plane}_f"].copy()
+    pkg.apply_dirichlet((g["dir_dofs"], g["dir_vals"]), K, b)
+    s = pkg.CgJacobiSolver(_mixed(record_history=True))
+    s.setup(K)
+    x = np.zeros(mesh.num_dofs)
+    st = s.solve(b, x)
+    assert st.converged and st.true_rel_residual < 1e-10, st.message
+    assert _rel(x, g[f"{plane}_u10"]) < REL_TOL
+    assert st.iterations <= 1.35 * g.meta[f"{plane}_iters10"]
+    assert st.refinements >= 1 and len(st.residual_history) == st.iterations + 1
+    K.ctx.close()
+
+
+def test_mixed_plate_and_repeat(pkg, gpu_lib, golden):
+    g = golden("plate_40x80")
+    p = pkg.plate.quarter_plate(40, 80)
+    K = pkg.build_stiffness_pattern(p)
+    pkg.assemble_stiffness(p, pkg.constitutive_matrix(1.0, 0.3), 1.0, K)
+    b = np.zeros(p.num_dofs)
+    pkg.add_traction(K, p.boundary_edges["right"], 1.0, 1.0, 0.0, b)
+    pkg.apply_dirichlet(pkg.plate.symmetry_dirichlet(p), K, b)
+    s = pkg.CgJacobiSolver(_mixed())
+    s.setup(K)
+    x1, x2 = np.zeros(p.num_dofs), np.zeros(p.num_dofs)
+    st1 = s.solve(b, x1)
+    st2 = s.solve(b, x2)  # the FP32 operator is reused; deterministic reductions: same bits
+    assert st1.converged and st1.true_rel_residual < 1e-10
+    assert np.array_equal(x1, x2) and st1.iterations == st2.iterations
+    assert _rel(x1, g["u"]) < REL_TOL
+    assert st1.iterations <= 1.35 * g.meta["iters"]
+    # zero right-hand side and max_iter behave like the FP64 solver
+    st0 = s.solve(np.zeros(p.num_dofs), x1)
+    assert st0.converged and st0.iterations == 0 and not x1.any()
+    s3 = pkg.CgJacobiSolver(pkg.SolverOptions(rtol=1e-10, precision="mixed", max_iter=5))
+    s3.setup(K)
+    st3 = s3.solve(b)
+    assert not st3.converged and st3.iterations == 5 and "NOT converged" in st3.message
+    K.ctx.close()
+
+
+def test_mixed_operator(pkg, gpu_lib):
+    """The FP32 difference-form SpMV agrees with the FP64 matrix to FP32 accuracy in proportion
+    to the local variation of x: exact on a rigid translation of the unconstrained matrix (zero
+    row sums), and on a smooth field its error is far below eps32 |K| |x|."""
+    import torch
+    p = pkg.plate.quarter_plate(30, 60)
+    K = pkg.build_stiffness_pattern(p)
+    pkg.assemble_stiffness(p, pkg.constitutive_matrix(1.0, 0.3), 1.0, K)
+    pkg.CgJacobiSolver().setup(K)
+    t = np.tile([1.0, 0.0], p.num_nodes)
+    y = K.multiply_mixed(torch.from_numpy(t).cuda())
+    torch.cuda.synchronize()
+    kmax = np.abs(K.download()[2]).max()
+    assert np.abs(y.cpu().numpy()).max() <= 1e-14 * kmax  # only the FP64 row-sum rounding remains
+    pkg.apply_dirichlet(pkg.plate.symmetry_dirichlet(p), K, np.zeros(p.num_dofs))
+    pkg.CgJacobiSolver().setup(K)
+    for x in (np.random.default_rng(3).standard_normal(p.num_dofs),
+              np.ravel(p.xy.reshape(-1, 2) ** 2 * [0.01, -0.02])):   # rough, then smooth
+        y64 = K.multiply(x)
+        ym = K.multiply_mixed(torch.from_numpy(x).cuda())
+        torch.cuda.synchronize()
+        err = np.abs(ym.cpu().numpy() - y64).max()
+        assert err <= 1e-6 * 14 * kmax * np.abs(x).max()
+    assert err <= 1e-8 * 14 * kmax * np.abs(x).max()  # smooth field: difference form pays off
+    K.ctx.close()
+
+
+def test_mixed_needs_mesh_pattern(pkg, gpu_lib):
+    A = pkg.GpuCsrMatrix.from_csr([0, 2, 4], [0, 1, 0, 1], [2.0, 1.0, 1.0, 3.0])
+    s = pkg.CgJacobiSolver(_mixed())
+    s.setup(A)
+    with pytest.raises(pkg.CstgError, match="mixed precision needs the mesh"):
+        s.solve(np.ones(2))
+    A.ctx.close()
+
+
+def test_mixed_on_2m_plate(pkg, gpu_lib):
+    p = pkg.plate.quarter_plate(565, 1766)
+    K = pkg.build_stiffness_pattern(p)
+    pkg.assemble_stiffness(p, pkg.constitutive_matrix(1.0, 0.3), 1.0, K)
+    b = np.zeros(p.num_dofs)
+    pkg.add_traction(K, p.boundary_edges["right"], 1.0, 1.0, 0.0, b)
+    pkg.apply_dirichlet(pkg.plate.symmetry_dirichlet(p), K, b)
+    s64 = pkg.CgJacobiSolver(pkg.SolverOptions(rtol=1e-10, max_iter=200000, true_residual_stop=True))
+    s64.setup(K)
+    x64 = np.zeros(p.num_dofs)
+    st64 = s64.solve(b, x64)
+    sm = pkg.CgJacobiSolver(_mixed())
+    sm.setup(K)
+    xm = np.zeros(p.num_dofs)
+    stm = sm.solve(b, xm)
+    assert stm.converged and stm.true_rel_residual < 1e-10
+    r = b - K.multiply(xm)
+    assert np.linalg.norm(r) / np.linalg.norm(b) < 1e-10
+    assert _rel(xm, x64) < REL_TOL
+    assert stm.iterations <= 1.35 * st64.iterations
+    print(f"2M plate: fp64 {st64.iterations} it {st64.solve_seconds:.3f} s, mixed {stm.iterations} it "
+          f"{stm.solve_seconds:.3f} s, rel diff {_rel(xm, x64):.2e}")
+    K.ctx.close()
