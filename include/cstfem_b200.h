@@ -73,8 +73,14 @@ typedef struct {
                                (recursive residual, solver.cpp:80-82)                      */
   int max_refinements;      /* cap on replacements/restarts when true_residual_stop (16)   */
   int check_interval;       /* iterations per device graph between host checks (0: auto)  */
-  int reserved[4];
+  int launch_mode;          /* CSTG_LAUNCH_*                                               */
+  int reserved[3];
 } cstg_solver_options;
+
+/* launch_mode of cstg_pcg_solve */
+#define CSTG_LAUNCH_AUTO 0        /* persistent kernel for mesh-pattern matrices, else graph  */
+#define CSTG_LAUNCH_PERSISTENT 1  /* one cooperative kernel runs all iterations (mesh pattern) */
+#define CSTG_LAUNCH_GRAPH 2       /* 3-4 kernels per iteration, chunks replayed as CUDA graphs */
 
 /* ≙ cstfem::SolverStats (include/cstfem/solver.hpp:99-107) plus counters. */
 typedef struct {

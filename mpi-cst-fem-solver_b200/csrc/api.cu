@@ -727,13 +727,16 @@ static int run_solve(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg_s
   }
   const long long per_iter = mixed ? 4 : 3;
 
-  const int chunk = o.check_interval > 0 ? o.check_interval : 50;
+  // Mesh-pattern matrices run as one persistent cooperative kernel per solve (unless the
+  // caller asks for the graph path); caller CSR matrices use the graph path.
+  const bool persist = ctx->kind == 1 && o.launch_mode != CSTG_LAUNCH_GRAPH;
+  const int chunk = persist ? o.max_iter + 1 : (o.check_interval > 0 ? o.check_interval : 50);
   // (Re)capture the chunk graph when a buffer, the shape or the method changed. The mixed
   // graph reads b (reliable updates), so it is also tied to the right-hand-side pointer.
-  if (!ctx->graph || ctx->graph_gen != ctx->generation || ctx->graph_chunk != chunk ||
+  if (!persist && (!ctx->graph || ctx->graph_gen != ctx->generation || ctx->graph_chunk != chunk ||
       ctx->graph_hist != (hist ? 1 : 0) || ctx->graph_kind != ctx->kind || ctx->graph_n != n ||
       ctx->graph_prec != o.precision || ctx->graph_refs != o.max_refinements ||
-      (mixed && ctx->graph_b != d_b)) {
+      (mixed && ctx->graph_b != d_b))) {
     if (ctx->graph) {
       cudaGraphExecDestroy(ctx->graph);
       ctx->graph = nullptr;
@@ -778,10 +781,16 @@ static int run_solve(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg_s
         return fail(ctx, CSTG_ERR_TIMEOUT, "pcg_solve: the device state did not finish after %lld chunks",
                     chunks);
       const int it0 = ctx->h_state->iter;
-      CK(cudaGraphLaunch(ctx->graph, ctx->stream));
-      count_launches(per_iter * chunk);
+      if (persist) {
+        CK(launch_pcg_persistent(w, bm, mixed ? &mm : nullptr, o.max_refinements, ctx->stream));
+      } else {
+        CK(cudaGraphLaunch(ctx->graph, ctx->stream));
+        count_launches(per_iter * chunk);
+      }
       rc = snapshot(ctx);
       if (rc) return rc;
+      if (ctx->h_state->done == CSTG_SOLVE_TIMEOUT + 1)
+        return fail(ctx, CSTG_ERR_TIMEOUT, "pcg_solve: a grid barrier of the persistent solve timed out");
       spmv_calls += ctx->h_state->iter - it0 + (ctx->h_state->done == CSTG_SOLVE_BREAKDOWN + 1);
     }
     // true residual (solver.cpp:117-122); with true_residual_stop it may re-open the solve

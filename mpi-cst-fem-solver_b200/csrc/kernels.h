@@ -70,6 +70,9 @@ struct alignas(128) PcgState {
   int fp64_mode;        // mixed: the FP32 operator reached its accuracy floor; SpMV in FP64
   int fp64_switch_iter; // mixed: iteration of that switch (0: none)
   double best_true;     // mixed: smallest FP64 true residual seen at a reliable update
+  unsigned int bar_count;  // persistent kernel: blocks arrived at the current grid barrier
+  unsigned int bar_gen;    // persistent kernel: barrier generation (bumped on release)
+  int bar_err;             // persistent kernel: a barrier wait ran out (the solve is abandoned)
   unsigned int ticket[8];  // last-block tickets, one per kernel kind
 };
 static_assert(sizeof(PcgState) <= 256, "PcgState must fit its 256-byte slot");
@@ -166,5 +169,10 @@ cudaError_t launch_spmv(const BlockMatrix* bm, const CsrMatrixDev* cm, const dou
 // With `restart`, also r = r_true, p = D^-1 r, rz, and done = 0 when the iteration may go on.
 cudaError_t launch_true_residual(const PcgBuffers& w, bool restart, int max_replacements,
                                  cudaStream_t s);
+
+// persistent.cu: every iteration of a mesh-pattern solve in one cooperative kernel (FP64, or
+// mixed when A32 is given); the state must be initialised (launch_pcg_init / launch_mixed_init).
+cudaError_t launch_pcg_persistent(const PcgBuffers& w, const BlockMatrix& A64, const MixedMatrix* A32,
+                                  int max_final_checks, cudaStream_t s);
 
 }  // namespace cstg

@@ -113,7 +113,6 @@ __global__ void k_make_mixed(int N, const int* __restrict__ node_ptr, const int*
 }
 
 // ---- FP32-matrix difference-form SpMV on FP64 vectors (+ p'Ap) -------------------------------
-// Same work split as the FP64 block SpMV: 8 lanes per node, two groups of four nodes per warp.
 // FP64 block SpMV of node groups (the FP64 path's loop) for the solve's last stretch after a
 // precision switch; returns this thread's share of p'Ap.
 __device__ __forceinline__ double spmv64_groups(const BlockMatrix& A, const double* __restrict__ x,
@@ -152,15 +151,16 @@ __device__ __forceinline__ double spmv64_groups(const BlockMatrix& A, const doub
   return dot;
 }
 
+// One thread per node: the node's off-diagonal blocks are one contiguous run of float4s, so a
+// warp reads 32 adjacent runs (~3 KB) through L1, and each thread keeps its six or so block
+// loads and x gathers in flight independently. (For FP32 blocks this beats the lane-per-block
+// split of the FP64 kernel, which is latency-bound at half the bytes per lane.)
 template <bool PCG>
 __global__ void __launch_bounds__(kThreads) k_spmv_mixed(MixedMatrix A, BlockMatrix A64,
                                                          const double* __restrict__ x,
                                                          double* __restrict__ y, double* partials,
                                                          PcgState* st) {
   if (PCG && __ldcg(&st->done)) return;
-  const int lane = threadIdx.x & 31, sub = lane >> 3, l8 = lane & 7;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nwarps = (gridDim.x * blockDim.x) >> 5;
   const double2* __restrict__ x2 = reinterpret_cast<const double2*>(x);
   int N = A.n_nodes;
   double dot = 0.0;
@@ -168,61 +168,24 @@ __global__ void __launch_bounds__(kThreads) k_spmv_mixed(MixedMatrix A, BlockMat
     dot = spmv64_groups(A64, x, y);
     N = 0;  // skip the FP32 loop below
   }
-  for (int base = warp * 8; base < N; base += nwarps * 8) {
-    const int n0 = base + sub, n1 = base + 4 + sub;
-    int o0 = 0, c0 = 0, o1 = 0, c1 = 0;
-    double2 xs0 = make_double2(0.0, 0.0), xs1 = xs0;
-    if (n0 < N) {
-      const int b = __ldg(&A.node_ptr[n0]);
-      o0 = b - n0;
-      c0 = __ldg(&A.node_ptr[n0 + 1]) - b - 1;
-      xs0 = x2[n0];
+  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < N; n += gridDim.x * blockDim.x) {
+    const int b = __ldg(&A.node_ptr[n]);
+    const int o = b - n, c = __ldg(&A.node_ptr[n + 1]) - b - 1;
+    const double2 xs = x2[n];
+    double ya = 0.0, yb = 0.0;
+    for (int k = 0; k < c; ++k) {
+      const int m = __ldg(&A.nbr32[o + k]);
+      const float4 a = __ldg(&A.val32[o + k]);
+      const double2 xm = x2[m];
+      const double dx = xm.x - xs.x, dy = xm.y - xs.y;
+      ya = fma((double)a.x, dx, fma((double)a.y, dy, ya));
+      yb = fma((double)a.z, dx, fma((double)a.w, dy, yb));
     }
-    if (n1 < N) {
-      const int b = __ldg(&A.node_ptr[n1]);
-      o1 = b - n1;
-      c1 = __ldg(&A.node_ptr[n1 + 1]) - b - 1;
-      xs1 = x2[n1];
-    }
-    double ya0 = 0.0, yb0 = 0.0, ya1 = 0.0, yb1 = 0.0;
-    const int cmax = max(c0, c1);
-    for (int k = l8; k < cmax; k += 8) {
-      const bool ok0 = k < c0, ok1 = k < c1;
-      const int m0 = ok0 ? __ldg(&A.nbr32[o0 + k]) : (n0 < N ? n0 : 0);
-      const int m1 = ok1 ? __ldg(&A.nbr32[o1 + k]) : (n1 < N ? n1 : 0);
-      const float4 a0 = ok0 ? __ldcs(&A.val32[o0 + k]) : make_float4(0.f, 0.f, 0.f, 0.f);
-      const float4 a1 = ok1 ? __ldcs(&A.val32[o1 + k]) : make_float4(0.f, 0.f, 0.f, 0.f);
-      const double2 xm0 = x2[m0], xm1 = x2[m1];
-      const double dx0 = xm0.x - xs0.x, dy0 = xm0.y - xs0.y;
-      const double dx1 = xm1.x - xs1.x, dy1 = xm1.y - xs1.y;
-      ya0 = fma((double)a0.x, dx0, fma((double)a0.y, dy0, ya0));
-      yb0 = fma((double)a0.z, dx0, fma((double)a0.w, dy0, yb0));
-      ya1 = fma((double)a1.x, dx1, fma((double)a1.y, dy1, ya1));
-      yb1 = fma((double)a1.z, dx1, fma((double)a1.w, dy1, yb1));
-    }
-#pragma unroll
-    for (int o = 4; o > 0; o >>= 1) {
-      ya0 += __shfl_xor_sync(kFull, ya0, o);
-      yb0 += __shfl_xor_sync(kFull, yb0, o);
-      ya1 += __shfl_xor_sync(kFull, ya1, o);
-      yb1 += __shfl_xor_sync(kFull, yb1, o);
-    }
-    if (l8 == 0) {
-      if (n0 < N) {
-        const double2 sa = __ldg(&A.S64[2 * n0]), sb = __ldg(&A.S64[2 * n0 + 1]);
-        ya0 = fma(sa.x, xs0.x, fma(sa.y, xs0.y, ya0));
-        yb0 = fma(sb.x, xs0.x, fma(sb.y, xs0.y, yb0));
-        st2(y, n0) = make_double2(ya0, yb0);
-        if (PCG) dot = fma(xs0.x, ya0, fma(xs0.y, yb0, dot));
-      }
-      if (n1 < N) {
-        const double2 sa = __ldg(&A.S64[2 * n1]), sb = __ldg(&A.S64[2 * n1 + 1]);
-        ya1 = fma(sa.x, xs1.x, fma(sa.y, xs1.y, ya1));
-        yb1 = fma(sb.x, xs1.x, fma(sb.y, xs1.y, yb1));
-        st2(y, n1) = make_double2(ya1, yb1);
-        if (PCG) dot = fma(xs1.x, ya1, fma(xs1.y, yb1, dot));
-      }
-    }
+    const double2 sa = __ldg(&A.S64[2 * n]), sb = __ldg(&A.S64[2 * n + 1]);
+    ya = fma(sa.x, xs.x, fma(sa.y, xs.y, ya));
+    yb = fma(sb.x, xs.x, fma(sb.y, xs.y, yb));
+    st2(y, n) = make_double2(ya, yb);
+    if (PCG) dot = fma(xs.x, ya, fma(xs.y, yb, dot));
   }
   if (!PCG) return;
   const double v[1] = {dot};

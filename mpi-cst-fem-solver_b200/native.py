@@ -49,7 +49,12 @@ class SolverOptions(C.Structure):
     _fields_ = [("rtol", C.c_double), ("max_iter", C.c_int), ("record_history", C.c_int),
                 ("precision", C.c_int), ("true_residual_stop", C.c_int),
                 ("max_refinements", C.c_int), ("check_interval", C.c_int),
-                ("reserved", C.c_int * 4)]
+                ("launch_mode", C.c_int), ("reserved", C.c_int * 3)]
+
+
+LAUNCH_AUTO = 0
+LAUNCH_PERSISTENT = 1
+LAUNCH_GRAPH = 2
 
 
 class Stats(C.Structure):

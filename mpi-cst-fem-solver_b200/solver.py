@@ -274,6 +274,7 @@ class SolverOptions:
     true_residual_stop: bool = False
     max_refinements: int = 16
     check_interval: int = 0
+    launch: str = "auto"  # "auto" | "persistent" | "graph"
 
     def native(self) -> native.SolverOptions:
         o = native.default_options()
@@ -284,6 +285,8 @@ class SolverOptions:
         o.true_residual_stop = int(self.true_residual_stop)
         o.max_refinements = self.max_refinements
         o.check_interval = self.check_interval
+        o.launch_mode = {"auto": native.LAUNCH_AUTO, "persistent": native.LAUNCH_PERSISTENT,
+                         "graph": native.LAUNCH_GRAPH}[self.launch]
         return o
 
 

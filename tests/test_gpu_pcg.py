@@ -185,3 +185,29 @@ def test_true_residual_stop_on_2m_plate(pkg, gpu_lib):
     scf, _ = pkg.scf_at_hole(es, 1.0)
     assert 3.0 < scf < 3.1
     K.ctx.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_persistent_matches_graph_path(pkg, gpu_lib, golden, precision):
+    """The persistent cooperative kernel (default for mesh matrices) and the graph-replayed
+    per-phase kernels run the same recurrence: same convergence, solutions within 1e-10."""
+    g = golden("plate_40x80")
+    p = pkg.plate.quarter_plate(40, 80)
+    K = pkg.build_stiffness_pattern(p)
+    pkg.assemble_stiffness(p, pkg.constitutive_matrix(1.0, 0.3), 1.0, K)
+    b = np.zeros(p.num_dofs)
+    pkg.add_traction(K, p.boundary_edges["right"], 1.0, 1.0, 0.0, b)
+    pkg.apply_dirichlet(pkg.plate.symmetry_dirichlet(p), K, b)
+    out = {}
+    for launch in ("graph", "persistent"):
+        s = pkg.CgJacobiSolver(pkg.SolverOptions(rtol=1e-10, precision=precision, launch=launch,
+                                                 record_history=True))
+        s.setup(K)
+        x = np.zeros(p.num_dofs)
+        out[launch] = (s.solve(b, x), x)
+    (sg, xg), (sp_, xp) = out["graph"], out["persistent"]
+    assert sg.converged and sp_.converged
+    assert abs(sg.iterations - sp_.iterations) <= 2
+    assert _rel(xp, xg) < 1e-10 and _rel(xp, g["u"]) < REL_TOL
+    assert len(sp_.residual_history) == sp_.iterations + 1
+    K.ctx.close()
