@@ -65,9 +65,11 @@ def parse():
     ap.add_argument("--cpu-sample-iters", type=int, default=150)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--only", choices=["spmv", "solve"], default=None,
+    ap.add_argument("--only", choices=["spmv", "solve", "batch"], default=None,
                     help="profiling modes: `spmv` runs --reps SpMV launches on the assembled plate, "
-                         "`solve` one full step; both print one JSON line")
+                         "`solve` one full step, `batch` the 64-plate x 4-load-case batched solve "
+                         "(every launch shape, autotuned, --reps graph replays, and the same systems "
+                         "solved one by one); each prints one JSON line")
     ap.add_argument("--reps", type=int, default=20)
     ap.add_argument("--max-iter", type=int, default=200000,
                     help="iteration cap of the solves (profiling captures use a small cap)")
@@ -285,6 +287,65 @@ def run_reference(a, dist: Dist):
 
 # ---- our arm --------------------------------------------------------------------------------------
 
+def run_batch(a, pkg):
+    """64 seeded plates (n_r 20..200, n_theta = 2 n_r) x 4 load cases: one batched persistent
+    launch (autotuned shape) against the same 256 systems solved one at a time."""
+    import torch
+    specs = pkg.plate.random_batch(count=64, seed=2026)
+    t0 = time.perf_counter()
+    batch = pkg.build_batch(specs)
+    solver = pkg.BatchSolver(pkg.SolverOptions(precision="mixed", max_iter=200000))
+    solver.setup(batch, device_rhs=True)
+    t_setup = time.perf_counter() - t0
+    print(f"batch setup {t_setup:.2f} s, {batch.mesh.num_dofs} DOFs", file=sys.stderr, flush=True)
+    shapes = {}
+    for c in (1, 2, 4, 8, 16):
+        for t in (256, 512):
+            try:
+                shapes[f"{c}x{t}"] = solver.solve(config=(c, t), device=True).seconds
+            except pkg.CstgError as e:
+                shapes[f"{c}x{t}"] = str(e)
+            print(f"shape {c}x{t}: {shapes[f'{c}x{t}']}", file=sys.stderr, flush=True)
+    t0 = time.perf_counter()
+    cfg, t_tune = solver.autotune(max_iter=300)
+    print(f"autotune {cfg} in {time.perf_counter() - t0:.2f} s", file=sys.stderr, flush=True)
+    times = [solver.solve(device=True).seconds for _ in range(a.reps)]
+    sol = solver.solve(device=True)
+    dofs = int(batch.mesh.num_dofs)
+    # the same systems one at a time through the single-system persistent solve
+    one, its_one = 0.0, 0
+    ctx = pkg.Context(0)
+    opts = pkg.SolverOptions(rtol=1e-10, max_iter=200000, precision="mixed", true_residual_stop=True)
+    for s, sp in enumerate(specs):
+        m = pkg.plate.quarter_plate(sp.n_r, sp.n_theta, a=sp.a)
+        K = pkg.build_stiffness_pattern(m, ctx=ctx)
+        pkg.assemble_stiffness(m, batch.D[s], 1.0, K)
+        sl = batch.dof_range(s)
+        bs = torch.from_numpy(np.ascontiguousarray(solver.b[:, sl])).to(0)
+        pkg.apply_dirichlet(pkg.plate.symmetry_dirichlet(m), K,
+                            torch.zeros(m.num_dofs, dtype=torch.float64, device=0))
+        cg = pkg.CgJacobiSolver(opts)
+        cg.setup(K)
+        x = torch.zeros(m.num_dofs, dtype=torch.float64, device=0)
+        for q in range(batch.n_cases):
+            st = cg.solve(bs[q].contiguous(), x)
+            one += st.solve_seconds
+            its_one += st.iterations
+    ctx.close()
+    out = {"mode": "batch", "workload": "64 plates (n_r 20..200, seed 2026) x 4 load cases",
+           "systems": batch.n_plates * batch.n_cases, "dofs_total": dofs, "dof_cases": dofs * batch.n_cases,
+           "setup_s": t_setup, "shapes_s": shapes, "autotuned": list(cfg), "tune_best_s": t_tune,
+           "batch_solve_s": statistics.median(times), "batch_solve_all_s": times,
+           "converged": int(np.sum(sol.converged)), "max_true_rel": float(sol.true_rel_residual.max()),
+           "iterations_total": int(sol.iterations.sum()), "iterations_max": int(sol.iterations.max()),
+           "fp64_switched_plates": int(np.sum(sol.fp64[:, 0])),
+           "refinements_total": int(sol.refinements.sum()),
+           "one_by_one_solve_s": one, "one_by_one_iterations": its_one,
+           "dof_cases_per_s": dofs * batch.n_cases / statistics.median(times)}
+    solver.close()
+    return out
+
+
 def run_ours(a, dist: Dist):
     import torch
     pkg = importlib.import_module("mpi-cst-fem-solver_b200")
@@ -342,7 +403,9 @@ def run_ours(a, dist: Dist):
     sync = torch.cuda.synchronize
     if a.only:
         out = {"mode": a.only, "workload": a.workload}
-        if a.only == "solve":
+        if a.only == "batch":
+            out = run_batch(a, pkg)
+        elif a.only == "solve":
             step()
             sync()
             out.update(iterations=last["st"].iterations, solve_s=last["st"].solve_seconds)

@@ -96,6 +96,26 @@ typedef struct {
   char warning[256];        /* SolverStats::warning (true residual > 10 rtol)               */
 } cstg_stats;
 
+/* ---- batched solves: launch shape and per-system results -------------------------------- */
+/* No reference counterpart. Launch shape of the batched persistent solve: each plate is solved
+ * by one thread-block cluster of `cluster_ctas` CTAs (1, 2, 4, 8 or 16) of `threads` threads
+ * (256 or 512). cluster_ctas == 0 means "not chosen" (the tuned or default shape is used). */
+typedef struct {
+  int cluster_ctas;
+  int threads;
+  int reserved[2];
+} cstg_batch_config;
+
+/* One per (system, load case), system-major: results[s * n_rhs + q]. */
+typedef struct {
+  int iterations;           /* CG iterations of this load case                          */
+  int status;               /* CSTG_SOLVE_*                                             */
+  int refinements;          /* FP64 residual replacements (reliable updates + checks)   */
+  int fp64;                 /* 1 when the system finished on the FP64 operator          */
+  double rel_residual;      /* recursive ||r|| / ||b|| at exit                          */
+  double true_rel_residual; /* FP64 ||b - A x|| / ||b|| at exit                         */
+} cstg_batch_result;
+
 /* ---- context --------------------------------------------------------------------------- */
 /* No reference counterpart (the reference keeps its state in caller objects). */
 cstg_ctx* cstg_create(int device, int* status);
@@ -124,6 +144,12 @@ int cstg_build_pattern(cstg_ctx* ctx, int64_t* nnz_out);
  * bit-identical to the reference (same FP64 operations, same per-entry summation order).
  * D is the 3x3 row-major constitutive matrix (constitutive_matrix, element.cpp:7-15). */
 int cstg_assemble(cstg_ctx* ctx, const double D[9], double thickness);
+/* assemble_stiffness for a mesh made of several disjoint parts with different materials
+ * (e.g. many plates concatenated for a batched solve): element e uses D[9 m .. 9 m + 8] and
+ * thickness[m], m = material_of_element[e] (host arrays). Each part's entries are bit-identical
+ * to assemble_stiffness (src/assembly.cpp:54-74) on that part alone. */
+int cstg_assemble_materials(cstg_ctx* ctx, int n_materials, const double* D, const double* thickness,
+                            const int32_t* material_of_element);
 
 /* ---- CSR access ----------------------------------------------------------------------------
  * cstg_get_csr copies the current matrix (pattern + values) to host arrays sized by
@@ -143,6 +169,13 @@ int cstg_apply_dirichlet(cstg_ctx* ctx, int n_fixed, const int32_t* dofs, const 
                          double* b_inout);
 int cstg_apply_dirichlet_device(cstg_ctx* ctx, int n_fixed, const int32_t* d_dofs,
                                 const double* d_values, double* d_b_inout);
+/* apply_dirichlet for n_rhs load vectors sharing K (b: n_rhs vectors of n_rows doubles, one
+ * after another): each vector gets exactly what a separate apply_dirichlet (bc.cpp:137-166)
+ * would give it; K is eliminated once. */
+int cstg_apply_dirichlet_multi(cstg_ctx* ctx, int n_fixed, const int32_t* dofs, const double* values,
+                               int n_rhs, double* b);
+int cstg_apply_dirichlet_multi_device(cstg_ctx* ctx, int n_fixed, const int32_t* d_dofs,
+                                      const double* d_values, int n_rhs, double* d_b);
 
 /* ---- LinearOperator::apply / CsrMatrix::multiply (solver.hpp:60-64, csr.cpp:19-26) ------
  * cstg_multiply returns when y is on the host; cstg_multiply_device only enqueues the SpMV on
@@ -201,6 +234,38 @@ int cstg_add_traction(cstg_ctx* ctx, int n_edges, const int32_t* edges, double t
 int cstg_pcg_solve_static(int n_rows, const int32_t* d_row_ptr, const int32_t* d_cols,
                           const double* d_vals, const double* d_b, double* d_x,
                           const cstg_solver_options* opt, cstg_stats* stats, void* stream);
+
+/* ---- batched Jacobi-PCG ------------------------------------------------------------------
+ * No counterpart in the reference (its driver solves one system per run, src/driver.cpp:164-188;
+ * a batch is what a caller gets by running that path once per plate and load case). The
+ * context's matrix must be block diagonal over the node ranges node_offsets[s] ..
+ * node_offsets[s+1] (0 = node_offsets[0] <= ... <= node_offsets[n_systems] = node count; no
+ * matrix entry couples two ranges, which is checked), set up with cstg_pcg_setup. All systems
+ * and all n_rhs load vectors (b: n_rhs vectors of n_rows doubles, one after another; x the
+ * same) are solved in one persistent launch: one thread-block cluster per system at a time,
+ * largest systems first, load cases in groups of up to four sharing each matrix read.
+ * opt->precision MIXED: FP32 difference-form SpMV with FP64 vectors and scalars; FP64: FP64
+ * SpMV. Every load case stops on the FP64 true residual ||b - A x|| <= rtol ||b|| (reliable
+ * updates replace the recursive residual by the FP64 one once per decade of reduction; a
+ * system switches to the FP64 operator when the FP32 one stops improving the true residual).
+ * max_iter and max_refinements apply per load case. `config` NULL: the shape from the last
+ * cstg_batch_autotune on this context, else 8 CTAs x 512 threads. The launches are captured
+ * once into a CUDA graph and replayed while the matrix, the vectors and the arguments are
+ * unchanged. `seconds` (optional): device time of the solve. Results in `results`
+ * (n_systems * n_rhs, system-major). */
+int cstg_batch_solve(cstg_ctx* ctx, int n_systems, const int32_t* node_offsets, int n_rhs,
+                     const double* b, double* x, const cstg_solver_options* opt,
+                     const cstg_batch_config* config, cstg_batch_result* results, double* seconds);
+int cstg_batch_solve_device(cstg_ctx* ctx, int n_systems, const int32_t* node_offsets, int n_rhs,
+                            const double* d_b, double* d_x, const cstg_solver_options* opt,
+                            const cstg_batch_config* config, cstg_batch_result* results,
+                            double* seconds);
+/* Times every feasible launch shape (cluster 1/2/4/8/16 CTAs x 256/512 threads) on this batch
+ * (device vectors; the solve runs with `opt`, e.g. a reduced max_iter to bound the tuning
+ * time), keeps the fastest for later cstg_batch_solve calls on this context and returns it. */
+int cstg_batch_autotune(cstg_ctx* ctx, int n_systems, const int32_t* node_offsets, int n_rhs,
+                        const double* d_b, double* d_x, const cstg_solver_options* opt,
+                        cstg_batch_config* best, double* best_seconds);
 
 #ifdef __cplusplus
 }

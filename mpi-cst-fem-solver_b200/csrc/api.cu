@@ -13,213 +13,10 @@
 #include <string>
 #include <vector>
 
-#include "../../include/cstfem_b200.h"
-#include "common.cuh"
-#include "kernels.h"
+#include "ctx.h"
 
 using namespace cstg;
 
-namespace {
-
-constexpr int kErrNone = 0x7f7f7f7f;  // memset(0x7f) sentinel of the device error word
-// Mixed precision: a reliable update replaces the FP32 recursive residual by the FP64 one when
-// it has dropped by this factor since the last update (~one replacement per decade).
-constexpr double kReliableDelta = 0.1;
-
-struct DevBuf {
-  void* p = nullptr;
-  size_t bytes = 0;
-};
-
-}  // namespace
-
-struct cstg_ctx {
-  int device = 0;
-  cudaStream_t own = nullptr;
-  cudaStream_t stream = nullptr;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  std::string err;
-  unsigned long long generation = 0;  // bumped whenever a device buffer moves
-
-  // pinned host staging: error word + state snapshot
-  int* h_err = nullptr;
-  PcgState* h_state = nullptr;
-
-  // mesh
-  int n_nodes = 0, n_tri = 0;
-  bool has_mesh = false, host_mesh = false;
-  std::vector<double> h_xy;
-  std::vector<int32_t> h_tri;
-  std::vector<int> h_ne_ptr, h_ne;  // host incidence for add_traction (built lazily)
-  DevBuf xy, tri;
-
-  // incidence + pattern
-  DevBuf cnt, cursor, ne_ptr, ne, scan_tmp, deg, node_ptr, bnbr, slot;
-  DevBuf row_ptr, cols, vals;
-  int kind = 0;  // 0 none, 1 mesh block pattern, 2 caller CSR
-  int n_rows = 0;
-  long long nnz = 0;
-  int csr_sub = 8;
-  bool has_values = false, setup_done = false;
-
-  // Dirichlet
-  DevBuf fixed, ubar, dofs, dvals;
-
-  // solver
-  DevBuf b_in, x, r, p, Ap, inv_diag, partials, state, err_word, hist, vec_in, vec_out, stress;
-  // mixed precision: FP32 difference-form operator and FP32 work vectors
-  DevBuf val32, nbr32, S32;
-  bool mixed_ready = false;
-  cudaGraphExec_t graph = nullptr;
-  unsigned long long graph_gen = ~0ull;
-  int graph_chunk = 0, graph_hist = -1, graph_kind = -1, graph_n = -1, graph_prec = -1, graph_refs = -1;
-  const double* graph_b = nullptr;
-};
-
-namespace {
-
-int fail(cstg_ctx* c, int code, const char* fmt, ...) {
-  char buf[512];
-  va_list ap;
-  va_start(ap, fmt);
-  std::vsnprintf(buf, sizeof buf, fmt, ap);
-  va_end(ap);
-  if (c) c->err = buf;
-  return code;
-}
-
-#define CK(call)                                                                           \
-  do {                                                                                     \
-    const cudaError_t e_ = (call);                                                         \
-    if (e_ != cudaSuccess)                                                                 \
-      return fail(ctx, CSTG_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_));            \
-  } while (0)
-
-template <class T>
-T* buf_ptr(DevBuf& b) {
-  return static_cast<T*>(b.p);
-}
-
-// Grow-only device buffer. Returns 0 or an error code.
-int ensure(cstg_ctx* ctx, DevBuf& b, size_t bytes) {
-  bytes = std::max<size_t>(bytes, 256);
-  if (b.bytes >= bytes) return CSTG_OK;
-  if (b.p) {
-    CK(cudaStreamSynchronize(ctx->stream));
-    CK(cudaFree(b.p));
-    b.p = nullptr;
-    b.bytes = 0;
-  }
-  CK(cudaMalloc(&b.p, bytes));
-  b.bytes = bytes;
-  ctx->generation++;
-  return CSTG_OK;
-}
-
-#define ENSURE(buf, bytes)                          \
-  do {                                              \
-    const int rc_ = ensure(ctx, (buf), (bytes));    \
-    if (rc_) return rc_;                            \
-  } while (0)
-
-void free_buf(DevBuf& b) {
-  if (b.p) cudaFree(b.p);
-  b.p = nullptr;
-  b.bytes = 0;
-}
-
-int begin(cstg_ctx* ctx) {
-  if (!ctx) return CSTG_ERR_INVALID_ARGUMENT;
-  ctx->err.clear();
-  CK(cudaSetDevice(ctx->device));
-  return CSTG_OK;
-}
-
-#define BEGIN(ctx)                 \
-  do {                             \
-    const int rb_ = begin(ctx);    \
-    if (rb_) return rb_;           \
-  } while (0)
-
-int reset_err(cstg_ctx* ctx) {
-  CK(cudaMemsetAsync(ctx->err_word.p, 0x7f, sizeof(int) * kErrSlots, ctx->stream));
-  return CSTG_OK;
-}
-
-// Copies the error word to the host and waits for the stream.
-int read_err(cstg_ctx* ctx) {
-  CK(cudaMemcpyAsync(ctx->h_err, ctx->err_word.p, sizeof(int) * kErrSlots, cudaMemcpyDeviceToHost,
-                     ctx->stream));
-  CK(cudaStreamSynchronize(ctx->stream));
-  return CSTG_OK;
-}
-
-#define RESET_ERR()                     \
-  do {                                  \
-    const int r_ = reset_err(ctx);      \
-    if (r_) return r_;                  \
-  } while (0)
-#define READ_ERR()                      \
-  do {                                  \
-    const int r_ = read_err(ctx);       \
-    if (r_) return r_;                  \
-  } while (0)
-
-// constitutive_matrix (element.cpp:7-15), host side, same operations.
-void constitutive(double E, double nu, int plane_strain, double D[9]) {
-  if (!plane_strain) {
-    const double c = E / (1.0 - nu * nu);
-    const double v[9] = {c, c * nu, 0.0, c * nu, c, 0.0, 0.0, 0.0, c * (1.0 - nu) / 2.0};
-    std::memcpy(D, v, sizeof v);
-  } else {
-    const double c = E / ((1.0 + nu) * (1.0 - 2.0 * nu));
-    const double v[9] = {c * (1.0 - nu), c * nu, 0.0, c * nu, c * (1.0 - nu), 0.0,
-                         0.0, 0.0, c * (1.0 - 2.0 * nu) / 2.0};
-    std::memcpy(D, v, sizeof v);
-  }
-}
-
-BlockMatrix block_view(cstg_ctx* ctx) {
-  BlockMatrix m;
-  m.n_nodes = ctx->n_nodes;
-  m.node_ptr = buf_ptr<int>(ctx->node_ptr);
-  m.bnbr = buf_ptr<int>(ctx->bnbr);
-  m.vals = buf_ptr<double>(ctx->vals);
-  return m;
-}
-
-CsrMatrixDev csr_view(cstg_ctx* ctx) {
-  CsrMatrixDev m;
-  m.n_rows = ctx->n_rows;
-  m.row_ptr = buf_ptr<int>(ctx->row_ptr);
-  m.cols = buf_ptr<int>(ctx->cols);
-  m.vals = buf_ptr<double>(ctx->vals);
-  m.sub = ctx->csr_sub;
-  return m;
-}
-
-int spmv(cstg_ctx* ctx, const double* x, double* y) {
-  if (ctx->kind == 1) {
-    const BlockMatrix bm = block_view(ctx);
-    CK(launch_spmv(&bm, nullptr, x, y, ctx->stream));
-  } else {
-    const CsrMatrixDev cm = csr_view(ctx);
-    CK(launch_spmv(nullptr, &cm, x, y, ctx->stream));
-  }
-  return CSTG_OK;
-}
-
-// The vector kernels load 16-byte pairs; caller device vectors must allow that.
-bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
-
-void g_fmt(char* out, size_t n, const char* fmt, ...) {
-  va_list ap;
-  va_start(ap, fmt);
-  std::vsnprintf(out, n, fmt, ap);
-  va_end(ap);
-}
-
-}  // namespace
 
 extern "C" {
 
@@ -277,13 +74,17 @@ void cstg_destroy(cstg_ctx* ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->graph) cudaGraphExecDestroy(ctx->graph);
+  if (ctx->bat_graph) cudaGraphExecDestroy(ctx->bat_graph);
   DevBuf* all[] = {&ctx->xy,      &ctx->tri,    &ctx->cnt,      &ctx->cursor,   &ctx->ne_ptr,
                    &ctx->ne,      &ctx->scan_tmp, &ctx->deg,    &ctx->node_ptr, &ctx->bnbr,
                    &ctx->slot,    &ctx->row_ptr, &ctx->cols,    &ctx->vals,     &ctx->fixed,
                    &ctx->ubar,    &ctx->dofs,   &ctx->dvals,    &ctx->b_in,     &ctx->x,
                    &ctx->r,       &ctx->p,      &ctx->Ap,       &ctx->inv_diag, &ctx->partials,
                    &ctx->state,   &ctx->err_word, &ctx->hist,   &ctx->vec_in,   &ctx->vec_out,
-                   &ctx->stress,    &ctx->val32,  &ctx->nbr32,    &ctx->S32};
+                   &ctx->stress,    &ctx->val32,  &ctx->nbr32,    &ctx->S32,      &ctx->mat,
+                   &ctx->mat_tab, &ctx->bat_sys, &ctx->bat_order, &ctx->bat_queue, &ctx->bat_b,
+                   &ctx->bat_x,   &ctx->bat_r,  &ctx->bat_p,    &ctx->bat_Ap,   &ctx->bat_stats,
+                   &ctx->bat_in,  &ctx->bat_out};
   for (DevBuf* b : all) free_buf(*b);
   if (ctx->h_err) cudaFreeHost(ctx->h_err);
   if (ctx->h_state) cudaFreeHost(ctx->h_state);
@@ -434,8 +235,45 @@ int cstg_assemble(cstg_ctx* ctx, const double D[9], double thickness) {
   std::memcpy(d.v, D, sizeof d.v);
   if (ctx->n_nodes)
     CK(launch_assemble(m, buf_ptr<int>(ctx->ne_ptr), buf_ptr<int>(ctx->ne), buf_ptr<int>(ctx->slot),
-                       buf_ptr<int>(ctx->node_ptr), d, thickness, buf_ptr<double>(ctx->vals),
-                       ctx->stream));
+                       buf_ptr<int>(ctx->node_ptr), d, thickness, nullptr, nullptr, nullptr,
+                       buf_ptr<double>(ctx->vals), ctx->stream));
+  ctx->has_values = true;
+  ctx->setup_done = false;
+  return CSTG_OK;
+}
+
+int cstg_assemble_materials(cstg_ctx* ctx, int n_materials, const double* D, const double* thickness,
+                            const int32_t* material_of_element) {
+  BEGIN(ctx);
+  if (n_materials < 1 || !D || !thickness || (ctx->n_tri > 0 && !material_of_element))
+    return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "assemble: bad material table");
+  if (ctx->kind != 1)
+    return fail(ctx, CSTG_ERR_STATE, "assemble: no mesh pattern (call cstg_build_pattern)");
+  for (int e = 0; e < ctx->n_tri; ++e)
+    if (material_of_element[e] < 0 || material_of_element[e] >= n_materials)
+      return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "assemble: element %d has material %d of %d", e,
+                  material_of_element[e], n_materials);
+  ENSURE(ctx->mat, sizeof(int) * (size_t)ctx->n_tri);
+  ENSURE(ctx->mat_tab, sizeof(double) * 10 * (size_t)n_materials);
+  double* tab = buf_ptr<double>(ctx->mat_tab);
+  if (ctx->n_tri)
+    CK(cudaMemcpyAsync(ctx->mat.p, material_of_element, sizeof(int) * (size_t)ctx->n_tri,
+                       cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(tab, D, sizeof(double) * 9 * (size_t)n_materials, cudaMemcpyHostToDevice,
+                     ctx->stream));
+  CK(cudaMemcpyAsync(tab + 9 * (size_t)n_materials, thickness, sizeof(double) * (size_t)n_materials,
+                     cudaMemcpyHostToDevice, ctx->stream));
+  MeshDev m;
+  m.n_nodes = ctx->n_nodes;
+  m.n_tri = ctx->n_tri;
+  m.xy = buf_ptr<double>(ctx->xy);
+  m.tri = buf_ptr<int>(ctx->tri);
+  Mat3 d{};
+  if (ctx->n_nodes)
+    CK(launch_assemble(m, buf_ptr<int>(ctx->ne_ptr), buf_ptr<int>(ctx->ne), buf_ptr<int>(ctx->slot),
+                       buf_ptr<int>(ctx->node_ptr), d, 0.0, buf_ptr<int>(ctx->mat), tab,
+                       tab + 9 * (size_t)n_materials, buf_ptr<double>(ctx->vals), ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));  // the host tables may go out of scope
   ctx->has_values = true;
   ctx->setup_done = false;
   return CSTG_OK;
@@ -509,12 +347,11 @@ int cstg_set_csr(cstg_ctx* ctx, int n, const int32_t* row_ptr, const int32_t* co
 
 // ---- apply_dirichlet -------------------------------------------------------------------------
 
-int cstg_apply_dirichlet_device(cstg_ctx* ctx, int n_fixed, const int32_t* d_dofs,
-                                const double* d_values, double* d_b) {
-  BEGIN(ctx);
+static int dirichlet_device(cstg_ctx* ctx, int n_fixed, const int32_t* d_dofs, const double* d_values,
+                            int n_rhs, double* d_b) {
   if (!ctx->kind || !ctx->has_values)
     return fail(ctx, CSTG_ERR_STATE, "apply_dirichlet: no assembled matrix");
-  if (n_fixed < 0 || (n_fixed > 0 && (!d_dofs || !d_values)) || (ctx->n_rows > 0 && !d_b))
+  if (n_fixed < 0 || n_rhs < 1 || (n_fixed > 0 && (!d_dofs || !d_values)) || (ctx->n_rows > 0 && !d_b))
     return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "apply_dirichlet: bad arguments");
   const int n = ctx->n_rows;
   ENSURE(ctx->fixed, (size_t)n);
@@ -522,7 +359,7 @@ int cstg_apply_dirichlet_device(cstg_ctx* ctx, int n_fixed, const int32_t* d_dof
   int* err = buf_ptr<int>(ctx->err_word);
   RESET_ERR();
   CK(launch_dirichlet(n, nullptr, nullptr, nullptr, n_fixed, d_dofs, d_values,
-                      buf_ptr<unsigned char>(ctx->fixed), buf_ptr<double>(ctx->ubar), nullptr, err,
+                      buf_ptr<unsigned char>(ctx->fixed), buf_ptr<double>(ctx->ubar), nullptr, 0, err,
                       ctx->stream, false));
   READ_ERR();
   if (ctx->h_err[kErrRange] != kErrNone) {
@@ -538,7 +375,7 @@ int cstg_apply_dirichlet_device(cstg_ctx* ctx, int n_fixed, const int32_t* d_dof
   }
   CK(launch_dirichlet(n, buf_ptr<int>(ctx->row_ptr), buf_ptr<int>(ctx->cols),
                       buf_ptr<double>(ctx->vals), n_fixed, d_dofs, d_values,
-                      buf_ptr<unsigned char>(ctx->fixed), buf_ptr<double>(ctx->ubar), d_b, err,
+                      buf_ptr<unsigned char>(ctx->fixed), buf_ptr<double>(ctx->ubar), d_b, n_rhs, err,
                       ctx->stream, true));
   ctx->setup_done = false;
   READ_ERR();
@@ -548,13 +385,24 @@ int cstg_apply_dirichlet_device(cstg_ctx* ctx, int n_fixed, const int32_t* d_dof
   return CSTG_OK;
 }
 
-int cstg_apply_dirichlet(cstg_ctx* ctx, int n_fixed, const int32_t* dofs, const double* values,
-                         double* b) {
+int cstg_apply_dirichlet_device(cstg_ctx* ctx, int n_fixed, const int32_t* d_dofs,
+                                const double* d_values, double* d_b) {
   BEGIN(ctx);
+  return dirichlet_device(ctx, n_fixed, d_dofs, d_values, 1, d_b);
+}
+
+int cstg_apply_dirichlet_multi_device(cstg_ctx* ctx, int n_fixed, const int32_t* d_dofs,
+                                      const double* d_values, int n_rhs, double* d_b) {
+  BEGIN(ctx);
+  return dirichlet_device(ctx, n_fixed, d_dofs, d_values, n_rhs, d_b);
+}
+
+static int dirichlet_host(cstg_ctx* ctx, int n_fixed, const int32_t* dofs, const double* values,
+                          int n_rhs, double* b) {
   if (!ctx->kind) return fail(ctx, CSTG_ERR_STATE, "apply_dirichlet: no assembled matrix");
-  if (n_fixed < 0 || (n_fixed > 0 && (!dofs || !values)) || (ctx->n_rows > 0 && !b))
+  if (n_fixed < 0 || n_rhs < 1 || (n_fixed > 0 && (!dofs || !values)) || (ctx->n_rows > 0 && !b))
     return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "apply_dirichlet: bad arguments");
-  const size_t n = (size_t)ctx->n_rows;
+  const size_t n = (size_t)ctx->n_rows * (size_t)n_rhs;
   ENSURE(ctx->dofs, sizeof(int) * (size_t)n_fixed);
   ENSURE(ctx->dvals, sizeof(double) * (size_t)n_fixed);
   ENSURE(ctx->b_in, sizeof(double) * n);
@@ -565,13 +413,13 @@ int cstg_apply_dirichlet(cstg_ctx* ctx, int n_fixed, const int32_t* dofs, const 
                        cudaMemcpyHostToDevice, ctx->stream));
   }
   if (n) CK(cudaMemcpyAsync(ctx->b_in.p, b, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
-  const int rc = cstg_apply_dirichlet_device(ctx, n_fixed, buf_ptr<int>(ctx->dofs),
-                                             buf_ptr<double>(ctx->dvals), buf_ptr<double>(ctx->b_in));
+  const int rc = dirichlet_device(ctx, n_fixed, buf_ptr<int>(ctx->dofs), buf_ptr<double>(ctx->dvals),
+                                  n_rhs, buf_ptr<double>(ctx->b_in));
   if (rc) {
     if (rc == CSTG_ERR_INVALID_ARGUMENT && ctx->err.find("out of range") != std::string::npos) {
       // report the DOF value from the host array
       for (int q = 0; q < n_fixed; ++q)
-        if (dofs[q] < 0 || dofs[q] >= (int)n)
+        if (dofs[q] < 0 || dofs[q] >= ctx->n_rows)
           return fail(ctx, rc, "apply_dirichlet: DOF %d out of range", dofs[q]);
     }
     return rc;
@@ -579,6 +427,18 @@ int cstg_apply_dirichlet(cstg_ctx* ctx, int n_fixed, const int32_t* dofs, const 
   if (n) CK(cudaMemcpyAsync(b, ctx->b_in.p, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   return CSTG_OK;
+}
+
+int cstg_apply_dirichlet(cstg_ctx* ctx, int n_fixed, const int32_t* dofs, const double* values,
+                         double* b) {
+  BEGIN(ctx);
+  return dirichlet_host(ctx, n_fixed, dofs, values, 1, b);
+}
+
+int cstg_apply_dirichlet_multi(cstg_ctx* ctx, int n_fixed, const int32_t* dofs, const double* values,
+                               int n_rhs, double* b) {
+  BEGIN(ctx);
+  return dirichlet_host(ctx, n_fixed, dofs, values, n_rhs, b);
 }
 
 // ---- multiply -----------------------------------------------------------------------------------
@@ -639,8 +499,10 @@ static int snapshot(cstg_ctx* ctx) {
   return CSTG_OK;
 }
 
+}  // extern "C"
+
 // The FP32 difference-form operator of the current matrix (built once per setup).
-static int ensure_mixed(cstg_ctx* ctx) {
+int cstg_host::ensure_mixed(cstg_ctx* ctx) {
   const int N = ctx->n_nodes;
   const size_t noff = (size_t)(ctx->nnz / 4) - (size_t)N;
   ENSURE(ctx->val32, sizeof(float4) * noff);
@@ -655,7 +517,7 @@ static int ensure_mixed(cstg_ctx* ctx) {
   return CSTG_OK;
 }
 
-static MixedMatrix mixed_view(cstg_ctx* ctx) {
+MixedMatrix cstg_host::mixed_view(cstg_ctx* ctx) {
   MixedMatrix mm;
   mm.n_nodes = ctx->n_nodes;
   mm.node_ptr = buf_ptr<int>(ctx->node_ptr);
@@ -664,6 +526,8 @@ static MixedMatrix mixed_view(cstg_ctx* ctx) {
   mm.S64 = buf_ptr<double2>(ctx->S32);
   return mm;
 }
+
+extern "C" {
 
 int cstg_multiply_mixed_device(cstg_ctx* ctx, const double* d_x, double* d_y) {
   BEGIN(ctx);

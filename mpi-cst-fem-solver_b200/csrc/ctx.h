@@ -1,0 +1,243 @@
+// Host-side context of the C ABI and the helpers every C-ABI file shares (device buffers,
+// error reporting with the reference's messages, error-word handling).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/cstfem_b200.h"
+#include "common.cuh"
+#include "kernels.h"
+
+using namespace cstg;
+
+namespace cstg_host {
+
+constexpr int kErrNone = 0x7f7f7f7f;  // memset(0x7f) sentinel of the device error word
+// Mixed precision: a reliable update replaces the FP32 recursive residual by the FP64 one when
+// it has dropped by this factor since the last update (~one replacement per decade).
+constexpr double kReliableDelta = 0.1;
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace cstg_host
+
+using cstg_host::DevBuf;
+
+struct cstg_ctx {
+  int device = 0;
+  cudaStream_t own = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::string err;
+  unsigned long long generation = 0;  // bumped whenever a device buffer moves
+
+  // pinned host staging: error word + state snapshot
+  int* h_err = nullptr;
+  PcgState* h_state = nullptr;
+
+  // mesh
+  int n_nodes = 0, n_tri = 0;
+  bool has_mesh = false, host_mesh = false;
+  std::vector<double> h_xy;
+  std::vector<int32_t> h_tri;
+  std::vector<int> h_ne_ptr, h_ne;  // host incidence for add_traction (built lazily)
+  DevBuf xy, tri;
+
+  // incidence + pattern
+  DevBuf cnt, cursor, ne_ptr, ne, scan_tmp, deg, node_ptr, bnbr, slot;
+  DevBuf row_ptr, cols, vals;
+  int kind = 0;  // 0 none, 1 mesh block pattern, 2 caller CSR
+  int n_rows = 0;
+  long long nnz = 0;
+  int csr_sub = 8;
+  bool has_values = false, setup_done = false;
+
+  // Dirichlet
+  DevBuf fixed, ubar, dofs, dvals;
+
+  // solver
+  DevBuf b_in, x, r, p, Ap, inv_diag, partials, state, err_word, hist, vec_in, vec_out, stress;
+  // mixed precision: FP32 difference-form operator and FP32 work vectors
+  DevBuf val32, nbr32, S32;
+  bool mixed_ready = false;
+  cudaGraphExec_t graph = nullptr;
+  unsigned long long graph_gen = ~0ull;
+  int graph_chunk = 0, graph_hist = -1, graph_kind = -1, graph_n = -1, graph_prec = -1, graph_refs = -1;
+  const double* graph_b = nullptr;
+
+  // multi-material assembly
+  DevBuf mat, mat_tab;
+
+  // batched solves: plate table, LPT order, interleaved load-case vectors, per-system results
+  DevBuf bat_sys, bat_order, bat_queue, bat_b, bat_x, bat_r, bat_p, bat_Ap, bat_stats, bat_in, bat_out;
+  std::vector<int32_t> bat_offsets;  // host copy of the last validated plate table
+  unsigned long long bat_checked_gen = ~0ull;
+  cstg_batch_config bat_cfg{};       // tuned launch shape (cluster_ctas == 0: not tuned)
+  cudaGraphExec_t bat_graph = nullptr;
+  unsigned long long bat_graph_key = 0;
+  long long bat_graph_launches = 0;  // kernel nodes per replay of bat_graph
+};
+
+namespace cstg_host {
+
+inline int fail(cstg_ctx* c, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (c) c->err = buf;
+  return code;
+}
+
+#define CK(call)                                                                           \
+  do {                                                                                     \
+    const cudaError_t e_ = (call);                                                         \
+    if (e_ != cudaSuccess)                                                                 \
+      return fail(ctx, CSTG_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_));            \
+  } while (0)
+
+template <class T>
+inline T* buf_ptr(DevBuf& b) {
+  return static_cast<T*>(b.p);
+}
+
+// Grow-only device buffer. Returns 0 or an error code.
+inline int ensure(cstg_ctx* ctx, DevBuf& b, size_t bytes) {
+  bytes = std::max<size_t>(bytes, 256);
+  if (b.bytes >= bytes) return CSTG_OK;
+  if (b.p) {
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaFree(b.p));
+    b.p = nullptr;
+    b.bytes = 0;
+  }
+  CK(cudaMalloc(&b.p, bytes));
+  b.bytes = bytes;
+  ctx->generation++;
+  return CSTG_OK;
+}
+
+#define ENSURE(buf, bytes)                          \
+  do {                                              \
+    const int rc_ = ensure(ctx, (buf), (bytes));    \
+    if (rc_) return rc_;                            \
+  } while (0)
+
+inline void free_buf(DevBuf& b) {
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.bytes = 0;
+}
+
+inline int begin(cstg_ctx* ctx) {
+  if (!ctx) return CSTG_ERR_INVALID_ARGUMENT;
+  ctx->err.clear();
+  CK(cudaSetDevice(ctx->device));
+  return CSTG_OK;
+}
+
+#define BEGIN(ctx)                 \
+  do {                             \
+    const int rb_ = begin(ctx);    \
+    if (rb_) return rb_;           \
+  } while (0)
+
+inline int reset_err(cstg_ctx* ctx) {
+  CK(cudaMemsetAsync(ctx->err_word.p, 0x7f, sizeof(int) * kErrSlots, ctx->stream));
+  return CSTG_OK;
+}
+
+// Copies the error word to the host and waits for the stream.
+inline int read_err(cstg_ctx* ctx) {
+  CK(cudaMemcpyAsync(ctx->h_err, ctx->err_word.p, sizeof(int) * kErrSlots, cudaMemcpyDeviceToHost,
+                     ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return CSTG_OK;
+}
+
+#define RESET_ERR()                     \
+  do {                                  \
+    const int r_ = reset_err(ctx);      \
+    if (r_) return r_;                  \
+  } while (0)
+#define READ_ERR()                      \
+  do {                                  \
+    const int r_ = read_err(ctx);       \
+    if (r_) return r_;                  \
+  } while (0)
+
+// constitutive_matrix (element.cpp:7-15), host side, same operations.
+inline void constitutive(double E, double nu, int plane_strain, double D[9]) {
+  if (!plane_strain) {
+    const double c = E / (1.0 - nu * nu);
+    const double v[9] = {c, c * nu, 0.0, c * nu, c, 0.0, 0.0, 0.0, c * (1.0 - nu) / 2.0};
+    std::memcpy(D, v, sizeof v);
+  } else {
+    const double c = E / ((1.0 + nu) * (1.0 - 2.0 * nu));
+    const double v[9] = {c * (1.0 - nu), c * nu, 0.0, c * nu, c * (1.0 - nu), 0.0,
+                         0.0, 0.0, c * (1.0 - 2.0 * nu) / 2.0};
+    std::memcpy(D, v, sizeof v);
+  }
+}
+
+inline BlockMatrix block_view(cstg_ctx* ctx) {
+  BlockMatrix m;
+  m.n_nodes = ctx->n_nodes;
+  m.node_ptr = buf_ptr<int>(ctx->node_ptr);
+  m.bnbr = buf_ptr<int>(ctx->bnbr);
+  m.vals = buf_ptr<double>(ctx->vals);
+  return m;
+}
+
+inline CsrMatrixDev csr_view(cstg_ctx* ctx) {
+  CsrMatrixDev m;
+  m.n_rows = ctx->n_rows;
+  m.row_ptr = buf_ptr<int>(ctx->row_ptr);
+  m.cols = buf_ptr<int>(ctx->cols);
+  m.vals = buf_ptr<double>(ctx->vals);
+  m.sub = ctx->csr_sub;
+  return m;
+}
+
+inline int spmv(cstg_ctx* ctx, const double* x, double* y) {
+  if (ctx->kind == 1) {
+    const BlockMatrix bm = block_view(ctx);
+    CK(launch_spmv(&bm, nullptr, x, y, ctx->stream));
+  } else {
+    const CsrMatrixDev cm = csr_view(ctx);
+    CK(launch_spmv(nullptr, &cm, x, y, ctx->stream));
+  }
+  return CSTG_OK;
+}
+
+// The vector kernels load 16-byte pairs; caller device vectors must allow that.
+inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+inline void g_fmt(char* out, size_t n, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(out, n, fmt, ap);
+  va_end(ap);
+}
+
+// Defined in api.cu: the FP32 difference-form operator of the current matrix.
+int ensure_mixed(cstg_ctx* ctx);
+MixedMatrix mixed_view(cstg_ctx* ctx);
+
+}  // namespace cstg_host
+
+using namespace cstg_host;

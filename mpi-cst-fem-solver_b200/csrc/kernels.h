@@ -14,6 +14,7 @@ enum ErrSlot {
   kErrConflict = 3,    // Dirichlet DOF given two different values
   kErrDiag = 4,        // non-positive diagonal (Dirichlet row or Jacobi setup)
   kErrTimeout = 5,     // bounded device wait gave up
+  kErrBatch = 6,       // batched solve: a node coupled to a node of another plate
   kErrSlots = 8
 };
 
@@ -111,6 +112,38 @@ cudaError_t launch_mixed_iteration(const MixedBuffers& w, const MixedMatrix& A32
                                    int max_final_checks, cudaStream_t s);
 cudaError_t launch_spmv_mixed(const MixedMatrix& A32, const double* x, double* y, cudaStream_t s);
 
+// batch.cu: one result per (plate, load case); the layout of cstg_batch_result.
+struct BatchResultDev {
+  int iterations, status, refinements, fp64;
+  double rel, true_rel;
+};
+
+struct BatchArgs {
+  int n_sys = 0;
+  const int* sys_node = nullptr;  // [n_sys + 1] first node of each plate
+  const int* order = nullptr;     // [n_sys] plates, largest first (the work queue's order)
+  int* queue = nullptr;           // work counter, zero at launch
+  MixedMatrix A32;                // FP32 difference-form operator (unused when start_fp64)
+  BlockMatrix A64;                // FP64 operator (true residuals, FP64 mode)
+  int start_fp64 = 0;
+  const double* inv_diag = nullptr;
+  const double* b = nullptr;      // [N][R][2]
+  double *x = nullptr, *r = nullptr, *p = nullptr, *Ap = nullptr;
+  double rtol = 1e-10;
+  int max_iter = 0, max_refine = 0;
+  BatchResultDev* res = nullptr;
+  int res_stride = 0, res_offset = 0;  // result index = plate * res_stride + res_offset + q
+};
+cudaError_t batch_max_clusters(int R, int cluster, int threads, int* n);
+cudaError_t launch_batch_pcg(const BatchArgs& a, int R, int cluster, int threads, int n_clusters,
+                             cudaStream_t s);
+cudaError_t launch_batch_pack(int N, int R, int q0, long long ld, const double* src, double* dst,
+                              cudaStream_t s);
+cudaError_t launch_batch_unpack(int N, int R, int q0, long long ld, const double* src, double* dst,
+                                cudaStream_t s);
+cudaError_t launch_batch_check(int N, int n_sys, const int* sys_node, const int* node_ptr, const int* bnbr,
+                               int* err, cudaStream_t s);
+
 // Process-wide count of kernel launches issued by this library (graph launches count every
 // kernel node they run).
 void count_launches(long long k);
@@ -127,12 +160,12 @@ cudaError_t launch_pattern_fill(const MeshDev& m, const int* ne_ptr, const int* 
                                 const int* node_ptr, int* bnbr, int* slot, int* row_ptr,
                                 int* cols, cudaStream_t s);
 cudaError_t launch_assemble(const MeshDev& m, const int* ne_ptr, const int* ne, const int* slot,
-                            const int* node_ptr, const Mat3& D, double t, double* vals,
-                            cudaStream_t s);
+                            const int* node_ptr, const Mat3& D, double t, const int* mat,
+                            const double* Dtab, const double* ttab, double* vals, cudaStream_t s);
 cudaError_t launch_dirichlet(int n_rows, const int* row_ptr, const int* cols, double* vals,
                              int n_fixed, const int* dofs, const double* values,
-                             unsigned char* fixed, double* ubar, double* b, int* err,
-                             cudaStream_t s, bool apply);
+                             unsigned char* fixed, double* ubar, double* b, int n_rhs,
+                             int* err, cudaStream_t s, bool apply);
 cudaError_t launch_inv_diag(int n_rows, const int* row_ptr, const int* cols, const double* vals,
                             double* inv_diag, int* err, cudaStream_t s);
 cudaError_t launch_element_stresses(const MeshDev& m, const double* u, const Mat3& D, double nu,

@@ -319,14 +319,17 @@ __device__ __forceinline__ double ke_entry(const CstB& o, int i, int j) {
 // One thread per node: the node's two rows are zeroed, then every incident element (in
 // ascending element order) adds its 2 x 6 slice of Ke. Each CSR entry therefore receives
 // its contributions in the reference's order (assembly.cpp:56-72), starting from 0.0.
+// With a material table (`mat` non-null: element e uses D = Dtab[9 mat[e] ..], t = ttab[mat[e]]),
+// disjoint plates of different materials assemble in one launch; each plate's entries are then
+// exactly what assemble_stiffness gives for that plate alone.
 __global__ void __launch_bounds__(128) k_assemble(
     int n_nodes, const double* __restrict__ xy, const int* __restrict__ tri,
     const int* __restrict__ ne_ptr, const int* __restrict__ ne, const int* __restrict__ slot,
     const int* __restrict__ node_ptr, const Mat3 Dm, double thickness,
+    const int* __restrict__ mat, const double* __restrict__ Dtab, const double* __restrict__ ttab,
     double* __restrict__ vals) {
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= n_nodes) return;
-  const double* D = Dm.v;
   const int b0 = node_ptr[n], deg = node_ptr[n + 1] - b0;
   double* ra = vals + 4L * b0;
   double* rb = ra + 2 * deg;
@@ -341,7 +344,12 @@ __global__ void __launch_bounds__(128) k_assemble(
       exy[2 * c + 1] = xy[2 * v + 1];
     }
     CstB o;
-    cst_element(exy, D, thickness, o);
+    if (mat) {
+      const int mi = mat[e];
+      cst_element(exy, Dtab + 9 * mi, ttab[mi], o);
+    } else {
+      cst_element(exy, Dm.v, thickness, o);
+    }
 #pragma unroll
     for (int b = 0; b < 3; ++b) {
       const int k = slot[3 * q + b] - b0;
@@ -398,10 +406,14 @@ __device__ __forceinline__ int find_col(const int* __restrict__ cols, int lo, in
 
 // One thread per row; the row's entries are visited in ascending position, so b_i receives
 // its corrections in the reference's order.
+// Several load vectors sharing K (n_rhs vectors, `ld` doubles apart) are eliminated in one
+// pass: each b receives exactly the corrections a separate apply_dirichlet would give it, and
+// K is zeroed once, after every vector has read the entries.
 __global__ void k_dir_apply(int n_rows, const int* __restrict__ row_ptr,
                             const int* __restrict__ cols, double* __restrict__ vals,
                             const unsigned char* __restrict__ fixed,
-                            const double* __restrict__ ubar, double* __restrict__ b, int* err) {
+                            const double* __restrict__ ubar, double* __restrict__ b, int n_rhs,
+                            long long ld, int* err) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n_rows) return;
   const int lo = row_ptr[i], hi = row_ptr[i + 1];
@@ -414,17 +426,18 @@ __global__ void k_dir_apply(int n_rows, const int* __restrict__ row_ptr,
     }
     for (int k = lo; k < hi; ++k)
       if (cols[k] != i) vals[k] = 0.0;
-    b[i] = __dmul_rn(diag, ubar[i]);
+    for (int q = 0; q < n_rhs; ++q) b[q * ld + i] = __dmul_rn(diag, ubar[i]);
   } else {
-    double bi = b[i];
-    for (int k = lo; k < hi; ++k) {
-      const int c = cols[k];
-      if (fixed[c]) {
-        bi = __dsub_rn(bi, __dmul_rn(vals[k], ubar[c]));
-        vals[k] = 0.0;
+    for (int q = 0; q < n_rhs; ++q) {
+      double bi = b[q * ld + i];
+      for (int k = lo; k < hi; ++k) {
+        const int c = cols[k];
+        if (fixed[c]) bi = __dsub_rn(bi, __dmul_rn(vals[k], ubar[c]));
       }
+      b[q * ld + i] = bi;
     }
-    b[i] = bi;
+    for (int k = lo; k < hi; ++k)
+      if (fixed[cols[k]]) vals[k] = 0.0;
   }
 }
 
@@ -530,18 +543,18 @@ cudaError_t launch_pattern_fill(const MeshDev& m, const int* ne_ptr, const int* 
 }
 
 cudaError_t launch_assemble(const MeshDev& m, const int* ne_ptr, const int* ne, const int* slot,
-                            const int* node_ptr, const Mat3& D, double t, double* vals,
-                            cudaStream_t s) {
+                            const int* node_ptr, const Mat3& D, double t, const int* mat,
+                            const double* Dtab, const double* ttab, double* vals, cudaStream_t s) {
   k_assemble<<<nblk(m.n_nodes, 128), 128, 0, s>>>(m.n_nodes, m.xy, m.tri, ne_ptr, ne, slot, node_ptr,
-                                                  D, t, vals);
+                                                  D, t, mat, Dtab, ttab, vals);
   count_launches(1);
   return cudaGetLastError();
 }
 
 cudaError_t launch_dirichlet(int n_rows, const int* row_ptr, const int* cols, double* vals,
                              int n_fixed, const int* dofs, const double* values,
-                             unsigned char* fixed, double* ubar, double* b, int* err,
-                             cudaStream_t s, bool apply) {
+                             unsigned char* fixed, double* ubar, double* b, int n_rhs,
+                             int* err, cudaStream_t s, bool apply) {
   if (!apply) {
     cudaMemsetAsync(fixed, 0, (size_t)n_rows, s);
     if (n_fixed) {
@@ -551,7 +564,8 @@ cudaError_t launch_dirichlet(int n_rows, const int* row_ptr, const int* cols, do
     }
   } else {
     if (n_rows)
-      k_dir_apply<<<nblk(n_rows, 128), 128, 0, s>>>(n_rows, row_ptr, cols, vals, fixed, ubar, b, err);
+      k_dir_apply<<<nblk(n_rows, 128), 128, 0, s>>>(n_rows, row_ptr, cols, vals, fixed, ubar, b, n_rhs,
+                                                    (long long)n_rows, err);
     count_launches(n_rows ? 1 : 0);
   }
   return cudaGetLastError();

@@ -65,6 +65,17 @@ class Stats(C.Structure):
                 ("warning", C.c_char * 256)]
 
 
+class BatchConfig(C.Structure):
+    """cstg_batch_config: CTAs per cluster (one cluster per plate) and threads per CTA."""
+    _fields_ = [("cluster_ctas", C.c_int), ("threads", C.c_int), ("reserved", C.c_int * 2)]
+
+
+class BatchResult(C.Structure):
+    """cstg_batch_result: one per (system, load case)."""
+    _fields_ = [("iterations", C.c_int), ("status", C.c_int), ("refinements", C.c_int),
+                ("fp64", C.c_int), ("rel_residual", C.c_double), ("true_rel_residual", C.c_double)]
+
+
 _vp = C.c_void_p
 _SIGS = {
     "cstg_version": (C.c_int, []),
@@ -94,6 +105,15 @@ _SIGS = {
     "cstg_add_traction": (C.c_int, [_vp, C.c_int, _vp, C.c_double, C.c_double, C.c_double, _vp]),
     "cstg_pcg_solve_static": (C.c_int, [C.c_int, _vp, _vp, _vp, _vp, _vp, C.POINTER(SolverOptions),
                                         C.POINTER(Stats), _vp]),
+    "cstg_assemble_materials": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp]),
+    "cstg_apply_dirichlet_multi": (C.c_int, [_vp, C.c_int, _vp, _vp, C.c_int, _vp]),
+    "cstg_apply_dirichlet_multi_device": (C.c_int, [_vp, C.c_int, _vp, _vp, C.c_int, _vp]),
+    "cstg_batch_solve": (C.c_int, [_vp, C.c_int, _vp, C.c_int, _vp, _vp, C.POINTER(SolverOptions),
+                                   C.POINTER(BatchConfig), _vp, C.POINTER(C.c_double)]),
+    "cstg_batch_solve_device": (C.c_int, [_vp, C.c_int, _vp, C.c_int, _vp, _vp, C.POINTER(SolverOptions),
+                                          C.POINTER(BatchConfig), _vp, C.POINTER(C.c_double)]),
+    "cstg_batch_autotune": (C.c_int, [_vp, C.c_int, _vp, C.c_int, _vp, _vp, C.POINTER(SolverOptions),
+                                      C.POINTER(BatchConfig), C.POINTER(C.c_double)]),
 }
 
 STATIC_MAX_ROWS = 65536  # CSTG_STATIC_MAX_ROWS

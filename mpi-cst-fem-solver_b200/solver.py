@@ -246,7 +246,9 @@ def apply_dirichlet(dofs, K: GpuCsrMatrix, b) -> None:
     dofs: DirichletDofs or a (dofs int32, values float64) pair."""
     d, v = dofs.arrays() if isinstance(dofs, DirichletDofs) else dofs
     if _is_device(b):
-        d, v = _i32(d), _f64(v)
+        import torch
+        d = torch.as_tensor(d, dtype=torch.int32, device=b.device).contiguous()
+        v = torch.as_tensor(v, dtype=torch.float64, device=b.device).contiguous()
         K.ctx.check(K.ctx.L.cstg_apply_dirichlet_device(K.ctx.h, d.numel(), _ptr(d), _ptr(v), _ptr(b)))
         return
     if not (isinstance(b, np.ndarray) and b.dtype == np.float64 and b.flags.c_contiguous):
