@@ -78,6 +78,15 @@ class Oracle:
                                       C.c_double, C.c_double, _dp]
         L.or_pcg_jacobi.argtypes = [C.c_int, _ip, _ip, _dp, _dp, _dp, C.c_double, C.c_int,
                                     C.c_void_p, C.POINTER(_Stats)]
+        L.mp_param_count.restype = C.c_long
+        L.mp_round_bf16.argtypes = [C.c_double]
+        L.mp_round_bf16.restype = C.c_double
+        L.mp_features.argtypes = [C.c_int, _dp, _dp, _dp, _dp, C.c_double, C.c_double, C.c_double, _dp]
+        L.mp_forward.argtypes = [C.c_int, _ip, _ip, _dp, _dp, C.c_int, _dp, _dp, _dp, _dp]
+        L.mp_apply.argtypes = [C.c_int, _dp, _dp, C.c_double, _dp, _dp]
+        L.mp_loss.argtypes = [C.c_int, _ip, _ip, _dp, _dp, _dp, _dp, C.c_double, _dp, C.c_void_p]
+        L.mp_loss.restype = C.c_double
+        L.mp_backward.argtypes = [C.c_int, _ip, _ip, _dp, _dp, C.c_int, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]
         self.L = L
 
     def _err(self, what):
@@ -158,6 +167,55 @@ class Oracle:
         if hist is not None:
             stats["residual_history"] = hist[: (st.iterations + 1 if st.iterations or st.converged else 1)]
         return x, stats
+
+
+    # ---- the learned preconditioner's network (mpnn_oracle.c; no reference counterpart) ----
+    MP_F, MP_L = 64, 3
+
+    def mp_param_count(self):
+        return int(self.L.mp_param_count())
+
+    def mp_round_bf16(self, a):
+        return np.array([self.L.mp_round_bf16(float(v)) for v in np.ravel(a)]).reshape(np.shape(a))
+
+    def mp_features(self, r, invd, xy, mat, coord_scale=10.0):
+        """Network inputs (N x 8) and the residual scale s = RMS(r)."""
+        r, invd = _f64(r), _f64(invd)
+        N = r.size // 2
+        s = float(np.sqrt(np.dot(r, r) / r.size))
+        d_mean = float(np.mean(1.0 / invd))
+        X = np.zeros(N * 8)
+        self.L.mp_features(N, r, invd, _f64(xy), _f64(mat), s, d_mean, float(coord_scale), X)
+        return X, s
+
+    def mp_forward(self, node_ptr, nbr, X, P, q=True):
+        N = node_ptr.size - 1
+        F, L = self.MP_F, self.MP_L
+        H = np.zeros((L + 1) * N * F)
+        G = np.zeros(L * N * F)
+        A = np.zeros(L * N * F)
+        Y = np.zeros(N * 2)
+        self.L.mp_forward(N, _i32(node_ptr), _i32(nbr), _f64(X), _f64(P), int(q), H, G, A, Y)
+        return Y, (H, G, A)
+
+    def mp_apply(self, r, invd, s, Y):
+        z = np.zeros(_f64(r).size)
+        self.L.mp_apply(z.size // 2, _f64(r), _f64(invd), float(s), _f64(Y), z)
+        return z
+
+    def mp_loss(self, rp, cols, vals, r, e, invd, s, Y, grad=True):
+        dY = np.zeros(_f64(r).size) if grad else None
+        L = self.L.mp_loss(_f64(r).size // 2, _i32(rp), _i32(cols), _f64(vals), _f64(r), _f64(e), _f64(invd),
+                           float(s), _f64(Y), dY.ctypes.data if grad else None)
+        return L, dY
+
+    def mp_backward(self, node_ptr, nbr, X, P, cache, dY, q=True):
+        N = node_ptr.size - 1
+        H, G, A = cache
+        dP = np.zeros(self.mp_param_count())
+        w = [np.zeros(N * self.MP_F) for _ in range(3)]
+        self.L.mp_backward(N, _i32(node_ptr), _i32(nbr), _f64(X), _f64(P), int(q), H, G, A, _f64(dY), dP, *w)
+        return dP
 
 
 class _RefStats(C.Structure):
