@@ -74,8 +74,14 @@ typedef struct {
   int max_refinements;      /* cap on replacements/restarts when true_residual_stop (16)   */
   int check_interval;       /* iterations per device graph between host checks (0: auto)  */
   int launch_mode;          /* CSTG_LAUNCH_*                                               */
-  int reserved[3];
+  int preconditioner;       /* CSTG_PRECOND_*                                              */
+  int reserved[2];
 } cstg_solver_options;
+
+/* preconditioner of cstg_pcg_solve */
+#define CSTG_PRECOND_JACOBI 0   /* Jacobi (the reference's CgJacobiSolver)                      */
+#define CSTG_PRECOND_LEARNED 1  /* the learned network inside flexible CG, Jacobi as fallback;
+                                   needs cstg_learned_setup after cstg_pcg_setup                */
 
 /* launch_mode of cstg_pcg_solve */
 #define CSTG_LAUNCH_AUTO 0        /* persistent kernel for mesh-pattern matrices, else graph  */
@@ -266,6 +272,47 @@ int cstg_batch_solve_device(cstg_ctx* ctx, int n_systems, const int32_t* node_of
 int cstg_batch_autotune(cstg_ctx* ctx, int n_systems, const int32_t* node_offsets, int n_rhs,
                         const double* d_b, double* d_x, const cstg_solver_options* opt,
                         cstg_batch_config* best, double* best_seconds);
+
+/* ---- learned preconditioner -----------------------------------------------------------------
+ * No counterpart in the reference. A message-passing network over the node graph of the
+ * stiffness pattern (3 layers of width 64, BF16 weights with FP32 accumulation, the layers on
+ * the tensor cores) maps a residual r to z = D^-1 (r + s Y(r / s)), s = RMS(r); with all weights
+ * zero it is the Jacobi step. Parameters: cstg_mpnn_param_count() floats, packed as
+ * W_in[64][8], b_in[64], (W_l[64][128], b_l[64]) for l = 1..3, W_out[2][64], b_out[2], every W
+ * row-major [out][in]. Inputs per node: r / s (2), diagonal / its mean (2), coordinates / 10 (2)
+ * and two material values (the caller's: log(D00) and D01/D00 of the node's constitutive matrix).
+ * cstg_learned_setup: after cstg_pcg_setup (host arrays; node_material has 2 floats per node).
+ * Then cstg_pcg_solve with opt->preconditioner = CSTG_PRECOND_LEARNED runs flexible CG
+ * (Polak-Ribiere) with the network; Jacobi takes over when the network's direction is not a
+ * descent direction (one step) or when ||r|| has not halved over 1000 iterations (for the rest
+ * of the solve). Mesh-pattern matrices only. */
+/* Training data: plain FP64 Jacobi-PCG (the reference's recurrence) on d_b, copying the iterate
+ * x_k to d_X + j * n_rows after every `every` iterations (k = every, 2 every, ...), at most
+ * max_snapshots of them; *n_snapshots receives the count. The solve itself ends as
+ * cstg_pcg_solve_device does. */
+int cstg_pcg_iterates_device(cstg_ctx* ctx, const double* d_b, int every, int max_snapshots, double* d_X,
+                             int* n_snapshots, const cstg_solver_options* opt, cstg_stats* stats);
+long long cstg_mpnn_param_count(void);
+int cstg_learned_setup(cstg_ctx* ctx, const float* params, const float* node_material);
+int cstg_learned_set_params(cstg_ctx* ctx, const float* params);
+/* z = M(r) on device vectors (2 x node count doubles each). */
+int cstg_learned_apply_device(cstg_ctx* ctx, const double* d_r, double* d_z);
+
+/* Training on the GPU with the library's forward and backward kernels. A sample is a residual
+ * r and the error e = A^-1 r of the context's matrix (device, n_rows doubles each, samples one
+ * after another); its loss is 1 - (z'r)^2 / ((z'Az)(e'r)), z = M(r). accumulate adds the
+ * gradients of n_samples losses (the context must have cstg_learned_setup done; its weights are
+ * not used, the trainer's are); step applies Adam (beta 0.9 / 0.999) with the accumulated
+ * gradient times grad_scale and clears it. */
+typedef struct cstg_trainer cstg_trainer;
+cstg_trainer* cstg_trainer_create(int device, const float* params, int* status);
+void cstg_trainer_destroy(cstg_trainer* tr);
+const char* cstg_trainer_last_error(const cstg_trainer* tr);
+int cstg_trainer_accumulate(cstg_trainer* tr, cstg_ctx* ctx, int n_samples, const double* d_R, const double* d_E,
+                            double* losses);
+int cstg_trainer_step(cstg_trainer* tr, float lr, float grad_scale);
+int cstg_trainer_params(cstg_trainer* tr, float* params, float* grads);
+int cstg_trainer_zero_grad(cstg_trainer* tr);
 
 #ifdef __cplusplus
 }

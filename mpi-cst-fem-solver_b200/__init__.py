@@ -7,7 +7,7 @@ C++ interface on top of it, `plate` generates the synthetic O-grid plates.
 The directory name is not a Python identifier; import it with
 ``importlib.import_module("mpi-cst-fem-solver_b200")``.
 """
-from . import batch, build, native, plate  # noqa: F401
+from . import batch, build, learned, native, plate  # noqa: F401
 from .native import CstgError, LogicError  # noqa: F401
 from .batch import BatchSolution, BatchSolver, PlateBatch, build_batch  # noqa: F401
 from .solver import (CgJacobiSolver, Context, DirichletDofs, GpuCsrMatrix,  # noqa: F401

@@ -75,6 +75,7 @@ void cstg_destroy(cstg_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->graph) cudaGraphExecDestroy(ctx->graph);
   if (ctx->bat_graph) cudaGraphExecDestroy(ctx->bat_graph);
+  if (ctx->fcg_graph) cudaGraphExecDestroy(ctx->fcg_graph);
   DevBuf* all[] = {&ctx->xy,      &ctx->tri,    &ctx->cnt,      &ctx->cursor,   &ctx->ne_ptr,
                    &ctx->ne,      &ctx->scan_tmp, &ctx->deg,    &ctx->node_ptr, &ctx->bnbr,
                    &ctx->slot,    &ctx->row_ptr, &ctx->cols,    &ctx->vals,     &ctx->fixed,
@@ -84,7 +85,8 @@ void cstg_destroy(cstg_ctx* ctx) {
                    &ctx->stress,    &ctx->val32,  &ctx->nbr32,    &ctx->S32,      &ctx->mat,
                    &ctx->mat_tab, &ctx->bat_sys, &ctx->bat_order, &ctx->bat_queue, &ctx->bat_b,
                    &ctx->bat_x,   &ctx->bat_r,  &ctx->bat_p,    &ctx->bat_Ap,   &ctx->bat_stats,
-                   &ctx->bat_in,  &ctx->bat_out};
+                   &ctx->bat_in,  &ctx->bat_out, &ctx->lp_p32, &ctx->lp_pb,   &ctx->lp_pf,
+                   &ctx->lp_sf,   &ctx->lp_h0,  &ctx->lp_h1,    &ctx->lp_sc,    &ctx->lp_z};
   for (DevBuf* b : all) free_buf(*b);
   if (ctx->h_err) cudaFreeHost(ctx->h_err);
   if (ctx->h_state) cudaFreeHost(ctx->h_state);
@@ -486,6 +488,7 @@ int cstg_pcg_setup(cstg_ctx* ctx) {
                 ctx->h_err[kErrDiag]);
   }
   ctx->setup_done = true;
+  ctx->setup_count++;
   ctx->mixed_ready = false;  // the FP32 operator is rebuilt from this matrix on first use
   return CSTG_OK;
 }
@@ -542,8 +545,15 @@ int cstg_multiply_mixed_device(cstg_ctx* ctx, const double* d_x, double* d_y) {
   return CSTG_OK;
 }
 
+// Snapshots of the iterate (training data of the learned preconditioner): every `every`
+// iterations x is copied to snap[k * n], k < max; the graph path runs with chunks of `every`.
+struct Snapshots {
+  double* x = nullptr;
+  int every = 0, max = 0, count = 0;
+};
+
 static int run_solve(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg_solver_options& o,
-                     cstg_stats* stats, double* d_hist, bool hist_host) {
+                     cstg_stats* stats, double* d_hist, bool hist_host, Snapshots* snap = nullptr) {
   const int n = ctx->n_rows;
   ENSURE(ctx->x, sizeof(double) * (size_t)n);
   ENSURE(ctx->r, sizeof(double) * (size_t)n);
@@ -593,8 +603,8 @@ static int run_solve(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg_s
 
   // Mesh-pattern matrices run as one persistent cooperative kernel per solve (unless the
   // caller asks for the graph path); caller CSR matrices use the graph path.
-  const bool persist = ctx->kind == 1 && o.launch_mode != CSTG_LAUNCH_GRAPH;
-  const int chunk = persist ? o.max_iter + 1 : (o.check_interval > 0 ? o.check_interval : 50);
+  const bool persist = ctx->kind == 1 && o.launch_mode != CSTG_LAUNCH_GRAPH && !snap;
+  const int chunk = snap ? snap->every : persist ? o.max_iter + 1 : (o.check_interval > 0 ? o.check_interval : 50);
   // (Re)capture the chunk graph when a buffer, the shape or the method changed. The mixed
   // graph reads b (reliable updates), so it is also tied to the right-hand-side pointer.
   if (!persist && (!ctx->graph || ctx->graph_gen != ctx->generation || ctx->graph_chunk != chunk ||
@@ -650,6 +660,9 @@ static int run_solve(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg_s
       } else {
         CK(cudaGraphLaunch(ctx->graph, ctx->stream));
         count_launches(per_iter * chunk);
+        if (snap && snap->count < snap->max && n)
+          CK(cudaMemcpyAsync(snap->x + (size_t)snap->count++ * n, w.x, sizeof(double) * (size_t)n,
+                             cudaMemcpyDeviceToDevice, ctx->stream));
       }
       rc = snapshot(ctx);
       if (rc) return rc;
@@ -742,6 +755,16 @@ static int check_solve_args(cstg_ctx* ctx, const cstg_solver_options* opt, cstg_
   if (o.precision == CSTG_PRECISION_MIXED && ctx->kind != 1)
     return fail(ctx, CSTG_ERR_UNSUPPORTED,
                 "pcg_solve: mixed precision needs the mesh (2x2-block) pattern of cstg_build_pattern");
+  if (o.preconditioner != CSTG_PRECOND_JACOBI && o.preconditioner != CSTG_PRECOND_LEARNED)
+    return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "pcg_solve: unknown preconditioner %d", o.preconditioner);
+  if (o.preconditioner == CSTG_PRECOND_LEARNED) {
+    if (ctx->kind != 1)
+      return fail(ctx, CSTG_ERR_UNSUPPORTED, "pcg_solve: the learned preconditioner needs the mesh pattern");
+    if (!ctx->learned_ready || ctx->learned_setup != ctx->setup_count)
+      return fail(ctx, CSTG_ERR_STATE, "pcg_solve: call cstg_learned_setup after cstg_pcg_setup");
+    if (o.record_history)
+      return fail(ctx, CSTG_ERR_UNSUPPORTED, "pcg_solve: no residual history with the learned preconditioner");
+  }
   return CSTG_OK;
 }
 
@@ -754,7 +777,29 @@ int cstg_pcg_solve_device(cstg_ctx* ctx, const double* d_b, double* d_x, const c
   if (ctx->n_rows && (!d_b || !d_x)) return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "pcg_solve: null vector");
   if (!aligned16(d_b) || !aligned16(d_x))
     return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "pcg_solve: device vectors must be 16-byte aligned");
+  if (o.preconditioner == CSTG_PRECOND_LEARNED) return run_fcg(ctx, d_b, d_x, o, stats);
   return run_solve(ctx, d_b, d_x, o, stats, d_history, false);
+}
+
+int cstg_pcg_iterates_device(cstg_ctx* ctx, const double* d_b, int every, int max_snapshots, double* d_X,
+                             int* n_snapshots, const cstg_solver_options* opt, cstg_stats* stats) {
+  BEGIN(ctx);
+  cstg_solver_options o;
+  int rc = check_solve_args(ctx, opt, o);
+  if (rc) return rc;
+  if (every < 1 || max_snapshots < 0 || (max_snapshots > 0 && !d_X) || (ctx->n_rows && !d_b))
+    return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "pcg_iterates: bad arguments");
+  if (o.precision != CSTG_PRECISION_FP64 || o.preconditioner != CSTG_PRECOND_JACOBI || o.record_history)
+    return fail(ctx, CSTG_ERR_UNSUPPORTED, "pcg_iterates: plain FP64 Jacobi-PCG only");
+  const size_t n = (size_t)ctx->n_rows;
+  ENSURE(ctx->vec_out, sizeof(double) * n);
+  Snapshots sn;
+  sn.x = d_X;
+  sn.every = every;
+  sn.max = max_snapshots;
+  rc = run_solve(ctx, d_b, buf_ptr<double>(ctx->vec_out), o, stats, nullptr, false, &sn);
+  if (n_snapshots) *n_snapshots = sn.count;
+  return rc;
 }
 
 int cstg_pcg_solve(cstg_ctx* ctx, const double* b, double* x, const cstg_solver_options* opt,
@@ -768,7 +813,9 @@ int cstg_pcg_solve(cstg_ctx* ctx, const double* b, double* x, const cstg_solver_
   ENSURE(ctx->b_in, sizeof(double) * n);
   ENSURE(ctx->vec_out, sizeof(double) * n);
   if (n) CK(cudaMemcpyAsync(ctx->b_in.p, b, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
-  rc = run_solve(ctx, buf_ptr<double>(ctx->b_in), buf_ptr<double>(ctx->vec_out), o, stats, history, true);
+  rc = o.preconditioner == CSTG_PRECOND_LEARNED
+           ? run_fcg(ctx, buf_ptr<double>(ctx->b_in), buf_ptr<double>(ctx->vec_out), o, stats)
+           : run_solve(ctx, buf_ptr<double>(ctx->b_in), buf_ptr<double>(ctx->vec_out), o, stats, history, true);
   if (rc) return rc;
   if (n) CK(cudaMemcpyAsync(x, ctx->vec_out.p, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));

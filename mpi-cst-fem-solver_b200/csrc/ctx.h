@@ -89,6 +89,16 @@ struct cstg_ctx {
   cudaGraphExec_t bat_graph = nullptr;
   unsigned long long bat_graph_key = 0;
   long long bat_graph_launches = 0;  // kernel nodes per replay of bat_graph
+
+  // learned preconditioner: packed weights (FP32 master, BF16 + FP32 copies), per-node static
+  // inputs, inference activations, network scalars, z; the flexible-CG chunk graph
+  unsigned long long setup_count = 0;  // bumped by every cstg_pcg_setup
+  DevBuf lp_p32, lp_pb, lp_pf, lp_sf, lp_h0, lp_h1, lp_sc, lp_z;
+  bool learned_ready = false;
+  unsigned long long learned_setup = ~0ull;  // setup_count the static inputs were built for
+  cudaGraphExec_t fcg_graph = nullptr;
+  unsigned long long fcg_key = 0;
+  long long fcg_graph_launches = 0;
 };
 
 namespace cstg_host {
@@ -233,6 +243,9 @@ inline void g_fmt(char* out, size_t n, const char* fmt, ...) {
   std::vsnprintf(out, n, fmt, ap);
   va_end(ap);
 }
+
+// Defined in learned_api.cu: flexible CG with the learned preconditioner.
+int run_fcg(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg_solver_options& o, cstg_stats* stats);
 
 // Defined in api.cu: the FP32 difference-form operator of the current matrix.
 int ensure_mixed(cstg_ctx* ctx);

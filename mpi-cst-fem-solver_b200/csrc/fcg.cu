@@ -1,0 +1,199 @@
+// Flexible conjugate gradients with the learned preconditioner z = M(r).
+//
+// M is a nonlinear map of r (a ReLU network), so the Fletcher-Reeves beta of pcg_iterate
+// (solver.cpp:84-99) is replaced by Polak-Ribiere, which keeps the iteration a flexible CG:
+//     beta = z_new'(r_new - r_old) / (z_old'r_old) = -alpha z_new'q / (z_old'r_old),   q = A p.
+// One iteration: q = A p and alpha = z'r / p'q (the PCG SpMV kernels); x += alpha p,
+// r -= alpha q and the convergence test (k_fcg_update); z = M(r) (mpnn.cu); z'r, z'q, r'D^-1 r
+// and beta (k_fcg_dots); p = z + beta p (k_fcg_pupdate).
+//
+// Jacobi is the fallback: when z'r <= 0 (the network returned a non-descent direction) the
+// iteration uses z = D^-1 r and restarts; when the residual norm has not halved over a window
+// of iterations (stagnation) the network is switched off for the rest of the solve and the
+// iteration continues as plain Jacobi-PCG (Fletcher-Reeves beta), restarted once.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "common.cuh"
+#include "kernels.h"
+
+namespace cstg {
+
+namespace {
+
+constexpr int kGrid = kSMs * 4;  // fixed grid: a fixed reduction order
+
+template <int NV>
+__device__ __forceinline__ bool fcg_reduce(const double (&v)[NV], double* partials, unsigned int* ticket,
+                                           double (&tot)[NV]) {
+  __shared__ double sm[kWarps];
+  __shared__ bool am_last;
+#pragma unroll
+  for (int q = 0; q < NV; ++q) {
+    const double s = block_sum<kThreads>(v[q], sm);
+    if (threadIdx.x == 0) partials[q * gridDim.x + blockIdx.x] = s;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) am_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!am_last) return false;
+  __threadfence();
+#pragma unroll
+  for (int q = 0; q < NV; ++q) {
+    double s = 0.0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) s += __ldcg(&partials[q * gridDim.x + i]);
+    tot[q] = block_sum<kThreads>(s, sm);
+  }
+  if (threadIdx.x == 0) *ticket = 0u;
+  return true;
+}
+
+// x = 0, r = b; ||b|| and the solver state (solver.cpp:42-58). The first p is set by
+// k_fcg_dots / k_fcg_pupdate after the first z = M(b) (restart_pending = 1: beta = 0).
+__global__ void __launch_bounds__(kThreads) k_fcg_init(int n, const double* __restrict__ b, double* __restrict__ x,
+                                                       double* __restrict__ r, double* partials, PcgState* st,
+                                                       double rtol, int max_iter) {
+  double bb = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double bi = b[i];
+    x[i] = 0.0;
+    r[i] = bi;
+    bb = fma(bi, bi, bb);
+  }
+  const double v[1] = {bb};
+  double tot[1];
+  if (fcg_reduce<1>(v, partials, &st->ticket[5], tot) && threadIdx.x == 0) {
+    st->bnorm = sqrt(tot[0]);
+    st->rr = tot[0];
+    st->rel = tot[0] > 0.0 ? 1.0 : 0.0;
+    st->rtol = rtol;
+    st->max_iter = max_iter;
+    st->iter = 0;
+    st->done = tot[0] > 0.0 ? (max_iter > 0 ? 0 : CSTG_SOLVE_MAX_ITER + 1) : CSTG_SOLVE_ZERO_RHS + 1;
+    st->alpha = st->beta = 0.0;
+    st->rz = 0.0;
+    st->replace_count = 0;
+    st->restart_pending = 1;
+    st->fallback = 0;
+    st->use_jacobi = 0;
+    st->mp_skip = st->done != 0;
+    st->fb_rr0 = tot[0];
+    st->fb_it0 = 0;
+    st->true_rel = 0.0;
+  }
+}
+
+// z'r, z'q and r'D^-1 r, r'D^-1 q; the last block picks z (network or Jacobi) and beta.
+__global__ void __launch_bounds__(kThreads) k_fcg_dots(int n, const double* __restrict__ z,
+                                                       const double* __restrict__ r, const double* __restrict__ q,
+                                                       const double* __restrict__ invd, double* partials,
+                                                       PcgState* st) {
+  if (__ldcg(&st->done)) return;
+  double zr = 0.0, zq = 0.0, jr = 0.0, jq = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double ri = r[i], qi = q[i], ji = invd[i] * ri;
+    zr = fma(z[i], ri, zr);
+    zq = fma(z[i], qi, zq);
+    jr = fma(ji, ri, jr);
+    jq = fma(ji, qi, jq);
+  }
+  const double v[4] = {zr, zq, jr, jq};
+  double tot[4];
+  if (fcg_reduce<4>(v, partials, &st->ticket[6], tot) && threadIdx.x == 0) {
+    bool restart = st->restart_pending != 0;
+    bool jac = st->fallback != 0;
+    if (!jac && !(tot[0] > 0.0)) {  // a non-descent network output: Jacobi this step, restarted
+      jac = true;
+      restart = true;
+    }
+    const double rz_new = jac ? tot[2] : tot[0];
+    double beta = 0.0;
+    if (!restart && st->rz > 0.0) {
+      if (st->fallback)
+        beta = rz_new / st->rz;  // plain Jacobi-PCG (Fletcher-Reeves), solver.cpp:84-99
+      else
+        beta = -st->alpha * (jac ? tot[3] : tot[1]) / st->rz;  // Polak-Ribiere
+    }
+    st->beta = beta;
+    st->rz = rz_new;
+    st->use_jacobi = jac ? 1 : 0;
+    st->restart_pending = 0;
+  }
+}
+
+// p = z + beta p (z = D^-1 r when use_jacobi)
+__global__ void __launch_bounds__(kThreads) k_fcg_pupdate(int n, const double* __restrict__ z,
+                                                          const double* __restrict__ r,
+                                                          const double* __restrict__ invd, double* __restrict__ p,
+                                                          const PcgState* st) {
+  if (__ldcg(&st->done)) return;
+  const double beta = __ldcg(&st->beta);
+  const bool jac = __ldcg(&st->use_jacobi) != 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double zi = jac ? invd[i] * r[i] : z[i];
+    p[i] = fma(beta, p[i], zi);
+  }
+}
+
+// x += alpha p, r -= alpha q; ||r||, convergence (solver.cpp:72-82), max_iter, stagnation.
+__global__ void __launch_bounds__(kThreads) k_fcg_update(int n, double* __restrict__ x, double* __restrict__ r,
+                                                         const double* __restrict__ p,
+                                                         const double* __restrict__ q, double* partials,
+                                                         PcgState* st, int window, double ratio2) {
+  if (__ldcg(&st->done)) return;
+  const double alpha = __ldcg(&st->alpha);
+  double rr = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    x[i] = fma(alpha, p[i], x[i]);
+    const double ri = fma(-alpha, q[i], r[i]);
+    r[i] = ri;
+    rr = fma(ri, ri, rr);
+  }
+  const double v[1] = {rr};
+  double tot[1];
+  if (fcg_reduce<1>(v, partials, &st->ticket[7], tot) && threadIdx.x == 0) {
+    const int it = st->iter + 1;
+    st->iter = it;
+    st->rr = tot[0];
+    st->rel = st->bnorm > 0.0 ? sqrt(tot[0]) / st->bnorm : 0.0;
+    if (st->rel <= st->rtol)
+      st->done = CSTG_SOLVE_CONVERGED + 1;
+    else if (it >= st->max_iter)
+      st->done = CSTG_SOLVE_MAX_ITER + 1;
+    if (!st->fallback && window > 0 && it - st->fb_it0 >= window) {
+      if (tot[0] > ratio2 * st->fb_rr0) {  // stagnation: the network is switched off
+        st->fallback = 1;
+        st->restart_pending = 1;
+      }
+      st->fb_rr0 = tot[0];
+      st->fb_it0 = it;
+    }
+    st->mp_skip = (st->done != 0 || st->fallback != 0) ? 1 : 0;
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_fcg_init(const FcgBuffers& w, double rtol, int max_iter, int window, cudaStream_t s) {
+  (void)window;
+  k_fcg_init<<<kGrid, kThreads, 0, s>>>(w.n, w.b, w.x, w.r, w.partials, w.st, rtol, max_iter);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fcg_dots(const FcgBuffers& w, cudaStream_t s) {
+  k_fcg_dots<<<kGrid, kThreads, 0, s>>>(w.n, w.z, w.r, w.q, w.inv_diag, w.partials, w.st);
+  k_fcg_pupdate<<<kGrid, kThreads, 0, s>>>(w.n, w.z, w.r, w.inv_diag, w.p, w.st);
+  count_launches(2);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fcg_update(const FcgBuffers& w, int window, double ratio2, cudaStream_t s) {
+  k_fcg_update<<<kGrid, kThreads, 0, s>>>(w.n, w.x, w.r, w.p, w.q, w.partials, w.st, window, ratio2);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+}  // namespace cstg

@@ -1,6 +1,7 @@
 // Internal launcher declarations shared by the C-ABI layer and the kernel files.
 #pragma once
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -71,6 +72,11 @@ struct alignas(128) PcgState {
   int fp64_mode;        // mixed: the FP32 operator reached its accuracy floor; SpMV in FP64
   int fp64_switch_iter; // mixed: iteration of that switch (0: none)
   double best_true;     // mixed: smallest FP64 true residual seen at a reliable update
+  double fb_rr0;        // learned (flexible CG): r'r at the start of the stagnation window
+  int fallback;         // learned: the network is off, Jacobi-PCG from here on
+  int use_jacobi;       // learned: this iteration's z is D^-1 r (fallback or a non-descent z)
+  int mp_skip;          // learned: the network kernels skip (done or fallback)
+  int fb_it0;           // learned: iteration at the start of the stagnation window
   unsigned int bar_count;  // persistent kernel: blocks arrived at the current grid barrier
   unsigned int bar_gen;    // persistent kernel: barrier generation (bumped on release)
   int bar_err;             // persistent kernel: a barrier wait ran out (the solve is abandoned)
@@ -143,6 +149,78 @@ cudaError_t launch_batch_unpack(int N, int R, int q0, long long ld, const double
                                 cudaStream_t s);
 cudaError_t launch_batch_check(int N, int n_sys, const int* sys_node, const int* node_ptr, const int* bnbr,
                                int* err, cudaStream_t s);
+
+// mpnn.cu: the learned preconditioner's network (F = 64 features, 3 message-passing layers).
+// Packed parameter vector: W_in[64][8], b_in[64], (W_l[64][128], b_l[64]) x 3, W_out[2][64], b_out[2].
+constexpr int kMpF = 64, kMpIn = 8, kMpL = 3;
+constexpr int kMpOffWin = 0, kMpOffBin = kMpF * kMpIn, kMpOffL0 = kMpOffBin + kMpF;
+constexpr int kMpLStride = kMpF * 2 * kMpF + kMpF;
+constexpr int kMpOffWout = kMpOffL0 + kMpL * kMpLStride, kMpOffBout = kMpOffWout + 2 * kMpF;
+constexpr int kMpParams = kMpOffBout + 2;
+constexpr int kMpPartBlocks = 148;  // blocks of the weight-gradient kernels (partials, fixed order)
+constexpr int kMpPartStride = kMpF * 2 * kMpF + kMpF;
+
+struct MpnnParams {  // device copies of the packed parameters
+  const __nv_bfloat16* pb = nullptr;  // BF16 (weights are read from here)
+  const float* pf = nullptr;          // FP32 (biases are read from here)
+};
+
+struct MpnnGraph {  // the node-block pattern (self included; the network skips self)
+  int n_nodes = 0;
+  const int* node_ptr = nullptr;
+  const int* nbr = nullptr;
+};
+
+struct MpnnWork {  // activations (training keeps every layer; inference ping-pongs H[0]/H[1])
+  __nv_bfloat16* H[kMpL + 1] = {};
+  __nv_bfloat16* G[kMpL] = {};
+  __nv_bfloat16* A[kMpL] = {};
+  __nv_bfloat16* X = nullptr;  // [N][8]
+  float* Y = nullptr;          // [N][2]
+  float* dY = nullptr;         // [2N]
+  float *dH = nullptr, *dH2 = nullptr, *dU = nullptr, *dAs = nullptr;  // [N][64]
+  float* part = nullptr;       // [kMpPartBlocks][kMpPartStride]
+};
+
+struct MpScratch {  // small device scalars of the network's reductions
+  double rr;        // r'r
+  double dots[3];   // z'r, z'Az, e'r
+  double loss;
+  unsigned int ticket[4];
+  double partials[3 * 296];
+};
+
+cudaError_t mpnn_prepare_device();
+cudaError_t launch_mp_params(const float* p32, __nv_bfloat16* pb, float* pf, cudaStream_t s);
+cudaError_t launch_mp_rr(int n, const double* r, MpScratch* sc, cudaStream_t s);
+// z = M(r): encoder, three tensor-core layers, decoder. `rr` points at r'r (device), `skip`
+// (device int, may be null) turns the network off (z = D^-1 r).
+cudaError_t launch_mp_forward(const MpnnGraph& g, const MpnnParams& P, const double* r, const double* invd,
+                              const double* rr, const float* sf, const int* skip, MpnnWork& w, bool train,
+                              double* z, int* err, cudaStream_t s);
+cudaError_t launch_mp_loss(int N, const double* z, const double* az, const double* r, const double* e,
+                           const double* invd, MpScratch* sc, MpnnWork& w, cudaStream_t s);
+cudaError_t launch_mp_backward(const MpnnGraph& g, const MpnnParams& P, MpnnWork& w, float* grad, cudaStream_t s);
+cudaError_t launch_mp_adam(float* p, float* m, float* v, const float* g, float lr, float b1, float b2, float eps,
+                           int step, float scale, __nv_bfloat16* pb, float* pf, cudaStream_t s);
+
+// fcg.cu: flexible CG with the learned preconditioner (Polak-Ribiere beta), Jacobi fallback.
+struct FcgBuffers {
+  int n = 0;  // rows (2 x nodes)
+  double *x = nullptr, *r = nullptr, *p = nullptr, *q = nullptr, *z = nullptr;
+  const double* b = nullptr;
+  const double* inv_diag = nullptr;
+  double* partials = nullptr;
+  PcgState* st = nullptr;
+};
+cudaError_t launch_fcg_init(const FcgBuffers& w, double rtol, int max_iter, int window, cudaStream_t s);
+cudaError_t launch_fcg_dots(const FcgBuffers& w, cudaStream_t s);  // beta, r'z; then p = z + beta p
+cudaError_t launch_fcg_update(const FcgBuffers& w, int window, double ratio2, cudaStream_t s);
+// q = A p with p'Ap and alpha = r'z / p'Ap (the PCG variants of the SpMVs)
+cudaError_t launch_spmv_pcg(const BlockMatrix& A, const double* p, double* q, double* partials, PcgState* st,
+                            cudaStream_t s);
+cudaError_t launch_spmv_mixed_pcg(const MixedMatrix& A32, const BlockMatrix& A64, const double* p, double* q,
+                                  double* partials, PcgState* st, cudaStream_t s);
 
 // Process-wide count of kernel launches issued by this library (graph launches count every
 // kernel node they run).

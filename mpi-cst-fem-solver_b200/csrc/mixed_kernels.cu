@@ -432,6 +432,13 @@ cudaError_t launch_mixed_iteration(const MixedBuffers& w, const MixedMatrix& A32
   return cudaGetLastError();
 }
 
+cudaError_t launch_spmv_mixed_pcg(const MixedMatrix& A32, const BlockMatrix& A64, const double* p, double* q,
+                                  double* partials, PcgState* st, cudaStream_t s) {
+  k_spmv_mixed<true><<<wave_grid_m<k_spmv_mixed<true>>(), kThreads, 0, s>>>(A32, A64, p, q, partials, st);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_spmv_mixed(const MixedMatrix& A32, const double* x, double* y, cudaStream_t s) {
   k_spmv_mixed<false><<<wave_grid_m<k_spmv_mixed<false>>(), kThreads, 0, s>>>(A32, BlockMatrix{}, x, y, nullptr,
                                                                             nullptr);

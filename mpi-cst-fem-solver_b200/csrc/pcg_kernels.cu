@@ -417,6 +417,12 @@ cudaError_t launch_pcg_iteration(const PcgBuffers& w, const BlockMatrix* bm,
   return cudaGetLastError();
 }
 
+cudaError_t launch_spmv_pcg(const BlockMatrix& A, const double* p, double* q, double* partials, PcgState* st,
+                            cudaStream_t s) {
+  spmv_dispatch<true>(&A, nullptr, p, q, partials, st, s);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_spmv(const BlockMatrix* bm, const CsrMatrixDev* cm, const double* x, double* y,
                         cudaStream_t s) {
   spmv_dispatch<false>(bm, cm, x, y, nullptr, nullptr, s);

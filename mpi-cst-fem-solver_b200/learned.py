@@ -1,0 +1,255 @@
+"""Learned preconditioner: set-up on a matrix, training data from the plain solver, training on
+the GPU, and the packaged weights.
+
+The network (cstfem_b200.h, "learned preconditioner") maps a residual r to
+z = D^-1 (r + s Y(r / s)); with the output layer at zero it is exactly the Jacobi step, which
+is where training starts. Training pairs (r_k, e_k) come from plain FP64 Jacobi-PCG runs on
+seeded random plates (the uneven batch distribution): r_k = b - A x_k and e_k = x* - x_k for
+iterates x_k sampled along the run and x* the converged solution. The loss of a pair is the
+squared sine of the energy-norm angle between z = M(r_k) and e_k (0 when z points along the
+error). Forward, loss and backward run in the library's kernels; Adam runs on the GPU.
+
+Command line (writes the packaged weights):
+    python -m mpi-cst-fem-solver_b200.learned train --out weights.npz
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import dataclasses
+import os
+import time
+
+import numpy as np
+
+from . import native
+from .native import CstgError
+from .plate import PlateSpec, quarter_plate, random_batch, symmetry_dirichlet
+from .solver import (CgJacobiSolver, Context, GpuCsrMatrix, PlaneCondition, SolverOptions, _f64, _ptr,
+                     add_traction, apply_dirichlet, assemble_stiffness, build_stiffness_pattern,
+                     constitutive_matrix)
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+WEIGHTS = os.path.join(HERE, "weights", "mpnn_plates.npz")
+N_PARAMS = 25474
+F, N_IN, N_LAYERS = 64, 8, 3
+
+
+def param_count() -> int:
+    return int(native.load().cstg_mpnn_param_count())
+
+
+def init_params(seed: int = 0) -> np.ndarray:
+    """He-normal hidden weights, zero biases and a zero output layer (the network starts as
+    the Jacobi step)."""
+    rng = np.random.default_rng(seed)
+    p = np.zeros(N_PARAMS, dtype=np.float32)
+    o = 0
+    p[o:o + F * N_IN] = rng.standard_normal(F * N_IN) * np.sqrt(2.0 / N_IN)
+    o += F * N_IN + F
+    for _ in range(N_LAYERS):
+        # small residual branches: the hidden state grows slowly through the layers
+        p[o:o + F * 2 * F] = rng.standard_normal(F * 2 * F) * np.sqrt(2.0 / (2 * F)) * 0.5
+        o += F * 2 * F + F
+    assert o + 2 * F + 2 == N_PARAMS
+    return p
+
+
+def node_material(D, n_nodes: int) -> np.ndarray:
+    """The two material inputs per node: log(D00) and D01 / D00 of the constitutive matrix."""
+    D = np.asarray(D, dtype=np.float64).reshape(-1, 9)
+    if D.shape[0] == 1:
+        D = np.repeat(D, n_nodes, axis=0)
+    return np.ascontiguousarray(np.stack([np.log(D[:, 0]), D[:, 1] / D[:, 0]], axis=1).reshape(-1),
+                                dtype=np.float32)
+
+
+def load_weights(path: str | None = None) -> np.ndarray:
+    path = path or WEIGHTS
+    if not os.path.exists(path):
+        raise CstgError(native.ERR_STATE, f"learned preconditioner weights not found: {path}")
+    p = np.load(path)["params"].astype(np.float32)
+    if p.size != N_PARAMS:
+        raise CstgError(native.ERR_INVALID_ARGUMENT, f"weights have {p.size} values, expected {N_PARAMS}")
+    return p
+
+
+def setup(K: GpuCsrMatrix, params: np.ndarray, material: np.ndarray) -> None:
+    """cstg_learned_setup on K's context (after the Jacobi set-up of K)."""
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    m = np.ascontiguousarray(material, dtype=np.float32)
+    K.ctx.check(K.ctx.L.cstg_learned_setup(K.ctx.h, _ptr(p), _ptr(m)))
+
+
+def apply(K: GpuCsrMatrix, r, z=None):
+    """z = M(r) on CUDA float64 tensors."""
+    import torch
+    z = torch.empty_like(r) if z is None else z
+    K.ctx.check(K.ctx.L.cstg_learned_apply_device(K.ctx.h, _ptr(r), _ptr(z)))
+    return z
+
+
+class Trainer:
+    """The GPU trainer (cstg_trainer): FP32 master weights + Adam state on the device."""
+
+    def __init__(self, params: np.ndarray, device: int = 0):
+        self.L = native.load()
+        st = C.c_int(0)
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        self.h = self.L.cstg_trainer_create(device, _ptr(p), C.byref(st))
+        if not self.h:
+            raise CstgError(st.value, f"cstg_trainer_create failed (status {st.value})")
+
+    def _check(self, rc):
+        if rc:
+            raise CstgError(rc, self.L.cstg_trainer_last_error(self.h).decode())
+
+    def accumulate(self, K: GpuCsrMatrix, R, E) -> np.ndarray:
+        """Adds the gradients of the samples (rows of the CUDA float64 tensors R, E)."""
+        ns = int(R.shape[0])
+        losses = np.zeros(ns)
+        self._check(self.L.cstg_trainer_accumulate(self.h, K.ctx.h, ns, _ptr(R.contiguous()),
+                                                   _ptr(E.contiguous()), _ptr(losses)))
+        return losses
+
+    def step(self, lr: float, grad_scale: float) -> None:
+        self._check(self.L.cstg_trainer_step(self.h, float(lr), float(grad_scale)))
+
+    def params(self, grads: bool = False):
+        p = np.zeros(N_PARAMS, dtype=np.float32)
+        g = np.zeros(N_PARAMS, dtype=np.float32) if grads else None
+        self._check(self.L.cstg_trainer_params(self.h, _ptr(p), _ptr(g)))
+        return (p, g) if grads else p
+
+    def zero_grad(self) -> None:
+        self._check(self.L.cstg_trainer_zero_grad(self.h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.cstg_trainer_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclasses.dataclass
+class PlateProblem:
+    """One training plate on the GPU: its matrix (learned set-up done) and sample pairs."""
+    spec: PlateSpec
+    K: GpuCsrMatrix
+    R: object  # CUDA float64 [samples, n]
+    E: object
+
+
+def plate_system(spec: PlateSpec, ctx: Context | None = None, load=("right", 1.0, 0.0)):
+    """Assembled, eliminated plate and its right-hand side (host b)."""
+    m = quarter_plate(spec.n_r, spec.n_theta, a=spec.a)
+    D = constitutive_matrix(spec.E, spec.nu, PlaneCondition.Strain if spec.plane_strain else PlaneCondition.Stress)
+    K = build_stiffness_pattern(m, ctx=ctx)
+    assemble_stiffness(m, D, 1.0, K)
+    b = np.zeros(m.num_dofs)
+    add_traction(K, m.boundary_edges[load[0]], 1.0, load[1], load[2], b)
+    apply_dirichlet(symmetry_dirichlet(m), K, b)
+    return m, D, K, b
+
+
+def harvest(spec: PlateSpec, samples: int, params: np.ndarray, seed: int = 0, device: int = 0) -> PlateProblem:
+    """Training pairs from plain FP64 Jacobi-PCG on one plate (a random load case mix)."""
+    import torch
+    rng = np.random.default_rng(seed)
+    ctx = Context(device)
+    loads = [("right", 1.0, 0.0), ("top", 0.0, 1.0), ("right", 0.0, 1.0), ("top", 1.0, 0.0)]
+    m, D, K, b = plate_system(spec, ctx, loads[int(rng.integers(0, 4))])
+    s = CgJacobiSolver(SolverOptions(rtol=1e-12, max_iter=200000))
+    s.setup(K)
+    d_b = torch.from_numpy(b).to(device)
+    x_star = torch.zeros_like(d_b)
+    st = s.solve(d_b, x_star)
+    if not st.converged:
+        raise CstgError(native.ERR_STATE, f"harvest: reference solve failed: {st.message}")
+    iters = max(st.iterations, samples)
+    every = max(1, iters // (samples + 1))
+    X = torch.zeros((samples, m.num_dofs), dtype=torch.float64, device=device)
+    o = SolverOptions(rtol=1e-12, max_iter=200000).native()
+    got = C.c_int(0)
+    stats = native.Stats()
+    ctx.check(ctx.L.cstg_pcg_iterates_device(ctx.h, _ptr(d_b), every, samples, _ptr(X), C.byref(got),
+                                             C.byref(o), C.byref(stats)))
+    X = X[:got.value]
+    E = (x_star[None, :] - X).contiguous()
+    R = torch.empty_like(E)
+    for i in range(E.shape[0]):
+        R[i] = d_b - K.multiply(X[i].contiguous())
+    keep = torch.linalg.vector_norm(R, dim=1) > 1e-9 * torch.linalg.vector_norm(d_b)
+    R, E = R[keep].contiguous(), E[keep].contiguous()
+    setup(K, params, node_material(D, m.num_nodes))
+    return PlateProblem(spec=spec, K=K, R=R, E=E)
+
+
+def train(n_plates: int = 100, samples_per_plate: int = 100, epochs: int = 3, batch: int = 8, lr: float = 1e-3,
+          seed: int = 2026, n_r_range=(20, 200), device: int = 0, log=print):
+    """Harvests n_plates x samples_per_plate pairs from the uneven plate distribution and trains
+    the network; returns (params, history of mean epoch losses, the Jacobi loss at the start)."""
+    import torch
+    params0 = init_params(seed)
+    specs = random_batch(count=n_plates, seed=seed + 1, n_r_range=n_r_range)
+    t0 = time.perf_counter()
+    probs = [harvest(sp, samples_per_plate, params0, seed=seed + 7 * i, device=device) for i, sp in enumerate(specs)]
+    n_pairs = sum(int(p.R.shape[0]) for p in probs)
+    log(f"harvested {n_pairs} pairs from {n_plates} plates in {time.perf_counter() - t0:.1f} s")
+    tr = Trainer(params0, device)
+    rng = np.random.default_rng(seed + 3)
+    hist = []
+    start = None
+    for ep in range(epochs):
+        order = [(i, j) for i, p in enumerate(probs) for j in range(0, int(p.R.shape[0]), batch)]
+        rng.shuffle(order)
+        tot, cnt = 0.0, 0
+        t1 = time.perf_counter()
+        for i, j in order:
+            p = probs[i]
+            Rb, Eb = p.R[j:j + batch], p.E[j:j + batch]
+            losses = tr.accumulate(p.K, Rb, Eb)
+            if not np.all(np.isfinite(losses)):
+                tr.zero_grad()
+                continue
+            tr.step(lr, 1.0 / len(losses))
+            tot += float(losses.sum())
+            cnt += len(losses)
+        mean = tot / max(cnt, 1)
+        if start is None:
+            start = mean
+        hist.append(mean)
+        log(f"epoch {ep}: mean loss {mean:.5f} ({time.perf_counter() - t1:.1f} s)")
+    params = tr.params()
+    tr.close()
+    for p in probs:
+        p.K.ctx.close()
+    return params, hist, n_pairs
+
+
+def main():
+    ap = argparse.ArgumentParser(description="train the learned preconditioner on the GPU")
+    ap.add_argument("cmd", choices=["train"])
+    ap.add_argument("--out", default=WEIGHTS)
+    ap.add_argument("--plates", type=int, default=100)
+    ap.add_argument("--samples", type=int, default=100)
+    ap.add_argument("--epochs", type=int, default=3)
+    ap.add_argument("--batch", type=int, default=8)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--seed", type=int, default=2026)
+    ap.add_argument("--n-r-max", type=int, default=200)
+    a = ap.parse_args()
+    params, hist, n_pairs = train(a.plates, a.samples, a.epochs, a.batch, a.lr, a.seed, (20, a.n_r_max))
+    os.makedirs(os.path.dirname(os.path.abspath(a.out)), exist_ok=True)
+    np.savez(a.out, params=params, loss_history=np.array(hist), pairs=n_pairs, plates=a.plates,
+             samples=a.samples, epochs=a.epochs, batch=a.batch, lr=a.lr, seed=a.seed)
+    print(f"wrote {a.out}")
+
+
+if __name__ == "__main__":
+    main()

@@ -49,8 +49,11 @@ class SolverOptions(C.Structure):
     _fields_ = [("rtol", C.c_double), ("max_iter", C.c_int), ("record_history", C.c_int),
                 ("precision", C.c_int), ("true_residual_stop", C.c_int),
                 ("max_refinements", C.c_int), ("check_interval", C.c_int),
-                ("launch_mode", C.c_int), ("reserved", C.c_int * 3)]
+                ("launch_mode", C.c_int), ("preconditioner", C.c_int), ("reserved", C.c_int * 2)]
 
+
+PRECOND_JACOBI = 0
+PRECOND_LEARNED = 1
 
 LAUNCH_AUTO = 0
 LAUNCH_PERSISTENT = 1
@@ -114,6 +117,19 @@ _SIGS = {
                                           C.POINTER(BatchConfig), _vp, C.POINTER(C.c_double)]),
     "cstg_batch_autotune": (C.c_int, [_vp, C.c_int, _vp, C.c_int, _vp, _vp, C.POINTER(SolverOptions),
                                       C.POINTER(BatchConfig), C.POINTER(C.c_double)]),
+    "cstg_pcg_iterates_device": (C.c_int, [_vp, _vp, C.c_int, C.c_int, _vp, C.POINTER(C.c_int),
+                                           C.POINTER(SolverOptions), C.POINTER(Stats)]),
+    "cstg_mpnn_param_count": (C.c_longlong, []),
+    "cstg_learned_setup": (C.c_int, [_vp, _vp, _vp]),
+    "cstg_learned_set_params": (C.c_int, [_vp, _vp]),
+    "cstg_learned_apply_device": (C.c_int, [_vp, _vp, _vp]),
+    "cstg_trainer_create": (_vp, [C.c_int, _vp, C.POINTER(C.c_int)]),
+    "cstg_trainer_destroy": (None, [_vp]),
+    "cstg_trainer_last_error": (C.c_char_p, [_vp]),
+    "cstg_trainer_accumulate": (C.c_int, [_vp, _vp, C.c_int, _vp, _vp, _vp]),
+    "cstg_trainer_step": (C.c_int, [_vp, C.c_float, C.c_float]),
+    "cstg_trainer_params": (C.c_int, [_vp, _vp, _vp]),
+    "cstg_trainer_zero_grad": (C.c_int, [_vp]),
 }
 
 STATIC_MAX_ROWS = 65536  # CSTG_STATIC_MAX_ROWS

@@ -277,6 +277,7 @@ class SolverOptions:
     max_refinements: int = 16
     check_interval: int = 0
     launch: str = "auto"  # "auto" | "persistent" | "graph"
+    preconditioner: str = "jacobi"  # "jacobi" | "learned" (flexible CG; needs learned setup)
 
     def native(self) -> native.SolverOptions:
         o = native.default_options()
@@ -289,6 +290,7 @@ class SolverOptions:
         o.check_interval = self.check_interval
         o.launch_mode = {"auto": native.LAUNCH_AUTO, "persistent": native.LAUNCH_PERSISTENT,
                          "graph": native.LAUNCH_GRAPH}[self.launch]
+        o.preconditioner = {"jacobi": native.PRECOND_JACOBI, "learned": native.PRECOND_LEARNED}[self.preconditioner]
         return o
 
 

@@ -1,0 +1,170 @@
+"""Learned preconditioner on the GPU: the tensor-core forward pass and the training gradients
+against the FP64 oracle (oracle/mpnn_oracle.c), training, and the flexible-CG solve with its
+Jacobi fallback, judged by the reference's FP64 Jacobi-PCG solution.
+
+Bars: forward z within relative 1e-2 of the oracle (BF16 activations on both sides; the rest
+is FP32-vs-FP64 accumulation); gradients within relative 5e-2; solves converged on the FP64 true
+residual <= 1e-10 with displacements within relative 1e-8 of the oracle's FP64 Jacobi-PCG."""
+import numpy as np
+import pytest
+
+from test_oracle_mpnn import node_graph
+
+pytestmark = pytest.mark.gpu
+
+REL_TOL = 1e-8
+
+
+def _rel(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+def _plate(pkg, n_r=6, n_t=12, E=1.0, nu=0.3):
+    m = pkg.plate.quarter_plate(n_r, n_t)
+    D = pkg.constitutive_matrix(E, nu)
+    K = pkg.build_stiffness_pattern(m)
+    pkg.assemble_stiffness(m, D, 1.0, K)
+    b = np.zeros(m.num_dofs)
+    pkg.add_traction(K, m.boundary_edges["right"], 1.0, 1.0, 0.0, b)
+    pkg.apply_dirichlet(pkg.plate.symmetry_dirichlet(m), K, b)
+    s = pkg.CgJacobiSolver()
+    s.setup(K)
+    return m, D, K, b
+
+
+def _bf16_params(oracle, pkg, seed=4, out_scale=0.3):
+    p = pkg.learned.init_params(seed)
+    rng = np.random.default_rng(seed + 1)
+    p[-130:] = rng.standard_normal(130) * out_scale  # a non-zero output layer
+    p = p.astype(np.float32)
+    # the oracle sees what the GPU computes with: BF16 weights, FP32 biases
+    q = p.astype(np.float64)
+    o = 0
+    w_idx = []
+    w_idx.append(np.arange(0, 64 * 8))
+    o = 64 * 8 + 64
+    for _ in range(3):
+        w_idx.append(np.arange(o, o + 64 * 128))
+        o += 64 * 128 + 64
+    w_idx.append(np.arange(o, o + 128))
+    for idx in w_idx:
+        q[idx] = oracle.mp_round_bf16(q[idx])
+    return p, q
+
+
+def test_learned_forward_matches_oracle(pkg, oracle, gpu_lib):
+    import torch
+    m, D, K, b = _plate(pkg)
+    p, q = _bf16_params(oracle, pkg)
+    mat = pkg.learned.node_material(D, m.num_nodes)
+    pkg.learned.setup(K, p, mat)
+    rng = np.random.default_rng(0)
+    r = rng.standard_normal(m.num_dofs)
+    z = pkg.learned.apply(K, torch.from_numpy(r).cuda()).cpu().numpy()
+    rp, cols, vals = K.download()
+    invd = 1.0 / vals[[np.searchsorted(cols[rp[i]:rp[i + 1]], i) + rp[i] for i in range(rp.size - 1)]]
+    node_ptr, nbr = node_graph(rp, cols)
+    X, s = oracle.mp_features(r, invd, m.xy, mat.astype(np.float64))
+    Y, _ = oracle.mp_forward(node_ptr, nbr, X, q, q=True)
+    z_ref = oracle.mp_apply(r, invd, s, Y)
+    assert np.abs(Y).max() > 1e-3  # the network is not trivially zero
+    assert _rel(z, z_ref) < 1e-2
+    # the network's own part (z - D^-1 r) is what the tensor cores compute
+    assert _rel(z - invd * r, z_ref - invd * r) < 2e-2
+    K.ctx.close()
+
+
+def test_learned_gradients_match_oracle(pkg, oracle, gpu_lib):
+    import torch
+    m, D, K, b = _plate(pkg)
+    p, q = _bf16_params(oracle, pkg, seed=9)
+    mat = pkg.learned.node_material(D, m.num_nodes)
+    pkg.learned.setup(K, p, mat)
+    rp, cols, vals = K.download()
+    Kd = np.zeros((m.num_dofs, m.num_dofs))
+    for i in range(m.num_dofs):
+        Kd[i, cols[rp[i]:rp[i + 1]]] = vals[rp[i]:rp[i + 1]]
+    rng = np.random.default_rng(1)
+    r = rng.standard_normal(m.num_dofs)
+    e = np.linalg.solve(Kd, r)
+    invd = 1.0 / np.diag(Kd)
+    tr = pkg.learned.Trainer(p)
+    loss = tr.accumulate(K, torch.from_numpy(r[None, :]).cuda(), torch.from_numpy(e[None, :]).cuda())
+    _, g = tr.params(grads=True)
+    node_ptr, nbr = node_graph(rp, cols)
+    X, s = oracle.mp_features(r, invd, m.xy, mat.astype(np.float64))
+    Y, cache = oracle.mp_forward(node_ptr, nbr, X, q, q=True)
+    L, dY = oracle.mp_loss(rp, cols, vals, r, e, invd, s, Y)
+    g_ref = oracle.mp_backward(node_ptr, nbr, X, q, cache, dY, q=True)
+    assert abs(loss[0] - L) < 1e-3 * max(1.0, abs(L))
+    assert _rel(g, g_ref) < 5e-2
+    # each block of the parameter vector separately (encoder, 3 layers, decoder)
+    bounds = [0, 576, 576 + 8256, 576 + 2 * 8256, 576 + 3 * 8256, 25474]
+    for a, c in zip(bounds[:-1], bounds[1:]):
+        assert _rel(g[a:c], g_ref[a:c]) < 5e-2, (a, c)
+    tr.close()
+    K.ctx.close()
+
+
+def test_zero_network_flexible_cg_is_jacobi_pcg(pkg, oracle, gpu_lib, golden):
+    """With all weights zero, z = D^-1 r: flexible CG reproduces Jacobi-PCG (same iterations
+    within 1 %, same solution to 1e-8)."""
+    g = golden("plate_40x80")
+    m = pkg.plate.quarter_plate(40, 80)
+    D = pkg.constitutive_matrix(1.0, 0.3)
+    K = pkg.build_stiffness_pattern(m)
+    pkg.assemble_stiffness(m, D, 1.0, K)
+    b = np.zeros(m.num_dofs)
+    pkg.add_traction(K, m.boundary_edges["right"], 1.0, 1.0, 0.0, b)
+    pkg.apply_dirichlet(pkg.plate.symmetry_dirichlet(m), K, b)
+    s = pkg.CgJacobiSolver(pkg.SolverOptions(rtol=1e-10, max_iter=100000, preconditioner="learned",
+                                             true_residual_stop=True))
+    s.setup(K)
+    pkg.learned.setup(K, np.zeros(pkg.learned.N_PARAMS, np.float32), pkg.learned.node_material(D, m.num_nodes))
+    x = np.zeros(m.num_dofs)
+    st = s.solve(b, x)
+    assert st.converged and st.true_rel_residual <= 1e-10, st.message
+    assert abs(st.iterations - g.meta["iters"]) <= 0.01 * g.meta["iters"] + 2
+    assert _rel(x, g["u"]) < REL_TOL
+    K.ctx.close()
+
+
+def test_fallback_on_a_bad_network(pkg, gpu_lib, golden):
+    """A network with large random weights: the solve still converges (Jacobi takes over) to the
+    reference's solution."""
+    g = golden("plate_40x80")
+    m = pkg.plate.quarter_plate(40, 80)
+    D = pkg.constitutive_matrix(1.0, 0.3)
+    K = pkg.build_stiffness_pattern(m)
+    pkg.assemble_stiffness(m, D, 1.0, K)
+    b = np.zeros(m.num_dofs)
+    pkg.add_traction(K, m.boundary_edges["right"], 1.0, 1.0, 0.0, b)
+    pkg.apply_dirichlet(pkg.plate.symmetry_dirichlet(m), K, b)
+    s = pkg.CgJacobiSolver(pkg.SolverOptions(rtol=1e-10, max_iter=200000, preconditioner="learned",
+                                             true_residual_stop=True))
+    s.setup(K)
+    p = (np.random.default_rng(3).standard_normal(pkg.learned.N_PARAMS) * 3.0).astype(np.float32)
+    pkg.learned.setup(K, p, pkg.learned.node_material(D, m.num_nodes))
+    x = np.zeros(m.num_dofs)
+    st = s.solve(b, x)
+    assert st.converged and st.true_rel_residual <= 1e-10, st.message
+    assert _rel(x, g["u"]) < REL_TOL
+    K.ctx.close()
+
+
+def test_training_lowers_the_loss(pkg, gpu_lib):
+    """A few Adam steps on one plate's pairs lower the mean loss from its Jacobi value."""
+    import torch
+    spec = pkg.plate.PlateSpec(n_r=16, n_theta=32, a=1.0, E=1.0, nu=0.3, plane_strain=False)
+    p0 = pkg.learned.init_params(0)
+    prob = pkg.learned.harvest(spec, 24, p0, seed=0)
+    tr = pkg.learned.Trainer(p0)
+    first = tr.accumulate(prob.K, prob.R, prob.E).mean()
+    tr.zero_grad()
+    for _ in range(60):
+        losses = tr.accumulate(prob.K, prob.R, prob.E)
+        tr.step(3e-3, 1.0 / len(losses))
+    last = tr.accumulate(prob.K, prob.R, prob.E).mean()
+    assert np.isfinite(first) and last < 0.9 * first, (first, last)
+    tr.close()
+    prob.K.ctx.close()
