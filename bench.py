@@ -65,6 +65,7 @@ def parse():
     ap.add_argument("--cpu-sample-iters", type=int, default=150)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-preconditioner comparison")
     ap.add_argument("--only", choices=["spmv", "solve", "batch"], default=None,
                     help="profiling modes: `spmv` runs --reps SpMV launches on the assembled plate, "
                          "`solve` one full step, `batch` the 64-plate x 4-load-case batched solve "
@@ -462,6 +463,25 @@ def run_ours(a, dist: Dist):
             st_64 = st
     sync()
 
+    # the learned preconditioner (packaged weights) inside flexible CG, mixed-precision SpMV:
+    # the north star's "learned + mixed" configuration, same matrix, same stopping rule
+    learned = None
+    if not a.no_learned:
+        with torch.cuda.stream(stream):
+            s_l = pkg.CgJacobiSolver(pkg.SolverOptions(rtol=1e-10, max_iter=200000, precision="mixed",
+                                                       preconditioner="learned", true_residual_stop=True))
+            s_l.setup(last["K"])
+            t0 = time.perf_counter()
+            pkg.learned.setup(last["K"], pkg.learned.load_weights(), pkg.learned.node_material(D, mesh.num_nodes))
+            t_setup = time.perf_counter() - t0
+            s_l.solve(d_b, torch.empty_like(d_x))  # warm-up (graph capture)
+            st_l = s_l.solve(d_b, torch.empty_like(d_x))
+        sync()
+        learned = {"solve_s": st_l.solve_seconds, "setup_s": t_setup, "iterations": st_l.iterations,
+                   "true_rel_residual": st_l.true_rel_residual, "converged": st_l.converged,
+                   "speedup_vs_plain_fp64": st_64.solve_seconds / st_l.solve_seconds,
+                   "message": st_l.message}
+
     # dominant kernels: the SpMVs, timed alone (CUDA events, back-to-back launches)
     K = last["K"]
     N = mesh.num_nodes
@@ -535,6 +555,7 @@ def run_ours(a, dist: Dist):
         "plain_fp64": {"solve_s": st_64.solve_seconds, "iterations": st_64.iterations,
                        "true_rel_residual": st_64.true_rel_residual,
                        "speedup_of_headline": st_64.solve_seconds / st.solve_seconds},
+        "learned_mixed": learned,
         "reference_rule_iterations": st_ref.iterations, "reference_rule_solve_s": st_ref.solve_seconds,
         "pcg_iteration_gbs": iter_bytes / iter_s / 1e9,
         "roofline": roofline,

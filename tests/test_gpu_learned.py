@@ -168,3 +168,46 @@ def test_training_lowers_the_loss(pkg, gpu_lib):
     assert np.isfinite(first) and last < 0.9 * first, (first, last)
     tr.close()
     prob.K.ctx.close()
+
+
+def test_trained_network_gain_on_held_out_plates(pkg, gpu_lib):
+    """What the packaged (trained) network gains over the method without it, measured on plates
+    it was not trained on: its loss (the energy-norm angle between M(r) and the error) is lower
+    than the Jacobi step's (the network with its output layer at zero), and the flexible-CG
+    solve with it still converges to the FP64 solution (Jacobi takes over on stagnation)."""
+    w = pkg.learned.load_weights()
+    jac = w.copy()
+    jac[-130:] = 0.0  # output layer off: z = D^-1 r
+    specs = pkg.plate.random_batch(count=3, seed=99, n_r_range=(20, 60))
+    gains = []
+    for i, spec in enumerate(specs):
+        prob = pkg.learned.harvest(spec, 40, w, seed=100 + i)
+        losses = {}
+        for name, p in (("trained", w), ("jacobi", jac)):
+            tr = pkg.learned.Trainer(p)
+            losses[name] = tr.accumulate(prob.K, prob.R, prob.E).mean()
+            tr.close()
+        gains.append(losses["jacobi"] - losses["trained"])
+        prob.K.ctx.close()
+    assert np.mean(gains) > 0.0, gains
+
+    m = pkg.plate.quarter_plate(30, 60)
+    D = pkg.constitutive_matrix(1.0, 0.3)
+    K = pkg.build_stiffness_pattern(m)
+    pkg.assemble_stiffness(m, D, 1.0, K)
+    b = np.zeros(m.num_dofs)
+    pkg.add_traction(K, m.boundary_edges["right"], 1.0, 1.0, 0.0, b)
+    pkg.apply_dirichlet(pkg.plate.symmetry_dirichlet(m), K, b)
+    ref = pkg.CgJacobiSolver(pkg.SolverOptions(rtol=1e-12, max_iter=100000))
+    ref.setup(K)
+    x_ref = np.zeros(m.num_dofs)
+    assert ref.solve(b, x_ref).converged
+    s = pkg.CgJacobiSolver(pkg.SolverOptions(rtol=1e-10, max_iter=200000, precision="mixed",
+                                             preconditioner="learned", true_residual_stop=True))
+    s.setup(K)
+    pkg.learned.setup(K, w, pkg.learned.node_material(D, m.num_nodes))
+    x = np.zeros(m.num_dofs)
+    st = s.solve(b, x)
+    assert st.converged and st.true_rel_residual <= 1e-10, st.message
+    assert _rel(x, x_ref) < REL_TOL
+    K.ctx.close()
