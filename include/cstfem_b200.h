@@ -219,6 +219,18 @@ int cstg_element_stresses(cstg_ctx* ctx, const double* u, double E, double nu, i
 int cstg_add_traction(cstg_ctx* ctx, int n_edges, const int32_t* edges, double thickness,
                       double tx, double ty, double* f);
 
+/* add_traction on the GPU (src/bc.cpp:190-253; kind CSTG_TRACTION_KIRSCH: the traction of the
+ * analytical Kirsch field, src/kirsch.cpp:40-45, with a = p0, sigma_inf = p1; CONSTANT: t = (p0,
+ * p1)). Edges (2 x n_edges node indices) and f (n_rows doubles, accumulated into) are device
+ * pointers; the node -> triangle incidence of cstg_build_pattern is used. A constant traction
+ * gives loads bit-identical to the reference; the Kirsch traction agrees to rounding (GPU sin,
+ * cos, atan2). An edge not adjacent to exactly one triangle leaves f untouched and returns
+ * CSTG_ERR_MESH with the reference's message. */
+#define CSTG_TRACTION_CONSTANT 0
+#define CSTG_TRACTION_KIRSCH 1
+int cstg_add_traction_device(cstg_ctx* ctx, int n_edges, const int32_t* d_edges, double thickness, int kind,
+                             double p0, double p1, double* d_f);
+
 /* ---- Jacobi-PCG without allocating ----------------------------------------------------------
  * No counterpart in the reference. For callers that cannot allocate device memory where they
  * solve: applications with a fixed device-memory budget whose pool allocator forbids foreign
@@ -313,6 +325,19 @@ int cstg_trainer_accumulate(cstg_trainer* tr, cstg_ctx* ctx, int n_samples, cons
 int cstg_trainer_step(cstg_trainer* tr, float lr, float grad_scale);
 int cstg_trainer_params(cstg_trainer* tr, float* params, float* grads);
 int cstg_trainer_zero_grad(cstg_trainer* tr);
+
+/* ---- Gmsh .msh 4.1 reader (host) --------------------------------------------------------------
+ * ≙ read_gmsh (include/cstfem/mesh.hpp, src/mesh_io.cpp): ASCII 4.1 only; triangles turned
+ * counter-clockwise (counted in `flipped`); line elements filed by physical-group name (groups in
+ * name order). On error returns CSTG_ERR_MESH with "path:line: message" in err. No GPU needed. */
+typedef struct cstg_mesh cstg_mesh;
+int cstg_read_gmsh(const char* path, cstg_mesh** mesh, char* err, int err_len);
+void cstg_mesh_destroy(cstg_mesh* mesh);
+int cstg_mesh_info(const cstg_mesh* mesh, int* n_nodes, int* n_tri, int* n_groups, int* flipped);
+/* xy: 2 per node, tri: 3 per triangle (0-based), node_tags: the file's tags (any may be NULL) */
+int cstg_mesh_arrays(const cstg_mesh* mesh, double* xy, int32_t* tri, long long* node_tags);
+/* group `index` (0 .. n_groups-1): its name and edges (2 node indices each; NULL to query) */
+int cstg_mesh_group(const cstg_mesh* mesh, int index, char* name, int name_len, int* n_edges, int32_t* edges);
 
 #ifdef __cplusplus
 }

@@ -7,12 +7,13 @@ C++ interface on top of it, `plate` generates the synthetic O-grid plates.
 The directory name is not a Python identifier; import it with
 ``importlib.import_module("mpi-cst-fem-solver_b200")``.
 """
-from . import batch, build, learned, native, plate  # noqa: F401
+from . import batch, build, learned, mesh_io, native, plate  # noqa: F401
+from .mesh_io import read_gmsh, write_gmsh  # noqa: F401
 from .native import CstgError, LogicError  # noqa: F401
 from .batch import BatchSolution, BatchSolver, PlateBatch, build_batch  # noqa: F401
 from .solver import (CgJacobiSolver, Context, DirichletDofs, GpuCsrMatrix,  # noqa: F401
                      PlaneCondition, SolverOptions, SolverStats, add_dirichlet_group,
-                     add_traction, apply_dirichlet, assemble_stiffness, build_stiffness_pattern,
+                     add_kirsch_traction, add_traction, apply_dirichlet, assemble_stiffness, build_stiffness_pattern,
                      compute_element_stresses, constitutive_matrix, pcg_jacobi, scf_at_hole)
 
 __version__ = "0.1.0"

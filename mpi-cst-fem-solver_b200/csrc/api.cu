@@ -86,7 +86,8 @@ void cstg_destroy(cstg_ctx* ctx) {
                    &ctx->mat_tab, &ctx->bat_sys, &ctx->bat_order, &ctx->bat_queue, &ctx->bat_b,
                    &ctx->bat_x,   &ctx->bat_r,  &ctx->bat_p,    &ctx->bat_Ap,   &ctx->bat_stats,
                    &ctx->bat_in,  &ctx->bat_out, &ctx->lp_p32, &ctx->lp_pb,   &ctx->lp_pf,
-                   &ctx->lp_sf,   &ctx->lp_h0,  &ctx->lp_h1,    &ctx->lp_sc,    &ctx->lp_z};
+                   &ctx->lp_sf,   &ctx->lp_h0,  &ctx->lp_h1,    &ctx->lp_sc,    &ctx->lp_z,
+                   &ctx->tr_con,  &ctx->tr_cnt, &ctx->tr_ptr,   &ctx->tr_cur,   &ctx->tr_rec};
   for (DevBuf* b : all) free_buf(*b);
   if (ctx->h_err) cudaFreeHost(ctx->h_err);
   if (ctx->h_state) cudaFreeHost(ctx->h_state);
@@ -919,6 +920,47 @@ int cstg_add_traction(cstg_ctx* ctx, int n_edges, const int32_t* edges, double t
     }
   }
   return CSTG_OK;
+}
+
+int cstg_add_traction_device(cstg_ctx* ctx, int n_edges, const int32_t* d_edges, double thickness, int kind,
+                             double p0, double p1, double* d_f) {
+  BEGIN(ctx);
+  if (ctx->kind != 1)
+    return fail(ctx, CSTG_ERR_STATE, "add_traction: needs the node incidence of cstg_build_pattern");
+  if (n_edges < 0 || (n_edges > 0 && (!d_edges || !d_f)))
+    return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "add_traction: bad arguments");
+  if (kind != CSTG_TRACTION_CONSTANT && kind != CSTG_TRACTION_KIRSCH)
+    return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "add_traction: unknown traction kind %d", kind);
+  if (n_edges == 0) return CSTG_OK;
+  const int N = ctx->n_nodes;
+  ENSURE(ctx->tr_con, sizeof(double) * 8 * (size_t)n_edges);
+  ENSURE(ctx->tr_cnt, sizeof(int) * (size_t)N);
+  ENSURE(ctx->tr_cur, sizeof(int) * (size_t)N);
+  ENSURE(ctx->tr_ptr, sizeof(int) * ((size_t)N + 1));
+  ENSURE(ctx->tr_rec, sizeof(int) * 2 * (size_t)n_edges);
+  ENSURE(ctx->scan_tmp, sizeof(int) * (size_t)scan_tmp_ints(std::max(N, 1)));
+  MeshDev m;
+  m.n_nodes = N;
+  m.n_tri = ctx->n_tri;
+  m.xy = buf_ptr<double>(ctx->xy);
+  m.tri = buf_ptr<int>(ctx->tri);
+  int* err = buf_ptr<int>(ctx->err_word);
+  RESET_ERR();
+  CK(launch_traction_edges(n_edges, d_edges, m, buf_ptr<int>(ctx->ne_ptr), buf_ptr<int>(ctx->ne), thickness, kind, p0,
+                           p1, buf_ptr<double>(ctx->tr_con), buf_ptr<int>(ctx->tr_cnt), err, ctx->stream));
+  READ_ERR();
+  if (ctx->h_err[kErrRange] != kErrNone)
+    return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "add_traction: edge %d has a node out of range",
+                ctx->h_err[kErrRange]);
+  if (ctx->h_err[kErrEdge] != kErrNone) {
+    int e2[2] = {0, 0};
+    CK(cudaMemcpy(e2, d_edges + 2 * (size_t)ctx->h_err[kErrEdge], sizeof e2, cudaMemcpyDeviceToHost));
+    return fail(ctx, CSTG_ERR_MESH, "traction edge (%d, %d) is not adjacent to exactly one triangle", e2[0], e2[1]);
+  }
+  CK(launch_traction_apply(n_edges, d_edges, N, buf_ptr<double>(ctx->tr_con), buf_ptr<int>(ctx->tr_cnt),
+                           buf_ptr<int>(ctx->tr_ptr), buf_ptr<int>(ctx->tr_cur), buf_ptr<int>(ctx->tr_rec),
+                           buf_ptr<int>(ctx->scan_tmp), d_f, ctx->stream));
+  return CSTG_OK;  // asynchronous on the context's stream
 }
 
 }  // extern "C"

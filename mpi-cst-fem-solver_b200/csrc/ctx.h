@@ -78,6 +78,9 @@ struct cstg_ctx {
   int graph_chunk = 0, graph_hist = -1, graph_kind = -1, graph_n = -1, graph_prec = -1, graph_refs = -1;
   const double* graph_b = nullptr;
 
+  // GPU traction: per-edge contributions and per-node records
+  DevBuf tr_con, tr_cnt, tr_ptr, tr_cur, tr_rec;
+
   // multi-material assembly
   DevBuf mat, mat_tab;
 

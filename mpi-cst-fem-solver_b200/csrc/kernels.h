@@ -16,6 +16,7 @@ enum ErrSlot {
   kErrDiag = 4,        // non-positive diagonal (Dirichlet row or Jacobi setup)
   kErrTimeout = 5,     // bounded device wait gave up
   kErrBatch = 6,       // batched solve: a node coupled to a node of another plate
+  kErrEdge = 7,        // traction edge not adjacent to exactly one triangle
   kErrSlots = 8
 };
 
@@ -221,6 +222,14 @@ cudaError_t launch_spmv_pcg(const BlockMatrix& A, const double* p, double* q, do
                             cudaStream_t s);
 cudaError_t launch_spmv_mixed_pcg(const MixedMatrix& A32, const BlockMatrix& A64, const double* p, double* q,
                                   double* partials, PcgState* st, cudaStream_t s);
+
+// traction.cu: add_traction on the GPU (con: 8 doubles per edge; cnt/cur: n_nodes ints;
+// ptr: n_nodes + 1 ints; rec: 2 n_edges ints)
+cudaError_t launch_traction_edges(int n_edges, const int* edges, const MeshDev& m, const int* ne_ptr, const int* ne,
+                                  double thickness, int kind, double p0, double p1, double* con, int* cnt, int* err,
+                                  cudaStream_t s);
+cudaError_t launch_traction_apply(int n_edges, const int* edges, int n_nodes, const double* con, const int* cnt,
+                                  int* ptr, int* cur, int* rec, int* scan_tmp, double* f, cudaStream_t s);
 
 // Process-wide count of kernel launches issued by this library (graph launches count every
 // kernel node they run).

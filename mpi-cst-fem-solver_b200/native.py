@@ -52,6 +52,9 @@ class SolverOptions(C.Structure):
                 ("launch_mode", C.c_int), ("preconditioner", C.c_int), ("reserved", C.c_int * 2)]
 
 
+TRACTION_CONSTANT = 0
+TRACTION_KIRSCH = 1
+
 PRECOND_JACOBI = 0
 PRECOND_LEARNED = 1
 
@@ -106,6 +109,7 @@ _SIGS = {
                                         _vp]),
     "cstg_element_stresses": (C.c_int, [_vp, _vp, C.c_double, C.c_double, C.c_int, _vp]),
     "cstg_add_traction": (C.c_int, [_vp, C.c_int, _vp, C.c_double, C.c_double, C.c_double, _vp]),
+    "cstg_add_traction_device": (C.c_int, [_vp, C.c_int, _vp, C.c_double, C.c_int, C.c_double, C.c_double, _vp]),
     "cstg_pcg_solve_static": (C.c_int, [C.c_int, _vp, _vp, _vp, _vp, _vp, C.POINTER(SolverOptions),
                                         C.POINTER(Stats), _vp]),
     "cstg_assemble_materials": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp]),
@@ -119,6 +123,12 @@ _SIGS = {
                                       C.POINTER(BatchConfig), C.POINTER(C.c_double)]),
     "cstg_pcg_iterates_device": (C.c_int, [_vp, _vp, C.c_int, C.c_int, _vp, C.POINTER(C.c_int),
                                            C.POINTER(SolverOptions), C.POINTER(Stats)]),
+    "cstg_read_gmsh": (C.c_int, [C.c_char_p, C.POINTER(_vp), C.c_char_p, C.c_int]),
+    "cstg_mesh_destroy": (None, [_vp]),
+    "cstg_mesh_info": (C.c_int, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                 C.POINTER(C.c_int)]),
+    "cstg_mesh_arrays": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "cstg_mesh_group": (C.c_int, [_vp, C.c_int, C.c_char_p, C.c_int, C.POINTER(C.c_int), _vp]),
     "cstg_mpnn_param_count": (C.c_longlong, []),
     "cstg_learned_setup": (C.c_int, [_vp, _vp, _vp]),
     "cstg_learned_set_params": (C.c_int, [_vp, _vp]),

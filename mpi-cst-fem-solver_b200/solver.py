@@ -259,11 +259,33 @@ def apply_dirichlet(dofs, K: GpuCsrMatrix, b) -> None:
 
 def add_traction(K_or_ctx, group_edges, thickness: float, tx: float, ty: float, f) -> None:
     """Consistent nodal forces of a constant traction on line edges (bc.cpp:190-253), added to
-    the host array f. Uses the host mesh held by the context."""
+    f. Host f (numpy): computed on the host from the context's host mesh. CUDA f (torch): on the
+    GPU with the pattern's node incidence (cstg_add_traction_device); same bits either way."""
     ctx = K_or_ctx.ctx if isinstance(K_or_ctx, GpuCsrMatrix) else K_or_ctx
+    if _is_device(f):
+        _traction_device(ctx, group_edges, thickness, native.TRACTION_CONSTANT, tx, ty, f)
+        return
     e = _i32(np.asarray(group_edges).reshape(-1))
     ctx.check(ctx.L.cstg_add_traction(ctx.h, e.size // 2, _ptr(e), float(thickness), float(tx),
                                       float(ty), _ptr(f)))
+
+
+def add_kirsch_traction(K_or_ctx, group_edges, thickness: float, a: float, sigma_inf: float, f) -> None:
+    """Traction sigma . n of the analytical Kirsch field (kirsch.cpp:40-45) on line edges, added
+    to the CUDA tensor f on the GPU."""
+    ctx = K_or_ctx.ctx if isinstance(K_or_ctx, GpuCsrMatrix) else K_or_ctx
+    if not _is_device(f):
+        raise CstgError(native.ERR_INVALID_ARGUMENT, "add_kirsch_traction: f must be a CUDA float64 tensor")
+    _traction_device(ctx, group_edges, thickness, native.TRACTION_KIRSCH, a, sigma_inf, f)
+
+
+def _traction_device(ctx, group_edges, thickness, kind, p0, p1, f):
+    import torch
+    e = torch.as_tensor(np.asarray(group_edges).reshape(-1) if not _is_device(group_edges) else group_edges,
+                        dtype=torch.int32, device=f.device).contiguous()
+    f = _f64(f)
+    ctx.check(ctx.L.cstg_add_traction_device(ctx.h, e.numel() // 2, _ptr(e), float(thickness), int(kind),
+                                             float(p0), float(p1), _ptr(f)))
 
 
 @dataclasses.dataclass
