@@ -82,6 +82,9 @@ typedef struct {
 #define CSTG_PRECOND_JACOBI 0   /* Jacobi (the reference's CgJacobiSolver)                      */
 #define CSTG_PRECOND_LEARNED 1  /* the learned network inside flexible CG, Jacobi as fallback;
                                    needs cstg_learned_setup after cstg_pcg_setup                */
+#define CSTG_PRECOND_AMG 2      /* smoothed-aggregation multigrid V(2,2) cycle (no reference
+                                   counterpart); hierarchy built on the first solve after
+                                   cstg_pcg_setup (or by cstg_amg_setup)                         */
 
 /* launch_mode of cstg_pcg_solve */
 #define CSTG_LAUNCH_AUTO 0        /* persistent kernel for mesh-pattern matrices, else graph  */
@@ -338,6 +341,24 @@ int cstg_mesh_info(const cstg_mesh* mesh, int* n_nodes, int* n_tri, int* n_group
 int cstg_mesh_arrays(const cstg_mesh* mesh, double* xy, int32_t* tri, long long* node_tags);
 /* group `index` (0 .. n_groups-1): its name and edges (2 node indices each; NULL to query) */
 int cstg_mesh_group(const cstg_mesh* mesh, int index, char* name, int name_len, int* n_edges, int32_t* edges);
+
+/* ---- multigrid preconditioner -------------------------------------------------------------------
+ * No counterpart in the reference. Smoothed aggregation on the GPU: distance-2 MIS aggregates of
+ * the node graph, tentative prolongator from the 2D rigid-body modes (per-aggregate QR), one
+ * damped-Jacobi prolongator smoothing step, Galerkin coarse operators (3 x 3 blocks), dense
+ * inverse of the coarsest level; the preconditioner is one V(2,2) cycle with damped Jacobi
+ * (weight 4 / (3 lambda_max(D^-1 A)), lambda_max by power iteration). Deterministic. Used by
+ * cstg_pcg_solve with opt->preconditioner = CSTG_PRECOND_AMG (flexible CG driver, FP64 true-
+ * residual check as for the other preconditioners). Mesh-pattern matrices only. */
+typedef struct {
+  int levels;
+  int dofs[16];
+  long long nnz[16];
+  double setup_seconds;
+} cstg_amg_info;
+int cstg_amg_setup(cstg_ctx* ctx, cstg_amg_info* info);
+/* z = M r (device vectors) with the context's hierarchy (built if missing). */
+int cstg_amg_apply_device(cstg_ctx* ctx, const double* d_r, double* d_z);
 
 #ifdef __cplusplus
 }

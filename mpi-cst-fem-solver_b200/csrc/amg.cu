@@ -1,0 +1,911 @@
+// Smoothed-aggregation algebraic multigrid (a preconditioner for the same Jacobi-PCG path; no
+// reference counterpart). Setup and V-cycle kernels; host orchestration in amg_api.cu.
+//
+// Levels hold block-sparse matrices (BSR, row-major B x B blocks, B = 2 on the finest level,
+// 3 = the rigid-body modes on coarser levels) and a near-nullspace basis per node (B x 3: the
+// 2D rigid-body modes on the finest level). One coarsening step:
+//   1. aggregation: roots = a distance-2 maximal independent set of the block graph (Luby rounds
+//      with fixed hash priorities), aggregate = root + its neighbours, leftovers join the
+//      aggregated neighbour with the strongest block (Frobenius norm), isolated leftovers become
+//      singletons;
+//   2. tentative prolongator: per aggregate, Gram-Schmidt QR of the stacked nullspace blocks:
+//      P0 = Q (one B x 3 block per node), coarse nullspace = R;
+//   3. smoothed prolongator P = (I - w D^-1 A) P0, w = 4 / (3 lambda_max(D^-1 A));
+//   4. Galerkin coarse operator A_c = P' (A P) (3 x 3 blocks).
+// Every kernel is thread-per-row with a fixed order of additions: the hierarchy and the cycle are
+// deterministic. Rows are built in two passes (count, then fill after a prefix sum); row widths
+// are bounded by kAmgMaxRow (checked: the error word records the first overflow).
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+#include "kernels.h"
+
+namespace cstg {
+
+namespace {
+
+constexpr int kU = 0, kRoot = 1, kOut = 2;  // aggregation states
+
+__device__ __forceinline__ unsigned long long node_key(int i) {
+  unsigned long long h = (unsigned long long)(unsigned)i * 0x9E3779B97F4A7C15ull;
+  h ^= h >> 29;
+  h *= 0xBF58476D1CE4E5B9ull;
+  h ^= h >> 32;
+  return (h & 0xFFFFFFFF00000000ull) | (unsigned)i;  // unique: low bits are the index
+}
+
+// sorted small set insert; returns position or -1 on overflow
+__device__ __forceinline__ int set_insert(int* s, int& n, int v, int cap) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (s[mid] < v)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  if (lo < n && s[lo] == v) return lo;
+  if (n >= cap) return -1;
+  for (int k = n; k > lo; --k) s[k] = s[k - 1];
+  s[lo] = v;
+  ++n;
+  return lo;
+}
+
+__device__ __forceinline__ int row_find(const int* cols, int lo, int hi, int v) {
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (cols[mid] < v)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+// ---- fine-level conversion: the node-run layout -> BSR 2x2 --------------------------------------
+
+__global__ void k_amg_bsr2(int N, const int* __restrict__ node_ptr, const double* __restrict__ vals,
+                           double* __restrict__ out) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  const int b0 = node_ptr[n], deg = node_ptr[n + 1] - b0;
+  const double* ra = vals + 4L * b0;
+  const double* rb = ra + 2 * deg;
+  for (int k = 0; k < deg; ++k) {
+    double* o = out + 4L * (b0 + k);
+    o[0] = ra[2 * k];
+    o[1] = ra[2 * k + 1];
+    o[2] = rb[2 * k];
+    o[3] = rb[2 * k + 1];
+  }
+}
+
+template <int B>
+__global__ void k_amg_dinv(int n, AmgBsr A, double* __restrict__ dinv, int* err) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int k = row_find(A.col, A.ptr[i], A.ptr[i + 1], i);
+  if (k >= A.ptr[i + 1] || A.col[k] != i) {
+    atomicMin(&err[kErrDiag], i);
+    return;
+  }
+  const double* blk = A.val + (size_t)k * B * B;
+  for (int c = 0; c < B; ++c) {
+    const double d = blk[c * B + c];
+    if (!(d > 0.0)) atomicMin(&err[kErrDiag], i);
+    dinv[(size_t)i * B + c] = d > 0.0 ? 1.0 / d : 0.0;
+  }
+}
+
+// ---- aggregation ----------------------------------------------------------------------------------
+
+__global__ void k_mis_m1(int n, AmgBsr A, const int* __restrict__ state, unsigned long long* __restrict__ m1) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  unsigned long long m = 0;
+  for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) {
+    const int j = A.col[k];
+    if (state[j] == kU) m = max(m, node_key(j) + 1);
+  }
+  m1[i] = m;
+}
+
+__global__ void k_mis_root(int n, AmgBsr A, int* __restrict__ state, const unsigned long long* __restrict__ m1,
+                           int* __restrict__ newroot) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  newroot[i] = 0;
+  if (state[i] != kU) return;
+  unsigned long long m = 0;
+  for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) m = max(m, m1[A.col[k]]);
+  if (m == node_key(i) + 1) newroot[i] = 1;
+}
+
+// near[i] = 1 if a new root is in N(i) (incl. i)
+__global__ void k_mis_near(int n, AmgBsr A, const int* __restrict__ newroot, int* __restrict__ near) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int f = 0;
+  for (int k = A.ptr[i]; k < A.ptr[i + 1] && !f; ++k) f = newroot[A.col[k]];
+  near[i] = f;
+}
+
+__global__ void k_mis_out(int n, AmgBsr A, int* __restrict__ state, const int* __restrict__ newroot,
+                          const int* __restrict__ near, int* __restrict__ undecided) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (newroot[i]) {
+    state[i] = kRoot;
+    return;
+  }
+  if (state[i] != kU) return;
+  int f = 0;
+  for (int k = A.ptr[i]; k < A.ptr[i + 1] && !f; ++k) f = near[A.col[k]];
+  if (f)
+    state[i] = kOut;
+  else
+    atomicAdd(undecided, 1);
+}
+
+// phase 1: roots (ids from the prefix sum of root flags) and their neighbours
+__global__ void k_agg_phase1(int n, AmgBsr A, const int* __restrict__ state, const int* __restrict__ root_id,
+                             int* __restrict__ agg) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int a = -1;
+  if (state[i] == kRoot) {
+    a = root_id[i];
+  } else {
+    for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) {
+      const int j = A.col[k];
+      if (state[j] == kRoot) {
+        a = root_id[j];
+        break;
+      }
+    }
+  }
+  agg[i] = a;
+}
+
+// phase 2: join the aggregated neighbour (phase-1 assignment) with the strongest block
+template <int B>
+__global__ void k_agg_phase2(int n, AmgBsr A, const int* __restrict__ agg1, int* __restrict__ agg2) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int a = agg1[i];
+  if (a < 0) {
+    double best = -1.0;
+    for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) {
+      const int j = A.col[k];
+      if (j == i || agg1[j] < 0) continue;
+      const double* blk = A.val + (size_t)k * B * B;
+      double s = 0.0;
+      for (int q = 0; q < B * B; ++q) s += blk[q] * blk[q];
+      if (s > best) {
+        best = s;
+        a = agg1[j];
+      }
+    }
+  }
+  agg2[i] = a;
+}
+
+// phase 3: leftovers become singleton aggregates numbered after the others
+__global__ void k_agg_phase3(int n, int n_agg, const int* __restrict__ left_id, int* __restrict__ agg) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (agg[i] < 0) agg[i] = n_agg + left_id[i];
+}
+
+__global__ void k_flag_negative(int n, const int* __restrict__ a, int* __restrict__ f) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) f[i] = a[i] < 0 ? 1 : 0;
+}
+
+__global__ void k_flag_eq(int n, const int* __restrict__ a, int v, int* __restrict__ f) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) f[i] = a[i] == v ? 1 : 0;
+}
+
+// members of each aggregate (count / fill / sort by node)
+__global__ void k_count_by(int n, const int* __restrict__ key, int* __restrict__ cnt) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) atomicAdd(&cnt[key[i]], 1);
+}
+
+__global__ void k_fill_by(int n, const int* __restrict__ key, const int* __restrict__ ptr, int* __restrict__ cur,
+                          int* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[ptr[key[i]] + atomicAdd(&cur[key[i]], 1)] = i;
+}
+
+__global__ void k_sort_segments(int m, const int* __restrict__ ptr, int* __restrict__ v) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= m) return;
+  for (int i = ptr[s] + 1; i < ptr[s + 1]; ++i) {
+    const int x = v[i];
+    int j = i - 1;
+    while (j >= ptr[s] && v[j] > x) {
+      v[j + 1] = v[j];
+      --j;
+    }
+    v[j + 1] = x;
+  }
+}
+
+// ---- tentative prolongator: per aggregate, QR (modified Gram-Schmidt) of the stacked B x 3 blocks ----
+
+template <int B>
+__global__ void k_amg_tentative(int n_agg, const int* __restrict__ agg_ptr, const int* __restrict__ members,
+                                const double* __restrict__ Bf, double* __restrict__ P0, double* __restrict__ Bc,
+                                int* err) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= n_agg) return;
+  const int lo = agg_ptr[a], hi = agg_ptr[a + 1], m = hi - lo;
+  if (m > kAmgMaxAgg) {
+    atomicMin(&err[kErrAmg], a);
+    return;
+  }
+  const int rows = m * B;
+  double R[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  // Q is written in place into P0 (node-major B x 3 blocks): column c of the stacked matrix
+  // lives at P0[node * B*3 + r * 3 + c]
+  for (int q = 0; q < m; ++q) {
+    const int node = members[lo + q];
+    for (int k = 0; k < B * 3; ++k) P0[(size_t)node * B * 3 + k] = Bf[(size_t)node * B * 3 + k];
+  }
+  auto at = [&](int row, int c) -> double& {
+    const int node = members[lo + row / B];
+    return P0[(size_t)node * B * 3 + (row % B) * 3 + c];
+  };
+  double scale = 0.0;
+  for (int r = 0; r < rows; ++r)
+    for (int c = 0; c < 3; ++c) scale = fmax(scale, fabs(at(r, c)));
+  for (int c = 0; c < 3; ++c) {
+    for (int p = 0; p < c; ++p) {
+      double d = 0.0;
+      for (int r = 0; r < rows; ++r) d += at(r, p) * at(r, c);
+      R[p * 3 + c] = d;
+      for (int r = 0; r < rows; ++r) at(r, c) -= d * at(r, p);
+    }
+    double nrm = 0.0;
+    for (int r = 0; r < rows; ++r) nrm += at(r, c) * at(r, c);
+    nrm = sqrt(nrm);
+    if (nrm <= 1e-10 * (scale > 0.0 ? scale : 1.0)) {  // dependent column (tiny aggregate): drop it
+      R[c * 3 + c] = 0.0;
+      for (int r = 0; r < rows; ++r) at(r, c) = 0.0;
+    } else {
+      R[c * 3 + c] = nrm;
+      for (int r = 0; r < rows; ++r) at(r, c) /= nrm;
+    }
+  }
+  for (int k = 0; k < 9; ++k) Bc[(size_t)a * 9 + k] = R[k];
+}
+
+// ---- lambda_max(D^-1 A) by power iteration: y = D^-1 A x, and ||y||^2 -----------------------------
+
+template <int B>
+__global__ void __launch_bounds__(kThreads) k_amg_dinva(int n, AmgBsr A, const double* __restrict__ dinv,
+                                                        const double* __restrict__ x, double* __restrict__ y,
+                                                        double* __restrict__ part) {
+  double ss = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double acc[B];
+#pragma unroll
+    for (int r = 0; r < B; ++r) acc[r] = 0.0;
+    for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) {
+      const double* blk = A.val + (size_t)k * B * B;
+      const double* xj = x + (size_t)A.col[k] * B;
+#pragma unroll
+      for (int r = 0; r < B; ++r)
+#pragma unroll
+        for (int c = 0; c < B; ++c) acc[r] = fma(blk[r * B + c], xj[c], acc[r]);
+    }
+#pragma unroll
+    for (int r = 0; r < B; ++r) {
+      const double v = dinv[(size_t)i * B + r] * acc[r];
+      y[(size_t)i * B + r] = v;
+      ss = fma(v, v, ss);
+    }
+  }
+  __shared__ double sm[kWarps];
+  const double s = block_sum<kThreads>(ss, sm);
+  if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+__global__ void k_amg_scale(int n, const double* __restrict__ part, int nparts, double* __restrict__ x,
+                            double* __restrict__ lam) {
+  double s = 0.0;
+  for (int b = 0; b < nparts; ++b) s += part[b];
+  const double nrm = sqrt(s);
+  if (blockIdx.x == 0 && threadIdx.x == 0) *lam = nrm;
+  const double inv = nrm > 0.0 ? 1.0 / nrm : 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] *= inv;
+}
+
+__global__ void k_amg_init_vec(int n, double* __restrict__ x) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    x[i] = 1.0 + 0.5 * (double)((node_key(i) >> 40) & 0xff) / 255.0;
+}
+
+// ---- smoothed prolongator P = P0 - w D^-1 A P0 --------------------------------------------------------
+
+template <int B>
+__global__ void k_amg_p_count(int n, AmgBsr A, const int* __restrict__ agg, int* __restrict__ cnt, int* err) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int s[kAmgMaxRow];
+  int m = 0;
+  for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k)
+    if (set_insert(s, m, agg[A.col[k]], kAmgMaxRow) < 0) {
+      atomicMin(&err[kErrAmg], i);
+      break;
+    }
+  if (set_insert(s, m, agg[i], kAmgMaxRow) < 0) atomicMin(&err[kErrAmg], i);
+  cnt[i] = m;
+}
+
+template <int B>
+__global__ void k_amg_p_fill(int n, AmgBsr A, const int* __restrict__ agg, const double* __restrict__ P0,
+                             const double* __restrict__ dinv, const double* __restrict__ wp, AmgBsr P) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double w = 4.0 / (3.0 * *wp);
+  int* cols = const_cast<int*>(P.col) + P.ptr[i];
+  double* vals = const_cast<double*>(P.val) + (size_t)P.ptr[i] * B * 3;
+  int m = 0;
+  for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) set_insert(cols, m, agg[A.col[k]], kAmgMaxRow);
+  set_insert(cols, m, agg[i], kAmgMaxRow);
+  for (int q = 0; q < m * B * 3; ++q) vals[q] = 0.0;
+  // - w D^-1 sum_j A_ij P0_j, in ascending j
+  for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) {
+    const int j = A.col[k];
+    const int s = row_find(cols, 0, m, agg[j]);
+    const double* blk = A.val + (size_t)k * B * B;
+    const double* p0 = P0 + (size_t)j * B * 3;
+    double* o = vals + (size_t)s * B * 3;
+    for (int r = 0; r < B; ++r) {
+      const double f = -w * dinv[(size_t)i * B + r];
+      for (int c = 0; c < 3; ++c) {
+        double t = 0.0;
+        for (int q = 0; q < B; ++q) t = fma(blk[r * B + q], p0[q * 3 + c], t);
+        o[r * 3 + c] = fma(f, t, o[r * 3 + c]);
+      }
+    }
+  }
+  const int s = row_find(cols, 0, m, agg[i]);
+  for (int q = 0; q < B * 3; ++q) vals[(size_t)s * B * 3 + q] += P0[(size_t)i * B * 3 + q];
+}
+
+// ---- AP = A P (rows: B x 3 blocks) --------------------------------------------------------------------
+
+template <int B>
+__global__ void k_amg_ap_count(int n, AmgBsr A, AmgBsr P, int* __restrict__ cnt, int* err) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int s[kAmgMaxRow];
+  int m = 0;
+  bool over = false;
+  for (int k = A.ptr[i]; k < A.ptr[i + 1] && !over; ++k) {
+    const int j = A.col[k];
+    for (int q = P.ptr[j]; q < P.ptr[j + 1]; ++q)
+      if (set_insert(s, m, P.col[q], kAmgMaxRow) < 0) {
+        over = true;
+        break;
+      }
+  }
+  if (over) atomicMin(&err[kErrAmg], i);
+  cnt[i] = m;
+}
+
+template <int B>
+__global__ void k_amg_ap_fill(int n, AmgBsr A, AmgBsr P, AmgBsr AP) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int* cols = const_cast<int*>(AP.col) + AP.ptr[i];
+  double* vals = const_cast<double*>(AP.val) + (size_t)AP.ptr[i] * B * 3;
+  int m = 0;
+  for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) {
+    const int j = A.col[k];
+    for (int q = P.ptr[j]; q < P.ptr[j + 1]; ++q) set_insert(cols, m, P.col[q], kAmgMaxRow);
+  }
+  for (int q = 0; q < m * B * 3; ++q) vals[q] = 0.0;
+  for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) {
+    const int j = A.col[k];
+    const double* blk = A.val + (size_t)k * B * B;
+    for (int q = P.ptr[j]; q < P.ptr[j + 1]; ++q) {
+      const int s = row_find(cols, 0, m, P.col[q]);
+      const double* pb = P.val + (size_t)q * B * 3;
+      double* o = vals + (size_t)s * B * 3;
+      for (int r = 0; r < B; ++r)
+        for (int c = 0; c < 3; ++c) {
+          double t = o[r * 3 + c];
+          for (int z = 0; z < B; ++z) t = fma(blk[r * B + z], pb[z * 3 + c], t);
+          o[r * 3 + c] = t;
+        }
+    }
+  }
+}
+
+// P' structure: for each coarse node J the P blocks (fine row, block index) in ascending fine row
+__global__ void k_pt_count(int n, AmgBsr P, int* __restrict__ cnt) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int q = P.ptr[i]; q < P.ptr[i + 1]; ++q) atomicAdd(&cnt[P.col[q]], 1);
+}
+
+__global__ void k_pt_fill(int n, AmgBsr P, const int* __restrict__ ptr, int* __restrict__ cur, int* __restrict__ idx) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int q = P.ptr[i]; q < P.ptr[i + 1]; ++q) {
+    const int J = P.col[q];
+    idx[ptr[J] + atomicAdd(&cur[J], 1)] = q;  // P block index (its fine row is found by search)
+  }
+}
+
+// A_c = P' (AP): coarse row J
+template <int B>
+__global__ void k_amg_ac_count(int nc, const int* __restrict__ pt_ptr, const int* __restrict__ pt_idx,
+                               const int* __restrict__ p_row, AmgBsr AP, int* __restrict__ cnt, int* err) {
+  const int J = blockIdx.x * blockDim.x + threadIdx.x;
+  if (J >= nc) return;
+  int s[kAmgMaxRow];
+  int m = 0;
+  bool over = false;
+  for (int t = pt_ptr[J]; t < pt_ptr[J + 1] && !over; ++t) {
+    const int i = p_row[pt_idx[t]];
+    for (int q = AP.ptr[i]; q < AP.ptr[i + 1]; ++q)
+      if (set_insert(s, m, AP.col[q], kAmgMaxRow) < 0) {
+        over = true;
+        break;
+      }
+  }
+  if (over) atomicMin(&err[kErrAmg], J);
+  cnt[J] = m;
+}
+
+template <int B>
+__global__ void k_amg_ac_fill(int nc, const int* __restrict__ pt_ptr, const int* __restrict__ pt_idx,
+                              const int* __restrict__ p_row, AmgBsr P, AmgBsr AP, AmgBsr Ac) {
+  const int J = blockIdx.x * blockDim.x + threadIdx.x;
+  if (J >= nc) return;
+  int* cols = const_cast<int*>(Ac.col) + Ac.ptr[J];
+  double* vals = const_cast<double*>(Ac.val) + (size_t)Ac.ptr[J] * 9;
+  int m = 0;
+  for (int t = pt_ptr[J]; t < pt_ptr[J + 1]; ++t) {
+    const int i = p_row[pt_idx[t]];
+    for (int q = AP.ptr[i]; q < AP.ptr[i + 1]; ++q) set_insert(cols, m, AP.col[q], kAmgMaxRow);
+  }
+  for (int q = 0; q < m * 9; ++q) vals[q] = 0.0;
+  for (int t = pt_ptr[J]; t < pt_ptr[J + 1]; ++t) {
+    const int pq = pt_idx[t];
+    const int i = p_row[pq];
+    const double* pb = P.val + (size_t)pq * B * 3;  // P_iJ (B x 3)
+    for (int q = AP.ptr[i]; q < AP.ptr[i + 1]; ++q) {
+      const int s = row_find(cols, 0, m, AP.col[q]);
+      const double* ab = AP.val + (size_t)q * B * 3;  // (AP)_iK (B x 3)
+      double* o = vals + (size_t)s * 9;
+      for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) {
+          double v = o[r * 3 + c];
+          for (int z = 0; z < B; ++z) v = fma(pb[z * 3 + r], ab[z * 3 + c], v);
+          o[r * 3 + c] = v;
+        }
+    }
+  }
+}
+
+// fine row of every P block (for P' traversal)
+__global__ void k_p_rows(int n, AmgBsr P, int* __restrict__ p_row) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int q = P.ptr[i]; q < P.ptr[i + 1]; ++q) p_row[q] = i;
+}
+
+// sort the P' lists by fine row (so that A_c's additions follow a fixed order)
+__global__ void k_sort_pt(int nc, const int* __restrict__ ptr, int* __restrict__ idx) {
+  const int J = blockIdx.x * blockDim.x + threadIdx.x;
+  if (J >= nc) return;
+  for (int i = ptr[J] + 1; i < ptr[J + 1]; ++i) {
+    const int x = idx[i];
+    int j = i - 1;
+    while (j >= ptr[J] && idx[j] > x) {  // block indices grow with the fine row
+      idx[j + 1] = idx[j];
+      --j;
+    }
+    idx[j + 1] = x;
+  }
+}
+
+// ---- coarsest level: dense inverse (Gauss-Jordan without pivoting: A is SPD) ---------------------------
+
+template <int B>
+__global__ void k_amg_dense(int nb, AmgBsr A, double* __restrict__ M) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nb) return;
+  const int n = nb * B;
+  for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) {
+    const int j = A.col[k];
+    for (int r = 0; r < B; ++r)
+      for (int c = 0; c < B; ++c) M[(size_t)(B * i + r) * n + B * j + c] = A.val[(size_t)k * B * B + r * B + c];
+  }
+}
+
+// One CTA. M (n x n) is replaced by its inverse; a zero pivot (a dropped nullspace direction
+// leaves an exactly singular coarse row) is skipped: that row and column of the inverse are 0.
+__global__ void __launch_bounds__(1024) k_amg_gauss_jordan(int n, double* __restrict__ M, double* __restrict__ piv) {
+  for (int k = 0; k < n; ++k) {
+    __syncthreads();
+    const double d = M[(size_t)k * n + k];
+    const double scale = fabs(d) > 0.0 ? 1.0 / d : 0.0;
+    if (threadIdx.x == 0) piv[k] = scale;
+    __syncthreads();
+    // column k of the other rows (kept before the row update)
+    for (int i = threadIdx.x; i < n; i += blockDim.x) piv[n + i] = i == k ? 0.0 : M[(size_t)i * n + k];
+    __syncthreads();
+    for (int j = threadIdx.x; j < n; j += blockDim.x) M[(size_t)k * n + j] = j == k ? scale : M[(size_t)k * n + j] * scale;
+    __syncthreads();
+    for (int t = threadIdx.x; t < n * n; t += blockDim.x) {
+      const int i = t / n, j = t - i * n;
+      if (i == k) continue;
+      const double f = piv[n + i];
+      if (j == k)
+        M[(size_t)i * n + j] = -f * scale;
+      else
+        M[(size_t)i * n + j] -= f * M[(size_t)k * n + j];
+    }
+  }
+}
+
+// ---- cycle kernels ----------------------------------------------------------------------------------
+
+// x = w D^-1 b  (first sweep from x = 0)
+template <int B>
+__global__ void k_amg_smooth0(int n, const double* __restrict__ dinv, const double* __restrict__ lam,
+                              const double* __restrict__ b, double* __restrict__ x) {
+  const double w = 4.0 / (3.0 * *lam);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n * B; i += gridDim.x * blockDim.x) x[i] = w * dinv[i] * b[i];
+}
+
+// xo = x + w D^-1 (b - A x)   (RES: xo = b - A x instead)
+template <int B, bool RES>
+__global__ void k_amg_sweep(int n, AmgBsr A, const double* __restrict__ dinv, const double* __restrict__ lam,
+                            const double* __restrict__ b, const double* __restrict__ x, double* __restrict__ xo) {
+  const double w = RES ? 0.0 : 4.0 / (3.0 * *lam);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double acc[B];
+#pragma unroll
+    for (int r = 0; r < B; ++r) acc[r] = 0.0;
+    for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) {
+      const double* blk = A.val + (size_t)k * B * B;
+      const double* xj = x + (size_t)A.col[k] * B;
+      double xv[B];
+#pragma unroll
+      for (int c = 0; c < B; ++c) xv[c] = xj[c];
+#pragma unroll
+      for (int r = 0; r < B; ++r)
+#pragma unroll
+        for (int c = 0; c < B; ++c) acc[r] = fma(blk[r * B + c], xv[c], acc[r]);
+    }
+#pragma unroll
+    for (int r = 0; r < B; ++r) {
+      const size_t d = (size_t)i * B + r;
+      const double res = b[d] - acc[r];
+      xo[d] = RES ? res : fma(w * dinv[d], res, x[d]);
+    }
+  }
+}
+
+// bc_J = sum over P blocks of column J of P_iJ' r_i
+template <int B>
+__global__ void k_amg_restrict(int nc, const int* __restrict__ pt_ptr, const int* __restrict__ pt_idx,
+                               const int* __restrict__ p_row, AmgBsr P, const double* __restrict__ r,
+                               double* __restrict__ bc) {
+  for (int J = blockIdx.x * blockDim.x + threadIdx.x; J < nc; J += gridDim.x * blockDim.x) {
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    for (int t = pt_ptr[J]; t < pt_ptr[J + 1]; ++t) {
+      const int q = pt_idx[t], i = p_row[q];
+      const double* pb = P.val + (size_t)q * B * 3;
+#pragma unroll
+      for (int z = 0; z < B; ++z) {
+        const double rv = r[(size_t)i * B + z];
+        a0 = fma(pb[z * 3 + 0], rv, a0);
+        a1 = fma(pb[z * 3 + 1], rv, a1);
+        a2 = fma(pb[z * 3 + 2], rv, a2);
+      }
+    }
+    bc[3 * (size_t)J] = a0;
+    bc[3 * (size_t)J + 1] = a1;
+    bc[3 * (size_t)J + 2] = a2;
+  }
+}
+
+// x += P xc
+template <int B>
+__global__ void k_amg_prolong(int n, AmgBsr P, const double* __restrict__ xc, double* __restrict__ x) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double acc[B];
+#pragma unroll
+    for (int r = 0; r < B; ++r) acc[r] = x[(size_t)i * B + r];
+    for (int q = P.ptr[i]; q < P.ptr[i + 1]; ++q) {
+      const double* pb = P.val + (size_t)q * B * 3;
+      const double* c = xc + 3 * (size_t)P.col[q];
+#pragma unroll
+      for (int r = 0; r < B; ++r) acc[r] = fma(pb[r * 3 + 2], c[2], fma(pb[r * 3 + 1], c[1], fma(pb[r * 3], c[0], acc[r])));
+    }
+#pragma unroll
+    for (int r = 0; r < B; ++r) x[(size_t)i * B + r] = acc[r];
+  }
+}
+
+// x = M b (dense, n x n): one warp per row
+__global__ void k_amg_gemv(int n, const double* __restrict__ M, const double* __restrict__ b, double* __restrict__ x) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  for (int i = warp; i < n; i += (gridDim.x * blockDim.x) >> 5) {
+    double s = 0.0;
+    for (int j = lane; j < n; j += 32) s = fma(M[(size_t)i * n + j], b[j], s);
+    s = warp_sum(s);
+    if (lane == 0) x[i] = s;
+  }
+}
+
+// 2D rigid-body modes per node: [[1, 0, -y], [0, 1, x]]
+__global__ void k_amg_rigid(int N, const double* __restrict__ xy, double* __restrict__ Bf) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  double* b = Bf + 6 * (size_t)n;
+  b[0] = 1.0;
+  b[1] = 0.0;
+  b[2] = -xy[2 * n + 1];
+  b[3] = 0.0;
+  b[4] = 1.0;
+  b[5] = xy[2 * n];
+}
+
+inline int g1(long long n, int t = 256) { return (int)std::max<long long>(1, std::min<long long>((n + t - 1) / t, 1LL << 30)); }
+inline int gw(long long n) { return (int)std::max<long long>(1, std::min<long long>((n + 255) / 256, 148LL * 8)); }
+
+}  // namespace
+
+// ---- launchers ---------------------------------------------------------------------------------------
+
+cudaError_t amg_fine_bsr(int N, const int* node_ptr, const double* vals, double* out, cudaStream_t s) {
+  k_amg_bsr2<<<g1(N), 256, 0, s>>>(N, node_ptr, vals, out);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t amg_dinv(int B, const AmgBsr& A, double* dinv, int* err, cudaStream_t s) {
+  if (B == 2)
+    k_amg_dinv<2><<<g1(A.n), 256, 0, s>>>(A.n, A, dinv, err);
+  else
+    k_amg_dinv<3><<<g1(A.n), 256, 0, s>>>(A.n, A, dinv, err);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t amg_mis_round(const AmgBsr& A, int* state, unsigned long long* m1, int* newroot, int* near, int* undecided,
+                          cudaStream_t s) {
+  const int n = A.n;
+  cudaMemsetAsync(undecided, 0, sizeof(int), s);
+  k_mis_m1<<<g1(n), 256, 0, s>>>(n, A, state, m1);
+  k_mis_root<<<g1(n), 256, 0, s>>>(n, A, state, m1, newroot);
+  k_mis_near<<<g1(n), 256, 0, s>>>(n, A, newroot, near);
+  k_mis_out<<<g1(n), 256, 0, s>>>(n, A, state, newroot, near, undecided);
+  count_launches(4);
+  return cudaGetLastError();
+}
+
+cudaError_t amg_flag_eq(int n, const int* a, int v, int* f, cudaStream_t s) {
+  k_flag_eq<<<g1(n), 256, 0, s>>>(n, a, v, f);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t amg_aggregate(int B, const AmgBsr& A, const int* state, const int* root_id, int* agg1, int* agg2,
+                          cudaStream_t s) {
+  const int n = A.n;
+  k_agg_phase1<<<g1(n), 256, 0, s>>>(n, A, state, root_id, agg1);
+  if (B == 2)
+    k_agg_phase2<2><<<g1(n), 256, 0, s>>>(n, A, agg1, agg2);
+  else
+    k_agg_phase2<3><<<g1(n), 256, 0, s>>>(n, A, agg1, agg2);
+  count_launches(2);
+  return cudaGetLastError();
+}
+
+cudaError_t amg_flag_negative(int n, const int* a, int* f, cudaStream_t s) {
+  k_flag_negative<<<g1(n), 256, 0, s>>>(n, a, f);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t amg_phase3(int n, int n_agg, const int* left_id, int* agg, cudaStream_t s) {
+  k_agg_phase3<<<g1(n), 256, 0, s>>>(n, n_agg, left_id, agg);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t amg_group(int n, const int* key, int m, int* ptr, int* cnt, int* cur, int* out, int* scan_tmp,
+                      cudaStream_t s) {
+  cudaMemsetAsync(cnt, 0, sizeof(int) * (size_t)m, s);
+  cudaMemsetAsync(cur, 0, sizeof(int) * (size_t)m, s);
+  k_count_by<<<g1(n), 256, 0, s>>>(n, key, cnt);
+  cudaError_t e = scan_exclusive(cnt, m, ptr, scan_tmp, s);
+  if (e != cudaSuccess) return e;
+  k_fill_by<<<g1(n), 256, 0, s>>>(n, key, ptr, cur, out);
+  k_sort_segments<<<g1(m), 256, 0, s>>>(m, ptr, out);
+  count_launches(3);
+  return cudaGetLastError();
+}
+
+cudaError_t amg_tentative(int B, int n_agg, const int* agg_ptr, const int* members, const double* Bf, double* P0,
+                          double* Bc, int* err, cudaStream_t s) {
+  if (B == 2)
+    k_amg_tentative<2><<<g1(n_agg, 128), 128, 0, s>>>(n_agg, agg_ptr, members, Bf, P0, Bc, err);
+  else
+    k_amg_tentative<3><<<g1(n_agg, 128), 128, 0, s>>>(n_agg, agg_ptr, members, Bf, P0, Bc, err);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t amg_lambda(int B, const AmgBsr& A, const double* dinv, double* x, double* y, double* part, double* lam,
+                       int iters, cudaStream_t s) {
+  const int n = A.n * B;
+  const int G = 148;
+  k_amg_init_vec<<<gw(n), 256, 0, s>>>(n, x);
+  for (int t = 0; t < iters; ++t) {
+    if (B == 2)
+      k_amg_dinva<2><<<G, kThreads, 0, s>>>(A.n, A, dinv, x, y, part);
+    else
+      k_amg_dinva<3><<<G, kThreads, 0, s>>>(A.n, A, dinv, x, y, part);
+    k_amg_scale<<<gw(n), 256, 0, s>>>(n, part, G, y, lam);
+    std::swap(x, y);
+  }
+  count_launches(1 + 2LL * iters);
+  return cudaGetLastError();
+}
+
+cudaError_t amg_p_count(int B, const AmgBsr& A, const int* agg, int* cnt, int* err, cudaStream_t s) {
+  if (B == 2)
+    k_amg_p_count<2><<<g1(A.n, 128), 128, 0, s>>>(A.n, A, agg, cnt, err);
+  else
+    k_amg_p_count<3><<<g1(A.n, 128), 128, 0, s>>>(A.n, A, agg, cnt, err);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t amg_p_fill(int B, const AmgBsr& A, const int* agg, const double* P0, const double* dinv, const double* lam,
+                       const AmgBsr& P, cudaStream_t s) {
+  if (B == 2)
+    k_amg_p_fill<2><<<g1(A.n, 128), 128, 0, s>>>(A.n, A, agg, P0, dinv, lam, P);
+  else
+    k_amg_p_fill<3><<<g1(A.n, 128), 128, 0, s>>>(A.n, A, agg, P0, dinv, lam, P);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t amg_ap_count(int B, const AmgBsr& A, const AmgBsr& P, int* cnt, int* err, cudaStream_t s) {
+  if (B == 2)
+    k_amg_ap_count<2><<<g1(A.n, 128), 128, 0, s>>>(A.n, A, P, cnt, err);
+  else
+    k_amg_ap_count<3><<<g1(A.n, 128), 128, 0, s>>>(A.n, A, P, cnt, err);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t amg_ap_fill(int B, const AmgBsr& A, const AmgBsr& P, const AmgBsr& AP, cudaStream_t s) {
+  if (B == 2)
+    k_amg_ap_fill<2><<<g1(A.n, 128), 128, 0, s>>>(A.n, A, P, AP);
+  else
+    k_amg_ap_fill<3><<<g1(A.n, 128), 128, 0, s>>>(A.n, A, P, AP);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t amg_pt(int n, int nc, const AmgBsr& P, int* p_row, int* pt_ptr, int* cnt, int* cur, int* pt_idx,
+                   int* scan_tmp, cudaStream_t s) {
+  cudaMemsetAsync(cnt, 0, sizeof(int) * (size_t)nc, s);
+  cudaMemsetAsync(cur, 0, sizeof(int) * (size_t)nc, s);
+  k_p_rows<<<g1(n), 256, 0, s>>>(n, P, p_row);
+  k_pt_count<<<g1(n), 256, 0, s>>>(n, P, cnt);
+  cudaError_t e = scan_exclusive(cnt, nc, pt_ptr, scan_tmp, s);
+  if (e != cudaSuccess) return e;
+  k_pt_fill<<<g1(n), 256, 0, s>>>(n, P, pt_ptr, cur, pt_idx);
+  k_sort_pt<<<g1(nc), 256, 0, s>>>(nc, pt_ptr, pt_idx);
+  count_launches(4);
+  return cudaGetLastError();
+}
+
+cudaError_t amg_ac_count(int B, int nc, const int* pt_ptr, const int* pt_idx, const int* p_row, const AmgBsr& AP,
+                         int* cnt, int* err, cudaStream_t s) {
+  if (B == 2)
+    k_amg_ac_count<2><<<g1(nc, 128), 128, 0, s>>>(nc, pt_ptr, pt_idx, p_row, AP, cnt, err);
+  else
+    k_amg_ac_count<3><<<g1(nc, 128), 128, 0, s>>>(nc, pt_ptr, pt_idx, p_row, AP, cnt, err);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t amg_ac_fill(int B, int nc, const int* pt_ptr, const int* pt_idx, const int* p_row, const AmgBsr& P,
+                        const AmgBsr& AP, const AmgBsr& Ac, cudaStream_t s) {
+  if (B == 2)
+    k_amg_ac_fill<2><<<g1(nc, 128), 128, 0, s>>>(nc, pt_ptr, pt_idx, p_row, P, AP, Ac);
+  else
+    k_amg_ac_fill<3><<<g1(nc, 128), 128, 0, s>>>(nc, pt_ptr, pt_idx, p_row, P, AP, Ac);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t amg_coarsest(int B, const AmgBsr& A, double* M, double* piv, cudaStream_t s) {
+  const int n = A.n * B;
+  cudaMemsetAsync(M, 0, sizeof(double) * (size_t)n * n, s);
+  if (B == 2)
+    k_amg_dense<2><<<g1(A.n), 256, 0, s>>>(A.n, A, M);
+  else
+    k_amg_dense<3><<<g1(A.n), 256, 0, s>>>(A.n, A, M);
+  k_amg_gauss_jordan<<<1, 1024, 0, s>>>(n, M, piv);
+  count_launches(2);
+  return cudaGetLastError();
+}
+
+cudaError_t amg_smooth0(int B, int n, const double* dinv, const double* lam, const double* b, double* x, cudaStream_t s) {
+  if (B == 2)
+    k_amg_smooth0<2><<<gw((long long)n * B), 256, 0, s>>>(n, dinv, lam, b, x);
+  else
+    k_amg_smooth0<3><<<gw((long long)n * B), 256, 0, s>>>(n, dinv, lam, b, x);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t amg_sweep(int B, bool residual, const AmgBsr& A, const double* dinv, const double* lam, const double* b,
+                      const double* x, double* xo, cudaStream_t s) {
+  const int n = A.n;
+  if (B == 2) {
+    if (residual)
+      k_amg_sweep<2, true><<<gw(n), 256, 0, s>>>(n, A, dinv, lam, b, x, xo);
+    else
+      k_amg_sweep<2, false><<<gw(n), 256, 0, s>>>(n, A, dinv, lam, b, x, xo);
+  } else {
+    if (residual)
+      k_amg_sweep<3, true><<<gw(n), 256, 0, s>>>(n, A, dinv, lam, b, x, xo);
+    else
+      k_amg_sweep<3, false><<<gw(n), 256, 0, s>>>(n, A, dinv, lam, b, x, xo);
+  }
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t amg_restrict(int B, int nc, const int* pt_ptr, const int* pt_idx, const int* p_row, const AmgBsr& P,
+                         const double* r, double* bc, cudaStream_t s) {
+  if (B == 2)
+    k_amg_restrict<2><<<gw(nc), 256, 0, s>>>(nc, pt_ptr, pt_idx, p_row, P, r, bc);
+  else
+    k_amg_restrict<3><<<gw(nc), 256, 0, s>>>(nc, pt_ptr, pt_idx, p_row, P, r, bc);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t amg_prolong(int B, const AmgBsr& P, const double* xc, double* x, cudaStream_t s) {
+  if (B == 2)
+    k_amg_prolong<2><<<gw(P.n), 256, 0, s>>>(P.n, P, xc, x);
+  else
+    k_amg_prolong<3><<<gw(P.n), 256, 0, s>>>(P.n, P, xc, x);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t amg_rigid_modes(int N, const double* xy, double* Bf, cudaStream_t s) {
+  k_amg_rigid<<<g1(N), 256, 0, s>>>(N, xy, Bf);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t amg_gemv(int n, const double* M, const double* b, double* x, cudaStream_t s) {
+  k_amg_gemv<<<gw((long long)n * 32), 256, 0, s>>>(n, M, b, x);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+}  // namespace cstg

@@ -1,0 +1,342 @@
+// Host side of the smoothed-aggregation multigrid preconditioner: the level hierarchy on a
+// context (built on the first CSTG_PRECOND_AMG solve after cstg_pcg_setup, or by cstg_amg_setup)
+// and the V(2,2) cycle z = M r used inside the flexible-CG driver of learned_api.cu.
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <vector>
+
+#include "ctx.h"
+
+namespace {
+
+constexpr int kCoarsestDofs = 600;  // dense inverse at or below this many coarse DOFs
+constexpr int kMaxLevels = 10;
+constexpr int kPowerIters = 20;
+constexpr int kMaxMisRounds = 200;
+
+}  // namespace
+
+struct AmgLevel {
+  int B = 2, n = 0, nc = 0;
+  DevBuf ptr, col, val;          // A (finest level: ptr/col are the context's node pattern)
+  const int* a_ptr = nullptr;
+  const int* a_col = nullptr;
+  DevBuf dinv, lam;
+  DevBuf p_ptr, p_col, p_val, p_row, pt_ptr, pt_idx;  // transfer to the next level
+  DevBuf xa, xb, r, bc;          // cycle vectors (bc: this level's right-hand side, levels >= 1)
+  AmgBsr A() const {
+    AmgBsr m;
+    m.n = n;
+    m.ptr = a_ptr;
+    m.col = a_col;
+    m.val = static_cast<const double*>(val.p);
+    return m;
+  }
+  AmgBsr P() const {
+    AmgBsr m;
+    m.n = n;
+    m.ptr = static_cast<const int*>(p_ptr.p);
+    m.col = static_cast<const int*>(p_col.p);
+    m.val = static_cast<const double*>(p_val.p);
+    return m;
+  }
+};
+
+struct AmgData {
+  std::vector<AmgLevel> L;
+  DevBuf Minv, piv;
+  int n_coarse = 0;           // DOFs of the dense coarsest level
+  unsigned long long built_for = ~0ull;  // setup_count of the matrix it was built from
+  double setup_seconds = 0.0;
+  // scratch of the setup
+  DevBuf state, m1, newroot, near, und, root_id, flags, agg1, agg2, agg_ptr, members, cnt, cur, P0, Bf, Bc, cnt2,
+      ap_ptr, ap_col, ap_val, part, vx, vy;
+};
+
+void cstg_host::amg_free(cstg_ctx* ctx) {
+  if (!ctx->amg) return;
+  AmgData* d = ctx->amg;
+  for (AmgLevel& l : d->L) {
+    DevBuf* all[] = {&l.ptr, &l.col, &l.val, &l.dinv, &l.lam, &l.p_ptr, &l.p_col, &l.p_val, &l.p_row, &l.pt_ptr,
+                     &l.pt_idx, &l.xa, &l.xb, &l.r, &l.bc};
+    for (DevBuf* b : all) free_buf(*b);
+  }
+  DevBuf* all[] = {&d->Minv, &d->piv, &d->state, &d->m1, &d->newroot, &d->near, &d->und, &d->root_id, &d->flags,
+                   &d->agg1, &d->agg2, &d->agg_ptr, &d->members, &d->cnt, &d->cur, &d->P0, &d->Bf, &d->Bc,
+                   &d->cnt2, &d->ap_ptr, &d->ap_col, &d->ap_val, &d->part, &d->vx, &d->vy};
+  for (DevBuf* b : all) free_buf(*b);
+  delete d;
+  ctx->amg = nullptr;
+}
+
+namespace {
+
+int read_int(cstg_ctx* ctx, const int* d, int* h) {
+  CK(cudaMemcpyAsync(h, d, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return CSTG_OK;
+}
+
+// exclusive scan of n ints into out[0..n] and the total
+int scan_total(cstg_ctx* ctx, const int* in, int n, int* out, int* total) {
+  ENSURE(ctx->scan_tmp, sizeof(int) * (size_t)scan_tmp_ints(std::max(n, 1)));
+  CK(scan_exclusive(in, n, out, buf_ptr<int>(ctx->scan_tmp), ctx->stream));
+  return read_int(ctx, out + n, total);
+}
+
+// One coarsening step from level l (matrix and nullspace Bf set) to level l + 1.
+int coarsen(cstg_ctx* ctx, AmgData* d, int l, bool* stop) {
+  AmgLevel& lv = d->L[l];
+  const int B = lv.B, n = lv.n;
+  const AmgBsr A = lv.A();
+  int* err = buf_ptr<int>(ctx->err_word);
+  ENSURE(d->state, sizeof(int) * (size_t)n);
+  ENSURE(d->m1, sizeof(unsigned long long) * (size_t)n);
+  ENSURE(d->newroot, sizeof(int) * (size_t)n);
+  ENSURE(d->near, sizeof(int) * (size_t)n);
+  ENSURE(d->und, 256);
+  ENSURE(d->root_id, sizeof(int) * ((size_t)n + 1));
+  ENSURE(d->flags, sizeof(int) * (size_t)n);
+  ENSURE(d->agg1, sizeof(int) * (size_t)n);
+  ENSURE(d->agg2, sizeof(int) * (size_t)n);
+  ENSURE(d->members, sizeof(int) * (size_t)n);
+  // lambda_max(D^-1 A)
+  ENSURE(lv.lam, sizeof(double));
+  ENSURE(d->part, sizeof(double) * 256);
+  ENSURE(d->vx, sizeof(double) * (size_t)n * B);
+  ENSURE(d->vy, sizeof(double) * (size_t)n * B);
+  CK(amg_lambda(B, A, buf_ptr<double>(lv.dinv), buf_ptr<double>(d->vx), buf_ptr<double>(d->vy),
+                buf_ptr<double>(d->part), buf_ptr<double>(lv.lam), kPowerIters, ctx->stream));
+  // distance-2 maximal independent set
+  CK(cudaMemsetAsync(d->state.p, 0, sizeof(int) * (size_t)n, ctx->stream));
+  int und = n;
+  for (int round = 0; und > 0; ++round) {
+    if (round >= kMaxMisRounds) return fail(ctx, CSTG_ERR_UNSUPPORTED, "amg_setup: aggregation did not settle");
+    CK(amg_mis_round(A, buf_ptr<int>(d->state), buf_ptr<unsigned long long>(d->m1), buf_ptr<int>(d->newroot),
+                     buf_ptr<int>(d->near), buf_ptr<int>(d->und), ctx->stream));
+    const int rc = read_int(ctx, buf_ptr<int>(d->und), &und);
+    if (rc) return rc;
+  }
+  int n_roots = 0, n_left = 0;
+  CK(amg_flag_eq(n, buf_ptr<int>(d->state), 1, buf_ptr<int>(d->flags), ctx->stream));
+  int rc = scan_total(ctx, buf_ptr<int>(d->flags), n, buf_ptr<int>(d->root_id), &n_roots);
+  if (rc) return rc;
+  CK(amg_aggregate(B, A, buf_ptr<int>(d->state), buf_ptr<int>(d->root_id), buf_ptr<int>(d->agg1),
+                   buf_ptr<int>(d->agg2), ctx->stream));
+  CK(amg_flag_negative(n, buf_ptr<int>(d->agg2), buf_ptr<int>(d->flags), ctx->stream));
+  ENSURE(d->cnt, sizeof(int) * ((size_t)n + 1));
+  rc = scan_total(ctx, buf_ptr<int>(d->flags), n, buf_ptr<int>(d->cnt), &n_left);
+  if (rc) return rc;
+  CK(amg_phase3(n, n_roots, buf_ptr<int>(d->cnt), buf_ptr<int>(d->agg2), ctx->stream));
+  const int nc = n_roots + n_left;
+  if (nc <= 0 || nc > (n * 4) / 5) {  // coarsening stalled: this level becomes the coarsest
+    *stop = true;
+    return CSTG_OK;
+  }
+  const int* agg = buf_ptr<int>(d->agg2);
+  // aggregate members, tentative prolongator, coarse nullspace
+  ENSURE(d->agg_ptr, sizeof(int) * ((size_t)nc + 1));
+  ENSURE(d->cnt, sizeof(int) * ((size_t)std::max(n, nc) + 1));
+  ENSURE(d->cur, sizeof(int) * ((size_t)std::max(n, nc) + 1));
+  ENSURE(ctx->scan_tmp, sizeof(int) * (size_t)scan_tmp_ints(std::max(std::max(n, nc), 1)));
+  CK(amg_group(n, agg, nc, buf_ptr<int>(d->agg_ptr), buf_ptr<int>(d->cnt), buf_ptr<int>(d->cur),
+               buf_ptr<int>(d->members), buf_ptr<int>(ctx->scan_tmp), ctx->stream));
+  ENSURE(d->P0, sizeof(double) * (size_t)n * B * 3);
+  ENSURE(d->Bc, sizeof(double) * (size_t)nc * 9);
+  CK(amg_tentative(B, nc, buf_ptr<int>(d->agg_ptr), buf_ptr<int>(d->members), buf_ptr<double>(d->Bf),
+                   buf_ptr<double>(d->P0), buf_ptr<double>(d->Bc), err, ctx->stream));
+  // smoothed prolongator
+  ENSURE(lv.p_ptr, sizeof(int) * ((size_t)n + 1));
+  CK(amg_p_count(B, A, agg, buf_ptr<int>(d->cnt), err, ctx->stream));
+  int nnz_p = 0;
+  rc = scan_total(ctx, buf_ptr<int>(d->cnt), n, buf_ptr<int>(lv.p_ptr), &nnz_p);
+  if (rc) return rc;
+  READ_ERR();
+  if (ctx->h_err[kErrAmg] != kErrNone)
+    return fail(ctx, CSTG_ERR_UNSUPPORTED, "amg_setup: level %d: an aggregate or a prolongator row is too large", l);
+  ENSURE(lv.p_col, sizeof(int) * (size_t)std::max(nnz_p, 1));
+  ENSURE(lv.p_val, sizeof(double) * (size_t)std::max(nnz_p, 1) * B * 3);
+  AmgBsr P = lv.P();
+  CK(amg_p_fill(B, A, agg, buf_ptr<double>(d->P0), buf_ptr<double>(lv.dinv), buf_ptr<double>(lv.lam), P, ctx->stream));
+  // AP
+  ENSURE(d->ap_ptr, sizeof(int) * ((size_t)n + 1));
+  CK(amg_ap_count(B, A, P, buf_ptr<int>(d->cnt), err, ctx->stream));
+  int nnz_ap = 0;
+  rc = scan_total(ctx, buf_ptr<int>(d->cnt), n, buf_ptr<int>(d->ap_ptr), &nnz_ap);
+  if (rc) return rc;
+  ENSURE(d->ap_col, sizeof(int) * (size_t)std::max(nnz_ap, 1));
+  ENSURE(d->ap_val, sizeof(double) * (size_t)std::max(nnz_ap, 1) * B * 3);
+  AmgBsr AP;
+  AP.n = n;
+  AP.ptr = buf_ptr<int>(d->ap_ptr);
+  AP.col = buf_ptr<int>(d->ap_col);
+  AP.val = buf_ptr<double>(d->ap_val);
+  CK(amg_ap_fill(B, A, P, AP, ctx->stream));
+  // P' lists
+  ENSURE(lv.p_row, sizeof(int) * (size_t)std::max(nnz_p, 1));
+  ENSURE(lv.pt_ptr, sizeof(int) * ((size_t)nc + 1));
+  ENSURE(lv.pt_idx, sizeof(int) * (size_t)std::max(nnz_p, 1));
+  CK(amg_pt(n, nc, P, buf_ptr<int>(lv.p_row), buf_ptr<int>(lv.pt_ptr), buf_ptr<int>(d->cnt), buf_ptr<int>(d->cur),
+            buf_ptr<int>(lv.pt_idx), buf_ptr<int>(ctx->scan_tmp), ctx->stream));
+  // coarse operator
+  d->L.emplace_back();
+  AmgLevel& nx = d->L.back();
+  AmgLevel& cur = d->L[l];  // (re-fetched: emplace_back may move the vector)
+  nx.B = 3;
+  nx.n = nc;
+  cur.nc = nc;
+  ENSURE(nx.ptr, sizeof(int) * ((size_t)nc + 1));
+  CK(amg_ac_count(B, nc, buf_ptr<int>(cur.pt_ptr), buf_ptr<int>(cur.pt_idx), buf_ptr<int>(cur.p_row), AP,
+                  buf_ptr<int>(d->cnt), err, ctx->stream));
+  int nnz_c = 0;
+  rc = scan_total(ctx, buf_ptr<int>(d->cnt), nc, buf_ptr<int>(nx.ptr), &nnz_c);
+  if (rc) return rc;
+  READ_ERR();
+  if (ctx->h_err[kErrAmg] != kErrNone)
+    return fail(ctx, CSTG_ERR_UNSUPPORTED, "amg_setup: level %d: a coarse row has more than %d blocks", l + 1,
+                kAmgMaxRow);
+  ENSURE(nx.col, sizeof(int) * (size_t)std::max(nnz_c, 1));
+  ENSURE(nx.val, sizeof(double) * (size_t)std::max(nnz_c, 1) * 9);
+  nx.a_ptr = buf_ptr<int>(nx.ptr);
+  nx.a_col = buf_ptr<int>(nx.col);
+  AmgBsr Ac = nx.A();
+  CK(amg_ac_fill(B, nc, buf_ptr<int>(cur.pt_ptr), buf_ptr<int>(cur.pt_idx), buf_ptr<int>(cur.p_row), cur.P(), AP, Ac,
+                 ctx->stream));
+  // the coarse nullspace becomes the next level's basis
+  ENSURE(d->Bf, sizeof(double) * (size_t)std::max(n * B * 3, nc * 9));
+  CK(cudaMemcpyAsync(d->Bf.p, d->Bc.p, sizeof(double) * (size_t)nc * 9, cudaMemcpyDeviceToDevice, ctx->stream));
+  return CSTG_OK;
+}
+
+int amg_build(cstg_ctx* ctx) {
+  if (!ctx->amg) ctx->amg = new AmgData();
+  AmgData* d = ctx->amg;
+  const auto t0 = std::chrono::steady_clock::now();
+  d->L.clear();
+  d->L.emplace_back();
+  {
+    AmgLevel& f = d->L[0];
+    f.B = 2;
+    f.n = ctx->n_nodes;
+    f.a_ptr = buf_ptr<int>(ctx->node_ptr);
+    f.a_col = buf_ptr<int>(ctx->bnbr);
+    ENSURE(f.val, sizeof(double) * (size_t)ctx->nnz);
+    CK(amg_fine_bsr(f.n, f.a_ptr, buf_ptr<double>(ctx->vals), buf_ptr<double>(f.val), ctx->stream));
+    ENSURE(d->Bf, sizeof(double) * (size_t)f.n * 6);
+    CK(amg_rigid_modes(f.n, buf_ptr<double>(ctx->xy), buf_ptr<double>(d->Bf), ctx->stream));
+  }
+  RESET_ERR();
+  for (int l = 0;; ++l) {
+    AmgLevel& lv = d->L[l];
+    ENSURE(lv.dinv, sizeof(double) * (size_t)lv.n * lv.B);
+    CK(amg_dinv(lv.B, lv.A(), buf_ptr<double>(lv.dinv), buf_ptr<int>(ctx->err_word), ctx->stream));
+    bool stop = lv.n * lv.B <= kCoarsestDofs || l + 1 >= kMaxLevels;
+    if (!stop) {
+      const int rc = coarsen(ctx, d, l, &stop);
+      if (rc) return rc;
+    }
+    if (stop) break;
+  }
+  READ_ERR();
+  if (ctx->h_err[kErrDiag] != kErrNone)
+    return fail(ctx, CSTG_ERR_NONPOSITIVE_DIAGONAL, "amg_setup: non-positive diagonal on a level");
+  AmgLevel& last = d->L.back();
+  d->n_coarse = last.n * last.B;
+  if (d->n_coarse > 1536)
+    return fail(ctx, CSTG_ERR_UNSUPPORTED, "amg_setup: coarsest level has %d DOFs (coarsening stalled)", d->n_coarse);
+  ENSURE(d->Minv, sizeof(double) * (size_t)d->n_coarse * d->n_coarse);
+  ENSURE(d->piv, sizeof(double) * 2 * (size_t)d->n_coarse);
+  // (a matrix at or below the coarsest size is its own coarsest level: the cycle is a direct solve)
+  CK(amg_coarsest(last.B, last.A(), buf_ptr<double>(d->Minv), buf_ptr<double>(d->piv), ctx->stream));
+  // cycle vectors
+  for (size_t l = 0; l < d->L.size(); ++l) {
+    AmgLevel& lv = d->L[l];
+    const size_t m = (size_t)lv.n * lv.B;
+    ENSURE(lv.xa, sizeof(double) * m);
+    ENSURE(lv.xb, sizeof(double) * m);
+    ENSURE(lv.r, sizeof(double) * m);
+    ENSURE(lv.bc, sizeof(double) * m);
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  d->built_for = ctx->setup_count;
+  d->setup_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  return CSTG_OK;
+}
+
+// V(2,2): x = cycle(l, b)
+int vcycle(cstg_ctx* ctx, AmgData* d, size_t l, const double* b, double* x) {
+  AmgLevel& lv = d->L[l];
+  cudaStream_t s = ctx->stream;
+  if (l + 1 == d->L.size()) {
+    CK(amg_gemv(d->n_coarse, buf_ptr<double>(d->Minv), b, x, s));
+    return CSTG_OK;
+  }
+  const AmgBsr A = lv.A();
+  const double* dinv = buf_ptr<double>(lv.dinv);
+  const double* lam = buf_ptr<double>(lv.lam);
+  double* xa = buf_ptr<double>(lv.xa);
+  double* r = buf_ptr<double>(lv.r);
+  AmgLevel& nx = d->L[l + 1];
+  CK(amg_smooth0(lv.B, lv.n, dinv, lam, b, xa, s));
+  CK(amg_sweep(lv.B, false, A, dinv, lam, b, xa, x, s));
+  CK(amg_sweep(lv.B, true, A, dinv, lam, b, x, r, s));
+  CK(amg_restrict(lv.B, lv.nc, buf_ptr<int>(lv.pt_ptr), buf_ptr<int>(lv.pt_idx), buf_ptr<int>(lv.p_row), lv.P(), r,
+                  buf_ptr<double>(nx.bc), s));
+  const int rc = vcycle(ctx, d, l + 1, buf_ptr<double>(nx.bc), buf_ptr<double>(nx.xb));
+  if (rc) return rc;
+  CK(amg_prolong(lv.B, lv.P(), buf_ptr<double>(nx.xb), x, s));
+  CK(amg_sweep(lv.B, false, A, dinv, lam, b, x, xa, s));
+  CK(amg_sweep(lv.B, false, A, dinv, lam, b, xa, x, s));
+  return CSTG_OK;
+}
+
+}  // namespace
+
+int cstg_host::amg_ready(cstg_ctx* ctx) {
+  if (ctx->amg && ctx->amg->built_for == ctx->setup_count) return CSTG_OK;
+  if (ctx->kind != 1 || !ctx->setup_done)
+    return fail(ctx, CSTG_ERR_STATE, "amg_setup: needs a mesh-pattern matrix after cstg_pcg_setup");
+  return amg_build(ctx);
+}
+
+int cstg_host::amg_levels(const cstg_ctx* ctx) { return ctx->amg ? (int)ctx->amg->L.size() : 0; }
+
+int cstg_host::amg_apply(cstg_ctx* ctx, const double* r, double* z) {
+  return vcycle(ctx, ctx->amg, 0, r, z);
+}
+
+extern "C" {
+
+int cstg_amg_setup(cstg_ctx* ctx, cstg_amg_info* info) {
+  BEGIN(ctx);
+  if (ctx->amg) ctx->amg->built_for = ~0ull;  // rebuild
+  const int rc = amg_ready(ctx);
+  if (rc) return rc;
+  if (info) {
+    AmgData* d = ctx->amg;
+    std::memset(info, 0, sizeof *info);
+    info->levels = (int)d->L.size();
+    for (int l = 0; l < info->levels && l < 16; ++l) info->dofs[l] = d->L[l].n * d->L[l].B;
+    for (int l = 0; l < info->levels && l < 16; ++l) {
+      const AmgLevel& lv = d->L[l];
+      int nnzb = 0;
+      CK(cudaMemcpy(&nnzb, lv.a_ptr + lv.n, sizeof(int), cudaMemcpyDeviceToHost));
+      info->nnz[l] = (long long)nnzb * lv.B * lv.B;
+    }
+    info->setup_seconds = d->setup_seconds;
+  }
+  return CSTG_OK;
+}
+
+int cstg_amg_apply_device(cstg_ctx* ctx, const double* d_r, double* d_z) {
+  BEGIN(ctx);
+  const int rc = amg_ready(ctx);
+  if (rc) return rc;
+  const int rc2 = amg_apply(ctx, d_r, d_z);
+  if (rc2) return rc2;
+  CK(cudaStreamSynchronize(ctx->stream));
+  return CSTG_OK;
+}
+
+}  // extern "C"

@@ -76,6 +76,7 @@ void cstg_destroy(cstg_ctx* ctx) {
   if (ctx->graph) cudaGraphExecDestroy(ctx->graph);
   if (ctx->bat_graph) cudaGraphExecDestroy(ctx->bat_graph);
   if (ctx->fcg_graph) cudaGraphExecDestroy(ctx->fcg_graph);
+  amg_free(ctx);
   DevBuf* all[] = {&ctx->xy,      &ctx->tri,    &ctx->cnt,      &ctx->cursor,   &ctx->ne_ptr,
                    &ctx->ne,      &ctx->scan_tmp, &ctx->deg,    &ctx->node_ptr, &ctx->bnbr,
                    &ctx->slot,    &ctx->row_ptr, &ctx->cols,    &ctx->vals,     &ctx->fixed,
@@ -756,8 +757,15 @@ static int check_solve_args(cstg_ctx* ctx, const cstg_solver_options* opt, cstg_
   if (o.precision == CSTG_PRECISION_MIXED && ctx->kind != 1)
     return fail(ctx, CSTG_ERR_UNSUPPORTED,
                 "pcg_solve: mixed precision needs the mesh (2x2-block) pattern of cstg_build_pattern");
-  if (o.preconditioner != CSTG_PRECOND_JACOBI && o.preconditioner != CSTG_PRECOND_LEARNED)
+  if (o.preconditioner != CSTG_PRECOND_JACOBI && o.preconditioner != CSTG_PRECOND_LEARNED &&
+      o.preconditioner != CSTG_PRECOND_AMG)
     return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "pcg_solve: unknown preconditioner %d", o.preconditioner);
+  if (o.preconditioner == CSTG_PRECOND_AMG) {
+    if (ctx->kind != 1)
+      return fail(ctx, CSTG_ERR_UNSUPPORTED, "pcg_solve: the multigrid preconditioner needs the mesh pattern");
+    if (o.record_history)
+      return fail(ctx, CSTG_ERR_UNSUPPORTED, "pcg_solve: no residual history with the multigrid preconditioner");
+  }
   if (o.preconditioner == CSTG_PRECOND_LEARNED) {
     if (ctx->kind != 1)
       return fail(ctx, CSTG_ERR_UNSUPPORTED, "pcg_solve: the learned preconditioner needs the mesh pattern");
@@ -778,7 +786,7 @@ int cstg_pcg_solve_device(cstg_ctx* ctx, const double* d_b, double* d_x, const c
   if (ctx->n_rows && (!d_b || !d_x)) return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "pcg_solve: null vector");
   if (!aligned16(d_b) || !aligned16(d_x))
     return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "pcg_solve: device vectors must be 16-byte aligned");
-  if (o.preconditioner == CSTG_PRECOND_LEARNED) return run_fcg(ctx, d_b, d_x, o, stats);
+  if (o.preconditioner != CSTG_PRECOND_JACOBI) return run_fcg(ctx, d_b, d_x, o, stats);
   return run_solve(ctx, d_b, d_x, o, stats, d_history, false);
 }
 
@@ -814,7 +822,7 @@ int cstg_pcg_solve(cstg_ctx* ctx, const double* b, double* x, const cstg_solver_
   ENSURE(ctx->b_in, sizeof(double) * n);
   ENSURE(ctx->vec_out, sizeof(double) * n);
   if (n) CK(cudaMemcpyAsync(ctx->b_in.p, b, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
-  rc = o.preconditioner == CSTG_PRECOND_LEARNED
+  rc = o.preconditioner != CSTG_PRECOND_JACOBI
            ? run_fcg(ctx, buf_ptr<double>(ctx->b_in), buf_ptr<double>(ctx->vec_out), o, stats)
            : run_solve(ctx, buf_ptr<double>(ctx->b_in), buf_ptr<double>(ctx->vec_out), o, stats, history, true);
   if (rc) return rc;

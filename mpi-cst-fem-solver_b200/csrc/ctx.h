@@ -35,6 +35,7 @@ struct DevBuf {
 }  // namespace cstg_host
 
 using cstg_host::DevBuf;
+struct AmgData;  // amg_api.cu: the multigrid hierarchy of a context
 
 struct cstg_ctx {
   int device = 0;
@@ -102,6 +103,10 @@ struct cstg_ctx {
   cudaGraphExec_t fcg_graph = nullptr;
   unsigned long long fcg_key = 0;
   long long fcg_graph_launches = 0;
+  int fcg_graph_precond = -1;
+
+  // smoothed-aggregation multigrid hierarchy (built on demand)
+  AmgData* amg = nullptr;
 };
 
 namespace cstg_host {
@@ -246,6 +251,12 @@ inline void g_fmt(char* out, size_t n, const char* fmt, ...) {
   std::vsnprintf(out, n, fmt, ap);
   va_end(ap);
 }
+
+// Defined in amg_api.cu: the multigrid hierarchy (built when missing or stale) and z = M r.
+int amg_ready(cstg_ctx* ctx);
+int amg_apply(cstg_ctx* ctx, const double* r, double* z);
+void amg_free(cstg_ctx* ctx);
+int amg_levels(const cstg_ctx* ctx);
 
 // Defined in learned_api.cu: flexible CG with the learned preconditioner.
 int run_fcg(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg_solver_options& o, cstg_stats* stats);

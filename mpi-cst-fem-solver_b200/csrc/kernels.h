@@ -17,7 +17,8 @@ enum ErrSlot {
   kErrTimeout = 5,     // bounded device wait gave up
   kErrBatch = 6,       // batched solve: a node coupled to a node of another plate
   kErrEdge = 7,        // traction edge not adjacent to exactly one triangle
-  kErrSlots = 8
+  kErrAmg = 8,         // multigrid setup: a row or an aggregate exceeded its bound
+  kErrSlots = 12
 };
 
 struct Mat3 {  // 3x3 row-major constitutive matrix, passed by value to kernels
@@ -230,6 +231,51 @@ cudaError_t launch_traction_edges(int n_edges, const int* edges, const MeshDev& 
                                   cudaStream_t s);
 cudaError_t launch_traction_apply(int n_edges, const int* edges, int n_nodes, const double* con, const int* cnt,
                                   int* ptr, int* cur, int* rec, int* scan_tmp, double* f, cudaStream_t s);
+
+// amg.cu: smoothed-aggregation multigrid (block-sparse rows; B = 2 on the finest level, 3 below)
+constexpr int kAmgMaxRow = 64;  // distinct block columns of a P, AP or coarse row
+constexpr int kAmgMaxAgg = 64;  // nodes of an aggregate
+struct AmgBsr {  // n block rows, ptr[n + 1], col[ptr[n]], val: B x B (or B x 3 for P) row-major blocks
+  int n = 0;
+  const int* ptr = nullptr;
+  const int* col = nullptr;
+  const double* val = nullptr;
+};
+cudaError_t amg_fine_bsr(int N, const int* node_ptr, const double* vals, double* out, cudaStream_t s);
+cudaError_t amg_dinv(int B, const AmgBsr& A, double* dinv, int* err, cudaStream_t s);
+cudaError_t amg_mis_round(const AmgBsr& A, int* state, unsigned long long* m1, int* newroot, int* near, int* undecided,
+                          cudaStream_t s);
+cudaError_t amg_flag_eq(int n, const int* a, int v, int* f, cudaStream_t s);
+cudaError_t amg_aggregate(int B, const AmgBsr& A, const int* state, const int* root_id, int* agg1, int* agg2,
+                          cudaStream_t s);
+cudaError_t amg_flag_negative(int n, const int* a, int* f, cudaStream_t s);
+cudaError_t amg_phase3(int n, int n_agg, const int* left_id, int* agg, cudaStream_t s);
+cudaError_t amg_group(int n, const int* key, int m, int* ptr, int* cnt, int* cur, int* out, int* scan_tmp,
+                      cudaStream_t s);
+cudaError_t amg_tentative(int B, int n_agg, const int* agg_ptr, const int* members, const double* Bf, double* P0,
+                          double* Bc, int* err, cudaStream_t s);
+cudaError_t amg_lambda(int B, const AmgBsr& A, const double* dinv, double* x, double* y, double* part, double* lam,
+                       int iters, cudaStream_t s);
+cudaError_t amg_p_count(int B, const AmgBsr& A, const int* agg, int* cnt, int* err, cudaStream_t s);
+cudaError_t amg_p_fill(int B, const AmgBsr& A, const int* agg, const double* P0, const double* dinv, const double* lam,
+                       const AmgBsr& P, cudaStream_t s);
+cudaError_t amg_ap_count(int B, const AmgBsr& A, const AmgBsr& P, int* cnt, int* err, cudaStream_t s);
+cudaError_t amg_ap_fill(int B, const AmgBsr& A, const AmgBsr& P, const AmgBsr& AP, cudaStream_t s);
+cudaError_t amg_pt(int n, int nc, const AmgBsr& P, int* p_row, int* pt_ptr, int* cnt, int* cur, int* pt_idx,
+                   int* scan_tmp, cudaStream_t s);
+cudaError_t amg_ac_count(int B, int nc, const int* pt_ptr, const int* pt_idx, const int* p_row, const AmgBsr& AP,
+                         int* cnt, int* err, cudaStream_t s);
+cudaError_t amg_ac_fill(int B, int nc, const int* pt_ptr, const int* pt_idx, const int* p_row, const AmgBsr& P,
+                        const AmgBsr& AP, const AmgBsr& Ac, cudaStream_t s);
+cudaError_t amg_coarsest(int B, const AmgBsr& A, double* M, double* piv, cudaStream_t s);
+cudaError_t amg_smooth0(int B, int n, const double* dinv, const double* lam, const double* b, double* x, cudaStream_t s);
+cudaError_t amg_sweep(int B, bool residual, const AmgBsr& A, const double* dinv, const double* lam, const double* b,
+                      const double* x, double* xo, cudaStream_t s);
+cudaError_t amg_restrict(int B, int nc, const int* pt_ptr, const int* pt_idx, const int* p_row, const AmgBsr& P,
+                         const double* r, double* bc, cudaStream_t s);
+cudaError_t amg_prolong(int B, const AmgBsr& P, const double* xc, double* x, cudaStream_t s);
+cudaError_t amg_gemv(int n, const double* M, const double* b, double* x, cudaStream_t s);
+cudaError_t amg_rigid_modes(int N, const double* xy, double* Bf, cudaStream_t s);
 
 // Process-wide count of kernel launches issued by this library (graph launches count every
 // kernel node they run).

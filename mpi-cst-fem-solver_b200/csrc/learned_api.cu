@@ -55,13 +55,20 @@ int upload_params(cstg_ctx* ctx, const float* params) {
 int cstg_host::run_fcg(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg_solver_options& o,
                        cstg_stats* stats) {
   const int n = ctx->n_rows, N = ctx->n_nodes;
+  const bool use_amg = o.preconditioner == CSTG_PRECOND_AMG;
+  if (use_amg) {
+    const int rc = amg_ready(ctx);  // the multigrid hierarchy of this matrix (built once per setup)
+    if (rc) return rc;
+  }
   ENSURE(ctx->x, sizeof(double) * (size_t)n);
   ENSURE(ctx->r, sizeof(double) * (size_t)n);
   ENSURE(ctx->p, sizeof(double) * (size_t)n);
   ENSURE(ctx->Ap, sizeof(double) * (size_t)n);
   ENSURE(ctx->lp_z, sizeof(double) * (size_t)n);
-  ENSURE(ctx->lp_h0, sizeof(__nv_bfloat16) * (size_t)N * kMpF);
-  ENSURE(ctx->lp_h1, sizeof(__nv_bfloat16) * (size_t)N * kMpF);
+  if (!use_amg) {
+    ENSURE(ctx->lp_h0, sizeof(__nv_bfloat16) * (size_t)N * kMpF);
+    ENSURE(ctx->lp_h1, sizeof(__nv_bfloat16) * (size_t)N * kMpF);
+  }
   const bool mixed = o.precision == CSTG_PRECISION_MIXED;
   if (mixed) {
     const int rc = ensure_mixed(ctx);
@@ -94,14 +101,19 @@ int cstg_host::run_fcg(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg
     else
       CK(launch_spmv_pcg(bm, w.p, w.q, w.partials, w.st, ctx->stream));
     CK(launch_fcg_update(w, kFcgWindow, kFcgRatio2, ctx->stream));
-    CK(launch_mp_forward(g, P, w.r, w.inv_diag, rr, sf, skip, mw, false, w.z, err, ctx->stream));
+    if (use_amg) {
+      const int rc = amg_apply(ctx, w.r, w.z);
+      if (rc) return rc;
+    } else {
+      CK(launch_mp_forward(g, P, w.r, w.inv_diag, rr, sf, skip, mw, false, w.z, err, ctx->stream));
+    }
     CK(launch_fcg_dots(w, ctx->stream));
     return CSTG_OK;
   };
   const int chunk = o.check_interval > 0 ? o.check_interval : 25;
   unsigned long long key = ctx->generation * 1000003ull + (unsigned long long)chunk * 31ull +
                            (unsigned long long)o.precision * 7ull + (unsigned long long)(uintptr_t)d_b;
-  if (!ctx->fcg_graph || ctx->fcg_key != key) {
+  if (!ctx->fcg_graph || ctx->fcg_key != key || ctx->fcg_graph_precond != o.preconditioner) {
     if (ctx->fcg_graph) {
       cudaGraphExecDestroy(ctx->fcg_graph);
       ctx->fcg_graph = nullptr;
@@ -124,6 +136,7 @@ int cstg_host::run_fcg(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg
     CK(ie);
     ctx->fcg_key = key;
     ctx->fcg_graph_launches = captured;
+    ctx->fcg_graph_precond = o.preconditioner;
   }
 
   RESET_ERR();
@@ -132,7 +145,12 @@ int cstg_host::run_fcg(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg
   int zero = 0;
   CK(cudaMemcpyAsync(&w.st->fp64_mode, &zero, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
   CK(launch_fcg_init(w, o.rtol, o.max_iter, kFcgWindow, ctx->stream));
-  CK(launch_mp_forward(g, P, w.r, w.inv_diag, rr, sf, skip, mw, false, w.z, err, ctx->stream));
+  if (use_amg) {
+    const int rc = amg_apply(ctx, w.r, w.z);
+    if (rc) return rc;
+  } else {
+    CK(launch_mp_forward(g, P, w.r, w.inv_diag, rr, sf, skip, mw, false, w.z, err, ctx->stream));
+  }
   CK(launch_fcg_dots(w, ctx->stream));
   CK(cudaMemcpyAsync(ctx->h_state, ctx->state.p, sizeof(PcgState), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
@@ -196,7 +214,9 @@ int cstg_host::run_fcg(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg
     stats->solve_seconds = ms * 1e-3;
     stats->spmv_calls = spmv_calls;
     char pre[160];
-    if (fallback_iter >= 0)
+    if (use_amg)
+      g_fmt(pre, sizeof pre, "smoothed-aggregation multigrid V(2,2), %d levels", amg_levels(ctx));
+    else if (fallback_iter >= 0)
       g_fmt(pre, sizeof pre, "learned preconditioner, switched to Jacobi at iteration %d (stagnation)",
             fallback_iter);
     else

@@ -57,6 +57,7 @@ TRACTION_KIRSCH = 1
 
 PRECOND_JACOBI = 0
 PRECOND_LEARNED = 1
+PRECOND_AMG = 2
 
 LAUNCH_AUTO = 0
 LAUNCH_PERSISTENT = 1
@@ -69,6 +70,12 @@ class Stats(C.Structure):
                 ("true_rel_residual", C.c_double), ("solve_seconds", C.c_double),
                 ("spmv_calls", C.c_longlong), ("message", C.c_char * 256),
                 ("warning", C.c_char * 256)]
+
+
+class AmgInfo(C.Structure):
+    """cstg_amg_info: the multigrid hierarchy."""
+    _fields_ = [("levels", C.c_int), ("dofs", C.c_int * 16), ("nnz", C.c_longlong * 16),
+                ("setup_seconds", C.c_double)]
 
 
 class BatchConfig(C.Structure):
@@ -129,6 +136,8 @@ _SIGS = {
                                  C.POINTER(C.c_int)]),
     "cstg_mesh_arrays": (C.c_int, [_vp, _vp, _vp, _vp]),
     "cstg_mesh_group": (C.c_int, [_vp, C.c_int, C.c_char_p, C.c_int, C.POINTER(C.c_int), _vp]),
+    "cstg_amg_setup": (C.c_int, [_vp, C.POINTER(AmgInfo)]),
+    "cstg_amg_apply_device": (C.c_int, [_vp, _vp, _vp]),
     "cstg_mpnn_param_count": (C.c_longlong, []),
     "cstg_learned_setup": (C.c_int, [_vp, _vp, _vp]),
     "cstg_learned_set_params": (C.c_int, [_vp, _vp]),

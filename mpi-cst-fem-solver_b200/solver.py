@@ -299,7 +299,7 @@ class SolverOptions:
     max_refinements: int = 16
     check_interval: int = 0
     launch: str = "auto"  # "auto" | "persistent" | "graph"
-    preconditioner: str = "jacobi"  # "jacobi" | "learned" (flexible CG; needs learned setup)
+    preconditioner: str = "jacobi"  # "jacobi" | "learned" (flexible CG; needs learned setup) | "amg"
 
     def native(self) -> native.SolverOptions:
         o = native.default_options()
@@ -312,7 +312,8 @@ class SolverOptions:
         o.check_interval = self.check_interval
         o.launch_mode = {"auto": native.LAUNCH_AUTO, "persistent": native.LAUNCH_PERSISTENT,
                          "graph": native.LAUNCH_GRAPH}[self.launch]
-        o.preconditioner = {"jacobi": native.PRECOND_JACOBI, "learned": native.PRECOND_LEARNED}[self.preconditioner]
+        o.preconditioner = {"jacobi": native.PRECOND_JACOBI, "learned": native.PRECOND_LEARNED,
+                            "amg": native.PRECOND_AMG}[self.preconditioner]
         return o
 
 
@@ -410,3 +411,20 @@ def scf_at_hole(stresses: dict, a: float, sigma_inf: float = 1.0):
     d = np.hypot(stresses["cx"], stresses["cy"] - a)
     e = int(np.argmin(d))
     return stresses["sxx"][e] / sigma_inf, e
+
+
+def amg_setup(K: GpuCsrMatrix) -> dict:
+    """Builds the multigrid hierarchy of K (after CgJacobiSolver.setup) and describes it."""
+    info = native.AmgInfo()
+    K.ctx.check(K.ctx.L.cstg_amg_setup(K.ctx.h, C.byref(info)))
+    return {"levels": info.levels, "dofs": list(info.dofs[:info.levels]), "nnz": list(info.nnz[:info.levels]),
+            "setup_seconds": info.setup_seconds}
+
+
+def amg_apply(K: GpuCsrMatrix, r, z=None):
+    """z = M r (one V-cycle) on CUDA float64 tensors."""
+    import torch
+    z = torch.empty_like(r) if z is None else z
+    K.ctx.check(K.ctx.L.cstg_amg_apply_device(K.ctx.h, _ptr(r), _ptr(z)))
+    return z
+
