@@ -66,11 +66,16 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-preconditioner comparison")
-    ap.add_argument("--only", choices=["spmv", "solve", "batch"], default=None,
+    ap.add_argument("--only", choices=["spmv", "solve", "batch", "batchsolve", "learned", "amg"], default=None,
                     help="profiling modes: `spmv` runs --reps SpMV launches on the assembled plate, "
                          "`solve` one full step, `batch` the 64-plate x 4-load-case batched solve "
                          "(every launch shape, autotuned, --reps graph replays, and the same systems "
-                         "solved one by one); each prints one JSON line")
+                         "solved one by one), `batchsolve` one batched solve (8 x 512 shape) of "
+                         "--batch-plates plates with n_r up to --batch-nr-max, `learned` --reps "
+                         "applications of the learned preconditioner on the plate; each prints one "
+                         "JSON line")
+    ap.add_argument("--batch-plates", type=int, default=64)
+    ap.add_argument("--batch-nr-max", type=int, default=200)
     ap.add_argument("--reps", type=int, default=20)
     ap.add_argument("--max-iter", type=int, default=200000,
                     help="iteration cap of the solves (profiling captures use a small cap)")
@@ -406,6 +411,43 @@ def run_ours(a, dist: Dist):
         out = {"mode": a.only, "workload": a.workload}
         if a.only == "batch":
             out = run_batch(a, pkg)
+        elif a.only == "batchsolve":
+            specs = pkg.plate.random_batch(count=a.batch_plates, seed=2026, n_r_range=(20, a.batch_nr_max))
+            solver = pkg.BatchSolver(pkg.SolverOptions(precision="mixed", max_iter=200000))
+            solver.setup(pkg.build_batch(specs), device_rhs=True)
+            sol = solver.solve(config=(8, 512), device=True)
+            out.update(plates=a.batch_plates, seconds=sol.seconds, converged=int(sol.converged.sum()),
+                       iterations_max=int(sol.iterations.max()))
+            solver.close()
+        elif a.only == "amg":
+            with torch.cuda.stream(stream):
+                K = pkg.build_stiffness_pattern(dmesh, ctx=ctx)
+                pkg.assemble_stiffness(dmesh, D, 1.0, K)
+                d_b.copy_(d_b0)
+                pkg.apply_dirichlet((d_dofs, d_vals), K, d_b)
+                pkg.CgJacobiSolver().setup(K)
+                info = pkg.amg_setup(K)
+                z = torch.empty_like(d_b)
+                pkg.amg_apply(K, d_b, z)
+                e0 = ev_start()
+                for _ in range(a.reps):
+                    pkg.amg_apply(K, d_b, z)
+                out.update(vcycle_us=ev_stop(e0) / a.reps * 1e6, levels=info["levels"], dofs=info["dofs"],
+                           nnz=info["nnz"], setup_s=info["setup_seconds"])
+        elif a.only == "learned":
+            with torch.cuda.stream(stream):
+                K = pkg.build_stiffness_pattern(dmesh, ctx=ctx)
+                pkg.assemble_stiffness(dmesh, D, 1.0, K)
+                d_b.copy_(d_b0)
+                pkg.apply_dirichlet((d_dofs, d_vals), K, d_b)
+                pkg.CgJacobiSolver().setup(K)
+                pkg.learned.setup(K, pkg.learned.load_weights(), pkg.learned.node_material(D, mesh.num_nodes))
+                z = torch.empty_like(d_b)
+                pkg.learned.apply(K, d_b, z)
+                e0 = ev_start()
+                for _ in range(a.reps):
+                    pkg.learned.apply(K, d_b, z)
+                out["apply_us"] = ev_stop(e0) / a.reps * 1e6
         elif a.only == "solve":
             step()
             sync()

@@ -597,6 +597,111 @@ __global__ void k_amg_sweep(int n, AmgBsr A, const double* __restrict__ dinv, co
   }
 }
 
+// Finest-level sweep on the FP32 difference-form operator of mixed_kernels.cu (the smoother is a
+// preconditioner: FP32 matrix values, FP64 vectors and accumulation). Thread per node.
+//   RES: xo = b - A x;   otherwise xo = x + w D^-1 (b - A x)
+template <bool RES>
+__global__ void __launch_bounds__(256) k_amg_sweep_f32(MixedMatrix M, const double* __restrict__ dinv,
+                                                       const double* __restrict__ lam, const double* __restrict__ b,
+                                                       const double* __restrict__ x, double* __restrict__ xo) {
+  const double w = RES ? 0.0 : 4.0 / (3.0 * *lam);
+  const double2* x2 = reinterpret_cast<const double2*>(x);
+  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < M.n_nodes; n += gridDim.x * blockDim.x) {
+    const int bb = __ldg(&M.node_ptr[n]);
+    const int o = bb - n, c = __ldg(&M.node_ptr[n + 1]) - bb - 1;
+    const double2 xs = x2[n];
+    double ya = 0.0, yb = 0.0;
+    for (int k = 0; k < c; ++k) {
+      const int m = __ldg(&M.nbr32[o + k]);
+      const float4 a = __ldg(&M.val32[o + k]);
+      const double2 xm = x2[m];
+      const double dx = xm.x - xs.x, dy = xm.y - xs.y;
+      ya = fma((double)a.x, dx, fma((double)a.y, dy, ya));
+      yb = fma((double)a.z, dx, fma((double)a.w, dy, yb));
+    }
+    const double2 sa = __ldg(&M.S64[2 * n]), sb = __ldg(&M.S64[2 * n + 1]);
+    ya = fma(sa.x, xs.x, fma(sa.y, xs.y, ya));
+    yb = fma(sb.x, xs.x, fma(sb.y, xs.y, yb));
+    const double2 bv = reinterpret_cast<const double2*>(b)[n];
+    const double ra = bv.x - ya, rbv = bv.y - yb;
+    double2 out;
+    if (RES) {
+      out = make_double2(ra, rbv);
+    } else {
+      const double2 dv = reinterpret_cast<const double2*>(dinv)[n];
+      out = make_double2(fma(w * dv.x, ra, xs.x), fma(w * dv.y, rbv, xs.y));
+    }
+    reinterpret_cast<double2*>(xo)[n] = out;
+  }
+}
+
+// Coarse-level (3 x 3 blocks) sweep: 8 lanes per row, lanes over the row's blocks, then a fixed
+// shuffle tree. RES: xo = b - A x; otherwise xo = x + w D^-1 (b - A x).
+template <bool RES>
+__global__ void __launch_bounds__(256) k_amg_sweep3_warp(AmgBsr A, const double* __restrict__ dinv,
+                                                         const double* __restrict__ lam,
+                                                         const double* __restrict__ b, const double* __restrict__ x,
+                                                         double* __restrict__ xo) {
+  const double w = RES ? 0.0 : 4.0 / (3.0 * *lam);
+  const int lane = threadIdx.x & 31, l8 = lane & 7, sub = lane >> 3;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+  for (int base = warp * 4; base < A.n; base += nw * 4) {
+    const int i = base + sub;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    if (i < A.n) {
+      for (int k = A.ptr[i] + l8; k < A.ptr[i + 1]; k += 8) {
+        const double* blk = A.val + (size_t)k * 9;
+        const double* xj = x + 3 * (size_t)A.col[k];
+        const double x0 = xj[0], x1 = xj[1], x2v = xj[2];
+        a0 = fma(blk[0], x0, fma(blk[1], x1, fma(blk[2], x2v, a0)));
+        a1 = fma(blk[3], x0, fma(blk[4], x1, fma(blk[5], x2v, a1)));
+        a2 = fma(blk[6], x0, fma(blk[7], x1, fma(blk[8], x2v, a2)));
+      }
+    }
+#pragma unroll
+    for (int off = 4; off > 0; off >>= 1) {
+      a0 += __shfl_xor_sync(0xffffffffu, a0, off);
+      a1 += __shfl_xor_sync(0xffffffffu, a1, off);
+      a2 += __shfl_xor_sync(0xffffffffu, a2, off);
+    }
+    if (i < A.n && l8 < 3) {
+      const size_t d = 3 * (size_t)i + l8;
+      const double acc = l8 == 0 ? a0 : l8 == 1 ? a1 : a2;
+      const double res = b[d] - acc;
+      xo[d] = RES ? res : fma(w * dinv[d], res, x[d]);
+    }
+  }
+}
+
+// bc_J = sum over the P blocks of column J of P_iJ' r_i: one warp per coarse row, lanes over the
+// row's P blocks, fixed shuffle tree (deterministic).
+template <int B>
+__global__ void __launch_bounds__(256) k_amg_restrict_warp(int nc, const int* __restrict__ pt_ptr,
+                                                           const int* __restrict__ pt_idx,
+                                                           const int* __restrict__ p_row, AmgBsr P,
+                                                           const double* __restrict__ r, double* __restrict__ bc) {
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+  for (int J = warp; J < nc; J += nw) {
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    for (int t = pt_ptr[J] + lane; t < pt_ptr[J + 1]; t += 32) {
+      const int q = pt_idx[t], i = p_row[q];
+      const double* pb = P.val + (size_t)q * B * 3;
+#pragma unroll
+      for (int z = 0; z < B; ++z) {
+        const double rv = r[(size_t)i * B + z];
+        a0 = fma(pb[z * 3 + 0], rv, a0);
+        a1 = fma(pb[z * 3 + 1], rv, a1);
+        a2 = fma(pb[z * 3 + 2], rv, a2);
+      }
+    }
+    a0 = warp_sum(a0);
+    a1 = warp_sum(a1);
+    a2 = warp_sum(a2);
+    if (lane < 3) bc[3 * (size_t)J + lane] = lane == 0 ? a0 : lane == 1 ? a1 : a2;
+  }
+}
+
 // bc_J = sum over P blocks of column J of P_iJ' r_i
 template <int B>
 __global__ void k_amg_restrict(int nc, const int* __restrict__ pt_ptr, const int* __restrict__ pt_idx,
@@ -859,9 +964,27 @@ cudaError_t amg_smooth0(int B, int n, const double* dinv, const double* lam, con
   return cudaGetLastError();
 }
 
+cudaError_t amg_sweep_f32(bool residual, const MixedMatrix& M, const double* dinv, const double* lam, const double* b,
+                          const double* x, double* xo, cudaStream_t s) {
+  if (residual)
+    k_amg_sweep_f32<true><<<gw(M.n_nodes), 256, 0, s>>>(M, dinv, lam, b, x, xo);
+  else
+    k_amg_sweep_f32<false><<<gw(M.n_nodes), 256, 0, s>>>(M, dinv, lam, b, x, xo);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
 cudaError_t amg_sweep(int B, bool residual, const AmgBsr& A, const double* dinv, const double* lam, const double* b,
                       const double* x, double* xo, cudaStream_t s) {
   const int n = A.n;
+  if (B == 3) {
+    if (residual)
+      k_amg_sweep3_warp<true><<<gw((long long)n * 8), 256, 0, s>>>(A, dinv, lam, b, x, xo);
+    else
+      k_amg_sweep3_warp<false><<<gw((long long)n * 8), 256, 0, s>>>(A, dinv, lam, b, x, xo);
+    count_launches(1);
+    return cudaGetLastError();
+  }
   if (B == 2) {
     if (residual)
       k_amg_sweep<2, true><<<gw(n), 256, 0, s>>>(n, A, dinv, lam, b, x, xo);
@@ -880,9 +1003,9 @@ cudaError_t amg_sweep(int B, bool residual, const AmgBsr& A, const double* dinv,
 cudaError_t amg_restrict(int B, int nc, const int* pt_ptr, const int* pt_idx, const int* p_row, const AmgBsr& P,
                          const double* r, double* bc, cudaStream_t s) {
   if (B == 2)
-    k_amg_restrict<2><<<gw(nc), 256, 0, s>>>(nc, pt_ptr, pt_idx, p_row, P, r, bc);
+    k_amg_restrict_warp<2><<<gw((long long)nc * 32), 256, 0, s>>>(nc, pt_ptr, pt_idx, p_row, P, r, bc);
   else
-    k_amg_restrict<3><<<gw(nc), 256, 0, s>>>(nc, pt_ptr, pt_idx, p_row, P, r, bc);
+    k_amg_restrict_warp<3><<<gw((long long)nc * 32), 256, 0, s>>>(nc, pt_ptr, pt_idx, p_row, P, r, bc);
   count_launches(1);
   return cudaGetLastError();
 }

@@ -278,25 +278,35 @@ int vcycle(cstg_ctx* ctx, AmgData* d, size_t l, const double* b, double* x) {
   double* xa = buf_ptr<double>(lv.xa);
   double* r = buf_ptr<double>(lv.r);
   AmgLevel& nx = d->L[l + 1];
+  // the finest level smooths with the FP32 difference-form operator (a preconditioner: FP32
+  // values, FP64 vectors); coarse levels with their FP64 Galerkin operators
+  const bool f32 = l == 0;
+  const MixedMatrix mm = f32 ? mixed_view(ctx) : MixedMatrix{};
+  auto sweep = [&](bool res, const double* xin, double* xout) -> cudaError_t {
+    return f32 ? amg_sweep_f32(res, mm, dinv, lam, b, xin, xout, s) : amg_sweep(lv.B, res, A, dinv, lam, b, xin, xout, s);
+  };
   CK(amg_smooth0(lv.B, lv.n, dinv, lam, b, xa, s));
-  CK(amg_sweep(lv.B, false, A, dinv, lam, b, xa, x, s));
-  CK(amg_sweep(lv.B, true, A, dinv, lam, b, x, r, s));
+  CK(sweep(false, xa, x));
+  CK(sweep(true, x, r));
   CK(amg_restrict(lv.B, lv.nc, buf_ptr<int>(lv.pt_ptr), buf_ptr<int>(lv.pt_idx), buf_ptr<int>(lv.p_row), lv.P(), r,
                   buf_ptr<double>(nx.bc), s));
   const int rc = vcycle(ctx, d, l + 1, buf_ptr<double>(nx.bc), buf_ptr<double>(nx.xb));
   if (rc) return rc;
   CK(amg_prolong(lv.B, lv.P(), buf_ptr<double>(nx.xb), x, s));
-  CK(amg_sweep(lv.B, false, A, dinv, lam, b, x, xa, s));
-  CK(amg_sweep(lv.B, false, A, dinv, lam, b, xa, x, s));
+  CK(sweep(false, x, xa));
+  CK(sweep(false, xa, x));
   return CSTG_OK;
 }
 
 }  // namespace
 
 int cstg_host::amg_ready(cstg_ctx* ctx) {
-  if (ctx->amg && ctx->amg->built_for == ctx->setup_count) return CSTG_OK;
+  if (ctx->amg && ctx->amg->built_for == ctx->setup_count && ctx->mixed_ready) return CSTG_OK;
   if (ctx->kind != 1 || !ctx->setup_done)
     return fail(ctx, CSTG_ERR_STATE, "amg_setup: needs a mesh-pattern matrix after cstg_pcg_setup");
+  const int rc = ensure_mixed(ctx);  // the finest-level smoother's FP32 operator
+  if (rc) return rc;
+  if (ctx->amg && ctx->amg->built_for == ctx->setup_count) return CSTG_OK;
   return amg_build(ctx);
 }
 

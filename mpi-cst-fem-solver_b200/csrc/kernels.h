@@ -271,6 +271,8 @@ cudaError_t amg_coarsest(int B, const AmgBsr& A, double* M, double* piv, cudaStr
 cudaError_t amg_smooth0(int B, int n, const double* dinv, const double* lam, const double* b, double* x, cudaStream_t s);
 cudaError_t amg_sweep(int B, bool residual, const AmgBsr& A, const double* dinv, const double* lam, const double* b,
                       const double* x, double* xo, cudaStream_t s);
+cudaError_t amg_sweep_f32(bool residual, const MixedMatrix& M, const double* dinv, const double* lam, const double* b,
+                          const double* x, double* xo, cudaStream_t s);
 cudaError_t amg_restrict(int B, int nc, const int* pt_ptr, const int* pt_idx, const int* p_row, const AmgBsr& P,
                          const double* r, double* bc, cudaStream_t s);
 cudaError_t amg_prolong(int B, const AmgBsr& P, const double* xc, double* x, cudaStream_t s);
