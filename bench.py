@@ -61,7 +61,12 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="plate2m", choices=sorted(WORKLOADS))
-    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
+    ap.add_argument("--precond", default="amg", choices=["amg", "jacobi", "learned"],
+                    help="preconditioner of the timed solve: smoothed-aggregation multigrid (default), "
+                         "Jacobi (the reference's method, persistent kernel) or the learned network")
+    ap.add_argument("--precision", default=None, choices=["fp64", "mixed"],
+                    help="outer CG precision; default fp64 with amg (its finest smoother is FP32 already), "
+                         "mixed otherwise")
     ap.add_argument("--cpu-sample-iters", type=int, default=150)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -81,6 +86,8 @@ def parse():
                     help="iteration cap of the solves (profiling captures use a small cap)")
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)
+    if a.precision is None:
+        a.precision = "fp64" if a.precond == "amg" else "mixed"
     return a
 
 
@@ -381,8 +388,11 @@ def run_ours(a, dist: Dist):
     d_x = torch.empty_like(d_b0)
     dmesh = pkg.plate.Mesh(xy=d_xy, triangles=d_tri, boundary_edges=mesh.boundary_edges)
     torch.cuda.synchronize()
-    opts = pkg.SolverOptions(rtol=1e-10, max_iter=a.max_iter, precision=a.precision, true_residual_stop=True)
+    opts = pkg.SolverOptions(rtol=1e-10, max_iter=a.max_iter, precision=a.precision, true_residual_stop=True,
+                             preconditioner=a.precond)
     last = {}
+    l_weights = pkg.learned.load_weights()
+    l_mat = pkg.learned.node_material(D, mesh.num_nodes)
 
     def step():
         with torch.cuda.stream(stream):
@@ -392,6 +402,8 @@ def run_ours(a, dist: Dist):
             pkg.apply_dirichlet((d_dofs, d_vals), K, d_b)
             s = pkg.CgJacobiSolver(opts)
             s.setup(K)
+            if a.precond == "learned":
+                pkg.learned.setup(K, l_weights, l_mat)
             last["st"] = s.solve(d_b, d_x)
             last["K"] = K
 
@@ -491,30 +503,34 @@ def run_ours(a, dist: Dist):
     t_step = el_max / a.steps
     value = a.gpus * n / t_step
 
-    # plain FP64 Jacobi-PCG on the same matrix, the reference's stopping rule: the iteration
-    # count for the CPU extrapolation and the plain-GPU comparison time (not in `value`)
+    # comparison solves on the same matrix (not in `value`):
+    #   ref_rule      FP64 Jacobi-PCG under the reference's own stopping rule (recursive residual,
+    #                 solver.cpp:80-82): its iteration count scales the CPU baseline
+    #   plain_fp64    FP64 Jacobi-PCG to the FP64 true residual: the plain GPU Jacobi-PCG
+    #   jacobi_mixed  Jacobi-PCG with the FP32 SpMV and preconditioner, FP64 scalars and
+    #                 true-residual refinement (the persistent kernel)
+    #   learned_mixed the learned preconditioner (packaged weights) in flexible CG, mixed SpMV
+    K = last["K"]
+
+    def solve_with(**kw):
+        s_ = pkg.CgJacobiSolver(pkg.SolverOptions(rtol=1e-10, max_iter=200000, **kw))
+        s_.setup(K)
+        return s_, s_.solve(d_b, torch.empty_like(d_x))
+
     with torch.cuda.stream(stream):
-        s_ref = pkg.CgJacobiSolver(pkg.SolverOptions(rtol=1e-10, max_iter=200000))
-        s_ref.setup(last["K"])
-        st_ref = s_ref.solve(d_b, torch.empty_like(d_x))
-        if a.precision != "fp64":
-            s_64 = pkg.CgJacobiSolver(pkg.SolverOptions(rtol=1e-10, max_iter=200000, true_residual_stop=True))
-            s_64.setup(last["K"])
-            st_64 = s_64.solve(d_b, torch.empty_like(d_x))
-        else:
-            st_64 = st
+        s_ref, st_ref = solve_with()
+        _, st_64 = solve_with(true_residual_stop=True)
+        _, st_jm = solve_with(precision="mixed", true_residual_stop=True)
     sync()
 
-    # the learned preconditioner (packaged weights) inside flexible CG, mixed-precision SpMV:
-    # the north star's "learned + mixed" configuration, same matrix, same stopping rule
     learned = None
     if not a.no_learned:
         with torch.cuda.stream(stream):
             s_l = pkg.CgJacobiSolver(pkg.SolverOptions(rtol=1e-10, max_iter=200000, precision="mixed",
                                                        preconditioner="learned", true_residual_stop=True))
-            s_l.setup(last["K"])
+            s_l.setup(K)
             t0 = time.perf_counter()
-            pkg.learned.setup(last["K"], pkg.learned.load_weights(), pkg.learned.node_material(D, mesh.num_nodes))
+            pkg.learned.setup(K, l_weights, l_mat)
             t_setup = time.perf_counter() - t0
             s_l.solve(d_b, torch.empty_like(d_x))  # warm-up (graph capture)
             st_l = s_l.solve(d_b, torch.empty_like(d_x))
@@ -524,8 +540,7 @@ def run_ours(a, dist: Dist):
                    "speedup_vs_plain_fp64": st_64.solve_seconds / st_l.solve_seconds,
                    "message": st_l.message}
 
-    # dominant kernels: the SpMVs, timed alone (CUDA events, back-to-back launches)
-    K = last["K"]
+    # dominant kernels timed alone (CUDA events, back-to-back launches)
     N = mesh.num_nodes
     nnz = K.nnz()
     nb = nnz // 4
@@ -541,68 +556,91 @@ def run_ours(a, dist: Dist):
                 fn()
             return ev_stop(e0) / reps
 
+    peak, peak_kind = measured_peaks()
+    peak_note = f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs, burst copy)"
+    full = a.workload == "plate2m"
+
+    def roof(kernel, nbytes, seconds, traffic=None, **extra):
+        return {"bound": "hbm", "kernel": kernel, "achieved": nbytes / seconds / 1e9, "peak": peak, "unit": "GB/s",
+                "frac": nbytes / seconds / 1e9 / peak, "peak_kind": peak_note, "traffic": traffic,
+                "algorithmic_bytes": nbytes, "launch_us": seconds * 1e6, **extra}
+
     xs = torch.randn(n, dtype=torch.float64, device=dev)
     ys = torch.empty_like(xs)
     spmv64_s = time_launches(lambda: K.multiply(xs, ys))
     spmv64_bytes = nnz * 8 + nb * 4 + (N + 1) * 4 + n * 8 + n * 8
-    peak, peak_kind = measured_peaks()
-    roof64 = {"bound": "hbm", "kernel": "k_spmv_block (FP64 2x2-block SpMV)",
-              "achieved": spmv64_bytes / spmv64_s / 1e9, "peak": peak, "unit": "GB/s",
-              "frac": spmv64_bytes / spmv64_s / 1e9 / peak,
-              "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs, burst copy)",
-              "traffic": profile_traffic("spmv_block_fp64_plate2m.md") if a.workload == "plate2m" else None,
-              "algorithmic_bytes": spmv64_bytes, "launch_us": spmv64_s * 1e6}
-    if a.precision == "mixed":
-        with torch.cuda.stream(stream):
-            s_ref.setup(K)  # the FP32 operator of this matrix
-        spmv32_s = time_launches(lambda: K.multiply_mixed(xs, ys))
-        spmv32_bytes = noff * (16 + 4) + N * 32 + (N + 1) * 4 + n * 8 + n * 8
-        spmv_head = {"kernel": "k_spmv_mixed (FP32 difference-form 2x2-block SpMV, FP64 vectors)",
-                     "achieved": spmv32_bytes / spmv32_s / 1e9, "peak": peak, "unit": "GB/s",
-                     "frac": spmv32_bytes / spmv32_s / 1e9 / peak, "algorithmic_bytes": spmv32_bytes,
-                     "traffic": profile_traffic("spmv_mixed_f32_plate2m.md") if a.workload == "plate2m" else None,
-                     "launch_us": spmv32_s * 1e6}
-        iter_bytes = spmv32_bytes + n * (5 * 8 + 2 * 8) + n * (2 * 8 + 2 * 8)
-    else:
-        spmv_head = roof64
-        iter_bytes = spmv64_bytes + n * (5 * 8 + 2 * 8) + n * (2 * 8 + 2 * 8)
-    iter_s = st.solve_seconds / max(st.iterations, 1)
-    # The dominant kernel of the timed step is the persistent PCG kernel (one cooperative launch
-    # runs every iteration); its algorithmic bytes per launch are the 3-pass iteration model
-    # (SpMV + x/r update + p update) times the iterations, its duration the solve time.
-    launch_bytes = iter_bytes * st.iterations
-    per_iter_traffic = profile_traffic(f"pcg_persistent_{a.precision}_plate2m.md",
-                                       "dram_bytes_per_iteration_full_size") if a.workload == "plate2m" else None
-    roofline = {"bound": "hbm", "kernel": f"k_pcg_persistent<{a.precision}> (whole PCG solve, one launch)",
-                "achieved": launch_bytes / st.solve_seconds / 1e9, "peak": peak, "unit": "GB/s",
-                "frac": launch_bytes / st.solve_seconds / 1e9 / peak,
-                "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs, burst copy)",
-                "traffic": per_iter_traffic * st.iterations if per_iter_traffic else None,
-                "algorithmic_bytes": launch_bytes, "bytes_per_iteration": iter_bytes,
-                "launch_us": st.solve_seconds * 1e6}
+    roof64 = roof("k_spmv_block (FP64 2x2-block SpMV)", spmv64_bytes, spmv64_s,
+                  profile_traffic("spmv_block_fp64_plate2m.md") if full else None)
+    with torch.cuda.stream(stream):
+        s_ref.setup(K)  # the FP32 operator of this matrix
+    spmv32_s = time_launches(lambda: K.multiply_mixed(xs, ys))
+    spmv32_bytes = noff * (16 + 4) + N * 32 + (N + 1) * 4 + n * 8 + n * 8
+    roof32 = roof("k_spmv_mixed (FP32 difference-form 2x2-block SpMV, FP64 vectors)", spmv32_bytes, spmv32_s,
+                  profile_traffic("spmv_mixed_f32_plate2m.md") if full else None)
 
+    # The persistent Jacobi-PCG kernel (one cooperative launch runs every iteration): algorithmic
+    # bytes per launch = the 3-pass iteration model (SpMV + x/r update + p update) x iterations.
+    def persistent_roof(stx, precision):
+        it_bytes = (spmv32_bytes if precision == "mixed" else spmv64_bytes) + n * (5 * 8 + 2 * 8) + n * (2 * 8 + 2 * 8)
+        per_it = profile_traffic(f"pcg_persistent_{precision}_plate2m.md",
+                                 "dram_bytes_per_iteration_full_size") if full else None
+        return roof(f"k_pcg_persistent<{precision}> (whole PCG solve, one launch)", it_bytes * stx.iterations,
+                    stx.solve_seconds, per_it * stx.iterations if per_it else None, bytes_per_iteration=it_bytes,
+                    iteration_gbs=it_bytes * stx.iterations / stx.solve_seconds / 1e9)
+
+    jacobi_mixed = {"solve_s": st_jm.solve_seconds, "iterations": st_jm.iterations,
+                    "refinements": st_jm.refinements, "true_rel_residual": st_jm.true_rel_residual,
+                    "speedup_vs_plain_fp64": st_64.solve_seconds / st_jm.solve_seconds,
+                    "roofline": persistent_roof(st_jm, "mixed")}
+
+    # the multigrid hierarchy of this matrix, its cycle and its finest-level smoother sweep
+    # (FP32 difference-form operator + FP64 b, D^-1, x in, x out per launch)
+    amg = None
+    if a.precond == "amg":
+        with torch.cuda.stream(stream):
+            info = pkg.amg_setup(K)
+            tm = pkg.amg_time(K, reps=50)
+        sync()
+        sweep_bytes = spmv32_bytes + 2 * n * 8
+        amg = {"levels": info["levels"], "level_dofs": info["dofs"], "level_nnz": info["nnz"],
+               "setup_s": info["setup_seconds"], "vcycle_us": tm["vcycle_s"] * 1e6,
+               "cycle": "V(2,2), damped Jacobi, FP32 finest-level operator, dense coarsest inverse",
+               "smoother_roofline": roof("k_amg_sweep_f32 (finest-level damped Jacobi sweep)", sweep_bytes,
+                                         tm["sweep_s"],
+                                         profile_traffic("amg_sweep_f32_plate2m.md") if full else None)}
+        roofline = amg["smoother_roofline"]
+    elif a.precond == "jacobi":
+        roofline = persistent_roof(st, a.precision)
+    else:
+        roofline = roof32
+
+    dtype = {"amg": "f64 (CG) + f32 (finest smoother matrix values)", "jacobi": "f64", "learned": "f32+f64+bf16"}
     line = {
         "metric": METRIC, "value": value, "unit": "DOF/s", "n_gpus": a.gpus, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64" if a.precision == "fp64" else "f32+f64", "data": "synthetic",
+        "vs_baseline": None,
+        "dtype": dtype[a.precond] if a.precision == "fp64" else "f32+f64",
+        "data": "synthetic",
         "config": {"workload": f"{a.workload}: {desc}, {n} DOFs, {nnz} nnz, E=1 nu=0.3 plane stress t=1, "
                                "traction (1,0) on x=10, u_x=0 on x=0, u_y=0 on y=0",
-                   "step": "pattern + assembly + Dirichlet + Jacobi setup + PCG to rtol 1e-10 on the "
-                           "FP64 true residual",
-                   "precision": a.precision, "dofs": n, "nnz": nnz,
+                   "step": f"pattern + assembly + Dirichlet + {a.precond} preconditioner setup + PCG to "
+                           "rtol 1e-10 on the FP64 true residual",
+                   "preconditioner": a.precond, "precision": a.precision, "dofs": n, "nnz": nnz,
                    "l2": f"inputs larger than L2 (FP64 matrix values {nnz * 8 / 1e6:.0f} MB)",
                    "parallelism": f"replicas x{a.gpus}"},
         "time_to_solve_s": t_step, "iterations": st.iterations, "refinements": st.refinements,
         "true_rel_residual": st.true_rel_residual, "solve_s": st.solve_seconds,
         "plain_fp64": {"solve_s": st_64.solve_seconds, "iterations": st_64.iterations,
                        "true_rel_residual": st_64.true_rel_residual,
-                       "speedup_of_headline": st_64.solve_seconds / st.solve_seconds},
+                       "speedup_of_headline_solve": st_64.solve_seconds / st.solve_seconds,
+                       "speedup_of_headline_step": st_64.solve_seconds / t_step},
+        "jacobi_mixed": jacobi_mixed,
         "learned_mixed": learned,
+        "amg": amg,
         "reference_rule_iterations": st_ref.iterations, "reference_rule_solve_s": st_ref.solve_seconds,
-        "pcg_iteration_gbs": iter_bytes / iter_s / 1e9,
         "roofline": roofline,
         "spmv_fp64": roof64,
-        "spmv_mixed": spmv_head if a.precision == "mixed" else None,
+        "spmv_mixed": roof32,
         "gpu_launches": int(launches),
         "clocks": clk,
     }
@@ -629,6 +667,8 @@ def run_ours(a, dist: Dist):
             pkg.apply_dirichlet((h_dofs, h_vals), K2, h_b)
             s2 = pkg.CgJacobiSolver(opts)
             s2.setup(K2)
+            if a.precond == "learned":
+                pkg.learned.setup(K2, l_weights, l_mat)
             last["e2e"] = s2.solve(h_b, h_x)
 
         def wall_start():

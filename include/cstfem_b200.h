@@ -359,6 +359,9 @@ typedef struct {
 int cstg_amg_setup(cstg_ctx* ctx, cstg_amg_info* info);
 /* z = M r (device vectors) with the context's hierarchy (built if missing). */
 int cstg_amg_apply_device(cstg_ctx* ctx, const double* d_r, double* d_z);
+/* Timing on the context's stream (CUDA events, `reps` back-to-back launches after a warm-up):
+ * out[0] = seconds per finest-level smoothing sweep, out[1] = seconds per V-cycle. */
+int cstg_amg_time(cstg_ctx* ctx, int reps, double* out);
 
 #ifdef __cplusplus
 }

@@ -6,8 +6,9 @@ on the GPU path.
 The file format and keys are the reference's (`key = value`, `#` comments, duplicate keys and
 keys with whitespace rejected, unknown keys warned about). `solver` selects the GPU method:
 `cg_jacobi` (the reference's recurrence and stopping rule, FP64), `gpu_cg` (FP64, stop on the
-FP64 true residual), `gpu_cg_mixed` (FP32 operator, FP64 vectors) or `gpu_cg_learned` (the learned
-preconditioner in flexible CG); `petsc` and `path = distributed` are not available on this path.
+FP64 true residual), `gpu_cg_mixed` (FP32 operator, FP64 vectors), `gpu_cg_learned` (the learned
+preconditioner in flexible CG) or `gpu_cg_amg` (smoothed-aggregation multigrid V-cycle in flexible
+CG); `petsc` and `path = distributed` are not available on this path.
 Outputs in `output_dir`: timings.json (the reference's layout, "path": "gpu"), displacement.npy
 (2 per node) and element_stresses.npz; Kirsch cases also report the stress concentration factor
 and the relative L2 error of the centroid stresses against the analytical field. VTU output is
@@ -35,7 +36,8 @@ KNOWN_KEYS = ["mesh", "plane", "E", "nu", "thickness", "partitioner", "solver", 
 SOLVERS = {"cg_jacobi": dict(precision="fp64", true_residual_stop=False),
            "gpu_cg": dict(precision="fp64", true_residual_stop=True),
            "gpu_cg_mixed": dict(precision="mixed", true_residual_stop=True),
-           "gpu_cg_learned": dict(precision="mixed", true_residual_stop=True, preconditioner="learned")}
+           "gpu_cg_learned": dict(precision="mixed", true_residual_stop=True, preconditioner="learned"),
+           "gpu_cg_amg": dict(precision="fp64", true_residual_stop=True, preconditioner="amg")}
 
 
 class CaseError(RuntimeError):

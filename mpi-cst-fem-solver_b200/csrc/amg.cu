@@ -12,9 +12,10 @@
 //      P0 = Q (one B x 3 block per node), coarse nullspace = R;
 //   3. smoothed prolongator P = (I - w D^-1 A) P0, w = 4 / (3 lambda_max(D^-1 A));
 //   4. Galerkin coarse operator A_c = P' (A P) (3 x 3 blocks).
-// Every kernel is thread-per-row with a fixed order of additions: the hierarchy and the cycle are
-// deterministic. Rows are built in two passes (count, then fill after a prefix sum); row widths
-// are bounded by kAmgMaxRow (checked: the error word records the first overflow).
+// Every kernel adds in a fixed order (thread-per-row kernels, or warp-per-row kernels whose lanes
+// own output blocks): the hierarchy and the cycle are deterministic. Rows are built in two passes
+// (count, then fill after a prefix sum); row widths are bounded by kAmgMaxRow (checked: the error
+// word records the first overflow).
 #include <cuda_runtime.h>
 
 #include "common.cuh"
@@ -399,32 +400,142 @@ __global__ void k_amg_ap_count(int n, AmgBsr A, AmgBsr P, int* __restrict__ cnt,
   cnt[i] = m;
 }
 
+// The fill of a Galerkin factor runs in two kernels: a thread per row writes the row's sorted
+// column set (as the count kernel found it), then a warp per row sums the row's block products.
+// The warp takes the row's candidate products (one per pair of input blocks) 32 at a time in
+// their fixed order, each lane computes one product into shared memory, and each lane then adds,
+// in candidate order, the products that fall on the two output blocks it owns (lane, lane + 32).
+// Every output block thus sees the same additions in the same order on every run.
+constexpr int kGalWarps = 8;
+
+template <int NV>
+struct GalerkinSmem {
+  int cols[kGalWarps][kAmgMaxRow];
+  int ofs[kGalWarps][33];
+  int slot[kGalWarps][32];
+  double prod[kGalWarps][32][NV];
+};
+
+// owner-lane accumulation of one chunk of `cnt` candidate products
+template <int NV>
+__device__ __forceinline__ void gal_accumulate(const int* slot, const double (*prod)[NV], int cnt, int lane,
+                                               double (&a0)[NV], double (&a1)[NV]) {
+  for (int u = 0; u < cnt; ++u) {
+    const int su = slot[u];
+    if (su == lane) {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) a0[v] += prod[u][v];
+    } else if (su == lane + 32) {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) a1[v] += prod[u][v];
+    }
+  }
+}
+
+// inclusive warp scan of `len` into ofs[1..32] (ofs[0] = 0); returns the total
+__device__ __forceinline__ int gal_offsets(int len, int lane, int* ofs) {
+  int incl = len;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  ofs[lane + 1] = incl;
+  if (lane == 0) ofs[0] = 0;
+  __syncwarp();
+  return __shfl_sync(0xffffffffu, incl, 31);
+}
+
+// the group member g (0..ng-1) whose candidate range [ofs[g], ofs[g+1]) holds t
+__device__ __forceinline__ int gal_member(const int* ofs, int ng, int t) {
+  int lo = 0, hi = ng - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (ofs[mid] <= t)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+// AP = A P: column sets
 template <int B>
-__global__ void k_amg_ap_fill(int n, AmgBsr A, AmgBsr P, AmgBsr AP) {
+__global__ void k_amg_ap_cols(int n, AmgBsr A, AmgBsr P, AmgBsr AP) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  int* cols = const_cast<int*>(AP.col) + AP.ptr[i];
-  double* vals = const_cast<double*>(AP.val) + (size_t)AP.ptr[i] * B * 3;
+  int s[kAmgMaxRow];
   int m = 0;
   for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) {
     const int j = A.col[k];
-    for (int q = P.ptr[j]; q < P.ptr[j + 1]; ++q) set_insert(cols, m, P.col[q], kAmgMaxRow);
+    for (int q = P.ptr[j]; q < P.ptr[j + 1]; ++q) set_insert(s, m, P.col[q], kAmgMaxRow);
   }
-  for (int q = 0; q < m * B * 3; ++q) vals[q] = 0.0;
-  for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) {
-    const int j = A.col[k];
-    const double* blk = A.val + (size_t)k * B * B;
-    for (int q = P.ptr[j]; q < P.ptr[j + 1]; ++q) {
-      const int s = row_find(cols, 0, m, P.col[q]);
-      const double* pb = P.val + (size_t)q * B * 3;
-      double* o = vals + (size_t)s * B * 3;
-      for (int r = 0; r < B; ++r)
-        for (int c = 0; c < 3; ++c) {
-          double t = o[r * 3 + c];
-          for (int z = 0; z < B; ++z) t = fma(blk[r * B + z], pb[z * 3 + c], t);
-          o[r * 3 + c] = t;
+  int* cols = const_cast<int*>(AP.col) + AP.ptr[i];
+  for (int q = 0; q < m; ++q) cols[q] = s[q];
+}
+
+// AP = A P: values. Row i's candidates: for each block k of A's row i (ascending), for each block
+// q of P's row A.col[k] (ascending), the B x 3 product A_k P_q.
+template <int B>
+__global__ void __launch_bounds__(32 * kGalWarps) k_amg_ap_vals(int n, AmgBsr A, AmgBsr P, AmgBsr AP) {
+  constexpr int NV = B * 3;
+  __shared__ GalerkinSmem<NV> sm;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int warp = blockIdx.x * kGalWarps + w, nw = gridDim.x * kGalWarps;
+  for (int i = warp; i < n; i += nw) {
+    const int c0 = AP.ptr[i], m = AP.ptr[i + 1] - c0;
+    for (int t = lane; t < m; t += 32) sm.cols[w][t] = AP.col[c0 + t];
+    double a0[NV], a1[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) a0[v] = a1[v] = 0.0;
+    const int k0 = A.ptr[i], k1 = A.ptr[i + 1];
+    for (int kb = k0; kb < k1; kb += 32) {
+      const int ng = min(32, k1 - kb);
+      int pbeg = 0, len = 0;
+      if (lane < ng) {
+        const int j = A.col[kb + lane];
+        pbeg = P.ptr[j];
+        len = P.ptr[j + 1] - pbeg;
+      }
+      const int total = gal_offsets(len, lane, sm.ofs[w]);
+      for (int cb = 0; cb < total; cb += 32) {
+        const int t = cb + lane;
+        const int g = gal_member(sm.ofs[w], ng, min(t, total - 1));
+        const int qb = __shfl_sync(0xffffffffu, pbeg, g);
+        if (t < total) {
+          const int k = kb + g, q = qb + (t - sm.ofs[w][g]);
+          const double* blk = A.val + (size_t)k * B * B;
+          const double* pb = P.val + (size_t)q * B * 3;
+          double a[B * B], p[B * 3];
+#pragma unroll
+          for (int v = 0; v < B * B; ++v) a[v] = blk[v];
+#pragma unroll
+          for (int v = 0; v < B * 3; ++v) p[v] = pb[v];
+#pragma unroll
+          for (int r = 0; r < B; ++r)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+              double x = 0.0;
+#pragma unroll
+              for (int z = 0; z < B; ++z) x = fma(a[r * B + z], p[z * 3 + c], x);
+              sm.prod[w][lane][r * 3 + c] = x;
+            }
+          sm.slot[w][lane] = row_find(sm.cols[w], 0, m, P.col[q]);
         }
+        __syncwarp();
+        gal_accumulate<NV>(sm.slot[w], sm.prod[w], min(32, total - cb), lane, a0, a1);
+        __syncwarp();
+      }
+      __syncwarp();
     }
+    double* out = const_cast<double*>(AP.val) + (size_t)c0 * NV;
+    if (lane < m)
+#pragma unroll
+      for (int v = 0; v < NV; ++v) out[(size_t)lane * NV + v] = a0[v];
+    if (lane + 32 < m)
+#pragma unroll
+      for (int v = 0; v < NV; ++v) out[(size_t)(lane + 32) * NV + v] = a1[v];
+    __syncwarp();
   }
 }
 
@@ -465,34 +576,89 @@ __global__ void k_amg_ac_count(int nc, const int* __restrict__ pt_ptr, const int
   cnt[J] = m;
 }
 
-template <int B>
-__global__ void k_amg_ac_fill(int nc, const int* __restrict__ pt_ptr, const int* __restrict__ pt_idx,
-                              const int* __restrict__ p_row, AmgBsr P, AmgBsr AP, AmgBsr Ac) {
+// A_c = P' (AP): column sets
+__global__ void k_amg_ac_cols(int nc, const int* __restrict__ pt_ptr, const int* __restrict__ pt_idx,
+                              const int* __restrict__ p_row, AmgBsr AP, AmgBsr Ac) {
   const int J = blockIdx.x * blockDim.x + threadIdx.x;
   if (J >= nc) return;
-  int* cols = const_cast<int*>(Ac.col) + Ac.ptr[J];
-  double* vals = const_cast<double*>(Ac.val) + (size_t)Ac.ptr[J] * 9;
+  int s[kAmgMaxRow];
   int m = 0;
   for (int t = pt_ptr[J]; t < pt_ptr[J + 1]; ++t) {
     const int i = p_row[pt_idx[t]];
-    for (int q = AP.ptr[i]; q < AP.ptr[i + 1]; ++q) set_insert(cols, m, AP.col[q], kAmgMaxRow);
+    for (int q = AP.ptr[i]; q < AP.ptr[i + 1]; ++q) set_insert(s, m, AP.col[q], kAmgMaxRow);
   }
-  for (int q = 0; q < m * 9; ++q) vals[q] = 0.0;
-  for (int t = pt_ptr[J]; t < pt_ptr[J + 1]; ++t) {
-    const int pq = pt_idx[t];
-    const int i = p_row[pq];
-    const double* pb = P.val + (size_t)pq * B * 3;  // P_iJ (B x 3)
-    for (int q = AP.ptr[i]; q < AP.ptr[i + 1]; ++q) {
-      const int s = row_find(cols, 0, m, AP.col[q]);
-      const double* ab = AP.val + (size_t)q * B * 3;  // (AP)_iK (B x 3)
-      double* o = vals + (size_t)s * 9;
-      for (int r = 0; r < 3; ++r)
-        for (int c = 0; c < 3; ++c) {
-          double v = o[r * 3 + c];
-          for (int z = 0; z < B; ++z) v = fma(pb[z * 3 + r], ab[z * 3 + c], v);
-          o[r * 3 + c] = v;
+  int* cols = const_cast<int*>(Ac.col) + Ac.ptr[J];
+  for (int q = 0; q < m; ++q) cols[q] = s[q];
+}
+
+// A_c = P' (AP): values. Coarse row J's candidates: for each P block (i, J) in ascending fine row
+// i, for each block q of AP's row i (ascending), the 3 x 3 product P_iJ' (AP)_q.
+template <int B>
+__global__ void __launch_bounds__(32 * kGalWarps) k_amg_ac_vals(int nc, const int* __restrict__ pt_ptr,
+                                                                const int* __restrict__ pt_idx,
+                                                                const int* __restrict__ p_row, AmgBsr P, AmgBsr AP,
+                                                                AmgBsr Ac) {
+  constexpr int NV = 9;
+  __shared__ GalerkinSmem<NV> sm;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int warp = blockIdx.x * kGalWarps + w, nw = gridDim.x * kGalWarps;
+  for (int J = warp; J < nc; J += nw) {
+    const int c0 = Ac.ptr[J], m = Ac.ptr[J + 1] - c0;
+    for (int t = lane; t < m; t += 32) sm.cols[w][t] = Ac.col[c0 + t];
+    double a0[NV], a1[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) a0[v] = a1[v] = 0.0;
+    const int t0 = pt_ptr[J], t1 = pt_ptr[J + 1];
+    for (int tb = t0; tb < t1; tb += 32) {
+      const int ng = min(32, t1 - tb);
+      int pq = 0, abeg = 0, len = 0;
+      if (lane < ng) {
+        pq = pt_idx[tb + lane];
+        const int i = p_row[pq];
+        abeg = AP.ptr[i];
+        len = AP.ptr[i + 1] - abeg;
+      }
+      const int total = gal_offsets(len, lane, sm.ofs[w]);
+      for (int cb = 0; cb < total; cb += 32) {
+        const int t = cb + lane;
+        const int g = gal_member(sm.ofs[w], ng, min(t, total - 1));
+        const int qb = __shfl_sync(0xffffffffu, abeg, g);
+        const int pqg = __shfl_sync(0xffffffffu, pq, g);
+        if (t < total) {
+          const int q = qb + (t - sm.ofs[w][g]);
+          const double* pb = P.val + (size_t)pqg * B * 3;  // P_iJ (B x 3)
+          const double* ab = AP.val + (size_t)q * B * 3;   // (AP)_iK (B x 3)
+          double p[B * 3], a[B * 3];
+#pragma unroll
+          for (int v = 0; v < B * 3; ++v) {
+            p[v] = pb[v];
+            a[v] = ab[v];
+          }
+#pragma unroll
+          for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+              double x = 0.0;
+#pragma unroll
+              for (int z = 0; z < B; ++z) x = fma(p[z * 3 + r], a[z * 3 + c], x);
+              sm.prod[w][lane][r * 3 + c] = x;
+            }
+          sm.slot[w][lane] = row_find(sm.cols[w], 0, m, AP.col[q]);
         }
+        __syncwarp();
+        gal_accumulate<NV>(sm.slot[w], sm.prod[w], min(32, total - cb), lane, a0, a1);
+        __syncwarp();
+      }
+      __syncwarp();
     }
+    double* out = const_cast<double*>(Ac.val) + (size_t)c0 * NV;
+    if (lane < m)
+#pragma unroll
+      for (int v = 0; v < NV; ++v) out[(size_t)lane * NV + v] = a0[v];
+    if (lane + 32 < m)
+#pragma unroll
+      for (int v = 0; v < NV; ++v) out[(size_t)(lane + 32) * NV + v] = a1[v];
+    __syncwarp();
   }
 }
 
@@ -568,35 +734,6 @@ __global__ void k_amg_smooth0(int n, const double* __restrict__ dinv, const doub
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n * B; i += gridDim.x * blockDim.x) x[i] = w * dinv[i] * b[i];
 }
 
-// xo = x + w D^-1 (b - A x)   (RES: xo = b - A x instead)
-template <int B, bool RES>
-__global__ void k_amg_sweep(int n, AmgBsr A, const double* __restrict__ dinv, const double* __restrict__ lam,
-                            const double* __restrict__ b, const double* __restrict__ x, double* __restrict__ xo) {
-  const double w = RES ? 0.0 : 4.0 / (3.0 * *lam);
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    double acc[B];
-#pragma unroll
-    for (int r = 0; r < B; ++r) acc[r] = 0.0;
-    for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) {
-      const double* blk = A.val + (size_t)k * B * B;
-      const double* xj = x + (size_t)A.col[k] * B;
-      double xv[B];
-#pragma unroll
-      for (int c = 0; c < B; ++c) xv[c] = xj[c];
-#pragma unroll
-      for (int r = 0; r < B; ++r)
-#pragma unroll
-        for (int c = 0; c < B; ++c) acc[r] = fma(blk[r * B + c], xv[c], acc[r]);
-    }
-#pragma unroll
-    for (int r = 0; r < B; ++r) {
-      const size_t d = (size_t)i * B + r;
-      const double res = b[d] - acc[r];
-      xo[d] = RES ? res : fma(w * dinv[d], res, x[d]);
-    }
-  }
-}
-
 // Finest-level sweep on the FP32 difference-form operator of mixed_kernels.cu (the smoother is a
 // preconditioner: FP32 matrix values, FP64 vectors and accumulation). Thread per node.
 //   RES: xo = b - A x;   otherwise xo = x + w D^-1 (b - A x)
@@ -611,7 +748,28 @@ __global__ void __launch_bounds__(256) k_amg_sweep_f32(MixedMatrix M, const doub
     const int o = bb - n, c = __ldg(&M.node_ptr[n + 1]) - bb - 1;
     const double2 xs = x2[n];
     double ya = 0.0, yb = 0.0;
-    for (int k = 0; k < c; ++k) {
+    int k = 0;
+    // four neighbours at a time: all index and value loads first, then the gathers, then the
+    // additions in neighbour order (the same order as the loop below)
+    for (; k + 4 <= c; k += 4) {
+      int m[4];
+      float4 a[4];
+      double2 xm[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        m[u] = __ldg(&M.nbr32[o + k + u]);
+        a[u] = __ldg(&M.val32[o + k + u]);
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) xm[u] = x2[m[u]];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const double dx = xm[u].x - xs.x, dy = xm[u].y - xs.y;
+        ya = fma((double)a[u].x, dx, fma((double)a[u].y, dy, ya));
+        yb = fma((double)a[u].z, dx, fma((double)a[u].w, dy, yb));
+      }
+    }
+    for (; k < c; ++k) {
       const int m = __ldg(&M.nbr32[o + k]);
       const float4 a = __ldg(&M.val32[o + k]);
       const double2 xm = x2[m];
@@ -635,13 +793,13 @@ __global__ void __launch_bounds__(256) k_amg_sweep_f32(MixedMatrix M, const doub
   }
 }
 
-// Coarse-level (3 x 3 blocks) sweep: 8 lanes per row, lanes over the row's blocks, then a fixed
-// shuffle tree. RES: xo = b - A x; otherwise xo = x + w D^-1 (b - A x).
+// Coarse-level sweep on the FP32 copy of a 3 x 3 block operator (FP64 vectors and accumulation):
+// 8 lanes per row, lanes over the row's blocks, then a fixed shuffle tree.
+// RES: xo = b - A x; otherwise xo = x + w D^-1 (b - A x).
 template <bool RES>
-__global__ void __launch_bounds__(256) k_amg_sweep3_warp(AmgBsr A, const double* __restrict__ dinv,
-                                                         const double* __restrict__ lam,
-                                                         const double* __restrict__ b, const double* __restrict__ x,
-                                                         double* __restrict__ xo) {
+__global__ void __launch_bounds__(256) k_amg_sweep3_f32(AmgBsr32 A, const double* __restrict__ dinv,
+                                                        const double* __restrict__ lam, const double* __restrict__ b,
+                                                        const double* __restrict__ x, double* __restrict__ xo) {
   const double w = RES ? 0.0 : 4.0 / (3.0 * *lam);
   const int lane = threadIdx.x & 31, l8 = lane & 7, sub = lane >> 3;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
@@ -649,13 +807,17 @@ __global__ void __launch_bounds__(256) k_amg_sweep3_warp(AmgBsr A, const double*
     const int i = base + sub;
     double a0 = 0.0, a1 = 0.0, a2 = 0.0;
     if (i < A.n) {
-      for (int k = A.ptr[i] + l8; k < A.ptr[i + 1]; k += 8) {
-        const double* blk = A.val + (size_t)k * 9;
-        const double* xj = x + 3 * (size_t)A.col[k];
+      const int k1 = __ldg(&A.ptr[i + 1]);
+      for (int k = __ldg(&A.ptr[i]) + l8; k < k1; k += 8) {
+        const float* blk = A.val + (size_t)k * 9;
+        const double* xj = x + 3 * (size_t)__ldg(&A.col[k]);
+        float v[9];
+#pragma unroll
+        for (int e = 0; e < 9; ++e) v[e] = __ldg(&blk[e]);
         const double x0 = xj[0], x1 = xj[1], x2v = xj[2];
-        a0 = fma(blk[0], x0, fma(blk[1], x1, fma(blk[2], x2v, a0)));
-        a1 = fma(blk[3], x0, fma(blk[4], x1, fma(blk[5], x2v, a1)));
-        a2 = fma(blk[6], x0, fma(blk[7], x1, fma(blk[8], x2v, a2)));
+        a0 = fma((double)v[0], x0, fma((double)v[1], x1, fma((double)v[2], x2v, a0)));
+        a1 = fma((double)v[3], x0, fma((double)v[4], x1, fma((double)v[5], x2v, a1)));
+        a2 = fma((double)v[6], x0, fma((double)v[7], x1, fma((double)v[8], x2v, a2)));
       }
     }
 #pragma unroll
@@ -673,26 +835,30 @@ __global__ void __launch_bounds__(256) k_amg_sweep3_warp(AmgBsr A, const double*
   }
 }
 
-// bc_J = sum over the P blocks of column J of P_iJ' r_i: one warp per coarse row, lanes over the
-// row's P blocks, fixed shuffle tree (deterministic).
+// bc_J = sum over the P blocks of column J of P_iJ' r_i, from the FP32 copy of P stored by coarse
+// row (pt32, pt_row): one warp per coarse row, lanes over the row's blocks, fixed shuffle tree.
 template <int B>
-__global__ void __launch_bounds__(256) k_amg_restrict_warp(int nc, const int* __restrict__ pt_ptr,
-                                                           const int* __restrict__ pt_idx,
-                                                           const int* __restrict__ p_row, AmgBsr P,
-                                                           const double* __restrict__ r, double* __restrict__ bc) {
+__global__ void __launch_bounds__(256) k_amg_restrict_f32(int nc, const int* __restrict__ pt_ptr,
+                                                          const int* __restrict__ pt_row,
+                                                          const float* __restrict__ pt32,
+                                                          const double* __restrict__ r, double* __restrict__ bc) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
   for (int J = warp; J < nc; J += nw) {
     double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-    for (int t = pt_ptr[J] + lane; t < pt_ptr[J + 1]; t += 32) {
-      const int q = pt_idx[t], i = p_row[q];
-      const double* pb = P.val + (size_t)q * B * 3;
+    const int t1 = __ldg(&pt_ptr[J + 1]);
+    for (int t = __ldg(&pt_ptr[J]) + lane; t < t1; t += 32) {
+      const int i = __ldg(&pt_row[t]);
+      const float* pb = pt32 + (size_t)t * B * 3;
+      float v[B * 3];
+#pragma unroll
+      for (int e = 0; e < B * 3; ++e) v[e] = __ldg(&pb[e]);
 #pragma unroll
       for (int z = 0; z < B; ++z) {
         const double rv = r[(size_t)i * B + z];
-        a0 = fma(pb[z * 3 + 0], rv, a0);
-        a1 = fma(pb[z * 3 + 1], rv, a1);
-        a2 = fma(pb[z * 3 + 2], rv, a2);
+        a0 = fma((double)v[z * 3 + 0], rv, a0);
+        a1 = fma((double)v[z * 3 + 1], rv, a1);
+        a2 = fma((double)v[z * 3 + 2], rv, a2);
       }
     }
     a0 = warp_sum(a0);
@@ -702,45 +868,69 @@ __global__ void __launch_bounds__(256) k_amg_restrict_warp(int nc, const int* __
   }
 }
 
-// bc_J = sum over P blocks of column J of P_iJ' r_i
+// x += P xc with the FP32 copy of P (thread per fine row)
 template <int B>
-__global__ void k_amg_restrict(int nc, const int* __restrict__ pt_ptr, const int* __restrict__ pt_idx,
-                               const int* __restrict__ p_row, AmgBsr P, const double* __restrict__ r,
-                               double* __restrict__ bc) {
-  for (int J = blockIdx.x * blockDim.x + threadIdx.x; J < nc; J += gridDim.x * blockDim.x) {
-    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-    for (int t = pt_ptr[J]; t < pt_ptr[J + 1]; ++t) {
-      const int q = pt_idx[t], i = p_row[q];
-      const double* pb = P.val + (size_t)q * B * 3;
-#pragma unroll
-      for (int z = 0; z < B; ++z) {
-        const double rv = r[(size_t)i * B + z];
-        a0 = fma(pb[z * 3 + 0], rv, a0);
-        a1 = fma(pb[z * 3 + 1], rv, a1);
-        a2 = fma(pb[z * 3 + 2], rv, a2);
-      }
-    }
-    bc[3 * (size_t)J] = a0;
-    bc[3 * (size_t)J + 1] = a1;
-    bc[3 * (size_t)J + 2] = a2;
-  }
-}
-
-// x += P xc
-template <int B>
-__global__ void k_amg_prolong(int n, AmgBsr P, const double* __restrict__ xc, double* __restrict__ x) {
+__global__ void __launch_bounds__(256) k_amg_prolong_f32(int n, const int* __restrict__ p_ptr,
+                                                         const int* __restrict__ p_col, const float* __restrict__ p32,
+                                                         const double* __restrict__ xc, double* __restrict__ x) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     double acc[B];
 #pragma unroll
     for (int r = 0; r < B; ++r) acc[r] = x[(size_t)i * B + r];
-    for (int q = P.ptr[i]; q < P.ptr[i + 1]; ++q) {
-      const double* pb = P.val + (size_t)q * B * 3;
-      const double* c = xc + 3 * (size_t)P.col[q];
+    const int q1 = __ldg(&p_ptr[i + 1]);
+    for (int q = __ldg(&p_ptr[i]); q < q1; ++q) {
+      const float* pb = p32 + (size_t)q * B * 3;
+      const double* c = xc + 3 * (size_t)__ldg(&p_col[q]);
+      const double c0 = c[0], c1 = c[1], c2 = c[2];
 #pragma unroll
-      for (int r = 0; r < B; ++r) acc[r] = fma(pb[r * 3 + 2], c[2], fma(pb[r * 3 + 1], c[1], fma(pb[r * 3], c[0], acc[r])));
+      for (int r = 0; r < B; ++r)
+        acc[r] = fma((double)__ldg(&pb[r * 3 + 2]), c2,
+                     fma((double)__ldg(&pb[r * 3 + 1]), c1, fma((double)__ldg(&pb[r * 3]), c0, acc[r])));
     }
 #pragma unroll
     for (int r = 0; r < B; ++r) x[(size_t)i * B + r] = acc[r];
+  }
+}
+
+// FP32 copy of a coarse operator that is exactly symmetric: block (I, J) with J < I is the
+// transpose of the rounded block (J, I) (the FP64 Galerkin product is symmetric only to rounding)
+__global__ void k_amg_coarse_f32(AmgBsr A, float* __restrict__ val32) {
+  const int I = blockIdx.x * blockDim.x + threadIdx.x;
+  if (I >= A.n) return;
+  for (int k = A.ptr[I]; k < A.ptr[I + 1]; ++k) {
+    const int J = A.col[k];
+    int src = k;
+    bool tr = false;
+    if (J < I) {
+      const int m = row_find(A.col, A.ptr[J], A.ptr[J + 1], I);
+      if (m < A.ptr[J + 1] && A.col[m] == I) {
+        src = m;
+        tr = true;
+      }
+    }
+    const double* sv = A.val + (size_t)src * 9;
+    float* o = val32 + (size_t)k * 9;
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) o[r * 3 + c] = (float)(tr ? sv[c * 3 + r] : sv[r * 3 + c]);
+  }
+}
+
+// FP32 copies of P: by fine row (p32, P's own layout) and by coarse row (pt32 with the fine row
+// of each block in pt_row, in the order of the P' lists)
+template <int B>
+__global__ void k_amg_transfer_f32(int nnz_p, const double* __restrict__ pval, const int* __restrict__ pt_idx,
+                                   const int* __restrict__ p_row, float* __restrict__ p32, int* __restrict__ pt_row,
+                                   float* __restrict__ pt32) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nnz_p) return;
+  const int q = pt_idx[t];
+  pt_row[t] = p_row[q];
+#pragma unroll
+  for (int v = 0; v < B * 3; ++v) {
+    p32[(size_t)t * B * 3 + v] = (float)pval[(size_t)t * B * 3 + v];
+    pt32[(size_t)t * B * 3 + v] = (float)pval[(size_t)q * B * 3 + v];
   }
 }
 
@@ -901,11 +1091,15 @@ cudaError_t amg_ap_count(int B, const AmgBsr& A, const AmgBsr& P, int* cnt, int*
 }
 
 cudaError_t amg_ap_fill(int B, const AmgBsr& A, const AmgBsr& P, const AmgBsr& AP, cudaStream_t s) {
-  if (B == 2)
-    k_amg_ap_fill<2><<<g1(A.n, 128), 128, 0, s>>>(A.n, A, P, AP);
-  else
-    k_amg_ap_fill<3><<<g1(A.n, 128), 128, 0, s>>>(A.n, A, P, AP);
-  count_launches(1);
+  const int gv = (int)std::max<long long>(1, std::min<long long>(((long long)A.n + kGalWarps - 1) / kGalWarps, 148LL * 16));
+  if (B == 2) {
+    k_amg_ap_cols<2><<<g1(A.n, 128), 128, 0, s>>>(A.n, A, P, AP);
+    k_amg_ap_vals<2><<<gv, 32 * kGalWarps, 0, s>>>(A.n, A, P, AP);
+  } else {
+    k_amg_ap_cols<3><<<g1(A.n, 128), 128, 0, s>>>(A.n, A, P, AP);
+    k_amg_ap_vals<3><<<gv, 32 * kGalWarps, 0, s>>>(A.n, A, P, AP);
+  }
+  count_launches(2);
   return cudaGetLastError();
 }
 
@@ -935,11 +1129,13 @@ cudaError_t amg_ac_count(int B, int nc, const int* pt_ptr, const int* pt_idx, co
 
 cudaError_t amg_ac_fill(int B, int nc, const int* pt_ptr, const int* pt_idx, const int* p_row, const AmgBsr& P,
                         const AmgBsr& AP, const AmgBsr& Ac, cudaStream_t s) {
+  const int gv = (int)std::max<long long>(1, std::min<long long>(((long long)nc + kGalWarps - 1) / kGalWarps, 148LL * 16));
+  k_amg_ac_cols<<<g1(nc, 128), 128, 0, s>>>(nc, pt_ptr, pt_idx, p_row, AP, Ac);
   if (B == 2)
-    k_amg_ac_fill<2><<<g1(nc, 128), 128, 0, s>>>(nc, pt_ptr, pt_idx, p_row, P, AP, Ac);
+    k_amg_ac_vals<2><<<gv, 32 * kGalWarps, 0, s>>>(nc, pt_ptr, pt_idx, p_row, P, AP, Ac);
   else
-    k_amg_ac_fill<3><<<g1(nc, 128), 128, 0, s>>>(nc, pt_ptr, pt_idx, p_row, P, AP, Ac);
-  count_launches(1);
+    k_amg_ac_vals<3><<<gv, 32 * kGalWarps, 0, s>>>(nc, pt_ptr, pt_idx, p_row, P, AP, Ac);
+  count_launches(2);
   return cudaGetLastError();
 }
 
@@ -974,47 +1170,49 @@ cudaError_t amg_sweep_f32(bool residual, const MixedMatrix& M, const double* din
   return cudaGetLastError();
 }
 
-cudaError_t amg_sweep(int B, bool residual, const AmgBsr& A, const double* dinv, const double* lam, const double* b,
-                      const double* x, double* xo, cudaStream_t s) {
-  const int n = A.n;
-  if (B == 3) {
-    if (residual)
-      k_amg_sweep3_warp<true><<<gw((long long)n * 8), 256, 0, s>>>(A, dinv, lam, b, x, xo);
-    else
-      k_amg_sweep3_warp<false><<<gw((long long)n * 8), 256, 0, s>>>(A, dinv, lam, b, x, xo);
-    count_launches(1);
-    return cudaGetLastError();
-  }
-  if (B == 2) {
-    if (residual)
-      k_amg_sweep<2, true><<<gw(n), 256, 0, s>>>(n, A, dinv, lam, b, x, xo);
-    else
-      k_amg_sweep<2, false><<<gw(n), 256, 0, s>>>(n, A, dinv, lam, b, x, xo);
-  } else {
-    if (residual)
-      k_amg_sweep<3, true><<<gw(n), 256, 0, s>>>(n, A, dinv, lam, b, x, xo);
-    else
-      k_amg_sweep<3, false><<<gw(n), 256, 0, s>>>(n, A, dinv, lam, b, x, xo);
-  }
+cudaError_t amg_sweep3_f32(bool residual, const AmgBsr32& A, const double* dinv, const double* lam, const double* b,
+                           const double* x, double* xo, cudaStream_t s) {
+  if (residual)
+    k_amg_sweep3_f32<true><<<gw((long long)A.n * 8), 256, 0, s>>>(A, dinv, lam, b, x, xo);
+  else
+    k_amg_sweep3_f32<false><<<gw((long long)A.n * 8), 256, 0, s>>>(A, dinv, lam, b, x, xo);
   count_launches(1);
   return cudaGetLastError();
 }
 
-cudaError_t amg_restrict(int B, int nc, const int* pt_ptr, const int* pt_idx, const int* p_row, const AmgBsr& P,
-                         const double* r, double* bc, cudaStream_t s) {
+cudaError_t amg_restrict_f32(int B, int nc, const int* pt_ptr, const int* pt_row, const float* pt32, const double* r,
+                             double* bc, cudaStream_t s) {
   if (B == 2)
-    k_amg_restrict_warp<2><<<gw((long long)nc * 32), 256, 0, s>>>(nc, pt_ptr, pt_idx, p_row, P, r, bc);
+    k_amg_restrict_f32<2><<<gw((long long)nc * 32), 256, 0, s>>>(nc, pt_ptr, pt_row, pt32, r, bc);
   else
-    k_amg_restrict_warp<3><<<gw((long long)nc * 32), 256, 0, s>>>(nc, pt_ptr, pt_idx, p_row, P, r, bc);
+    k_amg_restrict_f32<3><<<gw((long long)nc * 32), 256, 0, s>>>(nc, pt_ptr, pt_row, pt32, r, bc);
   count_launches(1);
   return cudaGetLastError();
 }
 
-cudaError_t amg_prolong(int B, const AmgBsr& P, const double* xc, double* x, cudaStream_t s) {
+cudaError_t amg_prolong_f32(int B, int n, const int* p_ptr, const int* p_col, const float* p32, const double* xc,
+                            double* x, cudaStream_t s) {
   if (B == 2)
-    k_amg_prolong<2><<<gw(P.n), 256, 0, s>>>(P.n, P, xc, x);
+    k_amg_prolong_f32<2><<<gw(n), 256, 0, s>>>(n, p_ptr, p_col, p32, xc, x);
   else
-    k_amg_prolong<3><<<gw(P.n), 256, 0, s>>>(P.n, P, xc, x);
+    k_amg_prolong_f32<3><<<gw(n), 256, 0, s>>>(n, p_ptr, p_col, p32, xc, x);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t amg_coarse_f32(const AmgBsr& A, float* val32, cudaStream_t s) {
+  k_amg_coarse_f32<<<g1(A.n), 256, 0, s>>>(A, val32);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t amg_transfer_f32(int B, const AmgBsr& P, int nnz_p, const int* pt_idx, const int* p_row, float* p32,
+                             int* pt_row, float* pt32, cudaStream_t s) {
+  if (nnz_p <= 0) return cudaSuccess;
+  if (B == 2)
+    k_amg_transfer_f32<2><<<g1(nnz_p), 256, 0, s>>>(nnz_p, P.val, pt_idx, p_row, p32, pt_row, pt32);
+  else
+    k_amg_transfer_f32<3><<<g1(nnz_p), 256, 0, s>>>(nnz_p, P.val, pt_idx, p_row, p32, pt_row, pt32);
   count_launches(1);
   return cudaGetLastError();
 }

@@ -25,12 +25,24 @@ struct AmgLevel {
   DevBuf dinv, lam;
   DevBuf p_ptr, p_col, p_val, p_row, pt_ptr, pt_idx;  // transfer to the next level
   DevBuf xa, xb, r, bc;          // cycle vectors (bc: this level's right-hand side, levels >= 1)
+  // the cycle's FP32 operators: this level's matrix (levels >= 1) and the transfer to the next
+  // level, by fine row (p32) and by coarse row (pt32 with the fine row of each block in pt_row)
+  DevBuf val32, p32, pt32, pt_row;
+  int nnz_p = 0;
   AmgBsr A() const {
     AmgBsr m;
     m.n = n;
     m.ptr = a_ptr;
     m.col = a_col;
     m.val = static_cast<const double*>(val.p);
+    return m;
+  }
+  AmgBsr32 A32() const {
+    AmgBsr32 m;
+    m.n = n;
+    m.ptr = a_ptr;
+    m.col = a_col;
+    m.val = static_cast<const float*>(val32.p);
     return m;
   }
   AmgBsr P() const {
@@ -44,7 +56,8 @@ struct AmgLevel {
 };
 
 struct AmgData {
-  std::vector<AmgLevel> L;
+  std::vector<AmgLevel> L;    // level storage: only grows, so rebuilds reuse the buffers
+  int nl = 0;                 // levels of the current hierarchy (L[0 .. nl-1])
   DevBuf Minv, piv;
   int n_coarse = 0;           // DOFs of the dense coarsest level
   unsigned long long built_for = ~0ull;  // setup_count of the matrix it was built from
@@ -59,7 +72,7 @@ void cstg_host::amg_free(cstg_ctx* ctx) {
   AmgData* d = ctx->amg;
   for (AmgLevel& l : d->L) {
     DevBuf* all[] = {&l.ptr, &l.col, &l.val, &l.dinv, &l.lam, &l.p_ptr, &l.p_col, &l.p_val, &l.p_row, &l.pt_ptr,
-                     &l.pt_idx, &l.xa, &l.xb, &l.r, &l.bc};
+                     &l.pt_idx, &l.xa, &l.xb, &l.r, &l.bc, &l.val32, &l.p32, &l.pt32, &l.pt_row};
     for (DevBuf* b : all) free_buf(*b);
   }
   DevBuf* all[] = {&d->Minv, &d->piv, &d->state, &d->m1, &d->newroot, &d->near, &d->und, &d->root_id, &d->flags,
@@ -179,9 +192,17 @@ int coarsen(cstg_ctx* ctx, AmgData* d, int l, bool* stop) {
   ENSURE(lv.pt_idx, sizeof(int) * (size_t)std::max(nnz_p, 1));
   CK(amg_pt(n, nc, P, buf_ptr<int>(lv.p_row), buf_ptr<int>(lv.pt_ptr), buf_ptr<int>(d->cnt), buf_ptr<int>(d->cur),
             buf_ptr<int>(lv.pt_idx), buf_ptr<int>(ctx->scan_tmp), ctx->stream));
+  // the cycle's FP32 copies of P
+  ENSURE(lv.p32, sizeof(float) * (size_t)std::max(nnz_p, 1) * B * 3);
+  ENSURE(lv.pt32, sizeof(float) * (size_t)std::max(nnz_p, 1) * B * 3);
+  ENSURE(lv.pt_row, sizeof(int) * (size_t)std::max(nnz_p, 1));
+  lv.nnz_p = nnz_p;
+  CK(amg_transfer_f32(B, P, nnz_p, buf_ptr<int>(lv.pt_idx), buf_ptr<int>(lv.p_row), buf_ptr<float>(lv.p32),
+                      buf_ptr<int>(lv.pt_row), buf_ptr<float>(lv.pt32), ctx->stream));
   // coarse operator
-  d->L.emplace_back();
-  AmgLevel& nx = d->L.back();
+  if ((int)d->L.size() < l + 2) d->L.emplace_back();
+  d->nl = l + 2;
+  AmgLevel& nx = d->L[l + 1];
   AmgLevel& cur = d->L[l];  // (re-fetched: emplace_back may move the vector)
   nx.B = 3;
   nx.n = nc;
@@ -203,6 +224,8 @@ int coarsen(cstg_ctx* ctx, AmgData* d, int l, bool* stop) {
   AmgBsr Ac = nx.A();
   CK(amg_ac_fill(B, nc, buf_ptr<int>(cur.pt_ptr), buf_ptr<int>(cur.pt_idx), buf_ptr<int>(cur.p_row), cur.P(), AP, Ac,
                  ctx->stream));
+  ENSURE(nx.val32, sizeof(float) * (size_t)std::max(nnz_c, 1) * 9);
+  CK(amg_coarse_f32(Ac, buf_ptr<float>(nx.val32), ctx->stream));
   // the coarse nullspace becomes the next level's basis
   ENSURE(d->Bf, sizeof(double) * (size_t)std::max(n * B * 3, nc * 9));
   CK(cudaMemcpyAsync(d->Bf.p, d->Bc.p, sizeof(double) * (size_t)nc * 9, cudaMemcpyDeviceToDevice, ctx->stream));
@@ -210,11 +233,14 @@ int coarsen(cstg_ctx* ctx, AmgData* d, int l, bool* stop) {
 }
 
 int amg_build(cstg_ctx* ctx) {
-  if (!ctx->amg) ctx->amg = new AmgData();
+  if (!ctx->amg) {
+    ctx->amg = new AmgData();
+    ctx->amg->L.reserve(kMaxLevels + 1);
+  }
   AmgData* d = ctx->amg;
   const auto t0 = std::chrono::steady_clock::now();
-  d->L.clear();
-  d->L.emplace_back();
+  if (d->L.empty()) d->L.emplace_back();
+  d->nl = 1;
   {
     AmgLevel& f = d->L[0];
     f.B = 2;
@@ -241,7 +267,7 @@ int amg_build(cstg_ctx* ctx) {
   READ_ERR();
   if (ctx->h_err[kErrDiag] != kErrNone)
     return fail(ctx, CSTG_ERR_NONPOSITIVE_DIAGONAL, "amg_setup: non-positive diagonal on a level");
-  AmgLevel& last = d->L.back();
+  AmgLevel& last = d->L[d->nl - 1];
   d->n_coarse = last.n * last.B;
   if (d->n_coarse > 1536)
     return fail(ctx, CSTG_ERR_UNSUPPORTED, "amg_setup: coarsest level has %d DOFs (coarsening stalled)", d->n_coarse);
@@ -250,7 +276,7 @@ int amg_build(cstg_ctx* ctx) {
   // (a matrix at or below the coarsest size is its own coarsest level: the cycle is a direct solve)
   CK(amg_coarsest(last.B, last.A(), buf_ptr<double>(d->Minv), buf_ptr<double>(d->piv), ctx->stream));
   // cycle vectors
-  for (size_t l = 0; l < d->L.size(); ++l) {
+  for (int l = 0; l < d->nl; ++l) {
     AmgLevel& lv = d->L[l];
     const size_t m = (size_t)lv.n * lv.B;
     ENSURE(lv.xa, sizeof(double) * m);
@@ -268,31 +294,33 @@ int amg_build(cstg_ctx* ctx) {
 int vcycle(cstg_ctx* ctx, AmgData* d, size_t l, const double* b, double* x) {
   AmgLevel& lv = d->L[l];
   cudaStream_t s = ctx->stream;
-  if (l + 1 == d->L.size()) {
+  if ((int)l + 1 == d->nl) {
     CK(amg_gemv(d->n_coarse, buf_ptr<double>(d->Minv), b, x, s));
     return CSTG_OK;
   }
-  const AmgBsr A = lv.A();
   const double* dinv = buf_ptr<double>(lv.dinv);
   const double* lam = buf_ptr<double>(lv.lam);
   double* xa = buf_ptr<double>(lv.xa);
   double* r = buf_ptr<double>(lv.r);
   AmgLevel& nx = d->L[l + 1];
-  // the finest level smooths with the FP32 difference-form operator (a preconditioner: FP32
-  // values, FP64 vectors); coarse levels with their FP64 Galerkin operators
-  const bool f32 = l == 0;
-  const MixedMatrix mm = f32 ? mixed_view(ctx) : MixedMatrix{};
+  // every operator of the cycle is FP32 (vectors and accumulation FP64): the finest level smooths
+  // with the difference-form operator of the mixed solve, coarse levels with their Galerkin
+  // operators rounded symmetrically, and the transfers use FP32 copies of P
+  const bool fine = l == 0;
+  const MixedMatrix mm = fine ? mixed_view(ctx) : MixedMatrix{};
+  const AmgBsr32 A32 = lv.A32();
   auto sweep = [&](bool res, const double* xin, double* xout) -> cudaError_t {
-    return f32 ? amg_sweep_f32(res, mm, dinv, lam, b, xin, xout, s) : amg_sweep(lv.B, res, A, dinv, lam, b, xin, xout, s);
+    return fine ? amg_sweep_f32(res, mm, dinv, lam, b, xin, xout, s) : amg_sweep3_f32(res, A32, dinv, lam, b, xin, xout, s);
   };
   CK(amg_smooth0(lv.B, lv.n, dinv, lam, b, xa, s));
   CK(sweep(false, xa, x));
   CK(sweep(true, x, r));
-  CK(amg_restrict(lv.B, lv.nc, buf_ptr<int>(lv.pt_ptr), buf_ptr<int>(lv.pt_idx), buf_ptr<int>(lv.p_row), lv.P(), r,
-                  buf_ptr<double>(nx.bc), s));
+  CK(amg_restrict_f32(lv.B, lv.nc, buf_ptr<int>(lv.pt_ptr), buf_ptr<int>(lv.pt_row), buf_ptr<float>(lv.pt32), r,
+                      buf_ptr<double>(nx.bc), s));
   const int rc = vcycle(ctx, d, l + 1, buf_ptr<double>(nx.bc), buf_ptr<double>(nx.xb));
   if (rc) return rc;
-  CK(amg_prolong(lv.B, lv.P(), buf_ptr<double>(nx.xb), x, s));
+  CK(amg_prolong_f32(lv.B, lv.n, buf_ptr<int>(lv.p_ptr), buf_ptr<int>(lv.p_col), buf_ptr<float>(lv.p32),
+                     buf_ptr<double>(nx.xb), x, s));
   CK(sweep(false, x, xa));
   CK(sweep(false, xa, x));
   return CSTG_OK;
@@ -310,7 +338,24 @@ int cstg_host::amg_ready(cstg_ctx* ctx) {
   return amg_build(ctx);
 }
 
-int cstg_host::amg_levels(const cstg_ctx* ctx) { return ctx->amg ? (int)ctx->amg->L.size() : 0; }
+int cstg_host::amg_levels(const cstg_ctx* ctx) { return ctx->amg ? ctx->amg->nl : 0; }
+
+unsigned long long cstg_host::amg_signature(const cstg_ctx* ctx) {
+  // the launch shapes and scalar arguments a captured cycle depends on (buffer moves are
+  // covered by the context's generation)
+  unsigned long long h = 1469598103934665603ull;
+  auto mix = [&h](unsigned long long v) { h = (h ^ v) * 1099511628211ull; };
+  const AmgData* d = ctx->amg;
+  if (!d) return h;
+  mix((unsigned long long)d->nl);
+  mix((unsigned long long)d->n_coarse);
+  for (int l = 0; l < d->nl; ++l) {
+    mix((unsigned long long)d->L[l].B);
+    mix((unsigned long long)d->L[l].n);
+    mix((unsigned long long)d->L[l].nc);
+  }
+  return h;
+}
 
 int cstg_host::amg_apply(cstg_ctx* ctx, const double* r, double* z) {
   return vcycle(ctx, ctx->amg, 0, r, z);
@@ -326,7 +371,7 @@ int cstg_amg_setup(cstg_ctx* ctx, cstg_amg_info* info) {
   if (info) {
     AmgData* d = ctx->amg;
     std::memset(info, 0, sizeof *info);
-    info->levels = (int)d->L.size();
+    info->levels = d->nl;
     for (int l = 0; l < info->levels && l < 16; ++l) info->dofs[l] = d->L[l].n * d->L[l].B;
     for (int l = 0; l < info->levels && l < 16; ++l) {
       const AmgLevel& lv = d->L[l];
@@ -336,6 +381,46 @@ int cstg_amg_setup(cstg_ctx* ctx, cstg_amg_info* info) {
     }
     info->setup_seconds = d->setup_seconds;
   }
+  return CSTG_OK;
+}
+
+int cstg_amg_time(cstg_ctx* ctx, int reps, double* out) {
+  BEGIN(ctx);
+  if (reps < 1 || !out) return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "amg_time: bad arguments");
+  const int rc = amg_ready(ctx);
+  if (rc) return rc;
+  AmgData* d = ctx->amg;
+  AmgLevel& f = d->L[0];
+  const size_t m = (size_t)f.n * f.B;
+  double* b = buf_ptr<double>(f.bc);
+  double* xa = buf_ptr<double>(f.xa);
+  double* xb = buf_ptr<double>(f.xb);
+  CK(cudaMemsetAsync(b, 0, sizeof(double) * m, ctx->stream));
+  CK(cudaMemsetAsync(xa, 0, sizeof(double) * m, ctx->stream));
+  const MixedMatrix mm = mixed_view(ctx);
+  float ms = 0.f;
+  for (int w = 0; w < 2; ++w) {  // warm-up, then timed
+    CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    for (int k = 0; k < reps; ++k)
+      CK(amg_sweep_f32(false, mm, buf_ptr<double>(f.dinv), buf_ptr<double>(f.lam), b, k & 1 ? xb : xa, k & 1 ? xa : xb,
+                       ctx->stream));
+    CK(cudaEventRecord(ctx->ev1, ctx->stream));
+  }
+  CK(cudaEventSynchronize(ctx->ev1));
+  CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+  out[0] = ms * 1e-3 / reps;
+  // (the finest level's xa and r are the cycle's scratch; its xb and bc are free)
+  for (int w = 0; w < 2; ++w) {
+    CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    for (int k = 0; k < reps; ++k) {
+      const int rc2 = vcycle(ctx, d, 0, b, xb);
+      if (rc2) return rc2;
+    }
+    CK(cudaEventRecord(ctx->ev1, ctx->stream));
+  }
+  CK(cudaEventSynchronize(ctx->ev1));
+  CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+  out[1] = ms * 1e-3 / reps;
   return CSTG_OK;
 }
 

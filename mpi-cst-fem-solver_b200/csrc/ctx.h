@@ -257,6 +257,7 @@ int amg_ready(cstg_ctx* ctx);
 int amg_apply(cstg_ctx* ctx, const double* r, double* z);
 void amg_free(cstg_ctx* ctx);
 int amg_levels(const cstg_ctx* ctx);
+unsigned long long amg_signature(const cstg_ctx* ctx);  // level shapes of the current hierarchy
 
 // Defined in learned_api.cu: flexible CG with the learned preconditioner.
 int run_fcg(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg_solver_options& o, cstg_stats* stats);

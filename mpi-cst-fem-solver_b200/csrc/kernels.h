@@ -241,6 +241,12 @@ struct AmgBsr {  // n block rows, ptr[n + 1], col[ptr[n]], val: B x B (or B x 3 
   const int* col = nullptr;
   const double* val = nullptr;
 };
+struct AmgBsr32 {  // a coarse operator's FP32 copy (3 x 3 blocks), same pattern
+  int n = 0;
+  const int* ptr = nullptr;
+  const int* col = nullptr;
+  const float* val = nullptr;
+};
 cudaError_t amg_fine_bsr(int N, const int* node_ptr, const double* vals, double* out, cudaStream_t s);
 cudaError_t amg_dinv(int B, const AmgBsr& A, double* dinv, int* err, cudaStream_t s);
 cudaError_t amg_mis_round(const AmgBsr& A, int* state, unsigned long long* m1, int* newroot, int* near, int* undecided,
@@ -269,13 +275,18 @@ cudaError_t amg_ac_fill(int B, int nc, const int* pt_ptr, const int* pt_idx, con
                         const AmgBsr& AP, const AmgBsr& Ac, cudaStream_t s);
 cudaError_t amg_coarsest(int B, const AmgBsr& A, double* M, double* piv, cudaStream_t s);
 cudaError_t amg_smooth0(int B, int n, const double* dinv, const double* lam, const double* b, double* x, cudaStream_t s);
-cudaError_t amg_sweep(int B, bool residual, const AmgBsr& A, const double* dinv, const double* lam, const double* b,
-                      const double* x, double* xo, cudaStream_t s);
 cudaError_t amg_sweep_f32(bool residual, const MixedMatrix& M, const double* dinv, const double* lam, const double* b,
                           const double* x, double* xo, cudaStream_t s);
-cudaError_t amg_restrict(int B, int nc, const int* pt_ptr, const int* pt_idx, const int* p_row, const AmgBsr& P,
-                         const double* r, double* bc, cudaStream_t s);
-cudaError_t amg_prolong(int B, const AmgBsr& P, const double* xc, double* x, cudaStream_t s);
+// cycle operators in FP32 (values only; vectors and accumulation stay FP64)
+cudaError_t amg_coarse_f32(const AmgBsr& A, float* val32, cudaStream_t s);
+cudaError_t amg_transfer_f32(int B, const AmgBsr& P, int nnz_p, const int* pt_idx, const int* p_row, float* p32,
+                             int* pt_row, float* pt32, cudaStream_t s);
+cudaError_t amg_sweep3_f32(bool residual, const AmgBsr32& A, const double* dinv, const double* lam, const double* b,
+                           const double* x, double* xo, cudaStream_t s);
+cudaError_t amg_restrict_f32(int B, int nc, const int* pt_ptr, const int* pt_row, const float* pt32, const double* r,
+                             double* bc, cudaStream_t s);
+cudaError_t amg_prolong_f32(int B, int n, const int* p_ptr, const int* p_col, const float* p32, const double* xc,
+                            double* x, cudaStream_t s);
 cudaError_t amg_gemv(int n, const double* M, const double* b, double* x, cudaStream_t s);
 cudaError_t amg_rigid_modes(int N, const double* xy, double* Bf, cudaStream_t s);
 

@@ -111,8 +111,12 @@ int cstg_host::run_fcg(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg
     return CSTG_OK;
   };
   const int chunk = o.check_interval > 0 ? o.check_interval : 25;
-  unsigned long long key = ctx->generation * 1000003ull + (unsigned long long)chunk * 31ull +
-                           (unsigned long long)o.precision * 7ull + (unsigned long long)(uintptr_t)d_b;
+  // the captured chunk depends on the buffers (generation), the shapes and the method
+  unsigned long long key = 1469598103934665603ull;
+  for (unsigned long long v : {ctx->generation, (unsigned long long)chunk, (unsigned long long)o.precision,
+                               (unsigned long long)(uintptr_t)d_b, (unsigned long long)n,
+                               (unsigned long long)ctx->n_nodes, use_amg ? amg_signature(ctx) : 0ull})
+    key = (key ^ v) * 1099511628211ull;
   if (!ctx->fcg_graph || ctx->fcg_key != key || ctx->fcg_graph_precond != o.preconditioner) {
     if (ctx->fcg_graph) {
       cudaGraphExecDestroy(ctx->fcg_graph);
@@ -366,6 +370,8 @@ int cstg_learned_setup(cstg_ctx* ctx, const float* params, const float* node_mat
   }
   ENSURE(ctx->lp_sf, sizeof(float) * sf.size());
   ENSURE(ctx->lp_sc, sizeof(MpScratch));
+  // the reductions' tickets must start at zero (a fresh allocation may hold old contents)
+  CK(cudaMemsetAsync(ctx->lp_sc.p, 0, sizeof(MpScratch), ctx->stream));
   if (N) CK(cudaMemcpyAsync(ctx->lp_sf.p, sf.data(), sizeof(float) * sf.size(), cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   ctx->learned_ready = true;

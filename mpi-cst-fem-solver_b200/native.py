@@ -138,6 +138,7 @@ _SIGS = {
     "cstg_mesh_group": (C.c_int, [_vp, C.c_int, C.c_char_p, C.c_int, C.POINTER(C.c_int), _vp]),
     "cstg_amg_setup": (C.c_int, [_vp, C.POINTER(AmgInfo)]),
     "cstg_amg_apply_device": (C.c_int, [_vp, _vp, _vp]),
+    "cstg_amg_time": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_double)]),
     "cstg_mpnn_param_count": (C.c_longlong, []),
     "cstg_learned_setup": (C.c_int, [_vp, _vp, _vp]),
     "cstg_learned_set_params": (C.c_int, [_vp, _vp]),

@@ -428,3 +428,10 @@ def amg_apply(K: GpuCsrMatrix, r, z=None):
     K.ctx.check(K.ctx.L.cstg_amg_apply_device(K.ctx.h, _ptr(r), _ptr(z)))
     return z
 
+
+def amg_time(K: GpuCsrMatrix, reps: int = 20) -> dict:
+    """Seconds per finest-level smoothing sweep and per V-cycle (CUDA events, back to back)."""
+    out = (C.c_double * 2)()
+    K.ctx.check(K.ctx.L.cstg_amg_time(K.ctx.h, int(reps), out))
+    return {"sweep_s": out[0], "vcycle_s": out[1]}
+

@@ -65,6 +65,10 @@ def test_amg_vcycle_is_symmetric_positive(pkg, gpu_lib):
     a, c = float(torch.dot(Mu, v)), float(torch.dot(u, Mv))
     assert abs(a - c) <= 1e-8 * max(abs(a), abs(c))
     assert float(torch.dot(Mu, u)) > 0 and float(torch.dot(Mv, v)) > 0
+    # timing the cycle leaves the preconditioner unchanged
+    t = pkg.amg_time(K, reps=3)
+    assert 0 < t["sweep_s"] < t["vcycle_s"]
+    assert torch.equal(pkg.amg_apply(K, u), Mu)
     K.ctx.close()
 
 

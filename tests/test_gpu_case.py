@@ -51,7 +51,7 @@ def test_case_kirsch_L0_matches_reference(pkg, gpu_lib, golden, tmp_path):
     assert t["solver"]["iterations"] == g.meta["stress_iters10"]
 
 
-@pytest.mark.parametrize("solver", ["gpu_cg", "gpu_cg_mixed"])
+@pytest.mark.parametrize("solver", ["gpu_cg", "gpu_cg_mixed", "gpu_cg_amg"])
 def test_case_kirsch_exact_scf(pkg, gpu_lib, tmp_path, solver):
     mesh = pkg.plate.quarter_plate(40, 80)
     rc, out, err, d = _run(pkg, tmp_path, mesh, solver=solver, traction="kirsch_exact")
