@@ -355,6 +355,8 @@ typedef struct {
   int dofs[16];
   long long nnz[16];
   double setup_seconds;
+  int tail_level;    /* first level run by the one-cluster tail launch (0: none) */
+  int tail_cluster;  /* CTAs in that cluster */
 } cstg_amg_info;
 int cstg_amg_setup(cstg_ctx* ctx, cstg_amg_info* info);
 /* z = M r (device vectors) with the context's hierarchy (built if missing). */
@@ -362,6 +364,10 @@ int cstg_amg_apply_device(cstg_ctx* ctx, const double* d_r, double* d_z);
 /* Timing on the context's stream (CUDA events, `reps` back-to-back launches after a warm-up):
  * out[0] = seconds per finest-level smoothing sweep, out[1] = seconds per V-cycle. */
 int cstg_amg_time(cstg_ctx* ctx, int reps, double* out);
+/* The small coarse levels and the coarsest solve run as one thread-block-cluster launch with
+ * cluster barriers between phases (default), or as one launch per level and phase (enable = 0).
+ * Both give the same bits. */
+int cstg_amg_set_tail(cstg_ctx* ctx, int enable);
 
 #ifdef __cplusplus
 }

@@ -16,12 +16,15 @@
 // own output blocks): the hierarchy and the cycle are deterministic. Rows are built in two passes
 // (count, then fill after a prefix sum); row widths are bounded by kAmgMaxRow (checked: the error
 // word records the first overflow).
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include "common.cuh"
 #include "kernels.h"
 
 namespace cstg {
+
+namespace cg = cooperative_groups;
 
 namespace {
 
@@ -284,45 +287,57 @@ __global__ void k_amg_tentative(int n_agg, const int* __restrict__ agg_ptr, cons
   for (int k = 0; k < 9; ++k) Bc[(size_t)a * 9 + k] = R[k];
 }
 
-// ---- lambda_max(D^-1 A) by power iteration: y = D^-1 A x, and ||y||^2 -----------------------------
+// ---- lambda_max(D^-1 A) by power iteration ----------------------------------------------------------
+// y = s D^-1 A x with s = 1 / ||x|| from the previous step (1 on the first), and per-block partial
+// sums of ||y||^2 on a fixed grid; k_amg_norm adds the partials in block order.
+constexpr int kLamGrid = 148 * 8;
 
 template <int B>
 __global__ void __launch_bounds__(kThreads) k_amg_dinva(int n, AmgBsr A, const double* __restrict__ dinv,
-                                                        const double* __restrict__ x, double* __restrict__ y,
-                                                        double* __restrict__ part) {
+                                                        const double* sc, const double* __restrict__ x,
+                                                        double* __restrict__ y, double* __restrict__ part) {
+  const double s = sc ? *sc : 1.0;
   double ss = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     double acc[B];
 #pragma unroll
     for (int r = 0; r < B; ++r) acc[r] = 0.0;
-    for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) {
+    const int k1 = __ldg(&A.ptr[i + 1]);
+    for (int k = __ldg(&A.ptr[i]); k < k1; ++k) {
       const double* blk = A.val + (size_t)k * B * B;
-      const double* xj = x + (size_t)A.col[k] * B;
+      const double* xj = x + (size_t)__ldg(&A.col[k]) * B;
+      double xv[B];
+#pragma unroll
+      for (int c = 0; c < B; ++c) xv[c] = xj[c];
 #pragma unroll
       for (int r = 0; r < B; ++r)
 #pragma unroll
-        for (int c = 0; c < B; ++c) acc[r] = fma(blk[r * B + c], xj[c], acc[r]);
+        for (int c = 0; c < B; ++c) acc[r] = fma(__ldg(&blk[r * B + c]), xv[c], acc[r]);
     }
 #pragma unroll
     for (int r = 0; r < B; ++r) {
-      const double v = dinv[(size_t)i * B + r] * acc[r];
+      const double v = s * (dinv[(size_t)i * B + r] * acc[r]);
       y[(size_t)i * B + r] = v;
       ss = fma(v, v, ss);
     }
   }
   __shared__ double sm[kWarps];
-  const double s = block_sum<kThreads>(ss, sm);
-  if (threadIdx.x == 0) part[blockIdx.x] = s;
+  const double t = block_sum<kThreads>(ss, sm);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
 }
 
-__global__ void k_amg_scale(int n, const double* __restrict__ part, int nparts, double* __restrict__ x,
-                            double* __restrict__ lam) {
+// lam = sqrt(sum of the partials, in block order), sc = 1 / lam (one block)
+__global__ void __launch_bounds__(kThreads) k_amg_norm(const double* __restrict__ part, int nparts, double* lam,
+                                                       double* sc) {
   double s = 0.0;
-  for (int b = 0; b < nparts; ++b) s += part[b];
-  const double nrm = sqrt(s);
-  if (blockIdx.x == 0 && threadIdx.x == 0) *lam = nrm;
-  const double inv = nrm > 0.0 ? 1.0 / nrm : 0.0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] *= inv;
+  for (int b = threadIdx.x; b < nparts; b += blockDim.x) s += part[b];
+  __shared__ double sm[kWarps];
+  const double t = block_sum<kThreads>(s, sm);
+  if (threadIdx.x == 0) {
+    const double nrm = sqrt(t);
+    *lam = nrm;
+    *sc = nrm > 0.0 ? 1.0 / nrm : 0.0;
+  }
 }
 
 __global__ void k_amg_init_vec(int n, double* __restrict__ x) {
@@ -347,36 +362,17 @@ __global__ void k_amg_p_count(int n, AmgBsr A, const int* __restrict__ agg, int*
   cnt[i] = m;
 }
 
+// P's column sets (sorted aggregates of the row's neighbours, the node's own included)
 template <int B>
-__global__ void k_amg_p_fill(int n, AmgBsr A, const int* __restrict__ agg, const double* __restrict__ P0,
-                             const double* __restrict__ dinv, const double* __restrict__ wp, AmgBsr P) {
+__global__ void k_amg_p_cols(int n, AmgBsr A, const int* __restrict__ agg, AmgBsr P) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const double w = 4.0 / (3.0 * *wp);
-  int* cols = const_cast<int*>(P.col) + P.ptr[i];
-  double* vals = const_cast<double*>(P.val) + (size_t)P.ptr[i] * B * 3;
+  int s[kAmgMaxRow];
   int m = 0;
-  for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) set_insert(cols, m, agg[A.col[k]], kAmgMaxRow);
-  set_insert(cols, m, agg[i], kAmgMaxRow);
-  for (int q = 0; q < m * B * 3; ++q) vals[q] = 0.0;
-  // - w D^-1 sum_j A_ij P0_j, in ascending j
-  for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) {
-    const int j = A.col[k];
-    const int s = row_find(cols, 0, m, agg[j]);
-    const double* blk = A.val + (size_t)k * B * B;
-    const double* p0 = P0 + (size_t)j * B * 3;
-    double* o = vals + (size_t)s * B * 3;
-    for (int r = 0; r < B; ++r) {
-      const double f = -w * dinv[(size_t)i * B + r];
-      for (int c = 0; c < 3; ++c) {
-        double t = 0.0;
-        for (int q = 0; q < B; ++q) t = fma(blk[r * B + q], p0[q * 3 + c], t);
-        o[r * 3 + c] = fma(f, t, o[r * 3 + c]);
-      }
-    }
-  }
-  const int s = row_find(cols, 0, m, agg[i]);
-  for (int q = 0; q < B * 3; ++q) vals[(size_t)s * B * 3 + q] += P0[(size_t)i * B * 3 + q];
+  for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) set_insert(s, m, agg[A.col[k]], kAmgMaxRow);
+  set_insert(s, m, agg[i], kAmgMaxRow);
+  int* cols = const_cast<int*>(P.col) + P.ptr[i];
+  for (int q = 0; q < m; ++q) cols[q] = s[q];
 }
 
 // ---- AP = A P (rows: B x 3 blocks) --------------------------------------------------------------------
@@ -457,6 +453,71 @@ __device__ __forceinline__ int gal_member(const int* ofs, int ng, int t) {
       hi = mid - 1;
   }
   return lo;
+}
+
+// P = P0 - w D^-1 A P0: values, warp per row i. Candidates: the blocks k of A's row i in order,
+// each the B x 3 product -w D_i^-1 A_k P0_{A.col[k]}; then P0_i is added to the node's own
+// aggregate's block.
+template <int B>
+__global__ void __launch_bounds__(32 * kGalWarps) k_amg_p_vals(int n, AmgBsr A, const int* __restrict__ agg,
+                                                               const double* __restrict__ P0,
+                                                               const double* __restrict__ dinv,
+                                                               const double* __restrict__ wp, AmgBsr P) {
+  constexpr int NV = B * 3;
+  __shared__ GalerkinSmem<NV> sm;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int warp = blockIdx.x * kGalWarps + w, nw = gridDim.x * kGalWarps;
+  const double om = 4.0 / (3.0 * *wp);
+  for (int i = warp; i < n; i += nw) {
+    const int c0 = P.ptr[i], m = P.ptr[i + 1] - c0;
+    for (int t = lane; t < m; t += 32) sm.cols[w][t] = P.col[c0 + t];
+    __syncwarp();
+    double f[B];
+#pragma unroll
+    for (int r = 0; r < B; ++r) f[r] = -om * dinv[(size_t)i * B + r];
+    double a0[NV], a1[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) a0[v] = a1[v] = 0.0;
+    const int k0 = A.ptr[i], k1 = A.ptr[i + 1];
+    for (int kb = k0; kb < k1; kb += 32) {
+      const int k = kb + lane;
+      if (k < k1) {
+        const int j = A.col[k];
+        const double* blk = A.val + (size_t)k * B * B;
+        const double* p0 = P0 + (size_t)j * B * 3;
+#pragma unroll
+        for (int r = 0; r < B; ++r)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            double t = 0.0;
+#pragma unroll
+            for (int q = 0; q < B; ++q) t = fma(blk[r * B + q], p0[q * 3 + c], t);
+            sm.prod[w][lane][r * 3 + c] = f[r] * t;
+          }
+        sm.slot[w][lane] = row_find(sm.cols[w], 0, m, agg[j]);
+      }
+      __syncwarp();
+      gal_accumulate<NV>(sm.slot[w], sm.prod[w], min(32, k1 - kb), lane, a0, a1);
+      __syncwarp();
+    }
+    const int own = row_find(sm.cols[w], 0, m, agg[i]);
+    const double* p0i = P0 + (size_t)i * B * 3;
+    if (own == lane) {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) a0[v] += p0i[v];
+    } else if (own == lane + 32) {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) a1[v] += p0i[v];
+    }
+    double* out = const_cast<double*>(P.val) + (size_t)c0 * NV;
+    if (lane < m)
+#pragma unroll
+      for (int v = 0; v < NV; ++v) out[(size_t)lane * NV + v] = a0[v];
+    if (lane + 32 < m)
+#pragma unroll
+      for (int v = 0; v < NV; ++v) out[(size_t)(lane + 32) * NV + v] = a1[v];
+    __syncwarp();
+  }
 }
 
 // AP = A P: column sets
@@ -726,31 +787,37 @@ __global__ void __launch_bounds__(1024) k_amg_gauss_jordan(int n, double* __rest
 
 // ---- cycle kernels ----------------------------------------------------------------------------------
 
-// x = w D^-1 b  (first sweep from x = 0)
-template <int B>
-__global__ void k_amg_smooth0(int n, const double* __restrict__ dinv, const double* __restrict__ lam,
-                              const double* __restrict__ b, double* __restrict__ x) {
-  const double w = 4.0 / (3.0 * *lam);
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n * B; i += gridDim.x * blockDim.x) x[i] = w * dinv[i] * b[i];
+// Sweep modes. kSweepSmooth: xo = x + w D^-1 (b - A x); kSweepResidual: xo = b - A x;
+// kSweepFirst: the first sweep from x = 0, whose input x0 = w D^-1 b is formed on the fly from b
+// and D^-1 (the same rounding as storing it first), so x is not read.
+
+// x0 = w D^-1 b, component i (the first sweep's input)
+__device__ __forceinline__ double first_x(double w, const double* __restrict__ dinv, const double* __restrict__ b,
+                                          size_t i) {
+  return w * dinv[i] * b[i];
 }
 
 // Finest-level sweep on the FP32 difference-form operator of mixed_kernels.cu (the smoother is a
-// preconditioner: FP32 matrix values, FP64 vectors and accumulation). Thread per node.
-//   RES: xo = b - A x;   otherwise xo = x + w D^-1 (b - A x)
-template <bool RES>
+// preconditioner: FP32 matrix values, FP64 vectors and accumulation). Thread per node; four
+// neighbours' index and value loads are in flight at once, their gathers next, and the additions
+// follow in neighbour order.
+template <int MODE>
 __global__ void __launch_bounds__(256) k_amg_sweep_f32(MixedMatrix M, const double* __restrict__ dinv,
                                                        const double* __restrict__ lam, const double* __restrict__ b,
                                                        const double* __restrict__ x, double* __restrict__ xo) {
-  const double w = RES ? 0.0 : 4.0 / (3.0 * *lam);
+  const double w = MODE == kSweepResidual ? 0.0 : 4.0 / (3.0 * *lam);
   const double2* x2 = reinterpret_cast<const double2*>(x);
+  auto xnode = [&](int m) -> double2 {
+    if (MODE == kSweepFirst)
+      return make_double2(first_x(w, dinv, b, 2 * (size_t)m), first_x(w, dinv, b, 2 * (size_t)m + 1));
+    return x2[m];
+  };
   for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < M.n_nodes; n += gridDim.x * blockDim.x) {
     const int bb = __ldg(&M.node_ptr[n]);
     const int o = bb - n, c = __ldg(&M.node_ptr[n + 1]) - bb - 1;
-    const double2 xs = x2[n];
+    const double2 xs = xnode(n);
     double ya = 0.0, yb = 0.0;
     int k = 0;
-    // four neighbours at a time: all index and value loads first, then the gathers, then the
-    // additions in neighbour order (the same order as the loop below)
     for (; k + 4 <= c; k += 4) {
       int m[4];
       float4 a[4];
@@ -761,7 +828,7 @@ __global__ void __launch_bounds__(256) k_amg_sweep_f32(MixedMatrix M, const doub
         a[u] = __ldg(&M.val32[o + k + u]);
       }
 #pragma unroll
-      for (int u = 0; u < 4; ++u) xm[u] = x2[m[u]];
+      for (int u = 0; u < 4; ++u) xm[u] = xnode(m[u]);
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
         const double dx = xm[u].x - xs.x, dy = xm[u].y - xs.y;
@@ -772,7 +839,7 @@ __global__ void __launch_bounds__(256) k_amg_sweep_f32(MixedMatrix M, const doub
     for (; k < c; ++k) {
       const int m = __ldg(&M.nbr32[o + k]);
       const float4 a = __ldg(&M.val32[o + k]);
-      const double2 xm = x2[m];
+      const double2 xm = xnode(m);
       const double dx = xm.x - xs.x, dy = xm.y - xs.y;
       ya = fma((double)a.x, dx, fma((double)a.y, dy, ya));
       yb = fma((double)a.z, dx, fma((double)a.w, dy, yb));
@@ -783,7 +850,7 @@ __global__ void __launch_bounds__(256) k_amg_sweep_f32(MixedMatrix M, const doub
     const double2 bv = reinterpret_cast<const double2*>(b)[n];
     const double ra = bv.x - ya, rbv = bv.y - yb;
     double2 out;
-    if (RES) {
+    if (MODE == kSweepResidual) {
       out = make_double2(ra, rbv);
     } else {
       const double2 dv = reinterpret_cast<const double2*>(dinv)[n];
@@ -793,28 +860,40 @@ __global__ void __launch_bounds__(256) k_amg_sweep_f32(MixedMatrix M, const doub
   }
 }
 
-// Coarse-level sweep on the FP32 copy of a 3 x 3 block operator (FP64 vectors and accumulation):
-// 8 lanes per row, lanes over the row's blocks, then a fixed shuffle tree.
-// RES: xo = b - A x; otherwise xo = x + w D^-1 (b - A x).
-template <bool RES>
-__global__ void __launch_bounds__(256) k_amg_sweep3_f32(AmgBsr32 A, const double* __restrict__ dinv,
-                                                        const double* __restrict__ lam, const double* __restrict__ b,
-                                                        const double* __restrict__ x, double* __restrict__ xo) {
-  const double w = RES ? 0.0 : 4.0 / (3.0 * *lam);
-  const int lane = threadIdx.x & 31, l8 = lane & 7, sub = lane >> 3;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+// Loads of vectors: COH = false for standalone launches (the vector was written by an earlier
+// launch), true inside the coarse-tail kernel, where another CTA of the cluster wrote it in an
+// earlier phase: those loads go to L2 (ld.global.cg), never through the non-coherent path.
+template <bool COH>
+__device__ __forceinline__ double ldv(const double* p) {
+  if (COH) return __ldcg(p);
+  return *p;
+}
+
+// Coarse-level sweep on the FP32 copy of a 3 x 3 block operator (FP64 vectors and accumulation).
+// The copy is stored entry-major (val[e * nnzb + k], e = 0..8). 8 lanes per row (4 rows per
+// warp): the lanes of a row take consecutive blocks, so each entry load of the 8 lanes is one
+// contiguous 32-byte run; a fixed 3-step shuffle tree adds the lanes. Row groups are strided over
+// `nw` warps (warp index `warp`): rows of any length keep 8 lanes busy, and small levels still
+// spread over the whole grid.
+template <int MODE, bool COH>
+__device__ __forceinline__ void sweep3_rows(const AmgBsr32& A, const double* dinv, double w, const double* b,
+                                            const double* x, double* xo, int warp, int nw, int lane) {
+  auto xval = [&](size_t d) -> double {
+    return MODE == kSweepFirst ? w * __ldg(&dinv[d]) * ldv<COH>(&b[d]) : ldv<COH>(&x[d]);
+  };
+  const size_t nb = (size_t)A.nnzb;
+  const int l8 = lane & 7, sub = lane >> 3;
   for (int base = warp * 4; base < A.n; base += nw * 4) {
     const int i = base + sub;
     double a0 = 0.0, a1 = 0.0, a2 = 0.0;
     if (i < A.n) {
       const int k1 = __ldg(&A.ptr[i + 1]);
       for (int k = __ldg(&A.ptr[i]) + l8; k < k1; k += 8) {
-        const float* blk = A.val + (size_t)k * 9;
-        const double* xj = x + 3 * (size_t)__ldg(&A.col[k]);
+        const int c = __ldg(&A.col[k]);
         float v[9];
 #pragma unroll
-        for (int e = 0; e < 9; ++e) v[e] = __ldg(&blk[e]);
-        const double x0 = xj[0], x1 = xj[1], x2v = xj[2];
+        for (int e = 0; e < 9; ++e) v[e] = __ldg(&A.val[(size_t)e * nb + k]);
+        const double x0 = xval(3 * (size_t)c), x1 = xval(3 * (size_t)c + 1), x2v = xval(3 * (size_t)c + 2);
         a0 = fma((double)v[0], x0, fma((double)v[1], x1, fma((double)v[2], x2v, a0)));
         a1 = fma((double)v[3], x0, fma((double)v[4], x1, fma((double)v[5], x2v, a1)));
         a2 = fma((double)v[6], x0, fma((double)v[7], x1, fma((double)v[8], x2v, a2)));
@@ -829,21 +908,26 @@ __global__ void __launch_bounds__(256) k_amg_sweep3_f32(AmgBsr32 A, const double
     if (i < A.n && l8 < 3) {
       const size_t d = 3 * (size_t)i + l8;
       const double acc = l8 == 0 ? a0 : l8 == 1 ? a1 : a2;
-      const double res = b[d] - acc;
-      xo[d] = RES ? res : fma(w * dinv[d], res, x[d]);
+      const double res = ldv<COH>(&b[d]) - acc;
+      xo[d] = MODE == kSweepResidual ? res : fma(w * __ldg(&dinv[d]), res, xval(d));
     }
   }
 }
 
+template <int MODE>
+__global__ void __launch_bounds__(256, 8) k_amg_sweep3_f32(AmgBsr32 A, const double* __restrict__ dinv,
+                                                        const double* __restrict__ lam, const double* b,
+                                                        const double* x, double* xo) {
+  const double w = MODE == kSweepResidual ? 0.0 : 4.0 / (3.0 * *lam);
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+  sweep3_rows<MODE, false>(A, dinv, w, b, x, xo, warp, nw, threadIdx.x & 31);
+}
+
 // bc_J = sum over the P blocks of column J of P_iJ' r_i, from the FP32 copy of P stored by coarse
 // row (pt32, pt_row): one warp per coarse row, lanes over the row's blocks, fixed shuffle tree.
-template <int B>
-__global__ void __launch_bounds__(256) k_amg_restrict_f32(int nc, const int* __restrict__ pt_ptr,
-                                                          const int* __restrict__ pt_row,
-                                                          const float* __restrict__ pt32,
-                                                          const double* __restrict__ r, double* __restrict__ bc) {
-  const int lane = threadIdx.x & 31;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+template <int B, bool COH>
+__device__ __forceinline__ void restrict_rows(int nc, const int* pt_ptr, const int* pt_row, const float* pt32,
+                                              const double* r, double* bc, int warp, int nw, int lane) {
   for (int J = warp; J < nc; J += nw) {
     double a0 = 0.0, a1 = 0.0, a2 = 0.0;
     const int t1 = __ldg(&pt_ptr[J + 1]);
@@ -855,7 +939,7 @@ __global__ void __launch_bounds__(256) k_amg_restrict_f32(int nc, const int* __r
       for (int e = 0; e < B * 3; ++e) v[e] = __ldg(&pb[e]);
 #pragma unroll
       for (int z = 0; z < B; ++z) {
-        const double rv = r[(size_t)i * B + z];
+        const double rv = ldv<COH>(&r[(size_t)i * B + z]);
         a0 = fma((double)v[z * 3 + 0], rv, a0);
         a1 = fma((double)v[z * 3 + 1], rv, a1);
         a2 = fma((double)v[z * 3 + 2], rv, a2);
@@ -868,20 +952,28 @@ __global__ void __launch_bounds__(256) k_amg_restrict_f32(int nc, const int* __r
   }
 }
 
-// x += P xc with the FP32 copy of P (thread per fine row)
 template <int B>
-__global__ void __launch_bounds__(256) k_amg_prolong_f32(int n, const int* __restrict__ p_ptr,
-                                                         const int* __restrict__ p_col, const float* __restrict__ p32,
-                                                         const double* __restrict__ xc, double* __restrict__ x) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+__global__ void __launch_bounds__(256) k_amg_restrict_f32(int nc, const int* __restrict__ pt_ptr,
+                                                          const int* __restrict__ pt_row,
+                                                          const float* __restrict__ pt32, const double* r,
+                                                          double* bc) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+  restrict_rows<B, false>(nc, pt_ptr, pt_row, pt32, r, bc, warp, nw, threadIdx.x & 31);
+}
+
+// x += P xc with the FP32 copy of P (thread per fine row)
+template <int B, bool COH>
+__device__ __forceinline__ void prolong_rows(int n, const int* p_ptr, const int* p_col, const float* p32,
+                                             const double* xc, double* x, int tid, int nt) {
+  for (int i = tid; i < n; i += nt) {
     double acc[B];
 #pragma unroll
-    for (int r = 0; r < B; ++r) acc[r] = x[(size_t)i * B + r];
+    for (int r = 0; r < B; ++r) acc[r] = ldv<COH>(&x[(size_t)i * B + r]);
     const int q1 = __ldg(&p_ptr[i + 1]);
     for (int q = __ldg(&p_ptr[i]); q < q1; ++q) {
       const float* pb = p32 + (size_t)q * B * 3;
       const double* c = xc + 3 * (size_t)__ldg(&p_col[q]);
-      const double c0 = c[0], c1 = c[1], c2 = c[2];
+      const double c0 = ldv<COH>(&c[0]), c1 = ldv<COH>(&c[1]), c2 = ldv<COH>(&c[2]);
 #pragma unroll
       for (int r = 0; r < B; ++r)
         acc[r] = fma((double)__ldg(&pb[r * 3 + 2]), c2,
@@ -892,8 +984,67 @@ __global__ void __launch_bounds__(256) k_amg_prolong_f32(int n, const int* __res
   }
 }
 
+template <int B>
+__global__ void __launch_bounds__(256) k_amg_prolong_f32(int n, const int* __restrict__ p_ptr,
+                                                         const int* __restrict__ p_col, const float* __restrict__ p32,
+                                                         const double* xc, double* x) {
+  prolong_rows<B, false>(n, p_ptr, p_col, p32, xc, x, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
+
+// x = M b (dense, n x n): one warp per row
+template <bool COH>
+__device__ __forceinline__ void gemv_rows(int n, const double* M, const double* b, double* x, int warp, int nw,
+                                          int lane) {
+  for (int i = warp; i < n; i += nw) {
+    double s = 0.0;
+    for (int j = lane; j < n; j += 32) s = fma(__ldg(&M[(size_t)i * n + j]), ldv<COH>(&b[j]), s);
+    s = warp_sum(s);
+    if (lane == 0) x[i] = s;
+  }
+}
+
+__global__ void k_amg_gemv(int n, const double* __restrict__ M, const double* b, double* x) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+  gemv_rows<false>(n, M, b, x, warp, nw, threadIdx.x & 31);
+}
+
+// The bottom of the V-cycle (the small coarse levels and the dense coarsest solve) in ONE launch
+// of one thread-block cluster: every phase (sweep, residual, restriction, coarsest product,
+// prolongation) is spread over all threads of the cluster and the phases are separated by
+// cluster barriers (release/acquire at cluster scope; vectors written in a phase are read in the
+// next through L2). The same row functions and orders of addition as the per-level launches, so
+// the result is bit-identical to them; only the ~13 launch latencies of these small levels go.
+__global__ void __launch_bounds__(kAmgTailThreads, 1) k_amg_tail(const __grid_constant__ AmgTail T) {
+  const cg::cluster_group cl = cg::this_cluster();
+  const int tid = (int)cl.block_rank() * blockDim.x + threadIdx.x;
+  const int nt = (int)cl.num_blocks() * blockDim.x;
+  const int lane = threadIdx.x & 31, warp = tid >> 5, nw = nt >> 5;
+  for (int l = 0; l + 1 < T.nl; ++l) {
+    const AmgTailLevel& v = T.L[l];
+    const double w = 4.0 / (3.0 * __ldg(v.lam));
+    sweep3_rows<kSweepFirst, true>(v.A, v.dinv, w, v.b, nullptr, v.x, warp, nw, lane);
+    cl.sync();
+    sweep3_rows<kSweepResidual, true>(v.A, v.dinv, 0.0, v.b, v.x, v.r, warp, nw, lane);
+    cl.sync();
+    restrict_rows<3, true>(v.nc, v.pt_ptr, v.pt_row, v.pt32, v.r, T.L[l + 1].b, warp, nw, lane);
+    cl.sync();
+  }
+  gemv_rows<true>(T.n_coarse, T.Minv, T.L[T.nl - 1].b, T.L[T.nl - 1].x, warp, nw, lane);
+  for (int l = T.nl - 2; l >= 0; --l) {
+    const AmgTailLevel& v = T.L[l];
+    const double w = 4.0 / (3.0 * __ldg(v.lam));
+    cl.sync();
+    prolong_rows<3, true>(v.A.n, v.p_ptr, v.p_col, v.p32, T.L[l + 1].x, v.x, tid, nt);
+    cl.sync();
+    sweep3_rows<kSweepSmooth, true>(v.A, v.dinv, w, v.b, v.x, v.xa, warp, nw, lane);
+    cl.sync();
+    sweep3_rows<kSweepSmooth, true>(v.A, v.dinv, w, v.b, v.xa, v.x, warp, nw, lane);
+  }
+}
+
 // FP32 copy of a coarse operator that is exactly symmetric: block (I, J) with J < I is the
-// transpose of the rounded block (J, I) (the FP64 Galerkin product is symmetric only to rounding)
+// transpose of the rounded block (J, I) (the FP64 Galerkin product is symmetric only to rounding).
+// Stored entry-major: entry e of block k at val32[e * nnzb + k].
 __global__ void k_amg_coarse_f32(AmgBsr A, float* __restrict__ val32) {
   const int I = blockIdx.x * blockDim.x + threadIdx.x;
   if (I >= A.n) return;
@@ -909,11 +1060,11 @@ __global__ void k_amg_coarse_f32(AmgBsr A, float* __restrict__ val32) {
       }
     }
     const double* sv = A.val + (size_t)src * 9;
-    float* o = val32 + (size_t)k * 9;
+    const size_t nb = (size_t)A.ptr[A.n];
 #pragma unroll
     for (int r = 0; r < 3; ++r)
 #pragma unroll
-      for (int c = 0; c < 3; ++c) o[r * 3 + c] = (float)(tr ? sv[c * 3 + r] : sv[r * 3 + c]);
+      for (int c = 0; c < 3; ++c) val32[(size_t)(r * 3 + c) * nb + k] = (float)(tr ? sv[c * 3 + r] : sv[r * 3 + c]);
   }
 }
 
@@ -931,17 +1082,6 @@ __global__ void k_amg_transfer_f32(int nnz_p, const double* __restrict__ pval, c
   for (int v = 0; v < B * 3; ++v) {
     p32[(size_t)t * B * 3 + v] = (float)pval[(size_t)t * B * 3 + v];
     pt32[(size_t)t * B * 3 + v] = (float)pval[(size_t)q * B * 3 + v];
-  }
-}
-
-// x = M b (dense, n x n): one warp per row
-__global__ void k_amg_gemv(int n, const double* __restrict__ M, const double* __restrict__ b, double* __restrict__ x) {
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  for (int i = warp; i < n; i += (gridDim.x * blockDim.x) >> 5) {
-    double s = 0.0;
-    for (int j = lane; j < n; j += 32) s = fma(M[(size_t)i * n + j], b[j], s);
-    s = warp_sum(s);
-    if (lane == 0) x[i] = s;
   }
 }
 
@@ -1048,19 +1188,21 @@ cudaError_t amg_tentative(int B, int n_agg, const int* agg_ptr, const int* membe
 cudaError_t amg_lambda(int B, const AmgBsr& A, const double* dinv, double* x, double* y, double* part, double* lam,
                        int iters, cudaStream_t s) {
   const int n = A.n * B;
-  const int G = 148;
+  double* sc = part + kLamGrid;  // the scale of the next step
   k_amg_init_vec<<<gw(n), 256, 0, s>>>(n, x);
   for (int t = 0; t < iters; ++t) {
     if (B == 2)
-      k_amg_dinva<2><<<G, kThreads, 0, s>>>(A.n, A, dinv, x, y, part);
+      k_amg_dinva<2><<<kLamGrid, kThreads, 0, s>>>(A.n, A, dinv, t ? sc : nullptr, x, y, part);
     else
-      k_amg_dinva<3><<<G, kThreads, 0, s>>>(A.n, A, dinv, x, y, part);
-    k_amg_scale<<<gw(n), 256, 0, s>>>(n, part, G, y, lam);
+      k_amg_dinva<3><<<kLamGrid, kThreads, 0, s>>>(A.n, A, dinv, t ? sc : nullptr, x, y, part);
+    k_amg_norm<<<1, kThreads, 0, s>>>(part, kLamGrid, lam, sc);
     std::swap(x, y);
   }
   count_launches(1 + 2LL * iters);
   return cudaGetLastError();
 }
+
+size_t amg_lambda_scratch() { return sizeof(double) * (kLamGrid + 8); }
 
 cudaError_t amg_p_count(int B, const AmgBsr& A, const int* agg, int* cnt, int* err, cudaStream_t s) {
   if (B == 2)
@@ -1073,11 +1215,15 @@ cudaError_t amg_p_count(int B, const AmgBsr& A, const int* agg, int* cnt, int* e
 
 cudaError_t amg_p_fill(int B, const AmgBsr& A, const int* agg, const double* P0, const double* dinv, const double* lam,
                        const AmgBsr& P, cudaStream_t s) {
-  if (B == 2)
-    k_amg_p_fill<2><<<g1(A.n, 128), 128, 0, s>>>(A.n, A, agg, P0, dinv, lam, P);
-  else
-    k_amg_p_fill<3><<<g1(A.n, 128), 128, 0, s>>>(A.n, A, agg, P0, dinv, lam, P);
-  count_launches(1);
+  const int gv = (int)std::max<long long>(1, std::min<long long>(((long long)A.n + kGalWarps - 1) / kGalWarps, 148LL * 16));
+  if (B == 2) {
+    k_amg_p_cols<2><<<g1(A.n, 128), 128, 0, s>>>(A.n, A, agg, P);
+    k_amg_p_vals<2><<<gv, 32 * kGalWarps, 0, s>>>(A.n, A, agg, P0, dinv, lam, P);
+  } else {
+    k_amg_p_cols<3><<<g1(A.n, 128), 128, 0, s>>>(A.n, A, agg, P);
+    k_amg_p_vals<3><<<gv, 32 * kGalWarps, 0, s>>>(A.n, A, agg, P0, dinv, lam, P);
+  }
+  count_launches(2);
   return cudaGetLastError();
 }
 
@@ -1151,31 +1297,27 @@ cudaError_t amg_coarsest(int B, const AmgBsr& A, double* M, double* piv, cudaStr
   return cudaGetLastError();
 }
 
-cudaError_t amg_smooth0(int B, int n, const double* dinv, const double* lam, const double* b, double* x, cudaStream_t s) {
-  if (B == 2)
-    k_amg_smooth0<2><<<gw((long long)n * B), 256, 0, s>>>(n, dinv, lam, b, x);
-  else
-    k_amg_smooth0<3><<<gw((long long)n * B), 256, 0, s>>>(n, dinv, lam, b, x);
-  count_launches(1);
-  return cudaGetLastError();
-}
-
-cudaError_t amg_sweep_f32(bool residual, const MixedMatrix& M, const double* dinv, const double* lam, const double* b,
+cudaError_t amg_sweep_f32(int mode, const MixedMatrix& M, const double* dinv, const double* lam, const double* b,
                           const double* x, double* xo, cudaStream_t s) {
-  if (residual)
-    k_amg_sweep_f32<true><<<gw(M.n_nodes), 256, 0, s>>>(M, dinv, lam, b, x, xo);
+  if (mode == kSweepResidual)
+    k_amg_sweep_f32<kSweepResidual><<<gw(M.n_nodes), 256, 0, s>>>(M, dinv, lam, b, x, xo);
+  else if (mode == kSweepFirst)
+    k_amg_sweep_f32<kSweepFirst><<<gw(M.n_nodes), 256, 0, s>>>(M, dinv, lam, b, x, xo);
   else
-    k_amg_sweep_f32<false><<<gw(M.n_nodes), 256, 0, s>>>(M, dinv, lam, b, x, xo);
+    k_amg_sweep_f32<kSweepSmooth><<<gw(M.n_nodes), 256, 0, s>>>(M, dinv, lam, b, x, xo);
   count_launches(1);
   return cudaGetLastError();
 }
 
-cudaError_t amg_sweep3_f32(bool residual, const AmgBsr32& A, const double* dinv, const double* lam, const double* b,
+cudaError_t amg_sweep3_f32(int mode, const AmgBsr32& A, const double* dinv, const double* lam, const double* b,
                            const double* x, double* xo, cudaStream_t s) {
-  if (residual)
-    k_amg_sweep3_f32<true><<<gw((long long)A.n * 8), 256, 0, s>>>(A, dinv, lam, b, x, xo);
+  const int g = gw((long long)A.n * 8);
+  if (mode == kSweepResidual)
+    k_amg_sweep3_f32<kSweepResidual><<<g, 256, 0, s>>>(A, dinv, lam, b, x, xo);
+  else if (mode == kSweepFirst)
+    k_amg_sweep3_f32<kSweepFirst><<<g, 256, 0, s>>>(A, dinv, lam, b, x, xo);
   else
-    k_amg_sweep3_f32<false><<<gw((long long)A.n * 8), 256, 0, s>>>(A, dinv, lam, b, x, xo);
+    k_amg_sweep3_f32<kSweepSmooth><<<g, 256, 0, s>>>(A, dinv, lam, b, x, xo);
   count_launches(1);
   return cudaGetLastError();
 }
@@ -1215,6 +1357,33 @@ cudaError_t amg_transfer_f32(int B, const AmgBsr& P, int nnz_p, const int* pt_id
     k_amg_transfer_f32<3><<<g1(nnz_p), 256, 0, s>>>(nnz_p, P.val, pt_idx, p_row, p32, pt_row, pt32);
   count_launches(1);
   return cudaGetLastError();
+}
+
+cudaError_t amg_tail(const AmgTail& t, int cluster, int* max_clusters, cudaStream_t s) {
+  if (cluster < 1 || cluster > 16) return cudaErrorInvalidValue;
+  if (cluster > 8 && max_clusters) {  // the shape query precedes any launch (never in a capture)
+    const cudaError_t e = cudaFuncSetAttribute(k_amg_tail, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (e != cudaSuccess) return e;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = (unsigned)cluster;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.gridDim = dim3((unsigned)cluster);
+  cfg.blockDim = dim3(kAmgTailThreads);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  if (max_clusters) {
+    *max_clusters = 0;
+    return cudaOccupancyMaxActiveClusters(max_clusters, (void*)k_amg_tail, &cfg);
+  }
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, k_amg_tail, t);
+  count_launches(1);
+  return e;
 }
 
 cudaError_t amg_rigid_modes(int N, const double* xy, double* Bf, cudaStream_t s) {

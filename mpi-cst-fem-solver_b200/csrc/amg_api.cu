@@ -14,6 +14,9 @@ constexpr int kCoarsestDofs = 600;  // dense inverse at or below this many coars
 constexpr int kMaxLevels = 10;
 constexpr int kPowerIters = 20;
 constexpr int kMaxMisRounds = 200;
+// coarse levels at or below this many DOFs run in the tail kernel: one cluster of at most 16 SMs
+// beats separate full-GPU launches only where a level's work is a few microseconds of latency
+constexpr int kTailMaxDofs = 5000;
 
 }  // namespace
 
@@ -29,6 +32,7 @@ struct AmgLevel {
   // level, by fine row (p32) and by coarse row (pt32 with the fine row of each block in pt_row)
   DevBuf val32, p32, pt32, pt_row;
   int nnz_p = 0;
+  int nnzb = 0;  // blocks of this level's matrix
   AmgBsr A() const {
     AmgBsr m;
     m.n = n;
@@ -40,6 +44,7 @@ struct AmgLevel {
   AmgBsr32 A32() const {
     AmgBsr32 m;
     m.n = n;
+    m.nnzb = nnzb;
     m.ptr = a_ptr;
     m.col = a_col;
     m.val = static_cast<const float*>(val32.p);
@@ -62,6 +67,11 @@ struct AmgData {
   int n_coarse = 0;           // DOFs of the dense coarsest level
   unsigned long long built_for = ~0ull;  // setup_count of the matrix it was built from
   double setup_seconds = 0.0;
+  // the bottom of the cycle in one cluster launch (tail_level 0: every level launches its own kernels)
+  bool tail_enabled = true;
+  int tail_cluster = -1;  // CTAs of the tail cluster on this device (-1 not yet queried, 0 none fits)
+  int tail_level = 0;
+  AmgTail tail;
   // scratch of the setup
   DevBuf state, m1, newroot, near, und, root_id, flags, agg1, agg2, agg_ptr, members, cnt, cur, P0, Bf, Bc, cnt2,
       ap_ptr, ap_col, ap_val, part, vx, vy;
@@ -116,7 +126,7 @@ int coarsen(cstg_ctx* ctx, AmgData* d, int l, bool* stop) {
   ENSURE(d->members, sizeof(int) * (size_t)n);
   // lambda_max(D^-1 A)
   ENSURE(lv.lam, sizeof(double));
-  ENSURE(d->part, sizeof(double) * 256);
+  ENSURE(d->part, amg_lambda_scratch());
   ENSURE(d->vx, sizeof(double) * (size_t)n * B);
   ENSURE(d->vy, sizeof(double) * (size_t)n * B);
   CK(amg_lambda(B, A, buf_ptr<double>(lv.dinv), buf_ptr<double>(d->vx), buf_ptr<double>(d->vy),
@@ -225,10 +235,60 @@ int coarsen(cstg_ctx* ctx, AmgData* d, int l, bool* stop) {
   CK(amg_ac_fill(B, nc, buf_ptr<int>(cur.pt_ptr), buf_ptr<int>(cur.pt_idx), buf_ptr<int>(cur.p_row), cur.P(), AP, Ac,
                  ctx->stream));
   ENSURE(nx.val32, sizeof(float) * (size_t)std::max(nnz_c, 1) * 9);
+  nx.nnzb = nnz_c;
   CK(amg_coarse_f32(Ac, buf_ptr<float>(nx.val32), ctx->stream));
   // the coarse nullspace becomes the next level's basis
   ENSURE(d->Bf, sizeof(double) * (size_t)std::max(n * B * 3, nc * 9));
   CK(cudaMemcpyAsync(d->Bf.p, d->Bc.p, sizeof(double) * (size_t)nc * 9, cudaMemcpyDeviceToDevice, ctx->stream));
+  return CSTG_OK;
+}
+
+// Maps the levels from the first level >= 1 with at most kTailMaxDofs DOFs down to the coarsest
+// onto one cluster launch (k_amg_tail), when a cluster of 16 (else 8) CTAs fits on the device.
+int setup_tail(cstg_ctx* ctx, AmgData* d) {
+  d->tail_level = 0;
+  if (!d->tail_enabled || d->nl < 3) return CSTG_OK;
+  if (d->tail_cluster < 0) {
+    d->tail_cluster = 0;
+    for (int c : {16, 8}) {
+      int m = 0;
+      const cudaError_t e = amg_tail(d->tail, c, &m, ctx->stream);
+      if (e == cudaSuccess && m >= 1) {
+        d->tail_cluster = c;
+        break;
+      }
+      cudaGetLastError();  // a shape that cannot launch is not an error of the setup
+    }
+  }
+  if (!d->tail_cluster) return CSTG_OK;
+  int lt = 1;
+  while (lt < d->nl - 1 && d->L[lt].n * d->L[lt].B > kTailMaxDofs) ++lt;
+  if (lt >= d->nl - 1 || d->nl - lt > kAmgTailMax) return CSTG_OK;
+  AmgTail& T = d->tail;
+  T = AmgTail{};
+  T.nl = d->nl - lt;
+  T.n_coarse = d->n_coarse;
+  T.Minv = buf_ptr<double>(d->Minv);
+  for (int t = 0; t < T.nl; ++t) {
+    AmgLevel& lv = d->L[lt + t];
+    AmgTailLevel& v = T.L[t];
+    v.b = buf_ptr<double>(lv.bc);
+    v.x = buf_ptr<double>(lv.xb);
+    if (t + 1 == T.nl) break;
+    v.A = lv.A32();
+    v.dinv = buf_ptr<double>(lv.dinv);
+    v.lam = buf_ptr<double>(lv.lam);
+    v.xa = buf_ptr<double>(lv.xa);
+    v.r = buf_ptr<double>(lv.r);
+    v.nc = lv.nc;
+    v.pt_ptr = buf_ptr<int>(lv.pt_ptr);
+    v.pt_row = buf_ptr<int>(lv.pt_row);
+    v.pt32 = buf_ptr<float>(lv.pt32);
+    v.p_ptr = buf_ptr<int>(lv.p_ptr);
+    v.p_col = buf_ptr<int>(lv.p_col);
+    v.p32 = buf_ptr<float>(lv.p32);
+  }
+  d->tail_level = lt;
   return CSTG_OK;
 }
 
@@ -284,6 +344,8 @@ int amg_build(cstg_ctx* ctx) {
     ENSURE(lv.r, sizeof(double) * m);
     ENSURE(lv.bc, sizeof(double) * m);
   }
+  const int rt = setup_tail(ctx, d);
+  if (rt) return rt;
   CK(cudaStreamSynchronize(ctx->stream));
   d->built_for = ctx->setup_count;
   d->setup_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -298,6 +360,10 @@ int vcycle(cstg_ctx* ctx, AmgData* d, size_t l, const double* b, double* x) {
     CK(amg_gemv(d->n_coarse, buf_ptr<double>(d->Minv), b, x, s));
     return CSTG_OK;
   }
+  if (d->tail_level > 0 && (int)l == d->tail_level && b == d->tail.L[0].b && x == d->tail.L[0].x) {
+    CK(amg_tail(d->tail, d->tail_cluster, nullptr, s));
+    return CSTG_OK;
+  }
   const double* dinv = buf_ptr<double>(lv.dinv);
   const double* lam = buf_ptr<double>(lv.lam);
   double* xa = buf_ptr<double>(lv.xa);
@@ -309,20 +375,19 @@ int vcycle(cstg_ctx* ctx, AmgData* d, size_t l, const double* b, double* x) {
   const bool fine = l == 0;
   const MixedMatrix mm = fine ? mixed_view(ctx) : MixedMatrix{};
   const AmgBsr32 A32 = lv.A32();
-  auto sweep = [&](bool res, const double* xin, double* xout) -> cudaError_t {
-    return fine ? amg_sweep_f32(res, mm, dinv, lam, b, xin, xout, s) : amg_sweep3_f32(res, A32, dinv, lam, b, xin, xout, s);
+  auto sweep = [&](int mode, const double* xin, double* xout) -> cudaError_t {
+    return fine ? amg_sweep_f32(mode, mm, dinv, lam, b, xin, xout, s) : amg_sweep3_f32(mode, A32, dinv, lam, b, xin, xout, s);
   };
-  CK(amg_smooth0(lv.B, lv.n, dinv, lam, b, xa, s));
-  CK(sweep(false, xa, x));
-  CK(sweep(true, x, r));
+  CK(sweep(kSweepFirst, nullptr, x));  // two pre-smoothing steps from x = 0
+  CK(sweep(kSweepResidual, x, r));
   CK(amg_restrict_f32(lv.B, lv.nc, buf_ptr<int>(lv.pt_ptr), buf_ptr<int>(lv.pt_row), buf_ptr<float>(lv.pt32), r,
                       buf_ptr<double>(nx.bc), s));
   const int rc = vcycle(ctx, d, l + 1, buf_ptr<double>(nx.bc), buf_ptr<double>(nx.xb));
   if (rc) return rc;
   CK(amg_prolong_f32(lv.B, lv.n, buf_ptr<int>(lv.p_ptr), buf_ptr<int>(lv.p_col), buf_ptr<float>(lv.p32),
                      buf_ptr<double>(nx.xb), x, s));
-  CK(sweep(false, x, xa));
-  CK(sweep(false, xa, x));
+  CK(sweep(kSweepSmooth, x, xa));
+  CK(sweep(kSweepSmooth, xa, x));
   return CSTG_OK;
 }
 
@@ -349,6 +414,8 @@ unsigned long long cstg_host::amg_signature(const cstg_ctx* ctx) {
   if (!d) return h;
   mix((unsigned long long)d->nl);
   mix((unsigned long long)d->n_coarse);
+  mix((unsigned long long)d->tail_level);
+  mix((unsigned long long)d->tail_cluster);
   for (int l = 0; l < d->nl; ++l) {
     mix((unsigned long long)d->L[l].B);
     mix((unsigned long long)d->L[l].n);
@@ -380,7 +447,20 @@ int cstg_amg_setup(cstg_ctx* ctx, cstg_amg_info* info) {
       info->nnz[l] = (long long)nnzb * lv.B * lv.B;
     }
     info->setup_seconds = d->setup_seconds;
+    info->tail_level = d->tail_level;
+    info->tail_cluster = d->tail_level > 0 ? d->tail_cluster : 0;
   }
+  return CSTG_OK;
+}
+
+int cstg_amg_set_tail(cstg_ctx* ctx, int enable) {
+  BEGIN(ctx);
+  if (!ctx->amg) {
+    ctx->amg = new AmgData();
+    ctx->amg->L.reserve(kMaxLevels + 1);
+  }
+  ctx->amg->tail_enabled = enable != 0;
+  if (ctx->amg->nl > 0) return setup_tail(ctx, ctx->amg);
   return CSTG_OK;
 }
 
@@ -402,7 +482,7 @@ int cstg_amg_time(cstg_ctx* ctx, int reps, double* out) {
   for (int w = 0; w < 2; ++w) {  // warm-up, then timed
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
     for (int k = 0; k < reps; ++k)
-      CK(amg_sweep_f32(false, mm, buf_ptr<double>(f.dinv), buf_ptr<double>(f.lam), b, k & 1 ? xb : xa, k & 1 ? xa : xb,
+      CK(amg_sweep_f32(kSweepSmooth, mm, buf_ptr<double>(f.dinv), buf_ptr<double>(f.lam), b, k & 1 ? xb : xa, k & 1 ? xa : xb,
                        ctx->stream));
     CK(cudaEventRecord(ctx->ev1, ctx->stream));
   }

@@ -241,8 +241,9 @@ struct AmgBsr {  // n block rows, ptr[n + 1], col[ptr[n]], val: B x B (or B x 3 
   const int* col = nullptr;
   const double* val = nullptr;
 };
-struct AmgBsr32 {  // a coarse operator's FP32 copy (3 x 3 blocks), same pattern
+struct AmgBsr32 {  // a coarse operator's FP32 copy (3 x 3 blocks), same pattern, entry-major values
   int n = 0;
+  int nnzb = 0;  // blocks: entry e of block k at val[e * nnzb + k]
   const int* ptr = nullptr;
   const int* col = nullptr;
   const float* val = nullptr;
@@ -262,6 +263,7 @@ cudaError_t amg_tentative(int B, int n_agg, const int* agg_ptr, const int* membe
                           double* Bc, int* err, cudaStream_t s);
 cudaError_t amg_lambda(int B, const AmgBsr& A, const double* dinv, double* x, double* y, double* part, double* lam,
                        int iters, cudaStream_t s);
+size_t amg_lambda_scratch();  // bytes of `part` that amg_lambda needs
 cudaError_t amg_p_count(int B, const AmgBsr& A, const int* agg, int* cnt, int* err, cudaStream_t s);
 cudaError_t amg_p_fill(int B, const AmgBsr& A, const int* agg, const double* P0, const double* dinv, const double* lam,
                        const AmgBsr& P, cudaStream_t s);
@@ -274,20 +276,51 @@ cudaError_t amg_ac_count(int B, int nc, const int* pt_ptr, const int* pt_idx, co
 cudaError_t amg_ac_fill(int B, int nc, const int* pt_ptr, const int* pt_idx, const int* p_row, const AmgBsr& P,
                         const AmgBsr& AP, const AmgBsr& Ac, cudaStream_t s);
 cudaError_t amg_coarsest(int B, const AmgBsr& A, double* M, double* piv, cudaStream_t s);
-cudaError_t amg_smooth0(int B, int n, const double* dinv, const double* lam, const double* b, double* x, cudaStream_t s);
-cudaError_t amg_sweep_f32(bool residual, const MixedMatrix& M, const double* dinv, const double* lam, const double* b,
+// smoother sweep modes: x + w D^-1 (b - A x); b - A x; the first sweep from x = 0 (x not read)
+constexpr int kSweepSmooth = 0, kSweepResidual = 1, kSweepFirst = 2;
+cudaError_t amg_sweep_f32(int mode, const MixedMatrix& M, const double* dinv, const double* lam, const double* b,
                           const double* x, double* xo, cudaStream_t s);
 // cycle operators in FP32 (values only; vectors and accumulation stay FP64)
 cudaError_t amg_coarse_f32(const AmgBsr& A, float* val32, cudaStream_t s);
 cudaError_t amg_transfer_f32(int B, const AmgBsr& P, int nnz_p, const int* pt_idx, const int* p_row, float* p32,
                              int* pt_row, float* pt32, cudaStream_t s);
-cudaError_t amg_sweep3_f32(bool residual, const AmgBsr32& A, const double* dinv, const double* lam, const double* b,
+cudaError_t amg_sweep3_f32(int mode, const AmgBsr32& A, const double* dinv, const double* lam, const double* b,
                            const double* x, double* xo, cudaStream_t s);
 cudaError_t amg_restrict_f32(int B, int nc, const int* pt_ptr, const int* pt_row, const float* pt32, const double* r,
                              double* bc, cudaStream_t s);
 cudaError_t amg_prolong_f32(int B, int n, const int* p_ptr, const int* p_col, const float* p32, const double* xc,
                             double* x, cudaStream_t s);
 cudaError_t amg_gemv(int n, const double* M, const double* b, double* x, cudaStream_t s);
+
+// The bottom of the V-cycle in one thread-block cluster (levels >= 1 with 3 x 3 blocks, then the
+// dense coarsest solve): level 0 of the tail takes b and writes x like the per-level path.
+constexpr int kAmgTailMax = 8;         // levels in a tail, the coarsest included
+constexpr int kAmgTailThreads = 512;   // threads per CTA of the tail cluster
+struct AmgTailLevel {
+  AmgBsr32 A;
+  const double* dinv = nullptr;
+  const double* lam = nullptr;
+  double* b = nullptr;   // right-hand side (level 0: the caller's; below: the restriction)
+  double* x = nullptr;   // the level's result
+  double* xa = nullptr;  // sweep scratch
+  double* r = nullptr;   // residual
+  int nc = 0;            // transfer to the next level
+  const int* pt_ptr = nullptr;
+  const int* pt_row = nullptr;
+  const float* pt32 = nullptr;
+  const int* p_ptr = nullptr;
+  const int* p_col = nullptr;
+  const float* p32 = nullptr;
+};
+struct AmgTail {
+  int nl = 0;  // levels, the last one the dense coarsest (only its b and x are used)
+  int n_coarse = 0;
+  const double* Minv = nullptr;
+  AmgTailLevel L[kAmgTailMax];
+};
+// cluster: CTAs in the one cluster (1..16); max_clusters != nullptr: only query how many such
+// clusters fit at once (0 = the shape cannot launch), nothing is launched
+cudaError_t amg_tail(const AmgTail& t, int cluster, int* max_clusters, cudaStream_t s);
 cudaError_t amg_rigid_modes(int N, const double* xy, double* Bf, cudaStream_t s);
 
 // Process-wide count of kernel launches issued by this library (graph launches count every

@@ -75,7 +75,7 @@ class Stats(C.Structure):
 class AmgInfo(C.Structure):
     """cstg_amg_info: the multigrid hierarchy."""
     _fields_ = [("levels", C.c_int), ("dofs", C.c_int * 16), ("nnz", C.c_longlong * 16),
-                ("setup_seconds", C.c_double)]
+                ("setup_seconds", C.c_double), ("tail_level", C.c_int), ("tail_cluster", C.c_int)]
 
 
 class BatchConfig(C.Structure):
@@ -139,6 +139,7 @@ _SIGS = {
     "cstg_amg_setup": (C.c_int, [_vp, C.POINTER(AmgInfo)]),
     "cstg_amg_apply_device": (C.c_int, [_vp, _vp, _vp]),
     "cstg_amg_time": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_double)]),
+    "cstg_amg_set_tail": (C.c_int, [_vp, C.c_int]),
     "cstg_mpnn_param_count": (C.c_longlong, []),
     "cstg_learned_setup": (C.c_int, [_vp, _vp, _vp]),
     "cstg_learned_set_params": (C.c_int, [_vp, _vp]),

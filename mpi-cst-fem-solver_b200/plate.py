@@ -27,19 +27,24 @@ import math
 import numpy as np
 
 
+def _count(a) -> int:
+    return int(a.numel()) if hasattr(a, "numel") else int(a.size)
+
+
 @dataclasses.dataclass
 class Mesh:
     xy: np.ndarray  # float64 [2 * n_nodes]
     triangles: np.ndarray  # int32 [3 * n_tri]
     boundary_edges: dict  # name -> int32 [n_edges, 2]
 
+    # (numpy arrays or CUDA tensors: both have numel via .size / .numel())
     @property
     def num_nodes(self) -> int:
-        return self.xy.size // 2
+        return _count(self.xy) // 2
 
     @property
     def num_triangles(self) -> int:
-        return self.triangles.size // 3
+        return _count(self.triangles) // 3
 
     @property
     def num_dofs(self) -> int:

@@ -418,7 +418,12 @@ def amg_setup(K: GpuCsrMatrix) -> dict:
     info = native.AmgInfo()
     K.ctx.check(K.ctx.L.cstg_amg_setup(K.ctx.h, C.byref(info)))
     return {"levels": info.levels, "dofs": list(info.dofs[:info.levels]), "nnz": list(info.nnz[:info.levels]),
-            "setup_seconds": info.setup_seconds}
+            "setup_seconds": info.setup_seconds, "tail_level": info.tail_level, "tail_cluster": info.tail_cluster}
+
+
+def amg_set_tail(K: GpuCsrMatrix, enable: bool) -> None:
+    """Runs the small coarse levels as one cluster launch (True, the default) or level by level."""
+    K.ctx.check(K.ctx.L.cstg_amg_set_tail(K.ctx.h, int(bool(enable))))
 
 
 def amg_apply(K: GpuCsrMatrix, r, z=None):

@@ -103,3 +103,30 @@ def test_amg_mixed_larger_plate(pkg, gpu_lib):
     assert _rel(x, x_ref) < REL_TOL
     assert st.iterations * 20 < st_ref.iterations, (st.iterations, st_ref.iterations)
     K.ctx.close()
+
+
+def test_amg_cluster_tail_matches_per_level_cycle(pkg, gpu_lib):
+    """The one-cluster launch of the small coarse levels gives the bits of the per-level
+    launches, and solves agree bit for bit either way."""
+    import torch
+    m, K, b = _plate(pkg, 200, 400)  # 161k DOFs: a level of ~1.4k DOFs above the dense coarsest
+    s = pkg.CgJacobiSolver(_amg())
+    s.setup(K)
+    info = pkg.amg_setup(K)
+    assert info["levels"] >= 3 and info["tail_level"] >= 1 and info["tail_cluster"] in (8, 16), info
+    r = torch.from_numpy(np.random.default_rng(3).standard_normal(m.num_dofs)).cuda()
+    z_tail = pkg.amg_apply(K, r)
+    x_tail = np.zeros(m.num_dofs)
+    st_tail = s.solve(b, x_tail)
+    pkg.amg_set_tail(K, False)
+    assert pkg.amg_setup(K)["tail_level"] == 0
+    z_lvl = pkg.amg_apply(K, r)
+    x_lvl = np.zeros(m.num_dofs)
+    st_lvl = s.solve(b, x_lvl)
+    assert torch.equal(z_tail, z_lvl)
+    assert np.array_equal(x_tail, x_lvl) and st_tail.iterations == st_lvl.iterations
+    assert st_tail.converged and st_tail.true_rel_residual <= 1e-10
+    pkg.amg_set_tail(K, True)
+    assert pkg.amg_setup(K)["tail_level"] == info["tail_level"]
+    assert torch.equal(pkg.amg_apply(K, r), z_tail)
+    K.ctx.close()
