@@ -65,6 +65,8 @@ def parse():
     ap.add_argument("--precond", default="amg", choices=["amg", "jacobi", "learned"],
                     help="preconditioner of the timed solve: smoothed-aggregation multigrid (default), "
                          "Jacobi (the reference's method, persistent kernel) or the learned network")
+    ap.add_argument("--amg-smoother", default="chebyshev", choices=["chebyshev", "jacobi"],
+                    help="smoother of the multigrid cycle")
     ap.add_argument("--precision", default=None, choices=["fp64", "mixed"],
                     help="outer CG precision; default fp64 with amg (its finest smoother is FP32 already), "
                          "mixed otherwise")
@@ -374,6 +376,8 @@ def run_ours(a, dist: Dist):
     stream = torch.cuda.Stream(device=dev)
     ctx = pkg.Context(dev)
     ctx.set_stream(stream)
+    smoother_code = {"chebyshev": pkg.native.AMG_CHEBYSHEV, "jacobi": pkg.native.AMG_JACOBI}[a.amg_smoother]
+    ctx.check(ctx.L.cstg_amg_set_smoother(ctx.h, smoother_code))
     # loads on the host (bc.cpp:190-253) once; the step starts from them
     ctx.set_mesh(mesh)
     b0 = np.zeros(n)
@@ -614,7 +618,8 @@ def run_ours(a, dist: Dist):
         sweep_bytes = spmv32_bytes + 2 * n * 8
         amg = {"levels": info["levels"], "level_dofs": info["dofs"], "level_nnz": info["nnz"],
                "setup_s": info["setup_seconds"], "vcycle_us": tm["vcycle_s"] * 1e6,
-               "cycle": "V(2,2), damped Jacobi, FP32 finest-level operator, dense coarsest inverse",
+               "cycle": f"V(2,2), {a.amg_smoother} smoothing, FP32 cycle operators, dense coarsest inverse",
+               "tail": {"level": info["tail_level"], "cluster_ctas": info["tail_cluster"]},
                "smoother_roofline": roof("k_amg_sweep_f32 (finest-level damped Jacobi sweep)", sweep_bytes,
                                          tm["sweep_s"],
                                          profile_traffic("amg_sweep_f32_plate2m.md") if full else None)}
@@ -678,6 +683,7 @@ def run_ours(a, dist: Dist):
         h_b = pinned(b0)
         h_x = pinned(np.zeros(n))
         ectx = pkg.Context(dev)
+        ectx.check(ectx.L.cstg_amg_set_smoother(ectx.h, smoother_code))
 
         def e2e_step():
             K2 = pkg.build_stiffness_pattern(hmesh, ctx=ectx)

@@ -346,8 +346,8 @@ int cstg_mesh_group(const cstg_mesh* mesh, int index, char* name, int name_len, 
  * No counterpart in the reference. Smoothed aggregation on the GPU: distance-2 MIS aggregates of
  * the node graph, tentative prolongator from the 2D rigid-body modes (per-aggregate QR), one
  * damped-Jacobi prolongator smoothing step, Galerkin coarse operators (3 x 3 blocks), dense
- * inverse of the coarsest level; the preconditioner is one V(2,2) cycle with damped Jacobi
- * (weight 4 / (3 lambda_max(D^-1 A)), lambda_max by power iteration). Deterministic. Used by
+ * inverse of the coarsest level; the preconditioner is one V(2,2) cycle with Chebyshev smoothing
+ * (or damped Jacobi, cstg_amg_set_smoother; lambda_max(D^-1 A) by power iteration). Deterministic. Used by
  * cstg_pcg_solve with opt->preconditioner = CSTG_PRECOND_AMG (flexible CG driver, FP64 true-
  * residual check as for the other preconditioners). Mesh-pattern matrices only. */
 typedef struct {
@@ -368,6 +368,12 @@ int cstg_amg_time(cstg_ctx* ctx, int reps, double* out);
  * cluster barriers between phases (default), or as one launch per level and phase (enable = 0).
  * Both give the same bits. */
 int cstg_amg_set_tail(cstg_ctx* ctx, int enable);
+/* Smoother of the cycle: Chebyshev polynomial of degree 2 on [1.1 lambda / 20, 1.1 lambda] of
+ * D^-1 A (default) or damped Jacobi with weight 4 / (3 lambda); two pre- and two post-smoothing
+ * steps either way (the same number of operator applications). */
+#define CSTG_AMG_CHEBYSHEV 0
+#define CSTG_AMG_JACOBI 1
+int cstg_amg_set_smoother(cstg_ctx* ctx, int kind);
 
 #ifdef __cplusplus
 }

@@ -787,14 +787,63 @@ __global__ void __launch_bounds__(1024) k_amg_gauss_jordan(int n, double* __rest
 
 // ---- cycle kernels ----------------------------------------------------------------------------------
 
-// Sweep modes. kSweepSmooth: xo = x + w D^-1 (b - A x); kSweepResidual: xo = b - A x;
-// kSweepFirst: the first sweep from x = 0, whose input x0 = w D^-1 b is formed on the fly from b
-// and D^-1 (the same rounding as storing it first), so x is not read.
+// Smoother steps. With r(x) = D^-1 (b - A x):
+//   kSweepFirst     xo = beta x0 + gamma r(x0), x0 = a0 D^-1 b formed on the fly (x not read)
+//   kSweepSmooth    xo = x + gamma r(x)
+//   kSweepSecond    xo = x + cd (x - xp) + gamma r(x)   (xp: the iterate before x)
+//   kSweepResidual  xo = b - A x
+// Damped Jacobi (weight w = 4 / (3 lam)): a0 = gamma = w, beta = 1, every post step kSweepSmooth.
+// Chebyshev of degree 2 on [hi / kChebRatio, hi], hi = kChebHi lam (the three-term recurrence:
+// theta = (hi + lo) / 2, delta = (hi - lo) / 2, sigma = theta / delta, rho1 = 1 / sigma,
+// rho2 = 1 / (2 sigma - rho1)): the two pre-smoothing steps from x = 0 are one kSweepFirst with
+// a0 = 1 / theta, beta = 1 + rho2 rho1, gamma = 2 rho2 / delta; the two post-smoothing steps are
+// kSweepSmooth with gamma = 1 / theta, then kSweepSecond with cd = rho2 rho1, gamma = 2 rho2 / delta.
+constexpr double kChebHi = 1.1, kChebRatio = 20.0;
 
-// x0 = w D^-1 b, component i (the first sweep's input)
-__device__ __forceinline__ double first_x(double w, const double* __restrict__ dinv, const double* __restrict__ b,
+struct SweepCoef {
+  double a0, beta, gamma, cd;
+};
+
+template <int MODE>
+__device__ __forceinline__ SweepCoef sweep_coef(const double* lam, int cheb) {
+  SweepCoef c{0.0, 1.0, 0.0, 0.0};
+  if (MODE == kSweepResidual) return c;
+  const double l = *lam;
+  if (!cheb) {
+    const double w = 4.0 / (3.0 * l);
+    c.a0 = w;
+    c.gamma = w;
+    return c;
+  }
+  const double hi = kChebHi * l, lo = hi / kChebRatio;
+  const double theta = 0.5 * (hi + lo), delta = 0.5 * (hi - lo), sigma = theta / delta;
+  const double rho1 = 1.0 / sigma, rho2 = 1.0 / (2.0 * sigma - rho1);
+  if (MODE == kSweepFirst) {
+    c.a0 = 1.0 / theta;
+    c.beta = 1.0 + rho2 * rho1;
+    c.gamma = 2.0 * rho2 / delta;
+  } else if (MODE == kSweepSmooth) {
+    c.gamma = 1.0 / theta;
+  } else {
+    c.cd = rho2 * rho1;
+    c.gamma = 2.0 * rho2 / delta;
+  }
+  return c;
+}
+
+// the update of component i given its current value xi (and previous value xpi for kSweepSecond)
+template <int MODE>
+__device__ __forceinline__ double sweep_out(const SweepCoef& c, double dinv_i, double res, double xi, double xpi) {
+  if (MODE == kSweepResidual) return res;
+  if (MODE == kSweepFirst) return fma(c.gamma * dinv_i, res, c.beta == 1.0 ? xi : c.beta * xi);
+  if (MODE == kSweepSecond) return fma(c.gamma * dinv_i, res, fma(c.cd, xi - xpi, xi));
+  return fma(c.gamma * dinv_i, res, xi);
+}
+
+// x0 = a0 D^-1 b, component i (the first step's iterate)
+__device__ __forceinline__ double first_x(double a0, const double* __restrict__ dinv, const double* __restrict__ b,
                                           size_t i) {
-  return w * dinv[i] * b[i];
+  return a0 * dinv[i] * b[i];
 }
 
 // Finest-level sweep on the FP32 difference-form operator of mixed_kernels.cu (the smoother is a
@@ -803,13 +852,14 @@ __device__ __forceinline__ double first_x(double w, const double* __restrict__ d
 // follow in neighbour order.
 template <int MODE>
 __global__ void __launch_bounds__(256) k_amg_sweep_f32(MixedMatrix M, const double* __restrict__ dinv,
-                                                       const double* __restrict__ lam, const double* __restrict__ b,
-                                                       const double* __restrict__ x, double* __restrict__ xo) {
-  const double w = MODE == kSweepResidual ? 0.0 : 4.0 / (3.0 * *lam);
+                                                       const double* __restrict__ lam, int cheb,
+                                                       const double* __restrict__ b, const double* __restrict__ x,
+                                                       const double* xp, double* xo) {
+  const SweepCoef cf = sweep_coef<MODE>(lam, cheb);
   const double2* x2 = reinterpret_cast<const double2*>(x);
   auto xnode = [&](int m) -> double2 {
     if (MODE == kSweepFirst)
-      return make_double2(first_x(w, dinv, b, 2 * (size_t)m), first_x(w, dinv, b, 2 * (size_t)m + 1));
+      return make_double2(first_x(cf.a0, dinv, b, 2 * (size_t)m), first_x(cf.a0, dinv, b, 2 * (size_t)m + 1));
     return x2[m];
   };
   for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < M.n_nodes; n += gridDim.x * blockDim.x) {
@@ -854,7 +904,8 @@ __global__ void __launch_bounds__(256) k_amg_sweep_f32(MixedMatrix M, const doub
       out = make_double2(ra, rbv);
     } else {
       const double2 dv = reinterpret_cast<const double2*>(dinv)[n];
-      out = make_double2(fma(w * dv.x, ra, xs.x), fma(w * dv.y, rbv, xs.y));
+      const double2 pv = MODE == kSweepSecond ? reinterpret_cast<const double2*>(xp)[n] : make_double2(0.0, 0.0);
+      out = make_double2(sweep_out<MODE>(cf, dv.x, ra, xs.x, pv.x), sweep_out<MODE>(cf, dv.y, rbv, xs.y, pv.y));
     }
     reinterpret_cast<double2*>(xo)[n] = out;
   }
@@ -876,10 +927,11 @@ __device__ __forceinline__ double ldv(const double* p) {
 // `nw` warps (warp index `warp`): rows of any length keep 8 lanes busy, and small levels still
 // spread over the whole grid.
 template <int MODE, bool COH>
-__device__ __forceinline__ void sweep3_rows(const AmgBsr32& A, const double* dinv, double w, const double* b,
-                                            const double* x, double* xo, int warp, int nw, int lane) {
+__device__ __forceinline__ void sweep3_rows(const AmgBsr32& A, const double* dinv, const SweepCoef& cf,
+                                            const double* b, const double* x, const double* xp, double* xo, int warp,
+                                            int nw, int lane) {
   auto xval = [&](size_t d) -> double {
-    return MODE == kSweepFirst ? w * __ldg(&dinv[d]) * ldv<COH>(&b[d]) : ldv<COH>(&x[d]);
+    return MODE == kSweepFirst ? cf.a0 * __ldg(&dinv[d]) * ldv<COH>(&b[d]) : ldv<COH>(&x[d]);
   };
   const size_t nb = (size_t)A.nnzb;
   const int l8 = lane & 7, sub = lane >> 3;
@@ -909,18 +961,20 @@ __device__ __forceinline__ void sweep3_rows(const AmgBsr32& A, const double* din
       const size_t d = 3 * (size_t)i + l8;
       const double acc = l8 == 0 ? a0 : l8 == 1 ? a1 : a2;
       const double res = ldv<COH>(&b[d]) - acc;
-      xo[d] = MODE == kSweepResidual ? res : fma(w * __ldg(&dinv[d]), res, xval(d));
+      xo[d] = MODE == kSweepResidual
+                  ? res
+                  : sweep_out<MODE>(cf, __ldg(&dinv[d]), res, xval(d), MODE == kSweepSecond ? ldv<COH>(&xp[d]) : 0.0);
     }
   }
 }
 
 template <int MODE>
 __global__ void __launch_bounds__(256, 8) k_amg_sweep3_f32(AmgBsr32 A, const double* __restrict__ dinv,
-                                                        const double* __restrict__ lam, const double* b,
-                                                        const double* x, double* xo) {
-  const double w = MODE == kSweepResidual ? 0.0 : 4.0 / (3.0 * *lam);
+                                                        const double* __restrict__ lam, int cheb, const double* b,
+                                                        const double* x, const double* xp, double* xo) {
+  const SweepCoef cf = sweep_coef<MODE>(lam, cheb);
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
-  sweep3_rows<MODE, false>(A, dinv, w, b, x, xo, warp, nw, threadIdx.x & 31);
+  sweep3_rows<MODE, false>(A, dinv, cf, b, x, xp, xo, warp, nw, threadIdx.x & 31);
 }
 
 // bc_J = sum over the P blocks of column J of P_iJ' r_i, from the FP32 copy of P stored by coarse
@@ -1021,10 +1075,11 @@ __global__ void __launch_bounds__(kAmgTailThreads, 1) k_amg_tail(const __grid_co
   const int lane = threadIdx.x & 31, warp = tid >> 5, nw = nt >> 5;
   for (int l = 0; l + 1 < T.nl; ++l) {
     const AmgTailLevel& v = T.L[l];
-    const double w = 4.0 / (3.0 * __ldg(v.lam));
-    sweep3_rows<kSweepFirst, true>(v.A, v.dinv, w, v.b, nullptr, v.x, warp, nw, lane);
+    sweep3_rows<kSweepFirst, true>(v.A, v.dinv, sweep_coef<kSweepFirst>(v.lam, T.cheb), v.b, nullptr, nullptr, v.x,
+                                   warp, nw, lane);
     cl.sync();
-    sweep3_rows<kSweepResidual, true>(v.A, v.dinv, 0.0, v.b, v.x, v.r, warp, nw, lane);
+    sweep3_rows<kSweepResidual, true>(v.A, v.dinv, SweepCoef{0.0, 1.0, 0.0, 0.0}, v.b, v.x, nullptr, v.r, warp, nw,
+                                      lane);
     cl.sync();
     restrict_rows<3, true>(v.nc, v.pt_ptr, v.pt_row, v.pt32, v.r, T.L[l + 1].b, warp, nw, lane);
     cl.sync();
@@ -1032,13 +1087,18 @@ __global__ void __launch_bounds__(kAmgTailThreads, 1) k_amg_tail(const __grid_co
   gemv_rows<true>(T.n_coarse, T.Minv, T.L[T.nl - 1].b, T.L[T.nl - 1].x, warp, nw, lane);
   for (int l = T.nl - 2; l >= 0; --l) {
     const AmgTailLevel& v = T.L[l];
-    const double w = 4.0 / (3.0 * __ldg(v.lam));
     cl.sync();
     prolong_rows<3, true>(v.A.n, v.p_ptr, v.p_col, v.p32, T.L[l + 1].x, v.x, tid, nt);
     cl.sync();
-    sweep3_rows<kSweepSmooth, true>(v.A, v.dinv, w, v.b, v.x, v.xa, warp, nw, lane);
+    sweep3_rows<kSweepSmooth, true>(v.A, v.dinv, sweep_coef<kSweepSmooth>(v.lam, T.cheb), v.b, v.x, nullptr, v.xa,
+                                    warp, nw, lane);
     cl.sync();
-    sweep3_rows<kSweepSmooth, true>(v.A, v.dinv, w, v.b, v.xa, v.x, warp, nw, lane);
+    if (T.cheb)
+      sweep3_rows<kSweepSecond, true>(v.A, v.dinv, sweep_coef<kSweepSecond>(v.lam, T.cheb), v.b, v.xa, v.x, v.x,
+                                      warp, nw, lane);
+    else
+      sweep3_rows<kSweepSmooth, true>(v.A, v.dinv, sweep_coef<kSweepSmooth>(v.lam, T.cheb), v.b, v.xa, nullptr, v.x,
+                                      warp, nw, lane);
   }
 }
 
@@ -1297,27 +1357,28 @@ cudaError_t amg_coarsest(int B, const AmgBsr& A, double* M, double* piv, cudaStr
   return cudaGetLastError();
 }
 
-cudaError_t amg_sweep_f32(int mode, const MixedMatrix& M, const double* dinv, const double* lam, const double* b,
-                          const double* x, double* xo, cudaStream_t s) {
-  if (mode == kSweepResidual)
-    k_amg_sweep_f32<kSweepResidual><<<gw(M.n_nodes), 256, 0, s>>>(M, dinv, lam, b, x, xo);
-  else if (mode == kSweepFirst)
-    k_amg_sweep_f32<kSweepFirst><<<gw(M.n_nodes), 256, 0, s>>>(M, dinv, lam, b, x, xo);
-  else
-    k_amg_sweep_f32<kSweepSmooth><<<gw(M.n_nodes), 256, 0, s>>>(M, dinv, lam, b, x, xo);
+cudaError_t amg_sweep_f32(int mode, int cheb, const MixedMatrix& M, const double* dinv, const double* lam,
+                          const double* b, const double* x, const double* xp, double* xo, cudaStream_t s) {
+  const int g = gw(M.n_nodes);
+  switch (mode) {
+    case kSweepResidual: k_amg_sweep_f32<kSweepResidual><<<g, 256, 0, s>>>(M, dinv, lam, cheb, b, x, xp, xo); break;
+    case kSweepFirst: k_amg_sweep_f32<kSweepFirst><<<g, 256, 0, s>>>(M, dinv, lam, cheb, b, x, xp, xo); break;
+    case kSweepSecond: k_amg_sweep_f32<kSweepSecond><<<g, 256, 0, s>>>(M, dinv, lam, cheb, b, x, xp, xo); break;
+    default: k_amg_sweep_f32<kSweepSmooth><<<g, 256, 0, s>>>(M, dinv, lam, cheb, b, x, xp, xo); break;
+  }
   count_launches(1);
   return cudaGetLastError();
 }
 
-cudaError_t amg_sweep3_f32(int mode, const AmgBsr32& A, const double* dinv, const double* lam, const double* b,
-                           const double* x, double* xo, cudaStream_t s) {
+cudaError_t amg_sweep3_f32(int mode, int cheb, const AmgBsr32& A, const double* dinv, const double* lam,
+                           const double* b, const double* x, const double* xp, double* xo, cudaStream_t s) {
   const int g = gw((long long)A.n * 8);
-  if (mode == kSweepResidual)
-    k_amg_sweep3_f32<kSweepResidual><<<g, 256, 0, s>>>(A, dinv, lam, b, x, xo);
-  else if (mode == kSweepFirst)
-    k_amg_sweep3_f32<kSweepFirst><<<g, 256, 0, s>>>(A, dinv, lam, b, x, xo);
-  else
-    k_amg_sweep3_f32<kSweepSmooth><<<g, 256, 0, s>>>(A, dinv, lam, b, x, xo);
+  switch (mode) {
+    case kSweepResidual: k_amg_sweep3_f32<kSweepResidual><<<g, 256, 0, s>>>(A, dinv, lam, cheb, b, x, xp, xo); break;
+    case kSweepFirst: k_amg_sweep3_f32<kSweepFirst><<<g, 256, 0, s>>>(A, dinv, lam, cheb, b, x, xp, xo); break;
+    case kSweepSecond: k_amg_sweep3_f32<kSweepSecond><<<g, 256, 0, s>>>(A, dinv, lam, cheb, b, x, xp, xo); break;
+    default: k_amg_sweep3_f32<kSweepSmooth><<<g, 256, 0, s>>>(A, dinv, lam, cheb, b, x, xp, xo); break;
+  }
   count_launches(1);
   return cudaGetLastError();
 }

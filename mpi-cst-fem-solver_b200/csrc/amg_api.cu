@@ -69,6 +69,7 @@ struct AmgData {
   double setup_seconds = 0.0;
   // the bottom of the cycle in one cluster launch (tail_level 0: every level launches its own kernels)
   bool tail_enabled = true;
+  int cheb = 1;  // smoother: Chebyshev (1) or damped Jacobi (0)
   int tail_cluster = -1;  // CTAs of the tail cluster on this device (-1 not yet queried, 0 none fits)
   int tail_level = 0;
   AmgTail tail;
@@ -266,6 +267,7 @@ int setup_tail(cstg_ctx* ctx, AmgData* d) {
   if (lt >= d->nl - 1 || d->nl - lt > kAmgTailMax) return CSTG_OK;
   AmgTail& T = d->tail;
   T = AmgTail{};
+  T.cheb = d->cheb;
   T.nl = d->nl - lt;
   T.n_coarse = d->n_coarse;
   T.Minv = buf_ptr<double>(d->Minv);
@@ -375,19 +377,24 @@ int vcycle(cstg_ctx* ctx, AmgData* d, size_t l, const double* b, double* x) {
   const bool fine = l == 0;
   const MixedMatrix mm = fine ? mixed_view(ctx) : MixedMatrix{};
   const AmgBsr32 A32 = lv.A32();
-  auto sweep = [&](int mode, const double* xin, double* xout) -> cudaError_t {
-    return fine ? amg_sweep_f32(mode, mm, dinv, lam, b, xin, xout, s) : amg_sweep3_f32(mode, A32, dinv, lam, b, xin, xout, s);
+  const int cheb = d->cheb;
+  auto sweep = [&](int mode, const double* xin, const double* xp, double* xout) -> cudaError_t {
+    return fine ? amg_sweep_f32(mode, cheb, mm, dinv, lam, b, xin, xp, xout, s)
+                : amg_sweep3_f32(mode, cheb, A32, dinv, lam, b, xin, xp, xout, s);
   };
-  CK(sweep(kSweepFirst, nullptr, x));  // two pre-smoothing steps from x = 0
-  CK(sweep(kSweepResidual, x, r));
+  CK(sweep(kSweepFirst, nullptr, nullptr, x));  // two pre-smoothing steps from x = 0
+  CK(sweep(kSweepResidual, x, nullptr, r));
   CK(amg_restrict_f32(lv.B, lv.nc, buf_ptr<int>(lv.pt_ptr), buf_ptr<int>(lv.pt_row), buf_ptr<float>(lv.pt32), r,
                       buf_ptr<double>(nx.bc), s));
   const int rc = vcycle(ctx, d, l + 1, buf_ptr<double>(nx.bc), buf_ptr<double>(nx.xb));
   if (rc) return rc;
   CK(amg_prolong_f32(lv.B, lv.n, buf_ptr<int>(lv.p_ptr), buf_ptr<int>(lv.p_col), buf_ptr<float>(lv.p32),
                      buf_ptr<double>(nx.xb), x, s));
-  CK(sweep(kSweepSmooth, x, xa));
-  CK(sweep(kSweepSmooth, xa, x));
+  CK(sweep(kSweepSmooth, x, nullptr, xa));  // two post-smoothing steps
+  if (cheb)
+    CK(sweep(kSweepSecond, xa, x, x));  // (the previous iterate x is read at each node before it is overwritten)
+  else
+    CK(sweep(kSweepSmooth, xa, nullptr, x));
   return CSTG_OK;
 }
 
@@ -415,6 +422,7 @@ unsigned long long cstg_host::amg_signature(const cstg_ctx* ctx) {
   mix((unsigned long long)d->nl);
   mix((unsigned long long)d->n_coarse);
   mix((unsigned long long)d->tail_level);
+  mix((unsigned long long)d->cheb);
   mix((unsigned long long)d->tail_cluster);
   for (int l = 0; l < d->nl; ++l) {
     mix((unsigned long long)d->L[l].B);
@@ -453,6 +461,19 @@ int cstg_amg_setup(cstg_ctx* ctx, cstg_amg_info* info) {
   return CSTG_OK;
 }
 
+int cstg_amg_set_smoother(cstg_ctx* ctx, int kind) {
+  BEGIN(ctx);
+  if (kind != CSTG_AMG_CHEBYSHEV && kind != CSTG_AMG_JACOBI)
+    return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "amg_set_smoother: unknown smoother %d", kind);
+  if (!ctx->amg) {
+    ctx->amg = new AmgData();
+    ctx->amg->L.reserve(kMaxLevels + 1);
+  }
+  ctx->amg->cheb = kind == CSTG_AMG_CHEBYSHEV ? 1 : 0;
+  if (ctx->amg->nl > 0) return setup_tail(ctx, ctx->amg);
+  return CSTG_OK;
+}
+
 int cstg_amg_set_tail(cstg_ctx* ctx, int enable) {
   BEGIN(ctx);
   if (!ctx->amg) {
@@ -482,7 +503,7 @@ int cstg_amg_time(cstg_ctx* ctx, int reps, double* out) {
   for (int w = 0; w < 2; ++w) {  // warm-up, then timed
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
     for (int k = 0; k < reps; ++k)
-      CK(amg_sweep_f32(kSweepSmooth, mm, buf_ptr<double>(f.dinv), buf_ptr<double>(f.lam), b, k & 1 ? xb : xa, k & 1 ? xa : xb,
+      CK(amg_sweep_f32(kSweepSmooth, d->cheb, mm, buf_ptr<double>(f.dinv), buf_ptr<double>(f.lam), b, k & 1 ? xb : xa, nullptr, k & 1 ? xa : xb,
                        ctx->stream));
     CK(cudaEventRecord(ctx->ev1, ctx->stream));
   }

@@ -276,16 +276,18 @@ cudaError_t amg_ac_count(int B, int nc, const int* pt_ptr, const int* pt_idx, co
 cudaError_t amg_ac_fill(int B, int nc, const int* pt_ptr, const int* pt_idx, const int* p_row, const AmgBsr& P,
                         const AmgBsr& AP, const AmgBsr& Ac, cudaStream_t s);
 cudaError_t amg_coarsest(int B, const AmgBsr& A, double* M, double* piv, cudaStream_t s);
-// smoother sweep modes: x + w D^-1 (b - A x); b - A x; the first sweep from x = 0 (x not read)
-constexpr int kSweepSmooth = 0, kSweepResidual = 1, kSweepFirst = 2;
-cudaError_t amg_sweep_f32(int mode, const MixedMatrix& M, const double* dinv, const double* lam, const double* b,
-                          const double* x, double* xo, cudaStream_t s);
+// smoother steps (amg.cu): x + gamma D^-1 (b - A x); b - A x; the two steps from x = 0 in one
+// launch (x not read); the second Chebyshev step (reads the previous iterate xp). cheb: Chebyshev
+// coefficients (else damped Jacobi), computed in the kernel from lambda_max.
+constexpr int kSweepSmooth = 0, kSweepResidual = 1, kSweepFirst = 2, kSweepSecond = 3;
+cudaError_t amg_sweep_f32(int mode, int cheb, const MixedMatrix& M, const double* dinv, const double* lam,
+                          const double* b, const double* x, const double* xp, double* xo, cudaStream_t s);
 // cycle operators in FP32 (values only; vectors and accumulation stay FP64)
 cudaError_t amg_coarse_f32(const AmgBsr& A, float* val32, cudaStream_t s);
 cudaError_t amg_transfer_f32(int B, const AmgBsr& P, int nnz_p, const int* pt_idx, const int* p_row, float* p32,
                              int* pt_row, float* pt32, cudaStream_t s);
-cudaError_t amg_sweep3_f32(int mode, const AmgBsr32& A, const double* dinv, const double* lam, const double* b,
-                           const double* x, double* xo, cudaStream_t s);
+cudaError_t amg_sweep3_f32(int mode, int cheb, const AmgBsr32& A, const double* dinv, const double* lam,
+                           const double* b, const double* x, const double* xp, double* xo, cudaStream_t s);
 cudaError_t amg_restrict_f32(int B, int nc, const int* pt_ptr, const int* pt_row, const float* pt32, const double* r,
                              double* bc, cudaStream_t s);
 cudaError_t amg_prolong_f32(int B, int n, const int* p_ptr, const int* p_col, const float* p32, const double* xc,
@@ -314,6 +316,7 @@ struct AmgTailLevel {
 };
 struct AmgTail {
   int nl = 0;  // levels, the last one the dense coarsest (only its b and x are used)
+  int cheb = 1;  // Chebyshev smoothing (else damped Jacobi)
   int n_coarse = 0;
   const double* Minv = nullptr;
   AmgTailLevel L[kAmgTailMax];

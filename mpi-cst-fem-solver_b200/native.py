@@ -58,6 +58,7 @@ TRACTION_KIRSCH = 1
 PRECOND_JACOBI = 0
 PRECOND_LEARNED = 1
 PRECOND_AMG = 2
+AMG_CHEBYSHEV, AMG_JACOBI = 0, 1  # cstg_amg_set_smoother
 
 LAUNCH_AUTO = 0
 LAUNCH_PERSISTENT = 1
@@ -140,6 +141,7 @@ _SIGS = {
     "cstg_amg_apply_device": (C.c_int, [_vp, _vp, _vp]),
     "cstg_amg_time": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_double)]),
     "cstg_amg_set_tail": (C.c_int, [_vp, C.c_int]),
+    "cstg_amg_set_smoother": (C.c_int, [_vp, C.c_int]),
     "cstg_mpnn_param_count": (C.c_longlong, []),
     "cstg_learned_setup": (C.c_int, [_vp, _vp, _vp]),
     "cstg_learned_set_params": (C.c_int, [_vp, _vp]),

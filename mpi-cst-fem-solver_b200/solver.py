@@ -421,6 +421,12 @@ def amg_setup(K: GpuCsrMatrix) -> dict:
             "setup_seconds": info.setup_seconds, "tail_level": info.tail_level, "tail_cluster": info.tail_cluster}
 
 
+def amg_set_smoother(K: GpuCsrMatrix, kind: str) -> None:
+    """The cycle's smoother: "chebyshev" (degree 2, the default) or "jacobi" (damped)."""
+    code = {"chebyshev": 0, "jacobi": 1}[kind]
+    K.ctx.check(K.ctx.L.cstg_amg_set_smoother(K.ctx.h, code))
+
+
 def amg_set_tail(K: GpuCsrMatrix, enable: bool) -> None:
     """Runs the small coarse levels as one cluster launch (True, the default) or level by level."""
     K.ctx.check(K.ctx.L.cstg_amg_set_tail(K.ctx.h, int(bool(enable))))
