@@ -19,6 +19,10 @@
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
+#include <mutex>
+#include <utility>
+#include <vector>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -787,6 +791,10 @@ __global__ void __launch_bounds__(1024) k_amg_gauss_jordan(int n, double* __rest
 
 // ---- cycle kernels ----------------------------------------------------------------------------------
 
+// A cycle launched inside the flexible-CG graph carries the solver's done flag: once the solve
+// has converged, the rest of the captured chunk's cycles return at once.
+__device__ __forceinline__ bool skipped(const int* skip) { return skip && *(volatile const int*)skip != 0; }
+
 // Smoother steps. With r(x) = D^-1 (b - A x):
 //   kSweepFirst     xo = beta x0 + gamma r(x0), x0 = a0 D^-1 b formed on the fly (x not read)
 //   kSweepSmooth    xo = x + gamma r(x)
@@ -851,10 +859,11 @@ __device__ __forceinline__ double first_x(double a0, const double* __restrict__ 
 // neighbours' index and value loads are in flight at once, their gathers next, and the additions
 // follow in neighbour order.
 template <int MODE>
-__global__ void __launch_bounds__(256) k_amg_sweep_f32(MixedMatrix M, const double* __restrict__ dinv,
+__global__ void __launch_bounds__(256) k_amg_sweep_f32(const int* skip, MixedMatrix M, const double* __restrict__ dinv,
                                                        const double* __restrict__ lam, int cheb,
                                                        const double* __restrict__ b, const double* __restrict__ x,
                                                        const double* xp, double* xo) {
+  if (skipped(skip)) return;
   const SweepCoef cf = sweep_coef<MODE>(lam, cheb);
   const double2* x2 = reinterpret_cast<const double2*>(x);
   auto xnode = [&](int m) -> double2 {
@@ -969,9 +978,11 @@ __device__ __forceinline__ void sweep3_rows(const AmgBsr32& A, const double* din
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(256, 8) k_amg_sweep3_f32(AmgBsr32 A, const double* __restrict__ dinv,
+__global__ void __launch_bounds__(256, 8) k_amg_sweep3_f32(const int* skip, AmgBsr32 A,
+                                                        const double* __restrict__ dinv,
                                                         const double* __restrict__ lam, int cheb, const double* b,
                                                         const double* x, const double* xp, double* xo) {
+  if (skipped(skip)) return;
   const SweepCoef cf = sweep_coef<MODE>(lam, cheb);
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
   sweep3_rows<MODE, false>(A, dinv, cf, b, x, xp, xo, warp, nw, threadIdx.x & 31);
@@ -1007,10 +1018,11 @@ __device__ __forceinline__ void restrict_rows(int nc, const int* pt_ptr, const i
 }
 
 template <int B>
-__global__ void __launch_bounds__(256) k_amg_restrict_f32(int nc, const int* __restrict__ pt_ptr,
+__global__ void __launch_bounds__(256) k_amg_restrict_f32(const int* skip, int nc, const int* __restrict__ pt_ptr,
                                                           const int* __restrict__ pt_row,
                                                           const float* __restrict__ pt32, const double* r,
                                                           double* bc) {
+  if (skipped(skip)) return;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
   restrict_rows<B, false>(nc, pt_ptr, pt_row, pt32, r, bc, warp, nw, threadIdx.x & 31);
 }
@@ -1039,9 +1051,10 @@ __device__ __forceinline__ void prolong_rows(int n, const int* p_ptr, const int*
 }
 
 template <int B>
-__global__ void __launch_bounds__(256) k_amg_prolong_f32(int n, const int* __restrict__ p_ptr,
+__global__ void __launch_bounds__(256) k_amg_prolong_f32(const int* skip, int n, const int* __restrict__ p_ptr,
                                                          const int* __restrict__ p_col, const float* __restrict__ p32,
                                                          const double* xc, double* x) {
+  if (skipped(skip)) return;
   prolong_rows<B, false>(n, p_ptr, p_col, p32, xc, x, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
@@ -1057,7 +1070,8 @@ __device__ __forceinline__ void gemv_rows(int n, const double* M, const double* 
   }
 }
 
-__global__ void k_amg_gemv(int n, const double* __restrict__ M, const double* b, double* x) {
+__global__ void k_amg_gemv(const int* skip, int n, const double* __restrict__ M, const double* b, double* x) {
+  if (skipped(skip)) return;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
   gemv_rows<false>(n, M, b, x, warp, nw, threadIdx.x & 31);
 }
@@ -1068,7 +1082,8 @@ __global__ void k_amg_gemv(int n, const double* __restrict__ M, const double* b,
 // cluster barriers (release/acquire at cluster scope; vectors written in a phase are read in the
 // next through L2). The same row functions and orders of addition as the per-level launches, so
 // the result is bit-identical to them; only the ~13 launch latencies of these small levels go.
-__global__ void __launch_bounds__(kAmgTailThreads, 1) k_amg_tail(const __grid_constant__ AmgTail T) {
+__global__ void __launch_bounds__(kAmgTailThreads, 1) k_amg_tail(const int* skip, const __grid_constant__ AmgTail T) {
+  if (skipped(skip)) return;  // (uniform over the cluster: every CTA leaves before any barrier)
   const cg::cluster_group cl = cg::this_cluster();
   const int tid = (int)cl.block_rank() * blockDim.x + threadIdx.x;
   const int nt = (int)cl.num_blocks() * blockDim.x;
@@ -1156,6 +1171,36 @@ __global__ void k_amg_rigid(int N, const double* __restrict__ xy, double* __rest
   b[3] = 0.0;
   b[4] = 1.0;
   b[5] = xy[2 * n];
+}
+
+// One full wave of a grid-stride kernel: every SM gets as many blocks as it can hold at once
+// (capped by the work), so no partial second wave idles part of the GPU. The occupancy of each
+// kernel (256 threads, no dynamic shared memory) is queried once and cached.
+int one_wave(const void* kern, long long n_threads) {
+  static std::mutex mu;
+  static std::vector<std::pair<const void*, int>> cache;
+  static int sms = 0;
+  int per_sm = 0;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    if (!sms) {
+      int dev = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      sms = std::max(sms, 1);
+    }
+    for (const auto& e : cache)
+      if (e.first == kern) per_sm = e.second;
+    if (!per_sm) {
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0) != cudaSuccess || per_sm < 1) {
+        cudaGetLastError();
+        per_sm = 1;
+      }
+      cache.emplace_back(kern, per_sm);
+    }
+  }
+  const long long need = (n_threads + 255) / 256;
+  return (int)std::max<long long>(1, std::min<long long>(need, (long long)per_sm * sms));
 }
 
 inline int g1(long long n, int t = 256) { return (int)std::max<long long>(1, std::min<long long>((n + t - 1) / t, 1LL << 30)); }
@@ -1357,48 +1402,75 @@ cudaError_t amg_coarsest(int B, const AmgBsr& A, double* M, double* piv, cudaStr
   return cudaGetLastError();
 }
 
-cudaError_t amg_sweep_f32(int mode, int cheb, const MixedMatrix& M, const double* dinv, const double* lam,
-                          const double* b, const double* x, const double* xp, double* xo, cudaStream_t s) {
-  const int g = gw(M.n_nodes);
+void amg_prepare_launch_shapes() {
+  // (the occupancy queries run here, outside any stream capture)
+  one_wave((const void*)k_amg_sweep_f32<kSweepResidual>, 1);
+  one_wave((const void*)k_amg_sweep_f32<kSweepFirst>, 1);
+  one_wave((const void*)k_amg_sweep_f32<kSweepSecond>, 1);
+  one_wave((const void*)k_amg_sweep_f32<kSweepSmooth>, 1);
+  one_wave((const void*)k_amg_restrict_f32<2>, 1);
+  one_wave((const void*)k_amg_prolong_f32<2>, 1);
+}
+
+cudaError_t amg_sweep_f32(const int* skip, int mode, int cheb, const MixedMatrix& M, const double* dinv,
+                          const double* lam, const double* b, const double* x, const double* xp, double* xo,
+                          cudaStream_t s) {
+  const long long t = M.n_nodes;
   switch (mode) {
-    case kSweepResidual: k_amg_sweep_f32<kSweepResidual><<<g, 256, 0, s>>>(M, dinv, lam, cheb, b, x, xp, xo); break;
-    case kSweepFirst: k_amg_sweep_f32<kSweepFirst><<<g, 256, 0, s>>>(M, dinv, lam, cheb, b, x, xp, xo); break;
-    case kSweepSecond: k_amg_sweep_f32<kSweepSecond><<<g, 256, 0, s>>>(M, dinv, lam, cheb, b, x, xp, xo); break;
-    default: k_amg_sweep_f32<kSweepSmooth><<<g, 256, 0, s>>>(M, dinv, lam, cheb, b, x, xp, xo); break;
+    case kSweepResidual:
+      k_amg_sweep_f32<kSweepResidual><<<one_wave((const void*)k_amg_sweep_f32<kSweepResidual>, t), 256, 0, s>>>(
+          skip, M, dinv, lam, cheb, b, x, xp, xo);
+      break;
+    case kSweepFirst:
+      k_amg_sweep_f32<kSweepFirst><<<one_wave((const void*)k_amg_sweep_f32<kSweepFirst>, t), 256, 0, s>>>(skip, M, dinv, lam, cheb,
+                                                                                             b, x, xp, xo);
+      break;
+    case kSweepSecond:
+      k_amg_sweep_f32<kSweepSecond><<<one_wave((const void*)k_amg_sweep_f32<kSweepSecond>, t), 256, 0, s>>>(
+          skip, M, dinv, lam, cheb, b, x, xp, xo);
+      break;
+    default:
+      k_amg_sweep_f32<kSweepSmooth><<<one_wave((const void*)k_amg_sweep_f32<kSweepSmooth>, t), 256, 0, s>>>(
+          skip, M, dinv, lam, cheb, b, x, xp, xo);
+      break;
   }
   count_launches(1);
   return cudaGetLastError();
 }
 
-cudaError_t amg_sweep3_f32(int mode, int cheb, const AmgBsr32& A, const double* dinv, const double* lam,
-                           const double* b, const double* x, const double* xp, double* xo, cudaStream_t s) {
+cudaError_t amg_sweep3_f32(const int* skip, int mode, int cheb, const AmgBsr32& A, const double* dinv,
+                           const double* lam, const double* b, const double* x, const double* xp, double* xo,
+                           cudaStream_t s) {
   const int g = gw((long long)A.n * 8);
   switch (mode) {
-    case kSweepResidual: k_amg_sweep3_f32<kSweepResidual><<<g, 256, 0, s>>>(A, dinv, lam, cheb, b, x, xp, xo); break;
-    case kSweepFirst: k_amg_sweep3_f32<kSweepFirst><<<g, 256, 0, s>>>(A, dinv, lam, cheb, b, x, xp, xo); break;
-    case kSweepSecond: k_amg_sweep3_f32<kSweepSecond><<<g, 256, 0, s>>>(A, dinv, lam, cheb, b, x, xp, xo); break;
-    default: k_amg_sweep3_f32<kSweepSmooth><<<g, 256, 0, s>>>(A, dinv, lam, cheb, b, x, xp, xo); break;
+    case kSweepResidual:
+      k_amg_sweep3_f32<kSweepResidual><<<g, 256, 0, s>>>(skip, A, dinv, lam, cheb, b, x, xp, xo);
+      break;
+    case kSweepFirst: k_amg_sweep3_f32<kSweepFirst><<<g, 256, 0, s>>>(skip, A, dinv, lam, cheb, b, x, xp, xo); break;
+    case kSweepSecond: k_amg_sweep3_f32<kSweepSecond><<<g, 256, 0, s>>>(skip, A, dinv, lam, cheb, b, x, xp, xo); break;
+    default: k_amg_sweep3_f32<kSweepSmooth><<<g, 256, 0, s>>>(skip, A, dinv, lam, cheb, b, x, xp, xo); break;
   }
   count_launches(1);
   return cudaGetLastError();
 }
 
-cudaError_t amg_restrict_f32(int B, int nc, const int* pt_ptr, const int* pt_row, const float* pt32, const double* r,
-                             double* bc, cudaStream_t s) {
+cudaError_t amg_restrict_f32(const int* skip, int B, int nc, const int* pt_ptr, const int* pt_row, const float* pt32,
+                             const double* r, double* bc, cudaStream_t s) {
   if (B == 2)
-    k_amg_restrict_f32<2><<<gw((long long)nc * 32), 256, 0, s>>>(nc, pt_ptr, pt_row, pt32, r, bc);
+    k_amg_restrict_f32<2><<<one_wave((const void*)k_amg_restrict_f32<2>, (long long)nc * 32), 256, 0, s>>>(skip, nc, pt_ptr, pt_row,
+                                                                                            pt32, r, bc);
   else
-    k_amg_restrict_f32<3><<<gw((long long)nc * 32), 256, 0, s>>>(nc, pt_ptr, pt_row, pt32, r, bc);
+    k_amg_restrict_f32<3><<<gw((long long)nc * 32), 256, 0, s>>>(skip, nc, pt_ptr, pt_row, pt32, r, bc);
   count_launches(1);
   return cudaGetLastError();
 }
 
-cudaError_t amg_prolong_f32(int B, int n, const int* p_ptr, const int* p_col, const float* p32, const double* xc,
-                            double* x, cudaStream_t s) {
+cudaError_t amg_prolong_f32(const int* skip, int B, int n, const int* p_ptr, const int* p_col, const float* p32,
+                            const double* xc, double* x, cudaStream_t s) {
   if (B == 2)
-    k_amg_prolong_f32<2><<<gw(n), 256, 0, s>>>(n, p_ptr, p_col, p32, xc, x);
+    k_amg_prolong_f32<2><<<one_wave((const void*)k_amg_prolong_f32<2>, n), 256, 0, s>>>(skip, n, p_ptr, p_col, p32, xc, x);
   else
-    k_amg_prolong_f32<3><<<gw(n), 256, 0, s>>>(n, p_ptr, p_col, p32, xc, x);
+    k_amg_prolong_f32<3><<<gw(n), 256, 0, s>>>(skip, n, p_ptr, p_col, p32, xc, x);
   count_launches(1);
   return cudaGetLastError();
 }
@@ -1420,7 +1492,7 @@ cudaError_t amg_transfer_f32(int B, const AmgBsr& P, int nnz_p, const int* pt_id
   return cudaGetLastError();
 }
 
-cudaError_t amg_tail(const AmgTail& t, int cluster, int* max_clusters, cudaStream_t s) {
+cudaError_t amg_tail(const int* skip, const AmgTail& t, int cluster, int* max_clusters, cudaStream_t s) {
   if (cluster < 1 || cluster > 16) return cudaErrorInvalidValue;
   if (cluster > 8 && max_clusters) {  // the shape query precedes any launch (never in a capture)
     const cudaError_t e = cudaFuncSetAttribute(k_amg_tail, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
@@ -1442,7 +1514,7 @@ cudaError_t amg_tail(const AmgTail& t, int cluster, int* max_clusters, cudaStrea
     *max_clusters = 0;
     return cudaOccupancyMaxActiveClusters(max_clusters, (void*)k_amg_tail, &cfg);
   }
-  const cudaError_t e = cudaLaunchKernelEx(&cfg, k_amg_tail, t);
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, k_amg_tail, skip, t);
   count_launches(1);
   return e;
 }
@@ -1453,8 +1525,8 @@ cudaError_t amg_rigid_modes(int N, const double* xy, double* Bf, cudaStream_t s)
   return cudaGetLastError();
 }
 
-cudaError_t amg_gemv(int n, const double* M, const double* b, double* x, cudaStream_t s) {
-  k_amg_gemv<<<gw((long long)n * 32), 256, 0, s>>>(n, M, b, x);
+cudaError_t amg_gemv(const int* skip, int n, const double* M, const double* b, double* x, cudaStream_t s) {
+  k_amg_gemv<<<gw((long long)n * 32), 256, 0, s>>>(skip, n, M, b, x);
   count_launches(1);
   return cudaGetLastError();
 }

@@ -253,7 +253,7 @@ int setup_tail(cstg_ctx* ctx, AmgData* d) {
     d->tail_cluster = 0;
     for (int c : {16, 8}) {
       int m = 0;
-      const cudaError_t e = amg_tail(d->tail, c, &m, ctx->stream);
+      const cudaError_t e = amg_tail(nullptr, d->tail, c, &m, ctx->stream);
       if (e == cudaSuccess && m >= 1) {
         d->tail_cluster = c;
         break;
@@ -301,6 +301,7 @@ int amg_build(cstg_ctx* ctx) {
   }
   AmgData* d = ctx->amg;
   const auto t0 = std::chrono::steady_clock::now();
+  amg_prepare_launch_shapes();
   if (d->L.empty()) d->L.emplace_back();
   d->nl = 1;
   {
@@ -355,15 +356,15 @@ int amg_build(cstg_ctx* ctx) {
 }
 
 // V(2,2): x = cycle(l, b)
-int vcycle(cstg_ctx* ctx, AmgData* d, size_t l, const double* b, double* x) {
+int vcycle(cstg_ctx* ctx, AmgData* d, size_t l, const double* b, double* x, const int* skip) {
   AmgLevel& lv = d->L[l];
   cudaStream_t s = ctx->stream;
   if ((int)l + 1 == d->nl) {
-    CK(amg_gemv(d->n_coarse, buf_ptr<double>(d->Minv), b, x, s));
+    CK(amg_gemv(skip, d->n_coarse, buf_ptr<double>(d->Minv), b, x, s));
     return CSTG_OK;
   }
   if (d->tail_level > 0 && (int)l == d->tail_level && b == d->tail.L[0].b && x == d->tail.L[0].x) {
-    CK(amg_tail(d->tail, d->tail_cluster, nullptr, s));
+    CK(amg_tail(skip, d->tail, d->tail_cluster, nullptr, s));
     return CSTG_OK;
   }
   const double* dinv = buf_ptr<double>(lv.dinv);
@@ -379,16 +380,16 @@ int vcycle(cstg_ctx* ctx, AmgData* d, size_t l, const double* b, double* x) {
   const AmgBsr32 A32 = lv.A32();
   const int cheb = d->cheb;
   auto sweep = [&](int mode, const double* xin, const double* xp, double* xout) -> cudaError_t {
-    return fine ? amg_sweep_f32(mode, cheb, mm, dinv, lam, b, xin, xp, xout, s)
-                : amg_sweep3_f32(mode, cheb, A32, dinv, lam, b, xin, xp, xout, s);
+    return fine ? amg_sweep_f32(skip, mode, cheb, mm, dinv, lam, b, xin, xp, xout, s)
+                : amg_sweep3_f32(skip, mode, cheb, A32, dinv, lam, b, xin, xp, xout, s);
   };
   CK(sweep(kSweepFirst, nullptr, nullptr, x));  // two pre-smoothing steps from x = 0
   CK(sweep(kSweepResidual, x, nullptr, r));
-  CK(amg_restrict_f32(lv.B, lv.nc, buf_ptr<int>(lv.pt_ptr), buf_ptr<int>(lv.pt_row), buf_ptr<float>(lv.pt32), r,
+  CK(amg_restrict_f32(skip, lv.B, lv.nc, buf_ptr<int>(lv.pt_ptr), buf_ptr<int>(lv.pt_row), buf_ptr<float>(lv.pt32), r,
                       buf_ptr<double>(nx.bc), s));
-  const int rc = vcycle(ctx, d, l + 1, buf_ptr<double>(nx.bc), buf_ptr<double>(nx.xb));
+  const int rc = vcycle(ctx, d, l + 1, buf_ptr<double>(nx.bc), buf_ptr<double>(nx.xb), skip);
   if (rc) return rc;
-  CK(amg_prolong_f32(lv.B, lv.n, buf_ptr<int>(lv.p_ptr), buf_ptr<int>(lv.p_col), buf_ptr<float>(lv.p32),
+  CK(amg_prolong_f32(skip, lv.B, lv.n, buf_ptr<int>(lv.p_ptr), buf_ptr<int>(lv.p_col), buf_ptr<float>(lv.p32),
                      buf_ptr<double>(nx.xb), x, s));
   CK(sweep(kSweepSmooth, x, nullptr, xa));  // two post-smoothing steps
   if (cheb)
@@ -412,6 +413,8 @@ int cstg_host::amg_ready(cstg_ctx* ctx) {
 
 int cstg_host::amg_levels(const cstg_ctx* ctx) { return ctx->amg ? ctx->amg->nl : 0; }
 
+int cstg_host::amg_chebyshev(const cstg_ctx* ctx) { return ctx->amg ? ctx->amg->cheb : 1; }
+
 unsigned long long cstg_host::amg_signature(const cstg_ctx* ctx) {
   // the launch shapes and scalar arguments a captured cycle depends on (buffer moves are
   // covered by the context's generation)
@@ -432,8 +435,8 @@ unsigned long long cstg_host::amg_signature(const cstg_ctx* ctx) {
   return h;
 }
 
-int cstg_host::amg_apply(cstg_ctx* ctx, const double* r, double* z) {
-  return vcycle(ctx, ctx->amg, 0, r, z);
+int cstg_host::amg_apply(cstg_ctx* ctx, const double* r, double* z, const int* skip) {
+  return vcycle(ctx, ctx->amg, 0, r, z, skip);
 }
 
 extern "C" {
@@ -503,7 +506,7 @@ int cstg_amg_time(cstg_ctx* ctx, int reps, double* out) {
   for (int w = 0; w < 2; ++w) {  // warm-up, then timed
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
     for (int k = 0; k < reps; ++k)
-      CK(amg_sweep_f32(kSweepSmooth, d->cheb, mm, buf_ptr<double>(f.dinv), buf_ptr<double>(f.lam), b, k & 1 ? xb : xa, nullptr, k & 1 ? xa : xb,
+      CK(amg_sweep_f32(nullptr, kSweepSmooth, d->cheb, mm, buf_ptr<double>(f.dinv), buf_ptr<double>(f.lam), b, k & 1 ? xb : xa, nullptr, k & 1 ? xa : xb,
                        ctx->stream));
     CK(cudaEventRecord(ctx->ev1, ctx->stream));
   }
@@ -514,7 +517,7 @@ int cstg_amg_time(cstg_ctx* ctx, int reps, double* out) {
   for (int w = 0; w < 2; ++w) {
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
     for (int k = 0; k < reps; ++k) {
-      const int rc2 = vcycle(ctx, d, 0, b, xb);
+      const int rc2 = vcycle(ctx, d, 0, b, xb, nullptr);
       if (rc2) return rc2;
     }
     CK(cudaEventRecord(ctx->ev1, ctx->stream));
@@ -529,7 +532,7 @@ int cstg_amg_apply_device(cstg_ctx* ctx, const double* d_r, double* d_z) {
   BEGIN(ctx);
   const int rc = amg_ready(ctx);
   if (rc) return rc;
-  const int rc2 = amg_apply(ctx, d_r, d_z);
+  const int rc2 = amg_apply(ctx, d_r, d_z, nullptr);
   if (rc2) return rc2;
   CK(cudaStreamSynchronize(ctx->stream));
   return CSTG_OK;

@@ -254,9 +254,10 @@ inline void g_fmt(char* out, size_t n, const char* fmt, ...) {
 
 // Defined in amg_api.cu: the multigrid hierarchy (built when missing or stale) and z = M r.
 int amg_ready(cstg_ctx* ctx);
-int amg_apply(cstg_ctx* ctx, const double* r, double* z);
+int amg_apply(cstg_ctx* ctx, const double* r, double* z, const int* skip);  // skip: see amg_sweep_f32
 void amg_free(cstg_ctx* ctx);
 int amg_levels(const cstg_ctx* ctx);
+int amg_chebyshev(const cstg_ctx* ctx);  // 1: Chebyshev smoothing, 0: damped Jacobi
 unsigned long long amg_signature(const cstg_ctx* ctx);  // level shapes of the current hierarchy
 
 // Defined in learned_api.cu: flexible CG with the learned preconditioner.

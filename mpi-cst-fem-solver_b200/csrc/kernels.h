@@ -280,19 +280,23 @@ cudaError_t amg_coarsest(int B, const AmgBsr& A, double* M, double* piv, cudaStr
 // launch (x not read); the second Chebyshev step (reads the previous iterate xp). cheb: Chebyshev
 // coefficients (else damped Jacobi), computed in the kernel from lambda_max.
 constexpr int kSweepSmooth = 0, kSweepResidual = 1, kSweepFirst = 2, kSweepSecond = 3;
-cudaError_t amg_sweep_f32(int mode, int cheb, const MixedMatrix& M, const double* dinv, const double* lam,
-                          const double* b, const double* x, const double* xp, double* xo, cudaStream_t s);
+void amg_prepare_launch_shapes();  // occupancy queries of the one-wave launches (call outside a capture)
+// skip (all cycle launchers): a device flag; non-zero makes the launch return at once (may be null)
+cudaError_t amg_sweep_f32(const int* skip, int mode, int cheb, const MixedMatrix& M, const double* dinv,
+                          const double* lam, const double* b, const double* x, const double* xp, double* xo,
+                          cudaStream_t s);
 // cycle operators in FP32 (values only; vectors and accumulation stay FP64)
 cudaError_t amg_coarse_f32(const AmgBsr& A, float* val32, cudaStream_t s);
 cudaError_t amg_transfer_f32(int B, const AmgBsr& P, int nnz_p, const int* pt_idx, const int* p_row, float* p32,
                              int* pt_row, float* pt32, cudaStream_t s);
-cudaError_t amg_sweep3_f32(int mode, int cheb, const AmgBsr32& A, const double* dinv, const double* lam,
-                           const double* b, const double* x, const double* xp, double* xo, cudaStream_t s);
-cudaError_t amg_restrict_f32(int B, int nc, const int* pt_ptr, const int* pt_row, const float* pt32, const double* r,
-                             double* bc, cudaStream_t s);
-cudaError_t amg_prolong_f32(int B, int n, const int* p_ptr, const int* p_col, const float* p32, const double* xc,
-                            double* x, cudaStream_t s);
-cudaError_t amg_gemv(int n, const double* M, const double* b, double* x, cudaStream_t s);
+cudaError_t amg_sweep3_f32(const int* skip, int mode, int cheb, const AmgBsr32& A, const double* dinv,
+                           const double* lam, const double* b, const double* x, const double* xp, double* xo,
+                           cudaStream_t s);
+cudaError_t amg_restrict_f32(const int* skip, int B, int nc, const int* pt_ptr, const int* pt_row, const float* pt32,
+                             const double* r, double* bc, cudaStream_t s);
+cudaError_t amg_prolong_f32(const int* skip, int B, int n, const int* p_ptr, const int* p_col, const float* p32,
+                            const double* xc, double* x, cudaStream_t s);
+cudaError_t amg_gemv(const int* skip, int n, const double* M, const double* b, double* x, cudaStream_t s);
 
 // The bottom of the V-cycle in one thread-block cluster (levels >= 1 with 3 x 3 blocks, then the
 // dense coarsest solve): level 0 of the tail takes b and writes x like the per-level path.
@@ -323,7 +327,7 @@ struct AmgTail {
 };
 // cluster: CTAs in the one cluster (1..16); max_clusters != nullptr: only query how many such
 // clusters fit at once (0 = the shape cannot launch), nothing is launched
-cudaError_t amg_tail(const AmgTail& t, int cluster, int* max_clusters, cudaStream_t s);
+cudaError_t amg_tail(const int* skip, const AmgTail& t, int cluster, int* max_clusters, cudaStream_t s);
 cudaError_t amg_rigid_modes(int N, const double* xy, double* Bf, cudaStream_t s);
 
 // Process-wide count of kernel launches issued by this library (graph launches count every

@@ -102,7 +102,7 @@ int cstg_host::run_fcg(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg
       CK(launch_spmv_pcg(bm, w.p, w.q, w.partials, w.st, ctx->stream));
     CK(launch_fcg_update(w, kFcgWindow, kFcgRatio2, ctx->stream));
     if (use_amg) {
-      const int rc = amg_apply(ctx, w.r, w.z);
+      const int rc = amg_apply(ctx, w.r, w.z, &w.st->done);  // (cycles after convergence return at once)
       if (rc) return rc;
     } else {
       CK(launch_mp_forward(g, P, w.r, w.inv_diag, rr, sf, skip, mw, false, w.z, err, ctx->stream));
@@ -150,7 +150,7 @@ int cstg_host::run_fcg(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg
   CK(cudaMemcpyAsync(&w.st->fp64_mode, &zero, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
   CK(launch_fcg_init(w, o.rtol, o.max_iter, kFcgWindow, ctx->stream));
   if (use_amg) {
-    const int rc = amg_apply(ctx, w.r, w.z);
+    const int rc = amg_apply(ctx, w.r, w.z, &w.st->done);
     if (rc) return rc;
   } else {
     CK(launch_mp_forward(g, P, w.r, w.inv_diag, rr, sf, skip, mw, false, w.z, err, ctx->stream));
@@ -219,7 +219,8 @@ int cstg_host::run_fcg(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg
     stats->spmv_calls = spmv_calls;
     char pre[160];
     if (use_amg)
-      g_fmt(pre, sizeof pre, "smoothed-aggregation multigrid V(2,2), %d levels", amg_levels(ctx));
+      g_fmt(pre, sizeof pre, "smoothed-aggregation multigrid V(2,2), %s smoothing, %d levels",
+            amg_chebyshev(ctx) ? "Chebyshev" : "damped-Jacobi", amg_levels(ctx));
     else if (fallback_iter >= 0)
       g_fmt(pre, sizeof pre, "learned preconditioner, switched to Jacobi at iteration %d (stagnation)",
             fallback_iter);
