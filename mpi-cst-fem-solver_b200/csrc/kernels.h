@@ -73,6 +73,7 @@ struct alignas(128) PcgState {
   int cycle_limit;      // mixed: force a reliable update after this many iterations
   int fp64_mode;        // mixed: the FP32 operator reached its accuracy floor; SpMV in FP64
   int fp64_switch_iter; // mixed: iteration of that switch (0: none)
+  int stall_cycles;     // mixed: forced replacements in a row that found no progress of the true residual
   double best_true;     // mixed: smallest FP64 true residual seen at a reliable update
   double fb_rr0;        // learned (flexible CG): r'r at the start of the stagnation window
   int fallback;         // learned: the network is off, Jacobi-PCG from here on

@@ -243,6 +243,7 @@ __global__ void __launch_bounds__(kThreads) k_init_mixed(int N, const double* __
     st->cycle_limit = kReplaceCycleLimit;
     st->fp64_mode = 0;
     st->fp64_switch_iter = 0;
+    st->stall_cycles = 0;
     st->best_true = 1.0;
     if (bnorm == 0.0) {
       st->rel = 0.0;
@@ -369,9 +370,14 @@ __global__ void __launch_bounds__(kThreads) k_replace_mixed(BlockMatrix A, const
       st->done = CSTG_SOLVE_CONVERGED + 1;
     } else {
       // Precision switch: the recursive residual met rtol but the FP64 true residual did not
-      // (or a delta cycle did not halve the true residual): the FP32 operator has reached its
+      // (or a delta cycle did not halve the true residual, or, within 1e4 x rtol, two forced
+      // replacements in a row found it no lower than 0.9 of its best — farther out such cycles
+      // are the early rise of the CG residual, not a floor): the FP32 operator has reached its
       // accuracy floor, so the remaining iterations use the FP64 matrix.
-      if (!st->fp64_mode && (kind == 2 || (kind == 1 && tr > 0.5 * st->best_true))) {
+      if (kind == 3)
+        st->stall_cycles = (tr > 0.9 * st->best_true && st->best_true < 1e4 * st->rtol) ? st->stall_cycles + 1 : 0;
+      if (!st->fp64_mode && (kind == 2 || (kind == 1 && tr > 0.5 * st->best_true) ||
+                                (kind == 3 && st->stall_cycles >= 2))) {
         st->fp64_mode = 1;
         st->fp64_switch_iter = st->iter;
         st->beta = 0.0;  // restart the direction: p = D^-1 r, plain FP64 CG from here

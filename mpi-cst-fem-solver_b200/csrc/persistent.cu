@@ -350,7 +350,12 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PersistArgs a) {
             if (tr < st->rtol) {
               st->done = CSTG_SOLVE_CONVERGED + 1;
             } else {
-              if (!st->fp64_mode && (kind == 2 || (kind == 1 && tr > 0.5 * st->best_true))) {
+              // (the precision switch of mixed_kernels.cu's k_replace_mixed, same rule)
+              if (kind == 3)
+                st->stall_cycles =
+                    (tr > 0.9 * st->best_true && st->best_true < 1e4 * st->rtol) ? st->stall_cycles + 1 : 0;
+              if (!st->fp64_mode && (kind == 2 || (kind == 1 && tr > 0.5 * st->best_true) ||
+                                (kind == 3 && st->stall_cycles >= 2))) {
                 st->fp64_mode = 1;
                 st->fp64_switch_iter = st->iter;
                 st->beta = 0.0;

@@ -127,3 +127,24 @@ def test_mixed_on_2m_plate(pkg, gpu_lib):
     print(f"2M plate: fp64 {st64.iterations} it {st64.solve_seconds:.3f} s, mixed {stm.iterations} it "
           f"{stm.solve_seconds:.3f} s, rel diff {_rel(xm, x64):.2e}")
     K.ctx.close()
+
+
+def test_mixed_switches_to_fp64_at_its_floor(pkg, gpu_lib):
+    """4M-DOF plate (n_r=800 x n_theta=2500): the FP32 operator's accuracy floor is above rtol
+    and the recursive residual falls by less than 10x per replacement cycle, so the floor shows
+    only as a whole cycle without progress of the true residual; the solve must switch to the FP64
+    operator there and converge (without the rule it replaced the residual every cycle until
+    max_iter)."""
+    p = pkg.plate.quarter_plate(800, 2500)
+    K = pkg.build_stiffness_pattern(p)
+    pkg.assemble_stiffness(p, pkg.constitutive_matrix(1.0, 0.3), 1.0, K)
+    b = np.zeros(p.num_dofs)
+    pkg.add_traction(K, p.boundary_edges["right"], 1.0, 1.0, 0.0, b)
+    pkg.apply_dirichlet(pkg.plate.symmetry_dirichlet(p), K, b)
+    sm = pkg.CgJacobiSolver(_mixed())
+    sm.setup(K)
+    xm = np.zeros(p.num_dofs)
+    stm = sm.solve(b, xm)
+    assert stm.converged and stm.true_rel_residual < 1e-10, stm.message
+    assert stm.iterations < 45000, stm.iterations  # FP64 Jacobi-PCG: 27,670
+    K.ctx.close()
