@@ -38,6 +38,7 @@ WORKLOADS = {
     "plate2m": (565, 1766, "quarter plate [0,10]^2 minus r<1, O-grid n_r=565 x n_theta=1766"),
     "plate1m": (400, 1250, "quarter plate [0,10]^2 minus r<1, O-grid n_r=400 x n_theta=1250"),
     "plate4m": (800, 2500, "quarter plate [0,10]^2 minus r<1, O-grid n_r=800 x n_theta=2500"),
+    "plate8m": (1131, 3536, "quarter plate [0,10]^2 minus r<1, O-grid n_r=1131 x n_theta=3536"),
     "plate40x80": (40, 80, "quarter plate [0,10]^2 minus r<1, O-grid n_r=40 x n_theta=80"),
 }
 

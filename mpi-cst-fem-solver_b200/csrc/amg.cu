@@ -292,43 +292,10 @@ __global__ void k_amg_tentative(int n_agg, const int* __restrict__ agg_ptr, cons
 }
 
 // ---- lambda_max(D^-1 A) by power iteration ----------------------------------------------------------
-// y = s D^-1 A x with s = 1 / ||x|| from the previous step (1 on the first), and per-block partial
-// sums of ||y||^2 on a fixed grid; k_amg_norm adds the partials in block order.
+// Each step y = s D^-1 A x with s = 1 / ||x|| from the previous step (1 on the first) writes
+// per-block partial sums of ||y||^2 on a fixed grid (k_amg_dinva_fine / _coarse, after the cycle
+// kernels); k_amg_norm adds the partials in block order.
 constexpr int kLamGrid = 148 * 8;
-
-template <int B>
-__global__ void __launch_bounds__(kThreads) k_amg_dinva(int n, AmgBsr A, const double* __restrict__ dinv,
-                                                        const double* sc, const double* __restrict__ x,
-                                                        double* __restrict__ y, double* __restrict__ part) {
-  const double s = sc ? *sc : 1.0;
-  double ss = 0.0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    double acc[B];
-#pragma unroll
-    for (int r = 0; r < B; ++r) acc[r] = 0.0;
-    const int k1 = __ldg(&A.ptr[i + 1]);
-    for (int k = __ldg(&A.ptr[i]); k < k1; ++k) {
-      const double* blk = A.val + (size_t)k * B * B;
-      const double* xj = x + (size_t)__ldg(&A.col[k]) * B;
-      double xv[B];
-#pragma unroll
-      for (int c = 0; c < B; ++c) xv[c] = xj[c];
-#pragma unroll
-      for (int r = 0; r < B; ++r)
-#pragma unroll
-        for (int c = 0; c < B; ++c) acc[r] = fma(__ldg(&blk[r * B + c]), xv[c], acc[r]);
-    }
-#pragma unroll
-    for (int r = 0; r < B; ++r) {
-      const double v = s * (dinv[(size_t)i * B + r] * acc[r]);
-      y[(size_t)i * B + r] = v;
-      ss = fma(v, v, ss);
-    }
-  }
-  __shared__ double sm[kWarps];
-  const double t = block_sum<kThreads>(ss, sm);
-  if (threadIdx.x == 0) part[blockIdx.x] = t;
-}
 
 // lam = sqrt(sum of the partials, in block order), sc = 1 / lam (one block)
 __global__ void __launch_bounds__(kThreads) k_amg_norm(const double* __restrict__ part, int nparts, double* lam,
@@ -1173,6 +1140,85 @@ __global__ void k_amg_rigid(int N, const double* __restrict__ xy, double* __rest
   b[5] = xy[2 * n];
 }
 
+// ---- lambda_max(D^-1 A) on the cycle's FP32 operators ---------------------------------------------------
+// The power-iteration step (y = s D^-1 A x, per-block partial sums of ||y||^2 on the fixed
+// kLamGrid grid) with the operators the smoother applies: the finest level's FP32 difference
+// form (thread per node) and a coarse level's entry-major FP32 copy (8 lanes per row).
+
+__global__ void __launch_bounds__(kThreads) k_amg_dinva_fine(MixedMatrix M, const double* __restrict__ dinv,
+                                                             const double* sc, const double* __restrict__ x,
+                                                             double* __restrict__ y, double* __restrict__ part) {
+  const double s = sc ? *sc : 1.0;
+  const double2* x2 = reinterpret_cast<const double2*>(x);
+  double ss = 0.0;
+  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < M.n_nodes; n += gridDim.x * blockDim.x) {
+    const int bb = __ldg(&M.node_ptr[n]);
+    const int o = bb - n, c = __ldg(&M.node_ptr[n + 1]) - bb - 1;
+    const double2 xs = x2[n];
+    double ya = 0.0, yb = 0.0;
+    for (int k = 0; k < c; ++k) {
+      const int m = __ldg(&M.nbr32[o + k]);
+      const float4 a = __ldg(&M.val32[o + k]);
+      const double2 xm = x2[m];
+      const double dx = xm.x - xs.x, dy = xm.y - xs.y;
+      ya = fma((double)a.x, dx, fma((double)a.y, dy, ya));
+      yb = fma((double)a.z, dx, fma((double)a.w, dy, yb));
+    }
+    const double2 sa = __ldg(&M.S64[2 * n]), sb = __ldg(&M.S64[2 * n + 1]);
+    ya = fma(sa.x, xs.x, fma(sa.y, xs.y, ya));
+    yb = fma(sb.x, xs.x, fma(sb.y, xs.y, yb));
+    const double2 dv = reinterpret_cast<const double2*>(dinv)[n];
+    const double va = s * (dv.x * ya), vb = s * (dv.y * yb);
+    reinterpret_cast<double2*>(y)[n] = make_double2(va, vb);
+    ss = fma(va, va, fma(vb, vb, ss));
+  }
+  __shared__ double sm[kWarps];
+  const double t = block_sum<kThreads>(ss, sm);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
+__global__ void __launch_bounds__(kThreads) k_amg_dinva_coarse(AmgBsr32 A, const double* __restrict__ dinv,
+                                                               const double* sc, const double* __restrict__ x,
+                                                               double* __restrict__ y, double* __restrict__ part) {
+  const double s = sc ? *sc : 1.0;
+  const size_t nb = (size_t)A.nnzb;
+  const int lane = threadIdx.x & 31, l8 = lane & 7, sub = lane >> 3;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+  double ss = 0.0;
+  for (int base = warp * 4; base < A.n; base += nw * 4) {
+    const int i = base + sub;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    if (i < A.n) {
+      const int k1 = __ldg(&A.ptr[i + 1]);
+      for (int k = __ldg(&A.ptr[i]) + l8; k < k1; k += 8) {
+        const int c = __ldg(&A.col[k]);
+        float v[9];
+#pragma unroll
+        for (int e = 0; e < 9; ++e) v[e] = __ldg(&A.val[(size_t)e * nb + k]);
+        const double x0 = x[3 * (size_t)c], x1 = x[3 * (size_t)c + 1], x2v = x[3 * (size_t)c + 2];
+        a0 = fma((double)v[0], x0, fma((double)v[1], x1, fma((double)v[2], x2v, a0)));
+        a1 = fma((double)v[3], x0, fma((double)v[4], x1, fma((double)v[5], x2v, a1)));
+        a2 = fma((double)v[6], x0, fma((double)v[7], x1, fma((double)v[8], x2v, a2)));
+      }
+    }
+#pragma unroll
+    for (int off = 4; off > 0; off >>= 1) {
+      a0 += __shfl_xor_sync(0xffffffffu, a0, off);
+      a1 += __shfl_xor_sync(0xffffffffu, a1, off);
+      a2 += __shfl_xor_sync(0xffffffffu, a2, off);
+    }
+    if (i < A.n && l8 < 3) {
+      const size_t d = 3 * (size_t)i + l8;
+      const double v = s * (dinv[d] * (l8 == 0 ? a0 : l8 == 1 ? a1 : a2));
+      y[d] = v;
+      ss = fma(v, v, ss);
+    }
+  }
+  __shared__ double sm[kWarps];
+  const double t = block_sum<kThreads>(ss, sm);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
 // One full wave of a grid-stride kernel: every SM gets as many blocks as it can hold at once
 // (capped by the work), so no partial second wave idles part of the GPU. The occupancy of each
 // kernel (256 threads, no dynamic shared memory) is queried once and cached.
@@ -1290,16 +1336,16 @@ cudaError_t amg_tentative(int B, int n_agg, const int* agg_ptr, const int* membe
   return cudaGetLastError();
 }
 
-cudaError_t amg_lambda(int B, const AmgBsr& A, const double* dinv, double* x, double* y, double* part, double* lam,
-                       int iters, cudaStream_t s) {
-  const int n = A.n * B;
+cudaError_t amg_lambda_f32(const MixedMatrix* fine, const AmgBsr32* coarse, const double* dinv, double* x, double* y,
+                           double* part, double* lam, int iters, cudaStream_t s) {
+  const int n = fine ? 2 * fine->n_nodes : 3 * coarse->n;
   double* sc = part + kLamGrid;  // the scale of the next step
   k_amg_init_vec<<<gw(n), 256, 0, s>>>(n, x);
   for (int t = 0; t < iters; ++t) {
-    if (B == 2)
-      k_amg_dinva<2><<<kLamGrid, kThreads, 0, s>>>(A.n, A, dinv, t ? sc : nullptr, x, y, part);
+    if (fine)
+      k_amg_dinva_fine<<<kLamGrid, kThreads, 0, s>>>(*fine, dinv, t ? sc : nullptr, x, y, part);
     else
-      k_amg_dinva<3><<<kLamGrid, kThreads, 0, s>>>(A.n, A, dinv, t ? sc : nullptr, x, y, part);
+      k_amg_dinva_coarse<<<kLamGrid, kThreads, 0, s>>>(*coarse, dinv, t ? sc : nullptr, x, y, part);
     k_amg_norm<<<1, kThreads, 0, s>>>(part, kLamGrid, lam, sc);
     std::swap(x, y);
   }

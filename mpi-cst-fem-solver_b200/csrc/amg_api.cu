@@ -130,8 +130,17 @@ int coarsen(cstg_ctx* ctx, AmgData* d, int l, bool* stop) {
   ENSURE(d->part, amg_lambda_scratch());
   ENSURE(d->vx, sizeof(double) * (size_t)n * B);
   ENSURE(d->vy, sizeof(double) * (size_t)n * B);
-  CK(amg_lambda(B, A, buf_ptr<double>(lv.dinv), buf_ptr<double>(d->vx), buf_ptr<double>(d->vy),
-                buf_ptr<double>(d->part), buf_ptr<double>(lv.lam), kPowerIters, ctx->stream));
+  // (on the FP32 operators the smoother applies: the finest level's difference form, else this
+  // level's entry-major copy, built with the Galerkin product of the level above)
+  if (l == 0) {
+    const MixedMatrix mm = mixed_view(ctx);
+    CK(amg_lambda_f32(&mm, nullptr, buf_ptr<double>(lv.dinv), buf_ptr<double>(d->vx), buf_ptr<double>(d->vy),
+                      buf_ptr<double>(d->part), buf_ptr<double>(lv.lam), kPowerIters, ctx->stream));
+  } else {
+    const AmgBsr32 a32 = lv.A32();
+    CK(amg_lambda_f32(nullptr, &a32, buf_ptr<double>(lv.dinv), buf_ptr<double>(d->vx), buf_ptr<double>(d->vy),
+                      buf_ptr<double>(d->part), buf_ptr<double>(lv.lam), kPowerIters, ctx->stream));
+  }
   // distance-2 maximal independent set
   CK(cudaMemsetAsync(d->state.p, 0, sizeof(int) * (size_t)n, ctx->stream));
   int und = n;

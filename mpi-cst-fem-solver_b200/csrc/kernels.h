@@ -50,6 +50,13 @@ struct CsrMatrixDev {  // generic scalar CSR (caller-supplied matrix)
 };
 
 // Solver state in device memory (scalars of the CG recurrence). 128-byte aligned.
+// Mixed precision: forced replacements count towards the FP32 accuracy floor only once the true
+// residual has fallen below this fraction of ||b|| (before that the CG residual may still rise).
+constexpr double kStallGate = 1e-2;
+// ... and a forced replacement whose true residual exceeds this multiple of the recursive one it
+// replaces shows the FP32 recursion moving on without the true residual.
+constexpr double kGapRatio = 1.5;
+
 struct alignas(128) PcgState {
   double rz;       // r'z of the current iterate
   double alpha, beta;
@@ -262,8 +269,11 @@ cudaError_t amg_group(int n, const int* key, int m, int* ptr, int* cnt, int* cur
                       cudaStream_t s);
 cudaError_t amg_tentative(int B, int n_agg, const int* agg_ptr, const int* members, const double* Bf, double* P0,
                           double* Bc, int* err, cudaStream_t s);
-cudaError_t amg_lambda(int B, const AmgBsr& A, const double* dinv, double* x, double* y, double* part, double* lam,
-                       int iters, cudaStream_t s);
+// lambda_max(D^-1 A) by `iters` power-iteration steps on the cycle's FP32 operators: the finest
+// level's difference form (fine) or a coarse level's entry-major copy (coarse); exactly one of
+// the two is given
+cudaError_t amg_lambda_f32(const MixedMatrix* fine, const AmgBsr32* coarse, const double* dinv, double* x, double* y,
+                           double* part, double* lam, int iters, cudaStream_t s);
 size_t amg_lambda_scratch();  // bytes of `part` that amg_lambda needs
 cudaError_t amg_p_count(int B, const AmgBsr& A, const int* agg, int* cnt, int* err, cudaStream_t s);
 cudaError_t amg_p_fill(int B, const AmgBsr& A, const int* agg, const double* P0, const double* dinv, const double* lam,

@@ -295,10 +295,12 @@ __global__ void __launch_bounds__(kThreads) k_update_mixed(int N, double* __rest
     st->rmax = fmax(st->rmax, rn);
     if (rel < st->rtol)
       st->restart_pending = 2;  // confirm on the FP64 true residual
-    else if (rn < st->delta * st->rmax)
+    else if (!st->fp64_mode && rn < st->delta * st->rmax)
       st->restart_pending = 1;  // reliable update
-    else if (it - st->last_replace >= st->cycle_limit)
-      st->restart_pending = 3;  // a long cycle: replace anyway (bounds the drift)
+    else if (!st->fp64_mode && it - st->last_replace >= st->cycle_limit)
+      st->restart_pending = 3;  // a long cycle: replace anyway (bounds the FP32 operator's drift)
+    // (after the switch to FP64 the iteration is plain FP64 CG: replacements at its accuracy
+    // limit break the conjugacy of p and made the recursion drift from x, measured at 8M DOFs)
     else if (it >= st->max_iter)
       st->done = CSTG_SOLVE_MAX_ITER + 1;
     st->rz_prev = st->rz;
@@ -355,6 +357,7 @@ __global__ void __launch_bounds__(kThreads) k_replace_mixed(BlockMatrix A, const
     const double rn = sqrt(tot[0]);
     const double tr = rn / st->bnorm;
     const int kind = st->restart_pending;
+    const double rec = st->rel;  // the recursive residual this replacement corrects
     st->true_rel = tr;
     st->rel = tr;
     st->rr = tot[0];
@@ -370,17 +373,23 @@ __global__ void __launch_bounds__(kThreads) k_replace_mixed(BlockMatrix A, const
       st->done = CSTG_SOLVE_CONVERGED + 1;
     } else {
       // Precision switch: the recursive residual met rtol but the FP64 true residual did not
-      // (or a delta cycle did not halve the true residual, or, within 1e4 x rtol, two forced
-      // replacements in a row found it no lower than 0.9 of its best — farther out such cycles
-      // are the early rise of the CG residual, not a floor): the FP32 operator has reached its
-      // accuracy floor, so the remaining iterations use the FP64 matrix.
+      // (or a delta cycle did not halve the true residual, or, below kStallGate, two forced
+      // replacements in a row found it no lower than 0.9 of its best or above kGapRatio times the
+      // recursive residual it replaced — the FP32 recursion still converges while the true
+      // residual does not; above kStallGate such cycles are the early rise of the CG residual):
+      // the FP32 operator has reached its accuracy floor, so the remaining iterations use the
+      // FP64 matrix.
       if (kind == 3)
-        st->stall_cycles = (tr > 0.9 * st->best_true && st->best_true < 1e4 * st->rtol) ? st->stall_cycles + 1 : 0;
+        st->stall_cycles = ((tr > 0.9 * st->best_true || tr > kGapRatio * rec) && st->best_true < kStallGate)
+                               ? st->stall_cycles + 1
+                               : 0;
       if (!st->fp64_mode && (kind == 2 || (kind == 1 && tr > 0.5 * st->best_true) ||
                                 (kind == 3 && st->stall_cycles >= 2))) {
         st->fp64_mode = 1;
         st->fp64_switch_iter = st->iter;
         st->beta = 0.0;  // restart the direction: p = D^-1 r, plain FP64 CG from here
+      } else if (st->fp64_mode) {
+        st->beta = 0.0;  // an FP64 confirmation that missed: restart from the true residual
       }
       if (kind == 2 && ++st->final_checks > max_final_checks) st->done = CSTG_SOLVE_CONVERGED + 1;
       if (st->iter >= st->max_iter) st->done = CSTG_SOLVE_MAX_ITER + 1;

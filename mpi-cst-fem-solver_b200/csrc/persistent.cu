@@ -314,10 +314,10 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PersistArgs a) {
               st->rmax = fmax(st->rmax, rn);
               if (rel < st->rtol)
                 st->restart_pending = 2;
-              else if (rn < st->delta * st->rmax)
+              else if (!st->fp64_mode && rn < st->delta * st->rmax)
                 st->restart_pending = 1;
-              else if (it - st->last_replace >= st->cycle_limit)
-                st->restart_pending = 3;
+              else if (!st->fp64_mode && it - st->last_replace >= st->cycle_limit)
+                st->restart_pending = 3;  // (plain FP64 CG after the switch, as in mixed_kernels.cu)
               else if (it >= st->max_iter)
                 st->done = CSTG_SOLVE_MAX_ITER + 1;
             }
@@ -337,6 +337,7 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PersistArgs a) {
             const double rn = sqrt(tot[0]);
             const double tr = rn / st->bnorm;
             const int kind = st->restart_pending;
+            const double rec = st->rel;  // the recursive residual this replacement corrects
             st->true_rel = tr;
             st->rel = tr;
             st->rr = tot[0];
@@ -353,11 +354,15 @@ __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PersistArgs a) {
               // (the precision switch of mixed_kernels.cu's k_replace_mixed, same rule)
               if (kind == 3)
                 st->stall_cycles =
-                    (tr > 0.9 * st->best_true && st->best_true < 1e4 * st->rtol) ? st->stall_cycles + 1 : 0;
+                    ((tr > 0.9 * st->best_true || tr > kGapRatio * rec) && st->best_true < kStallGate)
+                        ? st->stall_cycles + 1
+                        : 0;
               if (!st->fp64_mode && (kind == 2 || (kind == 1 && tr > 0.5 * st->best_true) ||
                                 (kind == 3 && st->stall_cycles >= 2))) {
                 st->fp64_mode = 1;
                 st->fp64_switch_iter = st->iter;
+                st->beta = 0.0;
+              } else if (st->fp64_mode) {
                 st->beta = 0.0;
               }
               if (kind == 2 && ++st->final_checks > a.max_final_checks) st->done = CSTG_SOLVE_CONVERGED + 1;
