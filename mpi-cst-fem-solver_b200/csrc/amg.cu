@@ -821,16 +821,57 @@ __device__ __forceinline__ double first_x(double a0, const double* __restrict__ 
   return a0 * dinv[i] * b[i];
 }
 
+// The flexible-CG scalars that follow a cycle (k_fcg_dots of fcg.cu), taken in the cycle's last
+// finest-level sweep, which already holds z (its output) and r (its right-hand side): z'r and
+// z'q reduced on the sweep's fixed grid (per-block partials, the last block by ticket adds them
+// in block order), then beta = -alpha z'q / (z'r)_old (Polak-Ribiere; a restart or a non-descent
+// z gives beta = 0). The cycle is symmetric positive, so the Jacobi fallback of the learned
+// network is not needed here.
+__device__ __forceinline__ void fcg_dots_epilogue(double zr, double zq, const FcgDotSink& d) {
+  __shared__ double sm[kWarps];
+  __shared__ bool am_last;
+  const double a = block_sum<kThreads>(zr, sm);
+  const double c = block_sum<kThreads>(zq, sm);
+  if (threadIdx.x == 0) {
+    d.partials[blockIdx.x] = a;
+    d.partials[gridDim.x + blockIdx.x] = c;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) am_last = atomicAdd(&d.st->ticket[6], 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!am_last) return;
+  __threadfence();
+  double s0 = 0.0, s1 = 0.0;
+  for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) {
+    s0 += __ldcg(&d.partials[i]);
+    s1 += __ldcg(&d.partials[gridDim.x + i]);
+  }
+  const double t0 = block_sum<kThreads>(s0, sm);
+  const double t1 = block_sum<kThreads>(s1, sm);
+  if (threadIdx.x == 0) {
+    PcgState* st = d.st;
+    const bool restart = st->restart_pending != 0 || !(t0 > 0.0);
+    st->beta = (!restart && st->rz > 0.0) ? -st->alpha * t1 / st->rz : 0.0;
+    st->rz = t0;
+    st->use_jacobi = 0;
+    st->restart_pending = 0;
+    st->ticket[6] = 0u;
+  }
+}
+
 // Finest-level sweep on the FP32 difference-form operator of mixed_kernels.cu (the smoother is a
 // preconditioner: FP32 matrix values, FP64 vectors and accumulation). Thread per node; four
 // neighbours' index and value loads are in flight at once, their gathers next, and the additions
-// follow in neighbour order.
-template <int MODE>
+// follow in neighbour order. DOTS: the cycle's last sweep inside flexible CG also takes z'r and
+// z'q (fcg_dots_epilogue).
+template <int MODE, bool DOTS = false>
 __global__ void __launch_bounds__(256) k_amg_sweep_f32(const int* skip, MixedMatrix M, const double* __restrict__ dinv,
                                                        const double* __restrict__ lam, int cheb,
                                                        const double* __restrict__ b, const double* __restrict__ x,
-                                                       const double* xp, double* xo) {
+                                                       const double* xp, double* xo, FcgDotSink dots) {
   if (skipped(skip)) return;
+  double zr = 0.0, zq = 0.0;
   const SweepCoef cf = sweep_coef<MODE>(lam, cheb);
   const double2* x2 = reinterpret_cast<const double2*>(x);
   auto xnode = [&](int m) -> double2 {
@@ -884,7 +925,13 @@ __global__ void __launch_bounds__(256) k_amg_sweep_f32(const int* skip, MixedMat
       out = make_double2(sweep_out<MODE>(cf, dv.x, ra, xs.x, pv.x), sweep_out<MODE>(cf, dv.y, rbv, xs.y, pv.y));
     }
     reinterpret_cast<double2*>(xo)[n] = out;
+    if (DOTS) {
+      const double2 qv = reinterpret_cast<const double2*>(dots.q)[n];
+      zr = fma(out.x, bv.x, fma(out.y, bv.y, zr));
+      zq = fma(out.x, qv.x, fma(out.y, qv.y, zq));
+    }
   }
+  if (DOTS) fcg_dots_epilogue(zr, zq, dots);
 }
 
 // Loads of vectors: COH = false for standalone launches (the vector was written by an earlier
@@ -1454,32 +1501,34 @@ void amg_prepare_launch_shapes() {
   one_wave((const void*)k_amg_sweep_f32<kSweepFirst>, 1);
   one_wave((const void*)k_amg_sweep_f32<kSweepSecond>, 1);
   one_wave((const void*)k_amg_sweep_f32<kSweepSmooth>, 1);
+  one_wave((const void*)k_amg_sweep_f32<kSweepSecond, true>, 1);
+  one_wave((const void*)k_amg_sweep_f32<kSweepSmooth, true>, 1);
   one_wave((const void*)k_amg_restrict_f32<2>, 1);
   one_wave((const void*)k_amg_prolong_f32<2>, 1);
 }
 
 cudaError_t amg_sweep_f32(const int* skip, int mode, int cheb, const MixedMatrix& M, const double* dinv,
                           const double* lam, const double* b, const double* x, const double* xp, double* xo,
-                          cudaStream_t s) {
+                          cudaStream_t s, const FcgDotSink* dots) {
   const long long t = M.n_nodes;
-  switch (mode) {
-    case kSweepResidual:
-      k_amg_sweep_f32<kSweepResidual><<<one_wave((const void*)k_amg_sweep_f32<kSweepResidual>, t), 256, 0, s>>>(
-          skip, M, dinv, lam, cheb, b, x, xp, xo);
-      break;
-    case kSweepFirst:
-      k_amg_sweep_f32<kSweepFirst><<<one_wave((const void*)k_amg_sweep_f32<kSweepFirst>, t), 256, 0, s>>>(skip, M, dinv, lam, cheb,
-                                                                                             b, x, xp, xo);
-      break;
-    case kSweepSecond:
-      k_amg_sweep_f32<kSweepSecond><<<one_wave((const void*)k_amg_sweep_f32<kSweepSecond>, t), 256, 0, s>>>(
-          skip, M, dinv, lam, cheb, b, x, xp, xo);
-      break;
-    default:
-      k_amg_sweep_f32<kSweepSmooth><<<one_wave((const void*)k_amg_sweep_f32<kSweepSmooth>, t), 256, 0, s>>>(
-          skip, M, dinv, lam, cheb, b, x, xp, xo);
-      break;
-  }
+  const FcgDotSink d = dots ? *dots : FcgDotSink{};
+  auto go = [&](auto kern) {
+    kern<<<one_wave((const void*)kern, t), 256, 0, s>>>(skip, M, dinv, lam, cheb, b, x, xp, xo, d);
+  };
+  if (dots && mode == kSweepSecond)
+    go(k_amg_sweep_f32<kSweepSecond, true>);
+  else if (dots && mode == kSweepSmooth)
+    go(k_amg_sweep_f32<kSweepSmooth, true>);
+  else if (dots)
+    return cudaErrorInvalidValue;  // the dots ride on a cycle's last (smoothing) sweep only
+  else if (mode == kSweepResidual)
+    go(k_amg_sweep_f32<kSweepResidual>);
+  else if (mode == kSweepFirst)
+    go(k_amg_sweep_f32<kSweepFirst>);
+  else if (mode == kSweepSecond)
+    go(k_amg_sweep_f32<kSweepSecond>);
+  else
+    go(k_amg_sweep_f32<kSweepSmooth>);
   count_launches(1);
   return cudaGetLastError();
 }

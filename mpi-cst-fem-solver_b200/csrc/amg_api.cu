@@ -365,7 +365,9 @@ int amg_build(cstg_ctx* ctx) {
 }
 
 // V(2,2): x = cycle(l, b)
-int vcycle(cstg_ctx* ctx, AmgData* d, size_t l, const double* b, double* x, const int* skip) {
+// dots (finest level only, may be null): the flexible-CG scalars, taken in the last sweep
+int vcycle(cstg_ctx* ctx, AmgData* d, size_t l, const double* b, double* x, const int* skip,
+           const FcgDotSink* dots) {
   AmgLevel& lv = d->L[l];
   cudaStream_t s = ctx->stream;
   if ((int)l + 1 == d->nl) {
@@ -388,23 +390,25 @@ int vcycle(cstg_ctx* ctx, AmgData* d, size_t l, const double* b, double* x, cons
   const MixedMatrix mm = fine ? mixed_view(ctx) : MixedMatrix{};
   const AmgBsr32 A32 = lv.A32();
   const int cheb = d->cheb;
-  auto sweep = [&](int mode, const double* xin, const double* xp, double* xout) -> cudaError_t {
-    return fine ? amg_sweep_f32(skip, mode, cheb, mm, dinv, lam, b, xin, xp, xout, s)
+  auto sweep = [&](int mode, const double* xin, const double* xp, double* xout,
+                   const FcgDotSink* dk = nullptr) -> cudaError_t {
+    return fine ? amg_sweep_f32(skip, mode, cheb, mm, dinv, lam, b, xin, xp, xout, s, dk)
                 : amg_sweep3_f32(skip, mode, cheb, A32, dinv, lam, b, xin, xp, xout, s);
   };
   CK(sweep(kSweepFirst, nullptr, nullptr, x));  // two pre-smoothing steps from x = 0
   CK(sweep(kSweepResidual, x, nullptr, r));
   CK(amg_restrict_f32(skip, lv.B, lv.nc, buf_ptr<int>(lv.pt_ptr), buf_ptr<int>(lv.pt_row), buf_ptr<float>(lv.pt32), r,
                       buf_ptr<double>(nx.bc), s));
-  const int rc = vcycle(ctx, d, l + 1, buf_ptr<double>(nx.bc), buf_ptr<double>(nx.xb), skip);
+  const int rc = vcycle(ctx, d, l + 1, buf_ptr<double>(nx.bc), buf_ptr<double>(nx.xb), skip, nullptr);
   if (rc) return rc;
   CK(amg_prolong_f32(skip, lv.B, lv.n, buf_ptr<int>(lv.p_ptr), buf_ptr<int>(lv.p_col), buf_ptr<float>(lv.p32),
                      buf_ptr<double>(nx.xb), x, s));
   CK(sweep(kSweepSmooth, x, nullptr, xa));  // two post-smoothing steps
+  const FcgDotSink* dk = fine ? dots : nullptr;
   if (cheb)
-    CK(sweep(kSweepSecond, xa, x, x));  // (the previous iterate x is read at each node before it is overwritten)
+    CK(sweep(kSweepSecond, xa, x, x, dk));  // (the previous iterate x is read at each node before it is overwritten)
   else
-    CK(sweep(kSweepSmooth, xa, nullptr, x));
+    CK(sweep(kSweepSmooth, xa, nullptr, x, dk));
   return CSTG_OK;
 }
 
@@ -444,8 +448,8 @@ unsigned long long cstg_host::amg_signature(const cstg_ctx* ctx) {
   return h;
 }
 
-int cstg_host::amg_apply(cstg_ctx* ctx, const double* r, double* z, const int* skip) {
-  return vcycle(ctx, ctx->amg, 0, r, z, skip);
+int cstg_host::amg_apply(cstg_ctx* ctx, const double* r, double* z, const int* skip, const FcgDotSink* dots) {
+  return vcycle(ctx, ctx->amg, 0, r, z, skip, ctx->amg->nl > 1 ? dots : nullptr);
 }
 
 extern "C" {
@@ -526,7 +530,7 @@ int cstg_amg_time(cstg_ctx* ctx, int reps, double* out) {
   for (int w = 0; w < 2; ++w) {
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
     for (int k = 0; k < reps; ++k) {
-      const int rc2 = vcycle(ctx, d, 0, b, xb, nullptr);
+      const int rc2 = vcycle(ctx, d, 0, b, xb, nullptr, nullptr);
       if (rc2) return rc2;
     }
     CK(cudaEventRecord(ctx->ev1, ctx->stream));

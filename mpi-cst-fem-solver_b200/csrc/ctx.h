@@ -254,7 +254,9 @@ inline void g_fmt(char* out, size_t n, const char* fmt, ...) {
 
 // Defined in amg_api.cu: the multigrid hierarchy (built when missing or stale) and z = M r.
 int amg_ready(cstg_ctx* ctx);
-int amg_apply(cstg_ctx* ctx, const double* r, double* z, const int* skip);  // skip: see amg_sweep_f32
+// skip: see amg_sweep_f32; dots (may be null): take the flexible-CG scalars in the cycle's last
+// sweep (only with two or more levels: a one-level hierarchy is the dense solve alone)
+int amg_apply(cstg_ctx* ctx, const double* r, double* z, const int* skip, const FcgDotSink* dots = nullptr);
 void amg_free(cstg_ctx* ctx);
 int amg_levels(const cstg_ctx* ctx);
 int amg_chebyshev(const cstg_ctx* ctx);  // 1: Chebyshev smoothing, 0: damped Jacobi

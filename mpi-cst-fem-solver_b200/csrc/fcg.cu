@@ -190,6 +190,12 @@ cudaError_t launch_fcg_dots(const FcgBuffers& w, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+cudaError_t launch_fcg_pupdate(const FcgBuffers& w, cudaStream_t s) {
+  k_fcg_pupdate<<<kGrid, kThreads, 0, s>>>(w.n, w.z, w.r, w.inv_diag, w.p, w.st);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_fcg_update(const FcgBuffers& w, int window, double ratio2, cudaStream_t s) {
   k_fcg_update<<<kGrid, kThreads, 0, s>>>(w.n, w.x, w.r, w.p, w.q, w.partials, w.st, window, ratio2);
   count_launches(1);

@@ -226,6 +226,7 @@ struct FcgBuffers {
 cudaError_t launch_fcg_init(const FcgBuffers& w, double rtol, int max_iter, int window, cudaStream_t s);
 cudaError_t launch_fcg_dots(const FcgBuffers& w, cudaStream_t s);  // beta, r'z; then p = z + beta p
 cudaError_t launch_fcg_update(const FcgBuffers& w, int window, double ratio2, cudaStream_t s);
+cudaError_t launch_fcg_pupdate(const FcgBuffers& w, cudaStream_t s);  // p = z + beta p alone
 // q = A p with p'Ap and alpha = r'z / p'Ap (the PCG variants of the SpMVs)
 cudaError_t launch_spmv_pcg(const BlockMatrix& A, const double* p, double* q, double* partials, PcgState* st,
                             cudaStream_t s);
@@ -293,9 +294,16 @@ cudaError_t amg_coarsest(int B, const AmgBsr& A, double* M, double* piv, cudaStr
 constexpr int kSweepSmooth = 0, kSweepResidual = 1, kSweepFirst = 2, kSweepSecond = 3;
 void amg_prepare_launch_shapes();  // occupancy queries of the one-wave launches (call outside a capture)
 // skip (all cycle launchers): a device flag; non-zero makes the launch return at once (may be null)
+// dots (may be null): the flexible-CG scalars taken in this sweep (its output is z, its b is r):
+// z'r and z'q reduced into partials (2 x grid doubles) with st->ticket[6], then beta and r'z in st
+struct FcgDotSink {
+  const double* q = nullptr;
+  double* partials = nullptr;
+  PcgState* st = nullptr;
+};
 cudaError_t amg_sweep_f32(const int* skip, int mode, int cheb, const MixedMatrix& M, const double* dinv,
                           const double* lam, const double* b, const double* x, const double* xp, double* xo,
-                          cudaStream_t s);
+                          cudaStream_t s, const FcgDotSink* dots = nullptr);
 // cycle operators in FP32 (values only; vectors and accumulation stay FP64)
 cudaError_t amg_coarse_f32(const AmgBsr& A, float* val32, cudaStream_t s);
 cudaError_t amg_transfer_f32(int B, const AmgBsr& P, int nnz_p, const int* pt_idx, const int* p_row, float* p32,

@@ -95,20 +95,34 @@ int cstg_host::run_fcg(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg
   const int* skip = &w.st->mp_skip;
   const double* rr = &w.st->rr;
 
+  // With the multigrid cycle the scalars z'r, z'q and beta are taken inside the cycle's last
+  // finest-level sweep (no separate dots pass), and there is no stagnation fallback (the cycle is
+  // a fixed symmetric positive operator).
+  const bool fused_dots = use_amg && amg_levels(ctx) > 1;
+  FcgDotSink sink;
+  sink.q = w.q;
+  sink.partials = w.partials;
+  sink.st = w.st;
+  auto precondition = [&]() -> int {
+    if (use_amg) {
+      const int rc = amg_apply(ctx, w.r, w.z, &w.st->done, fused_dots ? &sink : nullptr);  // (cycles after
+      if (rc) return rc;                                                                   // convergence return at once)
+    } else {
+      CK(launch_mp_forward(g, P, w.r, w.inv_diag, rr, sf, skip, mw, false, w.z, err, ctx->stream));
+    }
+    if (fused_dots)
+      CK(launch_fcg_pupdate(w, ctx->stream));
+    else
+      CK(launch_fcg_dots(w, ctx->stream));
+    return CSTG_OK;
+  };
   auto iteration = [&]() -> int {
     if (mixed)
       CK(launch_spmv_mixed_pcg(mm, bm, w.p, w.q, w.partials, w.st, ctx->stream));
     else
       CK(launch_spmv_pcg(bm, w.p, w.q, w.partials, w.st, ctx->stream));
-    CK(launch_fcg_update(w, kFcgWindow, kFcgRatio2, ctx->stream));
-    if (use_amg) {
-      const int rc = amg_apply(ctx, w.r, w.z, &w.st->done);  // (cycles after convergence return at once)
-      if (rc) return rc;
-    } else {
-      CK(launch_mp_forward(g, P, w.r, w.inv_diag, rr, sf, skip, mw, false, w.z, err, ctx->stream));
-    }
-    CK(launch_fcg_dots(w, ctx->stream));
-    return CSTG_OK;
+    CK(launch_fcg_update(w, use_amg ? 0 : kFcgWindow, kFcgRatio2, ctx->stream));
+    return precondition();
   };
   const int chunk = o.check_interval > 0 ? o.check_interval : 25;
   // the captured chunk depends on the buffers (generation), the shapes and the method
@@ -149,13 +163,10 @@ int cstg_host::run_fcg(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg
   int zero = 0;
   CK(cudaMemcpyAsync(&w.st->fp64_mode, &zero, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
   CK(launch_fcg_init(w, o.rtol, o.max_iter, kFcgWindow, ctx->stream));
-  if (use_amg) {
-    const int rc = amg_apply(ctx, w.r, w.z, &w.st->done);
+  {
+    const int rc = precondition();
     if (rc) return rc;
-  } else {
-    CK(launch_mp_forward(g, P, w.r, w.inv_diag, rr, sf, skip, mw, false, w.z, err, ctx->stream));
   }
-  CK(launch_fcg_dots(w, ctx->stream));
   CK(cudaMemcpyAsync(ctx->h_state, ctx->state.p, sizeof(PcgState), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   PcgBuffers pw;  // the true-residual kernel's view
