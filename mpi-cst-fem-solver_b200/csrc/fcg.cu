@@ -131,7 +131,25 @@ __global__ void __launch_bounds__(kThreads) k_fcg_pupdate(int n, const double* _
   if (__ldcg(&st->done)) return;
   const double beta = __ldcg(&st->beta);
   const bool jac = __ldcg(&st->use_jacobi) != 0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  // pairs of DOFs (16-byte loads); an odd last row on its own
+  const int n2 = n >> 1;
+  const double2* z2 = reinterpret_cast<const double2*>(z);
+  const double2* r2 = reinterpret_cast<const double2*>(r);
+  const double2* d2 = reinterpret_cast<const double2*>(invd);
+  double2* p2 = reinterpret_cast<double2*>(p);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n2; i += gridDim.x * blockDim.x) {
+    double2 zi;
+    if (jac) {
+      const double2 ri = r2[i], di = d2[i];
+      zi = make_double2(di.x * ri.x, di.y * ri.y);
+    } else {
+      zi = z2[i];
+    }
+    const double2 pi = p2[i];
+    p2[i] = make_double2(fma(beta, pi.x, zi.x), fma(beta, pi.y, zi.y));
+  }
+  if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+    const int i = n - 1;
     const double zi = jac ? invd[i] * r[i] : z[i];
     p[i] = fma(beta, p[i], zi);
   }
@@ -145,7 +163,25 @@ __global__ void __launch_bounds__(kThreads) k_fcg_update(int n, double* __restri
   if (__ldcg(&st->done)) return;
   const double alpha = __ldcg(&st->alpha);
   double rr = 0.0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  // pairs of DOFs (16-byte loads); an odd last row on its own
+  const int n2 = n >> 1;
+  double2* x2 = reinterpret_cast<double2*>(x);
+  double2* r2 = reinterpret_cast<double2*>(r);
+  const double2* p2 = reinterpret_cast<const double2*>(p);
+  const double2* q2 = reinterpret_cast<const double2*>(q);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n2; i += gridDim.x * blockDim.x) {
+    const double2 pi = p2[i], qi = q2[i];
+    double2 xi = x2[i], ri = r2[i];
+    xi.x = fma(alpha, pi.x, xi.x);
+    xi.y = fma(alpha, pi.y, xi.y);
+    ri.x = fma(-alpha, qi.x, ri.x);
+    ri.y = fma(-alpha, qi.y, ri.y);
+    x2[i] = xi;
+    r2[i] = ri;
+    rr = fma(ri.x, ri.x, fma(ri.y, ri.y, rr));
+  }
+  if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+    const int i = n - 1;
     x[i] = fma(alpha, p[i], x[i]);
     const double ri = fma(-alpha, q[i], r[i]);
     r[i] = ri;
