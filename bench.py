@@ -621,7 +621,7 @@ def run_ours(a, dist: Dist):
                "setup_s": info["setup_seconds"], "vcycle_us": tm["vcycle_s"] * 1e6,
                "cycle": f"V(2,2), {a.amg_smoother} smoothing, FP32 cycle operators, dense coarsest inverse",
                "tail": {"level": info["tail_level"], "cluster_ctas": info["tail_cluster"]},
-               "smoother_roofline": roof("k_amg_sweep_f32 (finest-level damped Jacobi sweep)", sweep_bytes,
+               "smoother_roofline": roof("k_amg_sweep_f32 (finest-level smoothing step)", sweep_bytes,
                                          tm["sweep_s"],
                                          profile_traffic("amg_sweep_f32_plate2m.md") if full else None)}
         roofline = amg["smoother_roofline"]
