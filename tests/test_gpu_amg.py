@@ -152,3 +152,29 @@ def test_amg_chebyshev_beats_jacobi_smoothing(pkg, gpu_lib):
         its[kind] = st.iterations
     assert its["chebyshev"] < 0.9 * its["jacobi"], its
     K.ctx.close()
+
+
+def test_amg_random_plates(pkg, gpu_lib):
+    """Seeded plates of the uneven-size batch workload (hole radius, modulus, Poisson ratio, plane
+    stress or strain, each of the four load cases) all reach the FP64 Jacobi-PCG solution."""
+    specs = pkg.plate.random_batch(count=4, seed=7, n_r_range=(20, 60))
+    for k, (spec, case) in enumerate(zip(specs, sorted(pkg.plate.LOAD_CASES))):
+        m = pkg.plate.quarter_plate(spec.n_r, spec.n_theta, a=spec.a)
+        K = pkg.build_stiffness_pattern(m)
+        plane = pkg.PlaneCondition.Strain if spec.plane_strain else pkg.PlaneCondition.Stress
+        pkg.assemble_stiffness(m, pkg.constitutive_matrix(spec.E, spec.nu, plane), 1.0, K)
+        b = np.zeros(m.num_dofs)
+        for group, tx, ty in pkg.plate.LOAD_CASES[case]:
+            pkg.add_traction(K, m.boundary_edges[group], 1.0, tx, ty, b)
+        pkg.apply_dirichlet(pkg.plate.symmetry_dirichlet(m), K, b)
+        ref = pkg.CgJacobiSolver(pkg.SolverOptions(rtol=1e-12, max_iter=100000))
+        ref.setup(K)
+        x_ref = np.zeros(m.num_dofs)
+        assert ref.solve(b, x_ref).converged
+        s = pkg.CgJacobiSolver(_amg("mixed" if k % 2 else "fp64"))
+        s.setup(K)
+        x = np.zeros(m.num_dofs)
+        st = s.solve(b, x)
+        assert st.converged and st.true_rel_residual <= 1e-10, (spec, case, st.message)
+        assert _rel(x, x_ref) < REL_TOL, (spec, case)
+        K.ctx.close()
