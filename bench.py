@@ -68,6 +68,8 @@ def parse():
                          "Jacobi (the reference's method, persistent kernel) or the learned network")
     ap.add_argument("--amg-smoother", default="chebyshev", choices=["chebyshev", "jacobi"],
                     help="smoother of the multigrid cycle")
+    ap.add_argument("--amg-theta", type=float, nargs=2, default=[0.0, 0.03], metavar=("FINE", "COARSE"),
+                    help="strength-of-connection thresholds of the multigrid aggregation")
     ap.add_argument("--precision", default=None, choices=["fp64", "mixed"],
                     help="outer CG precision; default fp64 with amg (its finest smoother is FP32 already), "
                          "mixed otherwise")
@@ -379,6 +381,7 @@ def run_ours(a, dist: Dist):
     ctx.set_stream(stream)
     smoother_code = {"chebyshev": pkg.native.AMG_CHEBYSHEV, "jacobi": pkg.native.AMG_JACOBI}[a.amg_smoother]
     ctx.check(ctx.L.cstg_amg_set_smoother(ctx.h, smoother_code))
+    ctx.check(ctx.L.cstg_amg_set_strength(ctx.h, *a.amg_theta))
     # loads on the host (bc.cpp:190-253) once; the step starts from them
     ctx.set_mesh(mesh)
     b0 = np.zeros(n)
@@ -620,6 +623,7 @@ def run_ours(a, dist: Dist):
         amg = {"levels": info["levels"], "level_dofs": info["dofs"], "level_nnz": info["nnz"],
                "setup_s": info["setup_seconds"], "vcycle_us": tm["vcycle_s"] * 1e6,
                "cycle": f"V(2,2), {a.amg_smoother} smoothing, FP32 cycle operators, dense coarsest inverse",
+               "strength_theta": {"fine": a.amg_theta[0], "coarse": a.amg_theta[1]},
                "tail": {"level": info["tail_level"], "cluster_ctas": info["tail_cluster"]},
                "smoother_roofline": roof("k_amg_sweep_f32 (finest-level smoothing step)", sweep_bytes,
                                          tm["sweep_s"],
@@ -685,6 +689,7 @@ def run_ours(a, dist: Dist):
         h_x = pinned(np.zeros(n))
         ectx = pkg.Context(dev)
         ectx.check(ectx.L.cstg_amg_set_smoother(ectx.h, smoother_code))
+        ectx.check(ectx.L.cstg_amg_set_strength(ectx.h, *a.amg_theta))
 
         def e2e_step():
             K2 = pkg.build_stiffness_pattern(hmesh, ctx=ectx)

@@ -344,7 +344,7 @@ int cstg_mesh_group(const cstg_mesh* mesh, int index, char* name, int name_len, 
 
 /* ---- multigrid preconditioner -------------------------------------------------------------------
  * No counterpart in the reference. Smoothed aggregation on the GPU: distance-2 MIS aggregates of
- * the node graph, tentative prolongator from the 2D rigid-body modes (per-aggregate QR), one
+ * the node graph (on coarse levels, of its strong connections: cstg_amg_set_strength), tentative prolongator from the 2D rigid-body modes (per-aggregate QR), one
  * damped-Jacobi prolongator smoothing step, Galerkin coarse operators (3 x 3 blocks), dense
  * inverse of the coarsest level; the preconditioner is one V(2,2) cycle with Chebyshev smoothing
  * (or damped Jacobi, cstg_amg_set_smoother; lambda_max(D^-1 A) by power iteration). Deterministic. Used by
@@ -374,6 +374,10 @@ int cstg_amg_set_tail(cstg_ctx* ctx, int enable);
 #define CSTG_AMG_CHEBYSHEV 0
 #define CSTG_AMG_JACOBI 1
 int cstg_amg_set_smoother(cstg_ctx* ctx, int kind);
+/* Strength-of-connection thresholds of the aggregation, on the finest level and on the coarser
+ * levels (each in [0, 1); default 0 and 0.03): block (i, j) joins the aggregation graph when
+ * ||A_ij||_F >= theta sqrt(||A_ii||_F ||A_jj||_F). A change rebuilds the hierarchy on next use. */
+int cstg_amg_set_strength(cstg_ctx* ctx, double theta_fine, double theta_coarse);
 
 #ifdef __cplusplus
 }

@@ -11,7 +11,7 @@ from . import batch, build, learned, mesh_io, native, plate  # noqa: F401
 from .mesh_io import read_gmsh, write_gmsh  # noqa: F401
 from .native import CstgError, LogicError  # noqa: F401
 from .batch import BatchSolution, BatchSolver, PlateBatch, build_batch  # noqa: F401
-from .solver import amg_apply, amg_set_smoother, amg_set_tail, amg_setup, amg_time  # noqa: F401
+from .solver import amg_apply, amg_set_smoother, amg_set_strength, amg_set_tail, amg_setup, amg_time  # noqa: F401
 from .solver import (CgJacobiSolver, Context, DirichletDofs, GpuCsrMatrix,  # noqa: F401
                      PlaneCondition, SolverOptions, SolverStats, add_dirichlet_group,
                      add_kirsch_traction, add_traction, apply_dirichlet, assemble_stiffness, build_stiffness_pattern,

@@ -108,39 +108,75 @@ __global__ void k_amg_dinv(int n, AmgBsr A, double* __restrict__ dinv, int* err)
 
 // ---- aggregation ----------------------------------------------------------------------------------
 
-__global__ void k_mis_m1(int n, AmgBsr A, const int* __restrict__ state, unsigned long long* __restrict__ m1) {
+// Strength of connection (the graph the aggregation walks): block (i, j) is strong when
+// ||A_ij||_F >= theta sqrt(||A_ii||_F ||A_jj||_F); diagonal blocks always are. strong == nullptr
+// (theta 0) keeps every block of the pattern.
+template <int B>
+__global__ void k_amg_diag_norm(int n, AmgBsr A, double* __restrict__ dn) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double s = 0.0;
+  for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k)
+    if (A.col[k] == i) {
+      const double* blk = A.val + (size_t)k * B * B;
+      for (int q = 0; q < B * B; ++q) s += blk[q] * blk[q];
+    }
+  dn[i] = sqrt(s);
+}
+
+template <int B>
+__global__ void k_amg_strength(int n, AmgBsr A, const double* __restrict__ dn, double theta,
+                               unsigned char* __restrict__ strong) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double t2 = theta * theta * dn[i];
+  for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) {
+    const int j = A.col[k];
+    const double* blk = A.val + (size_t)k * B * B;
+    double s = 0.0;
+    for (int q = 0; q < B * B; ++q) s += blk[q] * blk[q];
+    strong[k] = (j == i || s >= t2 * dn[j]) ? 1 : 0;
+  }
+}
+
+__device__ __forceinline__ bool is_strong(const unsigned char* strong, int k) { return !strong || strong[k]; }
+
+__global__ void k_mis_m1(int n, AmgBsr A, const unsigned char* __restrict__ strong, const int* __restrict__ state,
+                         unsigned long long* __restrict__ m1) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   unsigned long long m = 0;
   for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) {
     const int j = A.col[k];
-    if (state[j] == kU) m = max(m, node_key(j) + 1);
+    if (is_strong(strong, k) && state[j] == kU) m = max(m, node_key(j) + 1);
   }
   m1[i] = m;
 }
 
-__global__ void k_mis_root(int n, AmgBsr A, int* __restrict__ state, const unsigned long long* __restrict__ m1,
-                           int* __restrict__ newroot) {
+__global__ void k_mis_root(int n, AmgBsr A, const unsigned char* __restrict__ strong, int* __restrict__ state,
+                           const unsigned long long* __restrict__ m1, int* __restrict__ newroot) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   newroot[i] = 0;
   if (state[i] != kU) return;
   unsigned long long m = 0;
-  for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) m = max(m, m1[A.col[k]]);
+  for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k)
+    if (is_strong(strong, k)) m = max(m, m1[A.col[k]]);
   if (m == node_key(i) + 1) newroot[i] = 1;
 }
 
 // near[i] = 1 if a new root is in N(i) (incl. i)
-__global__ void k_mis_near(int n, AmgBsr A, const int* __restrict__ newroot, int* __restrict__ near) {
+__global__ void k_mis_near(int n, AmgBsr A, const unsigned char* __restrict__ strong,
+                           const int* __restrict__ newroot, int* __restrict__ near) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   int f = 0;
-  for (int k = A.ptr[i]; k < A.ptr[i + 1] && !f; ++k) f = newroot[A.col[k]];
+  for (int k = A.ptr[i]; k < A.ptr[i + 1] && !f; ++k) f = is_strong(strong, k) && newroot[A.col[k]];
   near[i] = f;
 }
 
-__global__ void k_mis_out(int n, AmgBsr A, int* __restrict__ state, const int* __restrict__ newroot,
-                          const int* __restrict__ near, int* __restrict__ undecided) {
+__global__ void k_mis_out(int n, AmgBsr A, const unsigned char* __restrict__ strong, int* __restrict__ state,
+                          const int* __restrict__ newroot, const int* __restrict__ near, int* __restrict__ undecided) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   if (newroot[i]) {
@@ -149,16 +185,16 @@ __global__ void k_mis_out(int n, AmgBsr A, int* __restrict__ state, const int* _
   }
   if (state[i] != kU) return;
   int f = 0;
-  for (int k = A.ptr[i]; k < A.ptr[i + 1] && !f; ++k) f = near[A.col[k]];
+  for (int k = A.ptr[i]; k < A.ptr[i + 1] && !f; ++k) f = is_strong(strong, k) && near[A.col[k]];
   if (f)
     state[i] = kOut;
   else
     atomicAdd(undecided, 1);
 }
 
-// phase 1: roots (ids from the prefix sum of root flags) and their neighbours
-__global__ void k_agg_phase1(int n, AmgBsr A, const int* __restrict__ state, const int* __restrict__ root_id,
-                             int* __restrict__ agg) {
+// phase 1: roots (ids from the prefix sum of root flags) and their strong neighbours
+__global__ void k_agg_phase1(int n, AmgBsr A, const unsigned char* __restrict__ strong,
+                             const int* __restrict__ state, const int* __restrict__ root_id, int* __restrict__ agg) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   int a = -1;
@@ -167,7 +203,7 @@ __global__ void k_agg_phase1(int n, AmgBsr A, const int* __restrict__ state, con
   } else {
     for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) {
       const int j = A.col[k];
-      if (state[j] == kRoot) {
+      if (is_strong(strong, k) && state[j] == kRoot) {
         a = root_id[j];
         break;
       }
@@ -426,6 +462,10 @@ __device__ __forceinline__ int gal_member(const int* ofs, int ng, int t) {
   return lo;
 }
 
+// Prolongator smoothing weight w = kProlongOmega / lambda_max(D^-1 A). 1.6 rather than the usual
+// 4/3: on the plates it gives 3-4 % fewer cycle iterations and slightly smaller coarse levels.
+constexpr double kProlongOmega = 1.6;
+
 // P = P0 - w D^-1 A P0: values, warp per row i. Candidates: the blocks k of A's row i in order,
 // each the B x 3 product -w D_i^-1 A_k P0_{A.col[k]}; then P0_i is added to the node's own
 // aggregate's block.
@@ -438,7 +478,7 @@ __global__ void __launch_bounds__(32 * kGalWarps) k_amg_p_vals(int n, AmgBsr A, 
   __shared__ GalerkinSmem<NV> sm;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int warp = blockIdx.x * kGalWarps + w, nw = gridDim.x * kGalWarps;
-  const double om = 4.0 / (3.0 * *wp);
+  const double om = kProlongOmega / *wp;
   for (int i = warp; i < n; i += nw) {
     const int c0 = P.ptr[i], m = P.ptr[i + 1] - c0;
     for (int t = lane; t < m; t += 32) sm.cols[w][t] = P.col[c0 + t];
@@ -1318,14 +1358,26 @@ cudaError_t amg_dinv(int B, const AmgBsr& A, double* dinv, int* err, cudaStream_
   return cudaGetLastError();
 }
 
-cudaError_t amg_mis_round(const AmgBsr& A, int* state, unsigned long long* m1, int* newroot, int* near, int* undecided,
-                          cudaStream_t s) {
+cudaError_t amg_strength(int B, const AmgBsr& A, double theta, double* dn, unsigned char* strong, cudaStream_t s) {
+  if (B == 2) {
+    k_amg_diag_norm<2><<<g1(A.n), 256, 0, s>>>(A.n, A, dn);
+    k_amg_strength<2><<<g1(A.n), 256, 0, s>>>(A.n, A, dn, theta, strong);
+  } else {
+    k_amg_diag_norm<3><<<g1(A.n), 256, 0, s>>>(A.n, A, dn);
+    k_amg_strength<3><<<g1(A.n), 256, 0, s>>>(A.n, A, dn, theta, strong);
+  }
+  count_launches(2);
+  return cudaGetLastError();
+}
+
+cudaError_t amg_mis_round(const AmgBsr& A, const unsigned char* strong, int* state, unsigned long long* m1,
+                          int* newroot, int* near, int* undecided, cudaStream_t s) {
   const int n = A.n;
   cudaMemsetAsync(undecided, 0, sizeof(int), s);
-  k_mis_m1<<<g1(n), 256, 0, s>>>(n, A, state, m1);
-  k_mis_root<<<g1(n), 256, 0, s>>>(n, A, state, m1, newroot);
-  k_mis_near<<<g1(n), 256, 0, s>>>(n, A, newroot, near);
-  k_mis_out<<<g1(n), 256, 0, s>>>(n, A, state, newroot, near, undecided);
+  k_mis_m1<<<g1(n), 256, 0, s>>>(n, A, strong, state, m1);
+  k_mis_root<<<g1(n), 256, 0, s>>>(n, A, strong, state, m1, newroot);
+  k_mis_near<<<g1(n), 256, 0, s>>>(n, A, strong, newroot, near);
+  k_mis_out<<<g1(n), 256, 0, s>>>(n, A, strong, state, newroot, near, undecided);
   count_launches(4);
   return cudaGetLastError();
 }
@@ -1336,10 +1388,10 @@ cudaError_t amg_flag_eq(int n, const int* a, int v, int* f, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-cudaError_t amg_aggregate(int B, const AmgBsr& A, const int* state, const int* root_id, int* agg1, int* agg2,
-                          cudaStream_t s) {
+cudaError_t amg_aggregate(int B, const AmgBsr& A, const unsigned char* strong, const int* state, const int* root_id,
+                          int* agg1, int* agg2, cudaStream_t s) {
   const int n = A.n;
-  k_agg_phase1<<<g1(n), 256, 0, s>>>(n, A, state, root_id, agg1);
+  k_agg_phase1<<<g1(n), 256, 0, s>>>(n, A, strong, state, root_id, agg1);
   if (B == 2)
     k_agg_phase2<2><<<g1(n), 256, 0, s>>>(n, A, agg1, agg2);
   else

@@ -259,11 +259,14 @@ struct AmgBsr32 {  // a coarse operator's FP32 copy (3 x 3 blocks), same pattern
 };
 cudaError_t amg_fine_bsr(int N, const int* node_ptr, const double* vals, double* out, cudaStream_t s);
 cudaError_t amg_dinv(int B, const AmgBsr& A, double* dinv, int* err, cudaStream_t s);
-cudaError_t amg_mis_round(const AmgBsr& A, int* state, unsigned long long* m1, int* newroot, int* near, int* undecided,
-                          cudaStream_t s);
+// strong[k] = block k of A is a strong connection (aggregation graph); dn: scratch of A.n doubles
+cudaError_t amg_strength(int B, const AmgBsr& A, double theta, double* dn, unsigned char* strong, cudaStream_t s);
+// strong == nullptr: every block of the pattern is a connection
+cudaError_t amg_mis_round(const AmgBsr& A, const unsigned char* strong, int* state, unsigned long long* m1,
+                          int* newroot, int* near, int* undecided, cudaStream_t s);
 cudaError_t amg_flag_eq(int n, const int* a, int v, int* f, cudaStream_t s);
-cudaError_t amg_aggregate(int B, const AmgBsr& A, const int* state, const int* root_id, int* agg1, int* agg2,
-                          cudaStream_t s);
+cudaError_t amg_aggregate(int B, const AmgBsr& A, const unsigned char* strong, const int* state, const int* root_id,
+                          int* agg1, int* agg2, cudaStream_t s);
 cudaError_t amg_flag_negative(int n, const int* a, int* f, cudaStream_t s);
 cudaError_t amg_phase3(int n, int n_agg, const int* left_id, int* agg, cudaStream_t s);
 cudaError_t amg_group(int n, const int* key, int m, int* ptr, int* cnt, int* cur, int* out, int* scan_tmp,

@@ -142,6 +142,7 @@ _SIGS = {
     "cstg_amg_time": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_double)]),
     "cstg_amg_set_tail": (C.c_int, [_vp, C.c_int]),
     "cstg_amg_set_smoother": (C.c_int, [_vp, C.c_int]),
+    "cstg_amg_set_strength": (C.c_int, [_vp, C.c_double, C.c_double]),
     "cstg_mpnn_param_count": (C.c_longlong, []),
     "cstg_learned_setup": (C.c_int, [_vp, _vp, _vp]),
     "cstg_learned_set_params": (C.c_int, [_vp, _vp]),

@@ -427,6 +427,12 @@ def amg_set_smoother(K: GpuCsrMatrix, kind: str) -> None:
     K.ctx.check(K.ctx.L.cstg_amg_set_smoother(K.ctx.h, code))
 
 
+def amg_set_strength(K: GpuCsrMatrix, theta_fine: float = 0.0, theta_coarse: float = 0.03) -> None:
+    """Strength-of-connection thresholds of the aggregation (finest level, coarser levels); the
+    hierarchy is rebuilt on next use when they change."""
+    K.ctx.check(K.ctx.L.cstg_amg_set_strength(K.ctx.h, float(theta_fine), float(theta_coarse)))
+
+
 def amg_set_tail(K: GpuCsrMatrix, enable: bool) -> None:
     """Runs the small coarse levels as one cluster launch (True, the default) or level by level."""
     K.ctx.check(K.ctx.L.cstg_amg_set_tail(K.ctx.h, int(bool(enable))))

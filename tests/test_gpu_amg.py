@@ -178,3 +178,31 @@ def test_amg_random_plates(pkg, gpu_lib):
         assert st.converged and st.true_rel_residual <= 1e-10, (spec, case, st.message)
         assert _rel(x, x_ref) < REL_TOL, (spec, case)
         K.ctx.close()
+
+
+def test_amg_coarse_strength_filter(pkg, gpu_lib):
+    """Aggregating the coarse levels over strong connections only (the default) keeps the first
+    coarsening, gives smaller aggregates below it and fewer iterations than aggregating over
+    every connection; both reach the FP64 Jacobi-PCG solution."""
+    m, K, b = _plate(pkg, 200, 400)
+    ref = pkg.CgJacobiSolver(pkg.SolverOptions(rtol=1e-12, max_iter=100000))
+    ref.setup(K)
+    x_ref = np.zeros(m.num_dofs)
+    ref.solve(b, x_ref)
+    out = {}
+    for theta_c in (0.0, 0.03):
+        pkg.amg_set_strength(K, 0.0, theta_c)
+        s = pkg.CgJacobiSolver(_amg())
+        s.setup(K)
+        info = pkg.amg_setup(K)
+        x = np.zeros(m.num_dofs)
+        st = s.solve(b, x)
+        assert st.converged and st.true_rel_residual <= 1e-10, (theta_c, st.message)
+        assert _rel(x, x_ref) < REL_TOL, theta_c
+        out[theta_c] = (info["dofs"], st.iterations)
+    (d0, it0), (d1, it1) = out[0.0], out[0.03]
+    assert d0[:2] == d1[:2] and d1[2] > d0[2], out
+    assert it1 < it0, out
+    with pytest.raises(pkg.CstgError):
+        pkg.amg_set_strength(K, 0.0, 1.5)
+    K.ctx.close()
