@@ -627,40 +627,79 @@ __global__ void k_pt_fill(int n, AmgBsr P, const int* __restrict__ ptr, int* __r
   }
 }
 
-// A_c = P' (AP): coarse row J
-template <int B>
-__global__ void k_amg_ac_count(int nc, const int* __restrict__ pt_ptr, const int* __restrict__ pt_idx,
-                               const int* __restrict__ p_row, AmgBsr AP, int* __restrict__ cnt, int* err) {
-  const int J = blockIdx.x * blockDim.x + threadIdx.x;
-  if (J >= nc) return;
-  int s[kAmgMaxRow];
-  int m = 0;
-  bool over = false;
-  for (int t = pt_ptr[J]; t < pt_ptr[J + 1] && !over; ++t) {
-    const int i = p_row[pt_idx[t]];
-    for (int q = AP.ptr[i]; q < AP.ptr[i + 1]; ++q)
-      if (set_insert(s, m, AP.col[q], kAmgMaxRow) < 0) {
-        over = true;
-        break;
-      }
-  }
-  if (over) atomicMin(&err[kErrAmg], J);
-  cnt[J] = m;
+// A_c = P' (AP): the column set of coarse row J, one warp per row. The lanes take the fine rows i
+// of column J of P (the P' list) and insert the columns of AP's row i into a per-warp open-
+// addressing set in shared memory (kAcSet slots, twice the row bound, so a row within the bound
+// never fills it). FILL = false: cnt[J] = the number of distinct columns (error word if above
+// kAmgMaxRow); FILL = true: the columns in ascending order, each written at its rank in the set.
+// Insertion order (and so the set's layout) varies between runs; the counts and sorted columns
+// do not.
+constexpr int kAcSet = 2 * kAmgMaxRow;
+constexpr int kAcWarps = 8;
+constexpr int ilog2(int v) { return v <= 1 ? 0 : 1 + ilog2(v >> 1); }
+constexpr int kAcShift = 32 - ilog2(kAcSet);
+static_assert((kAcSet & (kAcSet - 1)) == 0 && kAcSet % 32 == 0, "set size: a power of two, whole warps");
+
+__device__ __forceinline__ unsigned ac_slot(int c) {
+  return ((unsigned)c * 2654435761u) >> kAcShift;  // multiplicative hash, top bits
 }
 
-// A_c = P' (AP): column sets
-__global__ void k_amg_ac_cols(int nc, const int* __restrict__ pt_ptr, const int* __restrict__ pt_idx,
-                              const int* __restrict__ p_row, AmgBsr AP, AmgBsr Ac) {
-  const int J = blockIdx.x * blockDim.x + threadIdx.x;
-  if (J >= nc) return;
-  int s[kAmgMaxRow];
-  int m = 0;
-  for (int t = pt_ptr[J]; t < pt_ptr[J + 1]; ++t) {
-    const int i = p_row[pt_idx[t]];
-    for (int q = AP.ptr[i]; q < AP.ptr[i + 1]; ++q) set_insert(s, m, AP.col[q], kAmgMaxRow);
+template <bool FILL>
+__global__ void __launch_bounds__(32 * kAcWarps) k_amg_ac_pattern(int nc, const int* __restrict__ pt_ptr,
+                                                                  const int* __restrict__ pt_idx,
+                                                                  const int* __restrict__ p_row, AmgBsr AP,
+                                                                  int* __restrict__ cnt, AmgBsr Ac, int* err) {
+  __shared__ int set[kAcWarps][kAcSet];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int J = blockIdx.x * kAcWarps + w; J < nc; J += gridDim.x * kAcWarps) {
+    for (int h = lane; h < kAcSet; h += 32) set[w][h] = -1;
+    __syncwarp();
+    int full = 0;
+    const int t1 = pt_ptr[J + 1];
+    for (int t = pt_ptr[J] + lane; t < t1; t += 32) {
+      const int i = p_row[pt_idx[t]];
+      for (int q = AP.ptr[i]; q < AP.ptr[i + 1]; ++q) {
+        const int c = AP.col[q];
+        unsigned h = ac_slot(c);
+        int probe = 0;
+        for (; probe < kAcSet; ++probe) {
+          const int old = atomicCAS(&set[w][h], -1, c);
+          if (old == -1 || old == c) break;
+          h = (h + 1) & (kAcSet - 1);
+        }
+        if (probe == kAcSet) full = 1;
+      }
+    }
+    __syncwarp();
+    int v[kAcSet / 32];
+    int m = 0;
+#pragma unroll
+    for (int u = 0; u < kAcSet / 32; ++u) {
+      v[u] = set[w][lane + 32 * u];
+      m += v[u] >= 0 ? 1 : 0;
+    }
+    m = __reduce_add_sync(0xffffffffu, m);
+    full = __any_sync(0xffffffffu, full);
+    if (!FILL) {
+      if (lane == 0) {
+        if (full || m > kAmgMaxRow) atomicMin(&err[kErrAmg], J);
+        cnt[J] = m;
+      }
+    } else {
+      int* cols = const_cast<int*>(Ac.col) + Ac.ptr[J];
+#pragma unroll
+      for (int u = 0; u < kAcSet / 32; ++u) {
+        if (v[u] < 0) continue;
+        int r = 0;
+        for (int h = 0; h < kAcSet; ++h) {
+          const int o = set[w][h];
+          r += (o >= 0 && o < v[u]) ? 1 : 0;
+        }
+        cols[r] = v[u];
+      }
+    }
+    __syncwarp();
   }
-  int* cols = const_cast<int*>(Ac.col) + Ac.ptr[J];
-  for (int q = 0; q < m; ++q) cols[q] = s[q];
 }
 
 // A_c = P' (AP): values. Coarse row J's candidates: for each P block (i, J) in ascending fine row
@@ -742,17 +781,19 @@ __global__ void k_p_rows(int n, AmgBsr P, int* __restrict__ p_row) {
 }
 
 // sort the P' lists by fine row (so that A_c's additions follow a fixed order)
-__global__ void k_sort_pt(int nc, const int* __restrict__ ptr, int* __restrict__ idx) {
-  const int J = blockIdx.x * blockDim.x + threadIdx.x;
-  if (J >= nc) return;
-  for (int i = ptr[J] + 1; i < ptr[J + 1]; ++i) {
-    const int x = idx[i];
-    int j = i - 1;
-    while (j >= ptr[J] && idx[j] > x) {  // block indices grow with the fine row
-      idx[j + 1] = idx[j];
-      --j;
+// P' lists in ascending block index (= ascending fine row): one warp per coarse node J; each
+// entry of the unsorted list `in` goes to its rank among the list's entries (all distinct).
+__global__ void __launch_bounds__(256) k_rank_pt(int nc, const int* __restrict__ ptr, const int* __restrict__ in,
+                                                 int* __restrict__ out) {
+  const int lane = threadIdx.x & 31;
+  for (int J = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; J < nc; J += (gridDim.x * blockDim.x) >> 5) {
+    const int lo = ptr[J], hi = ptr[J + 1];
+    for (int a = lo + lane; a < hi; a += 32) {
+      const int x = in[a];
+      int r = 0;
+      for (int b = lo; b < hi; ++b) r += in[b] < x ? 1 : 0;
+      out[lo + r] = x;
     }
-    idx[j + 1] = x;
   }
 }
 
@@ -1337,6 +1378,9 @@ int one_wave(const void* kern, long long n_threads) {
 }
 
 inline int g1(long long n, int t = 256) { return (int)std::max<long long>(1, std::min<long long>((n + t - 1) / t, 1LL << 30)); }
+inline int ac_grid(long long nc) {
+  return (int)std::max<long long>(1, std::min<long long>((nc + kAcWarps - 1) / kAcWarps, 148LL * 16));
+}
 inline int gw(long long n) { return (int)std::max<long long>(1, std::min<long long>((n + 255) / 256, 148LL * 8)); }
 
 }  // namespace
@@ -1499,26 +1543,24 @@ cudaError_t amg_ap_fill(int B, const AmgBsr& A, const AmgBsr& P, const AmgBsr& A
   return cudaGetLastError();
 }
 
-cudaError_t amg_pt(int n, int nc, const AmgBsr& P, int* p_row, int* pt_ptr, int* cnt, int* cur, int* pt_idx,
-                   int* scan_tmp, cudaStream_t s) {
+cudaError_t amg_pt(int n, int nc, const AmgBsr& P, int* p_row, int* pt_ptr, int* cnt, int* cur, int* pt_tmp,
+                   int* pt_idx, int* scan_tmp, cudaStream_t s) {
   cudaMemsetAsync(cnt, 0, sizeof(int) * (size_t)nc, s);
   cudaMemsetAsync(cur, 0, sizeof(int) * (size_t)nc, s);
   k_p_rows<<<g1(n), 256, 0, s>>>(n, P, p_row);
   k_pt_count<<<g1(n), 256, 0, s>>>(n, P, cnt);
   cudaError_t e = scan_exclusive(cnt, nc, pt_ptr, scan_tmp, s);
   if (e != cudaSuccess) return e;
-  k_pt_fill<<<g1(n), 256, 0, s>>>(n, P, pt_ptr, cur, pt_idx);
-  k_sort_pt<<<g1(nc), 256, 0, s>>>(nc, pt_ptr, pt_idx);
+  k_pt_fill<<<g1(n), 256, 0, s>>>(n, P, pt_ptr, cur, pt_tmp);
+  k_rank_pt<<<gw((long long)nc * 32), 256, 0, s>>>(nc, pt_ptr, pt_tmp, pt_idx);
   count_launches(4);
   return cudaGetLastError();
 }
 
 cudaError_t amg_ac_count(int B, int nc, const int* pt_ptr, const int* pt_idx, const int* p_row, const AmgBsr& AP,
                          int* cnt, int* err, cudaStream_t s) {
-  if (B == 2)
-    k_amg_ac_count<2><<<g1(nc, 128), 128, 0, s>>>(nc, pt_ptr, pt_idx, p_row, AP, cnt, err);
-  else
-    k_amg_ac_count<3><<<g1(nc, 128), 128, 0, s>>>(nc, pt_ptr, pt_idx, p_row, AP, cnt, err);
+  (void)B;
+  k_amg_ac_pattern<false><<<ac_grid(nc), 32 * kAcWarps, 0, s>>>(nc, pt_ptr, pt_idx, p_row, AP, cnt, AmgBsr{}, err);
   count_launches(1);
   return cudaGetLastError();
 }
@@ -1526,7 +1568,7 @@ cudaError_t amg_ac_count(int B, int nc, const int* pt_ptr, const int* pt_idx, co
 cudaError_t amg_ac_fill(int B, int nc, const int* pt_ptr, const int* pt_idx, const int* p_row, const AmgBsr& P,
                         const AmgBsr& AP, const AmgBsr& Ac, cudaStream_t s) {
   const int gv = (int)std::max<long long>(1, std::min<long long>(((long long)nc + kGalWarps - 1) / kGalWarps, 148LL * 16));
-  k_amg_ac_cols<<<g1(nc, 128), 128, 0, s>>>(nc, pt_ptr, pt_idx, p_row, AP, Ac);
+  k_amg_ac_pattern<true><<<ac_grid(nc), 32 * kAcWarps, 0, s>>>(nc, pt_ptr, pt_idx, p_row, AP, nullptr, Ac, nullptr);
   if (B == 2)
     k_amg_ac_vals<2><<<gv, 32 * kGalWarps, 0, s>>>(nc, pt_ptr, pt_idx, p_row, P, AP, Ac);
   else

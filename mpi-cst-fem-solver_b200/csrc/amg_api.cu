@@ -87,7 +87,7 @@ struct AmgData {
   AmgTail tail;
   // scratch of the setup
   DevBuf state, m1, newroot, near, und, root_id, flags, agg1, agg2, agg_ptr, members, cnt, cur, P0, Bf, Bc, cnt2,
-      ap_ptr, ap_col, ap_val, part, vx, vy, strong, dn;
+      ap_ptr, ap_col, ap_val, part, vx, vy, strong, dn, pt_tmp;
 };
 
 void cstg_host::amg_free(cstg_ctx* ctx) {
@@ -100,7 +100,7 @@ void cstg_host::amg_free(cstg_ctx* ctx) {
   }
   DevBuf* all[] = {&d->Minv, &d->piv, &d->state, &d->m1, &d->newroot, &d->near, &d->und, &d->root_id, &d->flags,
                    &d->agg1, &d->agg2, &d->agg_ptr, &d->members, &d->cnt, &d->cur, &d->P0, &d->Bf, &d->Bc,
-                   &d->cnt2, &d->ap_ptr, &d->ap_col, &d->ap_val, &d->part, &d->vx, &d->vy, &d->strong, &d->dn};
+                   &d->cnt2, &d->ap_ptr, &d->ap_col, &d->ap_val, &d->part, &d->vx, &d->vy, &d->strong, &d->dn, &d->pt_tmp};
   for (DevBuf* b : all) free_buf(*b);
   delete d;
   ctx->amg = nullptr;
@@ -234,8 +234,9 @@ int coarsen(cstg_ctx* ctx, AmgData* d, int l, double theta, bool* stop) {
   ENSURE(lv.p_row, sizeof(int) * (size_t)std::max(nnz_p, 1));
   ENSURE(lv.pt_ptr, sizeof(int) * ((size_t)nc + 1));
   ENSURE(lv.pt_idx, sizeof(int) * (size_t)std::max(nnz_p, 1));
+  ENSURE(d->pt_tmp, sizeof(int) * (size_t)std::max(nnz_p, 1));
   CK(amg_pt(n, nc, P, buf_ptr<int>(lv.p_row), buf_ptr<int>(lv.pt_ptr), buf_ptr<int>(d->cnt), buf_ptr<int>(d->cur),
-            buf_ptr<int>(lv.pt_idx), buf_ptr<int>(ctx->scan_tmp), ctx->stream));
+            buf_ptr<int>(d->pt_tmp), buf_ptr<int>(lv.pt_idx), buf_ptr<int>(ctx->scan_tmp), ctx->stream));
   // the cycle's FP32 copies of P
   ENSURE(lv.p32, sizeof(float) * (size_t)std::max(nnz_p, 1) * B * 3);
   ENSURE(lv.pt32, sizeof(float) * (size_t)std::max(nnz_p, 1) * B * 3);

@@ -284,8 +284,8 @@ cudaError_t amg_p_fill(int B, const AmgBsr& A, const int* agg, const double* P0,
                        const AmgBsr& P, cudaStream_t s);
 cudaError_t amg_ap_count(int B, const AmgBsr& A, const AmgBsr& P, int* cnt, int* err, cudaStream_t s);
 cudaError_t amg_ap_fill(int B, const AmgBsr& A, const AmgBsr& P, const AmgBsr& AP, cudaStream_t s);
-cudaError_t amg_pt(int n, int nc, const AmgBsr& P, int* p_row, int* pt_ptr, int* cnt, int* cur, int* pt_idx,
-                   int* scan_tmp, cudaStream_t s);
+cudaError_t amg_pt(int n, int nc, const AmgBsr& P, int* p_row, int* pt_ptr, int* cnt, int* cur, int* pt_tmp,
+                   int* pt_idx, int* scan_tmp, cudaStream_t s);
 cudaError_t amg_ac_count(int B, int nc, const int* pt_ptr, const int* pt_idx, const int* p_row, const AmgBsr& AP,
                          int* cnt, int* err, cudaStream_t s);
 cudaError_t amg_ac_fill(int B, int nc, const int* pt_ptr, const int* pt_idx, const int* p_row, const AmgBsr& P,
