@@ -280,12 +280,17 @@ def add_kirsch_traction(K_or_ctx, group_edges, thickness: float, a: float, sigma
 
 
 def _traction_device(ctx, group_edges, thickness, kind, p0, p1, f):
+    # cstg_add_traction_device runs on the context's stream, which is not ordered with torch's:
+    # the edge list and f are finished on torch's stream before the call, and the added loads on
+    # the device before this returns, so torch work issued afterwards sees them
     import torch
     e = torch.as_tensor(np.asarray(group_edges).reshape(-1) if not _is_device(group_edges) else group_edges,
                         dtype=torch.int32, device=f.device).contiguous()
     f = _f64(f)
+    torch.cuda.current_stream(f.device).synchronize()
     ctx.check(ctx.L.cstg_add_traction_device(ctx.h, e.numel() // 2, _ptr(e), float(thickness), int(kind),
                                              float(p0), float(p1), _ptr(f)))
+    torch.cuda.synchronize(f.device)
 
 
 @dataclasses.dataclass
