@@ -131,6 +131,14 @@ cstg_ctx* cstg_create(int device, int* status);
 void cstg_destroy(cstg_ctx* ctx);
 const char* cstg_last_error(const cstg_ctx* ctx);
 int cstg_set_stream(cstg_ctx* ctx, void* cuda_stream); /* NULL: the context's own stream */
+/* The stream the context's work is ordered on (its own or the one given to cstg_set_stream), so
+ * a caller can order its own streams against it with events. Asynchronous entry points (the
+ * *_device calls that only enqueue: cstg_multiply_device, cstg_multiply_mixed_device,
+ * cstg_add_traction_device) return before their kernels have run; every other entry point
+ * returns after its work on this stream has finished. No entry point waits for work the caller
+ * issued on other streams: inputs written there must be finished (or the context's stream made
+ * to wait for them) before the call. */
+int cstg_get_stream(cstg_ctx* ctx, void** cuda_stream);
 void cstg_default_options(cstg_solver_options* opt);
 int cstg_version(void);
 /* Kernel launches issued by this library in this process so far (every kernel node of a
@@ -245,9 +253,10 @@ int cstg_add_traction_device(cstg_ctx* ctx, int n_edges, const int32_t* d_edges,
  * device and `stream` (NULL: the legacy default stream); returns when the solve has ended.
  * Every work vector lives in one static device array of the library sized for at most
  * CSTG_STATIC_MAX_ROWS rows (2.06 MiB on every GPU that loads the library, held until the
- * process exits); larger systems are rejected with CSTG_ERR_INVALID_ARGUMENT. The first call
- * on a device looks up the array's device address (cudaGetSymbolAddress): make that first
- * call before any stream capture. All calls share the array and it keeps the last call's
+ * process exits); larger systems are rejected with CSTG_ERR_INVALID_ARGUMENT. Every call looks
+ * up the array's device address in the current device context (cudaGetSymbolAddress); the
+ * first call on a device also loads the library's device code there, so make that first call
+ * before any stream capture. All calls share the array and it keeps the last call's
  * contents (each call resets the state it needs): calls that overlap on a GPU race, so
  * serialise them. Needs precision CSTG_PRECISION_FP64 and record_history 0. Errors return a
  * status code with the text in stats->message. */

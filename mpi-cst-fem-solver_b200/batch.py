@@ -164,8 +164,9 @@ class BatchSolver:
         best = native.BatchConfig()
         sec = C.c_double(0.0)
         offs = _i32(batch.node_offsets)
-        ctx.check(ctx.L.cstg_batch_autotune(ctx.h, batch.n_plates, _ptr(offs), batch.n_cases, _ptr(d_b),
-                                            _ptr(d_x), C.byref(o), C.byref(best), C.byref(sec)))
+        with ctx.ordered(d_b.device):
+            ctx.check(ctx.L.cstg_batch_autotune(ctx.h, batch.n_plates, _ptr(offs), batch.n_cases, _ptr(d_b),
+                                                _ptr(d_x), C.byref(o), C.byref(best), C.byref(sec)))
         self.config = (best.cluster_ctas, best.threads)
         return self.config, sec.value
 
@@ -185,8 +186,9 @@ class BatchSolver:
             if self.d_b is None:
                 raise CstgError(native.ERR_STATE, "batch_solve: setup(device_rhs=True) first")
             x = self.d_x
-            ctx.check(ctx.L.cstg_batch_solve_device(ctx.h, n_p, _ptr(offs), n_c, _ptr(self.d_b), _ptr(x),
-                                                    C.byref(o), cfg, res, C.byref(sec)))
+            with ctx.ordered(self.d_b.device):
+                ctx.check(ctx.L.cstg_batch_solve_device(ctx.h, n_p, _ptr(offs), n_c, _ptr(self.d_b), _ptr(x),
+                                                        C.byref(o), cfg, res, C.byref(sec)))
         else:
             x = np.zeros_like(self.b)
             ctx.check(ctx.L.cstg_batch_solve(ctx.h, n_p, _ptr(offs), n_c, _ptr(self.b), _ptr(x), C.byref(o),

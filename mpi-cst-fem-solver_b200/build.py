@@ -34,17 +34,42 @@ def up_to_date() -> bool:
     return all(os.path.getmtime(p) <= t for p in _deps())
 
 
+def _flags() -> list:
+    return ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
+            "-Xcompiler", "-fPIC,-ffp-contract=off", "-ccbin", "/usr/bin/g++"]
+
+
 def build_library(force: bool = False, verbose: bool = False) -> str:
-    """Compile the library unless it is newer than every source; returns its path."""
+    """Compile the library unless it is newer than every source; returns its path. Each source
+    is compiled to its own object (in parallel, one nvcc per file) and the objects are linked."""
     if not force and up_to_date():
         return LIB
-    cmd = [NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
-           "-Xcompiler", "-fPIC,-ffp-contract=off", "-shared", "-ccbin", "/usr/bin/g++",
-           "-o", LIB + ".tmp"] + sources()
-    if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True)
+    from concurrent.futures import ThreadPoolExecutor
+    obj_dir = os.path.join(HERE, "_build")
+    os.makedirs(obj_dir, exist_ok=True)
+    headers = [p for p in _deps() if not p.endswith(".cu")]
+    newest_header = max(os.path.getmtime(p) for p in headers)
+    jobs = []
+    for src in sources():
+        obj = os.path.join(obj_dir, os.path.basename(src)[:-3] + ".o")
+        stale = force or not os.path.exists(obj) or \
+            os.path.getmtime(obj) < max(os.path.getmtime(src), newest_header)
+        cmd = [NVCC] + (["-Xptxas=-v"] if verbose else []) + _flags() + ["-c", src, "-o", obj + ".tmp"]
+        jobs.append((obj, cmd if stale else None))
+
+    def run(job):
+        obj, cmd = job
+        if cmd is None:
+            return obj
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+        os.replace(obj + ".tmp", obj)
+        return obj
+
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        objs = list(ex.map(run, jobs))
+    subprocess.run([NVCC] + _flags() + ["-shared", "-o", LIB + ".tmp"] + objs, check=True)
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

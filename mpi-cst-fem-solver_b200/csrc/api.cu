@@ -107,6 +107,13 @@ int cstg_set_stream(cstg_ctx* ctx, void* s) {
   return CSTG_OK;
 }
 
+int cstg_get_stream(cstg_ctx* ctx, void** stream) {
+  BEGIN(ctx);
+  if (!stream) return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "get_stream: null output");
+  *stream = static_cast<void*>(ctx->stream);
+  return CSTG_OK;
+}
+
 // ---- mesh --------------------------------------------------------------------------------
 
 static int set_mesh_common(cstg_ctx* ctx, int n_nodes, int n_tri) {

@@ -21,7 +21,6 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
-#include <mutex>
 
 #include "../../include/cstfem_b200.h"
 #include "common.cuh"
@@ -42,21 +41,15 @@ static_assert(kPartialBytes % 256 == 0, "partials must keep 256-byte alignment")
 // The scratch of every cstg_pcg_solve_static call (see the file comment).
 static __device__ __align__(256) double g_pcg_scratch[kScratchBytes / sizeof(double)];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-void* g_scratch_addr[kMaxDevices] = {};
-
-// Device address of g_pcg_scratch on the current device. The first call on a device looks it
-// up (cudaGetSymbolAddress with that device current); later calls reuse it.
-cudaError_t scratch_address(int dev, char** out) {
-  std::lock_guard<std::mutex> lk(g_mu);
-  if (!g_scratch_addr[dev]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_pcg_scratch);
-    if (e != cudaSuccess) return e;
-    g_scratch_addr[dev] = p;
-  }
-  *out = static_cast<char*>(g_scratch_addr[dev]);
+// Device address of g_pcg_scratch in the current device's context. Looked up on every call:
+// a cached address would go stale when the context is torn down and re-created
+// (cudaDeviceReset), while the lookup itself is a host-side table read once the module is
+// loaded (the first call on a device loads it, so that call comes before any stream capture).
+cudaError_t scratch_address(char** out) {
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_pcg_scratch);
+  if (e != cudaSuccess) return e;
+  *out = static_cast<char*>(p);
   return cudaSuccess;
 }
 
@@ -104,12 +97,8 @@ extern "C" int cstg_pcg_solve_static(int n_rows, const int32_t* d_row_ptr, const
     return fail_msg(stats, CSTG_ERR_UNSUPPORTED,
                     "pcg_solve_static: needs FP64 precision, no history and valid options");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  int dev = 0;
-  SCK(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= kMaxDevices)
-    return fail_msg(stats, CSTG_ERR_CUDA, "pcg_solve_static: device %d out of range", dev);
   char* base = nullptr;
-  SCK(scratch_address(dev, &base));
+  SCK(scratch_address(&base));
   PcgState* st = reinterpret_cast<PcgState*>(base);
   int* err = reinterpret_cast<int*>(base + kStateBytes);
   double* partials = reinterpret_cast<double*>(base + kStateBytes + kErrBytes);

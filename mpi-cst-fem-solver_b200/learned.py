@@ -85,7 +85,8 @@ def apply(K: GpuCsrMatrix, r, z=None):
     """z = M(r) on CUDA float64 tensors."""
     import torch
     z = torch.empty_like(r) if z is None else z
-    K.ctx.check(K.ctx.L.cstg_learned_apply_device(K.ctx.h, _ptr(r), _ptr(z)))
+    with K.ctx.ordered(r.device):
+        K.ctx.check(K.ctx.L.cstg_learned_apply_device(K.ctx.h, _ptr(r), _ptr(z)))
     return z
 
 
@@ -108,8 +109,9 @@ class Trainer:
         """Adds the gradients of the samples (rows of the CUDA float64 tensors R, E)."""
         ns = int(R.shape[0])
         losses = np.zeros(ns)
-        self._check(self.L.cstg_trainer_accumulate(self.h, K.ctx.h, ns, _ptr(R.contiguous()),
-                                                   _ptr(E.contiguous()), _ptr(losses)))
+        R, E = R.contiguous(), E.contiguous()
+        with K.ctx.ordered(R.device):  # (the trainer starts by waiting for the context's stream)
+            self._check(self.L.cstg_trainer_accumulate(self.h, K.ctx.h, ns, _ptr(R), _ptr(E), _ptr(losses)))
         return losses
 
     def step(self, lr: float, grad_scale: float) -> None:
@@ -177,8 +179,9 @@ def harvest(spec: PlateSpec, samples: int, params: np.ndarray, seed: int = 0, de
     o = SolverOptions(rtol=1e-12, max_iter=200000).native()
     got = C.c_int(0)
     stats = native.Stats()
-    ctx.check(ctx.L.cstg_pcg_iterates_device(ctx.h, _ptr(d_b), every, samples, _ptr(X), C.byref(got),
-                                             C.byref(o), C.byref(stats)))
+    with ctx.ordered(d_b.device):
+        ctx.check(ctx.L.cstg_pcg_iterates_device(ctx.h, _ptr(d_b), every, samples, _ptr(X), C.byref(got),
+                                                 C.byref(o), C.byref(stats)))
     X = X[:got.value]
     E = (x_star[None, :] - X).contiguous()
     R = torch.empty_like(E)

@@ -98,6 +98,7 @@ _SIGS = {
     "cstg_destroy": (None, [_vp]),
     "cstg_last_error": (C.c_char_p, [_vp]),
     "cstg_set_stream": (C.c_int, [_vp, _vp]),
+    "cstg_get_stream": (C.c_int, [_vp, C.POINTER(_vp)]),
     "cstg_default_options": (None, [C.POINTER(SolverOptions)]),
     "cstg_set_mesh": (C.c_int, [_vp, C.c_int, _vp, C.c_int, _vp]),
     "cstg_set_mesh_device": (C.c_int, [_vp, C.c_int, _vp, C.c_int, _vp]),

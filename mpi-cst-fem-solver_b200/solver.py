@@ -24,6 +24,7 @@ Vectors are numpy float64 arrays (host) or torch CUDA float64 tensors (device, n
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes as C
 import dataclasses
 
@@ -97,6 +98,35 @@ class Context:
         """stream: a torch.cuda.Stream, a raw cudaStream_t (int) or None (own stream)."""
         ptr = getattr(stream, "cuda_stream", stream)
         self.check(self.L.cstg_set_stream(self.h, ptr or None))
+        self._ext = None
+
+    def stream_handle(self) -> int:
+        """The cudaStream_t the context's work is ordered on (cstg_get_stream)."""
+        s = C.c_void_p(0)
+        self.check(self.L.cstg_get_stream(self.h, C.byref(s)))
+        return s.value or 0
+
+    @contextlib.contextmanager
+    def ordered(self, device):
+        """Orders a device call between torch's current stream and the context's stream.
+
+        The context works on its own stream, which torch does not know about: before the call
+        the context's stream waits (an event, not a host synchronisation) for everything torch
+        has queued so far, so inputs written by torch kernels or copies are complete; after it
+        torch's current stream waits for the context's, so torch work issued afterwards sees
+        the outputs, also of the entry points that return before their kernels have run."""
+        import torch
+        dev = torch.device(device)
+        ext = getattr(self, "_ext", None)
+        if ext is None:
+            ext = torch.cuda.ExternalStream(self.stream_handle(), device=dev)
+            self._ext = ext
+        cur = torch.cuda.current_stream(dev)
+        ext.wait_stream(cur)
+        try:
+            yield
+        finally:
+            cur.wait_stream(ext)
 
     def close(self) -> None:
         if getattr(self, "h", None):
@@ -112,8 +142,9 @@ class Context:
     def set_mesh(self, mesh) -> None:
         xy, tri = mesh.xy, mesh.triangles
         if _is_device(xy):
-            self.check(self.L.cstg_set_mesh_device(self.h, xy.numel() // 2, _ptr(_f64(xy)),
-                                                   tri.numel() // 3, _ptr(_i32(tri))))
+            with self.ordered(xy.device):
+                self.check(self.L.cstg_set_mesh_device(self.h, xy.numel() // 2, _ptr(_f64(xy)),
+                                                       tri.numel() // 3, _ptr(_i32(tri))))
         else:
             xy, tri = _f64(xy), _i32(tri)
             self.check(self.L.cstg_set_mesh(self.h, xy.size // 2, _ptr(xy), tri.size // 3, _ptr(tri)))
@@ -165,7 +196,8 @@ class GpuCsrMatrix:
         if _is_device(x):
             import torch
             y = torch.empty_like(x) if y is None else y
-            self.ctx.check(self.ctx.L.cstg_multiply_device(self.ctx.h, _ptr(x), _ptr(y)))
+            with self.ctx.ordered(x.device):
+                self.ctx.check(self.ctx.L.cstg_multiply_device(self.ctx.h, _ptr(x), _ptr(y)))
             return y
         y = np.zeros(self.num_rows) if y is None else y
         self.ctx.check(self.ctx.L.cstg_multiply(self.ctx.h, _ptr(x), _ptr(y)))
@@ -179,7 +211,8 @@ class GpuCsrMatrix:
         if not (_is_device(x) and x.dtype == torch.float64 and x.is_contiguous()):
             raise CstgError(native.ERR_INVALID_ARGUMENT, "multiply_mixed: x must be a contiguous CUDA float64 tensor")
         y = torch.empty_like(x) if y is None else y
-        self.ctx.check(self.ctx.L.cstg_multiply_mixed_device(self.ctx.h, _ptr(x), _ptr(y)))
+        with self.ctx.ordered(x.device):
+            self.ctx.check(self.ctx.L.cstg_multiply_mixed_device(self.ctx.h, _ptr(x), _ptr(y)))
         return y
 
 
@@ -249,7 +282,8 @@ def apply_dirichlet(dofs, K: GpuCsrMatrix, b) -> None:
         import torch
         d = torch.as_tensor(d, dtype=torch.int32, device=b.device).contiguous()
         v = torch.as_tensor(v, dtype=torch.float64, device=b.device).contiguous()
-        K.ctx.check(K.ctx.L.cstg_apply_dirichlet_device(K.ctx.h, d.numel(), _ptr(d), _ptr(v), _ptr(b)))
+        with K.ctx.ordered(b.device):
+            K.ctx.check(K.ctx.L.cstg_apply_dirichlet_device(K.ctx.h, d.numel(), _ptr(d), _ptr(v), _ptr(b)))
         return
     if not (isinstance(b, np.ndarray) and b.dtype == np.float64 and b.flags.c_contiguous):
         raise CstgError(native.ERR_INVALID_ARGUMENT, "apply_dirichlet: b must be a float64 C array")
@@ -280,17 +314,15 @@ def add_kirsch_traction(K_or_ctx, group_edges, thickness: float, a: float, sigma
 
 
 def _traction_device(ctx, group_edges, thickness, kind, p0, p1, f):
-    # cstg_add_traction_device runs on the context's stream, which is not ordered with torch's:
-    # the edge list and f are finished on torch's stream before the call, and the added loads on
-    # the device before this returns, so torch work issued afterwards sees them
+    # cstg_add_traction_device only enqueues its kernels on the context's stream: ctx.ordered
+    # puts them after torch's pending work (the edge list copy, f) and torch's later work after them
     import torch
     e = torch.as_tensor(np.asarray(group_edges).reshape(-1) if not _is_device(group_edges) else group_edges,
                         dtype=torch.int32, device=f.device).contiguous()
     f = _f64(f)
-    torch.cuda.current_stream(f.device).synchronize()
-    ctx.check(ctx.L.cstg_add_traction_device(ctx.h, e.numel() // 2, _ptr(e), float(thickness), int(kind),
-                                             float(p0), float(p1), _ptr(f)))
-    torch.cuda.synchronize(f.device)
+    with ctx.ordered(f.device):
+        ctx.check(ctx.L.cstg_add_traction_device(ctx.h, e.numel() // 2, _ptr(e), float(thickness), int(kind),
+                                                 float(p0), float(p1), _ptr(f)))
 
 
 @dataclasses.dataclass
@@ -368,8 +400,9 @@ class CgJacobiSolver:
             x = torch.empty_like(b) if x is None else x
             hist = torch.zeros(o.max_iter + 1, dtype=torch.float64, device=b.device) \
                 if self.options.record_history else None
-            ctx.check(ctx.L.cstg_pcg_solve_device(ctx.h, _ptr(b), _ptr(x), C.byref(o), C.byref(st),
-                                                  _ptr(hist)))
+            with ctx.ordered(b.device):
+                ctx.check(ctx.L.cstg_pcg_solve_device(ctx.h, _ptr(b), _ptr(x), C.byref(o), C.byref(st),
+                                                      _ptr(hist)))
         else:
             n = b.size
             x = np.zeros(n) if x is None else x
@@ -447,7 +480,8 @@ def amg_apply(K: GpuCsrMatrix, r, z=None):
     """z = M r (one V-cycle) on CUDA float64 tensors."""
     import torch
     z = torch.empty_like(r) if z is None else z
-    K.ctx.check(K.ctx.L.cstg_amg_apply_device(K.ctx.h, _ptr(r), _ptr(z)))
+    with K.ctx.ordered(r.device):
+        K.ctx.check(K.ctx.L.cstg_amg_apply_device(K.ctx.h, _ptr(r), _ptr(z)))
     return z
 
 

@@ -5,7 +5,8 @@ budgets with their own pool allocator, callbacks where cudaMalloc would stall th
 real-time loops); its work vectors live in a static device array of at most 65,536 rows.
 Its output is checked against the context-based solve (cstg_pcg_solve on the same CSR) within
 the parity tolerance of the other solver tests, on two calls in a row (the second call finds
-the first call's contents in the shared array). Kept last in collection order.
+the first call's contents in the shared array), and against the CPU oracle's Jacobi-PCG (the
+reference's recurrence) on the same system. Kept last in collection order.
 """
 import ctypes as C
 
@@ -29,11 +30,13 @@ def _plate_system(pkg):
     return rp, cols, vals, b
 
 
-def test_static_solve_matches_context_solve(pkg, gpu_lib):
+def test_static_solve_matches_context_solve(pkg, gpu_lib, oracle):
     import torch
     rp, cols, vals, b = _plate_system(pkg)
     n = rp.size - 1
     assert n <= pkg.native.STATIC_MAX_ROWS
+    x_or, st_or = oracle.pcg_jacobi(rp, cols, vals, b, rtol=1e-10, max_iter=20000)
+    assert st_or["converged"]
     # the existing entry point: the context solve on the same CSR
     A = pkg.GpuCsrMatrix.from_csr(rp, cols, vals)
     s = pkg.CgJacobiSolver()
@@ -63,6 +66,8 @@ def test_static_solve_matches_context_solve(pkg, gpu_lib):
         x = d_x.cpu().numpy()
         assert st.converged and st.iterations == st_ref.iterations, (call, st.message)
         assert np.linalg.norm(x - x_ref) / np.linalg.norm(x_ref) < REL_TOL, call
+        assert np.linalg.norm(x - x_or) / np.linalg.norm(x_or) < REL_TOL, call
+        assert abs(st.iterations - st_or["iterations"]) <= max(2, st_or["iterations"] // 50), call
         assert abs(st.true_rel_residual - st_ref.true_rel_residual) <= 1e-3 * st_ref.true_rel_residual
         assert st.message.decode() == st_ref.message
 
