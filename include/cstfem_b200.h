@@ -85,6 +85,11 @@ typedef struct {
 #define CSTG_PRECOND_AMG 2      /* smoothed-aggregation multigrid V(2,2) cycle (no reference
                                    counterpart); hierarchy built on the first solve after
                                    cstg_pcg_setup (or by cstg_amg_setup)                         */
+#define CSTG_PRECOND_LEARNED_MG 3 /* the learned network as the finest-level post-smoother of the
+                                   multigrid cycle (global reach through the hierarchy), inside
+                                   flexible CG with Jacobi-PCG as the stagnation fallback; needs
+                                   cstg_learned_setup (with the smoother's weights) after
+                                   cstg_pcg_setup                                                */
 
 /* launch_mode of cstg_pcg_solve */
 #define CSTG_LAUNCH_AUTO 0        /* persistent kernel for mesh-pattern matrices, else graph  */
@@ -141,6 +146,14 @@ int cstg_set_stream(cstg_ctx* ctx, void* cuda_stream); /* NULL: the context's ow
 int cstg_get_stream(cstg_ctx* ctx, void** cuda_stream);
 void cstg_default_options(cstg_solver_options* opt);
 int cstg_version(void);
+/* Bounded device waits (no reference counterpart). Every device-side wait of the library gives
+ * up after a number of polls and reports CSTG_ERR_TIMEOUT (stats->status CSTG_SOLVE_TIMEOUT where
+ * a solve was running) with the context still usable: the persistent solve's grid barriers
+ * (default 50,000,000 polls, about 2 s) and the learned network's tensor-core waits (default
+ * 4,194,304 polls). 0 makes a wait give up at once (failure-detection tests); -1 restores the
+ * default. A tensor-core wait that gives up still lets its matrix multiply finish (bounded)
+ * before the kernel releases its memory. */
+int cstg_set_wait_limits(cstg_ctx* ctx, long long barrier_polls, long long mma_polls);
 /* Kernel launches issued by this library in this process so far (every kernel node of a
  * replayed CUDA graph counts). Benchmarks read it around a timed region. */
 long long cstg_kernel_launches(void);
@@ -335,6 +348,19 @@ const char* cstg_trainer_last_error(const cstg_trainer* tr);
 int cstg_trainer_accumulate(cstg_trainer* tr, cstg_ctx* ctx, int n_samples, const double* d_R, const double* d_E,
                             double* losses);
 int cstg_trainer_step(cstg_trainer* tr, float lr, float grad_scale);
+/* The same for the network as the post-smoother of the learned multigrid cycle
+ * (CSTG_PRECOND_LEARNED_MG): per sample, x_fix = pre-smoothing + coarse correction of r (fixed),
+ * r2 = r - A x_fix, z = x_fix + omega D^-1 (r2 + s2 Y(r2 / s2)), s2 = RMS(r2), omega =
+ * 4 / (3 lambda_max(D^-1 A)), and the loss 1 - (z'r)^2 / ((z'Az)(e'r)) of the whole cycle's
+ * output; the gradient flows through the network's one application. Needs cstg_learned_setup
+ * on the context (its multigrid hierarchy is built when missing). */
+int cstg_trainer_accumulate_cycle(cstg_trainer* tr, cstg_ctx* ctx, int n_samples, const double* d_R,
+                                  const double* d_E, double* losses);
+/* The learned cycle's parts for one residual (device vectors of n_rows doubles; any output may be
+ * NULL): x_fix (pre-smoothing + coarse correction), r2 = r - A x_fix (FP32 finest operator),
+ * winvd = omega D^-1, and z = the whole cycle's output. For checks against the CPU oracle. */
+int cstg_learned_cycle_parts_device(cstg_ctx* ctx, const double* d_r, double* d_xfix, double* d_r2,
+                                    double* d_winvd, double* d_z);
 int cstg_trainer_params(cstg_trainer* tr, float* params, float* grads);
 int cstg_trainer_zero_grad(cstg_trainer* tr);
 

@@ -444,7 +444,50 @@ int vcycle(cstg_ctx* ctx, AmgData* d, size_t l, const double* b, double* x, cons
   return CSTG_OK;
 }
 
+// The learned cycle's fixed part on the finest level: x = two Chebyshev (or damped-Jacobi)
+// pre-smoothing steps from x = 0, then the coarse correction x += P V(P'(b - A x)); the
+// post-smoothing step is the network's (learned_api.cu). With a one-level hierarchy x is the
+// dense solve.
+int vcycle_pre(cstg_ctx* ctx, AmgData* d, const double* b, double* x, const int* skip) {
+  if (d->nl == 1) return vcycle(ctx, d, 0, b, x, skip, nullptr);
+  AmgLevel& lv = d->L[0];
+  cudaStream_t s = ctx->stream;
+  AmgLevel& nx = d->L[1];
+  const MixedMatrix mm = mixed_view(ctx);
+  const double* dinv = buf_ptr<double>(lv.dinv);
+  const double* lam = buf_ptr<double>(lv.lam);
+  double* r = buf_ptr<double>(lv.r);
+  CK(amg_sweep_f32(skip, kSweepFirst, d->cheb, mm, dinv, lam, b, nullptr, nullptr, x, s));
+  CK(amg_sweep_f32(skip, kSweepResidual, d->cheb, mm, dinv, lam, b, x, nullptr, r, s));
+  CK(amg_restrict_f32(skip, lv.B, lv.nc, buf_ptr<int>(lv.pt_ptr), buf_ptr<int>(lv.pt_row), buf_ptr<float>(lv.pt32), r,
+                      buf_ptr<double>(nx.bc), s));
+  const int rc = vcycle(ctx, d, 1, buf_ptr<double>(nx.bc), buf_ptr<double>(nx.xb), skip, nullptr);
+  if (rc) return rc;
+  CK(amg_prolong_f32(skip, lv.B, lv.n, buf_ptr<int>(lv.p_ptr), buf_ptr<int>(lv.p_col), buf_ptr<float>(lv.p32),
+                     buf_ptr<double>(nx.xb), x, s));
+  return CSTG_OK;
+}
+
 }  // namespace
+
+int cstg_host::amg_apply_pre(cstg_ctx* ctx, const double* b, double* x, const int* skip) {
+  return vcycle_pre(ctx, ctx->amg, b, x, skip);
+}
+
+int cstg_host::amg_residual_fine(cstg_ctx* ctx, const double* b, const double* x, double* out, const int* skip) {
+  AmgData* d = ctx->amg;
+  AmgLevel& lv = d->L[0];
+  const MixedMatrix mm = mixed_view(ctx);
+  CK(amg_sweep_f32(skip, kSweepResidual, d->cheb, mm, buf_ptr<double>(lv.dinv), buf_ptr<double>(lv.lam), b, x, nullptr,
+                   out, ctx->stream));
+  return CSTG_OK;
+}
+
+double* cstg_host::amg_fine_scratch(cstg_ctx* ctx) { return buf_ptr<double>(ctx->amg->L[0].r); }
+
+const double* cstg_host::amg_fine_lambda(cstg_ctx* ctx) { return buf_ptr<double>(ctx->amg->L[0].lam); }
+
+unsigned long long cstg_host::amg_built_for(const cstg_ctx* ctx) { return ctx->amg ? ctx->amg->built_for : ~0ull; }
 
 int cstg_host::amg_ready(cstg_ctx* ctx) {
   if (ctx->amg && ctx->amg->built_for == ctx->setup_count && ctx->mixed_ready) return CSTG_OK;

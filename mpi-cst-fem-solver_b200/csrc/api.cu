@@ -665,7 +665,7 @@ static int run_solve(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg_s
                     chunks);
       const int it0 = ctx->h_state->iter;
       if (persist) {
-        CK(launch_pcg_persistent(w, bm, mixed ? &mm : nullptr, o.max_refinements, ctx->stream));
+        CK(launch_pcg_persistent(w, bm, mixed ? &mm : nullptr, o.max_refinements, ctx->barrier_spin, ctx->stream));
       } else {
         CK(cudaGraphLaunch(ctx->graph, ctx->stream));
         count_launches(per_iter * chunk);
@@ -675,8 +675,15 @@ static int run_solve(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg_s
       }
       rc = snapshot(ctx);
       if (rc) return rc;
-      if (ctx->h_state->done == CSTG_SOLVE_TIMEOUT + 1)
+      if (ctx->h_state->done == CSTG_SOLVE_TIMEOUT + 1) {
+        if (stats) {
+          std::memset(stats, 0, sizeof *stats);
+          stats->status = CSTG_SOLVE_TIMEOUT;
+          stats->iterations = ctx->h_state->iter;
+          g_fmt(stats->message, sizeof stats->message, "a grid barrier of the persistent solve timed out");
+        }
         return fail(ctx, CSTG_ERR_TIMEOUT, "pcg_solve: a grid barrier of the persistent solve timed out");
+      }
       spmv_calls += ctx->h_state->iter - it0 + (ctx->h_state->done == CSTG_SOLVE_BREAKDOWN + 1);
     }
     // true residual (solver.cpp:117-122); with true_residual_stop it may re-open the solve
@@ -765,7 +772,7 @@ static int check_solve_args(cstg_ctx* ctx, const cstg_solver_options* opt, cstg_
     return fail(ctx, CSTG_ERR_UNSUPPORTED,
                 "pcg_solve: mixed precision needs the mesh (2x2-block) pattern of cstg_build_pattern");
   if (o.preconditioner != CSTG_PRECOND_JACOBI && o.preconditioner != CSTG_PRECOND_LEARNED &&
-      o.preconditioner != CSTG_PRECOND_AMG)
+      o.preconditioner != CSTG_PRECOND_AMG && o.preconditioner != CSTG_PRECOND_LEARNED_MG)
     return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "pcg_solve: unknown preconditioner %d", o.preconditioner);
   if (o.preconditioner == CSTG_PRECOND_AMG) {
     if (ctx->kind != 1)
@@ -773,7 +780,7 @@ static int check_solve_args(cstg_ctx* ctx, const cstg_solver_options* opt, cstg_
     if (o.record_history)
       return fail(ctx, CSTG_ERR_UNSUPPORTED, "pcg_solve: no residual history with the multigrid preconditioner");
   }
-  if (o.preconditioner == CSTG_PRECOND_LEARNED) {
+  if (o.preconditioner == CSTG_PRECOND_LEARNED || o.preconditioner == CSTG_PRECOND_LEARNED_MG) {
     if (ctx->kind != 1)
       return fail(ctx, CSTG_ERR_UNSUPPORTED, "pcg_solve: the learned preconditioner needs the mesh pattern");
     if (!ctx->learned_ready || ctx->learned_setup != ctx->setup_count)

@@ -107,6 +107,15 @@ struct cstg_ctx {
 
   // smoothed-aggregation multigrid hierarchy (built on demand)
   AmgData* amg = nullptr;
+
+  // learned multigrid cycle: the post-smoother's weights omega D^-1 (omega = 4 / (3 lambda_max)),
+  // built for the hierarchy of setup `lm_winvd_for`
+  DevBuf lm_winvd;
+  unsigned long long lm_winvd_for = ~0ull;
+
+  // bounded device waits (polls before a wait gives up; cstg_set_wait_limits)
+  long long barrier_spin = kBarrierSpinDefault;
+  long long mbar_spin = kMpMbarSpinDefault;
 };
 
 namespace cstg_host {
@@ -261,6 +270,14 @@ void amg_free(cstg_ctx* ctx);
 int amg_levels(const cstg_ctx* ctx);
 int amg_chebyshev(const cstg_ctx* ctx);  // 1: Chebyshev smoothing, 0: damped Jacobi
 unsigned long long amg_signature(const cstg_ctx* ctx);  // level shapes of the current hierarchy
+// The learned cycle's pieces (the hierarchy must be ready): x = pre-smoothing + coarse correction
+// of b (no post-smoothing); out = b - A x with the finest level's FP32 operator; the finest
+// level's residual scratch (free outside a cycle); lambda_max(D^-1 A) of the finest level (device).
+int amg_apply_pre(cstg_ctx* ctx, const double* b, double* x, const int* skip);
+int amg_residual_fine(cstg_ctx* ctx, const double* b, const double* x, double* out, const int* skip);
+double* amg_fine_scratch(cstg_ctx* ctx);
+const double* amg_fine_lambda(cstg_ctx* ctx);
+unsigned long long amg_built_for(const cstg_ctx* ctx);  // setup_count of the hierarchy (~0: none)
 
 // Defined in learned_api.cu: flexible CG with the learned preconditioner.
 int run_fcg(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg_solver_options& o, cstg_stats* stats);

@@ -200,14 +200,20 @@ struct MpScratch {  // small device scalars of the network's reductions
   double partials[3 * 296];
 };
 
+constexpr long long kMpMbarSpinDefault = 1LL << 22;  // polls of the tensor-core wait before it gives up
 cudaError_t mpnn_prepare_device();
 cudaError_t launch_mp_params(const float* p32, __nv_bfloat16* pb, float* pf, cudaStream_t s);
-cudaError_t launch_mp_rr(int n, const double* r, MpScratch* sc, cudaStream_t s);
-// z = M(r): encoder, three tensor-core layers, decoder. `rr` points at r'r (device), `skip`
-// (device int, may be null) turns the network off (z = D^-1 r).
+cudaError_t launch_mp_rr(int n, const double* r, MpScratch* sc, cudaStream_t s, const int* skip = nullptr);
+// out = factor / lambda (lambda: one device double) * invd
+cudaError_t launch_mp_smoother_weights(int n, const double* invd, const double* lam, double factor, double* out,
+                                       cudaStream_t s);
+// z = zbase + M(r): encoder, three tensor-core layers (the last with the decoder). `rr` points at
+// r'r (device), `skip` (device int, may be null) turns the network off (z = zbase + D^-1 r),
+// zbase may be null (z = M(r)) or z itself. spin_limit: polls of the tensor-core wait before it
+// reports a timeout (kMpMbarSpinDefault normally).
 cudaError_t launch_mp_forward(const MpnnGraph& g, const MpnnParams& P, const double* r, const double* invd,
                               const double* rr, const float* sf, const int* skip, MpnnWork& w, bool train,
-                              double* z, int* err, cudaStream_t s);
+                              const double* zbase, double* z, long long spin_limit, int* err, cudaStream_t s);
 cudaError_t launch_mp_loss(int N, const double* z, const double* az, const double* r, const double* e,
                            const double* invd, MpScratch* sc, MpnnWork& w, cudaStream_t s);
 cudaError_t launch_mp_backward(const MpnnGraph& g, const MpnnParams& P, MpnnWork& w, float* grad, cudaStream_t s);
@@ -413,7 +419,9 @@ cudaError_t launch_true_residual(const PcgBuffers& w, bool restart, int max_repl
 
 // persistent.cu: every iteration of a mesh-pattern solve in one cooperative kernel (FP64, or
 // mixed when A32 is given); the state must be initialised (launch_pcg_init / launch_mixed_init).
+// spin_limit: polls of a grid-barrier wait before the solve gives up (kBarrierSpinDefault).
+constexpr long long kBarrierSpinDefault = 50000000LL;  // polls of ~40 ns: ~2 s
 cudaError_t launch_pcg_persistent(const PcgBuffers& w, const BlockMatrix& A64, const MixedMatrix* A32,
-                                  int max_final_checks, cudaStream_t s);
+                                  int max_final_checks, long long spin_limit, cudaStream_t s);
 
 }  // namespace cstg

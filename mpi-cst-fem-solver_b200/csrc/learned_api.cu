@@ -48,6 +48,36 @@ int upload_params(cstg_ctx* ctx, const float* params) {
   return CSTG_OK;
 }
 
+// The learned cycle's post-smoother weights omega D^-1 (omega = 4 / (3 lambda_max(D^-1 A))) for the
+// current hierarchy, which is built when missing.
+int cycle_ready(cstg_ctx* ctx) {
+  const int rc = amg_ready(ctx);
+  if (rc) return rc;
+  if (ctx->lm_winvd_for == amg_built_for(ctx)) return CSTG_OK;
+  const int n = ctx->n_rows;
+  ENSURE(ctx->lm_winvd, sizeof(double) * (size_t)std::max(n, 1));
+  CK(launch_mp_smoother_weights(n, buf_ptr<double>(ctx->inv_diag), amg_fine_lambda(ctx), 4.0 / 3.0,
+                                buf_ptr<double>(ctx->lm_winvd), ctx->stream));
+  ctx->lm_winvd_for = amg_built_for(ctx);
+  return CSTG_OK;
+}
+
+// z = learned cycle of r on stream s (the context's): z = x_fix (pre-smoothing + coarse
+// correction), r2 = r - A z in the finest level's scratch, z += omega D^-1 (r2 + s2 Y(r2 / s2)).
+// train: the network keeps its activations in mw (the trainer's buffers).
+int cycle_apply(cstg_ctx* ctx, const MpnnGraph& g, const MpnnParams& P, MpnnWork& mw, MpScratch* msc,
+                const double* winvd, const double* r, double* z, const int* skip, bool train, cudaStream_t s) {
+  int rc = amg_apply_pre(ctx, r, z, skip);
+  if (rc) return rc;
+  double* r2 = amg_fine_scratch(ctx);
+  rc = amg_residual_fine(ctx, r, z, r2, skip);
+  if (rc) return rc;
+  CK(launch_mp_rr(ctx->n_rows, r2, msc, s, skip));
+  CK(launch_mp_forward(g, P, r2, winvd, &msc->rr, buf_ptr<float>(ctx->lp_sf), skip, mw, train, z, z, ctx->mbar_spin,
+                       buf_ptr<int>(ctx->err_word), s));
+  return CSTG_OK;
+}
+
 }  // namespace
 
 // ---- flexible CG ------------------------------------------------------------------------------
@@ -55,9 +85,17 @@ int upload_params(cstg_ctx* ctx, const float* params) {
 int cstg_host::run_fcg(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg_solver_options& o,
                        cstg_stats* stats) {
   const int n = ctx->n_rows, N = ctx->n_nodes;
-  const bool use_amg = o.preconditioner == CSTG_PRECOND_AMG;
+  // the learned cycle: multigrid pre-smoothing and coarse correction, the network as the
+  // finest level's post-smoother
+  const bool cycle_net = o.preconditioner == CSTG_PRECOND_LEARNED_MG;
+  const bool use_amg = o.preconditioner == CSTG_PRECOND_AMG || cycle_net;
+  const bool use_net = o.preconditioner == CSTG_PRECOND_LEARNED || cycle_net;
   if (use_amg) {
     const int rc = amg_ready(ctx);  // the multigrid hierarchy of this matrix (built once per setup)
+    if (rc) return rc;
+  }
+  if (cycle_net) {
+    const int rc = cycle_ready(ctx);
     if (rc) return rc;
   }
   ENSURE(ctx->x, sizeof(double) * (size_t)n);
@@ -65,7 +103,7 @@ int cstg_host::run_fcg(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg
   ENSURE(ctx->p, sizeof(double) * (size_t)n);
   ENSURE(ctx->Ap, sizeof(double) * (size_t)n);
   ENSURE(ctx->lp_z, sizeof(double) * (size_t)n);
-  if (!use_amg) {
+  if (use_net) {
     ENSURE(ctx->lp_h0, sizeof(__nv_bfloat16) * (size_t)N * kMpF);
     ENSURE(ctx->lp_h1, sizeof(__nv_bfloat16) * (size_t)N * kMpF);
   }
@@ -98,17 +136,23 @@ int cstg_host::run_fcg(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg
   // With the multigrid cycle the scalars z'r, z'q and beta are taken inside the cycle's last
   // finest-level sweep (no separate dots pass), and there is no stagnation fallback (the cycle is
   // a fixed symmetric positive operator).
-  const bool fused_dots = use_amg && amg_levels(ctx) > 1;
+  const bool fused_dots = o.preconditioner == CSTG_PRECOND_AMG && amg_levels(ctx) > 1;
+  MpScratch* msc = buf_ptr<MpScratch>(ctx->lp_sc);
+  const double* winvd = cycle_net ? buf_ptr<double>(ctx->lm_winvd) : nullptr;
   FcgDotSink sink;
   sink.q = w.q;
   sink.partials = w.partials;
   sink.st = w.st;
   auto precondition = [&]() -> int {
-    if (use_amg) {
+    if (cycle_net) {
+      const int rc = cycle_apply(ctx, g, P, mw, msc, winvd, w.r, w.z, skip, false, ctx->stream);
+      if (rc) return rc;
+    } else if (use_amg) {
       const int rc = amg_apply(ctx, w.r, w.z, &w.st->done, fused_dots ? &sink : nullptr);  // (cycles after
       if (rc) return rc;                                                                   // convergence return at once)
     } else {
-      CK(launch_mp_forward(g, P, w.r, w.inv_diag, rr, sf, skip, mw, false, w.z, err, ctx->stream));
+      CK(launch_mp_forward(g, P, w.r, w.inv_diag, rr, sf, skip, mw, false, nullptr, w.z, ctx->mbar_spin, err,
+                           ctx->stream));
     }
     if (fused_dots)
       CK(launch_fcg_pupdate(w, ctx->stream));
@@ -121,7 +165,7 @@ int cstg_host::run_fcg(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg
       CK(launch_spmv_mixed_pcg(mm, bm, w.p, w.q, w.partials, w.st, ctx->stream));
     else
       CK(launch_spmv_pcg(bm, w.p, w.q, w.partials, w.st, ctx->stream));
-    CK(launch_fcg_update(w, use_amg ? 0 : kFcgWindow, kFcgRatio2, ctx->stream));
+    CK(launch_fcg_update(w, o.preconditioner == CSTG_PRECOND_AMG ? 0 : kFcgWindow, kFcgRatio2, ctx->stream));
     return precondition();
   };
   const int chunk = o.check_interval > 0 ? o.check_interval : 25;
@@ -229,7 +273,13 @@ int cstg_host::run_fcg(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg
     stats->solve_seconds = ms * 1e-3;
     stats->spmv_calls = spmv_calls;
     char pre[160];
-    if (use_amg)
+    if (cycle_net && fallback_iter >= 0)
+      g_fmt(pre, sizeof pre, "learned multigrid cycle, switched to Jacobi at iteration %d (stagnation)",
+            fallback_iter);
+    else if (cycle_net)
+      g_fmt(pre, sizeof pre, "learned multigrid cycle: %s pre-smoothing, network post-smoothing, %d levels",
+            amg_chebyshev(ctx) ? "Chebyshev" : "damped-Jacobi", amg_levels(ctx));
+    else if (use_amg)
       g_fmt(pre, sizeof pre, "smoothed-aggregation multigrid V(2,2), %s smoothing, %d levels",
             amg_chebyshev(ctx) ? "Chebyshev" : "damped-Jacobi", amg_levels(ctx));
     else if (fallback_iter >= 0)
@@ -406,6 +456,8 @@ int cstg_learned_apply_device(cstg_ctx* ctx, const double* d_r, double* d_z) {
   if (!ctx->learned_ready || ctx->learned_setup != ctx->setup_count)
     return fail(ctx, CSTG_ERR_STATE, "learned_apply: call cstg_learned_setup after cstg_pcg_setup");
   if (ctx->n_rows && (!d_r || !d_z)) return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "learned_apply: null vector");
+  if (!aligned16(d_r) || !aligned16(d_z))
+    return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "learned_apply: device vectors must be 16-byte aligned");
   const int N = ctx->n_nodes;
   ENSURE(ctx->lp_h0, sizeof(__nv_bfloat16) * (size_t)N * kMpF);
   ENSURE(ctx->lp_h1, sizeof(__nv_bfloat16) * (size_t)N * kMpF);
@@ -414,8 +466,8 @@ int cstg_learned_apply_device(cstg_ctx* ctx, const double* d_r, double* d_z) {
   RESET_ERR();
   CK(launch_mp_rr(ctx->n_rows, d_r, sc, ctx->stream));
   CK(launch_mp_forward(graph_view(ctx), params_view(ctx), d_r, buf_ptr<double>(ctx->inv_diag), &sc->rr,
-                       buf_ptr<float>(ctx->lp_sf), nullptr, mw, false, d_z, buf_ptr<int>(ctx->err_word),
-                       ctx->stream));
+                       buf_ptr<float>(ctx->lp_sf), nullptr, mw, false, nullptr, d_z, ctx->mbar_spin,
+                       buf_ptr<int>(ctx->err_word), ctx->stream));
   READ_ERR();
   if (ctx->h_err[kErrTimeout] != kErrNone)
     return fail(ctx, CSTG_ERR_TIMEOUT, "learned_apply: a tensor-core wait timed out");
@@ -493,6 +545,8 @@ int cstg_trainer_accumulate(cstg_trainer* tr, cstg_ctx* ctx, int n_samples, cons
     return tfail(tr, CSTG_ERR_STATE, "trainer_accumulate: call cstg_learned_setup on the context first");
   if (n_samples < 0 || (n_samples > 0 && (!d_R || !d_E)))
     return tfail(tr, CSTG_ERR_INVALID_ARGUMENT, "trainer_accumulate: bad samples");
+  if (!aligned16(d_R) || !aligned16(d_E))
+    return tfail(tr, CSTG_ERR_INVALID_ARGUMENT, "trainer_accumulate: samples must be 16-byte aligned");
   const int N = ctx->n_nodes, n = ctx->n_rows;
   MpnnWork w;
   int rc = trainer_work(tr, N, w);
@@ -514,7 +568,8 @@ int cstg_trainer_accumulate(cstg_trainer* tr, cstg_ctx* ctx, int n_samples, cons
     const double* r = d_R + (size_t)i * n;
     const double* e = d_E + (size_t)i * n;
     TK(launch_mp_rr(n, r, sc, tr->stream));
-    TK(launch_mp_forward(g, P, r, invd, &sc->rr, buf_ptr<float>(ctx->lp_sf), nullptr, w, true, z, err, tr->stream));
+    TK(launch_mp_forward(g, P, r, invd, &sc->rr, buf_ptr<float>(ctx->lp_sf), nullptr, w, true, nullptr, z,
+                         ctx->mbar_spin, err, tr->stream));
     TK(launch_spmv(&bm, nullptr, z, az, tr->stream));
     TK(launch_mp_loss(N, z, az, r, e, invd, sc, w, tr->stream));
     if (losses) TK(cudaMemcpyAsync(&losses[i], &sc->loss, sizeof(double), cudaMemcpyDeviceToHost, tr->stream));
@@ -558,6 +613,112 @@ int cstg_trainer_zero_grad(cstg_trainer* tr) {
   TK(cudaSetDevice(tr->device));
   TK(cudaMemsetAsync(tr->grad.p, 0, sizeof(float) * kMpParams, tr->stream));
   TK(cudaStreamSynchronize(tr->stream));
+  return CSTG_OK;
+}
+
+}  // extern "C"
+
+// ---- the learned multigrid cycle: training and parts ------------------------------------------
+
+extern "C" {
+
+int cstg_set_wait_limits(cstg_ctx* ctx, long long barrier_polls, long long mma_polls) {
+  BEGIN(ctx);
+  if (barrier_polls < -1 || mma_polls < -1)
+    return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "set_wait_limits: limits must be >= 0 (or -1 for the default)");
+  ctx->barrier_spin = barrier_polls < 0 ? kBarrierSpinDefault : barrier_polls;
+  ctx->mbar_spin = mma_polls < 0 ? kMpMbarSpinDefault : mma_polls;
+  return CSTG_OK;
+}
+
+int cstg_learned_cycle_parts_device(cstg_ctx* ctx, const double* d_r, double* d_xfix, double* d_r2, double* d_winvd,
+                                    double* d_z) {
+  BEGIN(ctx);
+  if (!ctx->learned_ready || ctx->learned_setup != ctx->setup_count)
+    return fail(ctx, CSTG_ERR_STATE, "learned_cycle_parts: call cstg_learned_setup after cstg_pcg_setup");
+  if (ctx->n_rows && !d_r) return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "learned_cycle_parts: null residual");
+  if (!aligned16(d_r) || !aligned16(d_xfix) || !aligned16(d_r2) || !aligned16(d_winvd) || !aligned16(d_z))
+    return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "learned_cycle_parts: device vectors must be 16-byte aligned");
+  int rc = cycle_ready(ctx);
+  if (rc) return rc;
+  const int n = ctx->n_rows, N = ctx->n_nodes;
+  const size_t bytes = sizeof(double) * (size_t)n;
+  ENSURE(ctx->lp_z, bytes);
+  ENSURE(ctx->lp_h0, sizeof(__nv_bfloat16) * (size_t)N * kMpF);
+  ENSURE(ctx->lp_h1, sizeof(__nv_bfloat16) * (size_t)N * kMpF);
+  double* z = buf_ptr<double>(ctx->lp_z);
+  MpScratch* msc = buf_ptr<MpScratch>(ctx->lp_sc);
+  MpnnWork mw = infer_work(ctx);
+  RESET_ERR();
+  rc = amg_apply_pre(ctx, d_r, z, nullptr);
+  if (rc) return rc;
+  if (d_xfix && n) CK(cudaMemcpyAsync(d_xfix, z, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+  double* r2 = amg_fine_scratch(ctx);
+  rc = amg_residual_fine(ctx, d_r, z, r2, nullptr);
+  if (rc) return rc;
+  if (d_r2 && n) CK(cudaMemcpyAsync(d_r2, r2, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+  if (d_winvd && n) CK(cudaMemcpyAsync(d_winvd, ctx->lm_winvd.p, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+  CK(launch_mp_rr(n, r2, msc, ctx->stream));
+  CK(launch_mp_forward(graph_view(ctx), params_view(ctx), r2, buf_ptr<double>(ctx->lm_winvd), &msc->rr,
+                       buf_ptr<float>(ctx->lp_sf), nullptr, mw, false, z, z, ctx->mbar_spin,
+                       buf_ptr<int>(ctx->err_word), ctx->stream));
+  if (d_z && n) CK(cudaMemcpyAsync(d_z, z, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+  READ_ERR();
+  if (ctx->h_err[kErrTimeout] != kErrNone)
+    return fail(ctx, CSTG_ERR_TIMEOUT, "learned_cycle_parts: a tensor-core wait timed out");
+  return CSTG_OK;
+}
+
+int cstg_trainer_accumulate_cycle(cstg_trainer* tr, cstg_ctx* ctx, int n_samples, const double* d_R,
+                                  const double* d_E, double* losses) {
+  if (!tr) return CSTG_ERR_INVALID_ARGUMENT;
+  tr->err.clear();
+  TK(cudaSetDevice(tr->device));
+  if (!ctx || ctx->device != tr->device)
+    return tfail(tr, CSTG_ERR_INVALID_ARGUMENT, "trainer_accumulate: the context must be on the trainer's device");
+  if (!ctx->learned_ready || ctx->learned_setup != ctx->setup_count)
+    return tfail(tr, CSTG_ERR_STATE, "trainer_accumulate: call cstg_learned_setup on the context first");
+  if (n_samples < 0 || (n_samples > 0 && (!d_R || !d_E)))
+    return tfail(tr, CSTG_ERR_INVALID_ARGUMENT, "trainer_accumulate: bad samples");
+  if (!aligned16(d_R) || !aligned16(d_E))
+    return tfail(tr, CSTG_ERR_INVALID_ARGUMENT, "trainer_accumulate: samples must be 16-byte aligned");
+  {
+    const int rc = cycle_ready(ctx);  // (the context's own error text on failure)
+    if (rc) return tfail(tr, rc, "trainer_accumulate: %s", ctx->err.c_str());
+  }
+  const int N = ctx->n_nodes, n = ctx->n_rows;
+  MpnnWork w;
+  int rc = trainer_work(tr, N, w);
+  if (rc) return rc;
+  // everything runs on the context's stream, where the hierarchy and the samples' producers are
+  TK(cudaStreamSynchronize(tr->stream));
+  cudaStream_t s = ctx->stream;
+  const MpnnGraph g = graph_view(ctx);
+  MpnnParams P;
+  P.pb = static_cast<const __nv_bfloat16*>(tr->pb.p);
+  P.pf = static_cast<const float*>(tr->pf.p);
+  MpScratch* sc = static_cast<MpScratch*>(tr->sc.p);
+  const BlockMatrix bm = block_view(ctx);
+  const double* winvd = buf_ptr<double>(ctx->lm_winvd);
+  double* z = static_cast<double*>(tr->z.p);
+  double* az = static_cast<double*>(tr->az.p);
+  float* grad = static_cast<float*>(tr->grad.p);
+  int* err = buf_ptr<int>(ctx->err_word);
+  TK(cudaMemsetAsync(err, 0x7f, sizeof(int) * kErrSlots, s));
+  for (int i = 0; i < n_samples; ++i) {
+    const double* r = d_R + (size_t)i * n;
+    const double* e = d_E + (size_t)i * n;
+    rc = cycle_apply(ctx, g, P, w, sc, winvd, r, z, nullptr, true, s);
+    if (rc) return tfail(tr, rc, "trainer_accumulate: %s", ctx->err.c_str());
+    TK(launch_spmv(&bm, nullptr, z, az, s));
+    TK(launch_mp_loss(N, z, az, r, e, winvd, sc, w, s));
+    if (losses) TK(cudaMemcpyAsync(&losses[i], &sc->loss, sizeof(double), cudaMemcpyDeviceToHost, s));
+    TK(launch_mp_backward(g, P, w, grad, s));
+  }
+  int h_err[kErrSlots];
+  TK(cudaMemcpyAsync(h_err, err, sizeof h_err, cudaMemcpyDeviceToHost, s));
+  TK(cudaStreamSynchronize(s));
+  if (h_err[kErrTimeout] != kErrNone) return tfail(tr, CSTG_ERR_TIMEOUT, "trainer: a tensor-core wait timed out");
   return CSTG_OK;
 }
 

@@ -37,8 +37,7 @@ constexpr int F = kMpF;
 constexpr int kTile = 128;             // nodes per tensor-core tile (the MMA's M)
 constexpr int kASmem = kTile * 2 * F * 2;  // A operand bytes (128 x 128 BF16)
 constexpr int kBSmem = F * 2 * F * 2;      // B operand bytes (64 x 128 BF16)
-constexpr int kTcSmem = kASmem + kBSmem + 1024;
-constexpr long long kMbarSpinLimit = 1LL << 22;  // bounded wait for the MMA (far above its ~us)
+constexpr long long kMbarSpinLimit = kMpMbarSpinDefault;  // bounded wait for the MMA (far above its ~us)
 
 __device__ __forceinline__ float bf_lo(uint32_t w) { return __uint_as_float(w << 16); }
 __device__ __forceinline__ float bf_hi(uint32_t w) { return __uint_as_float(w & 0xffff0000u); }
@@ -69,9 +68,9 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint
 constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(F >> 3) << 17) |
                             ((uint32_t)(kTile >> 4) << 24);
 
-// Bounded wait on an mbarrier phase; false when the limit ran out.
-__device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t parity) {
-  for (long long i = 0; i < kMbarSpinLimit; ++i) {
+// Bounded wait on an mbarrier phase; false when `limit` polls ran out (0: give up at once).
+__device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t parity, long long limit) {
+  for (long long i = 0; i < limit; ++i) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -83,15 +82,6 @@ __device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t parity) {
     if (ok) return true;
   }
   return false;
-}
-
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];\n"
-      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-      : "r"(taddr));
 }
 
 // Deterministic sum over the grid: per-block sums, then the last block adds them in order.
@@ -125,12 +115,21 @@ constexpr int kRedGrid = 296;  // fixed grid of the reductions here (2 x 148): a
 
 // ---- residual scale ----------------------------------------------------------------------------
 
-__global__ void __launch_bounds__(256) k_mp_rr(int n, const double* __restrict__ r, MpScratch* sc) {
+__global__ void __launch_bounds__(256) k_mp_rr(int n, const double* __restrict__ r, MpScratch* sc, const int* skip) {
+  if (skip && *skip) return;  // uniform: every block returns before the ticket
   double a = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a = fma(r[i], r[i], a);
   const double v[1] = {a};
   double tot[1];
   if (grid_sum<1, 256>(v, sc->partials, &sc->ticket[0], tot) && threadIdx.x == 0) sc->rr = tot[0];
+}
+
+// ---- the learned cycle's post-smoother weights: out = factor / lambda_max * D^-1 ------------------
+
+__global__ void k_mp_smoother_weights(int n, const double* __restrict__ invd, const double* lam, double factor,
+                                      double* __restrict__ out) {
+  const double w = factor / *lam;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = w * invd[i];
 }
 
 // ---- encoder: H0 = relu(W_in X + b_in) ------------------------------------------------------------
@@ -181,30 +180,101 @@ __global__ void __launch_bounds__(256) k_mp_encode(int N, const double* __restri
 }
 
 // ---- message-passing layer on the tensor cores ----------------------------------------------------
+//
+// A CTA of 8 warps owns a tile of 128 nodes at a time (persistent over tiles).
+//  gather:   each warp builds 16 rows of the A operand, four nodes at once with 8 lanes per node
+//            (lane c holds features 8c..8c+7, one 16-byte chunk): the node's own chunk and the sum
+//            of its neighbours' chunks, four neighbour loads in flight per lane, neighbours in
+//            ascending pattern order (the mean is the same sum in the same order as a serial loop).
+//  MMA:      one thread issues 8 x tcgen05.mma (M=128, N=64, K=16) into 64 TMEM columns and waits
+//            on the commit's mbarrier (bounded); the block learns the outcome through shared memory.
+//  epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31, columns 32 (w / 4) .. +31 (its node's half
+//            row), adds bias, ReLU and the residual, and stages the BF16 row half in shared memory
+//            (16-byte chunks XOR-swizzled by row, so the stores do not collide on banks); the tile
+//            then leaves in coalesced 16-byte stores. The last layer also runs the decoder there:
+//            y = W_out H3 + b_out, summed over the 64 features in order (the first half by the
+//            warps of columns 0..31, handed through shared memory to those of columns 32..63), and
+//            z = zbase + invd (r + s y).
+constexpr int kLT = 256;                            // threads of the layer kernel
+constexpr int kTcSmem = kASmem + kBSmem + 1024;     // dynamic shared memory (1024-byte aligned base)
 
-template <bool TRAIN>
-__global__ void __launch_bounds__(128, 3) k_mp_layer_tc(int N, const int* __restrict__ node_ptr,
-                                                         const int* __restrict__ nbr,
-                                                         const __nv_bfloat16* __restrict__ Hin, MpnnParams P,
-                                                         int layer, const int* skip,
-                                                         __nv_bfloat16* __restrict__ Hout,
-                                                         __nv_bfloat16* __restrict__ Gout,
-                                                         __nv_bfloat16* __restrict__ Aout, int* err) {
-  if (skip && *skip) return;  // uniform: before any barrier or tensor-memory allocation
+struct MpLayerArgs {
+  int N;
+  const int* node_ptr;
+  const int* nbr;
+  const __nv_bfloat16* Hin;
+  MpnnParams P;
+  int layer;
+  const int* skip;
+  __nv_bfloat16* Hout;  // may be null in the last layer (inference)
+  __nv_bfloat16* Gout;  // TRAIN: ReLU outputs
+  __nv_bfloat16* Aout;  // TRAIN: neighbour means
+  // decoder (last layer)
+  const double* r;
+  const double* invd;
+  const double* rr;
+  double inv_n;
+  const double* zbase;  // may be null (z = the network's output alone)
+  double* z;
+  float* Yout;          // TRAIN
+  long long spin_limit;
+  int* err;
+};
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+        "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+        "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+      : "r"(taddr));
+}
+
+__device__ __forceinline__ void add_chunk(float (&acc)[8], const uint4 v) {
+  acc[0] += bf_lo(v.x);
+  acc[1] += bf_hi(v.x);
+  acc[2] += bf_lo(v.y);
+  acc[3] += bf_hi(v.y);
+  acc[4] += bf_lo(v.z);
+  acc[5] += bf_hi(v.z);
+  acc[6] += bf_lo(v.w);
+  acc[7] += bf_hi(v.w);
+}
+
+template <bool TRAIN, bool LAST>
+__global__ void __launch_bounds__(kLT, 3) k_mp_layer_tc(const MpLayerArgs a) {
+  const int N = a.N;
+  if (a.skip && *a.skip) {  // uniform: before any barrier or tensor-memory allocation
+    if (LAST)                 // the network is off: the Jacobi step
+      for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 2 * N; i += gridDim.x * blockDim.x)
+        a.z[i] = (a.zbase ? a.zbase[i] : 0.0) + a.invd[i] * a.r[i];
+    return;
+  }
   extern __shared__ uint8_t smem_raw[];
   __shared__ uint64_t mbar;
   __shared__ uint32_t tmem_slot;
+  __shared__ int mma_ok;
+  __shared__ float wout[2 * F], bout[2];
+  __shared__ float2 ypart[kTile];
   uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
   uint8_t* sA = base;            // element (m, k): (k/8)*2048 + (m/8)*128 + (m%8)*16 + (k%8)*2
   uint8_t* sB = base + kASmem;   // element (n, k): (k/8)*1024 + (n/8)*128 + (n%8)*16 + (k%8)*2
-  const int t = threadIdx.x, warp = t >> 5;
-  const __nv_bfloat16* W = P.pb + kMpOffL0 + layer * kMpLStride;
-  const float* bias = P.pf + kMpOffL0 + layer * kMpLStride + F * 2 * F;
+  uint8_t* sOut = sA + kASmem / 2;  // staged output tile (the mean half of A, free after the MMA)
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const __nv_bfloat16* W = a.P.pb + kMpOffL0 + a.layer * kMpLStride;
+  const float* bias = a.P.pf + kMpOffL0 + a.layer * kMpLStride + F * 2 * F;
 
-  for (int idx = t; idx < F * 16; idx += 128) {  // 64 rows x 16 chunks of 8 BF16
+  for (int idx = t; idx < F * 16; idx += kLT) {  // 64 rows x 16 chunks of 8 BF16
     const int n = idx >> 4, kc = idx & 15;
     const uint4 v = *reinterpret_cast<const uint4*>(W + n * 2 * F + kc * 8);
     *reinterpret_cast<uint4*>(sB + kc * 1024 + (n >> 3) * 128 + (n & 7) * 16) = v;
+  }
+  if (LAST) {
+    for (int i = t; i < 2 * F; i += kLT) wout[i] = bf(a.P.pb[kMpOffWout + i]);
+    if (t < 2) bout[t] = a.P.pf[kMpOffBout + t];
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_slot)),
@@ -220,54 +290,52 @@ __global__ void __launch_bounds__(128, 3) k_mp_layer_tc(int N, const int* __rest
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   const uint32_t tmem = tmem_slot;
   const uint32_t a_addr = smem_u32(sA), b_addr = smem_u32(sB), mbar_addr = smem_u32(&mbar);
+  const double s = LAST ? sqrt(*a.rr * a.inv_n) : 0.0;
   uint32_t phase = 0;
+  const int g = lane >> 3, c = lane & 7;    // gather: node group of the warp, feature chunk
+  const int q = warp & 3, h = warp >> 2;    // epilogue: TMEM lane quarter, column half
 
   for (int tile = blockIdx.x; tile * kTile < N; tile += gridDim.x) {
-    const int n = tile * kTile + t;
-    uint4 own[8];
-    float acc[F];
+    // ---- gather: own chunk and the neighbours' mean chunk of 16 nodes per warp
+#pragma unroll 1
+    for (int rnd = 0; rnd < 4; ++rnd) {
+      const int m = warp * 16 + rnd * 4 + g;
+      const int n = tile * kTile + m;
+      uint4 own = make_uint4(0u, 0u, 0u, 0u);
+      float acc[8];
 #pragma unroll
-    for (int o = 0; o < F; ++o) acc[o] = 0.f;
-    int deg = 0;
-    if (n < N) {
-      const uint4* hr = reinterpret_cast<const uint4*>(Hin + (size_t)n * F);
+      for (int j = 0; j < 8; ++j) acc[j] = 0.f;
+      int deg = 0;
+      if (n < N) {
+        own = __ldg(reinterpret_cast<const uint4*>(a.Hin + (size_t)n * F) + c);
+        const int k0 = __ldg(&a.node_ptr[n]), k1 = __ldg(&a.node_ptr[n + 1]);
+        for (int k = k0; k < k1; k += 4) {
+          int mm[4];
+          uint4 v[4];
 #pragma unroll
-      for (int c = 0; c < 8; ++c) own[c] = __ldg(hr + c);
-      const int k0 = __ldg(&node_ptr[n]), k1 = __ldg(&node_ptr[n + 1]);
-      for (int k = k0; k < k1; ++k) {
-        const int m = __ldg(&nbr[k]);
-        if (m == n) continue;
-        ++deg;
-        const uint4* hm = reinterpret_cast<const uint4*>(Hin + (size_t)m * F);
+          for (int j = 0; j < 4; ++j) mm[j] = k + j < k1 ? __ldg(&a.nbr[k + j]) : n;
 #pragma unroll
-        for (int c = 0; c < 8; ++c) {
-          const uint4 v = __ldg(hm + c);
-          acc[c * 8 + 0] += bf_lo(v.x);
-          acc[c * 8 + 1] += bf_hi(v.x);
-          acc[c * 8 + 2] += bf_lo(v.y);
-          acc[c * 8 + 3] += bf_hi(v.y);
-          acc[c * 8 + 4] += bf_lo(v.z);
-          acc[c * 8 + 5] += bf_hi(v.z);
-          acc[c * 8 + 6] += bf_lo(v.w);
-          acc[c * 8 + 7] += bf_hi(v.w);
+          for (int j = 0; j < 4; ++j)
+            v[j] = mm[j] != n ? __ldg(reinterpret_cast<const uint4*>(a.Hin + (size_t)mm[j] * F) + c)
+                              : make_uint4(0u, 0u, 0u, 0u);
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+            if (mm[j] != n) {
+              ++deg;
+              add_chunk(acc, v[j]);
+            }
         }
       }
-    } else {
-#pragma unroll
-      for (int c = 0; c < 8; ++c) own[c] = make_uint4(0u, 0u, 0u, 0u);
-    }
-    const float inv = deg ? 1.f / (float)deg : 0.f;
-    const uint32_t row_off = (uint32_t)((t >> 3) * 128 + (t & 7) * 16);
-#pragma unroll
-    for (int c = 0; c < 8; ++c) {
-      *reinterpret_cast<uint4*>(sA + c * 2048 + row_off) = own[c];
+      const float inv = deg ? 1.f / (float)deg : 0.f;
       uint4 av;
-      av.x = pack_bf2(acc[c * 8 + 0] * inv, acc[c * 8 + 1] * inv);
-      av.y = pack_bf2(acc[c * 8 + 2] * inv, acc[c * 8 + 3] * inv);
-      av.z = pack_bf2(acc[c * 8 + 4] * inv, acc[c * 8 + 5] * inv);
-      av.w = pack_bf2(acc[c * 8 + 6] * inv, acc[c * 8 + 7] * inv);
+      av.x = pack_bf2(acc[0] * inv, acc[1] * inv);
+      av.y = pack_bf2(acc[2] * inv, acc[3] * inv);
+      av.z = pack_bf2(acc[4] * inv, acc[5] * inv);
+      av.w = pack_bf2(acc[6] * inv, acc[7] * inv);
+      const uint32_t row_off = (uint32_t)((m >> 3) * 128 + (m & 7) * 16);
+      *reinterpret_cast<uint4*>(sA + c * 2048 + row_off) = own;
       *reinterpret_cast<uint4*>(sA + (8 + c) * 2048 + row_off) = av;
-      if (TRAIN && n < N) reinterpret_cast<uint4*>(Aout + (size_t)n * F)[c] = av;
+      if (TRAIN && n < N) reinterpret_cast<uint4*>(a.Aout + (size_t)n * F)[c] = av;
     }
     // generic-proxy shared-memory writes -> visible to the tensor core (async proxy)
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
@@ -289,88 +357,112 @@ __global__ void __launch_bounds__(128, 3) k_mp_layer_tc(int N, const int* __rest
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
                        mbar_addr)
                    : "memory");
+      int ok = mbar_wait(mbar_addr, phase, a.spin_limit) ? 1 : 0;
+      if (!ok) {
+        // the wait gave up: report it, then let the MMA finish (bounded) before the tile's
+        // shared memory and tensor memory are released
+        if (a.err) atomicMin(&a.err[kErrTimeout], tile);
+        mbar_wait(mbar_addr, phase, kMbarSpinLimit);
+      }
+      mma_ok = ok;
+      asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     }
-    if (!mbar_wait(mbar_addr, phase) && err) atomicMin(&err[kErrTimeout], tile);
     phase ^= 1u;
+    __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-    uint32_t v[F];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      uint32_t part[16];
-      tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(q * 16), part);
-#pragma unroll
-      for (int j = 0; j < 16; ++j) v[q * 16 + j] = part[j];
-    }
+    if (!mma_ok) break;  // uniform: every thread reads the same flag
+
+    // ---- epilogue: bias, ReLU, residual; stage the output half row
+    const int m = q * 32 + lane;
+    const int n = tile * kTile + m;
+    uint32_t v[32];
+    tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(h * 32), v);
     asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-    if (n < N) {
-      uint4* ho = reinterpret_cast<uint4*>(Hout + (size_t)n * F);
-      uint4* go = TRAIN ? reinterpret_cast<uint4*>(Gout + (size_t)n * F) : nullptr;
+    uint32_t hw[16];
+    const uint32_t row_off = (uint32_t)((m >> 3) * 128 + (m & 7) * 16);
 #pragma unroll
-      for (int c = 0; c < 8; ++c) {
-        const uint32_t ow[4] = {own[c].x, own[c].y, own[c].z, own[c].w};
-        uint32_t hw[4], gw[4];
+    for (int cc = 0; cc < 4; ++cc) {
+      const int ch = 4 * h + cc;
+      const uint4 o4 = *reinterpret_cast<const uint4*>(sA + ch * 2048 + row_off);
+      const uint32_t ow[4] = {o4.x, o4.y, o4.z, o4.w};
+      uint32_t gw[4];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          const int o = c * 8 + 2 * j;
-          const float g0 = fmaxf(__uint_as_float(v[o]) + bias[o], 0.f);
-          const float g1 = fmaxf(__uint_as_float(v[o + 1]) + bias[o + 1], 0.f);
-          hw[j] = pack_bf2(bf_lo(ow[j]) + g0, bf_hi(ow[j]) + g1);
-          gw[j] = pack_bf2(g0, g1);
-        }
-        ho[c] = make_uint4(hw[0], hw[1], hw[2], hw[3]);
-        if (TRAIN) go[c] = make_uint4(gw[0], gw[1], gw[2], gw[3]);
+      for (int j = 0; j < 4; ++j) {
+        const int o = ch * 8 + 2 * j;
+        const float g0 = fmaxf(__uint_as_float(v[cc * 8 + 2 * j]) + bias[o], 0.f);
+        const float g1 = fmaxf(__uint_as_float(v[cc * 8 + 2 * j + 1]) + bias[o + 1], 0.f);
+        hw[cc * 4 + j] = pack_bf2(bf_lo(ow[j]) + g0, bf_hi(ow[j]) + g1);
+        gw[j] = pack_bf2(g0, g1);
+      }
+      if (TRAIN && n < N)
+        reinterpret_cast<uint4*>(a.Gout + (size_t)n * F)[ch] = make_uint4(gw[0], gw[1], gw[2], gw[3]);
+    }
+    if (a.Hout) {
+#pragma unroll
+      for (int cc = 0; cc < 4; ++cc) {
+        const int ch = 4 * h + cc;
+        *reinterpret_cast<uint4*>(sOut + m * 128 + ((ch ^ (m & 7)) * 16)) =
+            make_uint4(hw[cc * 4], hw[cc * 4 + 1], hw[cc * 4 + 2], hw[cc * 4 + 3]);
       }
     }
+    float y0 = 0.f, y1 = 0.f;
+    if (LAST) {
+      // decoder: y = b_out + sum over features 0..63 in order of W_out[:, f] H3[f]
+      if (h == 0) {
+        y0 = bout[0];
+        y1 = bout[1];
+      }
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const int f = 32 * h + 2 * j;
+        if (h == 0) {
+          y0 = fmaf(wout[f], bf_lo(hw[j]), y0);
+          y0 = fmaf(wout[f + 1], bf_hi(hw[j]), y0);
+          y1 = fmaf(wout[F + f], bf_lo(hw[j]), y1);
+          y1 = fmaf(wout[F + f + 1], bf_hi(hw[j]), y1);
+        }
+      }
+      if (h == 0) ypart[m] = make_float2(y0, y1);
+    }
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (LAST && h == 1 && n < N) {
+      const float2 yp = ypart[m];
+      y0 = yp.x;
+      y1 = yp.y;
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const int f = 32 + 2 * j;
+        y0 = fmaf(wout[f], bf_lo(hw[j]), y0);
+        y0 = fmaf(wout[f + 1], bf_hi(hw[j]), y0);
+        y1 = fmaf(wout[F + f], bf_lo(hw[j]), y1);
+        y1 = fmaf(wout[F + f + 1], bf_hi(hw[j]), y1);
+      }
+      if (TRAIN) reinterpret_cast<float2*>(a.Yout)[n] = make_float2(y0, y1);
+      const double2 rn = reinterpret_cast<const double2*>(a.r)[n];
+      const double2 dn = reinterpret_cast<const double2*>(a.invd)[n];
+      double2 zn = make_double2(dn.x * (rn.x + s * (double)y0), dn.y * (rn.y + s * (double)y1));
+      if (a.zbase) {
+        const double2 zb = reinterpret_cast<const double2*>(a.zbase)[n];
+        zn.x += zb.x;
+        zn.y += zb.y;
+      }
+      reinterpret_cast<double2*>(a.z)[n] = zn;
+    }
+    if (a.Hout) {  // the staged tile, in coalesced 16-byte stores
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int u = t + kLT * i, row = u >> 3, ch = u & 7;
+        const int nr = tile * kTile + row;
+        if (nr < N)
+          reinterpret_cast<uint4*>(a.Hout + (size_t)nr * F)[ch] =
+              *reinterpret_cast<const uint4*>(sOut + row * 128 + ((ch ^ (row & 7)) * 16));
+      }
+    }
     __syncthreads();  // tensor memory and the A tile are free for the next tile
   }
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(F));
-}
-
-// ---- decoder + preconditioner output: z = D^-1 (r + s (W_out H3 + b_out)) -------------------------
-
-template <bool TRAIN>
-__global__ void __launch_bounds__(256) k_mp_decode(int N, const __nv_bfloat16* __restrict__ H3, MpnnParams P,
-                                                   const double* __restrict__ r, const double* __restrict__ invd,
-                                                   const double* rr, double inv_n, const int* skip,
-                                                   double* __restrict__ z, float* __restrict__ Yout) {
-  const bool jacobi = skip && *skip;
-  __shared__ float w[2 * F];
-  __shared__ float b[2];
-  for (int i = threadIdx.x; i < 2 * F; i += blockDim.x) w[i] = bf(P.pb[kMpOffWout + i]);
-  if (threadIdx.x < 2) b[threadIdx.x] = P.pf[kMpOffBout + threadIdx.x];
-  __syncthreads();
-  const double s = sqrt(*rr * inv_n);
-  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < N; n += gridDim.x * blockDim.x) {
-    const double r0 = r[2 * n], r1 = r[2 * n + 1];
-    if (jacobi) {
-      z[2 * n] = invd[2 * n] * r0;
-      z[2 * n + 1] = invd[2 * n + 1] * r1;
-      continue;
-    }
-    float y0 = b[0], y1 = b[1];
-    const uint4* h = reinterpret_cast<const uint4*>(H3 + (size_t)n * F);
-#pragma unroll 2
-    for (int c = 0; c < 8; ++c) {
-      const uint4 v = h[c];
-      const uint32_t hw[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int k = c * 8 + 2 * j;
-        y0 = fmaf(w[k], bf_lo(hw[j]), y0);
-        y0 = fmaf(w[k + 1], bf_hi(hw[j]), y0);
-        y1 = fmaf(w[F + k], bf_lo(hw[j]), y1);
-        y1 = fmaf(w[F + k + 1], bf_hi(hw[j]), y1);
-      }
-    }
-    if (TRAIN) {
-      Yout[2 * n] = y0;
-      Yout[2 * n + 1] = y1;
-    }
-    z[2 * n] = invd[2 * n] * (r0 + s * (double)y0);
-    z[2 * n + 1] = invd[2 * n + 1] * (r1 + s * (double)y1);
-  }
 }
 
 // ---- training: loss and dL/dY ------------------------------------------------------------------
@@ -600,29 +692,42 @@ int grid_nodes(long long work, int per_block) {
   return (int)std::max<long long>(1, std::min<long long>(g, 148LL * 16));
 }
 
-int tc_grid(int N) {
-  const int tiles = (N + kTile - 1) / kTile;
-  return std::max(1, std::min(tiles, 148 * 3));
-}
+int g_tc_grid[4][64] = {};  // one wave of the layer kernel per device: [TRAIN * 2 + LAST][device]
 
-template <bool TRAIN>
+template <bool TRAIN, bool LAST>
 cudaError_t set_tc_attr() {
-  static bool done[64] = {};
   int dev = 0;
   cudaGetDevice(&dev);
-  if (dev >= 0 && dev < 64 && done[dev]) return cudaSuccess;
-  const cudaError_t e =
-      cudaFuncSetAttribute(k_mp_layer_tc<TRAIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
-  if (e == cudaSuccess && dev >= 0 && dev < 64) done[dev] = true;
-  return e;
+  int& slot = g_tc_grid[(TRAIN ? 2 : 0) + (LAST ? 1 : 0)][dev >= 0 && dev < 64 ? dev : 0];
+  if (slot > 0) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(k_mp_layer_tc<TRAIN, LAST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       kTcSmem);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0, sms = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mp_layer_tc<TRAIN, LAST>, kLT, kTcSmem);
+  if (e != cudaSuccess) return e;
+  e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return e;
+  slot = std::max(1, per_sm) * std::max(1, sms);
+  return cudaSuccess;
+}
+
+int tc_grid(int N, bool train, bool last) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const int wave = g_tc_grid[(train ? 2 : 0) + (last ? 1 : 0)][dev >= 0 && dev < 64 ? dev : 0];
+  const int tiles = (N + kTile - 1) / kTile;
+  return std::max(1, std::min(tiles, wave > 0 ? wave : kSMs * 2));
 }
 
 }  // namespace
 
 cudaError_t mpnn_prepare_device() {
-  cudaError_t e = set_tc_attr<false>();
-  if (e != cudaSuccess) return e;
-  return set_tc_attr<true>();
+  cudaError_t e = set_tc_attr<false, false>();
+  if (e == cudaSuccess) e = set_tc_attr<false, true>();
+  if (e == cudaSuccess) e = set_tc_attr<true, false>();
+  if (e == cudaSuccess) e = set_tc_attr<true, true>();
+  return e;
 }
 
 cudaError_t launch_mp_params(const float* p32, __nv_bfloat16* pb, float* pf, cudaStream_t s) {
@@ -631,15 +736,23 @@ cudaError_t launch_mp_params(const float* p32, __nv_bfloat16* pb, float* pf, cud
   return cudaGetLastError();
 }
 
-cudaError_t launch_mp_rr(int n, const double* r, MpScratch* sc, cudaStream_t s) {
-  k_mp_rr<<<kRedGrid, 256, 0, s>>>(n, r, sc);
+cudaError_t launch_mp_rr(int n, const double* r, MpScratch* sc, cudaStream_t s, const int* skip) {
+  k_mp_rr<<<kRedGrid, 256, 0, s>>>(n, r, sc, skip);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mp_smoother_weights(int n, const double* invd, const double* lam, double factor, double* out,
+                                       cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  k_mp_smoother_weights<<<grid_nodes(n, 256), 256, 0, s>>>(n, invd, lam, factor, out);
   count_launches(1);
   return cudaGetLastError();
 }
 
 cudaError_t launch_mp_forward(const MpnnGraph& g, const MpnnParams& P, const double* r, const double* invd,
                               const double* rr, const float* sf, const int* skip, MpnnWork& w, bool train,
-                              double* z, int* err, cudaStream_t s) {
+                              const double* zbase, double* z, long long spin_limit, int* err, cudaStream_t s) {
   const int N = g.n_nodes;
   if (N <= 0) return cudaSuccess;
   const double inv_n = 1.0 / (2.0 * N);
@@ -648,22 +761,39 @@ cudaError_t launch_mp_forward(const MpnnGraph& g, const MpnnParams& P, const dou
     k_mp_encode<true><<<ge, 256, 0, s>>>(N, r, rr, inv_n, sf, P, skip, w.H[0], w.X);
   else
     k_mp_encode<false><<<ge, 256, 0, s>>>(N, r, rr, inv_n, sf, P, skip, w.H[0], nullptr);
+  MpLayerArgs a{};
+  a.N = N;
+  a.node_ptr = g.node_ptr;
+  a.nbr = g.nbr;
+  a.P = P;
+  a.skip = skip;
+  a.r = r;
+  a.invd = invd;
+  a.rr = rr;
+  a.inv_n = inv_n;
+  a.zbase = zbase;
+  a.z = z;
+  a.Yout = train ? w.Y : nullptr;
+  a.spin_limit = spin_limit;
+  a.err = err;
   for (int l = 0; l < kMpL; ++l) {
-    __nv_bfloat16* hout = train ? w.H[l + 1] : w.H[(l + 1) & 1];
-    const __nv_bfloat16* hin = train ? w.H[l] : w.H[l & 1];
-    if (train)
-      k_mp_layer_tc<true><<<tc_grid(N), 128, kTcSmem, s>>>(N, g.node_ptr, g.nbr, hin, P, l, skip, hout,
-                                                           w.G[l], w.A[l], err);
+    const bool last = l + 1 == kMpL;
+    a.layer = l;
+    a.Hin = train ? w.H[l] : w.H[l & 1];
+    a.Hout = train ? w.H[l + 1] : (last ? nullptr : w.H[(l + 1) & 1]);
+    a.Gout = train ? w.G[l] : nullptr;
+    a.Aout = train ? w.A[l] : nullptr;
+    const int grid = tc_grid(N, train, last);
+    if (train && last)
+      k_mp_layer_tc<true, true><<<grid, kLT, kTcSmem, s>>>(a);
+    else if (train)
+      k_mp_layer_tc<true, false><<<grid, kLT, kTcSmem, s>>>(a);
+    else if (last)
+      k_mp_layer_tc<false, true><<<grid, kLT, kTcSmem, s>>>(a);
     else
-      k_mp_layer_tc<false><<<tc_grid(N), 128, kTcSmem, s>>>(N, g.node_ptr, g.nbr, hin, P, l, skip, hout,
-                                                            nullptr, nullptr, err);
+      k_mp_layer_tc<false, false><<<grid, kLT, kTcSmem, s>>>(a);
   }
-  const __nv_bfloat16* h3 = train ? w.H[kMpL] : w.H[kMpL & 1];
-  if (train)
-    k_mp_decode<true><<<ge, 256, 0, s>>>(N, h3, P, r, invd, rr, inv_n, skip, z, w.Y);
-  else
-    k_mp_decode<false><<<ge, 256, 0, s>>>(N, h3, P, r, invd, rr, inv_n, skip, z, nullptr);
-  count_launches(2 + kMpL);
+  count_launches(1 + kMpL);
   return cudaGetLastError();
 }
 

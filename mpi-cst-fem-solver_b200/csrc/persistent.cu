@@ -11,7 +11,8 @@
 // Grid barriers: the grid is one wave of co-resident blocks (cooperative launch). A block
 // writes its partial sums, fences, and arrives on an atomic counter; the last block to arrive
 // sums all partials in index order (deterministic), runs the scalar update and releases the
-// others by bumping a generation word. Every wait is bounded (kBarrierSpinLimit polls, ~2 s):
+// others by bumping a generation word. Every wait is bounded (spin_limit polls, by default
+// kBarrierSpinDefault ~ 2 s):
 // a block that gives up sets bar_err and done = TIMEOUT and returns, and so do all others,
 // so a fault can never leave the GPU spinning. Data written by other blocks inside this
 // kernel is read with ld.global.cg (L2), since L1 is not coherent within a kernel.
@@ -27,7 +28,6 @@ namespace cstg {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
-constexpr long long kBarrierSpinLimit = 50000000LL;  // polls of ~40 ns: ~2 s
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
   unsigned v;
@@ -47,6 +47,7 @@ constexpr int kPT = 1024;
 
 struct Shared {
   double red[kPT / 32];
+  long long limit;  // polls of a barrier wait before it gives up
   int last;
   int ok;
 };
@@ -73,7 +74,7 @@ __device__ __forceinline__ bool grid_reduce(const double (&v)[NV], double* parti
     if (!sh.last) {
       long long spins = 0;
       while (ld_acquire(&st->bar_gen) == gen) {
-        if (++spins > kBarrierSpinLimit || __ldcg(&st->bar_err)) {
+        if (++spins > sh.limit || __ldcg(&st->bar_err)) {
           atomicExch(&st->bar_err, 1);
           st->done = CSTG_SOLVE_TIMEOUT + 1;
           sh.ok = 0;
@@ -254,11 +255,14 @@ struct PersistArgs {
   double* history;
   PcgState* st;
   int max_final_checks;
+  long long spin_limit;
 };
 
 template <bool MIXED>
 __global__ void __launch_bounds__(kPT, 1) k_pcg_persistent(PersistArgs a) {
   __shared__ Shared sh;
+  if (threadIdx.x == 0) sh.limit = a.spin_limit;
+  __syncthreads();
   PcgState* st = a.st;
   const int npairs = a.A64.n_nodes;  // DOF pairs = nodes
   const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
@@ -405,7 +409,7 @@ static int persistent_grid() {
 
 // Launches the persistent solve on an initialised state (k_init / k_init_mixed done).
 cudaError_t launch_pcg_persistent(const PcgBuffers& w, const BlockMatrix& A64, const MixedMatrix* A32,
-                                  int max_final_checks, cudaStream_t s) {
+                                  int max_final_checks, long long spin_limit, cudaStream_t s) {
   PersistArgs a;
   a.A64 = A64;
   if (A32) a.A32 = *A32;
@@ -419,6 +423,7 @@ cudaError_t launch_pcg_persistent(const PcgBuffers& w, const BlockMatrix& A64, c
   a.history = w.history;
   a.st = w.st;
   a.max_final_checks = max_final_checks;
+  a.spin_limit = spin_limit;
   // barrier words start from zero
   cudaError_t e = cudaMemsetAsync(&w.st->bar_count, 0, sizeof(unsigned) * 2 + sizeof(int), s);
   if (e != cudaSuccess) return e;

@@ -9,8 +9,15 @@ iterates x_k sampled along the run and x* the converged solution. The loss of a 
 squared sine of the energy-norm angle between z = M(r_k) and e_k (0 when z points along the
 error). Forward, loss and backward run in the library's kernels; Adam runs on the GPU.
 
+The same network also serves as the finest-level post-smoother of the multigrid cycle
+(preconditioner "learned_mg"): the cycle's Chebyshev pre-smoothing and coarse correction give it
+global reach, and the network maps the remaining residual r2 to omega D^-1 (r2 + s Y(r2 / s)),
+omega = 4 / (3 lambda_max(D^-1 A)); with the output layer at zero it is one damped-Jacobi
+post-smoothing step. It is trained on the same pairs with the loss of the whole cycle's output
+(`--mode cycle`); its weights ship separately.
+
 Command line (writes the packaged weights):
-    python -m mpi-cst-fem-solver_b200.learned train --out weights.npz
+    python -m mpi-cst-fem-solver_b200.learned train --mode local|cycle --out weights.npz
 """
 from __future__ import annotations
 
@@ -31,6 +38,7 @@ from .solver import (CgJacobiSolver, Context, GpuCsrMatrix, PlaneCondition, Solv
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 WEIGHTS = os.path.join(HERE, "weights", "mpnn_plates.npz")
+WEIGHTS_CYCLE = os.path.join(HERE, "weights", "mpnn_cycle_smoother.npz")
 N_PARAMS = 25474
 F, N_IN, N_LAYERS = 64, 8, 3
 
@@ -64,8 +72,10 @@ def node_material(D, n_nodes: int) -> np.ndarray:
                                 dtype=np.float32)
 
 
-def load_weights(path: str | None = None) -> np.ndarray:
-    path = path or WEIGHTS
+def load_weights(path: str | None = None, mode: str = "local") -> np.ndarray:
+    """The packaged weights of the network alone (mode "local") or of the cycle's post-smoother
+    ("cycle")."""
+    path = path or (WEIGHTS if mode == "local" else WEIGHTS_CYCLE)
     if not os.path.exists(path):
         raise CstgError(native.ERR_STATE, f"learned preconditioner weights not found: {path}")
     p = np.load(path)["params"].astype(np.float32)
@@ -90,6 +100,17 @@ def apply(K: GpuCsrMatrix, r, z=None):
     return z
 
 
+def cycle_parts(K: GpuCsrMatrix, r) -> dict:
+    """The learned cycle's parts for the CUDA float64 residual r: x_fix (pre-smoothing + coarse
+    correction), r2 = r - A x_fix, winvd = omega D^-1 and the cycle's output z."""
+    import torch
+    out = {k: torch.empty_like(r) for k in ("xfix", "r2", "winvd", "z")}
+    with K.ctx.ordered(r.device):
+        K.ctx.check(K.ctx.L.cstg_learned_cycle_parts_device(K.ctx.h, _ptr(r), _ptr(out["xfix"]), _ptr(out["r2"]),
+                                                            _ptr(out["winvd"]), _ptr(out["z"])))
+    return out
+
+
 class Trainer:
     """The GPU trainer (cstg_trainer): FP32 master weights + Adam state on the device."""
 
@@ -112,6 +133,16 @@ class Trainer:
         R, E = R.contiguous(), E.contiguous()
         with K.ctx.ordered(R.device):  # (the trainer starts by waiting for the context's stream)
             self._check(self.L.cstg_trainer_accumulate(self.h, K.ctx.h, ns, _ptr(R), _ptr(E), _ptr(losses)))
+        return losses
+
+    def accumulate_cycle(self, K: GpuCsrMatrix, R, E) -> np.ndarray:
+        """As accumulate, with the network as the multigrid cycle's post-smoother and the loss of
+        the whole cycle's output."""
+        ns = int(R.shape[0])
+        losses = np.zeros(ns)
+        R, E = R.contiguous(), E.contiguous()
+        with K.ctx.ordered(R.device):
+            self._check(self.L.cstg_trainer_accumulate_cycle(self.h, K.ctx.h, ns, _ptr(R), _ptr(E), _ptr(losses)))
         return losses
 
     def step(self, lr: float, grad_scale: float) -> None:
@@ -194,9 +225,12 @@ def harvest(spec: PlateSpec, samples: int, params: np.ndarray, seed: int = 0, de
 
 
 def train(n_plates: int = 100, samples_per_plate: int = 100, epochs: int = 3, batch: int = 8, lr: float = 1e-3,
-          seed: int = 2026, n_r_range=(20, 200), device: int = 0, log=print):
+          seed: int = 2026, n_r_range=(20, 200), device: int = 0, log=print, mode: str = "local"):
     """Harvests n_plates x samples_per_plate pairs from the uneven plate distribution and trains
-    the network; returns (params, history of mean epoch losses, the Jacobi loss at the start)."""
+    the network (mode "local": the network alone; "cycle": as the multigrid cycle's
+    post-smoother); returns (params, history of mean epoch losses, number of pairs)."""
+    if mode not in ("local", "cycle"):
+        raise ValueError(f"train: unknown mode {mode!r}")
     import torch
     params0 = init_params(seed)
     specs = random_batch(count=n_plates, seed=seed + 1, n_r_range=n_r_range)
@@ -216,7 +250,7 @@ def train(n_plates: int = 100, samples_per_plate: int = 100, epochs: int = 3, ba
         for i, j in order:
             p = probs[i]
             Rb, Eb = p.R[j:j + batch], p.E[j:j + batch]
-            losses = tr.accumulate(p.K, Rb, Eb)
+            losses = tr.accumulate(p.K, Rb, Eb) if mode == "local" else tr.accumulate_cycle(p.K, Rb, Eb)
             if not np.all(np.isfinite(losses)):
                 tr.zero_grad()
                 continue
@@ -238,7 +272,8 @@ def train(n_plates: int = 100, samples_per_plate: int = 100, epochs: int = 3, ba
 def main():
     ap = argparse.ArgumentParser(description="train the learned preconditioner on the GPU")
     ap.add_argument("cmd", choices=["train"])
-    ap.add_argument("--out", default=WEIGHTS)
+    ap.add_argument("--mode", choices=["local", "cycle"], default="local")
+    ap.add_argument("--out", default=None)
     ap.add_argument("--plates", type=int, default=100)
     ap.add_argument("--samples", type=int, default=100)
     ap.add_argument("--epochs", type=int, default=3)
@@ -247,11 +282,15 @@ def main():
     ap.add_argument("--seed", type=int, default=2026)
     ap.add_argument("--n-r-max", type=int, default=200)
     a = ap.parse_args()
-    params, hist, n_pairs = train(a.plates, a.samples, a.epochs, a.batch, a.lr, a.seed, (20, a.n_r_max))
-    os.makedirs(os.path.dirname(os.path.abspath(a.out)), exist_ok=True)
-    np.savez(a.out, params=params, loss_history=np.array(hist), pairs=n_pairs, plates=a.plates,
-             samples=a.samples, epochs=a.epochs, batch=a.batch, lr=a.lr, seed=a.seed)
-    print(f"wrote {a.out}")
+    out = a.out or (WEIGHTS if a.mode == "local" else WEIGHTS_CYCLE)
+    t0 = time.perf_counter()
+    params, hist, n_pairs = train(a.plates, a.samples, a.epochs, a.batch, a.lr, a.seed, (20, a.n_r_max),
+                                  mode=a.mode)
+    os.makedirs(os.path.dirname(os.path.abspath(out)), exist_ok=True)
+    np.savez(out, params=params, loss_history=np.array(hist), pairs=n_pairs, plates=a.plates,
+             samples=a.samples, epochs=a.epochs, batch=a.batch, lr=a.lr, seed=a.seed, mode=a.mode,
+             seconds=time.perf_counter() - t0)
+    print(f"wrote {out}")
 
 
 if __name__ == "__main__":

@@ -58,6 +58,7 @@ TRACTION_KIRSCH = 1
 PRECOND_JACOBI = 0
 PRECOND_LEARNED = 1
 PRECOND_AMG = 2
+PRECOND_LEARNED_MG = 3
 AMG_CHEBYSHEV, AMG_JACOBI = 0, 1  # cstg_amg_set_smoother
 
 LAUNCH_AUTO = 0
@@ -152,6 +153,9 @@ _SIGS = {
     "cstg_trainer_destroy": (None, [_vp]),
     "cstg_trainer_last_error": (C.c_char_p, [_vp]),
     "cstg_trainer_accumulate": (C.c_int, [_vp, _vp, C.c_int, _vp, _vp, _vp]),
+    "cstg_trainer_accumulate_cycle": (C.c_int, [_vp, _vp, C.c_int, _vp, _vp, _vp]),
+    "cstg_learned_cycle_parts_device": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    "cstg_set_wait_limits": (C.c_int, [_vp, C.c_longlong, C.c_longlong]),
     "cstg_trainer_step": (C.c_int, [_vp, C.c_float, C.c_float]),
     "cstg_trainer_params": (C.c_int, [_vp, _vp, _vp]),
     "cstg_trainer_zero_grad": (C.c_int, [_vp]),

@@ -100,6 +100,10 @@ class Context:
         self.check(self.L.cstg_set_stream(self.h, ptr or None))
         self._ext = None
 
+    def set_wait_limits(self, barrier_polls: int = -1, mma_polls: int = -1) -> None:
+        """Polls before a device wait gives up (cstg_set_wait_limits; -1: the default, 0: at once)."""
+        self.check(self.L.cstg_set_wait_limits(self.h, int(barrier_polls), int(mma_polls)))
+
     def stream_handle(self) -> int:
         """The cudaStream_t the context's work is ordered on (cstg_get_stream)."""
         s = C.c_void_p(0)
@@ -336,7 +340,9 @@ class SolverOptions:
     max_refinements: int = 16
     check_interval: int = 0
     launch: str = "auto"  # "auto" | "persistent" | "graph"
-    preconditioner: str = "jacobi"  # "jacobi" | "learned" (flexible CG; needs learned setup) | "amg"
+    # "jacobi" | "learned" (the network alone in flexible CG; needs learned setup) | "amg" |
+    # "learned_mg" (the network as the multigrid cycle's post-smoother; needs learned setup)
+    preconditioner: str = "jacobi"
 
     def native(self) -> native.SolverOptions:
         o = native.default_options()
@@ -350,7 +356,8 @@ class SolverOptions:
         o.launch_mode = {"auto": native.LAUNCH_AUTO, "persistent": native.LAUNCH_PERSISTENT,
                          "graph": native.LAUNCH_GRAPH}[self.launch]
         o.preconditioner = {"jacobi": native.PRECOND_JACOBI, "learned": native.PRECOND_LEARNED,
-                            "amg": native.PRECOND_AMG}[self.preconditioner]
+                            "amg": native.PRECOND_AMG,
+                            "learned_mg": native.PRECOND_LEARNED_MG}[self.preconditioner]
         return o
 
 

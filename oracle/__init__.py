@@ -86,6 +86,9 @@ class Oracle:
         L.mp_apply.argtypes = [C.c_int, _dp, _dp, C.c_double, _dp, _dp]
         L.mp_loss.argtypes = [C.c_int, _ip, _ip, _dp, _dp, _dp, _dp, C.c_double, _dp, C.c_void_p]
         L.mp_loss.restype = C.c_double
+        L.mp_loss_cycle.argtypes = [C.c_int, _ip, _ip, _dp, _dp, _dp, _dp, _dp, _dp, C.c_double, _dp,
+                                    C.c_void_p]
+        L.mp_loss_cycle.restype = C.c_double
         L.mp_backward.argtypes = [C.c_int, _ip, _ip, _dp, _dp, C.c_int, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]
         self.L = L
 
@@ -207,6 +210,13 @@ class Oracle:
         dY = np.zeros(_f64(r).size) if grad else None
         L = self.L.mp_loss(_f64(r).size // 2, _i32(rp), _i32(cols), _f64(vals), _f64(r), _f64(e), _f64(invd),
                            float(s), _f64(Y), dY.ctypes.data if grad else None)
+        return L, dY
+
+    def mp_loss_cycle(self, rp, cols, vals, r, e, xfix, r2, winvd, s, Y, grad=True):
+        """Loss of the learned multigrid cycle's output z = xfix + winvd (r2 + s Y) and dL/dY."""
+        dY = np.zeros(_f64(r).size) if grad else None
+        L = self.L.mp_loss_cycle(_f64(r).size // 2, _i32(rp), _i32(cols), _f64(vals), _f64(r), _f64(e), _f64(xfix),
+                                 _f64(r2), _f64(winvd), float(s), _f64(Y), dY.ctypes.data if grad else None)
         return L, dY
 
     def mp_backward(self, node_ptr, nbr, X, P, cache, dY, q=True):

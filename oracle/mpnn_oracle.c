@@ -143,6 +143,41 @@ void mp_apply(int N, const double* r, const double* invd, double s, const double
   for (long i = 0; i < 2L * N; ++i) z[i] = invd[i] * (r[i] + s * Y[i]);
 }
 
+/* Loss of the learned multigrid cycle's output for one sample (r, e) and dL/dY: the network reads
+ * r2 (the residual left after the cycle's fixed part x_fix, features and s from r2) and its
+ * output is the post-smoothing step, z = x_fix + winvd (r2 + s Y), winvd = omega D^-1. The loss is
+ * the same energy-norm angle as mp_loss, of z against e, on the sample's r. Returns L. */
+double mp_loss_cycle(int N, const int* rp, const int* cols, const double* vals, const double* r, const double* e,
+                     const double* xfix, const double* r2, const double* winvd, double s, const double* Y,
+                     double* dY) {
+  const long n = 2L * N;
+  double c = 0.0, zaz = 0.0, er = 0.0;
+  for (long i = 0; i < n; ++i) {
+    const double zi = xfix[i] + winvd[i] * (r2[i] + s * Y[i]);
+    c += zi * r[i];
+    er += e[i] * r[i];
+    double az = 0.0;
+    for (int k = rp[i]; k < rp[i + 1]; ++k) {
+      const int j = cols[k];
+      az += vals[k] * (xfix[j] + winvd[j] * (r2[j] + s * Y[j]));
+    }
+    zaz += zi * az;
+  }
+  const double L = 1.0 - c * c / (zaz * er);
+  if (dY) {
+    const double f1 = -2.0 * c / (zaz * er), f2 = 2.0 * c * c / (zaz * zaz * er);
+    for (long i = 0; i < n; ++i) {
+      double az = 0.0;
+      for (int k = rp[i]; k < rp[i + 1]; ++k) {
+        const int j = cols[k];
+        az += vals[k] * (xfix[j] + winvd[j] * (r2[j] + s * Y[j]));
+      }
+      dY[i] = s * winvd[i] * (f1 * r[i] + f2 * az);
+    }
+  }
+  return L;
+}
+
 /* Loss of one sample and dL/dY. K: the plate's CSR (n = 2N rows). Returns L. */
 double mp_loss(int N, const int* rp, const int* cols, const double* vals, const double* r, const double* e,
                const double* invd, double s, const double* Y, double* dY) {

@@ -1,0 +1,188 @@
+"""The learned multigrid cycle (preconditioner "learned_mg") on the GPU: the network as the
+finest-level post-smoother of the multigrid cycle, inside flexible CG.
+
+Bars: the network's part of the cycle output within relative 2e-2 of the FP64 oracle (BF16
+activations on both sides), training gradients within relative 5e-2 of the oracle's, solves
+converged on the FP64 true residual <= 1e-10 with displacements within relative 1e-8 of the
+reference's serial CG solution (golden fixture) or of the oracle's FP64 Jacobi-PCG."""
+import numpy as np
+import pytest
+
+from test_gpu_learned import _bf16_params, _plate, _rel
+from test_oracle_mpnn import node_graph
+
+pytestmark = pytest.mark.gpu
+
+REL_TOL = 1e-8
+
+
+def _dense(rp, cols, vals):
+    n = rp.size - 1
+    Kd = np.zeros((n, n))
+    for i in range(n):
+        Kd[i, cols[rp[i]:rp[i + 1]]] = vals[rp[i]:rp[i + 1]]
+    return Kd
+
+
+def test_cycle_output_matches_oracle(pkg, oracle, gpu_lib):
+    import torch
+    m, D, K, b = _plate(pkg, 12, 24)
+    p, q = _bf16_params(oracle, pkg, seed=11)
+    mat = pkg.learned.node_material(D, m.num_nodes)
+    pkg.learned.setup(K, p, mat)
+    rp, cols, vals = K.download()
+    rng = np.random.default_rng(2)
+    r = rng.standard_normal(m.num_dofs)
+    parts = {k: v.cpu().numpy() for k, v in pkg.learned.cycle_parts(K, torch.from_numpy(r).cuda()).items()}
+    invd = 1.0 / np.diag(_dense(rp, cols, vals))
+    # winvd = omega D^-1 with one omega for every DOF
+    ratio = parts["winvd"] / invd
+    assert np.allclose(ratio, ratio[0], rtol=1e-14) and 0.0 < ratio[0] < 2.0
+    # r2 = r - A x_fix (the cycle's FP32 operator against the oracle's FP64 product)
+    r2_ref = r - oracle.multiply(rp, cols, vals, parts["xfix"])
+    assert _rel(parts["r2"], r2_ref) < 1e-5
+    # the post-smoothing step against the oracle's network on r2
+    node_ptr, nbr = node_graph(rp, cols)
+    X, s = oracle.mp_features(parts["r2"], invd, m.xy, mat.astype(np.float64))
+    Y, _ = oracle.mp_forward(node_ptr, nbr, X, q, q=True)
+    net = parts["z"] - parts["xfix"] - parts["winvd"] * parts["r2"]
+    net_ref = parts["winvd"] * s * Y
+    assert np.abs(Y).max() > 1e-3
+    assert _rel(net, net_ref) < 2e-2
+    K.ctx.close()
+
+
+def test_cycle_gradients_match_oracle(pkg, oracle, gpu_lib):
+    import torch
+    m, D, K, b = _plate(pkg, 8, 16)
+    p, q = _bf16_params(oracle, pkg, seed=13)
+    mat = pkg.learned.node_material(D, m.num_nodes)
+    pkg.learned.setup(K, p, mat)
+    rp, cols, vals = K.download()
+    Kd = _dense(rp, cols, vals)
+    rng = np.random.default_rng(3)
+    r = rng.standard_normal(m.num_dofs)
+    e = np.linalg.solve(Kd, r)
+    invd = 1.0 / np.diag(Kd)
+    tr = pkg.learned.Trainer(p)
+    R = torch.from_numpy(r[None, :]).cuda()
+    loss = tr.accumulate_cycle(K, R, torch.from_numpy(e[None, :]).cuda())
+    _, g = tr.params(grads=True)
+    # the cycle's fixed part with the same weights (x_fix and r2 do not depend on them)
+    parts = {k: v.cpu().numpy() for k, v in pkg.learned.cycle_parts(K, R[0].contiguous()).items()}
+    node_ptr, nbr = node_graph(rp, cols)
+    X, s = oracle.mp_features(parts["r2"], invd, m.xy, mat.astype(np.float64))
+    Y, cache = oracle.mp_forward(node_ptr, nbr, X, q, q=True)
+    L, dY = oracle.mp_loss_cycle(rp, cols, vals, r, e, parts["xfix"], parts["r2"], parts["winvd"], s, Y)
+    g_ref = oracle.mp_backward(node_ptr, nbr, X, q, cache, dY, q=True)
+    assert abs(loss[0] - L) < 1e-3 * max(1.0, abs(L))
+    assert _rel(g, g_ref) < 5e-2
+    bounds = [0, 576, 576 + 8256, 576 + 2 * 8256, 576 + 3 * 8256, 25474]
+    for a, c in zip(bounds[:-1], bounds[1:]):
+        assert _rel(g[a:c], g_ref[a:c]) < 5e-2, (a, c)
+    tr.close()
+    K.ctx.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_cycle_solve_matches_reference(pkg, gpu_lib, golden, precision):
+    """The packaged smoother weights and the untrained network (one damped-Jacobi post-smoothing
+    step): both converge on the FP64 true residual to the reference's displacements."""
+    g = golden("plate_40x80")
+    m, D, K, b = _plate(pkg, 40, 80)
+    mat = pkg.learned.node_material(D, m.num_nodes)
+    for params in (pkg.learned.load_weights(mode="cycle"), np.zeros(pkg.learned.N_PARAMS, np.float32)):
+        s = pkg.CgJacobiSolver(pkg.SolverOptions(rtol=1e-10, max_iter=5000, precision=precision,
+                                                 preconditioner="learned_mg", true_residual_stop=True))
+        s.setup(K)
+        pkg.learned.setup(K, params, mat)
+        x = np.zeros(m.num_dofs)
+        st = s.solve(b, x)
+        assert st.converged and st.true_rel_residual <= 1e-10, st.message
+        assert "learned multigrid cycle" in st.message
+        assert _rel(x, g["u"]) < REL_TOL
+        assert st.iterations < 200, st.message
+    K.ctx.close()
+
+
+def test_cycle_fallback_on_a_bad_network(pkg, gpu_lib, golden):
+    """Large random weights: flexible CG still converges to the reference's solution (a
+    non-descent direction is replaced by the Jacobi step, stagnation switches to Jacobi-PCG)."""
+    g = golden("plate_40x80")
+    m, D, K, b = _plate(pkg, 40, 80)
+    s = pkg.CgJacobiSolver(pkg.SolverOptions(rtol=1e-10, max_iter=200000, preconditioner="learned_mg",
+                                             true_residual_stop=True))
+    s.setup(K)
+    p = (np.random.default_rng(3).standard_normal(pkg.learned.N_PARAMS) * 3.0).astype(np.float32)
+    pkg.learned.setup(K, p, pkg.learned.node_material(D, m.num_nodes))
+    x = np.zeros(m.num_dofs)
+    st = s.solve(b, x)
+    assert st.converged and st.true_rel_residual <= 1e-10, st.message
+    assert _rel(x, g["u"]) < REL_TOL
+    K.ctx.close()
+
+
+def test_cycle_training_lowers_the_loss(pkg, gpu_lib):
+    """A few Adam steps on one plate's pairs lower the cycle's mean loss from its value with the
+    network at zero (the damped-Jacobi post-smoother)."""
+    spec = pkg.plate.PlateSpec(n_r=24, n_theta=48, a=1.0, E=1.0, nu=0.3, plane_strain=False)
+    p0 = pkg.learned.init_params(0)
+    prob = pkg.learned.harvest(spec, 24, p0, seed=0)
+    tr = pkg.learned.Trainer(p0)
+    first = tr.accumulate_cycle(prob.K, prob.R, prob.E).mean()
+    tr.zero_grad()
+    for _ in range(60):
+        losses = tr.accumulate_cycle(prob.K, prob.R, prob.E)
+        tr.step(2e-3, 1.0 / len(losses))
+    last = tr.accumulate_cycle(prob.K, prob.R, prob.E).mean()
+    assert np.isfinite(first) and last < first, (first, last)
+    tr.close()
+    prob.K.ctx.close()
+
+
+def _held_out_system(pkg, spec):
+    m = pkg.plate.quarter_plate(spec.n_r, spec.n_theta, a=spec.a)
+    D = pkg.constitutive_matrix(spec.E, spec.nu, pkg.PlaneCondition.Strain if spec.plane_strain
+                                else pkg.PlaneCondition.Stress)
+    K = pkg.build_stiffness_pattern(m)
+    pkg.assemble_stiffness(m, D, 1.0, K)
+    b = np.zeros(m.num_dofs)
+    pkg.add_traction(K, m.boundary_edges["right"], 1.0, 1.0, 0.0, b)
+    pkg.apply_dirichlet(pkg.plate.symmetry_dirichlet(m), K, b)
+    return m, D, K, b
+
+
+def test_trained_smoother_gain_on_held_out_plates(pkg, oracle, gpu_lib):
+    """What the trained network gains, on plates it was not trained on (seeded draws from the
+    same distribution, not in the training seed's batch):
+      * over the method without it, the same cycle with the network at zero (one damped-Jacobi
+        post-smoothing step): fewer flexible-CG iterations on every plate;
+      * over plain Jacobi-PCG: fewer iterations and less device time on every plate.
+    Every solve converges on the FP64 true residual <= 1e-10 to the oracle's FP64 solution."""
+    w = pkg.learned.load_weights(mode="cycle")
+    zero = np.zeros_like(w)
+    specs = pkg.plate.random_batch(count=4, seed=4242, n_r_range=(60, 160))
+    for spec in specs:
+        m, D, K, b = _held_out_system(pkg, spec)
+        rp, cols, vals = K.download()
+        x_ref, _ = oracle.pcg_jacobi(rp, cols, vals, b, rtol=1e-12, max_iter=200000)
+        mat = pkg.learned.node_material(D, m.num_nodes)
+        res = {}
+        for name, pre, params in (("jacobi", "jacobi", None), ("zero", "learned_mg", zero),
+                                  ("trained", "learned_mg", w)):
+            s = pkg.CgJacobiSolver(pkg.SolverOptions(rtol=1e-10, max_iter=200000, precision="mixed",
+                                                     preconditioner=pre, true_residual_stop=True))
+            s.setup(K)
+            if params is not None:
+                pkg.learned.setup(K, params, mat)
+            x = np.zeros(m.num_dofs)
+            s.solve(b, x)  # warm-up: hierarchy, graphs
+            st = s.solve(b, x)
+            assert st.converged and st.true_rel_residual <= 1e-10, (name, st.message)
+            assert _rel(x, x_ref) < REL_TOL, name
+            res[name] = st
+        assert res["trained"].iterations < res["zero"].iterations, (spec, res["trained"].iterations,
+                                                                   res["zero"].iterations)
+        assert res["trained"].iterations < res["jacobi"].iterations / 5, spec
+        assert res["trained"].solve_seconds < res["jacobi"].solve_seconds, spec
+        K.ctx.close()

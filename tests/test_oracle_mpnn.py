@@ -89,3 +89,40 @@ def test_mpnn_oracle_homogeneous_in_r(pkg, oracle):
         Y, _ = oracle.mp_forward(node_ptr, nbr, X, P, q=False)
         zs.append(oracle.mp_apply(c * r, invd, s, Y))
     assert np.allclose(zs[1], 8.0 * zs[0], rtol=1e-12, atol=0)
+
+
+def test_mpnn_oracle_cycle_gradient_matches_finite_differences(pkg, oracle):
+    """The learned multigrid cycle's loss: the network reads the residual r2 left after the
+    cycle's fixed part x_fix and adds omega D^-1 (r2 + s Y); the gradient of the loss of the
+    cycle's output (against the sample's r and e) must match central differences."""
+    m, rp, cols, vals, r, e, invd, mat = small_problem(pkg, oracle, seed=4)
+    node_ptr, nbr = node_graph(rp, cols)
+    rng = np.random.default_rng(8)
+    xfix = 0.5 * e + 0.1 * rng.standard_normal(e.size) * np.abs(e).max()
+    r2 = r - oracle.multiply(rp, cols, vals, xfix)
+    winvd = 0.6 * invd
+    X, s = oracle.mp_features(r2, invd, m.xy, mat)
+    P = random_params(oracle, seed=2)
+
+    def loss(P):
+        Y, _ = oracle.mp_forward(node_ptr, nbr, X, P, q=False)
+        return oracle.mp_loss_cycle(rp, cols, vals, r, e, xfix, r2, winvd, s, Y, grad=False)[0]
+
+    Y, cache = oracle.mp_forward(node_ptr, nbr, X, P, q=False)
+    L0, dY = oracle.mp_loss_cycle(rp, cols, vals, r, e, xfix, r2, winvd, s, Y)
+    assert 0.0 <= L0 <= 1.0
+    g = oracle.mp_backward(node_ptr, nbr, X, P, cache, dY, q=False)
+    idx = np.concatenate([rng.choice(P.size, 60, replace=False), [P.size - 1, P.size - 2, 0, 520]])
+    h = 1e-6
+    fd = []
+    for k in idx:
+        Pp, Pm = P.copy(), P.copy()
+        Pp[k] += h
+        Pm[k] -= h
+        fd.append((loss(Pp) - loss(Pm)) / (2 * h))
+    fd = np.array(fd)
+    assert np.linalg.norm(g[idx] - fd) <= 1e-5 * np.linalg.norm(fd) + 1e-12
+    # with the network at zero the cycle's post-smoothing is one damped-Jacobi step
+    Y0, _ = oracle.mp_forward(node_ptr, nbr, X, np.zeros(P.size), q=False)
+    z0 = xfix + winvd * (r2 + s * Y0)
+    assert np.array_equal(z0, xfix + winvd * r2)
