@@ -196,6 +196,7 @@ __global__ void __launch_bounds__(256) k_mp_encode(int N, const double* __restri
 //            warps of columns 0..31, handed through shared memory to those of columns 32..63), and
 //            z = zbase + invd (r + s y).
 constexpr int kLT = 256;                            // threads of the layer kernel
+constexpr int kNbrCache = 128;                      // neighbour-list entries a warp keeps in shared memory
 constexpr int kTcSmem = kASmem + kBSmem + 1024;     // dynamic shared memory (1024-byte aligned base)
 
 struct MpLayerArgs {
@@ -259,6 +260,7 @@ __global__ void __launch_bounds__(kLT, 3) k_mp_layer_tc(const MpLayerArgs a) {
   __shared__ int mma_ok;
   __shared__ float wout[2 * F], bout[2];
   __shared__ float2 ypart[kTile];
+  __shared__ int s_nbr[(kLT / 32) * kNbrCache];  // each warp's neighbour lists (the first kNbrCache entries)
   uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
   uint8_t* sA = base;            // element (m, k): (k/8)*2048 + (m/8)*128 + (m%8)*16 + (k%8)*2
   uint8_t* sB = base + kASmem;   // element (n, k): (k/8)*1024 + (n/8)*128 + (n%8)*16 + (k%8)*2
@@ -296,11 +298,25 @@ __global__ void __launch_bounds__(kLT, 3) k_mp_layer_tc(const MpLayerArgs a) {
   const int q = warp & 3, h = warp >> 2;    // epilogue: TMEM lane quarter, column half
 
   for (int tile = blockIdx.x; tile * kTile < N; tile += gridDim.x) {
-    // ---- gather: own chunk and the neighbours' mean chunk of 16 nodes per warp
+    // ---- gather: own chunk and the neighbours' mean chunk of 16 nodes per warp. The warp's 17
+    // node pointers come in one load, its nodes' neighbour lists (contiguous in the pattern) in
+    // one more into shared memory, so each round of four nodes is one round trip: the own
+    // chunk and up to eight neighbour chunks per lane in flight.
+    const int wbase = tile * kTile + warp * 16;
+    int np = 0;
+    if (lane <= 16) np = __ldg(&a.node_ptr[min(wbase + lane, N)]);
+    const int np0 = __shfl_sync(0xffffffffu, np, 0);
+    const int cnt = __shfl_sync(0xffffffffu, np, 16) - np0;
+    int* wnbr = s_nbr + warp * kNbrCache;
+    for (int j = lane; j < min(cnt, kNbrCache); j += 32) wnbr[j] = __ldg(&a.nbr[np0 + j]);
+    __syncwarp();
 #pragma unroll 1
     for (int rnd = 0; rnd < 4; ++rnd) {
-      const int m = warp * 16 + rnd * 4 + g;
-      const int n = tile * kTile + m;
+      const int li = rnd * 4 + g;
+      const int m = warp * 16 + li;
+      const int n = wbase + li;
+      const int k0 = __shfl_sync(0xffffffffu, np, li) - np0;
+      const int k1 = __shfl_sync(0xffffffffu, np, li + 1) - np0;
       uint4 own = make_uint4(0u, 0u, 0u, 0u);
       float acc[8];
 #pragma unroll
@@ -308,18 +324,20 @@ __global__ void __launch_bounds__(kLT, 3) k_mp_layer_tc(const MpLayerArgs a) {
       int deg = 0;
       if (n < N) {
         own = __ldg(reinterpret_cast<const uint4*>(a.Hin + (size_t)n * F) + c);
-        const int k0 = __ldg(&a.node_ptr[n]), k1 = __ldg(&a.node_ptr[n + 1]);
-        for (int k = k0; k < k1; k += 4) {
-          int mm[4];
-          uint4 v[4];
+        for (int k = k0; k < k1; k += 8) {
+          int mm[8];
+          uint4 v[8];
 #pragma unroll
-          for (int j = 0; j < 4; ++j) mm[j] = k + j < k1 ? __ldg(&a.nbr[k + j]) : n;
+          for (int j = 0; j < 8; ++j) {
+            const int q8 = k + j;
+            mm[j] = q8 < k1 ? (q8 < kNbrCache ? wnbr[q8] : __ldg(&a.nbr[np0 + q8])) : n;
+          }
 #pragma unroll
-          for (int j = 0; j < 4; ++j)
+          for (int j = 0; j < 8; ++j)
             v[j] = mm[j] != n ? __ldg(reinterpret_cast<const uint4*>(a.Hin + (size_t)mm[j] * F) + c)
                               : make_uint4(0u, 0u, 0u, 0u);
 #pragma unroll
-          for (int j = 0; j < 4; ++j)
+          for (int j = 0; j < 8; ++j)
             if (mm[j] != n) {
               ++deg;
               add_chunk(acc, v[j]);

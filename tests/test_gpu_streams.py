@@ -35,7 +35,9 @@ def test_spmv_orders_with_torch_stream(pkg, oracle, gpu_lib):
     rp, cols, vals = K.download()
     rng = np.random.default_rng(5)
     x_h = rng.standard_normal(m.num_dofs)
-    y_ref = oracle.multiply(rp, cols, vals, x_h)
+    # the same kernel through the host path (synchronous): the device path must give its bits
+    y_ref = K.multiply(x_h)
+    assert np.linalg.norm(y_ref - oracle.multiply(rp, cols, vals, x_h)) <= 1e-13 * np.linalg.norm(y_ref)
     for _ in range(3):
         _busy(torch, dev)
         x = torch.zeros(m.num_dofs, dtype=torch.float64, device=dev)
