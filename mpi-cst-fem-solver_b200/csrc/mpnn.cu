@@ -134,27 +134,41 @@ __global__ void k_mp_smoother_weights(int n, const double* __restrict__ invd, co
 
 // ---- encoder: H0 = relu(W_in X + b_in) ------------------------------------------------------------
 
+// Eight threads per node, thread c computing features 8c..8c+7 with its 64 weights and 8 biases in
+// registers (loaded once per thread); a warp writes four whole 128-byte rows per step. Each
+// feature is the same chain of FMAs in the same order for every launch shape.
 template <bool TRAIN>
 __global__ void __launch_bounds__(256) k_mp_encode(int N, const double* __restrict__ r, const double* rr,
                                                    double inv_n, const float* __restrict__ sf, MpnnParams P,
                                                    const int* skip, __nv_bfloat16* __restrict__ H0,
                                                    __nv_bfloat16* __restrict__ Xout) {
   if (skip && *skip) return;
-  __shared__ float w[F * kMpIn], b[F];
-  for (int i = threadIdx.x; i < F * kMpIn; i += blockDim.x) w[i] = bf(P.pb[kMpOffWin + i]);
-  for (int i = threadIdx.x; i < F; i += blockDim.x) b[i] = P.pf[kMpOffBin + i];
-  __syncthreads();
+  const int c = threadIdx.x & 7;
+  float w[8][kMpIn], b[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    b[j] = P.pf[kMpOffBin + c * 8 + j];
+#pragma unroll
+    for (int k = 0; k < kMpIn; ++k) w[j][k] = bf(P.pb[kMpOffWin + (c * 8 + j) * kMpIn + k]);
+  }
   const double s = sqrt(*rr * inv_n);
   const double sd = s > 0.0 ? s : 1.0;
-  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < N; n += gridDim.x * blockDim.x) {
+  const int per_step = (gridDim.x * blockDim.x) >> 3;
+  for (int n = (blockIdx.x * blockDim.x + threadIdx.x) >> 3; n < N; n += per_step) {
+    const double2 rn = reinterpret_cast<const double2*>(r)[n];
     float x[kMpIn];
-    x[0] = (float)(r[2 * n] / sd);
-    x[1] = (float)(r[2 * n + 1] / sd);
+    x[0] = (float)(rn.x / sd);
+    x[1] = (float)(rn.y / sd);
+    const float2* sfn = reinterpret_cast<const float2*>(sf + (size_t)n * 6);
 #pragma unroll
-    for (int k = 0; k < 6; ++k) x[2 + k] = sf[(size_t)n * 6 + k];
+    for (int k = 0; k < 3; ++k) {
+      const float2 v = sfn[k];
+      x[2 + 2 * k] = v.x;
+      x[3 + 2 * k] = v.y;
+    }
 #pragma unroll
     for (int k = 0; k < kMpIn; ++k) x[k] = __bfloat162float(__float2bfloat16_rn(x[k]));
-    if (TRAIN) {
+    if (TRAIN && c == 0) {
       uint4 xv;
       xv.x = pack_bf2(x[0], x[1]);
       xv.y = pack_bf2(x[2], x[3]);
@@ -162,20 +176,16 @@ __global__ void __launch_bounds__(256) k_mp_encode(int N, const double* __restri
       xv.w = pack_bf2(x[6], x[7]);
       reinterpret_cast<uint4*>(Xout)[n] = xv;
     }
-    uint4* out = reinterpret_cast<uint4*>(H0 + (size_t)n * F);
-#pragma unroll 1
-    for (int c = 0; c < F / 8; ++c) {
-      float h[8];
+    float h[8];
 #pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const int o = c * 8 + j;
-        float u = b[o];
+    for (int j = 0; j < 8; ++j) {
+      float u = b[j];
 #pragma unroll
-        for (int k = 0; k < kMpIn; ++k) u = fmaf(w[o * kMpIn + k], x[k], u);
-        h[j] = fmaxf(u, 0.f);
-      }
-      out[c] = make_uint4(pack_bf2(h[0], h[1]), pack_bf2(h[2], h[3]), pack_bf2(h[4], h[5]), pack_bf2(h[6], h[7]));
+      for (int k = 0; k < kMpIn; ++k) u = fmaf(w[j][k], x[k], u);
+      h[j] = fmaxf(u, 0.f);
     }
+    reinterpret_cast<uint4*>(H0 + (size_t)n * F)[c] =
+        make_uint4(pack_bf2(h[0], h[1]), pack_bf2(h[2], h[3]), pack_bf2(h[4], h[5]), pack_bf2(h[6], h[7]));
   }
 }
 
@@ -721,6 +731,9 @@ cudaError_t set_tc_attr() {
   cudaError_t e = cudaFuncSetAttribute(k_mp_layer_tc<TRAIN, LAST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        kTcSmem);
   if (e != cudaSuccess) return e;
+  // the whole unified L1 / shared array as shared memory: three CTAs of ~56 KB per SM
+  e = cudaFuncSetAttribute(k_mp_layer_tc<TRAIN, LAST>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  if (e != cudaSuccess) return e;
   int per_sm = 0, sms = 0;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mp_layer_tc<TRAIN, LAST>, kLT, kTcSmem);
   if (e != cudaSuccess) return e;
@@ -774,7 +787,7 @@ cudaError_t launch_mp_forward(const MpnnGraph& g, const MpnnParams& P, const dou
   const int N = g.n_nodes;
   if (N <= 0) return cudaSuccess;
   const double inv_n = 1.0 / (2.0 * N);
-  const int ge = grid_nodes(N, 256);
+  const int ge = grid_nodes(8LL * N, 256);
   if (train)
     k_mp_encode<true><<<ge, 256, 0, s>>>(N, r, rr, inv_n, sf, P, skip, w.H[0], w.X);
   else
