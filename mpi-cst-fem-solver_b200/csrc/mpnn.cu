@@ -134,40 +134,45 @@ __global__ void k_mp_smoother_weights(int n, const double* __restrict__ invd, co
 
 // ---- encoder: H0 = relu(W_in X + b_in) ------------------------------------------------------------
 
-// Eight threads per node, thread c computing features 8c..8c+7 with its 64 weights and 8 biases in
-// registers (loaded once per thread); a warp writes four whole 128-byte rows per step. Each
-// feature is the same chain of FMAs in the same order for every launch shape.
+// Eight threads per node, thread c computing features 8c..8c+7; the weights sit in shared memory
+// transposed ([input][feature], a thread's eight features in two float4 reads). Four nodes per
+// thread and step, all four nodes' inputs loaded before any is used; a warp writes four whole
+// 128-byte rows per node step. Each feature is the same chain of FMAs in the same order for
+// every launch shape.
 template <bool TRAIN>
-__global__ void __launch_bounds__(256) k_mp_encode(int N, const double* __restrict__ r, const double* rr,
+__global__ void __launch_bounds__(256, 2) k_mp_encode(int N, const double* __restrict__ r, const double* rr,
                                                    double inv_n, const float* __restrict__ sf, MpnnParams P,
                                                    const int* skip, __nv_bfloat16* __restrict__ H0,
                                                    __nv_bfloat16* __restrict__ Xout) {
   if (skip && *skip) return;
-  const int c = threadIdx.x & 7;
-  float w[8][kMpIn], b[8];
-#pragma unroll
-  for (int j = 0; j < 8; ++j) {
-    b[j] = P.pf[kMpOffBin + c * 8 + j];
-#pragma unroll
-    for (int k = 0; k < kMpIn; ++k) w[j][k] = bf(P.pb[kMpOffWin + (c * 8 + j) * kMpIn + k]);
+  __shared__ __align__(16) float wt[kMpIn][F];
+  __shared__ __align__(16) float bs[F];
+  for (int i = threadIdx.x; i < F * kMpIn; i += blockDim.x) {
+    const int o = i / kMpIn, k = i % kMpIn;
+    wt[k][o] = bf(P.pb[kMpOffWin + i]);
   }
+  for (int i = threadIdx.x; i < F; i += blockDim.x) bs[i] = P.pf[kMpOffBin + i];
+  __syncthreads();
+  const int c = threadIdx.x & 7;
   const double s = sqrt(*rr * inv_n);
   const double sd = s > 0.0 ? s : 1.0;
   const int per_step = (gridDim.x * blockDim.x) >> 3;
-  for (int n = (blockIdx.x * blockDim.x + threadIdx.x) >> 3; n < N; n += per_step) {
+  auto inputs = [&](int n, float (&x)[kMpIn]) {
     const double2 rn = reinterpret_cast<const double2*>(r)[n];
-    float x[kMpIn];
+    const float2* sfn = reinterpret_cast<const float2*>(sf + (size_t)n * 6);
+    const float2 a0 = sfn[0], a1 = sfn[1], a2 = sfn[2];
     x[0] = (float)(rn.x / sd);
     x[1] = (float)(rn.y / sd);
-    const float2* sfn = reinterpret_cast<const float2*>(sf + (size_t)n * 6);
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      const float2 v = sfn[k];
-      x[2 + 2 * k] = v.x;
-      x[3 + 2 * k] = v.y;
-    }
+    x[2] = a0.x;
+    x[3] = a0.y;
+    x[4] = a1.x;
+    x[5] = a1.y;
+    x[6] = a2.x;
+    x[7] = a2.y;
 #pragma unroll
     for (int k = 0; k < kMpIn; ++k) x[k] = __bfloat162float(__float2bfloat16_rn(x[k]));
+  };
+  auto emit = [&](int n, const float (&x)[kMpIn]) {
     if (TRAIN && c == 0) {
       uint4 xv;
       xv.x = pack_bf2(x[0], x[1]);
@@ -176,16 +181,42 @@ __global__ void __launch_bounds__(256) k_mp_encode(int N, const double* __restri
       xv.w = pack_bf2(x[6], x[7]);
       reinterpret_cast<uint4*>(Xout)[n] = xv;
     }
-    float h[8];
+    const float4 b0 = *reinterpret_cast<const float4*>(&bs[c * 8]);
+    const float4 b1 = *reinterpret_cast<const float4*>(&bs[c * 8 + 4]);
+    float u[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      float u = b[j];
-#pragma unroll
-      for (int k = 0; k < kMpIn; ++k) u = fmaf(w[j][k], x[k], u);
-      h[j] = fmaxf(u, 0.f);
+    for (int k = 0; k < kMpIn; ++k) {
+      const float4 w0 = *reinterpret_cast<const float4*>(&wt[k][c * 8]);
+      const float4 w1 = *reinterpret_cast<const float4*>(&wt[k][c * 8 + 4]);
+      u[0] = fmaf(w0.x, x[k], u[0]);
+      u[1] = fmaf(w0.y, x[k], u[1]);
+      u[2] = fmaf(w0.z, x[k], u[2]);
+      u[3] = fmaf(w0.w, x[k], u[3]);
+      u[4] = fmaf(w1.x, x[k], u[4]);
+      u[5] = fmaf(w1.y, x[k], u[5]);
+      u[6] = fmaf(w1.z, x[k], u[6]);
+      u[7] = fmaf(w1.w, x[k], u[7]);
     }
     reinterpret_cast<uint4*>(H0 + (size_t)n * F)[c] =
-        make_uint4(pack_bf2(h[0], h[1]), pack_bf2(h[2], h[3]), pack_bf2(h[4], h[5]), pack_bf2(h[6], h[7]));
+        make_uint4(pack_bf2(fmaxf(u[0], 0.f), fmaxf(u[1], 0.f)), pack_bf2(fmaxf(u[2], 0.f), fmaxf(u[3], 0.f)),
+                   pack_bf2(fmaxf(u[4], 0.f), fmaxf(u[5], 0.f)), pack_bf2(fmaxf(u[6], 0.f), fmaxf(u[7], 0.f)));
+  };
+  int n = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+  for (; n + 3 * per_step < N; n += 4 * per_step) {
+    float x0[kMpIn], x1[kMpIn], x2[kMpIn], x3[kMpIn];
+    inputs(n, x0);
+    inputs(n + per_step, x1);
+    inputs(n + 2 * per_step, x2);
+    inputs(n + 3 * per_step, x3);
+    emit(n, x0);
+    emit(n + per_step, x1);
+    emit(n + 2 * per_step, x2);
+    emit(n + 3 * per_step, x3);
+  }
+  for (; n < N; n += per_step) {
+    float x0[kMpIn];
+    inputs(n, x0);
+    emit(n, x0);
   }
 }
 
@@ -207,6 +238,7 @@ __global__ void __launch_bounds__(256) k_mp_encode(int N, const double* __restri
 //            z = zbase + invd (r + s y).
 constexpr int kLT = 256;                            // threads of the layer kernel
 constexpr int kNbrCache = 128;                      // neighbour-list entries a warp keeps in shared memory
+constexpr int kLayerCtasPerSm = 4;                  // resident CTAs per SM (registers capped to fit them)
 constexpr int kTcSmem = kASmem + kBSmem + 1024;     // dynamic shared memory (1024-byte aligned base)
 
 struct MpLayerArgs {
@@ -256,7 +288,7 @@ __device__ __forceinline__ void add_chunk(float (&acc)[8], const uint4 v) {
 }
 
 template <bool TRAIN, bool LAST>
-__global__ void __launch_bounds__(kLT, 3) k_mp_layer_tc(const MpLayerArgs a) {
+__global__ void __launch_bounds__(kLT, kLayerCtasPerSm) k_mp_layer_tc(const MpLayerArgs a) {
   const int N = a.N;
   if (a.skip && *a.skip) {  // uniform: before any barrier or tensor-memory allocation
     if (LAST)                 // the network is off: the Jacobi step
@@ -734,12 +766,12 @@ cudaError_t set_tc_attr() {
   // the whole unified L1 / shared array as shared memory: three CTAs of ~56 KB per SM
   e = cudaFuncSetAttribute(k_mp_layer_tc<TRAIN, LAST>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
   if (e != cudaSuccess) return e;
-  int per_sm = 0, sms = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mp_layer_tc<TRAIN, LAST>, kLT, kTcSmem);
-  if (e != cudaSuccess) return e;
+  // one wave: kLayerCtasPerSm CTAs on every SM (the register cap of __launch_bounds__ and the
+  // ~56 KB of shared memory per CTA are sized for it)
+  int sms = 0;
   e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   if (e != cudaSuccess) return e;
-  slot = std::max(1, per_sm) * std::max(1, sms);
+  slot = kLayerCtasPerSm * std::max(1, sms);
   return cudaSuccess;
 }
 
@@ -787,7 +819,11 @@ cudaError_t launch_mp_forward(const MpnnGraph& g, const MpnnParams& P, const dou
   const int N = g.n_nodes;
   if (N <= 0) return cudaSuccess;
   const double inv_n = 1.0 / (2.0 * N);
-  const int ge = grid_nodes(8LL * N, 256);
+  int dev = 0, sms = kSMs;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  // one wave of the encoder (2 blocks of 256 per SM), at most 8 threads per node
+  const int ge = (int)std::max<long long>(1, std::min<long long>(2LL * sms, (8LL * N + 255) / 256));
   if (train)
     k_mp_encode<true><<<ge, 256, 0, s>>>(N, r, rr, inv_n, sf, P, skip, w.H[0], w.X);
   else
