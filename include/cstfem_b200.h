@@ -75,7 +75,11 @@ typedef struct {
   int check_interval;       /* iterations per device graph between host checks (0: auto)  */
   int launch_mode;          /* CSTG_LAUNCH_*                                               */
   int preconditioner;       /* CSTG_PRECOND_*                                              */
-  int reserved[2];
+  int fcg_depth;            /* flexible CG with a nonlinear (learned) preconditioner: each new
+                               direction is A-orthogonalised against this many earlier ones
+                               (1: the one-term flexible CG; at most 5); 0: automatic (3 for
+                               the learned preconditioners, 1 otherwise)                     */
+  int reserved[1];
 } cstg_solver_options;
 
 /* preconditioner of cstg_pcg_solve */

@@ -88,8 +88,13 @@ void cstg_destroy(cstg_ctx* ctx) {
                    &ctx->bat_x,   &ctx->bat_r,  &ctx->bat_p,    &ctx->bat_Ap,   &ctx->bat_stats,
                    &ctx->bat_in,  &ctx->bat_out, &ctx->lp_p32, &ctx->lp_pb,   &ctx->lp_pf,
                    &ctx->lp_sf,   &ctx->lp_h0,  &ctx->lp_h1,    &ctx->lp_sc,    &ctx->lp_z,
-                   &ctx->tr_con,  &ctx->tr_cnt, &ctx->tr_ptr,   &ctx->tr_cur,   &ctx->tr_rec};
+                   &ctx->tr_con,  &ctx->tr_cnt, &ctx->tr_ptr,   &ctx->tr_cur,   &ctx->tr_rec,
+                   &ctx->lm_winvd, &ctx->fcg_ring};
   for (DevBuf* b : all) free_buf(*b);
+  for (int j = 0; j < kFcgMaxHist; ++j) {
+    free_buf(ctx->fcg_ph[j]);
+    free_buf(ctx->fcg_qh[j]);
+  }
   if (ctx->h_err) cudaFreeHost(ctx->h_err);
   if (ctx->h_state) cudaFreeHost(ctx->h_state);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
@@ -771,6 +776,9 @@ static int check_solve_args(cstg_ctx* ctx, const cstg_solver_options* opt, cstg_
   if (o.precision == CSTG_PRECISION_MIXED && ctx->kind != 1)
     return fail(ctx, CSTG_ERR_UNSUPPORTED,
                 "pcg_solve: mixed precision needs the mesh (2x2-block) pattern of cstg_build_pattern");
+  if (o.fcg_depth < 0 || o.fcg_depth > kFcgMaxHist + 1)
+    return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "pcg_solve: fcg_depth %d outside 0..%d", o.fcg_depth,
+                kFcgMaxHist + 1);
   if (o.preconditioner != CSTG_PRECOND_JACOBI && o.preconditioner != CSTG_PRECOND_LEARNED &&
       o.preconditioner != CSTG_PRECOND_AMG && o.preconditioner != CSTG_PRECOND_LEARNED_MG)
     return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "pcg_solve: unknown preconditioner %d", o.preconditioner);

@@ -112,6 +112,8 @@ struct cstg_ctx {
   // built for the hierarchy of setup `lm_winvd_for`
   DevBuf lm_winvd;
   unsigned long long lm_winvd_for = ~0ull;
+  // truncated flexible CG: ring of earlier directions and their A-products, ring state
+  DevBuf fcg_ph[kFcgMaxHist], fcg_qh[kFcgMaxHist], fcg_ring;
 
   // bounded device waits (polls before a wait gives up; cstg_set_wait_limits)
   long long barrier_spin = kBarrierSpinDefault;

@@ -210,7 +210,151 @@ __global__ void __launch_bounds__(kThreads) k_fcg_update(int n, double* __restri
   }
 }
 
+// ---- truncated flexible CG (depth H + 1) -----------------------------------------------------------
+
+// Age of ring slot j (0: the most recent push); the slot holds a direction when age < count.
+__device__ __forceinline__ int ring_age(const FcgRing* R, int j, int H) { return (R->head - 1 - j + 2 * H) % H; }
+
+// As k_fcg_dots, plus z'q_j (and (D^-1 r)'q_j) for the ring's directions: the last block sets
+// beta[0] = -z'q / p'q for the current p and beta[1 + j] = -z'q_j / p_j'q_j for every stored one,
+// then registers the push of the current p / q into the ring (not on a restart, which clears it).
+template <int H>
+__global__ void __launch_bounds__(kThreads) k_fcg_dots_ring(FcgBuffers w) {
+  PcgState* st = w.st;
+  if (__ldcg(&st->done)) return;
+  FcgRing* R = w.ring;
+  bool valid[H];
+#pragma unroll
+  for (int j = 0; j < H; ++j) valid[j] = ring_age(R, j, H) < R->count;
+  double zr = 0.0, zq = 0.0, jr = 0.0, jq = 0.0, zqh[H], jqh[H];
+#pragma unroll
+  for (int j = 0; j < H; ++j) zqh[j] = jqh[j] = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < w.n; i += gridDim.x * blockDim.x) {
+    const double ri = w.r[i], qi = w.q[i], ji = w.inv_diag[i] * ri, zi = w.z[i];
+    zr = fma(zi, ri, zr);
+    zq = fma(zi, qi, zq);
+    jr = fma(ji, ri, jr);
+    jq = fma(ji, qi, jq);
+#pragma unroll
+    for (int j = 0; j < H; ++j)
+      if (valid[j]) {
+        const double qj = w.qh[j][i];
+        zqh[j] = fma(zi, qj, zqh[j]);
+        jqh[j] = fma(ji, qj, jqh[j]);
+      }
+  }
+  double v[4 + 2 * H];
+  v[0] = zr;
+  v[1] = zq;
+  v[2] = jr;
+  v[3] = jq;
+#pragma unroll
+  for (int j = 0; j < H; ++j) {
+    v[4 + j] = zqh[j];
+    v[4 + H + j] = jqh[j];
+  }
+  double tot[4 + 2 * H];
+  if (fcg_reduce<4 + 2 * H>(v, w.partials, &st->ticket[6], tot) && threadIdx.x == 0) {
+    bool restart = st->restart_pending != 0;
+    bool jac = st->fallback != 0;
+    if (!jac && !(tot[0] > 0.0)) {  // a non-descent network output: Jacobi this step, restarted
+      jac = true;
+      restart = true;
+    }
+    const double rz_new = jac ? tot[2] : tot[0];
+    double beta = 0.0;
+#pragma unroll
+    for (int j = 0; j < H; ++j) R->beta[1 + j] = 0.0;
+    if (!restart && st->rz > 0.0) {
+      if (st->fallback) {
+        beta = rz_new / st->rz;  // plain Jacobi-PCG (Fletcher-Reeves), solver.cpp:84-99
+      } else {
+        beta = -st->alpha * (jac ? tot[3] : tot[1]) / st->rz;  // -z'q / p'q
+#pragma unroll
+        for (int j = 0; j < H; ++j)
+          if (valid[j] && R->pq[j] > 0.0) R->beta[1 + j] = -(jac ? tot[4 + H + j] : tot[4 + j]) / R->pq[j];
+      }
+    }
+    st->beta = beta;
+    R->beta[0] = beta;
+    if (restart || st->fallback) {
+      R->count = 0;
+      R->push = 0;
+    } else {
+      R->push = 1;
+      R->push_slot = R->head;
+      R->pq[R->head] = st->pAp;
+      R->head = (R->head + 1) % H;
+      if (R->count < H) R->count += 1;
+    }
+    st->rz = rz_new;
+    st->use_jacobi = jac ? 1 : 0;
+    st->restart_pending = 0;
+  }
+}
+
+// p = z + beta[0] p + sum_j beta[1 + j] p_j (z = D^-1 r when use_jacobi); the old p and q go into
+// the ring slot registered by k_fcg_dots_ring (read before they are overwritten, element by element).
+template <int H>
+__global__ void __launch_bounds__(kThreads) k_fcg_pupdate_ring(FcgBuffers w) {
+  const PcgState* st = w.st;
+  if (__ldcg(&st->done)) return;
+  const FcgRing* R = w.ring;
+  const bool jac = __ldcg(&st->use_jacobi) != 0;
+  double beta[H + 1];
+#pragma unroll
+  for (int j = 0; j <= H; ++j) beta[j] = __ldcg(&R->beta[j]);
+  const bool push = __ldcg(&R->push) != 0;
+  const int slot = __ldcg(&R->push_slot);
+  double* ps = push ? w.ph[0] : nullptr;
+  double* qs = push ? w.qh[0] : nullptr;
+#pragma unroll
+  for (int j = 1; j < H; ++j)
+    if (push && slot == j) {
+      ps = w.ph[j];
+      qs = w.qh[j];
+    }
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < w.n; i += gridDim.x * blockDim.x) {
+    const double zi = jac ? w.inv_diag[i] * w.r[i] : w.z[i];
+    const double pi = w.p[i];
+    double pn = fma(beta[0], pi, zi);
+#pragma unroll
+    for (int j = 0; j < H; ++j)
+      if (beta[1 + j] != 0.0) pn = fma(beta[1 + j], w.ph[j][i], pn);
+    if (push) {
+      ps[i] = pi;
+      qs[i] = w.q[i];
+    }
+    w.p[i] = pn;
+  }
+}
+
 }  // namespace
+
+cudaError_t launch_fcg_dots_ring(const FcgBuffers& w, cudaStream_t s) {
+  switch (w.hist) {
+    case 1:
+      k_fcg_dots_ring<1><<<kGrid, kThreads, 0, s>>>(w);
+      k_fcg_pupdate_ring<1><<<kGrid, kThreads, 0, s>>>(w);
+      break;
+    case 2:
+      k_fcg_dots_ring<2><<<kGrid, kThreads, 0, s>>>(w);
+      k_fcg_pupdate_ring<2><<<kGrid, kThreads, 0, s>>>(w);
+      break;
+    case 3:
+      k_fcg_dots_ring<3><<<kGrid, kThreads, 0, s>>>(w);
+      k_fcg_pupdate_ring<3><<<kGrid, kThreads, 0, s>>>(w);
+      break;
+    case 4:
+      k_fcg_dots_ring<4><<<kGrid, kThreads, 0, s>>>(w);
+      k_fcg_pupdate_ring<4><<<kGrid, kThreads, 0, s>>>(w);
+      break;
+    default:
+      return launch_fcg_dots(w, s);
+  }
+  count_launches(2);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_fcg_init(const FcgBuffers& w, double rtol, int max_iter, int window, cudaStream_t s) {
   (void)window;

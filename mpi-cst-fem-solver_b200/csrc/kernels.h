@@ -221,6 +221,18 @@ cudaError_t launch_mp_adam(float* p, float* m, float* v, const float* g, float l
                            int step, float scale, __nv_bfloat16* pb, float* pf, cudaStream_t s);
 
 // fcg.cu: flexible CG with the learned preconditioner (Polak-Ribiere beta), Jacobi fallback.
+// Truncated flexible CG: besides the current direction p (and q = A p), up to kFcgMaxHist earlier
+// directions and their products sit in a ring, and each new direction is A-orthogonalised
+// against all of them (depth = ring size + 1; depth 1 is the one-term flexible CG).
+constexpr int kFcgMaxHist = 4;
+struct FcgRing {
+  double pq[kFcgMaxHist];         // p_j'q_j of the ring's directions
+  double beta[kFcgMaxHist + 1];   // this step's coefficients: [0] current p, [1 + j] ring slot j
+  int count;                      // directions in the ring
+  int head;                       // slot the current p is pushed into (the oldest when full)
+  int push;                       // 1: this step pushes the current p / q into slot `head` (before it moves)
+  int push_slot;
+};
 struct FcgBuffers {
   int n = 0;  // rows (2 x nodes)
   double *x = nullptr, *r = nullptr, *p = nullptr, *q = nullptr, *z = nullptr;
@@ -228,11 +240,18 @@ struct FcgBuffers {
   const double* inv_diag = nullptr;
   double* partials = nullptr;
   PcgState* st = nullptr;
+  int hist = 0;                   // ring size (0: one-term flexible CG)
+  double* ph[kFcgMaxHist] = {};   // ring of earlier directions
+  double* qh[kFcgMaxHist] = {};   // and of their A-products
+  FcgRing* ring = nullptr;
 };
 cudaError_t launch_fcg_init(const FcgBuffers& w, double rtol, int max_iter, int window, cudaStream_t s);
 cudaError_t launch_fcg_dots(const FcgBuffers& w, cudaStream_t s);  // beta, r'z; then p = z + beta p
 cudaError_t launch_fcg_update(const FcgBuffers& w, int window, double ratio2, cudaStream_t s);
 cudaError_t launch_fcg_pupdate(const FcgBuffers& w, cudaStream_t s);  // p = z + beta p alone
+// the truncated variant (w.hist ring directions; 0 falls back to launch_fcg_dots): the betas against
+// the current and the stored directions, then the new p (the ring state must start cleared)
+cudaError_t launch_fcg_dots_ring(const FcgBuffers& w, cudaStream_t s);
 // q = A p with p'Ap and alpha = r'z / p'Ap (the PCG variants of the SpMVs)
 cudaError_t launch_spmv_pcg(const BlockMatrix& A, const double* p, double* q, double* partials, PcgState* st,
                             cudaStream_t s);

@@ -10,6 +10,10 @@
 
 namespace {
 
+// Depth of the truncated flexible CG with a learned preconditioner (each new direction is
+// A-orthogonalised against this many earlier ones): the network's output varies nonlinearly with
+// r, and the one-term recurrence then loses the conjugacy that a linear preconditioner keeps.
+constexpr int kFcgDepthLearned = 3;
 // Stagnation rule of the flexible CG: the network is switched off when ||r|| has not halved
 // over this many iterations.
 constexpr int kFcgWindow = 1000;
@@ -124,6 +128,14 @@ int cstg_host::run_fcg(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg
   w.partials = buf_ptr<double>(ctx->partials);
   w.st = buf_ptr<PcgState>(ctx->state);
   const BlockMatrix bm = block_view(ctx);
+  const auto set_ring = [&](int h) {
+    w.hist = h;
+    for (int j = 0; j < h; ++j) {
+      w.ph[j] = buf_ptr<double>(ctx->fcg_ph[j]);
+      w.qh[j] = buf_ptr<double>(ctx->fcg_qh[j]);
+    }
+    w.ring = h > 0 ? buf_ptr<FcgRing>(ctx->fcg_ring) : nullptr;
+  };
   const MixedMatrix mm = mixed ? mixed_view(ctx) : MixedMatrix{};
   const MpnnGraph g = graph_view(ctx);
   const MpnnParams P = params_view(ctx);
@@ -137,6 +149,17 @@ int cstg_host::run_fcg(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg
   // finest-level sweep (no separate dots pass), and there is no stagnation fallback (the cycle is
   // a fixed symmetric positive operator).
   const bool fused_dots = o.preconditioner == CSTG_PRECOND_AMG && amg_levels(ctx) > 1;
+  // truncated flexible CG for the nonlinear (learned) preconditioners: the ring of earlier directions
+  const int depth = o.fcg_depth > 0 ? o.fcg_depth : (use_net ? kFcgDepthLearned : 1);
+  const int hist = fused_dots ? 0 : std::min(depth - 1, kFcgMaxHist);
+  if (hist > 0) {
+    for (int j = 0; j < hist; ++j) {
+      ENSURE(ctx->fcg_ph[j], sizeof(double) * (size_t)std::max(n, 1));
+      ENSURE(ctx->fcg_qh[j], sizeof(double) * (size_t)std::max(n, 1));
+    }
+    ENSURE(ctx->fcg_ring, sizeof(FcgRing));
+  }
+  set_ring(hist);
   MpScratch* msc = buf_ptr<MpScratch>(ctx->lp_sc);
   const double* winvd = cycle_net ? buf_ptr<double>(ctx->lm_winvd) : nullptr;
   FcgDotSink sink;
@@ -156,6 +179,8 @@ int cstg_host::run_fcg(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg
     }
     if (fused_dots)
       CK(launch_fcg_pupdate(w, ctx->stream));
+    else if (w.hist > 0)
+      CK(launch_fcg_dots_ring(w, ctx->stream));
     else
       CK(launch_fcg_dots(w, ctx->stream));
     return CSTG_OK;
@@ -173,7 +198,8 @@ int cstg_host::run_fcg(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg
   unsigned long long key = 1469598103934665603ull;
   for (unsigned long long v : {ctx->generation, (unsigned long long)chunk, (unsigned long long)o.precision,
                                (unsigned long long)(uintptr_t)d_b, (unsigned long long)n,
-                               (unsigned long long)ctx->n_nodes, use_amg ? amg_signature(ctx) : 0ull})
+                               (unsigned long long)ctx->n_nodes, use_amg ? amg_signature(ctx) : 0ull,
+                               (unsigned long long)hist})
     key = (key ^ v) * 1099511628211ull;
   if (!ctx->fcg_graph || ctx->fcg_key != key || ctx->fcg_graph_precond != o.preconditioner) {
     if (ctx->fcg_graph) {
@@ -204,6 +230,7 @@ int cstg_host::run_fcg(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg
   RESET_ERR();
   CK(cudaEventRecord(ctx->ev0, ctx->stream));
   if (n) CK(cudaMemsetAsync(w.q, 0, sizeof(double) * (size_t)n, ctx->stream));
+  if (hist > 0) CK(cudaMemsetAsync(w.ring, 0, sizeof(FcgRing), ctx->stream));  // an empty ring
   int zero = 0;
   CK(cudaMemcpyAsync(&w.st->fp64_mode, &zero, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
   CK(launch_fcg_init(w, o.rtol, o.max_iter, kFcgWindow, ctx->stream));

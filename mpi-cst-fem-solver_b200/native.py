@@ -49,7 +49,8 @@ class SolverOptions(C.Structure):
     _fields_ = [("rtol", C.c_double), ("max_iter", C.c_int), ("record_history", C.c_int),
                 ("precision", C.c_int), ("true_residual_stop", C.c_int),
                 ("max_refinements", C.c_int), ("check_interval", C.c_int),
-                ("launch_mode", C.c_int), ("preconditioner", C.c_int), ("reserved", C.c_int * 2)]
+                ("launch_mode", C.c_int), ("preconditioner", C.c_int), ("fcg_depth", C.c_int),
+                ("reserved", C.c_int * 1)]
 
 
 TRACTION_CONSTANT = 0

@@ -343,6 +343,7 @@ class SolverOptions:
     # "jacobi" | "learned" (the network alone in flexible CG; needs learned setup) | "amg" |
     # "learned_mg" (the network as the multigrid cycle's post-smoother; needs learned setup)
     preconditioner: str = "jacobi"
+    fcg_depth: int = 0  # flexible CG: earlier directions each new one is A-orthogonalised against (0: auto)
 
     def native(self) -> native.SolverOptions:
         o = native.default_options()
@@ -358,6 +359,7 @@ class SolverOptions:
         o.preconditioner = {"jacobi": native.PRECOND_JACOBI, "learned": native.PRECOND_LEARNED,
                             "amg": native.PRECOND_AMG,
                             "learned_mg": native.PRECOND_LEARNED_MG}[self.preconditioner]
+        o.fcg_depth = self.fcg_depth
         return o
 
 
