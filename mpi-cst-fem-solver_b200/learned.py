@@ -269,6 +269,45 @@ def train(n_plates: int = 100, samples_per_plate: int = 100, epochs: int = 3, ba
     return params, hist, n_pairs
 
 
+def scale_output(params: np.ndarray, gain: float) -> np.ndarray:
+    """The network with its output layer (W_out, b_out) multiplied by `gain`."""
+    p = np.array(params, dtype=np.float32, copy=True)
+    p[-(2 * F + 2):] *= np.float32(gain)
+    return p
+
+
+def select_gain(params: np.ndarray, n_plates: int = 4, seed: int = 5151, gains=(0.25, 0.5, 0.75, 1.0),
+                n_r_range=(60, 160), device: int = 0, log=print):
+    """Chooses the output gain of the cycle's post-smoother on validation plates (seeded draws
+    from the training distribution, not the training batch): the gain with the fewest flexible-CG
+    iterations of the learned cycle in total. The network's output varies nonlinearly with r; a
+    full-strength correction lowers the per-step loss most but can cost Krylov iterations, so the
+    gain is chosen on the solve itself. Returns (gain, {gain: total iterations})."""
+    from .solver import CgJacobiSolver, SolverOptions
+    specs = random_batch(count=n_plates, seed=seed, n_r_range=n_r_range)
+    systems = []
+    for spec in specs:
+        m, D, K, b = plate_system(spec, Context(device))
+        systems.append((m, D, K, b))
+    totals = {}
+    for g in gains:
+        p = scale_output(params, g)
+        tot = 0
+        for m, D, K, b in systems:
+            s = CgJacobiSolver(SolverOptions(rtol=1e-10, max_iter=5000, precision="mixed",
+                                             preconditioner="learned_mg", true_residual_stop=True))
+            s.setup(K)
+            setup(K, p, node_material(D, m.num_nodes))
+            st = s.solve(b, np.zeros(m.num_dofs))
+            tot += st.iterations if st.converged else 10 ** 6
+        totals[float(g)] = tot
+        log(f"gain {g}: {tot} iterations on {n_plates} validation plates")
+    for m, D, K, b in systems:
+        K.ctx.close()
+    best = min(totals, key=lambda g: (totals[g], -g))
+    return best, totals
+
+
 def main():
     ap = argparse.ArgumentParser(description="train the learned preconditioner on the GPU")
     ap.add_argument("cmd", choices=["train"])
@@ -286,10 +325,16 @@ def main():
     t0 = time.perf_counter()
     params, hist, n_pairs = train(a.plates, a.samples, a.epochs, a.batch, a.lr, a.seed, (20, a.n_r_max),
                                   mode=a.mode)
+    extra = {}
+    if a.mode == "cycle":
+        gain, totals = select_gain(params)
+        params = scale_output(params, gain)
+        extra = dict(output_gain=gain, gain_iterations=np.array([[g, it] for g, it in sorted(totals.items())]))
+        print(f"output gain {gain} (validation iterations {totals})")
     os.makedirs(os.path.dirname(os.path.abspath(out)), exist_ok=True)
     np.savez(out, params=params, loss_history=np.array(hist), pairs=n_pairs, plates=a.plates,
              samples=a.samples, epochs=a.epochs, batch=a.batch, lr=a.lr, seed=a.seed, mode=a.mode,
-             seconds=time.perf_counter() - t0)
+             seconds=time.perf_counter() - t0, **extra)
     print(f"wrote {out}")
 
 
