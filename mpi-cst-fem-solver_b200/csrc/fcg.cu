@@ -82,6 +82,8 @@ __global__ void __launch_bounds__(kThreads) k_fcg_init(int n, const double* __re
     st->fb_rr0 = tot[0];
     st->fb_it0 = 0;
     st->true_rel = 0.0;
+    st->rmax = st->rel;
+    st->reliable_due = 0;
   }
 }
 
@@ -159,7 +161,8 @@ __global__ void __launch_bounds__(kThreads) k_fcg_pupdate(int n, const double* _
 __global__ void __launch_bounds__(kThreads) k_fcg_update(int n, double* __restrict__ x, double* __restrict__ r,
                                                          const double* __restrict__ p,
                                                          const double* __restrict__ q, double* partials,
-                                                         PcgState* st, int window, double ratio2) {
+                                                         PcgState* st, int window, double ratio2,
+                                                         double reliable_delta) {
   if (__ldcg(&st->done)) return;
   const double alpha = __ldcg(&st->alpha);
   double rr = 0.0;
@@ -207,6 +210,47 @@ __global__ void __launch_bounds__(kThreads) k_fcg_update(int n, double* __restri
       st->fb_it0 = it;
     }
     st->mp_skip = (st->done != 0 || st->fallback != 0) ? 1 : 0;
+    if (reliable_delta > 0.0 && st->done == 0) {
+      st->rmax = fmax(st->rmax, st->rel);
+      if (st->rel < reliable_delta * st->rmax) st->reliable_due = 1;
+    }
+  }
+}
+
+// r = b - A x with the FP64 2x2-block matrix, thread per node, and ||r||; the recursive residual
+// becomes the true one (van der Vorst-Ye reliable update, the direction and the ring are kept).
+__global__ void __launch_bounds__(kThreads) k_fcg_reliable(int n_nodes, BlockMatrix A, const double* __restrict__ b,
+                                                           const double* __restrict__ x, double* __restrict__ r,
+                                                           double* partials, PcgState* st) {
+  if (__ldcg(&st->done) || !__ldcg(&st->reliable_due)) return;  // uniform
+  const double2* x2 = reinterpret_cast<const double2*>(x);
+  const double2* b2 = reinterpret_cast<const double2*>(b);
+  double2* r2 = reinterpret_cast<double2*>(r);
+  const double2* v2 = reinterpret_cast<const double2*>(A.vals);
+  double rr = 0.0;
+  for (int nd = blockIdx.x * blockDim.x + threadIdx.x; nd < n_nodes; nd += gridDim.x * blockDim.x) {
+    const int k0 = A.node_ptr[nd], d = A.node_ptr[nd + 1] - k0;
+    const size_t base = 2 * (size_t)k0;  // node nd's rows start at value 4 k0 (double2 index 2 k0)
+    double y0 = 0.0, y1 = 0.0;
+    for (int k = 0; k < d; ++k) {
+      const double2 xm = x2[A.bnbr[k0 + k]];
+      const double2 a0 = v2[base + k], a1 = v2[base + d + k];
+      y0 = fma(a0.x, xm.x, fma(a0.y, xm.y, y0));
+      y1 = fma(a1.x, xm.x, fma(a1.y, xm.y, y1));
+    }
+    const double2 bn = b2[nd];
+    const double2 rn = make_double2(bn.x - y0, bn.y - y1);
+    r2[nd] = rn;
+    rr = fma(rn.x, rn.x, fma(rn.y, rn.y, rr));
+  }
+  const double v[1] = {rr};
+  double tot[1];
+  if (fcg_reduce<1>(v, partials, &st->ticket[4], tot) && threadIdx.x == 0) {
+    st->rr = tot[0];
+    st->rel = st->bnorm > 0.0 ? sqrt(tot[0]) / st->bnorm : 0.0;
+    st->rmax = st->rel;
+    st->reliable_due = 0;
+    st->replace_count += 1;
   }
 }
 
@@ -376,8 +420,16 @@ cudaError_t launch_fcg_pupdate(const FcgBuffers& w, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-cudaError_t launch_fcg_update(const FcgBuffers& w, int window, double ratio2, cudaStream_t s) {
-  k_fcg_update<<<kGrid, kThreads, 0, s>>>(w.n, w.x, w.r, w.p, w.q, w.partials, w.st, window, ratio2);
+cudaError_t launch_fcg_update(const FcgBuffers& w, int window, double ratio2, cudaStream_t s,
+                              double reliable_delta) {
+  k_fcg_update<<<kGrid, kThreads, 0, s>>>(w.n, w.x, w.r, w.p, w.q, w.partials, w.st, window, ratio2,
+                                          reliable_delta);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fcg_reliable(const FcgBuffers& w, const BlockMatrix& A, cudaStream_t s) {
+  k_fcg_reliable<<<kGrid, kThreads, 0, s>>>(A.n_nodes, A, w.b, w.x, w.r, w.partials, w.st);
   count_launches(1);
   return cudaGetLastError();
 }

@@ -91,6 +91,7 @@ struct alignas(128) PcgState {
   unsigned int bar_gen;    // persistent kernel: barrier generation (bumped on release)
   int bar_err;             // persistent kernel: a barrier wait ran out (the solve is abandoned)
   unsigned int ticket[8];  // last-block tickets, one per kernel kind
+  int reliable_due;        // flexible CG, mixed: the recursive residual fell by the reliable-update factor
 };
 static_assert(sizeof(PcgState) <= 256, "PcgState must fit its 256-byte slot");
 
@@ -247,7 +248,12 @@ struct FcgBuffers {
 };
 cudaError_t launch_fcg_init(const FcgBuffers& w, double rtol, int max_iter, int window, cudaStream_t s);
 cudaError_t launch_fcg_dots(const FcgBuffers& w, cudaStream_t s);  // beta, r'z; then p = z + beta p
-cudaError_t launch_fcg_update(const FcgBuffers& w, int window, double ratio2, cudaStream_t s);
+cudaError_t launch_fcg_update(const FcgBuffers& w, int window, double ratio2, cudaStream_t s,
+                              double reliable_delta = 0.0);
+// Reliable update of the flexible CG (mixed precision): when k_fcg_update found the recursive
+// residual below reliable_delta times its largest value since the last update, r = b - A x with
+// the FP64 matrix (p, z and the ring are kept: no restart); a no-op otherwise.
+cudaError_t launch_fcg_reliable(const FcgBuffers& w, const BlockMatrix& A, cudaStream_t s);
 cudaError_t launch_fcg_pupdate(const FcgBuffers& w, cudaStream_t s);  // p = z + beta p alone
 // the truncated variant (w.hist ring directions; 0 falls back to launch_fcg_dots): the betas against
 // the current and the stored directions, then the new p (the ring state must start cleared)

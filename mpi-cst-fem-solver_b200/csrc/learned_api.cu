@@ -190,7 +190,11 @@ int cstg_host::run_fcg(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg
       CK(launch_spmv_mixed_pcg(mm, bm, w.p, w.q, w.partials, w.st, ctx->stream));
     else
       CK(launch_spmv_pcg(bm, w.p, w.q, w.partials, w.st, ctx->stream));
-    CK(launch_fcg_update(w, o.preconditioner == CSTG_PRECOND_AMG ? 0 : kFcgWindow, kFcgRatio2, ctx->stream));
+    CK(launch_fcg_update(w, o.preconditioner == CSTG_PRECOND_AMG ? 0 : kFcgWindow, kFcgRatio2, ctx->stream,
+                         mixed ? kReliableDelta : 0.0));
+    // mixed precision: the FP32 operator's rounding accumulates in the recursive residual, which
+    // is replaced by the FP64 b - A x once per decade of reduction (no restart)
+    if (mixed) CK(launch_fcg_reliable(w, bm, ctx->stream));
     return precondition();
   };
   const int chunk = o.check_interval > 0 ? o.check_interval : 25;
