@@ -1,19 +1,29 @@
 #!/usr/bin/env python
-"""Time-to-solve benchmark of the CST assembly -> Dirichlet -> Jacobi-PCG path on B200.
+"""Time-to-solve benchmark of the CST assembly -> loads -> Dirichlet -> preconditioned CG path on B200.
 
 A step is one full pass of the path over one synthetic plate: stiffness pattern, assembly,
-Dirichlet elimination, Jacobi setup and PCG to rtol 1e-10 on the FP64 TRUE residual
-(||b - A x|| / ||b||). The default workload is the 2M-DOF quarter plate (O-grid n_r = 565 x
-n_theta = 1766, 2,000,244 DOFs, ~28M nonzeros; E = 1, nu = 0.3, plane stress, t = 1,
-traction (1, 0) on x = 10, u_x = 0 on x = 0, u_y = 0 on y = 0).
+traction loads (on the GPU), Dirichlet elimination, Jacobi setup, preconditioner setup and
+flexible CG to rtol 1e-10 on the FP64 TRUE residual (||b - A x|| / ||b||). The default workload
+is the 2M-DOF quarter plate (O-grid n_r = 565 x n_theta = 1766, 2,000,244 DOFs, 27,966,096
+nonzeros; E = 1, nu = 0.3, plane stress, t = 1, traction (1, 0) on x = 10, u_x = 0 on x = 0,
+u_y = 0 on y = 0).
+
+The timed solve is the learned preconditioner in mixed precision: the multigrid cycle whose
+finest-level post-smoother is the trained message-passing network (BF16 tensor-core layers),
+FP32 cycle operators and SpMV, FP64 vectors, scalars and reliable updates, inside flexible CG.
+Beside it, on the same matrix: plain FP64 Jacobi-PCG on the GPU (the method the learned solve is
+compared with), mixed Jacobi-PCG, the Chebyshev multigrid cycle without a network, the same
+learned cycle with the network at zero, and each solution's error against the reference
+serial core's displacements (tests/golden, computed by the reference's own code).
 
   value  DOFs solved per second with the mesh, loads and BCs already in HBM (CUDA events on
          the work stream), summed over all GPUs (independent replicas, weak scaling).
   e2e    the same through the C ABI with pinned HOST buffers: every step uploads the mesh,
-         loads and BCs and downloads the displacements (wall clock around the step).
+         edges and BCs and downloads the displacements (wall clock around the step).
 
 One JSON line on rank 0. `--impl reference` times the reference's own CPU path (compiled from
-its sources into oracle/_ref) on this host's cores instead, on bounded samples.
+its sources into oracle/_ref) on this host's cores instead, on bounded samples of its solve,
+next to the committed record of its full run.
 """
 from __future__ import annotations
 
@@ -42,14 +52,15 @@ WORKLOADS = {
     "plate40x80": (40, 80, "quarter plate [0,10]^2 minus r<1, O-grid n_r=40 x n_theta=80"),
 }
 
-# FP64 Jacobi-PCG iterations to the reference's own stopping rule (recursive residual < 1e-10,
-# solver.cpp:80-82) on each workload, measured with this library's FP64 solver (same
-# recurrence; the GPU-vs-reference parity tests hold the count to 2 %). The CPU baseline and
-# the reference arm time a bounded number of the reference's iterations and scale to this.
-REF_RULE_ITERS = {"plate2m": 19530, "plate1m": 13812, "plate4m": 27665, "plate40x80": 897}
+# Committed records of the reference serial core run to convergence on the build host
+# (tests/golden/make_golden_large.py): iterations, wall seconds per phase, host.
+GOLDEN = os.path.join(REPO, "tests", "golden")
+RECORDS = {"plate2m": "plate_565x1766", "plate1m": "plate_400x1250", "plate40x80": "plate_40x80"}
 
-METRIC = ("time-to-solve @rtol 1e-10 (FP64 true residual), 2M-DOF plate, as DOFs solved per "
-          "second")
+METRIC = ("time-to-solve @rtol 1e-10 (FP64 true residual), 2M-DOF plate, learned preconditioner + mixed "
+          "precision, as DOFs solved per second")
+
+PRECONDS = {"learned": "learned_mg", "learned_local": "learned", "amg": "amg", "jacobi": "jacobi"}
 
 
 def log(*a):
@@ -63,37 +74,25 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="plate2m", choices=sorted(WORKLOADS))
-    ap.add_argument("--precond", default="amg", choices=["amg", "jacobi", "learned"],
-                    help="preconditioner of the timed solve: smoothed-aggregation multigrid (default), "
-                         "Jacobi (the reference's method, persistent kernel) or the learned network")
-    ap.add_argument("--amg-smoother", default="chebyshev", choices=["chebyshev", "jacobi"],
-                    help="smoother of the multigrid cycle")
-    ap.add_argument("--amg-theta", type=float, nargs=2, default=[0.0, 0.03], metavar=("FINE", "COARSE"),
-                    help="strength-of-connection thresholds of the multigrid aggregation")
-    ap.add_argument("--precision", default=None, choices=["fp64", "mixed"],
-                    help="outer CG precision; default fp64 with amg (its finest smoother is FP32 already), "
-                         "mixed otherwise")
+    ap.add_argument("--precond", default="learned", choices=sorted(PRECONDS),
+                    help="preconditioner of the timed solve: the learned multigrid cycle (default: the "
+                         "trained network as the cycle's post-smoother), the network alone "
+                         "(learned_local), the Chebyshev multigrid cycle (amg) or Jacobi")
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--cpu-sample-iters", type=int, default=150)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--no-learned", action="store_true", help="skip the learned-preconditioner comparison")
-    ap.add_argument("--only", choices=["spmv", "solve", "batch", "batchsolve", "learned", "amg"], default=None,
-                    help="profiling modes: `spmv` runs --reps SpMV launches on the assembled plate, "
-                         "`solve` one full step, `batch` the 64-plate x 4-load-case batched solve "
-                         "(every launch shape, autotuned, --reps graph replays, and the same systems "
-                         "solved one by one), `batchsolve` one batched solve (8 x 512 shape) of "
-                         "--batch-plates plates with n_r up to --batch-nr-max, `learned` --reps "
-                         "applications of the learned preconditioner on the plate; each prints one "
-                         "JSON line")
-    ap.add_argument("--batch-plates", type=int, default=64)
-    ap.add_argument("--batch-nr-max", type=int, default=200)
+    ap.add_argument("--no-compare", action="store_true", help="skip the comparison solves")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-solve measurement")
+    ap.add_argument("--only", choices=["spmv", "solve", "batch", "learned", "amg"], default=None,
+                    help="profiling modes (one JSON line each): `spmv` --reps SpMV launches, `solve` one "
+                         "full step, `batch` the 64-plate x 4-load-case batched solve, `learned` the "
+                         "network's stages, `amg` the multigrid cycle")
     ap.add_argument("--reps", type=int, default=20)
     ap.add_argument("--max-iter", type=int, default=200000,
                     help="iteration cap of the solves (profiling captures use a small cap)")
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)
-    if a.precision is None:
-        a.precision = "fp64" if a.precond == "amg" else "mixed"
     return a
 
 
@@ -221,6 +220,33 @@ def make_inputs(pkg, workload):
     return mesh, D, dofs, vals
 
 
+def reference_record(workload):
+    """The reference serial core's full run on this workload (tests/golden/plate_*.json/.npz):
+    its iterations, true residual, SCF, displacements (all or a subsample) and wall-clock record."""
+    name = RECORDS.get(workload)
+    if not name or not os.path.exists(os.path.join(GOLDEN, name + ".json")):
+        return None
+    meta = json.load(open(os.path.join(GOLDEN, name + ".json")))
+    npz = np.load(os.path.join(GOLDEN, name + ".npz"))
+    if "u_sub" in npz.files:
+        stride = int(meta.get("u_stride_nodes", 8))
+        n_nodes = meta["n_dofs"] // 2
+        nodes = np.arange(0, n_nodes, stride)
+        idx = np.stack([2 * nodes, 2 * nodes + 1], axis=1).reshape(-1)
+        u = npz["u_sub"]
+    else:
+        idx, u = None, npz["u"]
+    return {"meta": meta, "u": u, "idx": idx, "file": f"tests/golden/{name}.json"}
+
+
+def rel_error_vs_reference(rec, x):
+    """||x - u_ref|| / ||u_ref|| over the DOFs the record holds (all, or every 8th node)."""
+    if rec is None:
+        return None
+    xs = x if rec["idx"] is None else x[rec["idx"]]
+    return float(np.linalg.norm(xs - rec["u"]) / np.linalg.norm(rec["u"]))
+
+
 # ---- CPU baseline: the reference's serial core on a bounded sample ---------------------------------
 
 def cpu_sample(mesh, dofs, vals, sample_iters: int):
@@ -237,11 +263,11 @@ def cpu_sample(mesh, dofs, vals, sample_iters: int):
         R.add_traction(m, "right", 1.0, 1.0, 0.0, f)
         R.apply_dirichlet(K, dofs, vals, f)
         t1 = time.perf_counter()
-        _, st = R.pcg(K, f, 1e-10, sample_iters)
+        _, st = R.pcg(K, f, 1e-30, sample_iters)
         t2 = time.perf_counter()
         R.free_csr(K)
         R.free_mesh(m)
-        return {"kind": "reference", "setup_s": t1 - t0, "solve_s": t2 - t1,
+        return {"kind": "reference", "setup_s": t1 - t0, "solve_s": t2 - t1, "wall_s": t2 - t0,
                 "iters": st["iterations"], "per_iter_s": st["t_solve"] / max(st["iterations"], 1)}
     O = oracle.Oracle()
     t0 = time.perf_counter()
@@ -251,20 +277,30 @@ def cpu_sample(mesh, dofs, vals, sample_iters: int):
     O.add_traction(mesh.xy, mesh.triangles, mesh.boundary_edges["right"], 1.0, 1.0, 0.0, f)
     O.apply_dirichlet(rp, cols, kv, dofs, vals, f)
     t1 = time.perf_counter()
-    _, st = O.pcg_jacobi(rp, cols, kv, f, 1e-10, sample_iters)
+    _, st = O.pcg_jacobi(rp, cols, kv, f, 1e-30, sample_iters)
     t2 = time.perf_counter()
-    return {"kind": "port", "setup_s": t1 - t0, "solve_s": t2 - t1, "iters": st["iterations"],
+    return {"kind": "port", "setup_s": t1 - t0, "solve_s": t2 - t1, "wall_s": t2 - t0, "iters": st["iterations"],
             "per_iter_s": (t2 - t1) / max(st["iterations"], 1)}
 
 
-def cpu_baseline_entry(s, n_dofs, iters_full, sample_iters):
+def cpu_baseline_entry(s, n_dofs, rec):
+    """The reference's time-to-solve on this host: its measured setup and per-iteration cost from
+    the bounded sample, times the iteration count its own full run needed (the committed record)."""
+    cr = rec["meta"]["cpu_run"]
+    iters_full = int(rec["meta"]["iters"])
     t = s["setup_s"] + s["per_iter_s"] * iters_full
-    return {"value": n_dofs / t, "unit": "DOF/s", "cores": 1, "kind": s["kind"],
-            "time_to_solve_s": t,
-            "sample": (f"full pattern+assembly+loads+BCs ({s['setup_s']:.2f} s) + {s['iters']} of "
-                       f"{iters_full} PCG iterations ({s['per_iter_s'] * 1e3:.2f} ms each, the "
-                       f"reference's recursive-residual rule), extrapolated; single-threaded "
-                       f"reference serial core, host has {os.cpu_count()} cores")}
+    return {"value": n_dofs / t, "unit": "DOF/s", "cores": 1, "kind": s["kind"], "time_to_solve_s": t,
+            "extrapolated": True, "sample_iters": s["iters"], "iterations_full_run": iters_full,
+            "sample": (f"full pattern+assembly+loads+BCs ({s['setup_s']:.2f} s) + {s['iters']} PCG iterations "
+                       f"({s['per_iter_s'] * 1e3:.2f} ms each) on this host, scaled to the {iters_full} iterations "
+                       f"of the reference's own full run (recursive residual < 1e-10, solver.cpp:80-82); "
+                       f"single-threaded reference serial core, host has {os.cpu_count()} cores"),
+            "full_run_record": {"file": rec["file"], "solve_s": cr["solve_s"], "per_iter_s": cr["per_iter_full_s"],
+                                "setup_s": cr["build_stiffness_pattern_s"] + cr["assemble_stiffness_s"] +
+                                cr["add_traction_s"] + cr["apply_dirichlet_s"] + cr["solver_setup_s"],
+                                "host": cr["cpu_model"], "nproc": cr["nproc"], "date": cr["date"],
+                                "sample_vs_full_per_iter_on_that_host": cr["sample_vs_full"]},
+            "per_iter_here_vs_record_host": s["per_iter_s"] / cr["per_iter_full_s"]}
 
 
 # ---- the reference arm ----------------------------------------------------------------------------
@@ -276,11 +312,11 @@ def run_reference(a, dist: Dist):
     n_r, n_t, desc = WORKLOADS[a.workload]
     mesh = pkg.quarter_plate(n_r, n_t)
     dofs, vals = pkg.symmetry_dirichlet(mesh)
-    iters_full = REF_RULE_ITERS.get(a.workload)
-    if iters_full is None:
-        print(json.dumps({"impl": "reference", "unavailable": f"no iteration count recorded for {a.workload}"}))
+    rec = reference_record(a.workload)
+    if rec is None or "cpu_run" not in rec["meta"]:
+        print(json.dumps({"impl": "reference", "unavailable": f"no full-run record of the reference for {a.workload}"}))
         return 0
-    sample_iters = max(10, a.cpu_sample_iters // 3)
+    sample_iters = 50
     samples = []
     for i in range(a.warmup + a.steps):
         s = cpu_sample(mesh, dofs, vals, sample_iters)
@@ -288,27 +324,31 @@ def run_reference(a, dist: Dist):
             samples.append(s)
     per_it = statistics.median(s["per_iter_s"] for s in samples)
     setup = statistics.median(s["setup_s"] for s in samples)
-    t = setup + per_it * iters_full
-    value = mesh.num_dofs / t
+    wall = statistics.median(s["wall_s"] for s in samples)
     cb = cpu_baseline_entry({"kind": samples[0]["kind"], "setup_s": setup, "per_iter_s": per_it,
-                             "iters": sample_iters}, mesh.num_dofs, iters_full, sample_iters)
-    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "DOF/s", "n_gpus": a.gpus,
-            "steps": a.steps, "warmup": a.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+                             "iters": sample_iters}, mesh.num_dofs, rec)
+    cb["value_note"] = "value = this line's value"
+    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "DOF/s", "n_gpus": a.gpus,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": wall * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "extrapolated": True, "sample_iters": sample_iters,
             "config": {"workload": f"{a.workload}: {desc}, {mesh.num_dofs} DOFs",
-                       "step": "reference serial core: pattern + assembly + loads + BCs + Jacobi-PCG "
-                               "(rtol 1e-10, its recursive-residual rule), bounded sample extrapolated"},
-            "cpu_baseline": cb, "time_to_solve_s": t,
-            "e2e": {"value": value, "unit": "DOF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+                       "step": (f"one bounded sample of the reference serial core: pattern + assembly + loads + "
+                                f"BCs + {sample_iters} Jacobi-PCG iterations (ms_per_step is that sample's wall "
+                                f"time); value = DOFs / (setup + per-iteration time x the "
+                                f"{rec['meta']['iters']} iterations of its own full run)")},
+            "cpu_baseline": cb, "time_to_solve_s": cb["time_to_solve_s"],
+            "e2e": {"value": cb["value"], "unit": "DOF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
 
 
-# ---- our arm --------------------------------------------------------------------------------------
+# ---- the batched solve (64 uneven plates x 4 load cases) -------------------------------------------
 
-def run_batch(a, pkg):
-    """64 seeded plates (n_r 20..200, n_theta = 2 n_r) x 4 load cases: one batched persistent
-    launch (autotuned shape) against the same 256 systems solved one at a time."""
+def run_batch(a, pkg, sweep_shapes: bool = False, reps: int = 3):
+    """64 seeded plates (n_r 20..200, n_theta = 2 n_r, a, E, nu, plane condition random) x 4 load
+    cases in one persistent, graph-captured launch with the autotuned shape, against the same 256
+    systems solved one at a time by the single-system mixed-precision solve."""
     import torch
     specs = pkg.plate.random_batch(count=64, seed=2026)
     t0 = time.perf_counter()
@@ -316,22 +356,20 @@ def run_batch(a, pkg):
     solver = pkg.BatchSolver(pkg.SolverOptions(precision="mixed", max_iter=200000))
     solver.setup(batch, device_rhs=True)
     t_setup = time.perf_counter() - t0
-    print(f"batch setup {t_setup:.2f} s, {batch.mesh.num_dofs} DOFs", file=sys.stderr, flush=True)
     shapes = {}
-    for c in (1, 2, 4, 8, 16):
-        for t in (256, 512):
-            try:
-                shapes[f"{c}x{t}"] = solver.solve(config=(c, t), device=True).seconds
-            except pkg.CstgError as e:
-                shapes[f"{c}x{t}"] = str(e)
-            print(f"shape {c}x{t}: {shapes[f'{c}x{t}']}", file=sys.stderr, flush=True)
+    if sweep_shapes:
+        for c in (1, 2, 4, 8, 16):
+            for t in (256, 512):
+                try:
+                    shapes[f"{c}x{t}"] = solver.solve(config=(c, t), device=True).seconds
+                except pkg.CstgError as e:
+                    shapes[f"{c}x{t}"] = str(e)
     t0 = time.perf_counter()
     cfg, t_tune = solver.autotune(max_iter=300)
-    print(f"autotune {cfg} in {time.perf_counter() - t0:.2f} s", file=sys.stderr, flush=True)
-    times = [solver.solve(device=True).seconds for _ in range(a.reps)]
+    tune_s = time.perf_counter() - t0
+    times = [solver.solve(device=True).seconds for _ in range(reps)]
     sol = solver.solve(device=True)
     dofs = int(batch.mesh.num_dofs)
-    # the same systems one at a time through the single-system persistent solve
     one, its_one = 0.0, 0
     ctx = pkg.Context(0)
     opts = pkg.SolverOptions(rtol=1e-10, max_iter=200000, precision="mixed", true_residual_stop=True)
@@ -341,8 +379,7 @@ def run_batch(a, pkg):
         pkg.assemble_stiffness(m, batch.D[s], 1.0, K)
         sl = batch.dof_range(s)
         bs = torch.from_numpy(np.ascontiguousarray(solver.b[:, sl])).to(0)
-        pkg.apply_dirichlet(pkg.plate.symmetry_dirichlet(m), K,
-                            torch.zeros(m.num_dofs, dtype=torch.float64, device=0))
+        pkg.apply_dirichlet(pkg.plate.symmetry_dirichlet(m), K, torch.zeros(m.num_dofs, dtype=torch.float64, device=0))
         cg = pkg.CgJacobiSolver(opts)
         cg.setup(K)
         x = torch.zeros(m.num_dofs, dtype=torch.float64, device=0)
@@ -351,19 +388,23 @@ def run_batch(a, pkg):
             one += st.solve_seconds
             its_one += st.iterations
     ctx.close()
-    out = {"mode": "batch", "workload": "64 plates (n_r 20..200, seed 2026) x 4 load cases",
+    med = statistics.median(times)
+    out = {"workload": "64 plates (n_r 20..200, n_theta = 2 n_r, seed 2026) x 4 load cases (tension x, tension y, "
+                       "shear, biaxial), mixed precision, rtol 1e-10 on each FP64 true residual",
            "systems": batch.n_plates * batch.n_cases, "dofs_total": dofs, "dof_cases": dofs * batch.n_cases,
-           "setup_s": t_setup, "shapes_s": shapes, "autotuned": list(cfg), "tune_best_s": t_tune,
-           "batch_solve_s": statistics.median(times), "batch_solve_all_s": times,
+           "setup_s": t_setup, "autotuned": {"cluster_ctas": cfg[0], "threads": cfg[1]}, "autotune_s": tune_s,
+           "batch_solve_s": med, "batch_solve_all_s": times,
            "converged": int(np.sum(sol.converged)), "max_true_rel": float(sol.true_rel_residual.max()),
            "iterations_total": int(sol.iterations.sum()), "iterations_max": int(sol.iterations.max()),
-           "fp64_switched_plates": int(np.sum(sol.fp64[:, 0])),
-           "refinements_total": int(sol.refinements.sum()),
            "one_by_one_solve_s": one, "one_by_one_iterations": its_one,
-           "dof_cases_per_s": dofs * batch.n_cases / statistics.median(times)}
+           "speedup_vs_one_by_one": one / med, "dof_cases_per_s": dofs * batch.n_cases / med}
+    if shapes:
+        out["shapes_s"] = shapes
     solver.close()
     return out
 
+
+# ---- our arm --------------------------------------------------------------------------------------
 
 def run_ours(a, dist: Dist):
     import torch
@@ -374,45 +415,43 @@ def run_ours(a, dist: Dist):
     L = pkg.native.load(build_if_missing=False)
     mesh, D, dofs, vals = make_inputs(pkg, a.workload)
     n_r, n_t, desc = WORKLOADS[a.workload]
-    n = mesh.num_dofs
+    n, N = mesh.num_dofs, mesh.num_nodes
+    rec = reference_record(a.workload)
+    precond = PRECONDS[a.precond]
+    learned_any = precond in ("learned", "learned_mg")
 
     stream = torch.cuda.Stream(device=dev)
     ctx = pkg.Context(dev)
     ctx.set_stream(stream)
-    smoother_code = {"chebyshev": pkg.native.AMG_CHEBYSHEV, "jacobi": pkg.native.AMG_JACOBI}[a.amg_smoother]
-    ctx.check(ctx.L.cstg_amg_set_smoother(ctx.h, smoother_code))
-    ctx.check(ctx.L.cstg_amg_set_strength(ctx.h, *a.amg_theta))
-    # loads on the host (bc.cpp:190-253) once; the step starts from them
-    ctx.set_mesh(mesh)
-    b0 = np.zeros(n)
-    pkg.add_traction(ctx, mesh.boundary_edges["right"], 1.0, 1.0, 0.0, b0)
-
-    # device-resident inputs
+    # device-resident inputs: mesh, the loaded edges, the prescribed DOFs
     d_xy = torch.from_numpy(mesh.xy).to(dev)
     d_tri = torch.from_numpy(mesh.triangles).to(dev)
+    d_right = torch.from_numpy(np.ascontiguousarray(mesh.boundary_edges["right"].reshape(-1))).to(dev)
     d_dofs = torch.from_numpy(dofs).to(dev)
     d_vals = torch.from_numpy(vals).to(dev)
-    d_b0 = torch.from_numpy(b0).to(dev)
-    d_b = torch.empty_like(d_b0)
-    d_x = torch.empty_like(d_b0)
-    dmesh = pkg.plate.Mesh(xy=d_xy, triangles=d_tri, boundary_edges=mesh.boundary_edges)
+    d_b = torch.zeros(n, dtype=torch.float64, device=dev)
+    d_x = torch.zeros_like(d_b)
+    dmesh = pkg.plate.Mesh(xy=d_xy, triangles=d_tri, boundary_edges={"right": d_right})
     torch.cuda.synchronize()
     opts = pkg.SolverOptions(rtol=1e-10, max_iter=a.max_iter, precision=a.precision, true_residual_stop=True,
-                             preconditioner=a.precond)
+                             preconditioner=precond)
+    w_cycle = pkg.learned.load_weights(mode="cycle")
+    w_local = pkg.learned.load_weights(mode="local")
+    weights = w_cycle if precond == "learned_mg" else w_local
+    mat = pkg.learned.node_material(D, N)
     last = {}
-    l_weights = pkg.learned.load_weights()
-    l_mat = pkg.learned.node_material(D, mesh.num_nodes)
 
     def step():
         with torch.cuda.stream(stream):
             K = pkg.build_stiffness_pattern(dmesh, ctx=ctx)
             pkg.assemble_stiffness(dmesh, D, 1.0, K)
-            d_b.copy_(d_b0)
+            d_b.zero_()
+            pkg.add_traction(K, d_right, 1.0, 1.0, 0.0, d_b)  # loads on the GPU (bc.cpp:190-253)
             pkg.apply_dirichlet((d_dofs, d_vals), K, d_b)
             s = pkg.CgJacobiSolver(opts)
             s.setup(K)
-            if a.precond == "learned":
-                pkg.learned.setup(K, l_weights, l_mat)
+            if learned_any:
+                pkg.learned.setup(K, weights, mat)
             last["st"] = s.solve(d_b, d_x)
             last["K"] = K
 
@@ -429,80 +468,11 @@ def run_ours(a, dist: Dist):
 
     sync = torch.cuda.synchronize
     if a.only:
-        out = {"mode": a.only, "workload": a.workload}
-        if a.only == "batch":
-            out = run_batch(a, pkg)
-        elif a.only == "batchsolve":
-            specs = pkg.plate.random_batch(count=a.batch_plates, seed=2026, n_r_range=(20, a.batch_nr_max))
-            solver = pkg.BatchSolver(pkg.SolverOptions(precision="mixed", max_iter=200000))
-            solver.setup(pkg.build_batch(specs), device_rhs=True)
-            sol = solver.solve(config=(8, 512), device=True)
-            out.update(plates=a.batch_plates, seconds=sol.seconds, converged=int(sol.converged.sum()),
-                       iterations_max=int(sol.iterations.max()))
-            solver.close()
-        elif a.only == "amg":
-            with torch.cuda.stream(stream):
-                K = pkg.build_stiffness_pattern(dmesh, ctx=ctx)
-                pkg.assemble_stiffness(dmesh, D, 1.0, K)
-                d_b.copy_(d_b0)
-                pkg.apply_dirichlet((d_dofs, d_vals), K, d_b)
-                pkg.CgJacobiSolver().setup(K)
-                info = pkg.amg_setup(K)
-                z = torch.empty_like(d_b)
-                pkg.amg_apply(K, d_b, z)
-                e0 = ev_start()
-                for _ in range(a.reps):
-                    pkg.amg_apply(K, d_b, z)
-                out.update(vcycle_us=ev_stop(e0) / a.reps * 1e6, levels=info["levels"], dofs=info["dofs"],
-                           nnz=info["nnz"], setup_s=info["setup_seconds"])
-                tm = pkg.amg_time(K, reps=max(a.reps, 3))
-                pkg.amg_set_tail(K, False)
-                tm2 = pkg.amg_time(K, reps=max(a.reps, 3))
-                pkg.amg_set_tail(K, True)
-                info2 = pkg.amg_setup(K)  # a rebuild on the same context (buffers reused)
-                out.update(fine_sweep_us=tm["sweep_s"] * 1e6, vcycle_timed_us=tm["vcycle_s"] * 1e6,
-                           vcycle_level_by_level_us=tm2["vcycle_s"] * 1e6, tail_level=info["tail_level"],
-                           tail_cluster=info["tail_cluster"], rebuild_s=info2["setup_seconds"])
-        elif a.only == "learned":
-            with torch.cuda.stream(stream):
-                K = pkg.build_stiffness_pattern(dmesh, ctx=ctx)
-                pkg.assemble_stiffness(dmesh, D, 1.0, K)
-                d_b.copy_(d_b0)
-                pkg.apply_dirichlet((d_dofs, d_vals), K, d_b)
-                pkg.CgJacobiSolver().setup(K)
-                pkg.learned.setup(K, pkg.learned.load_weights(), pkg.learned.node_material(D, mesh.num_nodes))
-                z = torch.empty_like(d_b)
-                pkg.learned.apply(K, d_b, z)
-                e0 = ev_start()
-                for _ in range(a.reps):
-                    pkg.learned.apply(K, d_b, z)
-                out["apply_us"] = ev_stop(e0) / a.reps * 1e6
-        elif a.only == "solve":
-            step()
-            sync()
-            out.update(iterations=last["st"].iterations, solve_s=last["st"].solve_seconds)
-        else:  # the assembled, eliminated matrix and `reps` plain SpMV launches, nothing else
-            with torch.cuda.stream(stream):
-                K = pkg.build_stiffness_pattern(dmesh, ctx=ctx)
-                pkg.assemble_stiffness(dmesh, D, 1.0, K)
-                d_b.copy_(d_b0)
-                pkg.apply_dirichlet((d_dofs, d_vals), K, d_b)
-                xs = torch.randn(n, dtype=torch.float64, device=dev)
-                ys = torch.empty_like(xs)
-                e0 = ev_start()
-                if a.precision == "mixed":
-                    pkg.CgJacobiSolver().setup(K)
-                    K.multiply_mixed(xs, ys)  # builds the FP32 operator (untimed)
-                    e0 = ev_start()
-                    for _ in range(a.reps):
-                        K.multiply_mixed(xs, ys)
-                else:
-                    for _ in range(a.reps):
-                        K.multiply(xs, ys)
-                out["spmv_us"] = ev_stop(e0) / a.reps * 1e6
+        out = run_only(a, pkg, step, last, ctx, stream, ev_start, ev_stop, d_b, D, N, n, w_cycle)
         print(json.dumps(out))
         ctx.close()
         return 0
+
     clocks = ClockSampler(dev)
     for _ in range(a.warmup):
         step()
@@ -519,213 +489,254 @@ def run_ours(a, dist: Dist):
                            f"true {st.true_rel_residual:.3e}")
     t_step = el_max / a.steps
     value = a.gpus * n / t_step
-
-    # comparison solves on the same matrix (not in `value`):
-    #   ref_rule      FP64 Jacobi-PCG under the reference's own stopping rule (recursive residual,
-    #                 solver.cpp:80-82): its iteration count scales the CPU baseline
-    #   plain_fp64    FP64 Jacobi-PCG to the FP64 true residual: the plain GPU Jacobi-PCG
-    #   jacobi_mixed  Jacobi-PCG with the FP32 SpMV and preconditioner, FP64 scalars and
-    #                 true-residual refinement (the persistent kernel)
-    #   learned_mixed the learned preconditioner (packaged weights) in flexible CG, mixed SpMV
     K = last["K"]
+    x_head = d_x.cpu().numpy()
+    line = {
+        "metric": METRIC, "value": value, "unit": "DOF/s", "n_gpus": a.gpus, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": ("f32 (SpMV, cycle operators) + f64 (vectors, scalars, reliable updates) + bf16 (network)"
+                  if learned_any and a.precision == "mixed" else
+                  "f32 (SpMV) + f64" if a.precision == "mixed" else "f64"),
+        "data": "synthetic",
+        "config": {"workload": f"{a.workload}: {desc}, {n} DOFs, {K.nnz()} nnz, E=1 nu=0.3 plane stress t=1, "
+                               "traction (1,0) on x=10, u_x=0 on x=0, u_y=0 on y=0",
+                   "step": (f"pattern + assembly + traction loads (GPU) + Dirichlet + Jacobi setup + {a.precond} "
+                            "preconditioner setup + flexible CG to rtol 1e-10 on the FP64 true residual"),
+                   "preconditioner": a.precond, "precision": a.precision, "dofs": n, "nnz": K.nnz(),
+                   "l2": f"inputs larger than L2 (FP64 matrix values {K.nnz() * 8 / 1e6:.0f} MB)",
+                   "parallelism": f"replicas x{a.gpus}"},
+        "time_to_solve_s": t_step, "iterations": st.iterations, "refinements": st.refinements,
+        "true_rel_residual": st.true_rel_residual, "solve_s": st.solve_seconds, "message": st.message,
+        "x_rel_vs_reference_u": rel_error_vs_reference(rec, x_head),
+        "gpu_launches": int(launches),
+        "clocks": clk,
+    }
+    if rec is not None:
+        line["reference_run"] = {"iterations": rec["meta"]["iters"], "true_rel_residual": rec["meta"]["true_rel"],
+                                 "scf": rec["meta"]["scf"], "file": rec["file"],
+                                 "u_compared": "every 8th node" if rec["idx"] is not None else "all DOFs"}
+    strs = pkg.compute_element_stresses(ctx, x_head, 1.0, 0.3)
+    scf, scf_elem = pkg.scf_at_hole(strs, 1.0)
+    line["scf"] = {"value": scf, "element": scf_elem, "analytic_infinite_plate": 3.0,
+                   "reference": rec["meta"]["scf"] if rec else None}
 
-    def solve_with(x_out=None, **kw):
-        s_ = pkg.CgJacobiSolver(pkg.SolverOptions(rtol=1e-10, max_iter=400000, **kw))
-        s_.setup(K)
-        return s_, s_.solve(d_b, torch.empty_like(d_x) if x_out is None else x_out)
+    if not a.no_compare:
+        line.update(compare_solves(a, pkg, K, d_b, d_x, stream, rec, st, t_step, mat, w_cycle))
+    line.update(rooflines(a, pkg, K, ctx, stream, ev_start, ev_stop, N, n, mat, weights, precond))
+    if not a.no_e2e:
+        line["e2e"] = run_e2e(a, pkg, dist, dev, mesh, D, dofs, vals, opts, weights, mat, learned_any, sync)
+    if dist.rank == 0 and not a.no_cpu_baseline and a.gpus == 1 and rec is not None and "cpu_run" in rec["meta"]:
+        s = cpu_sample(mesh, dofs, vals, a.cpu_sample_iters)
+        line["cpu_baseline"] = cpu_baseline_entry(s, n, rec)
+    if dist.rank == 0 and not a.no_batch and a.gpus == 1:
+        line["batch"] = run_batch(a, pkg)
+    ctx.close()
+    if dist.rank == 0:
+        print(json.dumps(line))
+    dist.close()
+    return 0
 
-    x_ref = torch.empty_like(d_x)
-    with torch.cuda.stream(stream):
-        s_ref, st_ref = solve_with(x_ref)
-        _, st_64 = solve_with(true_residual_stop=True)
-        _, st_jm = solve_with(precision="mixed", true_residual_stop=True)
-    sync()
 
-    learned = None
-    if not a.no_learned:
+def compare_solves(a, pkg, K, d_b, d_x, stream, rec, st_head, t_step, mat, w_cycle):
+    """The comparison solves on the step's matrix (not in `value`), each with its error against the
+    reference's displacements:
+      reference_rule  FP64 Jacobi-PCG under the reference's own stopping rule (recursive residual,
+                      solver.cpp:80-82): iterations against the reference's full run
+      plain_fp64      FP64 Jacobi-PCG to the FP64 true residual: the plain GPU Jacobi-PCG
+      jacobi_mixed    Jacobi-PCG with FP32 SpMV, FP64 vectors/scalars and reliable updates
+      amg_mixed       the Chebyshev multigrid cycle (no network), flexible CG, mixed
+      learned_zero    the learned cycle with the network at zero (its post-smoother is one damped
+                      Jacobi step): the method without the trained network"""
+    import torch
+    out = {}
+
+    def solve_with(name, setup=None, **kw):
+        x = torch.zeros_like(d_x)
         with torch.cuda.stream(stream):
-            s_l = pkg.CgJacobiSolver(pkg.SolverOptions(rtol=1e-10, max_iter=200000, precision="mixed",
-                                                       preconditioner="learned", true_residual_stop=True))
-            s_l.setup(K)
+            s_ = pkg.CgJacobiSolver(pkg.SolverOptions(rtol=1e-10, max_iter=400000, **kw))
+            s_.setup(K)
+            if setup:
+                setup()
+            if kw.get("preconditioner", "jacobi") != "jacobi":
+                s_.solve(d_b, x)  # warm-up: hierarchy, graph capture
             t0 = time.perf_counter()
-            pkg.learned.setup(K, l_weights, l_mat)
-            t_setup = time.perf_counter() - t0
-            s_l.solve(d_b, torch.empty_like(d_x))  # warm-up (graph capture)
-            st_l = s_l.solve(d_b, torch.empty_like(d_x))
-        sync()
-        learned = {"solve_s": st_l.solve_seconds, "setup_s": t_setup, "iterations": st_l.iterations,
-                   "true_rel_residual": st_l.true_rel_residual, "converged": st_l.converged,
-                   "speedup_vs_plain_fp64": st_64.solve_seconds / st_l.solve_seconds,
-                   "message": st_l.message}
+            st = s_.solve(d_b, x)
+            wall = time.perf_counter() - t0
+        torch.cuda.synchronize()
+        xh = x.cpu().numpy()
+        out[name] = {"solve_s": st.solve_seconds, "wall_s": wall, "iterations": st.iterations,
+                     "refinements": st.refinements, "true_rel_residual": st.true_rel_residual,
+                     "converged": st.converged, "x_rel_vs_reference_u": rel_error_vs_reference(rec, xh)}
+        return st
 
-    # dominant kernels timed alone (CUDA events, back-to-back launches)
-    N = mesh.num_nodes
-    nnz = K.nnz()
-    nb = nnz // 4
-    noff = nb - N
-    reps = 100
+    st_ref = solve_with("reference_rule")
+    if rec is not None:
+        out["reference_rule"]["iterations_reference_run"] = rec["meta"]["iters"]
+    st_64 = solve_with("plain_fp64", true_residual_stop=True)
+    solve_with("jacobi_mixed", precision="mixed", true_residual_stop=True)
+    solve_with("amg_mixed", precision="mixed", preconditioner="amg", true_residual_stop=True)
+    zero = np.zeros_like(w_cycle)
+    st_z = solve_with("learned_zero", setup=lambda: pkg.learned.setup(K, zero, mat), precision="mixed",
+                      preconditioner="learned_mg", true_residual_stop=True)
+    st_64s = st_64.solve_seconds
+    out["speedup"] = {
+        "headline_step_vs_plain_fp64_solve": st_64s / t_step,
+        "headline_solve_vs_plain_fp64_solve": st_64s / st_head.solve_seconds,
+        "iterations_plain_fp64": st_64.iterations, "iterations_headline": st_head.iterations,
+        "iteration_ratio": st_64.iterations / max(st_head.iterations, 1),
+        "time_per_iteration_ratio": (st_head.solve_seconds / max(st_head.iterations, 1)) /
+                                    (st_64s / max(st_64.iterations, 1)),
+        "network_vs_zero_network_iterations": (st_head.iterations, st_z.iterations),
+        "note": "speedup = iteration_ratio / time_per_iteration_ratio (solve); the step adds pattern, assembly, "
+                "loads, Dirichlet and every setup"}
+    return out
 
-    def time_launches(fn):
-        with torch.cuda.stream(stream):
-            for _ in range(20):
-                fn()
-            e0 = ev_start()
-            for _ in range(reps):
-                fn()
-            return ev_stop(e0) / reps
 
+def rooflines(a, pkg, K, ctx, stream, ev_start, ev_stop, N, n, mat, weights, precond):
+    """The dominant kernel of the step (the network's message-passing layer for the learned
+    preconditioners) and the two SpMVs, timed alone with CUDA events on the context's stream."""
+    import torch
     peak, peak_kind = measured_peaks()
     peak_note = f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs, burst copy)"
     full = a.workload == "plate2m"
+    nnz = K.nnz()
+    nb = nnz // 4
+    noff = nb - N
 
     def roof(kernel, nbytes, seconds, traffic=None, **extra):
         return {"bound": "hbm", "kernel": kernel, "achieved": nbytes / seconds / 1e9, "peak": peak, "unit": "GB/s",
                 "frac": nbytes / seconds / 1e9 / peak, "peak_kind": peak_note, "traffic": traffic,
                 "algorithmic_bytes": nbytes, "launch_us": seconds * 1e6, **extra}
 
-    xs = torch.randn(n, dtype=torch.float64, device=dev)
+    def time_launches(fn, reps=100):
+        with torch.cuda.stream(stream):
+            for _ in range(10):
+                fn()
+            e0 = ev_start()
+            for _ in range(reps):
+                fn()
+            return ev_stop(e0) / reps
+
+    xs = torch.randn(n, dtype=torch.float64, device=K.ctx.device)
     ys = torch.empty_like(xs)
-    spmv64_s = time_launches(lambda: K.multiply(xs, ys))
-    spmv64_bytes = nnz * 8 + nb * 4 + (N + 1) * 4 + n * 8 + n * 8
-    roof64 = roof("k_spmv_block (FP64 2x2-block SpMV)", spmv64_bytes, spmv64_s,
-                  profile_traffic("spmv_block_fp64_plate2m.md") if full else None)
     with torch.cuda.stream(stream):
-        s_ref.setup(K)  # the FP32 operator of this matrix
-    spmv32_s = time_launches(lambda: K.multiply_mixed(xs, ys))
+        s0 = pkg.CgJacobiSolver()
+        s0.setup(K)
+    spmv64_bytes = nnz * 8 + nb * 4 + (N + 1) * 4 + n * 8 + n * 8
     spmv32_bytes = noff * (16 + 4) + N * 32 + (N + 1) * 4 + n * 8 + n * 8
-    roof32 = roof("k_spmv_mixed (FP32 difference-form 2x2-block SpMV, FP64 vectors)", spmv32_bytes, spmv32_s,
-                  profile_traffic("spmv_mixed_f32_plate2m.md") if full else None)
+    r64 = roof("k_spmv_block (FP64 2x2-block SpMV)", spmv64_bytes, time_launches(lambda: K.multiply(xs, ys)),
+               profile_traffic("spmv_block_fp64_plate2m.md") if full else None)
+    r32 = roof("k_spmv_mixed (FP32 difference-form 2x2-block SpMV, FP64 vectors)", spmv32_bytes,
+               time_launches(lambda: K.multiply_mixed(xs, ys)),
+               profile_traffic("spmv_mixed_f32_plate2m.md") if full else None)
+    out = {"spmv_fp64": r64, "spmv_mixed": r32}
+    # the network's layer: H in (128 B / node, BF16), H out, node pointers and neighbour indices once
+    with torch.cuda.stream(stream):
+        pkg.learned.setup(K, weights, mat)
+        tm = pkg.learned.time_stages(K, reps=50)
+    layer_bytes = N * 2 * 128 + (N + 1) * 4 + nb * 4
+    last_bytes = N * 128 + (N + 1) * 4 + nb * 4 + n * 8 * 3  # H in; r, D^-1 in, z out
+    enc_bytes = N * (16 + 24 + 128)
+    lay = roof("k_mp_layer_tc (message-passing layer, tcgen05 BF16, layer 2 of 3)", layer_bytes, tm["layer_s"][1],
+               profile_traffic("mp_layer_tc_plate2m.md") if full else None,
+               layers_us=[t * 1e6 for t in tm["layer_s"]], encoder_us=tm["encoder_s"] * 1e6,
+               last_layer_gbs=last_bytes / tm["layer_s"][2] / 1e9, encoder_gbs=enc_bytes / tm["encoder_s"] / 1e9,
+               network_apply_us=(tm["encoder_s"] + sum(tm["layer_s"])) * 1e6)
+    out["network"] = lay
+    if precond in ("learned", "learned_mg"):
+        out["roofline"] = lay
+    elif precond == "amg":
+        with torch.cuda.stream(stream):
+            tma = pkg.amg_time(K, reps=50)
+        out["roofline"] = roof("k_amg_sweep_f32 (finest-level smoothing step)", spmv32_bytes + 2 * n * 8,
+                               tma["sweep_s"], profile_traffic("amg_sweep_f32_plate2m.md") if full else None)
+    else:
+        out["roofline"] = r32 if a.precision == "mixed" else r64
+    return out
 
-    # The persistent Jacobi-PCG kernel (one cooperative launch runs every iteration): algorithmic
-    # bytes per launch = the 3-pass iteration model (SpMV + x/r update + p update) x iterations.
-    def persistent_roof(stx, precision):
-        it_bytes = (spmv32_bytes if precision == "mixed" else spmv64_bytes) + n * (5 * 8 + 2 * 8) + n * (2 * 8 + 2 * 8)
-        per_it = profile_traffic(f"pcg_persistent_{precision}_plate2m.md",
-                                 "dram_bytes_per_iteration_full_size") if full else None
-        return roof(f"k_pcg_persistent<{precision}> (whole PCG solve, one launch)", it_bytes * stx.iterations,
-                    stx.solve_seconds, per_it * stx.iterations if per_it else None, bytes_per_iteration=it_bytes,
-                    iteration_gbs=it_bytes * stx.iterations / stx.solve_seconds / 1e9)
 
-    jacobi_mixed = {"solve_s": st_jm.solve_seconds, "iterations": st_jm.iterations,
-                    "refinements": st_jm.refinements, "true_rel_residual": st_jm.true_rel_residual,
-                    "speedup_vs_plain_fp64": st_64.solve_seconds / st_jm.solve_seconds,
-                    "roofline": persistent_roof(st_jm, "mixed")}
+def run_e2e(a, pkg, dist, dev, mesh, D, dofs, vals, opts, weights, mat, learned_any, sync):
+    """The step through the C ABI with pinned host buffers: mesh, loaded edges and BCs up, the
+    traction loads and the elimination through the host-pointer calls, displacements down."""
+    import torch
 
-    # the multigrid hierarchy of this matrix, its cycle and its finest-level smoother sweep
-    # (FP32 difference-form operator + FP64 b, D^-1, x in, x out per launch)
-    amg = None
-    if a.precond == "amg":
+    def pinned(arr):
+        t = torch.empty(arr.shape, dtype={np.float64: torch.float64, np.int32: torch.int32}[arr.dtype.type],
+                        pin_memory=True)
+        v = t.numpy()
+        v[...] = arr
+        return v
+    hmesh = pkg.plate.Mesh(xy=pinned(mesh.xy), triangles=pinned(mesh.triangles),
+                           boundary_edges={"right": pinned(np.ascontiguousarray(mesh.boundary_edges["right"]))})
+    h_dofs, h_vals = pinned(dofs), pinned(vals)
+    h_b = pinned(np.zeros(mesh.num_dofs))
+    h_x = pinned(np.zeros(mesh.num_dofs))
+    ectx = pkg.Context(dev)
+    last = {}
+
+    def e2e_step():
+        K2 = pkg.build_stiffness_pattern(hmesh, ctx=ectx)
+        pkg.assemble_stiffness(hmesh, D, 1.0, K2)
+        h_b.fill(0.0)
+        pkg.add_traction(K2, hmesh.boundary_edges["right"], 1.0, 1.0, 0.0, h_b)
+        pkg.apply_dirichlet((h_dofs, h_vals), K2, h_b)
+        s2 = pkg.CgJacobiSolver(opts)
+        s2.setup(K2)
+        if learned_any:
+            pkg.learned.setup(K2, weights, mat)
+        last["st"] = s2.solve(h_b, h_x)
+
+    def wall_start():
+        return time.perf_counter()
+
+    def wall_stop(t0):
+        return time.perf_counter() - t0
+
+    el2 = timed_region(e2e_step, a.steps, a.warmup, dist, wall_start, wall_stop, sync)
+    el2 = dist.max(el2, device=f"cuda:{dev}")
+    h2d = mesh.xy.nbytes + mesh.triangles.nbytes + mesh.boundary_edges["right"].nbytes + dofs.nbytes + vals.nbytes \
+        + h_b.nbytes + mat.nbytes
+    d2h = h_b.nbytes + h_x.nbytes
+    ectx.close()
+    return {"value": a.gpus * mesh.num_dofs / (el2 / a.steps), "unit": "DOF/s", "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(d2h), "ms_per_step": el2 / a.steps * 1e3,
+            "converged": bool(last["st"].converged),
+            "path": "C ABI, host pinned buffers (cstg_set_mesh .. cstg_pcg_solve)"}
+
+
+def run_only(a, pkg, step, last, ctx, stream, ev_start, ev_stop, d_b, D, N, n, w_cycle):
+    import torch
+    out = {"mode": a.only, "workload": a.workload}
+    if a.only == "batch":
+        out.update(run_batch(a, pkg, sweep_shapes=True, reps=a.reps))
+        return out
+    step()
+    torch.cuda.synchronize()
+    K = last["K"]
+    if a.only == "solve":
+        out.update(iterations=last["st"].iterations, solve_s=last["st"].solve_seconds, message=last["st"].message)
+    elif a.only == "learned":
+        with torch.cuda.stream(stream):
+            pkg.learned.setup(K, w_cycle, pkg.learned.node_material(D, N))
+            out.update(pkg.learned.time_stages(K, reps=a.reps))
+    elif a.only == "amg":
         with torch.cuda.stream(stream):
             info = pkg.amg_setup(K)
-            tm = pkg.amg_time(K, reps=50)
-        sync()
-        sweep_bytes = spmv32_bytes + 2 * n * 8
-        amg = {"levels": info["levels"], "level_dofs": info["dofs"], "level_nnz": info["nnz"],
-               "setup_s": info["setup_seconds"], "vcycle_us": tm["vcycle_s"] * 1e6,
-               "cycle": f"V(2,2), {a.amg_smoother} smoothing, FP32 cycle operators, dense coarsest inverse",
-               "strength_theta": {"fine": a.amg_theta[0], "coarse": a.amg_theta[1]},
-               "tail": {"level": info["tail_level"], "cluster_ctas": info["tail_cluster"]},
-               "smoother_roofline": roof("k_amg_sweep_f32 (finest-level smoothing step)", sweep_bytes,
-                                         tm["sweep_s"],
-                                         profile_traffic("amg_sweep_f32_plate2m.md") if full else None)}
-        roofline = amg["smoother_roofline"]
-    elif a.precond == "jacobi":
-        roofline = persistent_roof(st, a.precision)
-    else:
-        roofline = roof32
-
-    # accuracy of the headline solution against FP64 Jacobi-PCG under the reference's rule, and
-    # the stress concentration factor at the hole (element stresses on the GPU)
-    sync()
-    x_rel = float(torch.linalg.vector_norm(d_x - x_ref) / torch.linalg.vector_norm(x_ref))
-    strs = pkg.compute_element_stresses(ctx, d_x.cpu().numpy(), 1.0, 0.3)
-    scf, scf_elem = pkg.scf_at_hole(strs, 1.0)
-
-    dtype = {"amg": "f64 (CG) + f32 (cycle matrix values)", "jacobi": "f64", "learned": "f32+f64+bf16"}
-    line = {
-        "metric": METRIC, "value": value, "unit": "DOF/s", "n_gpus": a.gpus, "steps": a.steps,
-        "warmup": a.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None,
-        "dtype": dtype[a.precond] if a.precision == "fp64" else "f32+f64",
-        "data": "synthetic",
-        "config": {"workload": f"{a.workload}: {desc}, {n} DOFs, {nnz} nnz, E=1 nu=0.3 plane stress t=1, "
-                               "traction (1,0) on x=10, u_x=0 on x=0, u_y=0 on y=0",
-                   "step": f"pattern + assembly + Dirichlet + {a.precond} preconditioner setup + PCG to "
-                           "rtol 1e-10 on the FP64 true residual",
-                   "preconditioner": a.precond, "precision": a.precision, "dofs": n, "nnz": nnz,
-                   "l2": f"inputs larger than L2 (FP64 matrix values {nnz * 8 / 1e6:.0f} MB)",
-                   "parallelism": f"replicas x{a.gpus}"},
-        "time_to_solve_s": t_step, "iterations": st.iterations, "refinements": st.refinements,
-        "true_rel_residual": st.true_rel_residual, "solve_s": st.solve_seconds,
-        "plain_fp64": {"solve_s": st_64.solve_seconds, "iterations": st_64.iterations,
-                       "true_rel_residual": st_64.true_rel_residual,
-                       "speedup_of_headline_solve": st_64.solve_seconds / st.solve_seconds,
-                       "speedup_of_headline_step": st_64.solve_seconds / t_step},
-        "jacobi_mixed": jacobi_mixed,
-        "learned_mixed": learned,
-        "amg": amg,
-        "reference_rule_iterations": st_ref.iterations, "reference_rule_solve_s": st_ref.solve_seconds,
-        "x_rel_vs_reference_rule_fp64": x_rel,
-        "scf": {"value": scf, "element": scf_elem, "analytic_infinite_plate": 3.0},
-        "roofline": roofline,
-        "spmv_fp64": roof64,
-        "spmv_mixed": roof32,
-        "gpu_launches": int(launches),
-        "clocks": clk,
-    }
-
-    # e2e: through the C ABI with pinned host buffers
-    if not a.no_e2e:
-        def pinned(arr):
-            t = torch.empty(arr.shape, dtype={np.float64: torch.float64, np.int32: torch.int32}[arr.dtype.type],
-                            pin_memory=True)
-            v = t.numpy()
-            v[...] = arr
-            return v
-        hmesh = pkg.plate.Mesh(xy=pinned(mesh.xy), triangles=pinned(mesh.triangles),
-                               boundary_edges=mesh.boundary_edges)
-        h_dofs, h_vals, h_b0 = pinned(dofs), pinned(vals), pinned(b0)
-        h_b = pinned(b0)
-        h_x = pinned(np.zeros(n))
-        ectx = pkg.Context(dev)
-        ectx.check(ectx.L.cstg_amg_set_smoother(ectx.h, smoother_code))
-        ectx.check(ectx.L.cstg_amg_set_strength(ectx.h, *a.amg_theta))
-
-        def e2e_step():
-            K2 = pkg.build_stiffness_pattern(hmesh, ctx=ectx)
-            pkg.assemble_stiffness(hmesh, D, 1.0, K2)
-            np.copyto(h_b, h_b0)
-            pkg.apply_dirichlet((h_dofs, h_vals), K2, h_b)
-            s2 = pkg.CgJacobiSolver(opts)
-            s2.setup(K2)
-            if a.precond == "learned":
-                pkg.learned.setup(K2, l_weights, l_mat)
-            last["e2e"] = s2.solve(h_b, h_x)
-
-        def wall_start():
-            return time.perf_counter()
-
-        def wall_stop(t0):
-            return time.perf_counter() - t0
-
-        el2 = timed_region(e2e_step, a.steps, a.warmup, dist, wall_start, wall_stop, sync)
-        el2 = dist.max(el2, device=f"cuda:{dev}")
-        h2d = mesh.xy.nbytes + mesh.triangles.nbytes + dofs.nbytes + vals.nbytes + 2 * b0.nbytes
-        d2h = b0.nbytes + h_x.nbytes
-        line["e2e"] = {"value": a.gpus * n / (el2 / a.steps), "unit": "DOF/s", "h2d_bytes_per_step": int(h2d),
-                       "d2h_bytes_per_step": int(d2h), "ms_per_step": el2 / a.steps * 1e3,
-                       "path": "C ABI, host pinned buffers (cstg_set_mesh .. cstg_pcg_solve)"}
-        ectx.close()
-
-    if dist.rank == 0 and not a.no_cpu_baseline and a.gpus == 1:
-        iters_full = st_ref.iterations
-        s = cpu_sample(mesh, dofs, vals, a.cpu_sample_iters)
-        line["cpu_baseline"] = cpu_baseline_entry(s, n, iters_full, a.cpu_sample_iters)
-    ctx.close()
-    if dist.rank == 0:
-        print(json.dumps(line))
-    dist.close()
-    return 0
+            tm = pkg.amg_time(K, reps=max(a.reps, 3))
+        out.update(levels=info["levels"], dofs=info["dofs"], setup_s=info["setup_seconds"],
+                   fine_sweep_us=tm["sweep_s"] * 1e6, vcycle_us=tm["vcycle_s"] * 1e6)
+    else:  # `reps` SpMV launches of the precision asked for on the assembled, eliminated matrix
+        with torch.cuda.stream(stream):
+            xs = torch.randn(n, dtype=torch.float64, device=K.ctx.device)
+            ys = torch.empty_like(xs)
+            mul = K.multiply_mixed if a.precision == "mixed" else K.multiply
+            mul(xs, ys)
+            e0 = ev_start()
+            for _ in range(a.reps):
+                mul(xs, ys)
+            out["spmv_us"] = ev_stop(e0) / a.reps * 1e6
+    return out
 
 
 def main():

@@ -338,6 +338,10 @@ int cstg_learned_setup(cstg_ctx* ctx, const float* params, const float* node_mat
 int cstg_learned_set_params(cstg_ctx* ctx, const float* params);
 /* z = M(r) on device vectors (2 x node count doubles each). */
 int cstg_learned_apply_device(cstg_ctx* ctx, const double* d_r, double* d_z);
+/* Timing of the network's inference launches on the context's stream (CUDA events, `reps`
+ * back-to-back launches of each after a warm-up): out[0] seconds per encoder launch, out[1 .. 3]
+ * per launch of message-passing layer 1 .. 3 (the third with the decoder). */
+int cstg_learned_time(cstg_ctx* ctx, int reps, double* out);
 
 /* Training on the GPU with the library's forward and backward kernels. A sample is a residual
  * r and the error e = A^-1 r of the context's matrix (device, n_rows doubles each, samples one

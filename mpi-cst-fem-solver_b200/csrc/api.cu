@@ -89,7 +89,7 @@ void cstg_destroy(cstg_ctx* ctx) {
                    &ctx->bat_in,  &ctx->bat_out, &ctx->lp_p32, &ctx->lp_pb,   &ctx->lp_pf,
                    &ctx->lp_sf,   &ctx->lp_h0,  &ctx->lp_h1,    &ctx->lp_sc,    &ctx->lp_z,
                    &ctx->tr_con,  &ctx->tr_cnt, &ctx->tr_ptr,   &ctx->tr_cur,   &ctx->tr_rec,
-                   &ctx->lm_winvd, &ctx->fcg_ring};
+                   &ctx->lm_winvd, &ctx->fcg_ring, &ctx->lp_mat};
   for (DevBuf* b : all) free_buf(*b);
   for (int j = 0; j < kFcgMaxHist; ++j) {
     free_buf(ctx->fcg_ph[j]);

@@ -97,7 +97,7 @@ struct cstg_ctx {
   // learned preconditioner: packed weights (FP32 master, BF16 + FP32 copies), per-node static
   // inputs, inference activations, network scalars, z; the flexible-CG chunk graph
   unsigned long long setup_count = 0;  // bumped by every cstg_pcg_setup
-  DevBuf lp_p32, lp_pb, lp_pf, lp_sf, lp_h0, lp_h1, lp_sc, lp_z;
+  DevBuf lp_p32, lp_pb, lp_pf, lp_sf, lp_h0, lp_h1, lp_sc, lp_z, lp_mat;
   bool learned_ready = false;
   unsigned long long learned_setup = ~0ull;  // setup_count the static inputs were built for
   cudaGraphExec_t fcg_graph = nullptr;

@@ -194,6 +194,7 @@ struct MpnnWork {  // activations (training keeps every layer; inference ping-po
 };
 
 struct MpScratch {  // small device scalars of the network's reductions
+  double dsum;      // sum of the matrix diagonal (the static inputs' scale)
   double rr;        // r'r
   double dots[3];   // z'r, z'Az, e'r
   double loss;
@@ -205,6 +206,10 @@ constexpr long long kMpMbarSpinDefault = 1LL << 22;  // polls of the tensor-core
 cudaError_t mpnn_prepare_device();
 cudaError_t launch_mp_params(const float* p32, __nv_bfloat16* pb, float* pf, cudaStream_t s);
 cudaError_t launch_mp_rr(int n, const double* r, MpScratch* sc, cudaStream_t s, const int* skip = nullptr);
+// The network's static inputs per node (6 floats): diagonal / its mean (2), xy / coord_scale (2),
+// the caller's two material values (mat, 2 floats per node, device).
+cudaError_t launch_mp_static(int N, const double* invd, const double* xy, const float* mat, double coord_scale,
+                             MpScratch* sc, float* sf, cudaStream_t s);
 // out = factor / lambda (lambda: one device double) * invd
 cudaError_t launch_mp_smoother_weights(int n, const double* invd, const double* lam, double factor, double* out,
                                        cudaStream_t s);
@@ -215,6 +220,11 @@ cudaError_t launch_mp_smoother_weights(int n, const double* invd, const double* 
 cudaError_t launch_mp_forward(const MpnnGraph& g, const MpnnParams& P, const double* r, const double* invd,
                               const double* rr, const float* sf, const int* skip, MpnnWork& w, bool train,
                               const double* zbase, double* z, long long spin_limit, int* err, cudaStream_t s);
+// One stage of the inference forward pass alone (timing): 0 the encoder, 1..kMpL the layers (the
+// last with the decoder), on the inference ping-pong buffers of w.
+cudaError_t launch_mp_stage(const MpnnGraph& g, const MpnnParams& P, int stage, const double* r, const double* invd,
+                            const double* rr, const float* sf, MpnnWork& w, double* z, long long spin_limit, int* err,
+                            cudaStream_t s);
 cudaError_t launch_mp_loss(int N, const double* z, const double* az, const double* r, const double* e,
                            const double* invd, MpScratch* sc, MpnnWork& w, cudaStream_t s);
 cudaError_t launch_mp_backward(const MpnnGraph& g, const MpnnParams& P, MpnnWork& w, float* grad, cudaStream_t s);

@@ -438,34 +438,21 @@ int cstg_learned_setup(cstg_ctx* ctx, const float* params, const float* node_mat
   if (ctx->kind != 1 || !ctx->setup_done)
     return fail(ctx, CSTG_ERR_STATE, "learned_setup: needs a mesh-pattern matrix after cstg_pcg_setup");
   CK(mpnn_prepare_device());
-  const int N = ctx->n_nodes, n = ctx->n_rows;
+  const int N = ctx->n_nodes;
   int rc = upload_params(ctx, params);
   if (rc) return rc;
-  // per-node static inputs: diagonal / its mean, coordinates / plate size, material
-  std::vector<double> invd((size_t)n), xy((size_t)n);
-  if (n) {
-    CK(cudaMemcpyAsync(invd.data(), ctx->inv_diag.p, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost,
-                       ctx->stream));
-    CK(cudaMemcpyAsync(xy.data(), ctx->xy.p, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
-  }
-  CK(cudaStreamSynchronize(ctx->stream));
-  double dsum = 0.0;
-  for (int i = 0; i < n; ++i) dsum += 1.0 / invd[i];
-  const double d_mean = n ? dsum / n : 1.0;
-  std::vector<float> sf((size_t)N * 6);
-  for (int k = 0; k < N; ++k) {
-    sf[6 * (size_t)k + 0] = (float)((1.0 / invd[2 * (size_t)k]) / d_mean);
-    sf[6 * (size_t)k + 1] = (float)((1.0 / invd[2 * (size_t)k + 1]) / d_mean);
-    sf[6 * (size_t)k + 2] = (float)(xy[2 * (size_t)k] / kCoordScale);
-    sf[6 * (size_t)k + 3] = (float)(xy[2 * (size_t)k + 1] / kCoordScale);
-    sf[6 * (size_t)k + 4] = node_material[2 * (size_t)k];
-    sf[6 * (size_t)k + 5] = node_material[2 * (size_t)k + 1];
-  }
-  ENSURE(ctx->lp_sf, sizeof(float) * sf.size());
+  // per-node static inputs on the GPU: diagonal / its mean, coordinates / plate size, material
+  ENSURE(ctx->lp_sf, sizeof(float) * (size_t)std::max(N, 1) * 6);
+  ENSURE(ctx->lp_mat, sizeof(float) * (size_t)std::max(N, 1) * 2);
   ENSURE(ctx->lp_sc, sizeof(MpScratch));
   // the reductions' tickets must start at zero (a fresh allocation may hold old contents)
   CK(cudaMemsetAsync(ctx->lp_sc.p, 0, sizeof(MpScratch), ctx->stream));
-  if (N) CK(cudaMemcpyAsync(ctx->lp_sf.p, sf.data(), sizeof(float) * sf.size(), cudaMemcpyHostToDevice, ctx->stream));
+  if (N) {
+    CK(cudaMemcpyAsync(ctx->lp_mat.p, node_material, sizeof(float) * 2 * (size_t)N, cudaMemcpyHostToDevice,
+                       ctx->stream));
+    CK(launch_mp_static(N, buf_ptr<double>(ctx->inv_diag), buf_ptr<double>(ctx->xy), buf_ptr<float>(ctx->lp_mat),
+                        kCoordScale, buf_ptr<MpScratch>(ctx->lp_sc), buf_ptr<float>(ctx->lp_sf), ctx->stream));
+  }
   CK(cudaStreamSynchronize(ctx->stream));
   ctx->learned_ready = true;
   ctx->learned_setup = ctx->setup_count;
@@ -754,3 +741,42 @@ int cstg_trainer_accumulate_cycle(cstg_trainer* tr, cstg_ctx* ctx, int n_samples
 }
 
 }  // extern "C"
+
+extern "C" int cstg_learned_time(cstg_ctx* ctx, int reps, double* out) {
+  BEGIN(ctx);
+  if (reps < 1 || !out) return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "learned_time: bad arguments");
+  if (!ctx->learned_ready || ctx->learned_setup != ctx->setup_count)
+    return fail(ctx, CSTG_ERR_STATE, "learned_time: call cstg_learned_setup after cstg_pcg_setup");
+  const int N = ctx->n_nodes, n = ctx->n_rows;
+  ENSURE(ctx->lp_h0, sizeof(__nv_bfloat16) * (size_t)N * kMpF);
+  ENSURE(ctx->lp_h1, sizeof(__nv_bfloat16) * (size_t)N * kMpF);
+  ENSURE(ctx->lp_z, sizeof(double) * (size_t)std::max(n, 1));
+  ENSURE(ctx->vec_in, sizeof(double) * (size_t)std::max(n, 1));
+  double* r = buf_ptr<double>(ctx->vec_in);
+  double* z = buf_ptr<double>(ctx->lp_z);
+  CK(cudaMemsetAsync(r, 0, sizeof(double) * (size_t)n, ctx->stream));
+  if (n) CK(launch_mp_smoother_weights(n, buf_ptr<double>(ctx->inv_diag), buf_ptr<double>(ctx->inv_diag), 1.0, r,
+                                       ctx->stream));  // r_i = invd_i / invd_0: a nonzero residual
+  MpScratch* sc = buf_ptr<MpScratch>(ctx->lp_sc);
+  MpnnWork mw = infer_work(ctx);
+  CK(launch_mp_rr(n, r, sc, ctx->stream));
+  RESET_ERR();
+  // whole applications, then each stage alone (the same launches launch_mp_forward issues)
+  float ms = 0.f;
+  for (int stage = 0; stage < 4; ++stage) {
+    for (int w = 0; w < 2; ++w) {  // warm-up, then timed
+      CK(cudaEventRecord(ctx->ev0, ctx->stream));
+      for (int k = 0; k < reps; ++k)
+        CK(launch_mp_stage(graph_view(ctx), params_view(ctx), stage, r, buf_ptr<double>(ctx->inv_diag), &sc->rr,
+                           buf_ptr<float>(ctx->lp_sf), mw, z, ctx->mbar_spin, buf_ptr<int>(ctx->err_word),
+                           ctx->stream));
+      CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    }
+    CK(cudaEventSynchronize(ctx->ev1));
+    CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    out[stage] = ms * 1e-3 / reps;
+  }
+  READ_ERR();
+  if (ctx->h_err[kErrTimeout] != kErrNone) return fail(ctx, CSTG_ERR_TIMEOUT, "learned_time: a tensor-core wait timed out");
+  return CSTG_OK;
+}

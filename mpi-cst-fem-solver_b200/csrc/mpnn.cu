@@ -124,6 +124,31 @@ __global__ void __launch_bounds__(256) k_mp_rr(int n, const double* __restrict__
   if (grid_sum<1, 256>(v, sc->partials, &sc->ticket[0], tot) && threadIdx.x == 0) sc->rr = tot[0];
 }
 
+// ---- per-node static inputs: diagonal / its mean, coordinates / scale, material ---------------------
+
+__global__ void __launch_bounds__(256) k_mp_dsum(int n, const double* __restrict__ invd, MpScratch* sc) {
+  double a = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a += 1.0 / invd[i];
+  const double v[1] = {a};
+  double tot[1];
+  if (grid_sum<1, 256>(v, sc->partials, &sc->ticket[2], tot) && threadIdx.x == 0) sc->dsum = tot[0];
+}
+
+__global__ void k_mp_static(int N, const double* __restrict__ invd, const double* __restrict__ xy,
+                            const float* __restrict__ mat, const MpScratch* sc, double coord_scale,
+                            float* __restrict__ sf) {
+  const double d_mean = N > 0 ? sc->dsum / (2.0 * N) : 1.0;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
+    float* o = sf + (size_t)k * 6;
+    o[0] = (float)((1.0 / invd[2 * k]) / d_mean);
+    o[1] = (float)((1.0 / invd[2 * k + 1]) / d_mean);
+    o[2] = (float)(xy[2 * k] / coord_scale);
+    o[3] = (float)(xy[2 * k + 1] / coord_scale);
+    o[4] = mat[2 * k];
+    o[5] = mat[2 * k + 1];
+  }
+}
+
 // ---- the learned cycle's post-smoother weights: out = factor / lambda_max * D^-1 ------------------
 
 __global__ void k_mp_smoother_weights(int n, const double* __restrict__ invd, const double* lam, double factor,
@@ -805,6 +830,15 @@ cudaError_t launch_mp_rr(int n, const double* r, MpScratch* sc, cudaStream_t s, 
   return cudaGetLastError();
 }
 
+cudaError_t launch_mp_static(int N, const double* invd, const double* xy, const float* mat, double coord_scale,
+                             MpScratch* sc, float* sf, cudaStream_t s) {
+  if (N <= 0) return cudaSuccess;
+  k_mp_dsum<<<kRedGrid, 256, 0, s>>>(2 * N, invd, sc);
+  k_mp_static<<<grid_nodes(N, 256), 256, 0, s>>>(N, invd, xy, mat, sc, coord_scale, sf);
+  count_launches(2);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_mp_smoother_weights(int n, const double* invd, const double* lam, double factor, double* out,
                                        cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
@@ -861,6 +895,44 @@ cudaError_t launch_mp_forward(const MpnnGraph& g, const MpnnParams& P, const dou
       k_mp_layer_tc<false, false><<<grid, kLT, kTcSmem, s>>>(a);
   }
   count_launches(1 + kMpL);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mp_stage(const MpnnGraph& g, const MpnnParams& P, int stage, const double* r, const double* invd,
+                            const double* rr, const float* sf, MpnnWork& w, double* z, long long spin_limit, int* err,
+                            cudaStream_t s) {
+  const int N = g.n_nodes;
+  if (N <= 0) return cudaSuccess;
+  const double inv_n = 1.0 / (2.0 * N);
+  if (stage == 0) {
+    int dev = 0, sms = kSMs;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int ge = (int)std::max<long long>(1, std::min<long long>(2LL * sms, (8LL * N + 255) / 256));
+    k_mp_encode<false><<<ge, 256, 0, s>>>(N, r, rr, inv_n, sf, P, nullptr, w.H[0], nullptr);
+  } else {
+    MpLayerArgs a{};
+    a.N = N;
+    a.node_ptr = g.node_ptr;
+    a.nbr = g.nbr;
+    a.P = P;
+    a.r = r;
+    a.invd = invd;
+    a.rr = rr;
+    a.inv_n = inv_n;
+    a.z = z;
+    a.spin_limit = spin_limit;
+    a.err = err;
+    a.layer = stage - 1;
+    const bool last = stage == kMpL;
+    a.Hin = w.H[(stage - 1) & 1];
+    a.Hout = last ? nullptr : w.H[stage & 1];
+    if (last)
+      k_mp_layer_tc<false, true><<<tc_grid(N, false, true), kLT, kTcSmem, s>>>(a);
+    else
+      k_mp_layer_tc<false, false><<<tc_grid(N, false, false), kLT, kTcSmem, s>>>(a);
+  }
+  count_launches(1);
   return cudaGetLastError();
 }
 

@@ -100,6 +100,13 @@ def apply(K: GpuCsrMatrix, r, z=None):
     return z
 
 
+def time_stages(K: GpuCsrMatrix, reps: int = 20) -> dict:
+    """Seconds per launch of the encoder and of each message-passing layer (cstg_learned_time)."""
+    out = (C.c_double * 4)()
+    K.ctx.check(K.ctx.L.cstg_learned_time(K.ctx.h, int(reps), out))
+    return {"encoder_s": out[0], "layer_s": [out[1], out[2], out[3]]}
+
+
 def cycle_parts(K: GpuCsrMatrix, r) -> dict:
     """The learned cycle's parts for the CUDA float64 residual r: x_fix (pre-smoothing + coarse
     correction), r2 = r - A x_fix, winvd = omega D^-1 and the cycle's output z."""
@@ -276,41 +283,52 @@ def scale_output(params: np.ndarray, gain: float) -> np.ndarray:
     return p
 
 
-def select_gain(params: np.ndarray, n_plates: int = 4, seed: int = 5151, gains=(0.25, 0.5, 0.75, 1.0),
+def select_gain(params: np.ndarray, n_plates: int = 8, seed: int = 5151, gains=(0.25, 0.5, 0.75, 1.0),
                 n_r_range=(60, 160), device: int = 0, log=print):
     """Chooses the output gain of the cycle's post-smoother on validation plates (seeded draws
-    from the training distribution, not the training batch): the gain with the fewest flexible-CG
-    iterations of the learned cycle in total. The network's output varies nonlinearly with r; a
-    full-strength correction lowers the per-step loss most but can cost Krylov iterations, so the
-    gain is chosen on the solve itself. Returns (gain, {gain: total iterations})."""
+    from the training distribution, not the training batch). The network's output varies
+    nonlinearly with r: a full-strength correction lowers the per-step loss most but can cost
+    Krylov iterations, so the gain is chosen on the solve itself, against the same cycle with the
+    network at zero (gain 0): the gain whose worst plate (iterations / iterations at gain 0) is
+    lowest, ties broken by the total. Returns (gain, {gain: [iterations per plate]})."""
     from .solver import CgJacobiSolver, SolverOptions
     specs = random_batch(count=n_plates, seed=seed, n_r_range=n_r_range)
-    systems = []
-    for spec in specs:
-        m, D, K, b = plate_system(spec, Context(device))
-        systems.append((m, D, K, b))
-    totals = {}
-    for g in gains:
+    systems = [plate_system(spec, Context(device)) for spec in specs]
+    its = {}
+    for g in (0.0,) + tuple(gains):
         p = scale_output(params, g)
-        tot = 0
+        row = []
         for m, D, K, b in systems:
             s = CgJacobiSolver(SolverOptions(rtol=1e-10, max_iter=5000, precision="mixed",
                                              preconditioner="learned_mg", true_residual_stop=True))
             s.setup(K)
             setup(K, p, node_material(D, m.num_nodes))
             st = s.solve(b, np.zeros(m.num_dofs))
-            tot += st.iterations if st.converged else 10 ** 6
-        totals[float(g)] = tot
-        log(f"gain {g}: {tot} iterations on {n_plates} validation plates")
+            row.append(st.iterations if st.converged else 10 ** 6)
+        its[float(g)] = row
+        log(f"gain {g}: iterations {row} (total {sum(row)})")
     for m, D, K, b in systems:
         K.ctx.close()
-    best = min(totals, key=lambda g: (totals[g], -g))
-    return best, totals
+    base = np.array(its[0.0], dtype=float)
+
+    def score(g):
+        r = np.array(its[g], dtype=float) / base
+        return (float(r.max()), sum(its[g]))
+    best = min((g for g in its if g > 0.0), key=score)
+    return best, its
+
+
+def gain_record(raw: np.ndarray) -> dict:
+    """select_gain on the raw (unscaled) parameters, as fields of the weights file."""
+    gain, its = select_gain(raw)
+    print(f"output gain {gain} (validation iterations {its})")
+    return dict(output_gain=gain, params_raw=raw,
+                gain_iterations=np.array([[g] + list(v) for g, v in sorted(its.items())], dtype=np.float64))
 
 
 def main():
     ap = argparse.ArgumentParser(description="train the learned preconditioner on the GPU")
-    ap.add_argument("cmd", choices=["train"])
+    ap.add_argument("cmd", choices=["train", "select-gain"])
     ap.add_argument("--mode", choices=["local", "cycle"], default="local")
     ap.add_argument("--out", default=None)
     ap.add_argument("--plates", type=int, default=100)
@@ -322,15 +340,21 @@ def main():
     ap.add_argument("--n-r-max", type=int, default=200)
     a = ap.parse_args()
     out = a.out or (WEIGHTS if a.mode == "local" else WEIGHTS_CYCLE)
+    if a.cmd == "select-gain":  # re-select the cycle smoother's output gain of a weights file
+        d = dict(np.load(WEIGHTS_CYCLE))
+        raw = d["params_raw"] if "params_raw" in d else scale_output(d["params"], 1.0 / float(d["output_gain"]))
+        d.update(gain_record(raw.astype(np.float32)))
+        d["params"] = scale_output(raw, float(d["output_gain"]))
+        np.savez(out, **d)
+        print(f"wrote {out}")
+        return
     t0 = time.perf_counter()
     params, hist, n_pairs = train(a.plates, a.samples, a.epochs, a.batch, a.lr, a.seed, (20, a.n_r_max),
                                   mode=a.mode)
     extra = {}
     if a.mode == "cycle":
-        gain, totals = select_gain(params)
-        params = scale_output(params, gain)
-        extra = dict(output_gain=gain, gain_iterations=np.array([[g, it] for g, it in sorted(totals.items())]))
-        print(f"output gain {gain} (validation iterations {totals})")
+        extra = gain_record(params)
+        params = scale_output(params, float(extra["output_gain"]))
     os.makedirs(os.path.dirname(os.path.abspath(out)), exist_ok=True)
     np.savez(out, params=params, loss_history=np.array(hist), pairs=n_pairs, plates=a.plates,
              samples=a.samples, epochs=a.epochs, batch=a.batch, lr=a.lr, seed=a.seed, mode=a.mode,

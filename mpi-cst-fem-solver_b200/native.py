@@ -157,6 +157,7 @@ _SIGS = {
     "cstg_trainer_accumulate_cycle": (C.c_int, [_vp, _vp, C.c_int, _vp, _vp, _vp]),
     "cstg_learned_cycle_parts_device": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
     "cstg_set_wait_limits": (C.c_int, [_vp, C.c_longlong, C.c_longlong]),
+    "cstg_learned_time": (C.c_int, [_vp, C.c_int, _vp]),
     "cstg_trainer_step": (C.c_int, [_vp, C.c_float, C.c_float]),
     "cstg_trainer_params": (C.c_int, [_vp, _vp, _vp]),
     "cstg_trainer_zero_grad": (C.c_int, [_vp]),
