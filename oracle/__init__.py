@@ -22,8 +22,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "libcst_oracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libcstfem_ref.so")
-# Reference checkout whose sources `make ref` compiles (the Makefile's REF).
-REF_DIR = os.environ.get("CSTFEM_REF", "/root/reference")
+# Reference checkout whose sources `make ref` compiles (the Makefile's REF): the directory
+# `reference` beside this repository unless CSTFEM_REF names another.
+REF_DIR = os.environ.get("CSTFEM_REF", os.path.abspath(os.path.join(HERE, "..", "..", "reference")))
 
 
 def ref_sources_present() -> bool:

@@ -1,10 +1,10 @@
 """Generates the golden fixtures of this directory from the reference's own serial core.
 
 Run where the reference sources exist (they are compiled by `make -C oracle ref` into
-oracle/_ref/libcstfem_ref.so; this script reads the reference checkout, default
-/root/reference, for its two committed Kirsch meshes):
+oracle/_ref/libcstfem_ref.so; this script reads the reference checkout, by default the
+directory `reference` beside this repository or $CSTFEM_REF, for its two committed Kirsch meshes):
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py [--ref PATH]
 
 Every number stored here was computed by the reference's code (read_gmsh, cst_stiffness,
 build_stiffness_pattern, assemble_stiffness, add_traction, add_dirichlet, apply_dirichlet,
@@ -26,7 +26,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, REPO)
 
-from oracle import RefCore, build  # noqa: E402
+from oracle import REF_DIR, RefCore, build  # noqa: E402
 
 plate = importlib.import_module("mpi-cst-fem-solver_b200.plate")
 GROUPS = ("hole", "left_sym", "bottom_sym", "right", "top")
@@ -156,7 +156,7 @@ def spd_case(R: RefCore, out: str):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=REF_DIR)
     a = ap.parse_args()
     build(ref=True)
     R = RefCore()

@@ -7,7 +7,7 @@ import re
 import numpy as np
 import pytest
 
-REF = os.environ.get("CSTFEM_REF", "/root/reference")
+from oracle import REF_DIR as REF  # the reference checkout (beside the repository, or $CSTFEM_REF)
 GROUPS = ("hole", "left_sym", "bottom_sym", "right", "top")
 
 
