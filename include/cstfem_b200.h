@@ -99,6 +99,8 @@ typedef struct {
 #define CSTG_LAUNCH_AUTO 0        /* persistent kernel for mesh-pattern matrices, else graph  */
 #define CSTG_LAUNCH_PERSISTENT 1  /* one cooperative kernel runs all iterations (mesh pattern) */
 #define CSTG_LAUNCH_GRAPH 2       /* 3-4 kernels per iteration, chunks replayed as CUDA graphs */
+#define CSTG_LAUNCH_INSTRUMENTED 3 /* FP64 Jacobi-PCG with its kernels launched one by one and CUDA
+                                      events between the phases (cstg_solve_breakdown); slower  */
 
 /* ≙ cstfem::SolverStats (include/cstfem/solver.hpp:99-107) plus counters. */
 typedef struct {
@@ -113,6 +115,20 @@ typedef struct {
   char message[256];        /* SolverStats::message                                         */
   char warning[256];        /* SolverStats::warning (true residual > 10 rtol)               */
 } cstg_stats;
+
+/* ≙ cstfem::SolveBreakdown (include/cstfem/solver.hpp:17-56): device seconds of the phases of the
+ * last solve run with launch_mode CSTG_LAUNCH_INSTRUMENTED (CUDA events between the phases of every
+ * iteration). setup: the Jacobi diagonal (cstg_pcg_setup); spmv_local: q = A p with its fused p'Ap
+ * partial sums, and A x of the true residual; dot_local: 0 (every dot product is fused into the
+ * SpMV or vector kernels and counted there); vector_ops: the x, r, p updates with their fused dots
+ * and b - A x; total: setup + the whole solve. The distributed fields of the reference (halo,
+ * allreduce) have no counterpart on one device. */
+typedef struct {
+  double setup, spmv_local, dot_local, vector_ops, total;
+  long long spmv_calls, reductions;
+  int valid;
+  int reserved[3];
+} cstg_breakdown;
 
 /* ---- batched solves: launch shape and per-system results -------------------------------- */
 /* No reference counterpart. Launch shape of the batched persistent solve: each plate is solved
@@ -148,6 +164,8 @@ int cstg_set_stream(cstg_ctx* ctx, void* cuda_stream); /* NULL: the context's ow
  * issued on other streams: inputs written there must be finished (or the context's stream made
  * to wait for them) before the call. */
 int cstg_get_stream(cstg_ctx* ctx, void** cuda_stream);
+/* The phase times of the last instrumented solve (CSTG_LAUNCH_INSTRUMENTED) since cstg_pcg_setup. */
+int cstg_solve_breakdown(cstg_ctx* ctx, cstg_breakdown* out);
 void cstg_default_options(cstg_solver_options* opt);
 int cstg_version(void);
 /* Bounded device waits (no reference counterpart). Every device-side wait of the library gives
@@ -256,6 +274,9 @@ int cstg_add_traction(cstg_ctx* ctx, int n_edges, const int32_t* edges, double t
  * CSTG_ERR_MESH with the reference's message. */
 #define CSTG_TRACTION_CONSTANT 0
 #define CSTG_TRACTION_KIRSCH 1
+/* the traction sigma . n of the uniform stress sigma = diag(p0, p1) (outward normal n of each
+ * edge): the loads of the reference's Neumann patch tests, tests/test_patch.cpp:86-112 */
+#define CSTG_TRACTION_STRESS 2
 int cstg_add_traction_device(cstg_ctx* ctx, int n_edges, const int32_t* d_edges, double thickness, int kind,
                              double p0, double p1, double* d_f);
 

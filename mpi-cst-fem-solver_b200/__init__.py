@@ -14,7 +14,7 @@ from .batch import BatchSolution, BatchSolver, PlateBatch, build_batch  # noqa: 
 from .solver import amg_apply, amg_set_smoother, amg_set_strength, amg_set_tail, amg_setup, amg_time  # noqa: F401
 from .solver import (CgJacobiSolver, Context, DirichletDofs, GpuCsrMatrix,  # noqa: F401
                      PlaneCondition, SolverOptions, SolverStats, add_dirichlet_group,
-                     add_kirsch_traction, add_traction, apply_dirichlet, assemble_stiffness, build_stiffness_pattern,
+                     add_kirsch_traction, add_stress_traction, add_traction, apply_dirichlet, assemble_stiffness, build_stiffness_pattern,
                      compute_element_stresses, constitutive_matrix, pcg_jacobi, scf_at_hole)
 
 __version__ = "0.1.0"

@@ -36,7 +36,8 @@ KNOWN_KEYS = ["mesh", "plane", "E", "nu", "thickness", "partitioner", "solver", 
 SOLVERS = {"cg_jacobi": dict(precision="fp64", true_residual_stop=False),
            "gpu_cg": dict(precision="fp64", true_residual_stop=True),
            "gpu_cg_mixed": dict(precision="mixed", true_residual_stop=True),
-           "gpu_cg_learned": dict(precision="mixed", true_residual_stop=True, preconditioner="learned"),
+           "gpu_cg_learned": dict(precision="mixed", true_residual_stop=True, preconditioner="learned_mg"),
+           "gpu_cg_learned_local": dict(precision="mixed", true_residual_stop=True, preconditioner="learned"),
            "gpu_cg_amg": dict(precision="fp64", true_residual_stop=True, preconditioner="amg")}
 
 
@@ -198,6 +199,7 @@ def read_case_settings(c: CaseFile) -> dict:
     inst = c.get_string("instrument", "true")
     if inst not in ("true", "false"):
         raise CaseError(f"{c.source}: instrument must be true or false")
+    s["instrument"] = inst == "true"
     path = c.get_string("path", "auto")
     if path not in ("auto", "serial", "distributed"):
         raise CaseError(f"{c.source}: path must be auto, serial or distributed, got '{path}'")
@@ -277,12 +279,16 @@ def run_case(case_path: str, out=sys.stdout, err=sys.stderr, device: int = 0) ->
         t_bcs = time.perf_counter() - t0
 
         t0 = time.perf_counter()
-        opts = SolverOptions(rtol=s["rtol"], max_iter=s["max_iter"], **SOLVERS[s["solver"]])
+        # cg_jacobi with instrument = true: the phases timed with CUDA events (SolveBreakdown)
+        instrumented = s["solver"] == "cg_jacobi" and s.get("instrument", False)
+        opts = SolverOptions(rtol=s["rtol"], max_iter=s["max_iter"], **SOLVERS[s["solver"]],
+                             **({"launch": "instrumented"} if instrumented else {}))
         solver = CgJacobiSolver(opts)
         solver.setup(K)
-        if opts.preconditioner == "learned":
+        if opts.preconditioner in ("learned", "learned_mg"):
             from . import learned
-            learned.setup(K, learned.load_weights(), learned.node_material(D, mesh.num_nodes))
+            mode = "cycle" if opts.preconditioner == "learned_mg" else "local"
+            learned.setup(K, learned.load_weights(mode=mode), learned.node_material(D, mesh.num_nodes))
         u_d = torch.zeros_like(f)
         st = solver.solve(f, u_d)
         u = u_d.cpu().numpy()
@@ -321,7 +327,7 @@ def run_case(case_path: str, out=sys.stdout, err=sys.stderr, device: int = 0) ->
                        "iterations": st.iterations, "rel_residual": st.rel_residual,
                        "true_rel_residual": st.true_rel_residual, "converged": st.converged,
                        "device_solve_seconds": st.solve_seconds},
-            "solve_breakdown": None,
+            "solve_breakdown": _breakdown_json(solver.breakdown(), st.iterations) if instrumented else None,
             "timings": {"read": t_read, "assembly": t_asm, "bcs": t_bcs, "solve": t_solve, "output": t_out,
                         "total": t_all},
             "kirsch": kj}
@@ -335,6 +341,20 @@ def run_case(case_path: str, out=sys.stdout, err=sys.stderr, device: int = 0) ->
     except (CaseError, CstgError, OSError) as e:
         err.write(f"error: {e}\n")
         return 1
+
+
+def _breakdown_json(bd: dict, iterations: int) -> dict:
+    """The reference's solve_breakdown entries (driver.cpp:92-110, one rank: min = max = mean) from
+    the device phase times of an instrumented solve; the halo and allreduce phases of the
+    distributed path have no counterpart on one device and are 0."""
+    acc = bd["setup"] + bd["spmv_local"] + bd["dot_local"] + bd["vector_ops"]
+    vals = [("setup", bd["setup"]), ("spmv_local", bd["spmv_local"]), ("halo_post", 0.0), ("halo_wait", 0.0),
+            ("spmv_ghost", 0.0), ("dot_local", bd["dot_local"]), ("allreduce", 0.0),
+            ("vector_ops", bd["vector_ops"]), ("unaccounted", bd["total"] - acc), ("total", bd["total"]),
+            ("time_per_iteration", bd["total"] / iterations if iterations > 0 else 0.0),
+            ("accounted_fraction", acc / bd["total"] if bd["total"] > 0 else 0.0),
+            ("halo_bytes_sent_per_iteration", 0.0), ("halo_messages_sent_per_iteration", 0.0)]
+    return {k: {"min": v, "max": v, "mean": v} for k, v in vals}
 
 
 def main():

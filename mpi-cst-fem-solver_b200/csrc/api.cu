@@ -97,6 +97,7 @@ void cstg_destroy(cstg_ctx* ctx) {
   }
   if (ctx->h_err) cudaFreeHost(ctx->h_err);
   if (ctx->h_state) cudaFreeHost(ctx->h_state);
+  for (cudaEvent_t e : ctx->bd_ev) cudaEventDestroy(e);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
   if (ctx->own) cudaStreamDestroy(ctx->own);
@@ -109,6 +110,15 @@ int cstg_set_stream(cstg_ctx* ctx, void* s) {
   BEGIN(ctx);
   CK(cudaStreamSynchronize(ctx->stream));
   ctx->stream = s ? static_cast<cudaStream_t>(s) : ctx->own;
+  return CSTG_OK;
+}
+
+int cstg_solve_breakdown(cstg_ctx* ctx, cstg_breakdown* out) {
+  BEGIN(ctx);
+  if (!out) return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "solve_breakdown: null output");
+  if (!ctx->bd.valid)
+    return fail(ctx, CSTG_ERR_STATE, "solve_breakdown: no instrumented solve since the last cstg_pcg_setup");
+  *out = ctx->bd;
   return CSTG_OK;
 }
 
@@ -492,10 +502,18 @@ int cstg_pcg_setup(cstg_ctx* ctx) {
   const int n = ctx->n_rows;
   ENSURE(ctx->inv_diag, sizeof(double) * (size_t)n);
   RESET_ERR();
+  CK(cudaEventRecord(ctx->ev0, ctx->stream));
   if (n)
     CK(launch_inv_diag(n, buf_ptr<int>(ctx->row_ptr), buf_ptr<int>(ctx->cols), buf_ptr<double>(ctx->vals),
                        buf_ptr<double>(ctx->inv_diag), buf_ptr<int>(ctx->err_word), ctx->stream));
+  CK(cudaEventRecord(ctx->ev1, ctx->stream));
   READ_ERR();
+  {
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    ctx->bd = cstg_breakdown{};
+    ctx->bd.setup = ms * 1e-3;  // the Jacobi setup of the next solves' breakdown
+  }
   if (ctx->h_err[kErrDiag] != kErrNone) {
     ctx->setup_done = false;
     return fail(ctx, CSTG_ERR_NONPOSITIVE_DIAGONAL, "cg_jacobi: non-positive diagonal at row %d",
@@ -617,11 +635,15 @@ static int run_solve(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg_s
 
   // Mesh-pattern matrices run as one persistent cooperative kernel per solve (unless the
   // caller asks for the graph path); caller CSR matrices use the graph path.
-  const bool persist = ctx->kind == 1 && o.launch_mode != CSTG_LAUNCH_GRAPH && !snap;
-  const int chunk = snap ? snap->every : persist ? o.max_iter + 1 : (o.check_interval > 0 ? o.check_interval : 50);
+  const bool instrumented = o.launch_mode == CSTG_LAUNCH_INSTRUMENTED;
+  if (instrumented && mixed)
+    return fail(ctx, CSTG_ERR_UNSUPPORTED, "pcg_solve: the instrumented launch mode runs FP64 Jacobi-PCG only");
+  const bool persist = ctx->kind == 1 && o.launch_mode != CSTG_LAUNCH_GRAPH && !instrumented && !snap;
+  const int chunk = snap ? snap->every : persist ? o.max_iter + 1 : instrumented ? kBdChunk
+                                                                  : (o.check_interval > 0 ? o.check_interval : 50);
   // (Re)capture the chunk graph when a buffer, the shape or the method changed. The mixed
   // graph reads b (reliable updates), so it is also tied to the right-hand-side pointer.
-  if (!persist && (!ctx->graph || ctx->graph_gen != ctx->generation || ctx->graph_chunk != chunk ||
+  if (!persist && !instrumented && (!ctx->graph || ctx->graph_gen != ctx->generation || ctx->graph_chunk != chunk ||
       ctx->graph_hist != (hist ? 1 : 0) || ctx->graph_kind != ctx->kind || ctx->graph_n != n ||
       ctx->graph_prec != o.precision || ctx->graph_refs != o.max_refinements ||
       (mixed && ctx->graph_b != d_b))) {
@@ -652,6 +674,12 @@ static int run_solve(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg_s
     ctx->graph_b = d_b;
   }
 
+  // instrumented: events around the phases of every iteration (kBdChunk iterations per batch)
+  double bd_spmv = 0.0, bd_vec = 0.0;
+  if (instrumented && ctx->bd_ev.empty()) {
+    ctx->bd_ev.resize(2 * kBdChunk + 1);
+    for (cudaEvent_t& e : ctx->bd_ev) CK(cudaEventCreate(&e));
+  }
   CK(cudaEventRecord(ctx->ev0, ctx->stream));
   if (mixed)
     CK(launch_mixed_init(mw, o.rtol, o.max_iter, hist, kReliableDelta, ctx->stream));
@@ -671,6 +699,24 @@ static int run_solve(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg_s
       const int it0 = ctx->h_state->iter;
       if (persist) {
         CK(launch_pcg_persistent(w, bm, mixed ? &mm : nullptr, o.max_refinements, ctx->barrier_spin, ctx->stream));
+      } else if (instrumented) {
+        // SpMV (with its fused p'Ap partials), then the vector phase (x, r, p updates with their
+        // fused dots), an event after each; the elapsed times are summed after the batch
+        CK(cudaEventRecord(ctx->bd_ev[0], ctx->stream));
+        for (int k = 0; k < kBdChunk; ++k) {
+          CK(launch_spmv_phase(w, pbm, pcm, ctx->stream));
+          CK(cudaEventRecord(ctx->bd_ev[2 * k + 1], ctx->stream));
+          CK(launch_vector_phase(w, ctx->stream));
+          CK(cudaEventRecord(ctx->bd_ev[2 * k + 2], ctx->stream));
+        }
+        CK(cudaEventSynchronize(ctx->bd_ev[2 * kBdChunk]));
+        for (int k = 0; k < kBdChunk; ++k) {
+          float a_ms = 0.f, b_ms = 0.f;
+          CK(cudaEventElapsedTime(&a_ms, ctx->bd_ev[2 * k], ctx->bd_ev[2 * k + 1]));
+          CK(cudaEventElapsedTime(&b_ms, ctx->bd_ev[2 * k + 1], ctx->bd_ev[2 * k + 2]));
+          bd_spmv += a_ms * 1e-3;
+          bd_vec += b_ms * 1e-3;
+        }
       } else {
         CK(cudaGraphLaunch(ctx->graph, ctx->stream));
         count_launches(per_iter * chunk);
@@ -692,11 +738,22 @@ static int run_solve(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg_s
       spmv_calls += ctx->h_state->iter - it0 + (ctx->h_state->done == CSTG_SOLVE_BREAKDOWN + 1);
     }
     // true residual (solver.cpp:117-122); with true_residual_stop it may re-open the solve
+    if (instrumented) CK(cudaEventRecord(ctx->bd_ev[0], ctx->stream));
     rc = spmv(ctx, w.x, w.Ap);
     if (rc) return rc;
     ++spmv_calls;
+    if (instrumented) CK(cudaEventRecord(ctx->bd_ev[1], ctx->stream));
     // (the mixed method confirms convergence on the FP64 true residual itself)
     CK(launch_true_residual(w, !mixed && o.true_residual_stop != 0, o.max_refinements, ctx->stream));
+    if (instrumented) {
+      CK(cudaEventRecord(ctx->bd_ev[2], ctx->stream));
+      CK(cudaEventSynchronize(ctx->bd_ev[2]));
+      float a_ms = 0.f, b_ms = 0.f;
+      CK(cudaEventElapsedTime(&a_ms, ctx->bd_ev[0], ctx->bd_ev[1]));
+      CK(cudaEventElapsedTime(&b_ms, ctx->bd_ev[1], ctx->bd_ev[2]));
+      bd_spmv += a_ms * 1e-3;
+      bd_vec += b_ms * 1e-3;
+    }
     rc = snapshot(ctx);
     if (rc) return rc;
     true_done = true;
@@ -713,6 +770,16 @@ static int run_solve(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg_s
   CK(cudaStreamSynchronize(ctx->stream));
   float ms = 0.f;
   CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+  if (instrumented) {
+    cstg_breakdown& bd = ctx->bd;
+    bd.spmv_local = bd_spmv;
+    bd.vector_ops = bd_vec;
+    bd.dot_local = 0.0;  // fused into the SpMV and vector kernels (counted there)
+    bd.total = bd.setup + ms * 1e-3;
+    bd.spmv_calls = spmv_calls;
+    bd.reductions = 2LL * s.iter + 1;
+    bd.valid = 1;
+  }
 
   if (stats) {
     std::memset(stats, 0, sizeof *stats);
@@ -959,7 +1026,7 @@ int cstg_add_traction_device(cstg_ctx* ctx, int n_edges, const int32_t* d_edges,
     return fail(ctx, CSTG_ERR_STATE, "add_traction: needs the node incidence of cstg_build_pattern");
   if (n_edges < 0 || (n_edges > 0 && (!d_edges || !d_f)))
     return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "add_traction: bad arguments");
-  if (kind != CSTG_TRACTION_CONSTANT && kind != CSTG_TRACTION_KIRSCH)
+  if (kind != CSTG_TRACTION_CONSTANT && kind != CSTG_TRACTION_KIRSCH && kind != CSTG_TRACTION_STRESS)
     return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "add_traction: unknown traction kind %d", kind);
   if (n_edges == 0) return CSTG_OK;
   const int N = ctx->n_nodes;

@@ -26,6 +26,8 @@ constexpr int kErrNone = 0x7f7f7f7f;  // memset(0x7f) sentinel of the device err
 // Mixed precision: a reliable update replaces the FP32 recursive residual by the FP64 one when
 // it has dropped by this factor since the last update (~one replacement per decade).
 constexpr double kReliableDelta = 0.1;
+// Iterations per batch of the instrumented solve (events between every phase, read per batch).
+constexpr int kBdChunk = 50;
 
 struct DevBuf {
   void* p = nullptr;
@@ -114,6 +116,10 @@ struct cstg_ctx {
   unsigned long long lm_winvd_for = ~0ull;
   // truncated flexible CG: ring of earlier directions and their A-products, ring state
   DevBuf fcg_ph[kFcgMaxHist], fcg_qh[kFcgMaxHist], fcg_ring;
+
+  // the last instrumented solve's phase times (CSTG_LAUNCH_INSTRUMENTED) and its event pool
+  cstg_breakdown bd{};
+  std::vector<cudaEvent_t> bd_ev;
 
   // bounded device waits (polls before a wait gives up; cstg_set_wait_limits)
   long long barrier_spin = kBarrierSpinDefault;

@@ -338,8 +338,11 @@ int cstg_host::run_fcg(cstg_ctx* ctx, const double* d_b, double* d_x, const cstg
               o.rtol, pre);
         break;
     }
-    if (stats->true_rel_residual > 10.0 * o.rtol)
-      g_fmt(stats->warning, sizeof stats->warning, "true residual %g exceeds 10 x rtol", stats->true_rel_residual);
+    if (stats->converged && s.done != CSTG_SOLVE_ZERO_RHS + 1 && stats->true_rel_residual > 10.0 * o.rtol)
+      g_fmt(stats->warning, sizeof stats->warning,
+            "WARNING: CG recursive residual converged (%g) but the true residual ||b - Ax|| / ||b|| = %g "
+            "exceeds 10 * rtol = %g",
+            s.rel, stats->true_rel_residual, 10.0 * o.rtol);
   }
   return CSTG_OK;
 }

@@ -417,6 +417,19 @@ cudaError_t launch_pcg_iteration(const PcgBuffers& w, const BlockMatrix* bm,
   return cudaGetLastError();
 }
 
+cudaError_t launch_spmv_phase(const PcgBuffers& w, const BlockMatrix* bm, const CsrMatrixDev* cm, cudaStream_t s) {
+  spmv_dispatch<true>(bm, cm, w.p, w.Ap, w.partials, w.st, s);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_vector_phase(const PcgBuffers& w, cudaStream_t s) {
+  k_update<<<wave_grid<k_update>(), kThreads, 0, s>>>(w.n, w.x, w.r, w.p, w.Ap, w.inv_diag, w.partials,
+                                              w.st, w.history);
+  k_pupdate<<<wave_grid<k_pupdate>(), kThreads, 0, s>>>(w.n, w.r, w.inv_diag, w.p, w.st);
+  count_launches(2);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_spmv_pcg(const BlockMatrix& A, const double* p, double* q, double* partials, PcgState* st,
                             cudaStream_t s) {
   spmv_dispatch<true>(&A, nullptr, p, q, partials, st, s);

@@ -102,7 +102,10 @@ __global__ void k_trac_edges(int n_edges, const int* __restrict__ edges, int n_n
     const double xi = i == 0 ? -g : g;
     const double Na = __dmul_rn(0.5, __dsub_rn(1.0, xi)), Nb = __dmul_rn(0.5, __dadd_rn(1.0, xi));
     double t0 = p0, t1 = p1;
-    if (kind == CSTG_TRACTION_KIRSCH) {
+    if (kind == CSTG_TRACTION_STRESS) {  // sigma . n of the uniform stress diag(p0, p1)
+      t0 = __dmul_rn(p0, nx);
+      t1 = __dmul_rn(p1, ny);
+    } else if (kind == CSTG_TRACTION_KIRSCH) {
       const double x = __dadd_rn(__dmul_rn(Na, xa), __dmul_rn(Nb, xb));
       const double y = __dadd_rn(__dmul_rn(Na, ya), __dmul_rn(Nb, yb));
       kirsch_traction(p0, p1, x, y, nx, ny, t0, t1);

@@ -55,6 +55,7 @@ class SolverOptions(C.Structure):
 
 TRACTION_CONSTANT = 0
 TRACTION_KIRSCH = 1
+TRACTION_STRESS = 2
 
 PRECOND_JACOBI = 0
 PRECOND_LEARNED = 1
@@ -65,6 +66,7 @@ AMG_CHEBYSHEV, AMG_JACOBI = 0, 1  # cstg_amg_set_smoother
 LAUNCH_AUTO = 0
 LAUNCH_PERSISTENT = 1
 LAUNCH_GRAPH = 2
+LAUNCH_INSTRUMENTED = 3
 
 
 class Stats(C.Structure):
@@ -73,6 +75,13 @@ class Stats(C.Structure):
                 ("true_rel_residual", C.c_double), ("solve_seconds", C.c_double),
                 ("spmv_calls", C.c_longlong), ("message", C.c_char * 256),
                 ("warning", C.c_char * 256)]
+
+
+class Breakdown(C.Structure):
+    """cstg_breakdown: the reference's SolveBreakdown fields of an instrumented solve."""
+    _fields_ = [("setup", C.c_double), ("spmv_local", C.c_double), ("dot_local", C.c_double),
+                ("vector_ops", C.c_double), ("total", C.c_double), ("spmv_calls", C.c_longlong),
+                ("reductions", C.c_longlong), ("valid", C.c_int), ("reserved", C.c_int * 3)]
 
 
 class AmgInfo(C.Structure):
@@ -101,6 +110,7 @@ _SIGS = {
     "cstg_last_error": (C.c_char_p, [_vp]),
     "cstg_set_stream": (C.c_int, [_vp, _vp]),
     "cstg_get_stream": (C.c_int, [_vp, C.POINTER(_vp)]),
+    "cstg_solve_breakdown": (C.c_int, [_vp, C.POINTER(Breakdown)]),
     "cstg_default_options": (None, [C.POINTER(SolverOptions)]),
     "cstg_set_mesh": (C.c_int, [_vp, C.c_int, _vp, C.c_int, _vp]),
     "cstg_set_mesh_device": (C.c_int, [_vp, C.c_int, _vp, C.c_int, _vp]),

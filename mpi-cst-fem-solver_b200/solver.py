@@ -317,6 +317,15 @@ def add_kirsch_traction(K_or_ctx, group_edges, thickness: float, a: float, sigma
     _traction_device(ctx, group_edges, thickness, native.TRACTION_KIRSCH, a, sigma_inf, f)
 
 
+def add_stress_traction(K_or_ctx, group_edges, thickness: float, sxx: float, syy: float, f) -> None:
+    """Traction sigma . n of the uniform stress diag(sxx, syy) on line edges (outward normals),
+    added to the CUDA tensor f on the GPU: the loads of the reference's Neumann patch tests."""
+    ctx = K_or_ctx.ctx if isinstance(K_or_ctx, GpuCsrMatrix) else K_or_ctx
+    if not _is_device(f):
+        raise CstgError(native.ERR_INVALID_ARGUMENT, "add_stress_traction: f must be a CUDA float64 tensor")
+    _traction_device(ctx, group_edges, thickness, native.TRACTION_STRESS, sxx, syy, f)
+
+
 def _traction_device(ctx, group_edges, thickness, kind, p0, p1, f):
     # cstg_add_traction_device only enqueues its kernels on the context's stream: ctx.ordered
     # puts them after torch's pending work (the edge list copy, f) and torch's later work after them
@@ -339,7 +348,7 @@ class SolverOptions:
     true_residual_stop: bool = False
     max_refinements: int = 16
     check_interval: int = 0
-    launch: str = "auto"  # "auto" | "persistent" | "graph"
+    launch: str = "auto"  # "auto" | "persistent" | "graph" | "instrumented" (phase times: breakdown())
     # "jacobi" | "learned" (the network alone in flexible CG; needs learned setup) | "amg" |
     # "learned_mg" (the network as the multigrid cycle's post-smoother; needs learned setup)
     preconditioner: str = "jacobi"
@@ -355,7 +364,7 @@ class SolverOptions:
         o.max_refinements = self.max_refinements
         o.check_interval = self.check_interval
         o.launch_mode = {"auto": native.LAUNCH_AUTO, "persistent": native.LAUNCH_PERSISTENT,
-                         "graph": native.LAUNCH_GRAPH}[self.launch]
+                         "graph": native.LAUNCH_GRAPH, "instrumented": native.LAUNCH_INSTRUMENTED}[self.launch]
         o.preconditioner = {"jacobi": native.PRECOND_JACOBI, "learned": native.PRECOND_LEARNED,
                             "amg": native.PRECOND_AMG,
                             "learned_mg": native.PRECOND_LEARNED_MG}[self.preconditioner]
@@ -432,6 +441,15 @@ class CgJacobiSolver:
 
     def stats(self) -> SolverStats:
         return self._stats
+
+    def breakdown(self) -> dict:
+        """The reference's SolveBreakdown fields (solver.hpp:17-56) of the last solve run with
+        launch="instrumented": device seconds of each phase (CUDA events) and the counts."""
+        bd = native.Breakdown()
+        self.A.ctx.check(self.A.ctx.L.cstg_solve_breakdown(self.A.ctx.h, C.byref(bd)))
+        return {"setup": bd.setup, "spmv_local": bd.spmv_local, "dot_local": bd.dot_local,
+                "vector_ops": bd.vector_ops, "total": bd.total, "spmv_calls": bd.spmv_calls,
+                "reductions": bd.reductions}
 
 
 def pcg_jacobi(A: GpuCsrMatrix, b, x=None, options: SolverOptions | None = None) -> SolverStats:

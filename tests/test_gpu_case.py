@@ -49,6 +49,41 @@ def test_case_kirsch_L0_matches_reference(pkg, gpu_lib, golden, tmp_path):
     t = json.load(open(os.path.join(d, "timings.json")))
     assert t["path"] == "gpu" and t["solver"]["converged"] and t["dofs"] == u.size
     assert t["solver"]["iterations"] == g.meta["stress_iters10"]
+    # instrument = true (the default): the reference's solve_breakdown entries from CUDA events
+    bd = t["solve_breakdown"]
+    names = ["setup", "spmv_local", "halo_post", "halo_wait", "spmv_ghost", "dot_local", "allreduce",
+             "vector_ops", "unaccounted", "total", "time_per_iteration", "accounted_fraction",
+             "halo_bytes_sent_per_iteration", "halo_messages_sent_per_iteration"]
+    assert list(bd) == names
+    assert all(set(v) == {"min", "max", "mean"} for v in bd.values())
+    assert bd["total"]["mean"] > 0 and bd["spmv_local"]["mean"] > 0 and bd["vector_ops"]["mean"] > 0
+    assert 0.9 <= bd["accounted_fraction"]["mean"] <= 1.0 + 1e-9
+
+
+def test_instrumented_solve_matches_graph_path(pkg, gpu_lib):
+    """The instrumented launch runs the graph path's kernels one by one: the same iterations
+    and the same bits; its phase times add up to the device time of the solve."""
+    m = pkg.plate.quarter_plate(30, 60)
+    K = pkg.build_stiffness_pattern(m)
+    pkg.assemble_stiffness(m, pkg.constitutive_matrix(1.0, 0.3), 1.0, K)
+    b = np.zeros(m.num_dofs)
+    pkg.add_traction(K, m.boundary_edges["right"], 1.0, 1.0, 0.0, b)
+    pkg.apply_dirichlet(pkg.plate.symmetry_dirichlet(m), K, b)
+    xs = {}
+    for launch in ("graph", "instrumented"):
+        s = pkg.CgJacobiSolver(pkg.SolverOptions(rtol=1e-10, launch=launch))
+        s.setup(K)
+        x = np.zeros(m.num_dofs)
+        st = s.solve(b, x)
+        assert st.converged
+        xs[launch] = (x, st.iterations)
+    assert xs["graph"][1] == xs["instrumented"][1]
+    assert np.array_equal(xs["graph"][0], xs["instrumented"][0])
+    bd = s.breakdown()
+    assert bd["spmv_calls"] == xs["instrumented"][1] + 1
+    acc = bd["setup"] + bd["spmv_local"] + bd["dot_local"] + bd["vector_ops"]
+    assert 0.5 * bd["total"] <= acc <= bd["total"] * (1 + 1e-9)
+    K.ctx.close()
 
 
 @pytest.mark.parametrize("solver", ["gpu_cg", "gpu_cg_mixed", "gpu_cg_amg"])
