@@ -227,7 +227,10 @@ cudaError_t launch_mp_stage(const MpnnGraph& g, const MpnnParams& P, int stage, 
                             cudaStream_t s);
 cudaError_t launch_mp_loss(int N, const double* z, const double* az, const double* r, const double* e,
                            const double* invd, MpScratch* sc, MpnnWork& w, cudaStream_t s);
-cudaError_t launch_mp_backward(const MpnnGraph& g, const MpnnParams& P, MpnnWork& w, float* grad, cudaStream_t s);
+// The backward pass; the layers' weight gradients run on the tensor cores (spin_limit / err: the
+// bounded wait of their matrix multiplies, as in launch_mp_forward).
+cudaError_t launch_mp_backward(const MpnnGraph& g, const MpnnParams& P, MpnnWork& w, float* grad, long long spin_limit,
+                               int* err, cudaStream_t s);
 cudaError_t launch_mp_adam(float* p, float* m, float* v, const float* g, float lr, float b1, float b2, float eps,
                            int step, float scale, __nv_bfloat16* pb, float* pf, cudaStream_t s);
 

@@ -594,7 +594,7 @@ int cstg_trainer_accumulate(cstg_trainer* tr, cstg_ctx* ctx, int n_samples, cons
     TK(launch_spmv(&bm, nullptr, z, az, tr->stream));
     TK(launch_mp_loss(N, z, az, r, e, invd, sc, w, tr->stream));
     if (losses) TK(cudaMemcpyAsync(&losses[i], &sc->loss, sizeof(double), cudaMemcpyDeviceToHost, tr->stream));
-    TK(launch_mp_backward(g, P, w, grad, tr->stream));
+    TK(launch_mp_backward(g, P, w, grad, ctx->mbar_spin, err, tr->stream));
   }
   int h_err[kErrSlots];
   TK(cudaMemcpyAsync(h_err, err, sizeof h_err, cudaMemcpyDeviceToHost, tr->stream));
@@ -734,7 +734,7 @@ int cstg_trainer_accumulate_cycle(cstg_trainer* tr, cstg_ctx* ctx, int n_samples
     TK(launch_spmv(&bm, nullptr, z, az, s));
     TK(launch_mp_loss(N, z, az, r, e, winvd, sc, w, s));
     if (losses) TK(cudaMemcpyAsync(&losses[i], &sc->loss, sizeof(double), cudaMemcpyDeviceToHost, s));
-    TK(launch_mp_backward(g, P, w, grad, s));
+    TK(launch_mp_backward(g, P, w, grad, ctx->mbar_spin, err, s));
   }
   int h_err[kErrSlots];
   TK(cudaMemcpyAsync(h_err, err, sizeof h_err, cudaMemcpyDeviceToHost, s));

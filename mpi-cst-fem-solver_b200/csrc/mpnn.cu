@@ -729,6 +729,162 @@ __global__ void __launch_bounds__(256) k_mp_wgrad(int N, const float* __restrict
   if (q == 0) p[F * KW + o] = bacc;
 }
 
+// Weight gradient of a message-passing layer on the tensor cores:
+//   dW^T[k][o] = sum_n Xc[n][k] dU[n][o]  (k < 128: Xc = [Hprev | A], o < 64),  db[o] = sum_n dU[n][o].
+// One CTA of 256 threads per contiguous node range (the same ranges as k_mp_wgrad, so the
+// partial sums per block keep their block order). Per chunk of 128 nodes: the Xc rows (BF16) and
+// the dU rows (FP32, rounded to BF16; db summed in FP32 on the CUDA cores in node order) are
+// staged row-major, transposed into the K-major core-matrix layouts of the MMA operands
+// (A = Xc^T: 128 features x 128 nodes, B = dU^T: 64 outputs x 128 nodes; 8 nodes per 16-byte unit),
+// and one thread issues 8 tcgen05.mma (M=128, N=64, K=16) accumulating into 64 TMEM columns over
+// all chunks. Each warp of the first four then reads its 32 feature rows x 64 outputs.
+constexpr int kWgNodes = 128;
+constexpr int kWgSmem = kWgNodes * 2 * F * 2 /*Xc rows*/ + kWgNodes * F * 2 /*dU rows*/ + kASmem + kBSmem + 1024;
+
+__global__ void __launch_bounds__(256, 1) k_mp_wgrad_tc(int N, const float* __restrict__ dU,
+                                                        const __nv_bfloat16* __restrict__ X1,
+                                                        const __nv_bfloat16* __restrict__ X2, long long spin_limit,
+                                                        float* __restrict__ part, int* err) {
+  extern __shared__ uint8_t smem_raw[];
+  __shared__ uint64_t mbar;
+  __shared__ uint32_t tmem_slot;
+  __shared__ int mma_ok;
+  __shared__ float bsum[4][F];
+  uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  uint8_t* sA = base;                                  // A: element (feat m, node k), K-major core matrices
+  uint8_t* sB = sA + kASmem;                           // B: element (output n, node k)
+  __nv_bfloat16* rowX = reinterpret_cast<__nv_bfloat16*>(sB + kBSmem);  // [128 nodes][128 feats]
+  __nv_bfloat16* rowU = rowX + kWgNodes * 2 * F;                          // [128 nodes][64 outputs]
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_slot)),
+                 "r"(F));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  if (t == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(&mbar)), "r"(1));
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const uint32_t tmem = tmem_slot;
+  const uint32_t a_addr = smem_u32(sA), b_addr = smem_u32(sB), mbar_addr = smem_u32(&mbar);
+  uint32_t phase = 0;
+  const int per = (N + gridDim.x - 1) / gridDim.x;
+  const int n0 = blockIdx.x * per, n1 = min(N, n0 + per);
+  // db: thread (column o = t % 64, node lane t / 64) sums its nodes in order
+  float db = 0.f;
+  bool any = false, ok_all = true;
+  for (int c0 = n0; c0 < n1; c0 += kWgNodes) {
+    // stage rows (zero past the range)
+    for (int u = t; u < kWgNodes * 16; u += 256) {  // Xc: 16 chunks of 8 BF16 per node
+      const int j = u >> 4, ch = u & 15, n = c0 + j;
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (n < n1) v = ch < 8 ? __ldg(reinterpret_cast<const uint4*>(X1 + (size_t)n * F) + ch)
+                             : __ldg(reinterpret_cast<const uint4*>(X2 + (size_t)n * F) + (ch - 8));
+      reinterpret_cast<uint4*>(rowX)[u] = v;
+    }
+    for (int u = t; u < kWgNodes * F / 4; u += 256) {  // dU: float4 -> 4 BF16
+      const int j = u / (F / 4), q = u % (F / 4), n = c0 + j;
+      float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (n < n1) v = __ldg(reinterpret_cast<const float4*>(dU + (size_t)n * F) + q);
+      uint2 pk;
+      pk.x = pack_bf2(v.x, v.y);
+      pk.y = pack_bf2(v.z, v.w);
+      reinterpret_cast<uint2*>(rowU)[u] = pk;
+    }
+    {
+      const int o = t & 63, jl = t >> 6;
+      for (int j = jl; j < kWgNodes; j += 4)
+        if (c0 + j < n1) db += __ldg(&dU[(size_t)(c0 + j) * F + o]);
+    }
+    __syncthreads();
+    // transpose into the K-major operands: unit (row m, node group g) = 8 consecutive nodes
+    for (int u = t; u < 2 * F * (kWgNodes / 8); u += 256) {
+      const int m = u % (2 * F), g = u / (2 * F);
+      uint32_t w4[4];
+#pragma unroll
+      for (int h = 0; h < 4; ++h) {
+        const uint16_t lo = reinterpret_cast<const uint16_t*>(rowX)[(size_t)(8 * g + 2 * h) * 2 * F + m];
+        const uint16_t hi = reinterpret_cast<const uint16_t*>(rowX)[(size_t)(8 * g + 2 * h + 1) * 2 * F + m];
+        w4[h] = (uint32_t)lo | ((uint32_t)hi << 16);
+      }
+      *reinterpret_cast<uint4*>(sA + g * 2048 + (m >> 3) * 128 + (m & 7) * 16) = make_uint4(w4[0], w4[1], w4[2], w4[3]);
+    }
+    for (int u = t; u < F * (kWgNodes / 8); u += 256) {
+      const int m = u % F, g = u / F;
+      uint32_t w4[4];
+#pragma unroll
+      for (int h = 0; h < 4; ++h) {
+        const uint16_t lo = reinterpret_cast<const uint16_t*>(rowU)[(size_t)(8 * g + 2 * h) * F + m];
+        const uint16_t hi = reinterpret_cast<const uint16_t*>(rowU)[(size_t)(8 * g + 2 * h + 1) * F + m];
+        w4[h] = (uint32_t)lo | ((uint32_t)hi << 16);
+      }
+      *reinterpret_cast<uint4*>(sB + g * 1024 + (m >> 3) * 128 + (m & 7) * 16) = make_uint4(w4[0], w4[1], w4[2], w4[3]);
+    }
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (t == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+#pragma unroll
+      for (int j = 0; j < kWgNodes / 16; ++j) {
+        const uint64_t ad = umma_desc(a_addr + (uint32_t)(2 * j) * 2048u, 2048u, 128u);
+        const uint64_t bd = umma_desc(b_addr + (uint32_t)(2 * j) * 1024u, 1024u, 128u);
+        const uint32_t acc_flag = (any || j > 0) ? 1u : 0u;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+            "l"(ad), "l"(bd), "r"(kIdesc), "r"(acc_flag), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(mbar_addr)
+                   : "memory");
+      int ok = mbar_wait(mbar_addr, phase, spin_limit) ? 1 : 0;
+      if (!ok) {
+        if (err) atomicMin(&err[kErrTimeout], blockIdx.x);
+        mbar_wait(mbar_addr, phase, kMbarSpinLimit);
+      }
+      mma_ok = ok;
+      asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    }
+    phase ^= 1u;
+    any = true;
+    __syncthreads();  // the operands are free for the next chunk
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    if (!mma_ok) {
+      ok_all = false;
+      break;
+    }
+  }
+  // db: the four node lanes added in order
+  bsum[t >> 6][t & 63] = db;
+  __syncthreads();
+  float* p = part + (size_t)blockIdx.x * (F * 2 * F + F);
+  if (t < F) p[F * 2 * F + t] = ((bsum[0][t] + bsum[1][t]) + bsum[2][t]) + bsum[3][t];
+  // dW: warp w < 4 holds features 32 w .. 32 w + 31 (TMEM lanes) x 64 outputs (columns)
+  if (warp < 4) {
+    uint32_t v[32];
+    for (int half = 0; half < 2; ++half) {
+      if (any && ok_all) {
+        tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(half * 32), v);
+        asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+      } else {
+#pragma unroll
+        for (int j = 0; j < 32; ++j) v[j] = 0u;
+      }
+      const int k = warp * 32 + lane;
+#pragma unroll
+      for (int j = 0; j < 32; ++j) p[(half * 32 + j) * 2 * F + k] = __uint_as_float(v[j]);
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(F));
+}
+
 // Encoder backward: dU0 = dH0 (H0 > 0)
 __global__ void __launch_bounds__(256) k_mp_enc_bwd(int N, const float* __restrict__ dH,
                                                     const __nv_bfloat16* __restrict__ H0, float* __restrict__ dU) {
@@ -811,6 +967,14 @@ int tc_grid(int N, bool train, bool last) {
 }  // namespace
 
 cudaError_t mpnn_prepare_device() {
+  static bool wg_done[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev >= 0 && dev < 64 && !wg_done[dev]) {
+    const cudaError_t ew = cudaFuncSetAttribute(k_mp_wgrad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kWgSmem);
+    if (ew != cudaSuccess) return ew;
+    wg_done[dev] = true;
+  }
   cudaError_t e = set_tc_attr<false, false>();
   if (e == cudaSuccess) e = set_tc_attr<false, true>();
   if (e == cudaSuccess) e = set_tc_attr<true, false>();
@@ -945,7 +1109,8 @@ cudaError_t launch_mp_loss(int N, const double* z, const double* az, const doubl
   return cudaGetLastError();
 }
 
-cudaError_t launch_mp_backward(const MpnnGraph& g, const MpnnParams& P, MpnnWork& w, float* grad, cudaStream_t s) {
+cudaError_t launch_mp_backward(const MpnnGraph& g, const MpnnParams& P, MpnnWork& w, float* grad, long long spin_limit,
+                               int* err, cudaStream_t s) {
   const int N = g.n_nodes;
   if (N <= 0) return cudaSuccess;
   const int G = kMpPartBlocks;
@@ -960,7 +1125,7 @@ cudaError_t launch_mp_backward(const MpnnGraph& g, const MpnnParams& P, MpnnWork
   for (int l = kMpL - 1; l >= 0; --l) {
     k_mp_layer_bwd_a<<<grid_nodes(N, 4), 256, F * 2 * F * sizeof(float), s>>>(N, g.node_ptr, g.nbr, P, l, dh,
                                                                                w.G[l], w.dU, dprev, w.dAs);
-    k_mp_wgrad<2 * F><<<G, 256, 0, s>>>(N, w.dU, w.H[l], w.A[l], w.part);
+    k_mp_wgrad_tc<<<G, 256, kWgSmem, s>>>(N, w.dU, w.H[l], w.A[l], spin_limit, w.part, err);
     k_mp_layer_bwd_b<<<grid_nodes(N, 4), 256, 0, s>>>(N, g.node_ptr, g.nbr, w.dAs, dprev);
     const int off = kMpOffL0 + l * kMpLStride;
     k_mp_reduce_parts<<<grid_nodes(F * 2 * F + F, 256), 256, 0, s>>>(w.part, G, F * 2 * F + F, 0, F * 2 * F + F,

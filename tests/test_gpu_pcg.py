@@ -211,3 +211,32 @@ def test_persistent_matches_graph_path(pkg, gpu_lib, golden, precision):
     assert _rel(xp, xg) < 1e-10 and _rel(xp, g["u"]) < REL_TOL
     assert len(sp_.residual_history) == sp_.iterations + 1
     K.ctx.close()
+
+
+def test_true_residual_warning(pkg, gpu_lib, golden, oracle):
+    """The reference's warning path (solver.cpp:123-129, tests/test_pcg.cpp:130-181): with an rtol
+    below what FP64 can reach on an ill-conditioned SPD system (D A D, diagonal spread over three
+    decades), the recursive residual converges while the true residual stays above 10 rtol. The
+    GPU solver (a caller CSR on the graph path) reports it with the reference's text, as does the
+    CPU oracle on the same system; a reachable rtol gives no warning."""
+    g = golden("spd")
+    A, b = g["A120"], g["b120"]
+    n = b.size
+    rp = np.arange(0, n * n + 1, n, dtype=np.int32)
+    cols = np.tile(np.arange(n, dtype=np.int32), n)
+    K = pkg.GpuCsrMatrix.from_csr(rp, cols, A.reshape(-1))
+    rtol = 1e-19
+    s = pkg.CgJacobiSolver(pkg.SolverOptions(rtol=rtol, max_iter=5000, launch="graph"))
+    s.setup(K)
+    x = np.zeros(n)
+    st = s.solve(b, x)
+    _, so = oracle.pcg_jacobi(rp, cols, A.reshape(-1), b, rtol=rtol, max_iter=5000)
+    assert so["converged"] and so["true_rel_residual"] > 10 * rtol  # the same situation on the CPU
+    assert st.converged and st.true_rel_residual > 10 * rtol, st.message
+    assert st.warning.startswith("WARNING: CG recursive residual converged (")
+    assert "but the true residual ||b - Ax|| / ||b|| = " in st.warning and "exceeds 10 * rtol = 1e-18" in st.warning
+    s2 = pkg.CgJacobiSolver(pkg.SolverOptions(rtol=1e-10, max_iter=5000, launch="graph"))
+    s2.setup(K)
+    st2 = s2.solve(b, np.zeros(n))
+    assert st2.converged and not st2.warning
+    K.ctx.close()
