@@ -327,7 +327,9 @@ __global__ void __launch_bounds__(kLT, kLayerCtasPerSm) k_mp_layer_tc(const MpLa
   __shared__ int mma_ok;
   __shared__ float wout[2 * F], bout[2];
   __shared__ float2 ypart[kTile];
-  __shared__ int s_nbr[(kLT / 32) * kNbrCache];  // each warp's neighbour lists (the first kNbrCache entries)
+  // each warp's neighbour lists (the first kNbrCache entries; the next tile's are prefetched
+  // into the same place once the current tile's rounds are done)
+  __shared__ int s_nbr[(kLT / 32) * kNbrCache];
   uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
   uint8_t* sA = base;            // element (m, k): (k/8)*2048 + (m/8)*128 + (m%8)*16 + (k%8)*2
   uint8_t* sB = base + kASmem;   // element (n, k): (k/8)*1024 + (n/8)*128 + (n%8)*16 + (k%8)*2
@@ -363,6 +365,8 @@ __global__ void __launch_bounds__(kLT, kLayerCtasPerSm) k_mp_layer_tc(const MpLa
   uint32_t phase = 0;
   const int g = lane >> 3, c = lane & 7;    // gather: node group of the warp, feature chunk
   const int q = warp & 3, h = warp >> 2;    // epilogue: TMEM lane quarter, column half
+  int np = 0;          // lanes 0..16: node pointers of the warp's 16 nodes (+ the end) in this tile
+  bool first = true;
 
   for (int tile = blockIdx.x; tile * kTile < N; tile += gridDim.x) {
     // ---- gather: own chunk and the neighbours' mean chunk of 16 nodes per warp. The warp's 17
@@ -370,13 +374,22 @@ __global__ void __launch_bounds__(kLT, kLayerCtasPerSm) k_mp_layer_tc(const MpLa
     // one more into shared memory, so each round of four nodes is one round trip: the own
     // chunk and up to eight neighbour chunks per lane in flight.
     const int wbase = tile * kTile + warp * 16;
-    int np = 0;
-    if (lane <= 16) np = __ldg(&a.node_ptr[min(wbase + lane, N)]);
-    const int np0 = __shfl_sync(0xffffffffu, np, 0);
-    const int cnt = __shfl_sync(0xffffffffu, np, 16) - np0;
     int* wnbr = s_nbr + warp * kNbrCache;
-    for (int j = lane; j < min(cnt, kNbrCache); j += 32) wnbr[j] = __ldg(&a.nbr[np0 + j]);
+    if (first) {  // the first tile's lists come synchronously; later ones were prefetched
+      if (lane <= 16) np = __ldg(&a.node_ptr[min(wbase + lane, N)]);
+      const int f0 = __shfl_sync(0xffffffffu, np, 0);
+      const int fc = __shfl_sync(0xffffffffu, np, 16) - f0;
+      for (int j = lane; j < min(fc, kNbrCache); j += 32) wnbr[j] = __ldg(&a.nbr[f0 + j]);
+      first = false;
+    } else {
+      asm volatile("cp.async.wait_all;\n" ::: "memory");
+    }
     __syncwarp();
+    const int np0 = __shfl_sync(0xffffffffu, np, 0);
+    // the next tile's node pointers, used after this tile's rounds
+    const int wnext = (tile + (int)gridDim.x) * kTile + warp * 16;
+    int np_next = 0;
+    if (lane <= 16 && (tile + (int)gridDim.x) * kTile < N) np_next = __ldg(&a.node_ptr[min(wnext + lane, N)]);
 #pragma unroll 1
     for (int rnd = 0; rnd < 4; ++rnd) {
       const int li = rnd * 4 + g;
@@ -421,6 +434,17 @@ __global__ void __launch_bounds__(kLT, kLayerCtasPerSm) k_mp_layer_tc(const MpLa
       *reinterpret_cast<uint4*>(sA + c * 2048 + row_off) = own;
       *reinterpret_cast<uint4*>(sA + (8 + c) * 2048 + row_off) = av;
       if (TRAIN && n < N) reinterpret_cast<uint4*>(a.Aout + (size_t)n * F)[c] = av;
+    }
+    {  // prefetch the next tile's neighbour lists (asynchronous copies, done during the MMA and
+       // the epilogue); every lane has finished reading this tile's lists
+      __syncwarp();
+      const int n0 = __shfl_sync(0xffffffffu, np_next, 0);
+      const int nc = __shfl_sync(0xffffffffu, np_next, 16) - n0;
+      for (int j = lane; j < min(nc, kNbrCache); j += 32)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(smem_u32(wnbr + j)), "l"(a.nbr + n0 + j)
+                     : "memory");
+      asm volatile("cp.async.commit_group;\n" ::: "memory");
+      np = np_next;
     }
     // generic-proxy shared-memory writes -> visible to the tensor core (async proxy)
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
@@ -546,6 +570,7 @@ __global__ void __launch_bounds__(kLT, kLayerCtasPerSm) k_mp_layer_tc(const MpLa
     }
     __syncthreads();  // tensor memory and the A tile are free for the next tile
   }
+  asm volatile("cp.async.wait_all;\n" ::: "memory");  // no copy in flight when the CTA leaves
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(F));
 }
