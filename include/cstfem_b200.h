@@ -168,6 +168,9 @@ int cstg_get_stream(cstg_ctx* ctx, void** cuda_stream);
 int cstg_solve_breakdown(cstg_ctx* ctx, cstg_breakdown* out);
 void cstg_default_options(cstg_solver_options* opt);
 int cstg_version(void);
+/* The compute architecture of the library's kernels as the CUDA runtime reports it for `device`
+ * (cudaFuncGetAttributes binaryVersion: 100 for sm_100a). */
+int cstg_binary_version(int device, int* version);
 /* Bounded device waits (no reference counterpart). Every device-side wait of the library gives
  * up after a number of polls and reports CSTG_ERR_TIMEOUT (stats->status CSTG_SOLVE_TIMEOUT where
  * a solve was running) with the context still usable: the persistent solve's grid barriers

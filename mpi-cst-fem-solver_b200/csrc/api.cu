@@ -113,6 +113,12 @@ int cstg_set_stream(cstg_ctx* ctx, void* s) {
   return CSTG_OK;
 }
 
+int cstg_binary_version(int device, int* version) {
+  if (!version) return CSTG_ERR_INVALID_ARGUMENT;
+  if (cudaSetDevice(device) != cudaSuccess) return CSTG_ERR_CUDA;
+  return kernel_binary_version(version) == cudaSuccess ? CSTG_OK : CSTG_ERR_CUDA;
+}
+
 int cstg_solve_breakdown(cstg_ctx* ctx, cstg_breakdown* out) {
   BEGIN(ctx);
   if (!out) return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "solve_breakdown: null output");

@@ -447,6 +447,8 @@ cudaError_t launch_pcg_init(const PcgBuffers& w, double rtol, int max_iter, bool
 // One CG iteration: SpMV + p'Ap, x/r update + norms, p update.
 // The two phases of launch_pcg_iteration, launched separately (the instrumented solve times
 // each): q = A p with p'Ap, then x / r / p updates with their dots.
+// The architecture the library's kernels were compiled for, as the runtime reports it (100: sm_100a).
+cudaError_t kernel_binary_version(int* version);
 cudaError_t launch_spmv_phase(const PcgBuffers& w, const BlockMatrix* bm, const CsrMatrixDev* cm, cudaStream_t s);
 cudaError_t launch_vector_phase(const PcgBuffers& w, cudaStream_t s);
 cudaError_t launch_pcg_iteration(const PcgBuffers& w, const BlockMatrix* bm,

@@ -417,6 +417,13 @@ cudaError_t launch_pcg_iteration(const PcgBuffers& w, const BlockMatrix* bm,
   return cudaGetLastError();
 }
 
+cudaError_t kernel_binary_version(int* version) {
+  cudaFuncAttributes attr{};
+  const cudaError_t e = cudaFuncGetAttributes(&attr, k_pupdate);
+  if (e == cudaSuccess) *version = attr.binaryVersion;
+  return e;
+}
+
 cudaError_t launch_spmv_phase(const PcgBuffers& w, const BlockMatrix* bm, const CsrMatrixDev* cm, cudaStream_t s) {
   spmv_dispatch<true>(bm, cm, w.p, w.Ap, w.partials, w.st, s);
   return cudaGetLastError();

@@ -110,6 +110,7 @@ _SIGS = {
     "cstg_last_error": (C.c_char_p, [_vp]),
     "cstg_set_stream": (C.c_int, [_vp, _vp]),
     "cstg_get_stream": (C.c_int, [_vp, C.POINTER(_vp)]),
+    "cstg_binary_version": (C.c_int, [C.c_int, C.POINTER(C.c_int)]),
     "cstg_solve_breakdown": (C.c_int, [_vp, C.POINTER(Breakdown)]),
     "cstg_default_options": (None, [C.POINTER(SolverOptions)]),
     "cstg_set_mesh": (C.c_int, [_vp, C.c_int, _vp, C.c_int, _vp]),

@@ -149,8 +149,10 @@ def test_batch_rejects_coupled_systems(pkg, small):
 
 def test_batch_64_plates_4_load_cases(pkg, oracle, gpu_lib):
     """The uneven batch workload: 64 seeded plates (n_r 20..200, n_theta = 2 n_r), 4 load cases,
-    one persistent launch. Every system converged on the host-recomputed FP64 true residual;
-    the smallest plate checked against the oracle."""
+    one persistent launch. Every system converged on the host-recomputed FP64 true residual; a
+    stratified sample of 8 plates by size (the smallest and the largest included) checked against
+    the oracle's FP64 Jacobi-PCG: every load case of the smallest and the largest, one case each
+    (in turn) of the six between."""
     specs = pkg.plate.random_batch(count=64, seed=2026)
     batch = pkg.build_batch(specs)
     solver = pkg.BatchSolver(pkg.SolverOptions(precision="mixed", max_iter=200000))
@@ -159,9 +161,14 @@ def test_batch_64_plates_4_load_cases(pkg, oracle, gpu_lib):
     assert np.all(sol.converged), sol.status
     host = _host_true_residuals(batch, K, solver.b, sol.x)
     assert np.all(host <= 1.0001e-10), host.max()
-    s = int(np.argmin(batch.node_offsets[1:] - batch.node_offsets[:-1]))
-    rp, cols, Kel, bs = _oracle_plate(oracle, pkg, specs[s], pkg.plate.LOAD_CASES)
-    for q in range(4):
-        x_ref, _ = oracle.pcg_jacobi(rp, cols, Kel, bs[q], rtol=1e-10, max_iter=100000)
-        assert _rel(sol.x[q][batch.dof_range(s)], x_ref) < REL_TOL
+    sizes = batch.node_offsets[1:] - batch.node_offsets[:-1]
+    order = np.argsort(sizes, kind="stable")
+    sample = [int(order[int(round(k * (len(order) - 1) / 7))]) for k in range(8)]
+    assert sample[0] == int(order[0]) and sample[-1] == int(order[-1]) and len(set(sample)) == 8
+    for i, s in enumerate(sample):
+        rp, cols, Kel, bs = _oracle_plate(oracle, pkg, specs[s], pkg.plate.LOAD_CASES)
+        cases = range(4) if i in (0, 7) else [i % 4]
+        for q in cases:
+            x_ref, _ = oracle.pcg_jacobi(rp, cols, Kel, bs[q], rtol=1e-10, max_iter=100000)
+            assert _rel(sol.x[q][batch.dof_range(s)], x_ref) < REL_TOL, (s, q)
     solver.close()

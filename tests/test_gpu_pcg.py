@@ -240,3 +240,11 @@ def test_true_residual_warning(pkg, gpu_lib, golden, oracle):
     st2 = s2.solve(b, np.zeros(n))
     assert st2.converged and not st2.warning
     K.ctx.close()
+
+
+def test_kernels_are_sm100a(pkg, gpu_lib):
+    """The CUDA runtime reports the loaded kernels' architecture as sm_100 (binaryVersion 100)."""
+    import ctypes as C
+    v = C.c_int(0)
+    assert gpu_lib.cstg_binary_version(0, C.byref(v)) == pkg.native.OK
+    assert v.value == 100

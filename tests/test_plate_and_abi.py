@@ -70,10 +70,12 @@ def test_library_exports_every_declared_symbol(pkg, gpu_lib):
     assert set(syms) <= exported
 
 
-def test_library_is_sm100a(pkg, gpu_lib):
-    out = subprocess.run(["/usr/local/cuda/bin/cuobjdump", "--list-elf", pkg.native.library_path()],
-                         capture_output=True, text=True).stdout
-    assert "sm_100a" in out
+def test_library_is_built_for_sm100a_only(pkg):
+    """The build compiles every source for sm_100a and nothing else (the runtime check of the
+    loaded kernels' architecture is tests/test_gpu_pcg.py::test_kernels_are_sm100a)."""
+    flags = pkg.build._flags()
+    assert flags[flags.index("-gencode") + 1] == "arch=compute_100a,code=sm_100a"
+    assert flags.count("-gencode") == 1 and not any(f.startswith("-arch") for f in flags)
 
 
 def test_host_only_calls(pkg, gpu_lib):
