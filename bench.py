@@ -84,6 +84,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the comparison solves")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-solve measurement")
+    ap.add_argument("--no-large", action="store_true",
+                    help="skip the large plate (n_r=800 x n_theta=2500): learned + mixed against plain FP64")
     ap.add_argument("--only", choices=["spmv", "solve", "batch", "learned", "amg"], default=None,
                     help="profiling modes (one JSON line each): `spmv` --reps SpMV launches, `solve` one "
                          "full step, `batch` the 64-plate x 4-load-case batched solve, `learned` the "
@@ -404,6 +406,43 @@ def run_batch(a, pkg, sweep_shapes: bool = False, reps: int = 3):
     return out
 
 
+# ---- the large plate (the config's n_r = 800 x n_theta = 2500 O-grid) --------------------------------
+
+def run_large(a, pkg, n_r=800, n_t=2500):
+    """The learned cycle in mixed precision on the large plate against plain FP64 Jacobi-PCG on the
+    same GPU (solve times, iterations, the two solutions' difference, the SCF at the hole)."""
+    import torch
+    m = pkg.plate.quarter_plate(n_r, n_t)
+    D = pkg.constitutive_matrix(1.0, 0.3)
+    ctx = pkg.Context(0)
+    K = pkg.build_stiffness_pattern(m, ctx=ctx)
+    pkg.assemble_stiffness(m, D, 1.0, K)
+    b = torch.zeros(m.num_dofs, dtype=torch.float64, device="cuda")
+    pkg.add_traction(K, m.boundary_edges["right"], 1.0, 1.0, 0.0, b)
+    pkg.apply_dirichlet(pkg.plate.symmetry_dirichlet(m), K, b)
+    out = {"workload": f"quarter plate O-grid n_r={n_r} x n_theta={n_t}, {m.num_dofs} DOFs, {K.nnz()} nnz"}
+    xs = {}
+    for name, kw in (("learned_mixed", dict(precision="mixed", preconditioner="learned_mg")),
+                     ("plain_fp64", dict())):
+        s = pkg.CgJacobiSolver(pkg.SolverOptions(rtol=1e-10, max_iter=400000, true_residual_stop=True, **kw))
+        s.setup(K)
+        if kw.get("preconditioner") == "learned_mg":
+            pkg.learned.setup(K, pkg.learned.load_weights(mode="cycle"), pkg.learned.node_material(D, m.num_nodes))
+            s.solve(b, torch.zeros_like(b))  # warm-up: hierarchy, graphs
+        x = torch.zeros_like(b)
+        st = s.solve(b, x)
+        xs[name] = x
+        out[name] = {"solve_s": st.solve_seconds, "iterations": st.iterations,
+                     "true_rel_residual": st.true_rel_residual, "converged": st.converged}
+    out["speedup_solve"] = out["plain_fp64"]["solve_s"] / out["learned_mixed"]["solve_s"]
+    out["x_rel_learned_vs_plain_fp64"] = float(torch.linalg.vector_norm(xs["learned_mixed"] - xs["plain_fp64"]) /
+                                               torch.linalg.vector_norm(xs["plain_fp64"]))
+    strs = pkg.compute_element_stresses(ctx, xs["learned_mixed"].cpu().numpy(), 1.0, 0.3)
+    out["scf"] = float(pkg.scf_at_hole(strs, 1.0)[0])
+    ctx.close()
+    return out
+
+
 # ---- our arm --------------------------------------------------------------------------------------
 
 def run_ours(a, dist: Dist):
@@ -531,6 +570,8 @@ def run_ours(a, dist: Dist):
         line["cpu_baseline"] = cpu_baseline_entry(s, n, rec)
     if dist.rank == 0 and not a.no_batch and a.gpus == 1:
         line["batch"] = run_batch(a, pkg)
+    if dist.rank == 0 and not a.no_large and a.gpus == 1:
+        line["large_plate"] = run_large(a, pkg)
     ctx.close()
     if dist.rank == 0:
         print(json.dumps(line))
