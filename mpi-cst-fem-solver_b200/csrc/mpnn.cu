@@ -159,13 +159,13 @@ __global__ void k_mp_smoother_weights(int n, const double* __restrict__ invd, co
 
 // ---- encoder: H0 = relu(W_in X + b_in) ------------------------------------------------------------
 
-// Eight threads per node, thread c computing features 8c..8c+7; the weights sit in shared memory
-// transposed ([input][feature], a thread's eight features in two float4 reads). Four nodes per
-// thread and step, all four nodes' inputs loaded before any is used; a warp writes four whole
-// 128-byte rows per node step. Each feature is the same chain of FMAs in the same order for
-// every launch shape.
+// Eight threads per node, thread c computing features 8c..8c+7 from the weights in shared
+// memory (transposed: [input][feature], a thread's eight features in two float4 reads); one node
+// per thread group and no loop, so nothing is held across nodes and the kernel runs at full
+// occupancy: the loads of many nodes are in flight at once. A warp writes four whole 128-byte
+// rows. Each feature is the same chain of FMAs in the same order for every launch shape.
 template <bool TRAIN>
-__global__ void __launch_bounds__(256, 2) k_mp_encode(int N, const double* __restrict__ r, const double* rr,
+__global__ void __launch_bounds__(256) k_mp_encode(int N, const double* __restrict__ r, const double* rr,
                                                    double inv_n, const float* __restrict__ sf, MpnnParams P,
                                                    const int* skip, __nv_bfloat16* __restrict__ H0,
                                                    __nv_bfloat16* __restrict__ Xout) {
@@ -179,70 +179,43 @@ __global__ void __launch_bounds__(256, 2) k_mp_encode(int N, const double* __res
   for (int i = threadIdx.x; i < F; i += blockDim.x) bs[i] = P.pf[kMpOffBin + i];
   __syncthreads();
   const int c = threadIdx.x & 7;
+  const int n = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 3);
+  if (n >= N) return;
   const double s = sqrt(*rr * inv_n);
   const double sd = s > 0.0 ? s : 1.0;
-  const int per_step = (gridDim.x * blockDim.x) >> 3;
-  auto inputs = [&](int n, float (&x)[kMpIn]) {
-    const double2 rn = reinterpret_cast<const double2*>(r)[n];
-    const float2* sfn = reinterpret_cast<const float2*>(sf + (size_t)n * 6);
-    const float2 a0 = sfn[0], a1 = sfn[1], a2 = sfn[2];
-    x[0] = (float)(rn.x / sd);
-    x[1] = (float)(rn.y / sd);
-    x[2] = a0.x;
-    x[3] = a0.y;
-    x[4] = a1.x;
-    x[5] = a1.y;
-    x[6] = a2.x;
-    x[7] = a2.y;
+  const double2 rn = reinterpret_cast<const double2*>(r)[n];
+  const float2* sfn = reinterpret_cast<const float2*>(sf + (size_t)n * 6);
+  const float2 a0 = sfn[0], a1 = sfn[1], a2 = sfn[2];
+  float x[kMpIn] = {(float)(rn.x / sd), (float)(rn.y / sd), a0.x, a0.y, a1.x, a1.y, a2.x, a2.y};
 #pragma unroll
-    for (int k = 0; k < kMpIn; ++k) x[k] = __bfloat162float(__float2bfloat16_rn(x[k]));
-  };
-  auto emit = [&](int n, const float (&x)[kMpIn]) {
-    if (TRAIN && c == 0) {
-      uint4 xv;
-      xv.x = pack_bf2(x[0], x[1]);
-      xv.y = pack_bf2(x[2], x[3]);
-      xv.z = pack_bf2(x[4], x[5]);
-      xv.w = pack_bf2(x[6], x[7]);
-      reinterpret_cast<uint4*>(Xout)[n] = xv;
-    }
-    const float4 b0 = *reinterpret_cast<const float4*>(&bs[c * 8]);
-    const float4 b1 = *reinterpret_cast<const float4*>(&bs[c * 8 + 4]);
-    float u[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+  for (int k = 0; k < kMpIn; ++k) x[k] = __bfloat162float(__float2bfloat16_rn(x[k]));
+  if (TRAIN && c == 0) {
+    uint4 xv;
+    xv.x = pack_bf2(x[0], x[1]);
+    xv.y = pack_bf2(x[2], x[3]);
+    xv.z = pack_bf2(x[4], x[5]);
+    xv.w = pack_bf2(x[6], x[7]);
+    reinterpret_cast<uint4*>(Xout)[n] = xv;
+  }
+  const float4 b0 = *reinterpret_cast<const float4*>(&bs[c * 8]);
+  const float4 b1 = *reinterpret_cast<const float4*>(&bs[c * 8 + 4]);
+  float u[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
 #pragma unroll
-    for (int k = 0; k < kMpIn; ++k) {
-      const float4 w0 = *reinterpret_cast<const float4*>(&wt[k][c * 8]);
-      const float4 w1 = *reinterpret_cast<const float4*>(&wt[k][c * 8 + 4]);
-      u[0] = fmaf(w0.x, x[k], u[0]);
-      u[1] = fmaf(w0.y, x[k], u[1]);
-      u[2] = fmaf(w0.z, x[k], u[2]);
-      u[3] = fmaf(w0.w, x[k], u[3]);
-      u[4] = fmaf(w1.x, x[k], u[4]);
-      u[5] = fmaf(w1.y, x[k], u[5]);
-      u[6] = fmaf(w1.z, x[k], u[6]);
-      u[7] = fmaf(w1.w, x[k], u[7]);
-    }
-    reinterpret_cast<uint4*>(H0 + (size_t)n * F)[c] =
-        make_uint4(pack_bf2(fmaxf(u[0], 0.f), fmaxf(u[1], 0.f)), pack_bf2(fmaxf(u[2], 0.f), fmaxf(u[3], 0.f)),
-                   pack_bf2(fmaxf(u[4], 0.f), fmaxf(u[5], 0.f)), pack_bf2(fmaxf(u[6], 0.f), fmaxf(u[7], 0.f)));
-  };
-  int n = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
-  for (; n + 3 * per_step < N; n += 4 * per_step) {
-    float x0[kMpIn], x1[kMpIn], x2[kMpIn], x3[kMpIn];
-    inputs(n, x0);
-    inputs(n + per_step, x1);
-    inputs(n + 2 * per_step, x2);
-    inputs(n + 3 * per_step, x3);
-    emit(n, x0);
-    emit(n + per_step, x1);
-    emit(n + 2 * per_step, x2);
-    emit(n + 3 * per_step, x3);
+  for (int k = 0; k < kMpIn; ++k) {
+    const float4 w0 = *reinterpret_cast<const float4*>(&wt[k][c * 8]);
+    const float4 w1 = *reinterpret_cast<const float4*>(&wt[k][c * 8 + 4]);
+    u[0] = fmaf(w0.x, x[k], u[0]);
+    u[1] = fmaf(w0.y, x[k], u[1]);
+    u[2] = fmaf(w0.z, x[k], u[2]);
+    u[3] = fmaf(w0.w, x[k], u[3]);
+    u[4] = fmaf(w1.x, x[k], u[4]);
+    u[5] = fmaf(w1.y, x[k], u[5]);
+    u[6] = fmaf(w1.z, x[k], u[6]);
+    u[7] = fmaf(w1.w, x[k], u[7]);
   }
-  for (; n < N; n += per_step) {
-    float x0[kMpIn];
-    inputs(n, x0);
-    emit(n, x0);
-  }
+  reinterpret_cast<uint4*>(H0 + (size_t)n * F)[c] =
+      make_uint4(pack_bf2(fmaxf(u[0], 0.f), fmaxf(u[1], 0.f)), pack_bf2(fmaxf(u[2], 0.f), fmaxf(u[3], 0.f)),
+                 pack_bf2(fmaxf(u[4], 0.f), fmaxf(u[5], 0.f)), pack_bf2(fmaxf(u[6], 0.f), fmaxf(u[7], 0.f)));
 }
 
 // ---- message-passing layer on the tensor cores ----------------------------------------------------
@@ -1042,11 +1015,7 @@ cudaError_t launch_mp_forward(const MpnnGraph& g, const MpnnParams& P, const dou
   const int N = g.n_nodes;
   if (N <= 0) return cudaSuccess;
   const double inv_n = 1.0 / (2.0 * N);
-  int dev = 0, sms = kSMs;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  // one wave of the encoder (2 blocks of 256 per SM), at most 8 threads per node
-  const int ge = (int)std::max<long long>(1, std::min<long long>(2LL * sms, (8LL * N + 255) / 256));
+  const int ge = (int)((8LL * N + 255) / 256);  // eight threads per node, one node each
   if (train)
     k_mp_encode<true><<<ge, 256, 0, s>>>(N, r, rr, inv_n, sf, P, skip, w.H[0], w.X);
   else
@@ -1094,10 +1063,7 @@ cudaError_t launch_mp_stage(const MpnnGraph& g, const MpnnParams& P, int stage, 
   if (N <= 0) return cudaSuccess;
   const double inv_n = 1.0 / (2.0 * N);
   if (stage == 0) {
-    int dev = 0, sms = kSMs;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int ge = (int)std::max<long long>(1, std::min<long long>(2LL * sms, (8LL * N + 255) / 256));
+    const int ge = (int)((8LL * N + 255) / 256);
     k_mp_encode<false><<<ge, 256, 0, s>>>(N, r, rr, inv_n, sf, P, nullptr, w.H[0], nullptr);
   } else {
     MpLayerArgs a{};
