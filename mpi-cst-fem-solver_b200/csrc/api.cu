@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -50,6 +51,8 @@ cstg_ctx* cstg_create(int device, int* status) {
   }
   auto* ctx = new cstg_ctx;
   ctx->device = device;
+  const char* gather = std::getenv("CSTG_MP_GATHER");
+  ctx->lp_plan_on = !(gather && std::strcmp(gather, "rows") == 0);
   bool ok = cudaStreamCreateWithFlags(&ctx->own, cudaStreamNonBlocking) == cudaSuccess &&
             cudaEventCreate(&ctx->ev0) == cudaSuccess && cudaEventCreate(&ctx->ev1) == cudaSuccess &&
             cudaMallocHost(&ctx->h_err, sizeof(int) * kErrSlots) == cudaSuccess &&
@@ -89,7 +92,8 @@ void cstg_destroy(cstg_ctx* ctx) {
                    &ctx->bat_in,  &ctx->bat_out, &ctx->lp_p32, &ctx->lp_pb,   &ctx->lp_pf,
                    &ctx->lp_sf,   &ctx->lp_h0,  &ctx->lp_h1,    &ctx->lp_sc,    &ctx->lp_z,
                    &ctx->tr_con,  &ctx->tr_cnt, &ctx->tr_ptr,   &ctx->tr_cur,   &ctx->tr_rec,
-                   &ctx->lm_winvd, &ctx->fcg_ring, &ctx->lp_mat};
+                   &ctx->lm_winvd, &ctx->fcg_ring, &ctx->lp_mat, &ctx->lp_plan_hdr, &ctx->lp_plan_runs,
+                   &ctx->lp_plan_local};
   for (DevBuf* b : all) free_buf(*b);
   for (int j = 0; j < kFcgMaxHist; ++j) {
     free_buf(ctx->fcg_ph[j]);
@@ -244,6 +248,7 @@ int cstg_build_pattern(cstg_ctx* ctx, int64_t* nnz_out) {
   else
     CK(cudaMemsetAsync(ctx->row_ptr.p, 0, sizeof(int), ctx->stream));
   ctx->kind = 1;
+  ctx->pattern_count++;
   ctx->n_rows = 2 * N;
   ctx->nnz = 4 * nb;
   ctx->has_values = ctx->setup_done = false;

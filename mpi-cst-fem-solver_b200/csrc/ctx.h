@@ -114,6 +114,11 @@ struct cstg_ctx {
   // built for the hierarchy of setup `lm_winvd_for`
   DevBuf lm_winvd;
   unsigned long long lm_winvd_for = ~0ull;
+  // the network layers' gather plan for the node pattern of `lp_plan_for` (the pattern count)
+  DevBuf lp_plan_hdr, lp_plan_runs, lp_plan_local;
+  unsigned long long pattern_count = 0;  // bumped by every cstg_build_pattern
+  unsigned long long lp_plan_for = ~0ull;
+  bool lp_plan_on = true;  // CSTG_MP_GATHER=rows turns the plan off (every tile gathers row by row)
   // truncated flexible CG: ring of earlier directions and their A-products, ring state
   DevBuf fcg_ph[kFcgMaxHist], fcg_qh[kFcgMaxHist], fcg_ring;
 

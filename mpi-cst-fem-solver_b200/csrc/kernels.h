@@ -163,7 +163,7 @@ cudaError_t launch_batch_check(int N, int n_sys, const int* sys_node, const int*
 
 // mpnn.cu: the learned preconditioner's network (F = 64 features, 3 message-passing layers).
 // Packed parameter vector: W_in[64][8], b_in[64], (W_l[64][128], b_l[64]) x 3, W_out[2][64], b_out[2].
-constexpr int kMpF = 64, kMpIn = 8, kMpL = 3;
+constexpr int kMpF = 64, kMpIn = 8, kMpL = 3, kMpTile = 128;  // features, inputs, layers, nodes per tile
 constexpr int kMpOffWin = 0, kMpOffBin = kMpF * kMpIn, kMpOffL0 = kMpOffBin + kMpF;
 constexpr int kMpLStride = kMpF * 2 * kMpF + kMpF;
 constexpr int kMpOffWout = kMpOffL0 + kMpL * kMpLStride, kMpOffBout = kMpOffWout + 2 * kMpF;
@@ -176,11 +176,26 @@ struct MpnnParams {  // device copies of the packed parameters
   const float* pf = nullptr;          // FP32 (biases are read from here)
 };
 
+// Per-tile gather plan of the message-passing layers (built on the GPU from the pattern, once
+// per matrix): for each tile of 128 consecutive nodes, the rows its nodes read (their own and
+// their neighbours') as at most kPlanMaxRuns runs of consecutive nodes holding at most
+// kPlanMaxUnion rows, and per node the positions of its own row and of its neighbours' rows
+// (ascending pattern order) in that union. A tile that does not fit is marked and gathered row by
+// row instead.
+constexpr int kPlanMaxRuns = 8, kPlanMaxUnion = 416, kPlanMaxLocal = 7, kPlanSpan = 4096;
+struct MpTilePlan {
+  const int4* hdr = nullptr;    // [tiles]: (runs, union rows, fallback, 0)
+  const int2* runs = nullptr;   // [tiles][kPlanMaxRuns]: (first node, rows)
+  const uint4* local = nullptr; // [nodes]: 8 uint16: [0] own row, [1..deg] neighbours, 0xFFFF unused
+};
 struct MpnnGraph {  // the node-block pattern (self included; the network skips self)
   int n_nodes = 0;
   const int* node_ptr = nullptr;
   const int* nbr = nullptr;
+  MpTilePlan plan;  // optional (hdr null: every tile gathers row by row)
 };
+cudaError_t launch_mp_tile_plan(int N, const int* node_ptr, const int* nbr, int4* hdr, int2* runs, uint4* local,
+                                cudaStream_t s);
 
 struct MpnnWork {  // activations (training keeps every layer; inference ping-pongs H[0]/H[1])
   __nv_bfloat16* H[kMpL + 1] = {};

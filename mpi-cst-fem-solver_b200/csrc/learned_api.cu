@@ -27,11 +27,33 @@ MpnnParams params_view(cstg_ctx* ctx) {
   return P;
 }
 
+// The layers' gather plan for the current node pattern (built once per pattern): per tile of 128
+// nodes the runs of consecutive rows its nodes read, and per node the slots of its own and its
+// neighbours' rows in that union.
+int plan_ready(cstg_ctx* ctx) {
+  if (!ctx->lp_plan_on || ctx->lp_plan_for == ctx->pattern_count) return CSTG_OK;
+  const int N = ctx->n_nodes;
+  const int tiles = std::max((N + kMpTile - 1) / kMpTile, 1);
+  ENSURE(ctx->lp_plan_hdr, sizeof(int4) * (size_t)tiles);
+  ENSURE(ctx->lp_plan_runs, sizeof(int2) * (size_t)tiles * kPlanMaxRuns);
+  ENSURE(ctx->lp_plan_local, sizeof(uint4) * (size_t)std::max(N, 1));
+  if (N)
+    CK(launch_mp_tile_plan(N, buf_ptr<int>(ctx->node_ptr), buf_ptr<int>(ctx->bnbr), buf_ptr<int4>(ctx->lp_plan_hdr),
+                           buf_ptr<int2>(ctx->lp_plan_runs), buf_ptr<uint4>(ctx->lp_plan_local), ctx->stream));
+  ctx->lp_plan_for = ctx->pattern_count;
+  return CSTG_OK;
+}
+
 MpnnGraph graph_view(cstg_ctx* ctx) {
   MpnnGraph g;
   g.n_nodes = ctx->n_nodes;
   g.node_ptr = buf_ptr<int>(ctx->node_ptr);
   g.nbr = buf_ptr<int>(ctx->bnbr);
+  if (ctx->lp_plan_on && ctx->lp_plan_for == ctx->pattern_count) {
+    g.plan.hdr = buf_ptr<int4>(ctx->lp_plan_hdr);
+    g.plan.runs = buf_ptr<int2>(ctx->lp_plan_runs);
+    g.plan.local = buf_ptr<uint4>(ctx->lp_plan_local);
+  }
   return g;
 }
 
@@ -445,11 +467,13 @@ int cstg_learned_setup(cstg_ctx* ctx, const float* params, const float* node_mat
   int rc = upload_params(ctx, params);
   if (rc) return rc;
   // per-node static inputs on the GPU: diagonal / its mean, coordinates / plate size, material
-  ENSURE(ctx->lp_sf, sizeof(float) * (size_t)std::max(N, 1) * 6);
+  ENSURE(ctx->lp_sf, sizeof(float) * (size_t)std::max(N, 1) * 6 + 16);  // + the encoder's copy rounding
   ENSURE(ctx->lp_mat, sizeof(float) * (size_t)std::max(N, 1) * 2);
   ENSURE(ctx->lp_sc, sizeof(MpScratch));
   // the reductions' tickets must start at zero (a fresh allocation may hold old contents)
   CK(cudaMemsetAsync(ctx->lp_sc.p, 0, sizeof(MpScratch), ctx->stream));
+  rc = plan_ready(ctx);
+  if (rc) return rc;
   if (N) {
     CK(cudaMemcpyAsync(ctx->lp_mat.p, node_material, sizeof(float) * 2 * (size_t)N, cudaMemcpyHostToDevice,
                        ctx->stream));

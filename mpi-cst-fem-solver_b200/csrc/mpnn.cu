@@ -8,13 +8,14 @@
 //   Y    = W_out H3 + b_out                                                FP32 [N][2]
 // Weights are BF16 (biases FP32); every product accumulates in FP32.
 //
-// The three message-passing layers run on the 5th-generation tensor cores: a CTA of 128
-// threads owns a tile of 128 nodes, gathers each node's own row and the mean of its
-// neighbours' rows into shared memory as the A operand ([128 nodes] x [128 = own 64 | mean 64],
-// K-major, no swizzle), holds W_l as the B operand, and one thread issues eight
-// tcgen05.mma.kind::f16 (M=128, N=64, K=16) into a 64-column FP32 accumulator in tensor memory.
-// tcgen05.commit signals an mbarrier; each warp then reads its 32 accumulator lanes
-// (tcgen05.ld.32x32b) and applies bias, ReLU and the residual add in the epilogue.
+// The three message-passing layers run on the 5th-generation tensor cores: a CTA owns a tile of
+// 128 nodes at a time, builds each node's own row and the mean of its neighbours' rows in shared
+// memory as the A operand ([128 nodes] x [128 = own 64 | mean 64], K-major, no swizzle), holds
+// W_l as the B operand, and one thread issues eight tcgen05.mma.kind::f16 (M=128, N=64, K=16)
+// into a 64-column FP32 accumulator in tensor memory. tcgen05.commit signals an mbarrier; each
+// warp then reads its 32 accumulator lanes (tcgen05.ld.32x32b) and applies bias, ReLU and the
+// residual add in the epilogue. On patterns with a gather plan a producer warp brings each
+// tile's rows into shared memory with bulk copies ahead of the tile warps.
 //
 // Training: the forward pass also stores the inputs X, the aggregates A_l and the ReLU outputs
 // G_l; the backward pass (CUDA cores, FP32 accumulation of BF16 operands) produces weight
@@ -25,6 +26,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 
 #include "common.cuh"
 #include "kernels.h"
@@ -35,6 +37,7 @@ namespace {
 
 constexpr int F = kMpF;
 constexpr int kTile = 128;             // nodes per tensor-core tile (the MMA's M)
+static_assert(kTile == kMpTile, "the gather plan is built per tensor-core tile");
 constexpr int kASmem = kTile * 2 * F * 2;  // A operand bytes (128 x 128 BF16)
 constexpr int kBSmem = F * 2 * F * 2;      // B operand bytes (64 x 128 BF16)
 constexpr long long kMbarSpinLimit = kMpMbarSpinDefault;  // bounded wait for the MMA (far above its ~us)
@@ -149,6 +152,109 @@ __global__ void k_mp_static(int N, const double* __restrict__ invd, const double
   }
 }
 
+// ---- the layers' gather plan: one CTA per tile of 128 nodes -------------------------------------
+
+__global__ void __launch_bounds__(256) k_mp_tile_plan(int N, const int* __restrict__ node_ptr,
+                                                      const int* __restrict__ nbr, int4* __restrict__ hdr,
+                                                      int2* __restrict__ runs, uint4* __restrict__ local) {
+  constexpr int W = kPlanSpan / 32;
+  __shared__ unsigned bits[W];
+  __shared__ int wpre[W + 1], spre[W + 1], epre[W + 1];
+  __shared__ int s_lo, s_hi, s_fail;
+  __shared__ int rs[kPlanMaxRuns], re[kPlanMaxRuns];
+  const int t = threadIdx.x, tile = blockIdx.x;
+  const int a = tile * kTile, b = min(N, a + kTile);
+  if (t == 0) {
+    s_lo = INT_MAX;
+    s_hi = -1;
+    s_fail = 0;
+  }
+  for (int w = t; w < W; w += blockDim.x) bits[w] = 0u;
+  __syncthreads();
+  const int e0 = node_ptr[a], e1 = node_ptr[b];
+  int lo = INT_MAX, hi = -1;
+  for (int e = e0 + t; e < e1; e += blockDim.x) {
+    const int v = nbr[e];
+    lo = min(lo, v);
+    hi = max(hi, v);
+  }
+  if (lo <= hi) {
+    atomicMin(&s_lo, lo);
+    atomicMax(&s_hi, hi);
+  }
+  if (t < b - a) {  // every node lists itself (first the own row) and at most kPlanMaxLocal others
+    const int d = node_ptr[a + t + 1] - node_ptr[a + t];
+    if (d < 1 || d - 1 > kPlanMaxLocal) s_fail = 1;
+  }
+  __syncthreads();
+  const int wlo = s_lo;
+  if (s_fail || s_hi - wlo + 1 > kPlanSpan) {
+    if (t == 0) hdr[tile] = make_int4(0, 0, 1, 0);
+    return;
+  }
+  for (int e = e0 + t; e < e1; e += blockDim.x) {
+    const int d = nbr[e] - wlo;
+    atomicOr(&bits[d >> 5], 1u << (d & 31));
+  }
+  __syncthreads();
+  if (t == 0) {  // word prefix counts of the set bits, the run starts and the run ends
+    int c = 0, cs = 0, ce = 0;
+    for (int w = 0; w < W; ++w) {
+      const unsigned x = bits[w];
+      const unsigned prev_top = w > 0 ? bits[w - 1] >> 31 : 0u;
+      const unsigned next_low = w + 1 < W ? (bits[w + 1] & 1u) << 31 : 0u;
+      const unsigned st = x & ~((x << 1) | prev_top);
+      const unsigned en = x & ~((x >> 1) | next_low);
+      wpre[w] = c;
+      spre[w] = cs;
+      epre[w] = ce;
+      c += __popc(x);
+      cs += __popc(st);
+      ce += __popc(en);
+    }
+    wpre[W] = c;
+    spre[W] = cs;
+    epre[W] = ce;
+    if (c > kPlanMaxUnion || cs > kPlanMaxRuns) s_fail = 1;
+  }
+  __syncthreads();
+  if (s_fail) {
+    if (t == 0) hdr[tile] = make_int4(0, 0, 1, 0);
+    return;
+  }
+  for (int w = t; w < W; w += blockDim.x) {  // the runs' first and last nodes, in order
+    const unsigned x = bits[w];
+    const unsigned prev_top = w > 0 ? bits[w - 1] >> 31 : 0u;
+    const unsigned next_low = w + 1 < W ? (bits[w + 1] & 1u) << 31 : 0u;
+    unsigned st = x & ~((x << 1) | prev_top), en = x & ~((x >> 1) | next_low);
+    for (int j = spre[w]; st; ++j, st &= st - 1) rs[j] = wlo + 32 * w + __ffs(st) - 1;
+    for (int j = epre[w]; en; ++j, en &= en - 1) re[j] = wlo + 32 * w + __ffs(en) - 1;
+  }
+  __syncthreads();
+  const int nruns = spre[W];
+  if (t < kPlanMaxRuns)
+    runs[(size_t)tile * kPlanMaxRuns + t] = t < nruns ? make_int2(rs[t], re[t] - rs[t] + 1) : make_int2(0, 0);
+  if (t == 0) hdr[tile] = make_int4(nruns, wpre[W], 0, 0);
+  if (t < b - a) {  // the node's own row first, then its neighbours in pattern order
+    const int n = a + t;
+    auto rank = [&](int v) {
+      const int d = v - wlo;
+      return wpre[d >> 5] + __popc(bits[d >> 5] & ((1u << (d & 31)) - 1u));
+    };
+    uint16_t slot[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) slot[j] = 0xFFFFu;
+    slot[0] = (uint16_t)rank(n);
+    int k = 1;
+    for (int e = node_ptr[n]; e < node_ptr[n + 1]; ++e) {
+      const int v = nbr[e];
+      if (v != n) slot[k++] = (uint16_t)rank(v);
+    }
+    local[n] = make_uint4((uint32_t)slot[0] | ((uint32_t)slot[1] << 16), (uint32_t)slot[2] | ((uint32_t)slot[3] << 16),
+                          (uint32_t)slot[4] | ((uint32_t)slot[5] << 16), (uint32_t)slot[6] | ((uint32_t)slot[7] << 16));
+  }
+}
+
 // ---- the learned cycle's post-smoother weights: out = factor / lambda_max * D^-1 ------------------
 
 __global__ void k_mp_smoother_weights(int n, const double* __restrict__ invd, const double* lam, double factor,
@@ -158,75 +264,140 @@ __global__ void k_mp_smoother_weights(int n, const double* __restrict__ invd, co
 }
 
 // ---- encoder: H0 = relu(W_in X + b_in) ------------------------------------------------------------
+//
+// Persistent CTAs over chunks of kEncChunk consecutive nodes. Thread 0 brings a chunk's inputs
+// (r: 16 B per node, the static inputs: 24 B per node, both contiguous) into shared memory with
+// two bulk copies completing on an mbarrier, one chunk ahead of the compute (two stages), so whole
+// chunks of loads are in flight rather than a few per thread. Eight threads per node: thread c
+// holds the weights and biases of features 8c..8c+7 in registers (64 + 8, loaded once), forms
+// input c of its node (r / s for c < 2, a static input otherwise), rounds it to BF16 and takes
+// the other seven from its group by shuffles. A warp writes four whole 128-byte rows. Each
+// feature is the same chain of FMAs in the same order for every launch shape. The static
+// inputs' buffer holds 16 bytes past its 24 N (a ragged last chunk's copy is rounded up to 16
+// bytes).
+constexpr int kEncChunk = 256;                              // nodes per chunk
+constexpr int kEncT = 256;                                  // threads of the encoder
+constexpr int kEncStage = kEncChunk * 16 + kEncChunk * 24;  // one stage: r, then the static inputs
+constexpr int kEncCtasPerSm = 2;
 
-// Eight threads per node, thread c computing features 8c..8c+7 from the weights in shared
-// memory (transposed: [input][feature], a thread's eight features in two float4 reads); one node
-// per thread group and no loop, so nothing is held across nodes and the kernel runs at full
-// occupancy: the loads of many nodes are in flight at once. A warp writes four whole 128-byte
-// rows. Each feature is the same chain of FMAs in the same order for every launch shape.
 template <bool TRAIN>
-__global__ void __launch_bounds__(256) k_mp_encode(int N, const double* __restrict__ r, const double* rr,
-                                                   double inv_n, const float* __restrict__ sf, MpnnParams P,
-                                                   const int* skip, __nv_bfloat16* __restrict__ H0,
-                                                   __nv_bfloat16* __restrict__ Xout) {
-  if (skip && *skip) return;
-  __shared__ __align__(16) float wt[kMpIn][F];
-  __shared__ __align__(16) float bs[F];
-  for (int i = threadIdx.x; i < F * kMpIn; i += blockDim.x) {
-    const int o = i / kMpIn, k = i % kMpIn;
-    wt[k][o] = bf(P.pb[kMpOffWin + i]);
+__global__ void __launch_bounds__(kEncT, kEncCtasPerSm) k_mp_encode(int N, const double* __restrict__ r, const double* rr,
+                                                     double inv_n, const float* __restrict__ sf, MpnnParams P,
+                                                     const int* skip, __nv_bfloat16* __restrict__ H0,
+                                                     __nv_bfloat16* __restrict__ Xout, long long spin_limit,
+                                                     int* err) {
+  if (skip && *skip) return;  // uniform: before any barrier
+  __shared__ __align__(128) uint8_t stage[2][kEncStage];
+  __shared__ uint64_t bar[2];
+  const int t = threadIdx.x, lane = t & 31;
+  const int c = t & 7, grp = t >> 3;
+  const int chunks = (N + kEncChunk - 1) / kEncChunk;
+  // this thread's weights W_in[8c + j][k] and biases b_in[8c + j]
+  float w[8][kMpIn], bsv[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const uint4 q = *reinterpret_cast<const uint4*>(P.pb + kMpOffWin + (8 * c + j) * kMpIn);
+    w[j][0] = bf_lo(q.x);
+    w[j][1] = bf_hi(q.x);
+    w[j][2] = bf_lo(q.y);
+    w[j][3] = bf_hi(q.y);
+    w[j][4] = bf_lo(q.z);
+    w[j][5] = bf_hi(q.z);
+    w[j][6] = bf_lo(q.w);
+    w[j][7] = bf_hi(q.w);
+    bsv[j] = P.pf[kMpOffBin + 8 * c + j];
   }
-  for (int i = threadIdx.x; i < F; i += blockDim.x) bs[i] = P.pf[kMpOffBin + i];
+  const uint32_t bar0 = smem_u32(&bar[0]), bar1 = smem_u32(&bar[1]);
+  auto issue = [&](int ch, int st) {  // thread 0: chunk ch into stage st
+    const int first = ch * kEncChunk, cnt = min(kEncChunk, N - first);
+    const uint32_t rb = (uint32_t)cnt * 16u, sb = ((uint32_t)cnt * 24u + 15u) & ~15u;
+    const uint32_t b = st ? bar1 : bar0;
+    // the stage's earlier generic reads are ordered before the copies' writes
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(b), "r"(rb + sb) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     smem_u32(stage[st])),
+                 "l"(r + 2 * (size_t)first), "r"(rb), "r"(b)
+                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     smem_u32(stage[st] + kEncChunk * 16)),
+                 "l"(sf + 6 * (size_t)first), "r"(sb), "r"(b)
+                 : "memory");
+  };
+  if (t == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar0), "r"(1));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar1), "r"(1));
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    if ((int)blockIdx.x < chunks) issue(blockIdx.x, 0);
+    if ((int)(blockIdx.x + gridDim.x) < chunks) issue(blockIdx.x + gridDim.x, 1);
+  }
   __syncthreads();
-  const int c = threadIdx.x & 7;
-  const int n = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 3);
-  if (n >= N) return;
   const double s = sqrt(*rr * inv_n);
   const double sd = s > 0.0 ? s : 1.0;
-  const double2 rn = reinterpret_cast<const double2*>(r)[n];
-  const float2* sfn = reinterpret_cast<const float2*>(sf + (size_t)n * 6);
-  const float2 a0 = sfn[0], a1 = sfn[1], a2 = sfn[2];
-  float x[kMpIn] = {(float)(rn.x / sd), (float)(rn.y / sd), a0.x, a0.y, a1.x, a1.y, a2.x, a2.y};
+  int it = 0;
+  for (int ch = blockIdx.x; ch < chunks; ch += gridDim.x, ++it) {
+    const int st = it & 1;
+    const uint32_t par = (uint32_t)(it >> 1) & 1u;
+    const uint32_t b = st ? bar1 : bar0;
+    const int got = mbar_wait(b, par, spin_limit) ? 1 : 0;
+    if (!__syncthreads_and(got)) {
+      if (t == 0) {  // report, then let the copies in flight land (bounded) before leaving
+        if (err) atomicMin(&err[kErrTimeout], ch);
+        mbar_wait(b, par, kMbarSpinLimit);
+        if (ch + (int)gridDim.x < chunks) mbar_wait(st ? bar0 : bar1, (uint32_t)((it + 1) >> 1) & 1u, kMbarSpinLimit);
+      }
+      return;
+    }
+    const double* sr = reinterpret_cast<const double*>(stage[st]);
+    const float* ss = reinterpret_cast<const float*>(stage[st] + kEncChunk * 16);
+    const int first = ch * kEncChunk, cnt = min(kEncChunk, N - first);
+#pragma unroll 1
+    for (int j = 0; j < kEncChunk / 32; ++j) {
+      const int ln0 = j * 32 + grp;
+      const bool live = ln0 < cnt;  // every lane takes part in the shuffles
+      const int ln = live ? ln0 : cnt - 1;
+      float xc = c < 2 ? (float)(sr[2 * ln + c] / sd) : ss[6 * ln + c - 2];
+      xc = __bfloat162float(__float2bfloat16_rn(xc));
+      float x[kMpIn];
 #pragma unroll
-  for (int k = 0; k < kMpIn; ++k) x[k] = __bfloat162float(__float2bfloat16_rn(x[k]));
-  if (TRAIN && c == 0) {
-    uint4 xv;
-    xv.x = pack_bf2(x[0], x[1]);
-    xv.y = pack_bf2(x[2], x[3]);
-    xv.z = pack_bf2(x[4], x[5]);
-    xv.w = pack_bf2(x[6], x[7]);
-    reinterpret_cast<uint4*>(Xout)[n] = xv;
-  }
-  const float4 b0 = *reinterpret_cast<const float4*>(&bs[c * 8]);
-  const float4 b1 = *reinterpret_cast<const float4*>(&bs[c * 8 + 4]);
-  float u[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+      for (int k = 0; k < kMpIn; ++k) x[k] = __shfl_sync(0xffffffffu, xc, (lane & 24) | k);
+      if (!live) continue;
+      const int n = first + ln;
+      if (TRAIN && c == 0) {
+        uint4 xv;
+        xv.x = pack_bf2(x[0], x[1]);
+        xv.y = pack_bf2(x[2], x[3]);
+        xv.z = pack_bf2(x[4], x[5]);
+        xv.w = pack_bf2(x[6], x[7]);
+        reinterpret_cast<uint4*>(Xout)[n] = xv;
+      }
+      float u[8];
 #pragma unroll
-  for (int k = 0; k < kMpIn; ++k) {
-    const float4 w0 = *reinterpret_cast<const float4*>(&wt[k][c * 8]);
-    const float4 w1 = *reinterpret_cast<const float4*>(&wt[k][c * 8 + 4]);
-    u[0] = fmaf(w0.x, x[k], u[0]);
-    u[1] = fmaf(w0.y, x[k], u[1]);
-    u[2] = fmaf(w0.z, x[k], u[2]);
-    u[3] = fmaf(w0.w, x[k], u[3]);
-    u[4] = fmaf(w1.x, x[k], u[4]);
-    u[5] = fmaf(w1.y, x[k], u[5]);
-    u[6] = fmaf(w1.z, x[k], u[6]);
-    u[7] = fmaf(w1.w, x[k], u[7]);
+      for (int jj = 0; jj < 8; ++jj) {
+        u[jj] = bsv[jj];
+#pragma unroll
+        for (int k = 0; k < kMpIn; ++k) u[jj] = fmaf(w[jj][k], x[k], u[jj]);
+      }
+      reinterpret_cast<uint4*>(H0 + (size_t)n * F)[c] =
+          make_uint4(pack_bf2(fmaxf(u[0], 0.f), fmaxf(u[1], 0.f)), pack_bf2(fmaxf(u[2], 0.f), fmaxf(u[3], 0.f)),
+                     pack_bf2(fmaxf(u[4], 0.f), fmaxf(u[5], 0.f)), pack_bf2(fmaxf(u[6], 0.f), fmaxf(u[7], 0.f)));
+    }
+    __syncthreads();  // every thread is done with the stage
+    if (t == 0 && ch + 2 * (int)gridDim.x < chunks) issue(ch + 2 * gridDim.x, st);
   }
-  reinterpret_cast<uint4*>(H0 + (size_t)n * F)[c] =
-      make_uint4(pack_bf2(fmaxf(u[0], 0.f), fmaxf(u[1], 0.f)), pack_bf2(fmaxf(u[2], 0.f), fmaxf(u[3], 0.f)),
-                 pack_bf2(fmaxf(u[4], 0.f), fmaxf(u[5], 0.f)), pack_bf2(fmaxf(u[6], 0.f), fmaxf(u[7], 0.f)));
 }
 
 // ---- message-passing layer on the tensor cores ----------------------------------------------------
 //
-// A CTA of 8 warps owns a tile of 128 nodes at a time (persistent over tiles).
-//  gather:   each warp builds 16 rows of the A operand, four nodes at once with 8 lanes per node
-//            (lane c holds features 8c..8c+7, one 16-byte chunk): the node's own chunk and the sum
-//            of its neighbours' chunks, four neighbour loads in flight per lane, neighbours in
-//            ascending pattern order (the mean is the same sum in the same order as a serial loop).
+// A CTA owns a tile of 128 nodes at a time (persistent over tiles); its 8 tile warps build the A
+// operand, issue the MMA and run the epilogue:
+//  A tile:   16 rows per warp, four nodes at once with 8 lanes per node (lane c holds features
+//            8c..8c+7, one 16-byte chunk): the node's own chunk and the sum of its neighbours'
+//            chunks in ascending pattern order (the mean is the same sum in the same order as a
+//            serial loop, wherever the rows come from).
 //  MMA:      one thread issues 8 x tcgen05.mma (M=128, N=64, K=16) into 64 TMEM columns and waits
-//            on the commit's mbarrier (bounded); the block learns the outcome through shared memory.
+//            on the commit's mbarrier (bounded); the tile warps learn the outcome through shared
+//            memory.
 //  epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31, columns 32 (w / 4) .. +31 (its node's half
 //            row), adds bias, ReLU and the residual, and stages the BF16 row half in shared memory
 //            (16-byte chunks XOR-swizzled by row, so the stores do not collide on banks); the tile
@@ -234,15 +405,32 @@ __global__ void __launch_bounds__(256) k_mp_encode(int N, const double* __restri
 //            y = W_out H3 + b_out, summed over the 64 features in order (the first half by the
 //            warps of columns 0..31, handed through shared memory to those of columns 32..63), and
 //            z = zbase + invd (r + s y).
-constexpr int kLT = 256;                            // threads of the layer kernel
-constexpr int kNbrCache = 128;                      // neighbour-list entries a warp keeps in shared memory
-constexpr int kLayerCtasPerSm = 4;                  // resident CTAs per SM (registers capped to fit them)
-constexpr int kTcSmem = kASmem + kBSmem + 1024;     // dynamic shared memory (1024-byte aligned base)
+// The rows reach the A tile one of two ways:
+//  rows (PLAN = false): four CTAs of 8 warps per SM; each lane loads its nodes' chunks from global
+//            memory, a warp's node pointers and neighbour lists in two loads (the next tile's lists
+//            prefetched with cp.async during the MMA and the epilogue).
+//  plan (PLAN = true, patterns with a gather plan): two CTAs of 9 warps per SM. A tile's union
+//            of rows is a few runs of consecutive nodes (three on the O-grid plates, about 3 rows
+//            per node); the ninth warp, the producer, brings the runs and the tile's per-node
+//            slots into shared memory with bulk copies (cp.async.bulk, no multicast) as soon as
+//            the tile warps have read the previous tile's (full / empty mbarriers), so the copies
+//            run during the MMA and the epilogue. A tile the plan cannot take is gathered row by
+//            row.
+constexpr int kLT = 256;                 // the tile warps' threads
+constexpr int kLTPlan = kLT + 32;        // + the producer warp
+constexpr int kNbrCache = 128;           // neighbour-list entries a warp keeps in shared memory
+constexpr int kLayerCtasPerSm = 4;       // rows: resident CTAs per SM (registers capped to fit them)
+constexpr int kPlanCtasPerSm = 2;        // plan: resident CTAs per SM
+constexpr int kUStages = 1;              // plan: union buffers per CTA
+constexpr int kUSmem = kPlanMaxUnion * 128 + kTile * 16;  // one buffer: the rows, then the node slots
+constexpr int kTcSmem = kASmem + kBSmem + 1024;           // dynamic shared memory (1024-byte aligned base)
+constexpr int kTcSmemPlan = kASmem + kBSmem + kUStages * kUSmem + 1024;
 
 struct MpLayerArgs {
   int N;
   const int* node_ptr;
   const int* nbr;
+  MpTilePlan plan;
   const __nv_bfloat16* Hin;
   MpnnParams P;
   int layer;
@@ -285,8 +473,126 @@ __device__ __forceinline__ void add_chunk(float (&acc)[8], const uint4 v) {
   acc[7] += bf_hi(v.w);
 }
 
-template <bool TRAIN, bool LAST>
-__global__ void __launch_bounds__(kLT, kLayerCtasPerSm) k_mp_layer_tc(const MpLayerArgs a) {
+// Barrier of the tile warps: the whole CTA (rows), or named barrier 1 over threads 0..255 (plan,
+// where the producer warp keeps its own pace).
+// Shared-memory accesses by 32-bit shared address (ld/st.shared, on the short scoreboard).
+__device__ __forceinline__ uint4 lds128(uint32_t addr) {
+  uint4 v;
+  asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];\n"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+               : "r"(addr)
+               : "memory");
+  return v;
+}
+__device__ __forceinline__ void sts128(uint32_t addr, const uint4 v) {
+  asm volatile("st.shared.v4.u32 [%0], {%1, %2, %3, %4};\n" ::"r"(addr), "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w)
+               : "memory");
+}
+
+template <bool PLAN>
+__device__ __forceinline__ void tile_sync() {
+  if constexpr (PLAN)
+    asm volatile("bar.sync 1, 256;\n" ::: "memory");
+  else
+    __syncthreads();
+}
+template <bool PLAN>
+__device__ __forceinline__ int tile_sync_and(int pred) {
+  if constexpr (PLAN) {
+    int out;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.b32 p, %1, 0;\n\t"
+        "bar.red.and.pred q, 1, 256, p;\n\t"
+        "selp.b32 %0, 1, 0, q;\n\t}\n"
+        : "=r"(out)
+        : "r"(pred)
+        : "memory");
+    return out;
+  } else {
+    return __syncthreads_and(pred);
+  }
+}
+
+// A tile the plan takes: its union fits one buffer in at most kPlanMaxRuns runs.
+__device__ __forceinline__ bool plan_takes(const int4 h) {
+  return h.z == 0 && h.x >= 1 && h.x <= kPlanMaxRuns && h.y >= 1 && h.y <= kPlanMaxUnion;
+}
+
+// As mbar_wait, also giving up when the tile warps have raised `abort_flag`.
+__device__ __forceinline__ bool mbar_wait_or_abort(uint32_t addr, uint32_t parity, long long limit,
+                                                   const volatile int* abort_flag) {
+  for (long long i = 0; i < limit; ++i) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    if (ok) return true;
+    if (*abort_flag) return false;
+  }
+  return false;
+}
+
+// The producer warp of the plan kernel: for each of the CTA's planned tiles, in order, waits until
+// the tile warps are done with the buffer it last filled (the empty barrier), then lane 0 sets the
+// full barrier's byte count and every lane of a run issues its bulk copy: run j lands at the sum
+// of the earlier runs' lengths (rows of 128 bytes), the tile's node slots after the rows.
+// Before it leaves, the copies it issued have landed (bounded waits), so none writes into the
+// CTA's shared memory after the CTA is gone.
+__device__ __forceinline__ void plan_producer(const MpLayerArgs& a, uint8_t* sU, uint32_t full0, uint32_t empty0,
+                                              const volatile int* abort_flag) {
+  const int lane = threadIdx.x & 31;
+  int k = 0;  // planned tiles issued
+  for (int tile = blockIdx.x; tile * kTile < a.N; tile += gridDim.x) {
+    const int4 ph = __ldg(&a.plan.hdr[tile]);
+    if (!plan_takes(ph)) continue;
+    const int st = k % kUStages;
+    const uint32_t fb = full0 + 8u * st, eb = empty0 + 8u * st;
+    if (k >= kUStages) {
+      // a phase that one lane saw complete is complete for all: the warp goes on if any lane saw it
+      const bool freed = mbar_wait_or_abort(eb, (uint32_t)(k / kUStages - 1) & 1u, a.spin_limit, abort_flag);
+      if (!__any_sync(0xffffffffu, freed)) break;  // the tile warps stopped or did not free it in time
+    }
+    const int2 rn = lane < ph.x ? __ldg(&a.plan.runs[(size_t)tile * kPlanMaxRuns + lane]) : make_int2(0, 0);
+    int off = rn.y;  // inclusive prefix of the run lengths over the lanes
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, off, d);
+      if (lane >= d) off += v;
+    }
+    off -= rn.y;
+    const int cnt = min(kTile, a.N - tile * kTile);
+    uint8_t* buf = sU + (size_t)st * kUSmem;
+    if (lane == 0) {
+      // the tile warps' generic reads of this buffer are ordered before the copies' writes
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(fb),
+                   "r"((uint32_t)ph.y * 128u + (uint32_t)cnt * 16u)
+                   : "memory");
+      asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                       smem_u32(buf + kPlanMaxUnion * 128)),
+                   "l"(a.plan.local + (size_t)tile * kTile), "r"((uint32_t)cnt * 16u), "r"(fb)
+                   : "memory");
+    }
+    __syncwarp();
+    if (lane < ph.x)
+      asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                       smem_u32(buf + (size_t)off * 128)),
+                   "l"(a.Hin + (size_t)rn.x * F), "r"((uint32_t)rn.y * 128u), "r"(fb)
+                   : "memory");
+    ++k;
+  }
+  for (int j = max(0, k - kUStages); j < k; ++j)
+    mbar_wait(full0 + 8u * (j % kUStages), (uint32_t)(j / kUStages) & 1u, kMbarSpinLimit);
+}
+
+template <bool TRAIN, bool LAST, bool PLAN>
+__global__ void __launch_bounds__(PLAN ? kLTPlan : kLT, PLAN ? kPlanCtasPerSm : kLayerCtasPerSm)
+    k_mp_layer_tc(const MpLayerArgs a) {
   const int N = a.N;
   if (a.skip && *a.skip) {  // uniform: before any barrier or tensor-memory allocation
     if (LAST)                 // the network is off: the Jacobi step
@@ -295,29 +601,31 @@ __global__ void __launch_bounds__(kLT, kLayerCtasPerSm) k_mp_layer_tc(const MpLa
     return;
   }
   extern __shared__ uint8_t smem_raw[];
-  __shared__ uint64_t mbar;
+  __shared__ uint64_t mbar, full_bar[kUStages], empty_bar[kUStages];
   __shared__ uint32_t tmem_slot;
-  __shared__ int mma_ok;
+  __shared__ int mma_ok, abort_flag;
   __shared__ float wout[2 * F], bout[2];
   __shared__ float2 ypart[kTile];
-  // each warp's neighbour lists (the first kNbrCache entries; the next tile's are prefetched
-  // into the same place once the current tile's rounds are done)
+  // each warp's neighbour lists for row-by-row tiles (the first kNbrCache entries)
   __shared__ int s_nbr[(kLT / 32) * kNbrCache];
   uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
-  uint8_t* sA = base;            // element (m, k): (k/8)*2048 + (m/8)*128 + (m%8)*16 + (k%8)*2
-  uint8_t* sB = base + kASmem;   // element (n, k): (k/8)*1024 + (n/8)*128 + (n%8)*16 + (k%8)*2
+  uint8_t* sA = base;               // element (m, k): (k/8)*2048 + (m/8)*128 + (m%8)*16 + (k%8)*2
+  uint8_t* sB = base + kASmem;      // element (n, k): (k/8)*1024 + (n/8)*128 + (n%8)*16 + (k%8)*2
   uint8_t* sOut = sA + kASmem / 2;  // staged output tile (the mean half of A, free after the MMA)
+  uint8_t* sU = sB + kBSmem;        // plan: the ring of union buffers
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const __nv_bfloat16* W = a.P.pb + kMpOffL0 + a.layer * kMpLStride;
-  const float* bias = a.P.pf + kMpOffL0 + a.layer * kMpLStride + F * 2 * F;
+  const float* bias_g = a.P.pf + kMpOffL0 + a.layer * kMpLStride + F * 2 * F;
+  __shared__ float bias[F];
+  for (int i = t; i < F; i += blockDim.x) bias[i] = bias_g[i];
 
-  for (int idx = t; idx < F * 16; idx += kLT) {  // 64 rows x 16 chunks of 8 BF16
+  for (int idx = t; idx < F * 16; idx += blockDim.x) {  // 64 rows x 16 chunks of 8 BF16
     const int n = idx >> 4, kc = idx & 15;
     const uint4 v = *reinterpret_cast<const uint4*>(W + n * 2 * F + kc * 8);
     *reinterpret_cast<uint4*>(sB + kc * 1024 + (n >> 3) * 128 + (n & 7) * 16) = v;
   }
   if (LAST) {
-    for (int i = t; i < 2 * F; i += kLT) wout[i] = bf(a.P.pb[kMpOffWout + i]);
+    for (int i = t; i < 2 * F; i += blockDim.x) wout[i] = bf(a.P.pb[kMpOffWout + i]);
     if (t < 2) bout[t] = a.P.pf[kMpOffBout + t];
   }
   if (warp == 0) {
@@ -327,102 +635,173 @@ __global__ void __launch_bounds__(kLT, kLayerCtasPerSm) k_mp_layer_tc(const MpLa
   }
   if (t == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(&mbar)), "r"(1));
+    if (PLAN)
+      for (int j = 0; j < kUStages; ++j) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(&full_bar[j])), "r"(1));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(&empty_bar[j])), "r"(1));
+      }
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    abort_flag = 0;
   }
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-  __syncthreads();
+  __syncthreads();  // the last barrier of the whole CTA: from here the producer keeps its own pace
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const uint32_t full0 = smem_u32(&full_bar[0]), empty0 = smem_u32(&empty_bar[0]);
+  if constexpr (PLAN) {
+    if (warp == kLT / 32) {
+      plan_producer(a, sU, full0, empty0, &abort_flag);
+      return;
+    }
+  }
+  volatile int* abort_v = &abort_flag;
   const uint32_t tmem = tmem_slot;
   const uint32_t a_addr = smem_u32(sA), b_addr = smem_u32(sB), mbar_addr = smem_u32(&mbar);
+  const uint32_t out_addr = smem_u32(sOut);
   const double s = LAST ? sqrt(*a.rr * a.inv_n) : 0.0;
   uint32_t phase = 0;
-  const int g = lane >> 3, c = lane & 7;    // gather: node group of the warp, feature chunk
-  const int q = warp & 3, h = warp >> 2;    // epilogue: TMEM lane quarter, column half
-  int np = 0;          // lanes 0..16: node pointers of the warp's 16 nodes (+ the end) in this tile
-  bool first = true;
+  const int g = lane >> 3, c = lane & 7;  // gather: node group of the warp, feature chunk
+  const int q = warp & 3, h = warp >> 2;  // epilogue: TMEM lane quarter, column half
+  int np = 0;         // lanes 0..16: node pointers of the warp's 16 nodes (+ the end) in this tile
+  bool first = true;  // rows: the first tile's lists come synchronously, later ones were prefetched
+  int kp = 0;         // plan: planned tiles consumed
+  int4 ph = make_int4(0, 0, 1, 0);
+  if (PLAN && (int)blockIdx.x * kTile < N) ph = __ldg(&a.plan.hdr[blockIdx.x]);
 
   for (int tile = blockIdx.x; tile * kTile < N; tile += gridDim.x) {
-    // ---- gather: own chunk and the neighbours' mean chunk of 16 nodes per warp. The warp's 17
-    // node pointers come in one load, its nodes' neighbour lists (contiguous in the pattern) in
-    // one more into shared memory, so each round of four nodes is one round trip: the own
-    // chunk and up to eight neighbour chunks per lane in flight.
-    const int wbase = tile * kTile + warp * 16;
-    int* wnbr = s_nbr + warp * kNbrCache;
-    if (first) {  // the first tile's lists come synchronously; later ones were prefetched
-      if (lane <= 16) np = __ldg(&a.node_ptr[min(wbase + lane, N)]);
-      const int f0 = __shfl_sync(0xffffffffu, np, 0);
-      const int fc = __shfl_sync(0xffffffffu, np, 16) - f0;
-      for (int j = lane; j < min(fc, kNbrCache); j += 32) wnbr[j] = __ldg(&a.nbr[f0 + j]);
-      first = false;
-    } else {
-      asm volatile("cp.async.wait_all;\n" ::: "memory");
-    }
-    __syncwarp();
-    const int np0 = __shfl_sync(0xffffffffu, np, 0);
-    // the next tile's node pointers, used after this tile's rounds
-    const int wnext = (tile + (int)gridDim.x) * kTile + warp * 16;
-    int np_next = 0;
-    if (lane <= 16 && (tile + (int)gridDim.x) * kTile < N) np_next = __ldg(&a.node_ptr[min(wnext + lane, N)]);
-#pragma unroll 1
-    for (int rnd = 0; rnd < 4; ++rnd) {
-      const int li = rnd * 4 + g;
-      const int m = warp * 16 + li;
-      const int n = wbase + li;
-      const int k0 = __shfl_sync(0xffffffffu, np, li) - np0;
-      const int k1 = __shfl_sync(0xffffffffu, np, li + 1) - np0;
-      uint4 own = make_uint4(0u, 0u, 0u, 0u);
-      float acc[8];
+    const int next = tile + (int)gridDim.x;
+    int4 ph_next = make_int4(0, 0, 1, 0);
+    if (PLAN && next * kTile < N) ph_next = __ldg(&a.plan.hdr[next]);
+    if (PLAN && plan_takes(ph)) {
+      // ---- A tile from the union buffer the producer filled
+      const int st = kp % kUStages;
+      const uint8_t* buf = sU + (size_t)st * kUSmem;
+      const int got = mbar_wait(full0 + 8u * st, (uint32_t)(kp / kUStages) & 1u, a.spin_limit) ? 1 : 0;
+      if (!tile_sync_and<PLAN>(got)) {  // report and stop; the producer drains its copies
+        if (t == 0) {
+          if (a.err) atomicMin(&a.err[kErrTimeout], tile);
+          *abort_v = 1;
+        }
+        break;
+      }
+      const uint32_t buf_u = smem_u32(buf), slots_u = buf_u + kPlanMaxUnion * 128;
 #pragma unroll
-      for (int j = 0; j < 8; ++j) acc[j] = 0.f;
-      int deg = 0;
-      if (n < N) {
-        own = __ldg(reinterpret_cast<const uint4*>(a.Hin + (size_t)n * F) + c);
-        for (int k = k0; k < k1; k += 8) {
-          int mm[8];
-          uint4 v[8];
+      for (int rnd = 0; rnd < 4; ++rnd) {
+        const int m = warp * 16 + rnd * 4 + g;
+        const int n = tile * kTile + m;
+        uint4 own = make_uint4(0u, 0u, 0u, 0u);
+        float acc[8];
 #pragma unroll
-          for (int j = 0; j < 8; ++j) {
-            const int q8 = k + j;
-            mm[j] = q8 < k1 ? (q8 < kNbrCache ? wnbr[q8] : __ldg(&a.nbr[np0 + q8])) : n;
-          }
+        for (int j = 0; j < 8; ++j) acc[j] = 0.f;
+        int deg = 0;
+        if (n < N) {
+          const uint4 lp = lds128(slots_u + (uint32_t)m * 16u);
+          const uint32_t sl[8] = {lp.x & 0xFFFFu, lp.x >> 16, lp.y & 0xFFFFu, lp.y >> 16,
+                                  lp.z & 0xFFFFu, lp.z >> 16, lp.w & 0xFFFFu, lp.w >> 16};
+          own = lds128(buf_u + sl[0] * 128u + c * 16);
 #pragma unroll
-          for (int j = 0; j < 8; ++j)
-            v[j] = mm[j] != n ? __ldg(reinterpret_cast<const uint4*>(a.Hin + (size_t)mm[j] * F) + c)
-                              : make_uint4(0u, 0u, 0u, 0u);
-#pragma unroll
-          for (int j = 0; j < 8; ++j)
-            if (mm[j] != n) {
+          for (int j = 1; j < 8; ++j)
+            if (sl[j] != 0xFFFFu) {
               ++deg;
-              add_chunk(acc, v[j]);
+              add_chunk(acc, lds128(buf_u + sl[j] * 128u + c * 16));
             }
         }
+        const float inv = deg ? 1.f / (float)deg : 0.f;
+        uint4 av;
+        av.x = pack_bf2(acc[0] * inv, acc[1] * inv);
+        av.y = pack_bf2(acc[2] * inv, acc[3] * inv);
+        av.z = pack_bf2(acc[4] * inv, acc[5] * inv);
+        av.w = pack_bf2(acc[6] * inv, acc[7] * inv);
+        const uint32_t row_off = (uint32_t)((m >> 3) * 128 + (m & 7) * 16);
+        sts128(a_addr + c * 2048 + row_off, own);
+        sts128(a_addr + (8 + c) * 2048 + row_off, av);
+        if (TRAIN && n < N) reinterpret_cast<uint4*>(a.Aout + (size_t)n * F)[c] = av;
       }
-      const float inv = deg ? 1.f / (float)deg : 0.f;
-      uint4 av;
-      av.x = pack_bf2(acc[0] * inv, acc[1] * inv);
-      av.y = pack_bf2(acc[2] * inv, acc[3] * inv);
-      av.z = pack_bf2(acc[4] * inv, acc[5] * inv);
-      av.w = pack_bf2(acc[6] * inv, acc[7] * inv);
-      const uint32_t row_off = (uint32_t)((m >> 3) * 128 + (m & 7) * 16);
-      *reinterpret_cast<uint4*>(sA + c * 2048 + row_off) = own;
-      *reinterpret_cast<uint4*>(sA + (8 + c) * 2048 + row_off) = av;
-      if (TRAIN && n < N) reinterpret_cast<uint4*>(a.Aout + (size_t)n * F)[c] = av;
-    }
-    {  // prefetch the next tile's neighbour lists (asynchronous copies, done during the MMA and
-       // the epilogue); every lane has finished reading this tile's lists
+      tile_sync<PLAN>();  // every tile warp is done with the buffer
+      if (t == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(empty0 + 8u * st) : "memory");
+      ++kp;
+    } else {
+      // ---- A tile row by row: the warp's 17 node pointers in one load, its nodes' neighbour lists
+      // (contiguous in the pattern) in one more into shared memory, so each round of four nodes is
+      // one round trip: the own chunk and up to eight neighbour chunks per lane in flight.
+      const int wbase = tile * kTile + warp * 16;
+      int* wnbr = s_nbr + warp * kNbrCache;
+      if (PLAN || first) {
+        if (lane <= 16) np = __ldg(&a.node_ptr[min(wbase + lane, N)]);
+        const int f0 = __shfl_sync(0xffffffffu, np, 0);
+        const int fc = __shfl_sync(0xffffffffu, np, 16) - f0;
+        for (int j = lane; j < min(fc, kNbrCache); j += 32) wnbr[j] = __ldg(&a.nbr[f0 + j]);
+        first = false;
+      } else {
+        asm volatile("cp.async.wait_all;\n" ::: "memory");
+      }
       __syncwarp();
-      const int n0 = __shfl_sync(0xffffffffu, np_next, 0);
-      const int nc = __shfl_sync(0xffffffffu, np_next, 16) - n0;
-      for (int j = lane; j < min(nc, kNbrCache); j += 32)
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(smem_u32(wnbr + j)), "l"(a.nbr + n0 + j)
-                     : "memory");
-      asm volatile("cp.async.commit_group;\n" ::: "memory");
-      np = np_next;
+      const int np0 = __shfl_sync(0xffffffffu, np, 0);
+      // rows: the next tile's node pointers, used after this tile's rounds
+      const int wnext = next * kTile + warp * 16;
+      int np_next = 0;
+      if (!PLAN && lane <= 16 && next * kTile < N) np_next = __ldg(&a.node_ptr[min(wnext + lane, N)]);
+#pragma unroll 1
+      for (int rnd = 0; rnd < 4; ++rnd) {
+        const int li = rnd * 4 + g;
+        const int m = warp * 16 + li;
+        const int n = wbase + li;
+        const int k0 = __shfl_sync(0xffffffffu, np, li) - np0;
+        const int k1 = __shfl_sync(0xffffffffu, np, li + 1) - np0;
+        uint4 own = make_uint4(0u, 0u, 0u, 0u);
+        float acc[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[j] = 0.f;
+        int deg = 0;
+        if (n < N) {
+          own = __ldg(reinterpret_cast<const uint4*>(a.Hin + (size_t)n * F) + c);
+          for (int k = k0; k < k1; k += 8) {
+            int mm[8];
+            uint4 v[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+              const int q8 = k + j;
+              mm[j] = q8 < k1 ? (q8 < kNbrCache ? wnbr[q8] : __ldg(&a.nbr[np0 + q8])) : n;
+            }
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+              v[j] = mm[j] != n ? __ldg(reinterpret_cast<const uint4*>(a.Hin + (size_t)mm[j] * F) + c)
+                                : make_uint4(0u, 0u, 0u, 0u);
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+              if (mm[j] != n) {
+                ++deg;
+                add_chunk(acc, v[j]);
+              }
+          }
+        }
+        const float inv = deg ? 1.f / (float)deg : 0.f;
+        uint4 av;
+        av.x = pack_bf2(acc[0] * inv, acc[1] * inv);
+        av.y = pack_bf2(acc[2] * inv, acc[3] * inv);
+        av.z = pack_bf2(acc[4] * inv, acc[5] * inv);
+        av.w = pack_bf2(acc[6] * inv, acc[7] * inv);
+        const uint32_t row_off = (uint32_t)((m >> 3) * 128 + (m & 7) * 16);
+        sts128(a_addr + c * 2048 + row_off, own);
+        sts128(a_addr + (8 + c) * 2048 + row_off, av);
+        if (TRAIN && n < N) reinterpret_cast<uint4*>(a.Aout + (size_t)n * F)[c] = av;
+      }
+      if (!PLAN) {  // prefetch the next tile's neighbour lists (asynchronous copies, done during the
+                    // MMA and the epilogue); every lane has finished reading this tile's lists
+        __syncwarp();
+        const int n0 = __shfl_sync(0xffffffffu, np_next, 0);
+        const int nc = __shfl_sync(0xffffffffu, np_next, 16) - n0;
+        for (int j = lane; j < min(nc, kNbrCache); j += 32)
+          asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(smem_u32(wnbr + j)), "l"(a.nbr + n0 + j)
+                       : "memory");
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+        np = np_next;
+      }
     }
+    ph = ph_next;
     // generic-proxy shared-memory writes -> visible to the tensor core (async proxy)
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-    __syncthreads();
+    tile_sync<PLAN>();
     if (t == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
 #pragma unroll
@@ -445,14 +824,15 @@ __global__ void __launch_bounds__(kLT, kLayerCtasPerSm) k_mp_layer_tc(const MpLa
         // shared memory and tensor memory are released
         if (a.err) atomicMin(&a.err[kErrTimeout], tile);
         mbar_wait(mbar_addr, phase, kMbarSpinLimit);
+        *abort_v = 1;
       }
       mma_ok = ok;
       asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     }
     phase ^= 1u;
-    __syncthreads();
+    tile_sync<PLAN>();
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-    if (!mma_ok) break;  // uniform: every thread reads the same flag
+    if (!mma_ok) break;  // uniform: every tile thread reads the same flag
 
     // ---- epilogue: bias, ReLU, residual; stage the output half row
     const int m = q * 32 + lane;
@@ -465,7 +845,7 @@ __global__ void __launch_bounds__(kLT, kLayerCtasPerSm) k_mp_layer_tc(const MpLa
 #pragma unroll
     for (int cc = 0; cc < 4; ++cc) {
       const int ch = 4 * h + cc;
-      const uint4 o4 = *reinterpret_cast<const uint4*>(sA + ch * 2048 + row_off);
+      const uint4 o4 = lds128(a_addr + ch * 2048 + row_off);
       const uint32_t ow[4] = {o4.x, o4.y, o4.z, o4.w};
       uint32_t gw[4];
 #pragma unroll
@@ -483,8 +863,8 @@ __global__ void __launch_bounds__(kLT, kLayerCtasPerSm) k_mp_layer_tc(const MpLa
 #pragma unroll
       for (int cc = 0; cc < 4; ++cc) {
         const int ch = 4 * h + cc;
-        *reinterpret_cast<uint4*>(sOut + m * 128 + ((ch ^ (m & 7)) * 16)) =
-            make_uint4(hw[cc * 4], hw[cc * 4 + 1], hw[cc * 4 + 2], hw[cc * 4 + 3]);
+        sts128(out_addr + m * 128 + ((ch ^ (m & 7)) * 16),
+               make_uint4(hw[cc * 4], hw[cc * 4 + 1], hw[cc * 4 + 2], hw[cc * 4 + 3]));
       }
     }
     float y0 = 0.f, y1 = 0.f;
@@ -507,7 +887,7 @@ __global__ void __launch_bounds__(kLT, kLayerCtasPerSm) k_mp_layer_tc(const MpLa
       if (h == 0) ypart[m] = make_float2(y0, y1);
     }
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-    __syncthreads();
+    tile_sync<PLAN>();
     if (LAST && h == 1 && n < N) {
       const float2 yp = ypart[m];
       y0 = yp.x;
@@ -538,10 +918,10 @@ __global__ void __launch_bounds__(kLT, kLayerCtasPerSm) k_mp_layer_tc(const MpLa
         const int nr = tile * kTile + row;
         if (nr < N)
           reinterpret_cast<uint4*>(a.Hout + (size_t)nr * F)[ch] =
-              *reinterpret_cast<const uint4*>(sOut + row * 128 + ((ch ^ (row & 7)) * 16));
+              lds128(out_addr + row * 128 + ((ch ^ (row & 7)) * 16));
       }
     }
-    __syncthreads();  // tensor memory and the A tile are free for the next tile
+    tile_sync<PLAN>();  // tensor memory and the A tile are free for the next tile
   }
   asm volatile("cp.async.wait_all;\n" ::: "memory");  // no copy in flight when the CTA leaves
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
@@ -931,35 +1311,62 @@ int grid_nodes(long long work, int per_block) {
   return (int)std::max<long long>(1, std::min<long long>(g, 148LL * 16));
 }
 
-int g_tc_grid[4][64] = {};  // one wave of the layer kernel per device: [TRAIN * 2 + LAST][device]
+int g_sms[64] = {};          // SM count per device (set by mpnn_prepare_device)
+bool g_tc_attr[8][64] = {};  // the layer kernel's attributes set: [TRAIN * 4 + LAST * 2 + PLAN][device]
 
-template <bool TRAIN, bool LAST>
-cudaError_t set_tc_attr() {
+int dev_slot() {
   int dev = 0;
   cudaGetDevice(&dev);
-  int& slot = g_tc_grid[(TRAIN ? 2 : 0) + (LAST ? 1 : 0)][dev >= 0 && dev < 64 ? dev : 0];
-  if (slot > 0) return cudaSuccess;
-  cudaError_t e = cudaFuncSetAttribute(k_mp_layer_tc<TRAIN, LAST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       kTcSmem);
+  return dev >= 0 && dev < 64 ? dev : 0;
+}
+
+template <bool TRAIN, bool LAST, bool PLAN>
+cudaError_t set_tc_attr() {
+  bool& done = g_tc_attr[(TRAIN ? 4 : 0) + (LAST ? 2 : 0) + (PLAN ? 1 : 0)][dev_slot()];
+  if (done) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(k_mp_layer_tc<TRAIN, LAST, PLAN>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, PLAN ? kTcSmemPlan : kTcSmem);
   if (e != cudaSuccess) return e;
-  // the whole unified L1 / shared array as shared memory: three CTAs of ~56 KB per SM
-  e = cudaFuncSetAttribute(k_mp_layer_tc<TRAIN, LAST>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  // the whole unified L1 / shared array as shared memory: four CTAs of ~54 KB per SM (rows), two
+  // of ~110 KB (plan)
+  e = cudaFuncSetAttribute(k_mp_layer_tc<TRAIN, LAST, PLAN>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
   if (e != cudaSuccess) return e;
-  // one wave: kLayerCtasPerSm CTAs on every SM (the register cap of __launch_bounds__ and the
-  // ~56 KB of shared memory per CTA are sized for it)
-  int sms = 0;
-  e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (e != cudaSuccess) return e;
-  slot = kLayerCtasPerSm * std::max(1, sms);
+  done = true;
   return cudaSuccess;
 }
 
-int tc_grid(int N, bool train, bool last) {
-  int dev = 0;
-  cudaGetDevice(&dev);
-  const int wave = g_tc_grid[(train ? 2 : 0) + (last ? 1 : 0)][dev >= 0 && dev < 64 ? dev : 0];
+int enc_grid(int N) {  // one wave of kEncCtasPerSm CTAs per SM at most
+  const int sms = g_sms[dev_slot()] > 0 ? g_sms[dev_slot()] : kSMs;
+  const int chunks = (N + kEncChunk - 1) / kEncChunk;
+  return std::max(1, std::min(chunks, kEncCtasPerSm * sms));
+}
+
+// One wave of the layer kernel: kLayerCtasPerSm CTAs on every SM (rows; the register cap of
+// __launch_bounds__ and the shared memory per CTA are sized for it), kPlanCtasPerSm (plan).
+int tc_grid(int N, bool plan) {
+  const int sms = g_sms[dev_slot()] > 0 ? g_sms[dev_slot()] : kSMs;
   const int tiles = (N + kTile - 1) / kTile;
-  return std::max(1, std::min(tiles, wave > 0 ? wave : kSMs * 2));
+  return std::max(1, std::min(tiles, (plan ? kPlanCtasPerSm : kLayerCtasPerSm) * sms));
+}
+
+template <bool TRAIN, bool LAST>
+void launch_layer_t(const MpLayerArgs& a, bool plan, cudaStream_t s) {
+  if (plan)
+    k_mp_layer_tc<TRAIN, LAST, true><<<tc_grid(a.N, true), kLTPlan, kTcSmemPlan, s>>>(a);
+  else
+    k_mp_layer_tc<TRAIN, LAST, false><<<tc_grid(a.N, false), kLT, kTcSmem, s>>>(a);
+}
+
+void launch_layer(const MpLayerArgs& a, bool train, bool last, cudaStream_t s) {
+  const bool plan = a.plan.hdr != nullptr;
+  if (train && last)
+    launch_layer_t<true, true>(a, plan, s);
+  else if (train)
+    launch_layer_t<true, false>(a, plan, s);
+  else if (last)
+    launch_layer_t<false, true>(a, plan, s);
+  else
+    launch_layer_t<false, false>(a, plan, s);
 }
 
 }  // namespace
@@ -973,10 +1380,20 @@ cudaError_t mpnn_prepare_device() {
     if (ew != cudaSuccess) return ew;
     wg_done[dev] = true;
   }
-  cudaError_t e = set_tc_attr<false, false>();
-  if (e == cudaSuccess) e = set_tc_attr<false, true>();
-  if (e == cudaSuccess) e = set_tc_attr<true, false>();
-  if (e == cudaSuccess) e = set_tc_attr<true, true>();
+  if (dev >= 0 && dev < 64 && g_sms[dev] == 0) {
+    int sms = 0;
+    const cudaError_t es = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (es != cudaSuccess) return es;
+    g_sms[dev] = std::max(1, sms);
+  }
+  cudaError_t e = set_tc_attr<false, false, false>();
+  if (e == cudaSuccess) e = set_tc_attr<false, true, false>();
+  if (e == cudaSuccess) e = set_tc_attr<true, false, false>();
+  if (e == cudaSuccess) e = set_tc_attr<true, true, false>();
+  if (e == cudaSuccess) e = set_tc_attr<false, false, true>();
+  if (e == cudaSuccess) e = set_tc_attr<false, true, true>();
+  if (e == cudaSuccess) e = set_tc_attr<true, false, true>();
+  if (e == cudaSuccess) e = set_tc_attr<true, true, true>();
   return e;
 }
 
@@ -1001,6 +1418,14 @@ cudaError_t launch_mp_static(int N, const double* invd, const double* xy, const 
   return cudaGetLastError();
 }
 
+cudaError_t launch_mp_tile_plan(int N, const int* node_ptr, const int* nbr, int4* hdr, int2* runs, uint4* local,
+                                cudaStream_t s) {
+  if (N <= 0) return cudaSuccess;
+  k_mp_tile_plan<<<(N + kTile - 1) / kTile, 256, 0, s>>>(N, node_ptr, nbr, hdr, runs, local);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_mp_smoother_weights(int n, const double* invd, const double* lam, double factor, double* out,
                                        cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
@@ -1015,15 +1440,17 @@ cudaError_t launch_mp_forward(const MpnnGraph& g, const MpnnParams& P, const dou
   const int N = g.n_nodes;
   if (N <= 0) return cudaSuccess;
   const double inv_n = 1.0 / (2.0 * N);
-  const int ge = (int)((8LL * N + 255) / 256);  // eight threads per node, one node each
+  if (reinterpret_cast<uintptr_t>(r) & 15u) return cudaErrorInvalidValue;  // the bulk copies' alignment
+  const int ge = enc_grid(N);
   if (train)
-    k_mp_encode<true><<<ge, 256, 0, s>>>(N, r, rr, inv_n, sf, P, skip, w.H[0], w.X);
+    k_mp_encode<true><<<ge, kEncT, 0, s>>>(N, r, rr, inv_n, sf, P, skip, w.H[0], w.X, spin_limit, err);
   else
-    k_mp_encode<false><<<ge, 256, 0, s>>>(N, r, rr, inv_n, sf, P, skip, w.H[0], nullptr);
+    k_mp_encode<false><<<ge, kEncT, 0, s>>>(N, r, rr, inv_n, sf, P, skip, w.H[0], nullptr, spin_limit, err);
   MpLayerArgs a{};
   a.N = N;
   a.node_ptr = g.node_ptr;
   a.nbr = g.nbr;
+  a.plan = g.plan;
   a.P = P;
   a.skip = skip;
   a.r = r;
@@ -1042,15 +1469,7 @@ cudaError_t launch_mp_forward(const MpnnGraph& g, const MpnnParams& P, const dou
     a.Hout = train ? w.H[l + 1] : (last ? nullptr : w.H[(l + 1) & 1]);
     a.Gout = train ? w.G[l] : nullptr;
     a.Aout = train ? w.A[l] : nullptr;
-    const int grid = tc_grid(N, train, last);
-    if (train && last)
-      k_mp_layer_tc<true, true><<<grid, kLT, kTcSmem, s>>>(a);
-    else if (train)
-      k_mp_layer_tc<true, false><<<grid, kLT, kTcSmem, s>>>(a);
-    else if (last)
-      k_mp_layer_tc<false, true><<<grid, kLT, kTcSmem, s>>>(a);
-    else
-      k_mp_layer_tc<false, false><<<grid, kLT, kTcSmem, s>>>(a);
+    launch_layer(a, train, last, s);
   }
   count_launches(1 + kMpL);
   return cudaGetLastError();
@@ -1063,13 +1482,15 @@ cudaError_t launch_mp_stage(const MpnnGraph& g, const MpnnParams& P, int stage, 
   if (N <= 0) return cudaSuccess;
   const double inv_n = 1.0 / (2.0 * N);
   if (stage == 0) {
-    const int ge = (int)((8LL * N + 255) / 256);
-    k_mp_encode<false><<<ge, 256, 0, s>>>(N, r, rr, inv_n, sf, P, nullptr, w.H[0], nullptr);
+    if (reinterpret_cast<uintptr_t>(r) & 15u) return cudaErrorInvalidValue;
+    k_mp_encode<false><<<enc_grid(N), kEncT, 0, s>>>(N, r, rr, inv_n, sf, P, nullptr, w.H[0], nullptr, spin_limit,
+                                                      err);
   } else {
     MpLayerArgs a{};
     a.N = N;
     a.node_ptr = g.node_ptr;
     a.nbr = g.nbr;
+    a.plan = g.plan;
     a.P = P;
     a.r = r;
     a.invd = invd;
@@ -1082,10 +1503,7 @@ cudaError_t launch_mp_stage(const MpnnGraph& g, const MpnnParams& P, int stage, 
     const bool last = stage == kMpL;
     a.Hin = w.H[(stage - 1) & 1];
     a.Hout = last ? nullptr : w.H[stage & 1];
-    if (last)
-      k_mp_layer_tc<false, true><<<tc_grid(N, false, true), kLT, kTcSmem, s>>>(a);
-    else
-      k_mp_layer_tc<false, false><<<tc_grid(N, false, false), kLT, kTcSmem, s>>>(a);
+    launch_layer(a, false, last, s);
   }
   count_launches(1);
   return cudaGetLastError();

@@ -211,3 +211,80 @@ def test_trained_network_gain_on_held_out_plates(pkg, gpu_lib):
     assert st.converged and st.true_rel_residual <= 1e-10, st.message
     assert _rel(x, x_ref) < REL_TOL
     K.ctx.close()
+
+
+def _mesh_system(pkg, m, D):
+    K = pkg.build_stiffness_pattern(m)
+    pkg.assemble_stiffness(m, D, 1.0, K)
+    s = pkg.CgJacobiSolver()
+    s.setup(K)
+    return K
+
+
+def _plan_fallback_tiles(m):
+    """Tiles of 128 nodes the layers' gather plan cannot take (more than 8 runs of consecutive
+    rows, more than 416 rows, a span over 4096 nodes or a node of more than 7 neighbours), counted
+    on the host from the mesh alone."""
+    tri = np.asarray(m.triangles).reshape(-1, 3).astype(np.int64)
+    N = m.num_nodes
+    a = np.unique(np.concatenate([tri[:, i] * N + tri[:, j] for i in range(3) for j in range(3)]))
+    src, dst = a // N, a % N
+    ptr = np.searchsorted(src, np.arange(N + 1))
+    out = 0
+    for t in range(0, N, 128):
+        u = np.unique(dst[ptr[t]:ptr[min(N, t + 128)]])
+        deg = np.diff(ptr[t:min(N, t + 128) + 1])
+        runs = 1 + int(np.sum(np.diff(u) > 1))
+        out += int(u[-1] - u[0] + 1 > 4096 or u.size > 416 or runs > 8 or deg.max() - 1 > 7)
+    return out, (N + 127) // 128
+
+
+def _renumbered_plate(pkg, n_r, n_t, first, seed):
+    """The quarter plate with the nodes from `first` on numbered at random."""
+    m = pkg.plate.quarter_plate(n_r, n_t)
+    N = m.num_nodes
+    perm = np.arange(N)
+    perm[first:] = first + np.random.default_rng(seed).permutation(N - first)
+    xy = np.empty_like(np.asarray(m.xy).reshape(-1, 2))
+    xy[perm] = np.asarray(m.xy).reshape(-1, 2)
+    tri = perm[np.asarray(m.triangles).reshape(-1, 3)].astype(np.int32)
+    return pkg.plate.Mesh(xy=xy.reshape(-1), triangles=tri.reshape(-1), boundary_edges={})
+
+
+def test_gather_plan_matches_row_gather(pkg, oracle, gpu_lib, golden, monkeypatch):
+    """The layers read each tile's rows either through its gather plan (bulk copies of runs of
+    consecutive rows into shared memory) or row by row; both sum the same neighbours in the same
+    order, so z and the training loss and gradients are bit-identical. Meshes: an O-grid plate
+    (every tile planned), the Kirsch L1 mesh (no tile planned) and a plate renumbered at random
+    past its 1000th node (both kinds in one launch)."""
+    import torch
+    D = pkg.constitutive_matrix(1.0, 0.3)
+    meshes = {"plate": pkg.plate.quarter_plate(60, 150), "kirsch_L1": golden("kirsch_L1").mesh(pkg),
+              "mixed": _renumbered_plate(pkg, 40, 80, 1000, 5)}
+    kinds = {k: _plan_fallback_tiles(m) for k, m in meshes.items()}
+    assert kinds["plate"][0] == 0 and kinds["kirsch_L1"][0] == kinds["kirsch_L1"][1]
+    assert 0 < kinds["mixed"][0] < kinds["mixed"][1], kinds
+    p, _ = _bf16_params(oracle, pkg, seed=6)
+    for name, m in meshes.items():
+        rng = np.random.default_rng(11)
+        r = rng.standard_normal((2, m.num_dofs))
+        e = rng.standard_normal((2, m.num_dofs))
+        mat = pkg.learned.node_material(D, m.num_nodes)
+        out = {}
+        for gather in ("plan", "rows"):
+            if gather == "rows":
+                monkeypatch.setenv("CSTG_MP_GATHER", "rows")
+            else:
+                monkeypatch.delenv("CSTG_MP_GATHER", raising=False)
+            K = _mesh_system(pkg, m, D)
+            pkg.learned.setup(K, p, mat)
+            z = pkg.learned.apply(K, torch.from_numpy(r[0]).cuda()).cpu().numpy()
+            tr = pkg.learned.Trainer(p)
+            loss = tr.accumulate(K, torch.from_numpy(r).cuda(), torch.from_numpy(e).cuda())
+            _, g = tr.params(grads=True)
+            out[gather] = (z, loss, g)
+            tr.close()
+            K.ctx.close()
+        monkeypatch.delenv("CSTG_MP_GATHER", raising=False)
+        for a, b in zip(out["plan"], out["rows"]):
+            assert np.array_equal(a, b), name
