@@ -86,10 +86,11 @@ def parse():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-solve measurement")
     ap.add_argument("--no-large", action="store_true",
                     help="skip the large plate (n_r=800 x n_theta=2500): learned + mixed against plain FP64")
-    ap.add_argument("--only", choices=["spmv", "solve", "batch", "learned", "amg"], default=None,
+    ap.add_argument("--only", choices=["spmv", "solve", "batch", "learned", "network", "amg"], default=None,
                     help="profiling modes (one JSON line each): `spmv` --reps SpMV launches, `solve` one "
                          "full step, `batch` the 64-plate x 4-load-case batched solve, `learned` the "
-                         "network's stages, `amg` the multigrid cycle")
+                         "network's stages after a step, `network` the network's stages on the assembled "
+                         "system without a solve, `amg` the multigrid cycle")
     ap.add_argument("--reps", type=int, default=20)
     ap.add_argument("--max-iter", type=int, default=200000,
                     help="iteration cap of the solves (profiling captures use a small cap)")
@@ -480,13 +481,17 @@ def run_ours(a, dist: Dist):
     mat = pkg.learned.node_material(D, N)
     last = {}
 
+    def system():  # pattern, assembly, loads and Dirichlet on the GPU (on the caller's stream)
+        K = pkg.build_stiffness_pattern(dmesh, ctx=ctx)
+        pkg.assemble_stiffness(dmesh, D, 1.0, K)
+        d_b.zero_()
+        pkg.add_traction(K, d_right, 1.0, 1.0, 0.0, d_b)  # loads on the GPU (bc.cpp:190-253)
+        pkg.apply_dirichlet((d_dofs, d_vals), K, d_b)
+        return K
+
     def step():
         with torch.cuda.stream(stream):
-            K = pkg.build_stiffness_pattern(dmesh, ctx=ctx)
-            pkg.assemble_stiffness(dmesh, D, 1.0, K)
-            d_b.zero_()
-            pkg.add_traction(K, d_right, 1.0, 1.0, 0.0, d_b)  # loads on the GPU (bc.cpp:190-253)
-            pkg.apply_dirichlet((d_dofs, d_vals), K, d_b)
+            K = system()
             s = pkg.CgJacobiSolver(opts)
             s.setup(K)
             if learned_any:
@@ -507,7 +512,7 @@ def run_ours(a, dist: Dist):
 
     sync = torch.cuda.synchronize
     if a.only:
-        out = run_only(a, pkg, step, last, ctx, stream, ev_start, ev_stop, d_b, D, N, n, w_cycle)
+        out = run_only(a, pkg, step, system, last, ctx, stream, ev_start, ev_stop, d_b, D, N, n, w_cycle)
         print(json.dumps(out))
         ctx.close()
         return 0
@@ -672,14 +677,20 @@ def rooflines(a, pkg, K, ctx, stream, ev_start, ev_stop, N, n, mat, weights, pre
                time_launches(lambda: K.multiply_mixed(xs, ys)),
                profile_traffic("spmv_mixed_f32_plate2m.md") if full else None)
     out = {"spmv_fp64": r64, "spmv_mixed": r32}
-    # the network's layer: H in (128 B / node, BF16), H out, node pointers and neighbour indices once
+    # the network's layer: H in (128 B / node, BF16) once, H out, and the graph once: with a gather
+    # plan (every tile of the O-grid plates) the node slots (16 B / node) and the tiles' runs
+    # (80 B / tile), else the node pointers and neighbour indices
     with torch.cuda.stream(stream):
         pkg.learned.setup(K, weights, mat)
         tm = pkg.learned.time_stages(K, reps=50)
-    layer_bytes = N * 2 * 128 + (N + 1) * 4 + nb * 4
-    last_bytes = N * 128 + (N + 1) * 4 + nb * 4 + n * 8 * 3  # H in; r, D^-1 in, z out
+    planned = os.environ.get("CSTG_MP_GATHER", "") != "rows"
+    tiles = (N + 127) // 128
+    graph_bytes = N * 16 + tiles * 80 if planned else (N + 1) * 4 + nb * 4
+    layer_bytes = N * 2 * 128 + graph_bytes
+    last_bytes = N * 128 + graph_bytes + n * 8 * 3  # H in; r, D^-1 in, z out
     enc_bytes = N * (16 + 24 + 128)
-    lay = roof("k_mp_layer_tc (message-passing layer, tcgen05 BF16, layer 2 of 3)", layer_bytes, tm["layer_s"][1],
+    lay = roof("k_mp_layer_tc (message-passing layer, tcgen05 BF16, layer 2 of 3, "
+               + ("gather plan" if planned else "row gather") + ")", layer_bytes, tm["layer_s"][1],
                profile_traffic("mp_layer_tc_plate2m.md") if full else None,
                layers_us=[t * 1e6 for t in tm["layer_s"]], encoder_us=tm["encoder_s"] * 1e6,
                last_layer_gbs=last_bytes / tm["layer_s"][2] / 1e9, encoder_gbs=enc_bytes / tm["encoder_s"] / 1e9,
@@ -746,11 +757,18 @@ def run_e2e(a, pkg, dist, dev, mesh, D, dofs, vals, opts, weights, mat, learned_
             "path": "C ABI, host pinned buffers (cstg_set_mesh .. cstg_pcg_solve)"}
 
 
-def run_only(a, pkg, step, last, ctx, stream, ev_start, ev_stop, d_b, D, N, n, w_cycle):
+def run_only(a, pkg, step, system, last, ctx, stream, ev_start, ev_stop, d_b, D, N, n, w_cycle):
     import torch
     out = {"mode": a.only, "workload": a.workload}
     if a.only == "batch":
         out.update(run_batch(a, pkg, sweep_shapes=True, reps=a.reps))
+        return out
+    if a.only == "network":  # the assembled system and the network's stages alone, no solve before
+        with torch.cuda.stream(stream):
+            K = system()
+            pkg.CgJacobiSolver().setup(K)
+            pkg.learned.setup(K, w_cycle, pkg.learned.node_material(D, N))
+            out.update(pkg.learned.time_stages(K, reps=a.reps))
         return out
     step()
     torch.cuda.synchronize()
