@@ -49,7 +49,6 @@ __device__ __forceinline__ uint32_t pack_bf2(float a, float b) {
   return *reinterpret_cast<const uint32_t*>(&v);
 }
 __device__ __forceinline__ float bf(const __nv_bfloat16 v) { return __bfloat162float(v); }
-
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
@@ -64,6 +63,27 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint
   d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
   d |= (uint64_t)1 << 46;
   return d;
+}
+
+// UMMA shared-memory descriptor, K-major, 128-byte swizzle: atoms of 8 rows x 128 bytes (1024-byte
+// aligned), the 16-byte chunk q of row r stored at chunk q ^ (r % 8); `sbo` = byte distance between
+// 8-row groups. A K=16 slice inside an atom starts 32 bytes further per slice (the hardware applies
+// the XOR to the address bits). Bits 61-63 = 2: 128-byte swizzle.
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)1 << 16;  // leading byte offset: unused by swizzled K-major layouts
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;
+  d |= (uint64_t)2 << 61;
+  return d;
+}
+
+// Offset of 16-byte chunk c (features 8c..8c+7) of row m of the A tile: half 0 = the node's own
+// row (K 0..63), half 1 = the neighbours' mean (K 64..127); each half is a 128-row column of
+// 128-byte-swizzled atoms (16 KB), so the 8 chunks of one row sit in 8 different bank groups.
+__device__ __forceinline__ uint32_t a_chunk(int m, int c, int half) {
+  return (uint32_t)(half * 16384 + m * 128 + ((c ^ (m & 7)) << 4));
 }
 
 // Instruction descriptor of tcgen05.mma.kind::f16: D FP32, A and B BF16, both K-major,
@@ -118,10 +138,37 @@ constexpr int kRedGrid = 296;  // fixed grid of the reductions here (2 x 148): a
 
 // ---- residual scale ----------------------------------------------------------------------------
 
+// r'r over a fixed grid (a fixed order). VEC: r 16-byte aligned, pairs read as double2, four
+// pairs in flight per thread.
+template <bool VEC>
 __global__ void __launch_bounds__(256) k_mp_rr(int n, const double* __restrict__ r, MpScratch* sc, const int* skip) {
   if (skip && *skip) return;  // uniform: every block returns before the ticket
   double a = 0.0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a = fma(r[i], r[i], a);
+  const int stride = gridDim.x * blockDim.x, t0 = blockIdx.x * blockDim.x + threadIdx.x;
+  if (VEC) {
+    const double2* r2 = reinterpret_cast<const double2*>(r);
+    const int n2 = n >> 1;
+    int i = t0;
+    for (; i + 3 * stride < n2; i += 4 * stride) {
+      const double2 x0 = r2[i], x1 = r2[i + stride], x2 = r2[i + 2 * stride], x3 = r2[i + 3 * stride];
+      a = fma(x0.x, x0.x, a);
+      a = fma(x0.y, x0.y, a);
+      a = fma(x1.x, x1.x, a);
+      a = fma(x1.y, x1.y, a);
+      a = fma(x2.x, x2.x, a);
+      a = fma(x2.y, x2.y, a);
+      a = fma(x3.x, x3.x, a);
+      a = fma(x3.y, x3.y, a);
+    }
+    for (; i < n2; i += stride) {
+      const double2 x = r2[i];
+      a = fma(x.x, x.x, a);
+      a = fma(x.y, x.y, a);
+    }
+    if ((n & 1) && t0 == 0) a = fma(r[n - 1], r[n - 1], a);
+  } else {
+    for (int i = t0; i < n; i += stride) a = fma(r[i], r[i], a);
+  }
   const double v[1] = {a};
   double tot[1];
   if (grid_sum<1, 256>(v, sc->partials, &sc->ticket[0], tot) && threadIdx.x == 0) sc->rr = tot[0];
@@ -339,7 +386,8 @@ __global__ void __launch_bounds__(kEncT, kEncCtasPerSm) k_mp_encode(int N, const
     const int st = it & 1;
     const uint32_t par = (uint32_t)(it >> 1) & 1u;
     const uint32_t b = st ? bar1 : bar0;
-    const int got = mbar_wait(b, par, spin_limit) ? 1 : 0;
+    // thread 0 waits for the copies; the barrier hands their data (and the outcome) to the block
+    const int got = t == 0 ? (mbar_wait(b, par, spin_limit) ? 1 : 0) : 1;
     if (!__syncthreads_and(got)) {
       if (t == 0) {  // report, then let the copies in flight land (bounded) before leaving
         if (err) atomicMin(&err[kErrTimeout], ch);
@@ -462,33 +510,35 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
       : "r"(taddr));
 }
 
-__device__ __forceinline__ void add_chunk(float (&acc)[8], const uint4 v) {
-  acc[0] += bf_lo(v.x);
-  acc[1] += bf_hi(v.x);
-  acc[2] += bf_lo(v.y);
-  acc[3] += bf_hi(v.y);
-  acc[4] += bf_lo(v.z);
-  acc[5] += bf_hi(v.z);
-  acc[6] += bf_lo(v.w);
-  acc[7] += bf_hi(v.w);
+// Neighbour sums in FP32 pairs: acc[q] holds features (2q, 2q+1) of the lane's chunk as an
+// f32x2 pair; each BF16 pair of v is widened (exact) and added with one add.rn.f32x2 (two IEEE
+// round-to-nearest adds, the same results as two scalar adds in the same order).
+__device__ __forceinline__ void add_chunk2(unsigned long long (&acc)[4], const uint4 v) {
+  const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+    asm("{\n\t.reg .b32 lo, hi;\n\t.reg .b64 p;\n\t"
+        "shl.b32 lo, %1, 16;\n\t"
+        "and.b32 hi, %1, 0xffff0000;\n\t"
+        "mov.b64 p, {lo, hi};\n\t"
+        "add.rn.f32x2 %0, %0, p;\n\t}\n"
+        : "+l"(acc[q])
+        : "r"(w[q]));
+}
+// The chunk's mean as 8 BF16: each f32 of the pairs times inv, rounded to nearest.
+__device__ __forceinline__ uint4 mean_chunk(const unsigned long long (&acc)[4], float inv) {
+  uint32_t o[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    float x, y;
+    asm("mov.b64 {%0, %1}, %2;\n" : "=f"(x), "=f"(y) : "l"(acc[q]));
+    o[q] = pack_bf2(x * inv, y * inv);
+  }
+  return make_uint4(o[0], o[1], o[2], o[3]);
 }
 
 // Barrier of the tile warps: the whole CTA (rows), or named barrier 1 over threads 0..255 (plan,
 // where the producer warp keeps its own pace).
-// Shared-memory accesses by 32-bit shared address (ld/st.shared, on the short scoreboard).
-__device__ __forceinline__ uint4 lds128(uint32_t addr) {
-  uint4 v;
-  asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];\n"
-               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
-               : "r"(addr)
-               : "memory");
-  return v;
-}
-__device__ __forceinline__ void sts128(uint32_t addr, const uint4 v) {
-  asm volatile("st.shared.v4.u32 [%0], {%1, %2, %3, %4};\n" ::"r"(addr), "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w)
-               : "memory");
-}
-
 template <bool PLAN>
 __device__ __forceinline__ void tile_sync() {
   if constexpr (PLAN)
@@ -608,15 +658,17 @@ __global__ void __launch_bounds__(PLAN ? kLTPlan : kLT, PLAN ? kPlanCtasPerSm : 
   __shared__ float2 ypart[kTile];
   // each warp's neighbour lists for row-by-row tiles (the first kNbrCache entries)
   __shared__ int s_nbr[(kLT / 32) * kNbrCache];
-  uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
-  uint8_t* sA = base;               // element (m, k): (k/8)*2048 + (m/8)*128 + (m%8)*16 + (k%8)*2
+  // 1024-byte aligned base as an offset into the shared array (the compiler keeps the shared
+  // address space through pointer arithmetic on it: plain C++ accesses become ld/st.shared)
+  uint8_t* base = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+  uint8_t* sA = base;               // chunk k/8 of row m at a_chunk(m, (k/8) % 8, k/64), + (k%8)*2
   uint8_t* sB = base + kASmem;      // element (n, k): (k/8)*1024 + (n/8)*128 + (n%8)*16 + (k%8)*2
   uint8_t* sOut = sA + kASmem / 2;  // staged output tile (the mean half of A, free after the MMA)
   uint8_t* sU = sB + kBSmem;        // plan: the ring of union buffers
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const __nv_bfloat16* W = a.P.pb + kMpOffL0 + a.layer * kMpLStride;
   const float* bias_g = a.P.pf + kMpOffL0 + a.layer * kMpLStride + F * 2 * F;
-  __shared__ float bias[F];
+  __shared__ __align__(16) float bias[F];
   for (int i = t; i < F; i += blockDim.x) bias[i] = bias_g[i];
 
   for (int idx = t; idx < F * 16; idx += blockDim.x) {  // 64 rows x 16 chunks of 8 BF16
@@ -656,7 +708,6 @@ __global__ void __launch_bounds__(PLAN ? kLTPlan : kLT, PLAN ? kPlanCtasPerSm : 
   volatile int* abort_v = &abort_flag;
   const uint32_t tmem = tmem_slot;
   const uint32_t a_addr = smem_u32(sA), b_addr = smem_u32(sB), mbar_addr = smem_u32(&mbar);
-  const uint32_t out_addr = smem_u32(sOut);
   const double s = LAST ? sqrt(*a.rr * a.inv_n) : 0.0;
   uint32_t phase = 0;
   const int g = lane >> 3, c = lane & 7;  // gather: node group of the warp, feature chunk
@@ -675,7 +726,9 @@ __global__ void __launch_bounds__(PLAN ? kLTPlan : kLT, PLAN ? kPlanCtasPerSm : 
       // ---- A tile from the union buffer the producer filled
       const int st = kp % kUStages;
       const uint8_t* buf = sU + (size_t)st * kUSmem;
-      const int got = mbar_wait(full0 + 8u * st, (uint32_t)(kp / kUStages) & 1u, a.spin_limit) ? 1 : 0;
+      // thread 0 waits for the producer's copies; the barrier hands their data (and the outcome)
+      // to the tile warps
+      const int got = t == 0 ? (mbar_wait(full0 + 8u * st, (uint32_t)(kp / kUStages) & 1u, a.spin_limit) ? 1 : 0) : 1;
       if (!tile_sync_and<PLAN>(got)) {  // report and stop; the producer drains its copies
         if (t == 0) {
           if (a.err) atomicMin(&a.err[kErrTimeout], tile);
@@ -683,37 +736,30 @@ __global__ void __launch_bounds__(PLAN ? kLTPlan : kLT, PLAN ? kPlanCtasPerSm : 
         }
         break;
       }
-      const uint32_t buf_u = smem_u32(buf), slots_u = buf_u + kPlanMaxUnion * 128;
+      const uint4* slots = reinterpret_cast<const uint4*>(buf + kPlanMaxUnion * 128);
 #pragma unroll
       for (int rnd = 0; rnd < 4; ++rnd) {
         const int m = warp * 16 + rnd * 4 + g;
         const int n = tile * kTile + m;
         uint4 own = make_uint4(0u, 0u, 0u, 0u);
-        float acc[8];
-#pragma unroll
-        for (int j = 0; j < 8; ++j) acc[j] = 0.f;
+        unsigned long long acc[4] = {0ull, 0ull, 0ull, 0ull};  // +0.0f pairs
         int deg = 0;
         if (n < N) {
-          const uint4 lp = lds128(slots_u + (uint32_t)m * 16u);
+          const uint4 lp = slots[m];
           const uint32_t sl[8] = {lp.x & 0xFFFFu, lp.x >> 16, lp.y & 0xFFFFu, lp.y >> 16,
                                   lp.z & 0xFFFFu, lp.z >> 16, lp.w & 0xFFFFu, lp.w >> 16};
-          own = lds128(buf_u + sl[0] * 128u + c * 16);
+          own = *reinterpret_cast<const uint4*>(buf + sl[0] * 128u + c * 16);
 #pragma unroll
           for (int j = 1; j < 8; ++j)
             if (sl[j] != 0xFFFFu) {
               ++deg;
-              add_chunk(acc, lds128(buf_u + sl[j] * 128u + c * 16));
+              add_chunk2(acc, *reinterpret_cast<const uint4*>(buf + sl[j] * 128u + c * 16));
             }
         }
         const float inv = deg ? 1.f / (float)deg : 0.f;
-        uint4 av;
-        av.x = pack_bf2(acc[0] * inv, acc[1] * inv);
-        av.y = pack_bf2(acc[2] * inv, acc[3] * inv);
-        av.z = pack_bf2(acc[4] * inv, acc[5] * inv);
-        av.w = pack_bf2(acc[6] * inv, acc[7] * inv);
-        const uint32_t row_off = (uint32_t)((m >> 3) * 128 + (m & 7) * 16);
-        sts128(a_addr + c * 2048 + row_off, own);
-        sts128(a_addr + (8 + c) * 2048 + row_off, av);
+        const uint4 av = mean_chunk(acc, inv);
+        *reinterpret_cast<uint4*>(sA + a_chunk(m, c, 0)) = own;
+        *reinterpret_cast<uint4*>(sA + a_chunk(m, c, 1)) = av;
         if (TRAIN && n < N) reinterpret_cast<uint4*>(a.Aout + (size_t)n * F)[c] = av;
       }
       tile_sync<PLAN>();  // every tile warp is done with the buffer
@@ -748,9 +794,7 @@ __global__ void __launch_bounds__(PLAN ? kLTPlan : kLT, PLAN ? kPlanCtasPerSm : 
         const int k0 = __shfl_sync(0xffffffffu, np, li) - np0;
         const int k1 = __shfl_sync(0xffffffffu, np, li + 1) - np0;
         uint4 own = make_uint4(0u, 0u, 0u, 0u);
-        float acc[8];
-#pragma unroll
-        for (int j = 0; j < 8; ++j) acc[j] = 0.f;
+        unsigned long long acc[4] = {0ull, 0ull, 0ull, 0ull};  // +0.0f pairs
         int deg = 0;
         if (n < N) {
           own = __ldg(reinterpret_cast<const uint4*>(a.Hin + (size_t)n * F) + c);
@@ -770,19 +814,14 @@ __global__ void __launch_bounds__(PLAN ? kLTPlan : kLT, PLAN ? kPlanCtasPerSm : 
             for (int j = 0; j < 8; ++j)
               if (mm[j] != n) {
                 ++deg;
-                add_chunk(acc, v[j]);
+                add_chunk2(acc, v[j]);
               }
           }
         }
         const float inv = deg ? 1.f / (float)deg : 0.f;
-        uint4 av;
-        av.x = pack_bf2(acc[0] * inv, acc[1] * inv);
-        av.y = pack_bf2(acc[2] * inv, acc[3] * inv);
-        av.z = pack_bf2(acc[4] * inv, acc[5] * inv);
-        av.w = pack_bf2(acc[6] * inv, acc[7] * inv);
-        const uint32_t row_off = (uint32_t)((m >> 3) * 128 + (m & 7) * 16);
-        sts128(a_addr + c * 2048 + row_off, own);
-        sts128(a_addr + (8 + c) * 2048 + row_off, av);
+        const uint4 av = mean_chunk(acc, inv);
+        *reinterpret_cast<uint4*>(sA + a_chunk(m, c, 0)) = own;
+        *reinterpret_cast<uint4*>(sA + a_chunk(m, c, 1)) = av;
         if (TRAIN && n < N) reinterpret_cast<uint4*>(a.Aout + (size_t)n * F)[c] = av;
       }
       if (!PLAN) {  // prefetch the next tile's neighbour lists (asynchronous copies, done during the
@@ -805,8 +844,8 @@ __global__ void __launch_bounds__(PLAN ? kLTPlan : kLT, PLAN ? kPlanCtasPerSm : 
     if (t == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
 #pragma unroll
-      for (int j = 0; j < 8; ++j) {  // K = 128 in slices of 16: two 8-element halves each
-        const uint64_t ad = umma_desc(a_addr + (uint32_t)(2 * j) * 2048u, 2048u, 128u);
+      for (int j = 0; j < 8; ++j) {  // K = 128 in slices of 16: four per 64-wide swizzled half
+        const uint64_t ad = umma_desc_sw128(a_addr + (uint32_t)(j >> 2) * 16384u + (uint32_t)(j & 3) * 32u, 1024u);
         const uint64_t bd = umma_desc(b_addr + (uint32_t)(2 * j) * 1024u, 1024u, 128u);
         const uint32_t acc_flag = j > 0 ? 1u : 0u;
         asm volatile(
@@ -841,18 +880,19 @@ __global__ void __launch_bounds__(PLAN ? kLTPlan : kLT, PLAN ? kPlanCtasPerSm : 
     tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(h * 32), v);
     asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
     uint32_t hw[16];
-    const uint32_t row_off = (uint32_t)((m >> 3) * 128 + (m & 7) * 16);
 #pragma unroll
     for (int cc = 0; cc < 4; ++cc) {
       const int ch = 4 * h + cc;
-      const uint4 o4 = lds128(a_addr + ch * 2048 + row_off);
+      const uint4 o4 = *reinterpret_cast<const uint4*>(sA + a_chunk(m, ch, 0));
       const uint32_t ow[4] = {o4.x, o4.y, o4.z, o4.w};
       uint32_t gw[4];
+      const float4 b0 = *reinterpret_cast<const float4*>(&bias[ch * 8]);
+      const float4 b1 = *reinterpret_cast<const float4*>(&bias[ch * 8 + 4]);
+      const float bb[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
-        const int o = ch * 8 + 2 * j;
-        const float g0 = fmaxf(__uint_as_float(v[cc * 8 + 2 * j]) + bias[o], 0.f);
-        const float g1 = fmaxf(__uint_as_float(v[cc * 8 + 2 * j + 1]) + bias[o + 1], 0.f);
+        const float g0 = fmaxf(__uint_as_float(v[cc * 8 + 2 * j]) + bb[2 * j], 0.f);
+        const float g1 = fmaxf(__uint_as_float(v[cc * 8 + 2 * j + 1]) + bb[2 * j + 1], 0.f);
         hw[cc * 4 + j] = pack_bf2(bf_lo(ow[j]) + g0, bf_hi(ow[j]) + g1);
         gw[j] = pack_bf2(g0, g1);
       }
@@ -863,8 +903,8 @@ __global__ void __launch_bounds__(PLAN ? kLTPlan : kLT, PLAN ? kPlanCtasPerSm : 
 #pragma unroll
       for (int cc = 0; cc < 4; ++cc) {
         const int ch = 4 * h + cc;
-        sts128(out_addr + m * 128 + ((ch ^ (m & 7)) * 16),
-               make_uint4(hw[cc * 4], hw[cc * 4 + 1], hw[cc * 4 + 2], hw[cc * 4 + 3]));
+        *reinterpret_cast<uint4*>(sOut + m * 128 + ((ch ^ (m & 7)) * 16)) =
+            make_uint4(hw[cc * 4], hw[cc * 4 + 1], hw[cc * 4 + 2], hw[cc * 4 + 3]);
       }
     }
     float y0 = 0.f, y1 = 0.f;
@@ -918,7 +958,7 @@ __global__ void __launch_bounds__(PLAN ? kLTPlan : kLT, PLAN ? kPlanCtasPerSm : 
         const int nr = tile * kTile + row;
         if (nr < N)
           reinterpret_cast<uint4*>(a.Hout + (size_t)nr * F)[ch] =
-              lds128(out_addr + row * 128 + ((ch ^ (row & 7)) * 16));
+              *reinterpret_cast<const uint4*>(sOut + row * 128 + ((ch ^ (row & 7)) * 16));
       }
     }
     tile_sync<PLAN>();  // tensor memory and the A tile are free for the next tile
@@ -1404,7 +1444,10 @@ cudaError_t launch_mp_params(const float* p32, __nv_bfloat16* pb, float* pf, cud
 }
 
 cudaError_t launch_mp_rr(int n, const double* r, MpScratch* sc, cudaStream_t s, const int* skip) {
-  k_mp_rr<<<kRedGrid, 256, 0, s>>>(n, r, sc, skip);
+  if (reinterpret_cast<uintptr_t>(r) & 15u)
+    k_mp_rr<false><<<kRedGrid, 256, 0, s>>>(n, r, sc, skip);
+  else
+    k_mp_rr<true><<<kRedGrid, 256, 0, s>>>(n, r, sc, skip);
   count_launches(1);
   return cudaGetLastError();
 }
