@@ -510,31 +510,24 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
       : "r"(taddr));
 }
 
-// Neighbour sums in FP32 pairs: acc[q] holds features (2q, 2q+1) of the lane's chunk as an
-// f32x2 pair; each BF16 pair of v is widened (exact) and added with one add.rn.f32x2 (two IEEE
-// round-to-nearest adds, the same results as two scalar adds in the same order).
-__device__ __forceinline__ void add_chunk2(unsigned long long (&acc)[4], const uint4 v) {
+// Neighbour sums in FP32: acc[j] += feature j of the chunk v (8 BF16) with the mixed-precision
+// add.rn.f32.bf16 (the BF16 operand widened exactly, one IEEE round-to-nearest add: the same result
+// as widening and a scalar add, in one instruction per feature).
+__device__ __forceinline__ void add_chunk_bf(float (&acc)[8], const uint4 v) {
   const uint32_t w[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
   for (int q = 0; q < 4; ++q)
-    asm("{\n\t.reg .b32 lo, hi;\n\t.reg .b64 p;\n\t"
-        "shl.b32 lo, %1, 16;\n\t"
-        "and.b32 hi, %1, 0xffff0000;\n\t"
-        "mov.b64 p, {lo, hi};\n\t"
-        "add.rn.f32x2 %0, %0, p;\n\t}\n"
-        : "+l"(acc[q])
+    asm("{\n\t.reg .b16 lo, hi;\n\t"
+        "mov.b32 {lo, hi}, %2;\n\t"
+        "add.rn.f32.bf16 %0, lo, %0;\n\t"
+        "add.rn.f32.bf16 %1, hi, %1;\n\t}\n"
+        : "+f"(acc[2 * q]), "+f"(acc[2 * q + 1])
         : "r"(w[q]));
 }
-// The chunk's mean as 8 BF16: each f32 of the pairs times inv, rounded to nearest.
-__device__ __forceinline__ uint4 mean_chunk(const unsigned long long (&acc)[4], float inv) {
-  uint32_t o[4];
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    float x, y;
-    asm("mov.b64 {%0, %1}, %2;\n" : "=f"(x), "=f"(y) : "l"(acc[q]));
-    o[q] = pack_bf2(x * inv, y * inv);
-  }
-  return make_uint4(o[0], o[1], o[2], o[3]);
+// The chunk's mean as 8 BF16: each sum times inv, rounded to nearest.
+__device__ __forceinline__ uint4 mean_chunk(const float (&acc)[8], float inv) {
+  return make_uint4(pack_bf2(acc[0] * inv, acc[1] * inv), pack_bf2(acc[2] * inv, acc[3] * inv),
+                    pack_bf2(acc[4] * inv, acc[5] * inv), pack_bf2(acc[6] * inv, acc[7] * inv));
 }
 
 // Barrier of the tile warps: the whole CTA (rows), or named barrier 1 over threads 0..255 (plan,
@@ -742,7 +735,7 @@ __global__ void __launch_bounds__(PLAN ? kLTPlan : kLT, PLAN ? kPlanCtasPerSm : 
         const int m = warp * 16 + rnd * 4 + g;
         const int n = tile * kTile + m;
         uint4 own = make_uint4(0u, 0u, 0u, 0u);
-        unsigned long long acc[4] = {0ull, 0ull, 0ull, 0ull};  // +0.0f pairs
+        float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         int deg = 0;
         if (n < N) {
           const uint4 lp = slots[m];
@@ -753,7 +746,7 @@ __global__ void __launch_bounds__(PLAN ? kLTPlan : kLT, PLAN ? kPlanCtasPerSm : 
           for (int j = 1; j < 8; ++j)
             if (sl[j] != 0xFFFFu) {
               ++deg;
-              add_chunk2(acc, *reinterpret_cast<const uint4*>(buf + sl[j] * 128u + c * 16));
+              add_chunk_bf(acc, *reinterpret_cast<const uint4*>(buf + sl[j] * 128u + c * 16));
             }
         }
         const float inv = deg ? 1.f / (float)deg : 0.f;
@@ -794,7 +787,7 @@ __global__ void __launch_bounds__(PLAN ? kLTPlan : kLT, PLAN ? kPlanCtasPerSm : 
         const int k0 = __shfl_sync(0xffffffffu, np, li) - np0;
         const int k1 = __shfl_sync(0xffffffffu, np, li + 1) - np0;
         uint4 own = make_uint4(0u, 0u, 0u, 0u);
-        unsigned long long acc[4] = {0ull, 0ull, 0ull, 0ull};  // +0.0f pairs
+        float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         int deg = 0;
         if (n < N) {
           own = __ldg(reinterpret_cast<const uint4*>(a.Hin + (size_t)n * F) + c);
@@ -814,7 +807,7 @@ __global__ void __launch_bounds__(PLAN ? kLTPlan : kLT, PLAN ? kPlanCtasPerSm : 
             for (int j = 0; j < 8; ++j)
               if (mm[j] != n) {
                 ++deg;
-                add_chunk2(acc, v[j]);
+                add_chunk_bf(acc, v[j]);
               }
           }
         }
