@@ -830,6 +830,16 @@ __global__ void __launch_bounds__(PLAN ? kLTPlan : kLT, PLAN ? kPlanCtasPerSm : 
       }
     }
     ph = ph_next;
+    // the decoder's per-node inputs (last layer), loaded now so they arrive during the MMA
+    double2 rn_e = make_double2(0.0, 0.0), dn_e = rn_e, zb_e = rn_e;
+    if (LAST && (warp >> 2) == 1) {
+      const int ne = tile * kTile + (warp & 3) * 32 + lane;
+      if (ne < N) {
+        rn_e = reinterpret_cast<const double2*>(a.r)[ne];
+        dn_e = reinterpret_cast<const double2*>(a.invd)[ne];
+        if (a.zbase) zb_e = reinterpret_cast<const double2*>(a.zbase)[ne];
+      }
+    }
     // generic-proxy shared-memory writes -> visible to the tensor core (async proxy)
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
@@ -934,13 +944,10 @@ __global__ void __launch_bounds__(PLAN ? kLTPlan : kLT, PLAN ? kPlanCtasPerSm : 
         y1 = fmaf(wout[F + f + 1], bf_hi(hw[j]), y1);
       }
       if (TRAIN) reinterpret_cast<float2*>(a.Yout)[n] = make_float2(y0, y1);
-      const double2 rn = reinterpret_cast<const double2*>(a.r)[n];
-      const double2 dn = reinterpret_cast<const double2*>(a.invd)[n];
-      double2 zn = make_double2(dn.x * (rn.x + s * (double)y0), dn.y * (rn.y + s * (double)y1));
+      double2 zn = make_double2(dn_e.x * (rn_e.x + s * (double)y0), dn_e.y * (rn_e.y + s * (double)y1));
       if (a.zbase) {
-        const double2 zb = reinterpret_cast<const double2*>(a.zbase)[n];
-        zn.x += zb.x;
-        zn.y += zb.y;
+        zn.x += zb_e.x;
+        zn.y += zb_e.y;
       }
       reinterpret_cast<double2*>(a.z)[n] = zn;
     }
