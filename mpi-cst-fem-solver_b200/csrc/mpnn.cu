@@ -6,7 +6,9 @@
 //   A_l  = mean over neighbours m of H_{l-1,m}                             BF16 [N][64]
 //   H_l  = H_{l-1} + relu(W_l [H_{l-1}; A_l] + b_l)      l = 1..3          BF16 [N][64]
 //   Y    = W_out H3 + b_out                                                FP32 [N][2]
-// Weights are BF16 (biases FP32); every product accumulates in FP32.
+// Weights are BF16 (biases FP32); every product accumulates in FP32. The encoder's 8 -> 64 product
+// runs on the tensor cores too (one K=16 MMA per 128 nodes, the FP32 bias entering as three exact
+// BF16 parts against constant ones in the A operand).
 //
 // The three message-passing layers run on the 5th-generation tensor cores: a CTA owns a tile of
 // 128 nodes at a time, builds each node's own row and the mean of its neighbours' rows in shared
@@ -310,131 +312,6 @@ __global__ void k_mp_smoother_weights(int n, const double* __restrict__ invd, co
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = w * invd[i];
 }
 
-// ---- encoder: H0 = relu(W_in X + b_in) ------------------------------------------------------------
-//
-// Persistent CTAs over chunks of kEncChunk consecutive nodes. Thread 0 brings a chunk's inputs
-// (r: 16 B per node, the static inputs: 24 B per node, both contiguous) into shared memory with
-// two bulk copies completing on an mbarrier, one chunk ahead of the compute (two stages), so whole
-// chunks of loads are in flight rather than a few per thread. Eight threads per node: thread c
-// holds the weights and biases of features 8c..8c+7 in registers (64 + 8, loaded once), forms
-// input c of its node (r / s for c < 2, a static input otherwise), rounds it to BF16 and takes
-// the other seven from its group by shuffles. A warp writes four whole 128-byte rows. Each
-// feature is the same chain of FMAs in the same order for every launch shape. The static
-// inputs' buffer holds 16 bytes past its 24 N (a ragged last chunk's copy is rounded up to 16
-// bytes).
-constexpr int kEncChunk = 256;                              // nodes per chunk
-constexpr int kEncT = 256;                                  // threads of the encoder
-constexpr int kEncStage = kEncChunk * 16 + kEncChunk * 24;  // one stage: r, then the static inputs
-constexpr int kEncCtasPerSm = 2;
-
-template <bool TRAIN>
-__global__ void __launch_bounds__(kEncT, kEncCtasPerSm) k_mp_encode(int N, const double* __restrict__ r, const double* rr,
-                                                     double inv_n, const float* __restrict__ sf, MpnnParams P,
-                                                     const int* skip, __nv_bfloat16* __restrict__ H0,
-                                                     __nv_bfloat16* __restrict__ Xout, long long spin_limit,
-                                                     int* err) {
-  if (skip && *skip) return;  // uniform: before any barrier
-  __shared__ __align__(128) uint8_t stage[2][kEncStage];
-  __shared__ uint64_t bar[2];
-  const int t = threadIdx.x, lane = t & 31;
-  const int c = t & 7, grp = t >> 3;
-  const int chunks = (N + kEncChunk - 1) / kEncChunk;
-  // this thread's weights W_in[8c + j][k] and biases b_in[8c + j]
-  float w[8][kMpIn], bsv[8];
-#pragma unroll
-  for (int j = 0; j < 8; ++j) {
-    const uint4 q = *reinterpret_cast<const uint4*>(P.pb + kMpOffWin + (8 * c + j) * kMpIn);
-    w[j][0] = bf_lo(q.x);
-    w[j][1] = bf_hi(q.x);
-    w[j][2] = bf_lo(q.y);
-    w[j][3] = bf_hi(q.y);
-    w[j][4] = bf_lo(q.z);
-    w[j][5] = bf_hi(q.z);
-    w[j][6] = bf_lo(q.w);
-    w[j][7] = bf_hi(q.w);
-    bsv[j] = P.pf[kMpOffBin + 8 * c + j];
-  }
-  const uint32_t bar0 = smem_u32(&bar[0]), bar1 = smem_u32(&bar[1]);
-  auto issue = [&](int ch, int st) {  // thread 0: chunk ch into stage st
-    const int first = ch * kEncChunk, cnt = min(kEncChunk, N - first);
-    const uint32_t rb = (uint32_t)cnt * 16u, sb = ((uint32_t)cnt * 24u + 15u) & ~15u;
-    const uint32_t b = st ? bar1 : bar0;
-    // the stage's earlier generic reads are ordered before the copies' writes
-    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(b), "r"(rb + sb) : "memory");
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
-                     smem_u32(stage[st])),
-                 "l"(r + 2 * (size_t)first), "r"(rb), "r"(b)
-                 : "memory");
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
-                     smem_u32(stage[st] + kEncChunk * 16)),
-                 "l"(sf + 6 * (size_t)first), "r"(sb), "r"(b)
-                 : "memory");
-  };
-  if (t == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar0), "r"(1));
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar1), "r"(1));
-    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-    if ((int)blockIdx.x < chunks) issue(blockIdx.x, 0);
-    if ((int)(blockIdx.x + gridDim.x) < chunks) issue(blockIdx.x + gridDim.x, 1);
-  }
-  __syncthreads();
-  const double s = sqrt(*rr * inv_n);
-  const double sd = s > 0.0 ? s : 1.0;
-  int it = 0;
-  for (int ch = blockIdx.x; ch < chunks; ch += gridDim.x, ++it) {
-    const int st = it & 1;
-    const uint32_t par = (uint32_t)(it >> 1) & 1u;
-    const uint32_t b = st ? bar1 : bar0;
-    // thread 0 waits for the copies; the barrier hands their data (and the outcome) to the block
-    const int got = t == 0 ? (mbar_wait(b, par, spin_limit) ? 1 : 0) : 1;
-    if (!__syncthreads_and(got)) {
-      if (t == 0) {  // report, then let the copies in flight land (bounded) before leaving
-        if (err) atomicMin(&err[kErrTimeout], ch);
-        mbar_wait(b, par, kMbarSpinLimit);
-        if (ch + (int)gridDim.x < chunks) mbar_wait(st ? bar0 : bar1, (uint32_t)((it + 1) >> 1) & 1u, kMbarSpinLimit);
-      }
-      return;
-    }
-    const double* sr = reinterpret_cast<const double*>(stage[st]);
-    const float* ss = reinterpret_cast<const float*>(stage[st] + kEncChunk * 16);
-    const int first = ch * kEncChunk, cnt = min(kEncChunk, N - first);
-#pragma unroll 1
-    for (int j = 0; j < kEncChunk / 32; ++j) {
-      const int ln0 = j * 32 + grp;
-      const bool live = ln0 < cnt;  // every lane takes part in the shuffles
-      const int ln = live ? ln0 : cnt - 1;
-      float xc = c < 2 ? (float)(sr[2 * ln + c] / sd) : ss[6 * ln + c - 2];
-      xc = __bfloat162float(__float2bfloat16_rn(xc));
-      float x[kMpIn];
-#pragma unroll
-      for (int k = 0; k < kMpIn; ++k) x[k] = __shfl_sync(0xffffffffu, xc, (lane & 24) | k);
-      if (!live) continue;
-      const int n = first + ln;
-      if (TRAIN && c == 0) {
-        uint4 xv;
-        xv.x = pack_bf2(x[0], x[1]);
-        xv.y = pack_bf2(x[2], x[3]);
-        xv.z = pack_bf2(x[4], x[5]);
-        xv.w = pack_bf2(x[6], x[7]);
-        reinterpret_cast<uint4*>(Xout)[n] = xv;
-      }
-      float u[8];
-#pragma unroll
-      for (int jj = 0; jj < 8; ++jj) {
-        u[jj] = bsv[jj];
-#pragma unroll
-        for (int k = 0; k < kMpIn; ++k) u[jj] = fmaf(w[jj][k], x[k], u[jj]);
-      }
-      reinterpret_cast<uint4*>(H0 + (size_t)n * F)[c] =
-          make_uint4(pack_bf2(fmaxf(u[0], 0.f), fmaxf(u[1], 0.f)), pack_bf2(fmaxf(u[2], 0.f), fmaxf(u[3], 0.f)),
-                     pack_bf2(fmaxf(u[4], 0.f), fmaxf(u[5], 0.f)), pack_bf2(fmaxf(u[6], 0.f), fmaxf(u[7], 0.f)));
-    }
-    __syncthreads();  // every thread is done with the stage
-    if (t == 0 && ch + 2 * (int)gridDim.x < chunks) issue(ch + 2 * gridDim.x, st);
-  }
-}
-
 // ---- message-passing layer on the tensor cores ----------------------------------------------------
 //
 // A CTA owns a tile of 128 nodes at a time (persistent over tiles); its 8 tile warps build the A
@@ -509,6 +386,206 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
         "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
       : "r"(taddr));
 }
+
+// ---- encoder on the tensor cores: H0 = relu(W_in X + b_in) -----------------------------------------
+//
+// Persistent CTAs over tiles of 128 consecutive nodes. Thread 0 brings a tile's inputs (r: 16 B
+// per node, the static inputs: 24 B per node, both contiguous) into shared memory with two bulk
+// copies completing on an mbarrier, one tile ahead (two stages). Two threads per node form the
+// node's BF16 input row X (thread pair half 0: r/s and the first two static inputs, half 1: the
+// other four) as the A operand (K-major, no swizzle; K = 16: the 8 inputs, then three ones and
+// zeros). B holds W_in (K 0..7) and the bias split exactly into three BF16 parts (K 8..10:
+// b = b_hi + b_mid + b_lo), so one tcgen05.mma (M=128, N=64, K=16) gives W_in X + b in FP32 in
+// tensor memory. Epilogue: each warp reads 32 lanes x 32 columns (tcgen05.ld.32x32b.x32), applies
+// ReLU, stages the BF16 rows XOR-swizzled in shared memory and the tile leaves in coalesced
+// 16-byte stores. Every wait is bounded; a timeout is recorded and the CTA leaves through the
+// common exit. The static inputs' buffer holds 16 bytes past its 24 N (a ragged last tile's copy
+// is rounded up to 16 bytes).
+constexpr int kEncT = 256;                          // threads of the encoder
+constexpr int kEncTile = 128;                       // nodes per tile (the MMA's M)
+constexpr int kEncStage = kEncTile * 16 + kEncTile * 24;  // one stage: r, then the static inputs
+constexpr int kEncCtasPerSm = 4;
+
+template <bool TRAIN>
+__global__ void __launch_bounds__(kEncT, kEncCtasPerSm) k_mp_encode(int N, const double* __restrict__ r, const double* rr,
+                                                     double inv_n, const float* __restrict__ sf, MpnnParams P,
+                                                     const int* skip, __nv_bfloat16* __restrict__ H0,
+                                                     __nv_bfloat16* __restrict__ Xout, long long spin_limit,
+                                                     int* err) {
+  if (skip && *skip) return;  // uniform: before any barrier or tensor-memory allocation
+  __shared__ __align__(128) uint8_t stage[2][kEncStage];
+  __shared__ __align__(128) uint8_t sX[4096];   // A: k 0..7 at +0, k 8..15 at +2048 (rows of 16 B)
+  __shared__ __align__(128) uint8_t sB[2048];   // B: k 0..7 at +0, k 8..15 at +1024
+  __shared__ __align__(128) uint8_t sOut[kEncTile * 128];
+  __shared__ uint64_t bar[2], mbar;
+  __shared__ uint32_t tmem_slot;
+  __shared__ int mma_ok;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const int tiles = (N + kEncTile - 1) / kEncTile;
+  // constant operand parts: the ones of A's second K half, W_in and the split bias in B
+  if (t < kEncTile) {
+    const int m = t;
+    *reinterpret_cast<uint4*>(sX + 2048 + (m >> 3) * 128 + (m & 7) * 16) =
+        make_uint4(0x3F803F80u, 0x00003F80u, 0u, 0u);  // BF16 1, 1, 1, 0, 0, 0, 0, 0
+  } else if (t < kEncTile + F) {
+    const int n = t - kEncTile;
+    const uint4 wrow = *reinterpret_cast<const uint4*>(P.pb + kMpOffWin + n * kMpIn);
+    *reinterpret_cast<uint4*>(sB + (n >> 3) * 128 + (n & 7) * 16) = wrow;
+    const float b = P.pf[kMpOffBin + n];
+    const __nv_bfloat16 b0 = __float2bfloat16_rn(b);
+    const float r1 = b - __bfloat162float(b0);
+    const __nv_bfloat16 b1 = __float2bfloat16_rn(r1);
+    const __nv_bfloat16 b2 = __float2bfloat16_rn(r1 - __bfloat162float(b1));
+    const uint32_t w0 = (uint32_t)__bfloat16_as_ushort(b0) | ((uint32_t)__bfloat16_as_ushort(b1) << 16);
+    *reinterpret_cast<uint4*>(sB + 1024 + (n >> 3) * 128 + (n & 7) * 16) =
+        make_uint4(w0, (uint32_t)__bfloat16_as_ushort(b2), 0u, 0u);
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_slot)),
+                 "r"(F));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  const uint32_t bar0 = smem_u32(&bar[0]), bar1 = smem_u32(&bar[1]), mbar_addr = smem_u32(&mbar);
+  auto issue = [&](int tl, int st) {  // thread 0: tile tl's inputs into stage st
+    const int first = tl * kEncTile, cnt = min(kEncTile, N - first);
+    const uint32_t rb = (uint32_t)cnt * 16u, sb = ((uint32_t)cnt * 24u + 15u) & ~15u;
+    const uint32_t b = st ? bar1 : bar0;
+    // the stage's earlier generic reads are ordered before the copies' writes
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(b), "r"(rb + sb) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     smem_u32(stage[st])),
+                 "l"(r + 2 * (size_t)first), "r"(rb), "r"(b)
+                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     smem_u32(stage[st] + kEncTile * 16)),
+                 "l"(sf + 6 * (size_t)first), "r"(sb), "r"(b)
+                 : "memory");
+  };
+  if (t == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar0), "r"(1));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar1), "r"(1));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(mbar_addr), "r"(1));
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    if ((int)blockIdx.x < tiles) issue(blockIdx.x, 0);
+    if ((int)(blockIdx.x + gridDim.x) < tiles) issue(blockIdx.x + gridDim.x, 1);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const uint32_t tmem = tmem_slot;
+  const uint64_t adesc = umma_desc(smem_u32(sX), 2048u, 128u);
+  const uint64_t bdesc = umma_desc(smem_u32(sB), 1024u, 128u);
+  const double s = sqrt(*rr * inv_n);
+  const double sd = s > 0.0 ? s : 1.0;
+  const int q = warp & 3, h = warp >> 2;  // epilogue: TMEM lane quarter, column half
+  uint32_t phase = 0;
+  int it = 0, used = 0;  // loop iterations; tiles whose inputs were consumed
+  // (thread 0) tiles whose inputs were issued and not yet consumed
+  int pending = ((int)blockIdx.x < tiles ? 1 : 0) + ((int)(blockIdx.x + gridDim.x) < tiles ? 1 : 0);
+  for (int tl = blockIdx.x; tl < tiles; tl += gridDim.x, ++it) {
+    const int st = it & 1;
+    const uint32_t b = st ? bar1 : bar0;
+    // thread 0 waits for the copies; the barrier hands their data (and the outcome) to the block
+    const int got = t == 0 ? (mbar_wait(b, (uint32_t)(it >> 1) & 1u, spin_limit) ? 1 : 0) : 1;
+    if (!__syncthreads_and(got)) {
+      if (t == 0 && err) atomicMin(&err[kErrTimeout], tl);
+      break;
+    }
+    --pending;
+    ++used;
+    const int first = tl * kEncTile, cnt = min(kEncTile, N - first);
+    {  // the input rows: thread pair (node m, half hf)
+      const int m = t & (kEncTile - 1), hf = t >> 7;
+      const double* sr = reinterpret_cast<const double*>(stage[st]);
+      const float* ss = reinterpret_cast<const float*>(stage[st] + kEncTile * 16);
+      uint2 xv = make_uint2(0u, 0u);
+      if (m < cnt) {
+        float x0, x1, x2, x3;
+        if (hf == 0) {
+          x0 = (float)(sr[2 * m] / sd);
+          x1 = (float)(sr[2 * m + 1] / sd);
+          x2 = ss[6 * m];
+          x3 = ss[6 * m + 1];
+        } else {
+          x0 = ss[6 * m + 2];
+          x1 = ss[6 * m + 3];
+          x2 = ss[6 * m + 4];
+          x3 = ss[6 * m + 5];
+        }
+        xv = make_uint2(pack_bf2(x0, x1), pack_bf2(x2, x3));
+        if (TRAIN) reinterpret_cast<uint2*>(Xout + (size_t)(first + m) * kMpIn)[hf] = xv;
+      }
+      *reinterpret_cast<uint2*>(sX + (m >> 3) * 128 + (m & 7) * 16 + hf * 8) = xv;
+    }
+    // generic-proxy shared-memory writes -> visible to the tensor core (async proxy)
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (t == 0) {
+      if (tl + 2 * (int)gridDim.x < tiles) {  // the stage is read: the tile after next into it
+        issue(tl + 2 * gridDim.x, st);
+        ++pending;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+      asm volatile(
+          "{\n\t.reg .pred p;\n\t"
+          "setp.ne.b32 p, %4, 0;\n\t"
+          "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+          "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(0u), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(mbar_addr)
+                   : "memory");
+      int ok = mbar_wait(mbar_addr, phase, spin_limit) ? 1 : 0;
+      if (!ok) {  // report, then let the MMA finish (bounded) before memory is released
+        if (err) atomicMin(&err[kErrTimeout], tl);
+        mbar_wait(mbar_addr, phase, kMbarSpinLimit);
+      }
+      mma_ok = ok;
+      asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    }
+    phase ^= 1u;
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    if (!mma_ok) break;  // uniform
+    {  // epilogue: ReLU, BF16, staged rows
+      const int m = q * 32 + lane;
+      uint32_t v[32];
+      tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(h * 32), v);
+      asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+      for (int cc = 0; cc < 4; ++cc) {
+        const int ch = 4 * h + cc;
+        uint32_t o[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          o[j] = pack_bf2(fmaxf(__uint_as_float(v[cc * 8 + 2 * j]), 0.f),
+                          fmaxf(__uint_as_float(v[cc * 8 + 2 * j + 1]), 0.f));
+        *reinterpret_cast<uint4*>(sOut + m * 128 + ((ch ^ (m & 7)) * 16)) = make_uint4(o[0], o[1], o[2], o[3]);
+      }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {  // the staged tile, in coalesced 16-byte stores
+      const int u = t + kEncT * i, row = u >> 3, ch = u & 7;
+      if (row < cnt)
+        reinterpret_cast<uint4*>(H0 + (size_t)(first + row) * F)[ch] =
+            *reinterpret_cast<const uint4*>(sOut + row * 128 + ((ch ^ (row & 7)) * 16));
+    }
+    __syncthreads();  // sOut, sX and tensor memory are free for the next tile
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  }
+  if (t == 0) {  // copies still in flight (after a timeout) land before the CTA leaves (bounded)
+    for (int j = 0; j < pending; ++j) {
+      const int jt = used + j;
+      mbar_wait((jt & 1) ? bar1 : bar0, (uint32_t)(jt >> 1) & 1u, kMbarSpinLimit);
+    }
+  }
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(F));
+}
+
 
 // Neighbour sums in FP32: acc[j] += feature j of the chunk v (8 BF16) with the mixed-precision
 // add.rn.f32.bf16 (the BF16 operand widened exactly, one IEEE round-to-nearest add: the same result
@@ -1377,8 +1454,8 @@ cudaError_t set_tc_attr() {
 
 int enc_grid(int N) {  // one wave of kEncCtasPerSm CTAs per SM at most
   const int sms = g_sms[dev_slot()] > 0 ? g_sms[dev_slot()] : kSMs;
-  const int chunks = (N + kEncChunk - 1) / kEncChunk;
-  return std::max(1, std::min(chunks, kEncCtasPerSm * sms));
+  const int tiles = (N + kEncTile - 1) / kEncTile;
+  return std::max(1, std::min(tiles, kEncCtasPerSm * sms));
 }
 
 // One wave of the layer kernel: kLayerCtasPerSm CTAs on every SM (rows; the register cap of
