@@ -119,6 +119,7 @@ struct cstg_ctx {
   unsigned long long pattern_count = 0;  // bumped by every cstg_build_pattern
   unsigned long long lp_plan_for = ~0ull;
   bool lp_plan_on = true;  // CSTG_MP_GATHER=rows turns the plan off (every tile gathers row by row)
+  bool lp_plan_use = false;  // the plan covers at least a quarter of the tiles
   // truncated flexible CG: ring of earlier directions and their A-products, ring state
   DevBuf fcg_ph[kFcgMaxHist], fcg_qh[kFcgMaxHist], fcg_ring;
 

@@ -182,7 +182,7 @@ struct MpnnParams {  // device copies of the packed parameters
 // kPlanMaxUnion rows, and per node the positions of its own row and of its neighbours' rows
 // (ascending pattern order) in that union. A tile that does not fit is marked and gathered row by
 // row instead.
-constexpr int kPlanMaxRuns = 8, kPlanMaxUnion = 416, kPlanMaxLocal = 7, kPlanSpan = 4096;
+constexpr int kPlanMaxRuns = 8, kPlanMaxUnion = 400, kPlanMaxLocal = 7, kPlanSpan = 4096;
 struct MpTilePlan {
   const int4* hdr = nullptr;    // [tiles]: (runs, union rows, fallback, 0)
   const int2* runs = nullptr;   // [tiles][kPlanMaxRuns]: (first node, rows)

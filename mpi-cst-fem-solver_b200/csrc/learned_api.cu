@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <vector>
 
 #include "ctx.h"
 
@@ -37,9 +38,19 @@ int plan_ready(cstg_ctx* ctx) {
   ENSURE(ctx->lp_plan_hdr, sizeof(int4) * (size_t)tiles);
   ENSURE(ctx->lp_plan_runs, sizeof(int2) * (size_t)tiles * kPlanMaxRuns);
   ENSURE(ctx->lp_plan_local, sizeof(uint4) * (size_t)std::max(N, 1));
-  if (N)
+  int planned = 0;
+  if (N) {
     CK(launch_mp_tile_plan(N, buf_ptr<int>(ctx->node_ptr), buf_ptr<int>(ctx->bnbr), buf_ptr<int4>(ctx->lp_plan_hdr),
                            buf_ptr<int2>(ctx->lp_plan_runs), buf_ptr<uint4>(ctx->lp_plan_local), ctx->stream));
+    std::vector<int4> hdr((size_t)tiles);
+    CK(cudaMemcpyAsync(hdr.data(), ctx->lp_plan_hdr.p, sizeof(int4) * hdr.size(), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (const int4& h : hdr) planned += h.z == 0 ? 1 : 0;
+  }
+  // the plan kernel (2 CTAs per SM, bulk-copied unions) pays off when a good share of the tiles
+  // is planned; patterns numbered without locality (most tiles rejected) keep the row kernel
+  ctx->lp_plan_use = 4 * planned >= tiles;
   ctx->lp_plan_for = ctx->pattern_count;
   return CSTG_OK;
 }
@@ -49,7 +60,7 @@ MpnnGraph graph_view(cstg_ctx* ctx) {
   g.n_nodes = ctx->n_nodes;
   g.node_ptr = buf_ptr<int>(ctx->node_ptr);
   g.nbr = buf_ptr<int>(ctx->bnbr);
-  if (ctx->lp_plan_on && ctx->lp_plan_for == ctx->pattern_count) {
+  if (ctx->lp_plan_on && ctx->lp_plan_use && ctx->lp_plan_for == ctx->pattern_count) {
     g.plan.hdr = buf_ptr<int4>(ctx->lp_plan_hdr);
     g.plan.runs = buf_ptr<int2>(ctx->lp_plan_runs);
     g.plan.local = buf_ptr<uint4>(ctx->lp_plan_local);

@@ -344,12 +344,14 @@ __global__ void k_mp_smoother_weights(int n, const double* __restrict__ invd, co
 constexpr int kLT = 256;                 // the tile warps' threads
 constexpr int kLTPlan = kLT + 32;        // + the producer warp
 constexpr int kNbrCache = 128;           // neighbour-list entries a warp keeps in shared memory
-constexpr int kLayerCtasPerSm = 4;       // rows: resident CTAs per SM (registers capped to fit them)
+constexpr int kLayerCtasPerSm = 3;       // rows: resident CTAs per SM (registers capped to fit them)
 constexpr int kPlanCtasPerSm = 2;        // plan: resident CTAs per SM
 constexpr int kUStages = 1;              // plan: union buffers per CTA
 constexpr int kUSmem = kPlanMaxUnion * 128 + kTile * 16;  // one buffer: the rows, then the node slots
-constexpr int kTcSmem = kASmem + kBSmem + 1024;           // dynamic shared memory (1024-byte aligned base)
-constexpr int kTcSmemPlan = kASmem + kBSmem + kUStages * kUSmem + 1024;
+// the bias slice: A's constant K-slice of ones (128 x 16 BF16) and B's bias rows (64 x 16 BF16)
+constexpr int kBiasSmem = 4096 + 2048;
+constexpr int kTcSmem = kASmem + kBSmem + kBiasSmem + 1024;  // dynamic shared memory (1024-byte aligned base)
+constexpr int kTcSmemPlan = kASmem + kBSmem + kUStages * kUSmem + kBiasSmem + 1024;
 
 struct MpLayerArgs {
   int N;
@@ -727,7 +729,7 @@ __global__ void __launch_bounds__(PLAN ? kLTPlan : kLT, PLAN ? kPlanCtasPerSm : 
   __shared__ float wout[2 * F], bout[2];
   __shared__ float2 ypart[kTile];
   // each warp's neighbour lists for row-by-row tiles (the first kNbrCache entries)
-  __shared__ int s_nbr[(kLT / 32) * kNbrCache];
+  __shared__ int s_nbr[PLAN ? 1 : (kLT / 32) * kNbrCache];
   // 1024-byte aligned base as an offset into the shared array (the compiler keeps the shared
   // address space through pointer arithmetic on it: plain C++ accesses become ld/st.shared)
   uint8_t* base = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
@@ -737,9 +739,25 @@ __global__ void __launch_bounds__(PLAN ? kLTPlan : kLT, PLAN ? kPlanCtasPerSm : 
   uint8_t* sU = sB + kBSmem;        // plan: the ring of union buffers
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const __nv_bfloat16* W = a.P.pb + kMpOffL0 + a.layer * kMpLStride;
-  const float* bias_g = a.P.pf + kMpOffL0 + a.layer * kMpLStride + F * 2 * F;
-  __shared__ __align__(16) float bias[F];
-  for (int i = t; i < F; i += blockDim.x) bias[i] = bias_g[i];
+  // the bias enters the MMA as a ninth K-slice: ones in A (K 0..2) against the FP32 bias split
+  // exactly into three BF16 parts in B (b = b_hi + b_mid + b_lo)
+  uint8_t* sOnes = sB + kBSmem + (PLAN ? kUStages * kUSmem : 0);
+  uint8_t* sBias = sOnes + 4096;
+  if (t < kTile) {
+    *reinterpret_cast<uint4*>(sOnes + (t >> 3) * 128 + (t & 7) * 16) = make_uint4(0x3F803F80u, 0x00003F80u, 0u, 0u);
+    *reinterpret_cast<uint4*>(sOnes + 2048 + (t >> 3) * 128 + (t & 7) * 16) = make_uint4(0u, 0u, 0u, 0u);
+  } else if (t < kTile + F) {
+    const int n = t - kTile;
+    const float b = a.P.pf[kMpOffL0 + a.layer * kMpLStride + F * 2 * F + n];
+    const __nv_bfloat16 b0 = __float2bfloat16_rn(b);
+    const float r1 = b - __bfloat162float(b0);
+    const __nv_bfloat16 b1 = __float2bfloat16_rn(r1);
+    const __nv_bfloat16 b2 = __float2bfloat16_rn(r1 - __bfloat162float(b1));
+    const uint32_t w0 = (uint32_t)__bfloat16_as_ushort(b0) | ((uint32_t)__bfloat16_as_ushort(b1) << 16);
+    *reinterpret_cast<uint4*>(sBias + (n >> 3) * 128 + (n & 7) * 16) =
+        make_uint4(w0, (uint32_t)__bfloat16_as_ushort(b2), 0u, 0u);
+    *reinterpret_cast<uint4*>(sBias + 1024 + (n >> 3) * 128 + (n & 7) * 16) = make_uint4(0u, 0u, 0u, 0u);
+  }
 
   for (int idx = t; idx < F * 16; idx += blockDim.x) {  // 64 rows x 16 chunks of 8 BF16
     const int n = idx >> 4, kc = idx & 15;
@@ -845,7 +863,8 @@ __global__ void __launch_bounds__(PLAN ? kLTPlan : kLT, PLAN ? kPlanCtasPerSm : 
         if (lane <= 16) np = __ldg(&a.node_ptr[min(wbase + lane, N)]);
         const int f0 = __shfl_sync(0xffffffffu, np, 0);
         const int fc = __shfl_sync(0xffffffffu, np, 16) - f0;
-        for (int j = lane; j < min(fc, kNbrCache); j += 32) wnbr[j] = __ldg(&a.nbr[f0 + j]);
+        if (!PLAN)  // (the plan kernel reads a fallback tile's lists from global memory)
+          for (int j = lane; j < min(fc, kNbrCache); j += 32) wnbr[j] = __ldg(&a.nbr[f0 + j]);
         first = false;
       } else {
         asm volatile("cp.async.wait_all;\n" ::: "memory");
@@ -874,7 +893,7 @@ __global__ void __launch_bounds__(PLAN ? kLTPlan : kLT, PLAN ? kPlanCtasPerSm : 
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
               const int q8 = k + j;
-              mm[j] = q8 < k1 ? (q8 < kNbrCache ? wnbr[q8] : __ldg(&a.nbr[np0 + q8])) : n;
+              mm[j] = q8 < k1 ? (!PLAN && q8 < kNbrCache ? wnbr[q8] : __ldg(&a.nbr[np0 + q8])) : n;
             }
 #pragma unroll
             for (int j = 0; j < 8; ++j)
@@ -934,6 +953,15 @@ __global__ void __launch_bounds__(PLAN ? kLTPlan : kLT, PLAN ? kPlanCtasPerSm : 
             "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
             "l"(ad), "l"(bd), "r"(kIdesc), "r"(acc_flag), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
       }
+      {  // + ones x bias parts
+        const uint64_t ad = umma_desc(smem_u32(sOnes), 2048u, 128u);
+        const uint64_t bd = umma_desc(smem_u32(sBias), 1024u, 128u);
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+            "l"(ad), "l"(bd), "r"(kIdesc), "r"(1u), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+      }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
                        mbar_addr)
                    : "memory");
@@ -966,13 +994,10 @@ __global__ void __launch_bounds__(PLAN ? kLTPlan : kLT, PLAN ? kPlanCtasPerSm : 
       const uint4 o4 = *reinterpret_cast<const uint4*>(sA + a_chunk(m, ch, 0));
       const uint32_t ow[4] = {o4.x, o4.y, o4.z, o4.w};
       uint32_t gw[4];
-      const float4 b0 = *reinterpret_cast<const float4*>(&bias[ch * 8]);
-      const float4 b1 = *reinterpret_cast<const float4*>(&bias[ch * 8 + 4]);
-      const float bb[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const float g0 = fmaxf(__uint_as_float(v[cc * 8 + 2 * j]) + bb[2 * j], 0.f);
-        const float g1 = fmaxf(__uint_as_float(v[cc * 8 + 2 * j + 1]) + bb[2 * j + 1], 0.f);
+      for (int j = 0; j < 4; ++j) {  // (the accumulator holds the bias already)
+        const float g0 = fmaxf(__uint_as_float(v[cc * 8 + 2 * j]), 0.f);
+        const float g1 = fmaxf(__uint_as_float(v[cc * 8 + 2 * j + 1]), 0.f);
         hw[cc * 4 + j] = pack_bf2(bf_lo(ow[j]) + g0, bf_hi(ow[j]) + g1);
         gw[j] = pack_bf2(g0, g1);
       }

@@ -223,7 +223,7 @@ def _mesh_system(pkg, m, D):
 
 def _plan_fallback_tiles(m):
     """Tiles of 128 nodes the layers' gather plan cannot take (more than 8 runs of consecutive
-    rows, more than 416 rows, a span over 4096 nodes or a node of more than 7 neighbours), counted
+    rows, more than 400 rows, a span over 4096 nodes or a node of more than 7 neighbours), counted
     on the host from the mesh alone."""
     tri = np.asarray(m.triangles).reshape(-1, 3).astype(np.int64)
     N = m.num_nodes
@@ -235,7 +235,7 @@ def _plan_fallback_tiles(m):
         u = np.unique(dst[ptr[t]:ptr[min(N, t + 128)]])
         deg = np.diff(ptr[t:min(N, t + 128) + 1])
         runs = 1 + int(np.sum(np.diff(u) > 1))
-        out += int(u[-1] - u[0] + 1 > 4096 or u.size > 416 or runs > 8 or deg.max() - 1 > 7)
+        out += int(u[-1] - u[0] + 1 > 4096 or u.size > 400 or runs > 8 or deg.max() - 1 > 7)
     return out, (N + 127) // 128
 
 
@@ -255,8 +255,9 @@ def test_gather_plan_matches_row_gather(pkg, oracle, gpu_lib, golden, monkeypatc
     """The layers read each tile's rows either through its gather plan (bulk copies of runs of
     consecutive rows into shared memory) or row by row; both sum the same neighbours in the same
     order, so z and the training loss and gradients are bit-identical. Meshes: an O-grid plate
-    (every tile planned), the Kirsch L1 mesh (no tile planned) and a plate renumbered at random
-    past its 1000th node (both kinds in one launch)."""
+    (every tile planned: the plan kernel), the Kirsch L1 mesh (no tile planned: the row kernel
+    either way) and a plate renumbered at random past its 1000th node (27 % of the tiles planned:
+    the plan kernel with row-by-row fallback tiles in the same launch)."""
     import torch
     D = pkg.constitutive_matrix(1.0, 0.3)
     meshes = {"plate": pkg.plate.quarter_plate(60, 150), "kirsch_L1": golden("kirsch_L1").mesh(pkg),
