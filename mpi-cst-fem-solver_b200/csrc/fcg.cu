@@ -24,16 +24,43 @@ namespace {
 
 constexpr int kGrid = kSMs * 4;  // fixed grid: a fixed reduction order
 
+// NV block sums at once: each warp sums its lanes' values, then warp q adds value q over the
+// warps (q = w, w + kWarps, ...); two block barriers for any NV. Every thread gets the totals.
+template <int NV>
+__device__ __forceinline__ void block_sums(double (&v)[NV], double* sm /* NV * (kWarps + 1) */) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < NV; ++q) v[q] = warp_sum(v[q]);
+  __syncthreads();  // sm may still be read from an earlier call
+  if (lane == 0)
+#pragma unroll
+    for (int q = 0; q < NV; ++q) sm[q * kWarps + w] = v[q];
+  __syncthreads();
+  for (int q = w; q < NV; q += kWarps) {
+    double t = lane < kWarps ? sm[q * kWarps + lane] : 0.0;
+    t = warp_sum(t);
+    if (lane == 0) sm[NV * kWarps + q] = t;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < NV; ++q) v[q] = sm[NV * kWarps + q];
+}
+
+// Grid reduction in a fixed order: per-block sums into `partials`, the last block to arrive adds
+// them (each thread a strided share of every value, all loads in flight together) and returns
+// true with the totals.
 template <int NV>
 __device__ __forceinline__ bool fcg_reduce(const double (&v)[NV], double* partials, unsigned int* ticket,
                                            double (&tot)[NV]) {
-  __shared__ double sm[kWarps];
+  __shared__ double sm[NV * (kWarps + 1)];
   __shared__ bool am_last;
+  double b[NV];
 #pragma unroll
-  for (int q = 0; q < NV; ++q) {
-    const double s = block_sum<kThreads>(v[q], sm);
-    if (threadIdx.x == 0) partials[q * gridDim.x + blockIdx.x] = s;
-  }
+  for (int q = 0; q < NV; ++q) b[q] = v[q];
+  block_sums<NV>(b, sm);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int q = 0; q < NV; ++q) partials[q * gridDim.x + blockIdx.x] = b[q];
   __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) am_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
@@ -41,11 +68,11 @@ __device__ __forceinline__ bool fcg_reduce(const double (&v)[NV], double* partia
   if (!am_last) return false;
   __threadfence();
 #pragma unroll
-  for (int q = 0; q < NV; ++q) {
-    double s = 0.0;
-    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) s += __ldcg(&partials[q * gridDim.x + i]);
-    tot[q] = block_sum<kThreads>(s, sm);
-  }
+  for (int q = 0; q < NV; ++q) tot[q] = 0.0;
+  for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x)
+#pragma unroll
+    for (int q = 0; q < NV; ++q) tot[q] += __ldcg(&partials[q * gridDim.x + i]);
+  block_sums<NV>(tot, sm);
   if (threadIdx.x == 0) *ticket = 0u;
   return true;
 }
