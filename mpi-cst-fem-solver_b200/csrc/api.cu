@@ -93,7 +93,7 @@ void cstg_destroy(cstg_ctx* ctx) {
                    &ctx->lp_sf,   &ctx->lp_h0,  &ctx->lp_h1,    &ctx->lp_sc,    &ctx->lp_z,
                    &ctx->tr_con,  &ctx->tr_cnt, &ctx->tr_ptr,   &ctx->tr_cur,   &ctx->tr_rec,
                    &ctx->lm_winvd, &ctx->fcg_ring, &ctx->lp_mat, &ctx->lp_plan_hdr, &ctx->lp_plan_runs,
-                   &ctx->lp_plan_local};
+                   &ctx->lp_plan_local, &ctx->tr_edges, &ctx->tr_f};
   for (DevBuf* b : all) free_buf(*b);
   for (int j = 0; j < kFcgMaxHist; ++j) {
     free_buf(ctx->fcg_ph[j]);
@@ -166,8 +166,10 @@ int cstg_set_mesh(cstg_ctx* ctx, int n_nodes, const double* xy, int n_tri, const
     return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "set_mesh: null array");
   const int rc = set_mesh_common(ctx, n_nodes, n_tri);
   if (rc) return rc;
-  ctx->h_xy.assign(xy, xy + 2 * (size_t)n_nodes);
-  ctx->h_tri.assign(tri, tri + 3 * (size_t)n_tri);
+  // the host copy of the mesh (the host traction path's input) is read back from the device when
+  // first needed, not copied here
+  ctx->h_xy.clear();
+  ctx->h_tri.clear();
   ctx->host_mesh = true;
   if (n_nodes)
     CK(cudaMemcpyAsync(ctx->xy.p, xy, sizeof(double) * 2 * (size_t)n_nodes, cudaMemcpyHostToDevice,
@@ -964,11 +966,44 @@ int cstg_add_traction(cstg_ctx* ctx, int n_edges, const int32_t* edges, double t
                       double ty, double* f) {
   if (!ctx) return CSTG_ERR_INVALID_ARGUMENT;
   ctx->err.clear();
-  if (!ctx->host_mesh)
-    return fail(ctx, CSTG_ERR_STATE, "add_traction: needs the host mesh of cstg_set_mesh");
   if (n_edges < 0 || (n_edges > 0 && (!edges || !f)))
     return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "add_traction: bad arguments");
+  if (ctx->kind == 1 && n_edges > 0) {
+    BEGIN(ctx);
+    // with the pattern built, the device path (the pattern's node incidence, the same bits): f
+    // goes up, the loads are added on the GPU, f comes back. An edge error is reported by the
+    // host path below (the reference's message, with the triangle count).
+    const size_t nf = (size_t)ctx->n_rows;
+    ENSURE(ctx->tr_edges, sizeof(int32_t) * 2 * (size_t)n_edges);
+    ENSURE(ctx->tr_f, sizeof(double) * std::max<size_t>(nf, 1));
+    CK(cudaMemcpyAsync(ctx->tr_edges.p, edges, sizeof(int32_t) * 2 * (size_t)n_edges, cudaMemcpyHostToDevice,
+                       ctx->stream));
+    CK(cudaMemcpyAsync(ctx->tr_f.p, f, sizeof(double) * nf, cudaMemcpyHostToDevice, ctx->stream));
+    const int rc = cstg_add_traction_device(ctx, n_edges, buf_ptr<int32_t>(ctx->tr_edges), thickness,
+                                            CSTG_TRACTION_CONSTANT, tx, ty, buf_ptr<double>(ctx->tr_f));
+    if (rc == CSTG_OK) {
+      CK(cudaMemcpyAsync(f, ctx->tr_f.p, sizeof(double) * nf, cudaMemcpyDeviceToHost, ctx->stream));
+      CK(cudaStreamSynchronize(ctx->stream));
+      return CSTG_OK;
+    }
+    if (rc != CSTG_ERR_MESH || !ctx->host_mesh) return rc;
+    ctx->err.clear();
+  }
+  if (!ctx->host_mesh)
+    return fail(ctx, CSTG_ERR_STATE, "add_traction: needs the host mesh of cstg_set_mesh");
   const int N = ctx->n_nodes, E = ctx->n_tri;
+  if (ctx->h_xy.size() != 2 * (size_t)N || ctx->h_tri.size() != 3 * (size_t)E) {
+    BEGIN(ctx);
+    ctx->h_xy.resize(2 * (size_t)N);
+    ctx->h_tri.resize(3 * (size_t)E);
+    if (N)
+      CK(cudaMemcpyAsync(ctx->h_xy.data(), ctx->xy.p, sizeof(double) * 2 * (size_t)N, cudaMemcpyDeviceToHost,
+                         ctx->stream));
+    if (E)
+      CK(cudaMemcpyAsync(ctx->h_tri.data(), ctx->tri.p, sizeof(int32_t) * 3 * (size_t)E, cudaMemcpyDeviceToHost,
+                         ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+  }
   const int32_t* tri = ctx->h_tri.data();
   const double* xy = ctx->h_xy.data();
   if (ctx->h_ne_ptr.empty()) {  // host node -> triangle incidence, built once per mesh
@@ -988,6 +1023,8 @@ int cstg_add_traction(cstg_ctx* ctx, int n_edges, const int32_t* edges, double t
   }
   const double g = 1.0 / std::sqrt(3.0);
   const double xi[2] = {-g, g};
+  // every edge is checked before any load is added: on an error f is left as it was
+  std::vector<int> opp((size_t)n_edges);
   for (int q = 0; q < n_edges; ++q) {
     const int a = edges[2 * q], b = edges[2 * q + 1];
     if (a < 0 || a >= N || b < 0 || b >= N)
@@ -1008,6 +1045,10 @@ int cstg_add_traction(cstg_ctx* ctx, int n_edges, const int32_t* edges, double t
     if (count != 1)
       return fail(ctx, CSTG_ERR_MESH, "traction edge (%d, %d) is adjacent to %d triangles (expected 1)",
                   a, b, count);
+    opp[(size_t)q] = c;
+  }
+  for (int q = 0; q < n_edges; ++q) {
+    const int a = edges[2 * q], b = edges[2 * q + 1], c = opp[(size_t)q];
     const double xa = xy[2 * a], ya = xy[2 * a + 1];
     const double xb = xy[2 * b], yb = xy[2 * b + 1];
     const double len = std::hypot(xb - xa, yb - ya);

@@ -83,6 +83,7 @@ struct cstg_ctx {
 
   // GPU traction: per-edge contributions and per-node records
   DevBuf tr_con, tr_cnt, tr_ptr, tr_cur, tr_rec;
+  DevBuf tr_edges, tr_f;  // host-pointer traction calls routed through the device path
 
   // multi-material assembly
   DevBuf mat, mat_tab;

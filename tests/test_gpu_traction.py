@@ -96,3 +96,37 @@ def test_device_traction_rejects_interior_edge(pkg, gpu_lib):
         pkg.add_traction(K, edges, 1.0, 1.0, 0.0, f)
     assert float(f.abs().sum()) == 0.0
     K.ctx.close()
+
+
+def test_host_pointer_traction_paths(pkg, gpu_lib):
+    """cstg_add_traction with a host f: after cstg_build_pattern it runs on the GPU (f up, the
+    pattern's node incidence, f down); before it, on the host from the mesh read back from the
+    device. Both give the same bits, accumulating into f; an interior edge is reported with the
+    reference's message (the triangle count) and f is left as it was."""
+    import ctypes as C
+    m = pkg.plate.quarter_plate(23, 52, a=1.1)
+    xy = np.ascontiguousarray(m.xy, dtype=np.float64)
+    tri = np.ascontiguousarray(m.triangles, dtype=np.int32)
+    groups = [("right", 1.0, 0.5), ("top", -0.25, 2.0), ("hole", 0.3, 0.1)]
+    out = {}
+    for name, build in (("host", False), ("device", True)):
+        ctx = pkg.Context(0)
+        ctx.check(ctx.L.cstg_set_mesh(ctx.h, m.num_nodes, xy.ctypes.data, m.num_triangles, tri.ctypes.data))
+        if build:
+            nnz = C.c_int64(0)
+            ctx.check(ctx.L.cstg_build_pattern(ctx.h, C.byref(nnz)))
+        f = np.full(m.num_dofs, 0.125)
+        for grp, tx, ty in groups:
+            e = np.ascontiguousarray(m.boundary_edges[grp], dtype=np.int32).reshape(-1)
+            ctx.check(ctx.L.cstg_add_traction(ctx.h, e.size // 2, e.ctypes.data, 0.7, tx, ty, f.ctypes.data))
+        out[name] = f
+        t3 = tri.reshape(-1, 3)
+        bad = np.ascontiguousarray(np.concatenate([m.boundary_edges["right"].reshape(-1, 2),
+                                                   [[t3[0][0], t3[0][2]]]]), dtype=np.int32).reshape(-1)
+        g = f.copy()
+        rc = ctx.L.cstg_add_traction(ctx.h, bad.size // 2, bad.ctypes.data, 1.0, 1.0, 0.0, g.ctypes.data)
+        assert rc == pkg.native.ERR_MESH
+        assert "is adjacent to 2 triangles" in ctx.L.cstg_last_error(ctx.h).decode()
+        assert np.array_equal(g, f)
+        ctx.close()
+    assert np.array_equal(out["host"], out["device"])
