@@ -70,7 +70,7 @@ def log(*a):
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="plate2m", choices=sorted(WORKLOADS))
@@ -163,7 +163,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={','.join(self.FIELDS)}", "--format=csv,noheader,nounits",
-                 "-lms", "200", "-i", str(self.device)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                 "-lms", "50", "-i", str(self.device)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
                 text=True)
         except OSError:
             self.proc = None
@@ -714,8 +714,8 @@ def run_e2e(a, pkg, dist, dev, mesh, D, dofs, vals, opts, weights, mat, learned_
     import torch
 
     def pinned(arr):
-        t = torch.empty(arr.shape, dtype={np.float64: torch.float64, np.int32: torch.int32}[arr.dtype.type],
-                        pin_memory=True)
+        t = torch.empty(arr.shape, dtype={np.float64: torch.float64, np.int32: torch.int32,
+                                          np.float32: torch.float32}[arr.dtype.type], pin_memory=True)
         v = t.numpy()
         v[...] = arr
         return v
@@ -724,6 +724,7 @@ def run_e2e(a, pkg, dist, dev, mesh, D, dofs, vals, opts, weights, mat, learned_
     h_dofs, h_vals = pinned(dofs), pinned(vals)
     h_b = pinned(np.zeros(mesh.num_dofs))
     h_x = pinned(np.zeros(mesh.num_dofs))
+    h_mat = pinned(np.ascontiguousarray(mat))
     ectx = pkg.Context(dev)
     last = {}
 
@@ -736,7 +737,7 @@ def run_e2e(a, pkg, dist, dev, mesh, D, dofs, vals, opts, weights, mat, learned_
         s2 = pkg.CgJacobiSolver(opts)
         s2.setup(K2)
         if learned_any:
-            pkg.learned.setup(K2, weights, mat)
+            pkg.learned.setup(K2, weights, h_mat)
         last["st"] = s2.solve(h_b, h_x)
 
     def wall_start():
