@@ -261,9 +261,12 @@ def test_gather_plan_matches_row_gather(pkg, oracle, gpu_lib, golden, monkeypatc
     import torch
     D = pkg.constitutive_matrix(1.0, 0.3)
     meshes = {"plate": pkg.plate.quarter_plate(60, 150), "kirsch_L1": golden("kirsch_L1").mesh(pkg),
-              "mixed": _renumbered_plate(pkg, 40, 80, 1000, 5)}
+              "mixed": _renumbered_plate(pkg, 40, 80, 1000, 5),
+              "tiny": pkg.plate.quarter_plate(2, 4),           # 15 nodes: one ragged tile
+              "ragged": pkg.plate.quarter_plate(8, 14)}        # 135 nodes: a full tile and 7 nodes
     kinds = {k: _plan_fallback_tiles(m) for k, m in meshes.items()}
     assert kinds["plate"][0] == 0 and kinds["kirsch_L1"][0] == kinds["kirsch_L1"][1]
+    assert kinds["tiny"] == (0, 1) and kinds["ragged"] == (0, 2), kinds
     assert 0 < kinds["mixed"][0] < kinds["mixed"][1], kinds
     p, _ = _bf16_params(oracle, pkg, seed=6)
     for name, m in meshes.items():
