@@ -1,5 +1,5 @@
-"""Smoothed-aggregation multigrid preconditioner on the GPU, judged like the other methods by the
-reference's FP64 Jacobi-PCG solution.
+"""Smoothed-aggregation multigrid preconditioner on the GPU, checked like the other methods against
+the reference's FP64 Jacobi-PCG solution.
 
 Bars: solutions within relative 1e-8 of the reference's (rtol 1e-10, FP64 true residual);
 the V-cycle is a symmetric positive operator (<Mu, v> = <u, Mv> to 1e-8 relative: the finest

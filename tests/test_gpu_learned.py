@@ -1,6 +1,6 @@
 """Learned preconditioner on the GPU: the tensor-core forward pass and the training gradients
 against the FP64 oracle (oracle/mpnn_oracle.c), training, and the flexible-CG solve with its
-Jacobi fallback, judged by the reference's FP64 Jacobi-PCG solution.
+Jacobi fallback, checked against the reference's FP64 Jacobi-PCG solution.
 
 Bars: forward z within relative 1e-2 of the oracle (BF16 activations on both sides; the rest
 is FP32-vs-FP64 accumulation); gradients within relative 5e-2; solves converged on the FP64 true

@@ -1,6 +1,6 @@
 """The learned preconditioner's CPU oracle (oracle/mpnn_oracle.c) checked against finite
 differences: the FP64 backward pass must match central differences of the loss, so that the
-oracle can judge the GPU gradients. CPU only."""
+oracle can check the GPU gradients. CPU only."""
 import numpy as np
 import pytest
 
