@@ -316,6 +316,23 @@ __device__ __forceinline__ double ke_entry(const CstB& o, int i, int j) {
   return __dmul_rn(o.scale, s);
 }
 
+// Rows 2A, 2A+1 of an element's Ke added into a node's two CSR rows (ra, rb) at the slots of
+// the element's three corners. A is a template parameter so that every index into B and DB is
+// known at compile time.
+template <int A>
+__device__ __forceinline__ void add_corner_rows(const CstB& o, const int* __restrict__ slot3, int b0, double* ra,
+                                                double* rb) {
+#pragma unroll
+  for (int b = 0; b < 3; ++b) {
+    const int k = slot3[b] - b0;
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      ra[2 * k + c] = __dadd_rn(ra[2 * k + c], ke_entry(o, 2 * A, 2 * b + c));
+      rb[2 * k + c] = __dadd_rn(rb[2 * k + c], ke_entry(o, 2 * A + 1, 2 * b + c));
+    }
+  }
+}
+
 // One thread per node: the node's two rows are zeroed, then every incident element (in
 // ascending element order) adds its 2 x 6 slice of Ke. Each CSR entry therefore receives
 // its contributions in the reference's order (assembly.cpp:56-72), starting from 0.0.
@@ -350,15 +367,13 @@ __global__ void __launch_bounds__(128) k_assemble(
     } else {
       cst_element(exy, Dm.v, thickness, o);
     }
-#pragma unroll
-    for (int b = 0; b < 3; ++b) {
-      const int k = slot[3 * q + b] - b0;
-#pragma unroll
-      for (int c = 0; c < 2; ++c) {
-        ra[2 * k + c] = __dadd_rn(ra[2 * k + c], ke_entry(o, 2 * a, 2 * b + c));
-        rb[2 * k + c] = __dadd_rn(rb[2 * k + c], ke_entry(o, 2 * a + 1, 2 * b + c));
-      }
-    }
+    // the corner's rows with compile-time indices (B and DB stay in registers)
+    if (a == 0)
+      add_corner_rows<0>(o, slot + 3 * q, b0, ra, rb);
+    else if (a == 1)
+      add_corner_rows<1>(o, slot + 3 * q, b0, ra, rb);
+    else
+      add_corner_rows<2>(o, slot + 3 * q, b0, ra, rb);
   }
 }
 
