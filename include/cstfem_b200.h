@@ -264,8 +264,8 @@ int cstg_element_stresses(cstg_ctx* ctx, const double* u, double E, double nu, i
 /* ---- add_traction (bc.hpp:74-75, bc.cpp:190-253) -----------------------------------------
  * Consistent nodal forces of a constant traction (tx, ty) on line edges (n_edges x 2 node
  * pairs), 2-point Gauss, times thickness, added to the host array f (2 per node). After
- * cstg_build_pattern the loads are computed on the GPU (f copied up and back, the pattern's node
- * incidence: cstg_add_traction_device); before it, on the host from the mesh of cstg_set_mesh.
+ * cstg_build_pattern the loads are computed on the GPU (the loaded nodes' entries of f copied up
+ * and back, the pattern's node incidence: cstg_add_traction_device); before it, on the host from the mesh of cstg_set_mesh.
  * Bit-identical to the reference either way. Every edge is checked first: an edge not adjacent
  * to exactly one triangle returns CSTG_ERR_MESH with the reference's message (the triangle
  * count) and f is left as it was. */

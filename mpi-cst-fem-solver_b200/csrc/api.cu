@@ -970,20 +970,41 @@ int cstg_add_traction(cstg_ctx* ctx, int n_edges, const int32_t* edges, double t
     return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "add_traction: bad arguments");
   if (ctx->kind == 1 && n_edges > 0) {
     BEGIN(ctx);
-    // with the pattern built, the device path (the pattern's node incidence, the same bits): f
-    // goes up, the loads are added on the GPU, f comes back. An edge error is reported by the
-    // host path below (the reference's message, with the triangle count).
-    const size_t nf = (size_t)ctx->n_rows;
-    ENSURE(ctx->tr_edges, sizeof(int32_t) * 2 * (size_t)n_edges);
-    ENSURE(ctx->tr_f, sizeof(double) * std::max<size_t>(nf, 1));
-    CK(cudaMemcpyAsync(ctx->tr_edges.p, edges, sizeof(int32_t) * 2 * (size_t)n_edges, cudaMemcpyHostToDevice,
-                       ctx->stream));
-    CK(cudaMemcpyAsync(ctx->tr_f.p, f, sizeof(double) * nf, cudaMemcpyHostToDevice, ctx->stream));
-    const int rc = cstg_add_traction_device(ctx, n_edges, buf_ptr<int32_t>(ctx->tr_edges), thickness,
-                                            CSTG_TRACTION_CONSTANT, tx, ty, buf_ptr<double>(ctx->tr_f));
+    // with the pattern built, the device path (the pattern's node incidence, the same bits): the
+    // loaded nodes' entries of f go up, the loads are added on the GPU, the entries come back.
+    // An edge error is reported by the host path below (the reference's message).
+    const int N = ctx->n_nodes;
+    std::vector<int32_t> nodes(edges, edges + 2 * (size_t)n_edges);
+    for (int q = 0; q < 2 * n_edges; ++q)
+      if (nodes[q] < 0 || nodes[q] >= N)
+        return fail(ctx, CSTG_ERR_INVALID_ARGUMENT, "add_traction: edge %d has a node out of range", q / 2);
+    std::sort(nodes.begin(), nodes.end());
+    nodes.erase(std::unique(nodes.begin(), nodes.end()), nodes.end());
+    const int m = (int)nodes.size();
+    std::vector<double> fc(2 * (size_t)m);
+    for (int i = 0; i < m; ++i) {
+      fc[2 * (size_t)i] = f[2 * (size_t)nodes[i]];
+      fc[2 * (size_t)i + 1] = f[2 * (size_t)nodes[i] + 1];
+    }
+    ENSURE(ctx->tr_edges, sizeof(int32_t) * (2 * (size_t)n_edges + (size_t)m));
+    ENSURE(ctx->tr_f, sizeof(double) * (std::max<size_t>((size_t)ctx->n_rows, 1) + 2 * (size_t)m));
+    int32_t* d_edges = buf_ptr<int32_t>(ctx->tr_edges);
+    int32_t* d_nodes = d_edges + 2 * (size_t)n_edges;
+    double* d_f = buf_ptr<double>(ctx->tr_f);
+    double* d_fc = d_f + (size_t)ctx->n_rows;
+    CK(cudaMemcpyAsync(d_edges, edges, sizeof(int32_t) * 2 * (size_t)n_edges, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(d_nodes, nodes.data(), sizeof(int32_t) * (size_t)m, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(d_fc, fc.data(), sizeof(double) * 2 * (size_t)m, cudaMemcpyHostToDevice, ctx->stream));
+    CK(launch_traction_compact(m, d_nodes, d_fc, d_f, 0, ctx->stream));
+    const int rc = cstg_add_traction_device(ctx, n_edges, d_edges, thickness, CSTG_TRACTION_CONSTANT, tx, ty, d_f);
     if (rc == CSTG_OK) {
-      CK(cudaMemcpyAsync(f, ctx->tr_f.p, sizeof(double) * nf, cudaMemcpyDeviceToHost, ctx->stream));
+      CK(launch_traction_compact(m, d_nodes, d_fc, d_f, 1, ctx->stream));
+      CK(cudaMemcpyAsync(fc.data(), d_fc, sizeof(double) * 2 * (size_t)m, cudaMemcpyDeviceToHost, ctx->stream));
       CK(cudaStreamSynchronize(ctx->stream));
+      for (int i = 0; i < m; ++i) {
+        f[2 * (size_t)nodes[i]] = fc[2 * (size_t)i];
+        f[2 * (size_t)nodes[i] + 1] = fc[2 * (size_t)i + 1];
+      }
       return CSTG_OK;
     }
     if (rc != CSTG_ERR_MESH || !ctx->host_mesh) return rc;

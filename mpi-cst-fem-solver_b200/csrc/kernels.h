@@ -297,6 +297,7 @@ cudaError_t launch_spmv_mixed_pcg(const MixedMatrix& A32, const BlockMatrix& A64
 cudaError_t launch_traction_edges(int n_edges, const int* edges, const MeshDev& m, const int* ne_ptr, const int* ne,
                                   double thickness, int kind, double p0, double p1, double* con, int* cnt, int* err,
                                   cudaStream_t s);
+cudaError_t launch_traction_compact(int m, const int* nodes, double* fc, double* f, int dir, cudaStream_t s);
 cudaError_t launch_traction_apply(int n_edges, const int* edges, int n_nodes, const double* con, const int* cnt,
                                   int* ptr, int* cur, int* rec, int* scan_tmp, double* f, cudaStream_t s);
 

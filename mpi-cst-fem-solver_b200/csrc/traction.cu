@@ -156,7 +156,30 @@ __global__ void k_trac_gather(int n_nodes, const int* __restrict__ ptr, int* __r
   f[2 * n + 1] = fy;
 }
 
+// Host-array tractions move only the loaded nodes' entries: dir = 0 scatters the compact values
+// (2 per node, in `nodes` order) into f, dir = 1 gathers them back.
+__global__ void k_trac_compact(int m, const int* __restrict__ nodes, double* __restrict__ fc, double* __restrict__ f,
+                               int dir) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const int n = nodes[i];
+  if (dir == 0) {
+    f[2 * (size_t)n] = fc[2 * i];
+    f[2 * (size_t)n + 1] = fc[2 * i + 1];
+  } else {
+    fc[2 * i] = f[2 * (size_t)n];
+    fc[2 * i + 1] = f[2 * (size_t)n + 1];
+  }
+}
+
 }  // namespace
+
+cudaError_t launch_traction_compact(int m, const int* nodes, double* fc, double* f, int dir, cudaStream_t s) {
+  if (m <= 0) return cudaSuccess;
+  k_trac_compact<<<(m + 255) / 256, 256, 0, s>>>(m, nodes, fc, f, dir);
+  count_launches(1);
+  return cudaGetLastError();
+}
 
 // Phase 1: per-edge contributions and per-node record counts (the caller checks the error word
 // before phase 2; a failed edge leaves f untouched).
