@@ -24,6 +24,7 @@
 // gradients as per-block partial sums added in block order (deterministic). The loss of a
 // (residual r, error e = A^-1 r) pair is 1 - (z'r)^2 / ((z'Az)(e'r)), the squared sine of the
 // energy-norm angle between z and e.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -292,7 +293,7 @@ __global__ void __launch_bounds__(256) k_mp_tile_plan(int N, const int* __restri
     };
     uint16_t slot[8];
 #pragma unroll
-    for (int j = 0; j < 8; ++j) slot[j] = 0xFFFFu;
+    for (int j = 0; j < 8; ++j) slot[j] = (uint16_t)kPlanNone;
     slot[0] = (uint16_t)rank(n);
     int k = 1;
     for (int e = node_ptr[n]; e < node_ptr[n + 1]; ++e) {
@@ -330,28 +331,16 @@ __global__ void k_mp_smoother_weights(int n, const double* __restrict__ invd, co
 //            y = W_out H3 + b_out, summed over the 64 features in order (the first half by the
 //            warps of columns 0..31, handed through shared memory to those of columns 32..63), and
 //            z = zbase + invd (r + s y).
-// The rows reach the A tile one of two ways:
-//  rows (PLAN = false): four CTAs of 8 warps per SM; each lane loads its nodes' chunks from global
-//            memory, a warp's node pointers and neighbour lists in two loads (the next tile's lists
-//            prefetched with cp.async during the MMA and the epilogue).
-//  plan (PLAN = true, patterns with a gather plan): two CTAs of 9 warps per SM. A tile's union
-//            of rows is a few runs of consecutive nodes (three on the O-grid plates, about 3 rows
-//            per node); the ninth warp, the producer, brings the runs and the tile's per-node
-//            slots into shared memory with bulk copies (cp.async.bulk, no multicast) as soon as
-//            the tile warps have read the previous tile's (full / empty mbarriers), so the copies
-//            run during the MMA and the epilogue. A tile the plan cannot take is gathered row by
-//            row.
+// The rows reach the A tile from global memory: four CTAs of 8 warps per SM; each lane loads its
+// nodes' chunks, a warp's node pointers and neighbour lists in two loads (the next tile's lists
+// prefetched with cp.async during the MMA and the epilogue). Patterns with a gather plan run the
+// warp-specialised kernel below (k_mp_layer_ws) instead; both give the same bits.
 constexpr int kLT = 256;                 // the tile warps' threads
-constexpr int kLTPlan = kLT + 32;        // + the producer warp
 constexpr int kNbrCache = 128;           // neighbour-list entries a warp keeps in shared memory
 constexpr int kLayerCtasPerSm = 3;       // rows: resident CTAs per SM (registers capped to fit them)
-constexpr int kPlanCtasPerSm = 2;        // plan: resident CTAs per SM
-constexpr int kUStages = 1;              // plan: union buffers per CTA
-constexpr int kUSmem = kPlanMaxUnion * 128 + kTile * 16;  // one buffer: the rows, then the node slots
 // the bias slice: A's constant K-slice of ones (128 x 16 BF16) and B's bias rows (64 x 16 BF16)
 constexpr int kBiasSmem = 4096 + 2048;
 constexpr int kTcSmem = kASmem + kBSmem + kBiasSmem + 1024;  // dynamic shared memory (1024-byte aligned base)
-constexpr int kTcSmemPlan = kASmem + kBSmem + kUStages * kUSmem + kBiasSmem + 1024;
 
 struct MpLayerArgs {
   int N;
@@ -603,118 +592,37 @@ __device__ __forceinline__ void add_chunk_bf(float (&acc)[8], const uint4 v) {
         : "+f"(acc[2 * q]), "+f"(acc[2 * q + 1])
         : "r"(w[q]));
 }
+// Eight BF16 -0.0: the chunk a missing neighbour contributes. x + (-0) = x exactly for every x
+// (both zeros included), so a sum padded with it has the bits of the sum without it, and the
+// neighbour loop needs no branch around its adds (a branch around inline assembly cannot be
+// predicated: it diverges).
+constexpr uint32_t kNegZero2 = 0x80008000u;
+// 1/deg as the IEEE quotient 1.f / deg (constants folded by the compiler), no division at run time.
+__device__ __forceinline__ float inv_deg(int deg) {
+  if (deg > 7) return 1.f / (float)deg;
+  float r = 0.f;
+  r = deg == 1 ? 1.f : r;
+  r = deg == 2 ? 1.f / 2.f : r;
+  r = deg == 3 ? 1.f / 3.f : r;
+  r = deg == 4 ? 1.f / 4.f : r;
+  r = deg == 5 ? 1.f / 5.f : r;
+  r = deg == 6 ? 1.f / 6.f : r;
+  r = deg == 7 ? 1.f / 7.f : r;
+  return r;
+}
 // The chunk's mean as 8 BF16: each sum times inv, rounded to nearest.
 __device__ __forceinline__ uint4 mean_chunk(const float (&acc)[8], float inv) {
   return make_uint4(pack_bf2(acc[0] * inv, acc[1] * inv), pack_bf2(acc[2] * inv, acc[3] * inv),
                     pack_bf2(acc[4] * inv, acc[5] * inv), pack_bf2(acc[6] * inv, acc[7] * inv));
 }
 
-// Barrier of the tile warps: the whole CTA (rows), or named barrier 1 over threads 0..255 (plan,
-// where the producer warp keeps its own pace).
-template <bool PLAN>
-__device__ __forceinline__ void tile_sync() {
-  if constexpr (PLAN)
-    asm volatile("bar.sync 1, 256;\n" ::: "memory");
-  else
-    __syncthreads();
-}
-template <bool PLAN>
-__device__ __forceinline__ int tile_sync_and(int pred) {
-  if constexpr (PLAN) {
-    int out;
-    asm volatile(
-        "{\n\t.reg .pred p, q;\n\t"
-        "setp.ne.b32 p, %1, 0;\n\t"
-        "bar.red.and.pred q, 1, 256, p;\n\t"
-        "selp.b32 %0, 1, 0, q;\n\t}\n"
-        : "=r"(out)
-        : "r"(pred)
-        : "memory");
-    return out;
-  } else {
-    return __syncthreads_and(pred);
-  }
-}
-
-// A tile the plan takes: its union fits one buffer in at most kPlanMaxRuns runs.
+// A tile the plan takes: its union fits one stage in at most kPlanMaxRuns runs.
 __device__ __forceinline__ bool plan_takes(const int4 h) {
   return h.z == 0 && h.x >= 1 && h.x <= kPlanMaxRuns && h.y >= 1 && h.y <= kPlanMaxUnion;
 }
 
-// As mbar_wait, also giving up when the tile warps have raised `abort_flag`.
-__device__ __forceinline__ bool mbar_wait_or_abort(uint32_t addr, uint32_t parity, long long limit,
-                                                   const volatile int* abort_flag) {
-  for (long long i = 0; i < limit; ++i) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}\n"
-        : "=r"(ok)
-        : "r"(addr), "r"(parity)
-        : "memory");
-    if (ok) return true;
-    if (*abort_flag) return false;
-  }
-  return false;
-}
-
-// The producer warp of the plan kernel: for each of the CTA's planned tiles, in order, waits until
-// the tile warps are done with the buffer it last filled (the empty barrier), then lane 0 sets the
-// full barrier's byte count and every lane of a run issues its bulk copy: run j lands at the sum
-// of the earlier runs' lengths (rows of 128 bytes), the tile's node slots after the rows.
-// Before it leaves, the copies it issued have landed (bounded waits), so none writes into the
-// CTA's shared memory after the CTA is gone.
-__device__ __forceinline__ void plan_producer(const MpLayerArgs& a, uint8_t* sU, uint32_t full0, uint32_t empty0,
-                                              const volatile int* abort_flag) {
-  const int lane = threadIdx.x & 31;
-  int k = 0;  // planned tiles issued
-  for (int tile = blockIdx.x; tile * kTile < a.N; tile += gridDim.x) {
-    const int4 ph = __ldg(&a.plan.hdr[tile]);
-    if (!plan_takes(ph)) continue;
-    const int st = k % kUStages;
-    const uint32_t fb = full0 + 8u * st, eb = empty0 + 8u * st;
-    if (k >= kUStages) {
-      // a phase that one lane saw complete is complete for all: the warp goes on if any lane saw it
-      const bool freed = mbar_wait_or_abort(eb, (uint32_t)(k / kUStages - 1) & 1u, a.spin_limit, abort_flag);
-      if (!__any_sync(0xffffffffu, freed)) break;  // the tile warps stopped or did not free it in time
-    }
-    const int2 rn = lane < ph.x ? __ldg(&a.plan.runs[(size_t)tile * kPlanMaxRuns + lane]) : make_int2(0, 0);
-    int off = rn.y;  // inclusive prefix of the run lengths over the lanes
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-      const int v = __shfl_up_sync(0xffffffffu, off, d);
-      if (lane >= d) off += v;
-    }
-    off -= rn.y;
-    const int cnt = min(kTile, a.N - tile * kTile);
-    uint8_t* buf = sU + (size_t)st * kUSmem;
-    if (lane == 0) {
-      // the tile warps' generic reads of this buffer are ordered before the copies' writes
-      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(fb),
-                   "r"((uint32_t)ph.y * 128u + (uint32_t)cnt * 16u)
-                   : "memory");
-      asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
-                       smem_u32(buf + kPlanMaxUnion * 128)),
-                   "l"(a.plan.local + (size_t)tile * kTile), "r"((uint32_t)cnt * 16u), "r"(fb)
-                   : "memory");
-    }
-    __syncwarp();
-    if (lane < ph.x)
-      asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
-                       smem_u32(buf + (size_t)off * 128)),
-                   "l"(a.Hin + (size_t)rn.x * F), "r"((uint32_t)rn.y * 128u), "r"(fb)
-                   : "memory");
-    ++k;
-  }
-  for (int j = max(0, k - kUStages); j < k; ++j)
-    mbar_wait(full0 + 8u * (j % kUStages), (uint32_t)(j / kUStages) & 1u, kMbarSpinLimit);
-}
-
-template <bool TRAIN, bool LAST, bool PLAN>
-__global__ void __launch_bounds__(PLAN ? kLTPlan : kLT, PLAN ? kPlanCtasPerSm : kLayerCtasPerSm)
-    k_mp_layer_tc(const MpLayerArgs a) {
+template <bool TRAIN, bool LAST>
+__global__ void __launch_bounds__(kLT, kLayerCtasPerSm) k_mp_layer_tc(const MpLayerArgs a) {
   const int N = a.N;
   if (a.skip && *a.skip) {  // uniform: before any barrier or tensor-memory allocation
     if (LAST)                 // the network is off: the Jacobi step
@@ -723,25 +631,24 @@ __global__ void __launch_bounds__(PLAN ? kLTPlan : kLT, PLAN ? kPlanCtasPerSm : 
     return;
   }
   extern __shared__ uint8_t smem_raw[];
-  __shared__ uint64_t mbar, full_bar[kUStages], empty_bar[kUStages];
+  __shared__ uint64_t mbar;
   __shared__ uint32_t tmem_slot;
-  __shared__ int mma_ok, abort_flag;
+  __shared__ int mma_ok;
   __shared__ float wout[2 * F], bout[2];
   __shared__ float2 ypart[kTile];
   // each warp's neighbour lists for row-by-row tiles (the first kNbrCache entries)
-  __shared__ int s_nbr[PLAN ? 1 : (kLT / 32) * kNbrCache];
+  __shared__ int s_nbr[(kLT / 32) * kNbrCache];
   // 1024-byte aligned base as an offset into the shared array (the compiler keeps the shared
   // address space through pointer arithmetic on it: plain C++ accesses become ld/st.shared)
   uint8_t* base = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
   uint8_t* sA = base;               // chunk k/8 of row m at a_chunk(m, (k/8) % 8, k/64), + (k%8)*2
   uint8_t* sB = base + kASmem;      // element (n, k): (k/8)*1024 + (n/8)*128 + (n%8)*16 + (k%8)*2
   uint8_t* sOut = sA + kASmem / 2;  // staged output tile (the mean half of A, free after the MMA)
-  uint8_t* sU = sB + kBSmem;        // plan: the ring of union buffers
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const __nv_bfloat16* W = a.P.pb + kMpOffL0 + a.layer * kMpLStride;
   // the bias enters the MMA as a ninth K-slice: ones in A (K 0..2) against the FP32 bias split
   // exactly into three BF16 parts in B (b = b_hi + b_mid + b_lo)
-  uint8_t* sOnes = sB + kBSmem + (PLAN ? kUStages * kUSmem : 0);
+  uint8_t* sOnes = sB + kBSmem;
   uint8_t* sBias = sOnes + 4096;
   if (t < kTile) {
     *reinterpret_cast<uint4*>(sOnes + (t >> 3) * 128 + (t & 7) * 16) = make_uint4(0x3F803F80u, 0x00003F80u, 0u, 0u);
@@ -775,25 +682,11 @@ __global__ void __launch_bounds__(PLAN ? kLTPlan : kLT, PLAN ? kPlanCtasPerSm : 
   }
   if (t == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(&mbar)), "r"(1));
-    if (PLAN)
-      for (int j = 0; j < kUStages; ++j) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(&full_bar[j])), "r"(1));
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(&empty_bar[j])), "r"(1));
-      }
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-    abort_flag = 0;
   }
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-  __syncthreads();  // the last barrier of the whole CTA: from here the producer keeps its own pace
+  __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-  const uint32_t full0 = smem_u32(&full_bar[0]), empty0 = smem_u32(&empty_bar[0]);
-  if constexpr (PLAN) {
-    if (warp == kLT / 32) {
-      plan_producer(a, sU, full0, empty0, &abort_flag);
-      return;
-    }
-  }
-  volatile int* abort_v = &abort_flag;
   const uint32_t tmem = tmem_slot;
   const uint32_t a_addr = smem_u32(sA), b_addr = smem_u32(sB), mbar_addr = smem_u32(&mbar);
   const double s = LAST ? sqrt(*a.rr * a.inv_n) : 0.0;
@@ -801,70 +694,21 @@ __global__ void __launch_bounds__(PLAN ? kLTPlan : kLT, PLAN ? kPlanCtasPerSm : 
   const int g = lane >> 3, c = lane & 7;  // gather: node group of the warp, feature chunk
   const int q = warp & 3, h = warp >> 2;  // epilogue: TMEM lane quarter, column half
   int np = 0;         // lanes 0..16: node pointers of the warp's 16 nodes (+ the end) in this tile
-  bool first = true;  // rows: the first tile's lists come synchronously, later ones were prefetched
-  int kp = 0;         // plan: planned tiles consumed
-  int4 ph = make_int4(0, 0, 1, 0);
-  if (PLAN && (int)blockIdx.x * kTile < N) ph = __ldg(&a.plan.hdr[blockIdx.x]);
+  bool first = true;  // the first tile's lists come synchronously, later ones were prefetched
 
   for (int tile = blockIdx.x; tile * kTile < N; tile += gridDim.x) {
     const int next = tile + (int)gridDim.x;
-    int4 ph_next = make_int4(0, 0, 1, 0);
-    if (PLAN && next * kTile < N) ph_next = __ldg(&a.plan.hdr[next]);
-    if (PLAN && plan_takes(ph)) {
-      // ---- A tile from the union buffer the producer filled
-      const int st = kp % kUStages;
-      const uint8_t* buf = sU + (size_t)st * kUSmem;
-      // thread 0 waits for the producer's copies; the barrier hands their data (and the outcome)
-      // to the tile warps
-      const int got = t == 0 ? (mbar_wait(full0 + 8u * st, (uint32_t)(kp / kUStages) & 1u, a.spin_limit) ? 1 : 0) : 1;
-      if (!tile_sync_and<PLAN>(got)) {  // report and stop; the producer drains its copies
-        if (t == 0) {
-          if (a.err) atomicMin(&a.err[kErrTimeout], tile);
-          *abort_v = 1;
-        }
-        break;
-      }
-      const uint4* slots = reinterpret_cast<const uint4*>(buf + kPlanMaxUnion * 128);
-#pragma unroll
-      for (int rnd = 0; rnd < 4; ++rnd) {
-        const int m = warp * 16 + rnd * 4 + g;
-        const int n = tile * kTile + m;
-        uint4 own = make_uint4(0u, 0u, 0u, 0u);
-        float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-        int deg = 0;
-        if (n < N) {
-          const uint4 lp = slots[m];
-          const uint32_t sl[8] = {lp.x & 0xFFFFu, lp.x >> 16, lp.y & 0xFFFFu, lp.y >> 16,
-                                  lp.z & 0xFFFFu, lp.z >> 16, lp.w & 0xFFFFu, lp.w >> 16};
-          own = *reinterpret_cast<const uint4*>(buf + sl[0] * 128u + c * 16);
-#pragma unroll
-          for (int j = 1; j < 8; ++j)
-            if (sl[j] != 0xFFFFu) {
-              ++deg;
-              add_chunk_bf(acc, *reinterpret_cast<const uint4*>(buf + sl[j] * 128u + c * 16));
-            }
-        }
-        const float inv = deg ? 1.f / (float)deg : 0.f;
-        const uint4 av = mean_chunk(acc, inv);
-        *reinterpret_cast<uint4*>(sA + a_chunk(m, c, 0)) = own;
-        *reinterpret_cast<uint4*>(sA + a_chunk(m, c, 1)) = av;
-        if (TRAIN && n < N) reinterpret_cast<uint4*>(a.Aout + (size_t)n * F)[c] = av;
-      }
-      tile_sync<PLAN>();  // every tile warp is done with the buffer
-      if (t == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(empty0 + 8u * st) : "memory");
-      ++kp;
-    } else {
+    {
       // ---- A tile row by row: the warp's 17 node pointers in one load, its nodes' neighbour lists
       // (contiguous in the pattern) in one more into shared memory, so each round of four nodes is
       // one round trip: the own chunk and up to eight neighbour chunks per lane in flight.
       const int wbase = tile * kTile + warp * 16;
       int* wnbr = s_nbr + warp * kNbrCache;
-      if (PLAN || first) {
+      if (first) {
         if (lane <= 16) np = __ldg(&a.node_ptr[min(wbase + lane, N)]);
         const int f0 = __shfl_sync(0xffffffffu, np, 0);
         const int fc = __shfl_sync(0xffffffffu, np, 16) - f0;
-        if (!PLAN)  // (the plan kernel reads a fallback tile's lists from global memory)
-          for (int j = lane; j < min(fc, kNbrCache); j += 32) wnbr[j] = __ldg(&a.nbr[f0 + j]);
+        for (int j = lane; j < min(fc, kNbrCache); j += 32) wnbr[j] = __ldg(&a.nbr[f0 + j]);
         first = false;
       } else {
         asm volatile("cp.async.wait_all;\n" ::: "memory");
@@ -874,7 +718,7 @@ __global__ void __launch_bounds__(PLAN ? kLTPlan : kLT, PLAN ? kPlanCtasPerSm : 
       // rows: the next tile's node pointers, used after this tile's rounds
       const int wnext = next * kTile + warp * 16;
       int np_next = 0;
-      if (!PLAN && lane <= 16 && next * kTile < N) np_next = __ldg(&a.node_ptr[min(wnext + lane, N)]);
+      if (lane <= 16 && next * kTile < N) np_next = __ldg(&a.node_ptr[min(wnext + lane, N)]);
 #pragma unroll 1
       for (int rnd = 0; rnd < 4; ++rnd) {
         const int li = rnd * 4 + g;
@@ -893,28 +737,27 @@ __global__ void __launch_bounds__(PLAN ? kLTPlan : kLT, PLAN ? kPlanCtasPerSm : 
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
               const int q8 = k + j;
-              mm[j] = q8 < k1 ? (!PLAN && q8 < kNbrCache ? wnbr[q8] : __ldg(&a.nbr[np0 + q8])) : n;
+              mm[j] = q8 < k1 ? (q8 < kNbrCache ? wnbr[q8] : __ldg(&a.nbr[np0 + q8])) : n;
             }
 #pragma unroll
             for (int j = 0; j < 8; ++j)
               v[j] = mm[j] != n ? __ldg(reinterpret_cast<const uint4*>(a.Hin + (size_t)mm[j] * F) + c)
-                                : make_uint4(0u, 0u, 0u, 0u);
+                                : make_uint4(kNegZero2, kNegZero2, kNegZero2, kNegZero2);
 #pragma unroll
-            for (int j = 0; j < 8; ++j)
-              if (mm[j] != n) {
-                ++deg;
-                add_chunk_bf(acc, v[j]);
-              }
+            for (int j = 0; j < 8; ++j) {  // (a missing neighbour adds -0: no branch)
+              deg += mm[j] != n ? 1 : 0;
+              add_chunk_bf(acc, v[j]);
+            }
           }
         }
-        const float inv = deg ? 1.f / (float)deg : 0.f;
+        const float inv = inv_deg(deg);
         const uint4 av = mean_chunk(acc, inv);
         *reinterpret_cast<uint4*>(sA + a_chunk(m, c, 0)) = own;
         *reinterpret_cast<uint4*>(sA + a_chunk(m, c, 1)) = av;
         if (TRAIN && n < N) reinterpret_cast<uint4*>(a.Aout + (size_t)n * F)[c] = av;
       }
-      if (!PLAN) {  // prefetch the next tile's neighbour lists (asynchronous copies, done during the
-                    // MMA and the epilogue); every lane has finished reading this tile's lists
+      {  // prefetch the next tile's neighbour lists (asynchronous copies, done during the MMA and the
+         // epilogue); every lane has finished reading this tile's lists
         __syncwarp();
         const int n0 = __shfl_sync(0xffffffffu, np_next, 0);
         const int nc = __shfl_sync(0xffffffffu, np_next, 16) - n0;
@@ -925,7 +768,6 @@ __global__ void __launch_bounds__(PLAN ? kLTPlan : kLT, PLAN ? kPlanCtasPerSm : 
         np = np_next;
       }
     }
-    ph = ph_next;
     // the decoder's per-node inputs (last layer), loaded now so they arrive during the MMA
     double2 rn_e = make_double2(0.0, 0.0), dn_e = rn_e, zb_e = rn_e;
     if (LAST && (warp >> 2) == 1) {
@@ -939,7 +781,7 @@ __global__ void __launch_bounds__(PLAN ? kLTPlan : kLT, PLAN ? kPlanCtasPerSm : 
     // generic-proxy shared-memory writes -> visible to the tensor core (async proxy)
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-    tile_sync<PLAN>();
+    __syncthreads();
     if (t == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
 #pragma unroll
@@ -971,13 +813,12 @@ __global__ void __launch_bounds__(PLAN ? kLTPlan : kLT, PLAN ? kPlanCtasPerSm : 
         // shared memory and tensor memory are released
         if (a.err) atomicMin(&a.err[kErrTimeout], tile);
         mbar_wait(mbar_addr, phase, kMbarSpinLimit);
-        *abort_v = 1;
       }
       mma_ok = ok;
       asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     }
     phase ^= 1u;
-    tile_sync<PLAN>();
+    __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     if (!mma_ok) break;  // uniform: every tile thread reads the same flag
 
@@ -1032,7 +873,7 @@ __global__ void __launch_bounds__(PLAN ? kLTPlan : kLT, PLAN ? kPlanCtasPerSm : 
       if (h == 0) ypart[m] = make_float2(y0, y1);
     }
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-    tile_sync<PLAN>();
+    __syncthreads();
     if (LAST && h == 1 && n < N) {
       const float2 yp = ypart[m];
       y0 = yp.x;
@@ -1063,11 +904,488 @@ __global__ void __launch_bounds__(PLAN ? kLTPlan : kLT, PLAN ? kPlanCtasPerSm : 
               *reinterpret_cast<const uint4*>(sOut + row * 128 + ((ch ^ (row & 7)) * 16));
       }
     }
-    tile_sync<PLAN>();  // tensor memory and the A tile are free for the next tile
+    __syncthreads();  // tensor memory and the A tile are free for the next tile
   }
   asm volatile("cp.async.wait_all;\n" ::: "memory");  // no copy in flight when the CTA leaves
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(F));
+}
+
+// ---- message-passing layer on planned patterns: one warp-specialised CTA per SM ------------------
+//
+// The same layer as k_mp_layer_tc (same operands, same order of every addition: the same bits),
+// arranged as a pipeline of roles over the CTA's tiles so that the copies, the gathers, the MMAs
+// and the epilogues of consecutive tiles overlap. Shared memory holds a ring of three stages of the
+// tiles' own rows in the layout the MMA reads (used by the MMA and the epilogue), a ring of two
+// stages of the tiles' unions in plain layout (used by the gathers alone, so a stage is refilled as
+// soon as its gathers are done), two buffers of the A operand's mean half and, in tensor memory,
+// two accumulators of 64 columns.
+//  own producer (warp 20): copies a tile's own 128 rows with one 2-D tensor copy
+//            (cp.async.bulk.tensor, no multicast) in the 128-byte swizzle (K-major: the A operand's
+//            own half needs no copy through registers) into a stage its previous tile's epilogue has
+//            released.
+//  union producer (warp 22): copies the tile's union, one bulk copy per run of consecutive rows
+//            (cp.async.bulk), and the node slots with one more, into a stage its previous tile's
+//            gathers have released. Row kPlanNone of every stage holds -0.0 (the unused slots'
+//            row). A tile the plan does not take gets no union: its neighbours come from global
+//            memory.
+//  gather (warps 0..15): 8 nodes per warp, four at once with 8 lanes per node (lane c: features
+//            8c..8c+7); each node's 7 neighbour slots read (row address = one multiply-add, unused
+//            slots at the -0.0 row) and summed in pattern order with add.rn.f32.bf16, times 1/deg,
+//            rounded to BF16 into the mean half (K-major, 128-byte swizzle); one arrival per warp on
+//            the union stage (free) and on the mean half (ready).
+//  MMA (warp 21, one thread): 8 x tcgen05.mma (M=128, N=64, K=16: four K-slices of the own rows,
+//            four of the means) and the bias slice (ones x the FP32 bias split into three BF16
+//            parts) into the accumulator; tcgen05.commit arrives on the accumulator's barrier,
+//            which frees the mean half and starts the epilogue.
+//  epilogue (warps 16..19, warp 16+q on TMEM lanes 32q..32q+31, one thread per node): reads the
+//            accumulator (2 x tcgen05.ld.32x32b.x32) and the node's own row (the residual) chunk by
+//            chunk, applies ReLU and the residual, writes each chunk into a 128-byte swizzled
+//            staging buffer, releases the accumulator and the own stage, and stores the warp's 32
+//            rows with one 2-D tensor store. The last layer runs the decoder per thread (features
+//            0..63 in order) and writes z.
+// Waits suspend in the hardware between polls (a 500 ns hint), so the waiting warps take few
+// issue slots; each is bounded (spin_limit polls). A role that gives up records the timeout and
+// raises the CTA's abort flag, which every other wait polls. Before the CTA leaves, the copies and
+// MMAs already issued have completed (bounded waits) and the tensor stores have read their staging.
+// Measured on the 2M-DOF plate (120.8 us for the previous two-CTA kernel whose tile warps gathered,
+// issued and ran the epilogue in turn): 8 gather warps and a union in swizzled 8-row boxes 186 us,
+// one own box and bulk runs 154 us; the gather was the limit, two warps per scheduler with a
+// swizzled-or-plain address per neighbour and a branch around each neighbour's adds.
+constexpr int kWsGatherWarps = 16, kWsEpiWarps = 4;
+constexpr int kWsEpi0 = kWsGatherWarps;                    // warps 16..19 (TMEM lane quarters 0..3)
+constexpr int kWsOwnProd = kWsEpi0 + kWsEpiWarps;          // warp 20
+constexpr int kWsMma = kWsOwnProd + 1;                     // warp 21
+constexpr int kWsUnionProd = kWsMma + 1;                   // warp 22
+constexpr int kWsT = (kWsUnionProd + 1) * 32;              // 736 threads (88 registers each)
+constexpr int kWsOwnStages = 3, kWsUStages = 2;
+constexpr int kWsOwn = kTile * 128;                        // own stage: 128 rows
+constexpr int kWsSlots = (kPlanMaxUnion + 1) * 128;        // union stage: the rows, the -0.0 row,
+constexpr int kWsUStage = kWsSlots + kTile * 16;           // then the tile's node slots
+constexpr int kWsStore = 32 * 128;                         // staging: a warp's 32 rows
+constexpr int kWsOffOwn = kBSmem + kBiasSmem;              // after B, the ones and the bias parts
+constexpr int kWsOffMean = kWsOffOwn + kWsOwnStages * kWsOwn;
+constexpr int kWsOffSt = kWsOffMean + 2 * kTile * 128;
+constexpr int kWsOffU = kWsOffSt + kWsEpiWarps * kWsStore;
+constexpr int kWsSmem = kWsOffU + kWsUStages * kWsUStage + 1024;  // (+ the 1024-byte alignment)
+static_assert(kWsOffOwn % 1024 == 0 && kWsOffMean % 1024 == 0 && kWsOffSt % 1024 == 0,
+              "the 128-byte swizzle's atoms start on 1024-byte boundaries");
+static_assert(kWsOffU % 16 == 0 && kWsUStage % 16 == 0, "bulk copies land on 16-byte boundaries");
+static_assert(kWsSmem + 1024 <= 227 * 1024, "one CTA per SM");
+constexpr uint32_t kWsSuspendNs = 500;  // suspend hint of a wait's poll
+
+// 2-D tensor copy of a box of rows into shared memory, completing on an mbarrier (no multicast).
+__device__ __forceinline__ void tma_load_rows(uint32_t dst, const CUtensorMap* map, int row, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(
+          dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(row), "r"(bar)
+      : "memory");
+}
+// 2-D tensor store of a box of rows from shared memory (rows past the tensor's end are not written).
+__device__ __forceinline__ void tma_store_rows(const CUtensorMap* map, int row, uint32_t src) {
+  asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.tile.bulk_group [%0, {%1, %2}], [%3];\n" ::"l"(
+                   reinterpret_cast<uint64_t>(map)),
+               "r"(0), "r"(row), "r"(src)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(bar) : "memory");
+}
+// 16-byte shared-memory accesses by 32-bit shared address (ordered with the barrier waits)
+__device__ __forceinline__ uint4 lds128(uint32_t addr) {
+  uint4 v;
+  asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];\n" : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "r"(addr)
+               : "memory");
+  return v;
+}
+__device__ __forceinline__ void sts128(uint32_t addr, const uint4 v) {
+  asm volatile("st.shared.v4.u32 [%0], {%1, %2, %3, %4};\n" ::"r"(addr), "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w)
+               : "memory");
+}
+
+// Bounded wait that suspends between polls (up to kWsSuspendNs each); false when `limit` polls
+// ran out or another role raised `abort_flag`.
+__device__ __forceinline__ bool ws_poll(uint32_t bar, uint32_t parity, long long limit, const volatile int* abort_flag) {
+  for (long long i = 0; i < limit; ++i) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity), "r"(kWsSuspendNs)
+        : "memory");
+    if (ok) return true;
+    if (*abort_flag) return false;
+  }
+  return false;
+}
+// A role's wait: true when the phase completed; false when another role stopped first or the limit
+// ran out (then the timeout is recorded and every role told to stop). `warp_wide`: the whole warp
+// waits and takes the same decision.
+__device__ __forceinline__ bool ws_wait(uint32_t bar, uint32_t parity, long long limit, volatile int* abort_v,
+                                        int* err, int tile, bool warp_wide = true) {
+  const bool ok = ws_poll(bar, parity, limit, abort_v);
+  if (!ok && !*abort_v) {
+    if (err) atomicMin(&err[kErrTimeout], tile);
+    *abort_v = 1;
+  }
+  return warp_wide ? __all_sync(0xffffffffu, ok) : ok;
+}
+
+template <bool TRAIN, bool LAST>
+__global__ void __launch_bounds__(kWsT, 1)
+    k_mp_layer_ws(const MpLayerArgs a, const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap tout) {
+  const int N = a.N;
+  if (a.skip && *a.skip) {  // uniform: before any barrier or tensor-memory allocation
+    if (LAST)               // the network is off: the Jacobi step
+      for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 2 * N; i += gridDim.x * blockDim.x)
+        a.z[i] = (a.zbase ? a.zbase[i] : 0.0) + a.invd[i] * a.r[i];
+    return;
+  }
+  extern __shared__ uint8_t smem_raw[];
+  // own ring (3): full / empty; union ring (2): full / empty; mean halves and accumulators (2):
+  // mean ready, MMA done, accumulator empty
+  __shared__ uint64_t o_full[kWsOwnStages], o_empty[kWsOwnStages], u_full[kWsUStages], u_empty[kWsUStages];
+  __shared__ uint64_t m_full[2], mma_done[2], acc_empty[2];
+  __shared__ uint32_t tmem_slot;
+  __shared__ int abort_flag;
+  __shared__ float wout[2 * F], bout[2];
+  uint8_t* base = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+  uint8_t* sB = base;  // element (n, k): (k/8)*1024 + (n/8)*128 + (n%8)*16 + (k%8)*2
+  uint8_t* sOnes = base + kBSmem;
+  uint8_t* sBias = sOnes + 4096;
+  uint8_t* sOwn = base + kWsOffOwn;    // own stage s: row m at m*128, 128-byte swizzle
+  uint8_t* sMean = base + kWsOffMean;  // mean half b: row m at m*128, 128-byte swizzle
+  uint8_t* sSt = base + kWsOffSt;      // epilogue warp q's staging: 32 rows, 128-byte swizzle
+  uint8_t* sU = base + kWsOffU;        // union stage s: slot j at j*128 (plain), then the node slots
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const __nv_bfloat16* W = a.P.pb + kMpOffL0 + a.layer * kMpLStride;
+  if (t < kTile) {
+    *reinterpret_cast<uint4*>(sOnes + (t >> 3) * 128 + (t & 7) * 16) = make_uint4(0x3F803F80u, 0x00003F80u, 0u, 0u);
+    *reinterpret_cast<uint4*>(sOnes + 2048 + (t >> 3) * 128 + (t & 7) * 16) = make_uint4(0u, 0u, 0u, 0u);
+  } else if (t < kTile + F) {
+    const int n = t - kTile;
+    const float b = a.P.pf[kMpOffL0 + a.layer * kMpLStride + F * 2 * F + n];
+    const __nv_bfloat16 b0 = __float2bfloat16_rn(b);
+    const float r1 = b - __bfloat162float(b0);
+    const __nv_bfloat16 b1 = __float2bfloat16_rn(r1);
+    const __nv_bfloat16 b2 = __float2bfloat16_rn(r1 - __bfloat162float(b1));
+    const uint32_t w0 = (uint32_t)__bfloat16_as_ushort(b0) | ((uint32_t)__bfloat16_as_ushort(b1) << 16);
+    *reinterpret_cast<uint4*>(sBias + (n >> 3) * 128 + (n & 7) * 16) =
+        make_uint4(w0, (uint32_t)__bfloat16_as_ushort(b2), 0u, 0u);
+    *reinterpret_cast<uint4*>(sBias + 1024 + (n >> 3) * 128 + (n & 7) * 16) = make_uint4(0u, 0u, 0u, 0u);
+  } else if (t < kTile + F + 8 * kWsUStages) {  // the -0.0 row of each union stage
+    const int j = t - kTile - F;
+    *reinterpret_cast<uint4*>(sU + (size_t)(j >> 3) * kWsUStage + kPlanNone * 128 + (j & 7) * 16) =
+        make_uint4(kNegZero2, kNegZero2, kNegZero2, kNegZero2);
+  }
+  for (int idx = t; idx < F * 16; idx += blockDim.x) {  // 64 rows x 16 chunks of 8 BF16
+    const int n = idx >> 4, kc = idx & 15;
+    const uint4 v = *reinterpret_cast<const uint4*>(W + n * 2 * F + kc * 8);
+    *reinterpret_cast<uint4*>(sB + kc * 1024 + (n >> 3) * 128 + (n & 7) * 16) = v;
+  }
+  if (LAST) {
+    for (int i = t; i < 2 * F; i += blockDim.x) wout[i] = bf(a.P.pb[kMpOffWout + i]);
+    if (t < 2) bout[t] = a.P.pf[kMpOffBout + t];
+  }
+  // B, the ones and the bias parts (generic writes) are read by the tensor core (async proxy)
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  if (warp == kWsMma) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_slot)),
+                 "r"(2 * F));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  if (t == 0) {
+    for (int j = 0; j < kWsOwnStages; ++j) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(&o_full[j])), "r"(1));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(&o_empty[j])), "r"(kWsEpiWarps));
+    }
+    for (int j = 0; j < kWsUStages; ++j) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(&u_full[j])), "r"(1));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(&u_empty[j])), "r"(kWsGatherWarps));
+    }
+    for (int j = 0; j < 2; ++j) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(&m_full[j])), "r"(kWsGatherWarps));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(&mma_done[j])), "r"(1));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(&acc_empty[j])), "r"(kWsEpiWarps));
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    abort_flag = 0;
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const uint32_t tmem = tmem_slot;
+  volatile int* abort_v = &abort_flag;
+  const long long lim = a.spin_limit;
+  const uint32_t ofull0 = smem_u32(&o_full[0]), oempty0 = smem_u32(&o_empty[0]), ufull0 = smem_u32(&u_full[0]),
+                 uempty0 = smem_u32(&u_empty[0]), mfull0 = smem_u32(&m_full[0]), mdone0 = smem_u32(&mma_done[0]),
+                 aempty0 = smem_u32(&acc_empty[0]);
+  // tile k of this CTA: own stage k % 3 (use k / 3); union stage, mean half and accumulator k % 2
+  // (use k / 2)
+
+  if (warp < kWsGatherWarps) {
+    // ---- gather: the mean half of the A operand
+    const int g = lane >> 3, c = lane & 7;
+    int kt = 0;
+    for (int tile = blockIdx.x; tile * kTile < N; tile += gridDim.x, ++kt) {
+      const int hs = kt & 1;
+      const uint32_t hpar = (uint32_t)(kt >> 1) & 1u;
+      if (!ws_wait(ufull0 + 8u * hs, hpar, lim, abort_v, a.err, tile)) break;
+      if (kt >= 2 && !ws_wait(mdone0 + 8u * hs, hpar ^ 1u, lim, abort_v, a.err, tile)) break;  // mean half free
+      const bool planned = plan_takes(__ldg(&a.plan.hdr[tile]));
+      const uint32_t row_a = smem_u32(sU + (size_t)hs * kWsUStage) + ((uint32_t)c << 4);  // chunk c of slot 0
+      const uint32_t slot_a = smem_u32(sU + (size_t)hs * kWsUStage + kWsSlots);
+      const uint32_t mean_a = smem_u32(sMean + (size_t)hs * kTile * 128);
+      uint4 lp[2];  // both rounds' slots first
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const int m = warp * 8 + u * 4 + g;
+        lp[u] = planned && tile * kTile + m < N ? lds128(slot_a + (uint32_t)m * 16u)
+                                                : make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu);
+      }
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const int m = warp * 8 + u * 4 + g;
+        const int n = tile * kTile + m;
+        float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        int deg = 0;
+        if (planned) {
+          const uint32_t sl[7] = {lp[u].x >> 16, lp[u].y & 0xFFFFu, lp[u].y >> 16, lp[u].z & 0xFFFFu,
+                                  lp[u].z >> 16, lp[u].w & 0xFFFFu, lp[u].w >> 16};
+          uint4 v[7];
+#pragma unroll
+          for (int j = 0; j < 7; ++j) {  // (a node past N reads the -0.0 row too: slots 0xFFFF masked)
+            const uint32_t q = n < N ? sl[j] : (uint32_t)kPlanNone;
+            v[j] = lds128(row_a + q * 128u);
+            deg += q != (uint32_t)kPlanNone ? 1 : 0;
+          }
+#pragma unroll
+          for (int j = 0; j < 7; ++j) add_chunk_bf(acc, v[j]);
+        } else if (n < N) {  // neighbours from global memory, in pattern order
+          const int k0 = __ldg(&a.node_ptr[n]), k1 = __ldg(&a.node_ptr[n + 1]);
+          for (int k = k0; k < k1; k += 8) {
+            int mm[8];
+            uint4 v[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) mm[j] = k + j < k1 ? __ldg(&a.nbr[k + j]) : n;
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+              v[j] = mm[j] != n ? __ldg(reinterpret_cast<const uint4*>(a.Hin + (size_t)mm[j] * F) + c)
+                                : make_uint4(kNegZero2, kNegZero2, kNegZero2, kNegZero2);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+              deg += mm[j] != n ? 1 : 0;
+              add_chunk_bf(acc, v[j]);
+            }
+          }
+        }
+        const uint4 av = mean_chunk(acc, inv_deg(deg));
+        sts128(mean_a + (uint32_t)m * 128u + ((uint32_t)(c ^ (m & 7)) << 4), av);
+        if (TRAIN && n < N) reinterpret_cast<uint4*>(a.Aout + (size_t)n * F)[c] = av;
+      }
+      // the mean half (generic writes) is read by the tensor core (async proxy)
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      __syncwarp();
+      if (lane == 0) {
+        mbar_arrive(uempty0 + 8u * hs);  // the union stage is free
+        mbar_arrive(mfull0 + 8u * hs);   // the mean half is ready
+      }
+    }
+  } else if (warp < kWsOwnProd) {
+    // ---- epilogue: one node per thread, its row chunk by chunk
+    const int q = warp - kWsEpi0;
+    const int m = q * 32 + lane;
+    const double sc = LAST ? sqrt(*a.rr * a.inv_n) : 0.0;
+    const uint32_t st = smem_u32(sSt + (size_t)q * kWsStore) + (uint32_t)lane * 128u;  // the thread's staged row
+    int kt = 0;
+    for (int tile = blockIdx.x; tile * kTile < N; tile += gridDim.x, ++kt) {
+      const int os = kt % kWsOwnStages, hs = kt & 1;
+      const uint32_t opar = (uint32_t)(kt / kWsOwnStages) & 1u, hpar = (uint32_t)(kt >> 1) & 1u;
+      const int n = tile * kTile + m;
+      const int row0 = tile * kTile + q * 32;
+      const bool store = a.Hout && row0 < N;  // warp-uniform
+      // the decoder's per-node inputs, loaded before the waits
+      double2 rn_e = make_double2(0.0, 0.0), dn_e = rn_e, zb_e = rn_e;
+      if (LAST && n < N) {
+        rn_e = reinterpret_cast<const double2*>(a.r)[n];
+        dn_e = reinterpret_cast<const double2*>(a.invd)[n];
+        if (a.zbase) zb_e = reinterpret_cast<const double2*>(a.zbase)[n];
+      }
+      if (store && lane == 0) asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory");  // staging free
+      if (!ws_wait(mdone0 + 8u * hs, hpar, lim, abort_v, a.err, tile)) break;
+      if (!ws_wait(ofull0 + 8u * os, opar, lim, abort_v, a.err, tile)) break;  // (complete: the MMA read it)
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+      const uint32_t own_a = smem_u32(sOwn + (size_t)os * kWsOwn) + (uint32_t)m * 128u;
+      float y0 = LAST ? bout[0] : 0.f, y1 = LAST ? bout[1] : 0.f;
+#pragma unroll
+      for (int hh = 0; hh < 2; ++hh) {
+        uint32_t v[32];
+        tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(hs * F + hh * 32), v);
+        asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+        for (int cc = 0; cc < 4; ++cc) {
+          const int ch = 4 * hh + cc;
+          const uint4 o = lds128(own_a + ((uint32_t)(ch ^ (m & 7)) << 4));  // the residual's chunk
+          const uint32_t ow[4] = {o.x, o.y, o.z, o.w};
+          uint32_t hw[4], gw[4];
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {  // (the accumulator holds the bias already)
+            const float g0 = fmaxf(__uint_as_float(v[cc * 8 + 2 * j]), 0.f);
+            const float g1 = fmaxf(__uint_as_float(v[cc * 8 + 2 * j + 1]), 0.f);
+            hw[j] = pack_bf2(bf_lo(ow[j]) + g0, bf_hi(ow[j]) + g1);
+            gw[j] = pack_bf2(g0, g1);
+          }
+          if (TRAIN && n < N)
+            reinterpret_cast<uint4*>(a.Gout + (size_t)n * F)[ch] = make_uint4(gw[0], gw[1], gw[2], gw[3]);
+          if (LAST) {  // decoder: y = b_out + sum over features 0..63 in order of W_out[:, f] H3[f]
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              const int f = 8 * ch + 2 * j;
+              y0 = fmaf(wout[f], bf_lo(hw[j]), y0);
+              y0 = fmaf(wout[f + 1], bf_hi(hw[j]), y0);
+              y1 = fmaf(wout[F + f], bf_lo(hw[j]), y1);
+              y1 = fmaf(wout[F + f + 1], bf_hi(hw[j]), y1);
+            }
+          }
+          if (store) sts128(st + ((uint32_t)(ch ^ (lane & 7)) << 4), make_uint4(hw[0], hw[1], hw[2], hw[3]));
+        }
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+      __syncwarp();
+      if (lane == 0) {
+        mbar_arrive(aempty0 + 8u * hs);  // the accumulator is free
+        mbar_arrive(oempty0 + 8u * os);  // the own stage is free (its MMA has completed)
+      }
+      if (LAST && n < N) {
+        if (TRAIN) reinterpret_cast<float2*>(a.Yout)[n] = make_float2(y0, y1);
+        double2 zn = make_double2(dn_e.x * (rn_e.x + sc * (double)y0), dn_e.y * (rn_e.y + sc * (double)y1));
+        if (a.zbase) {
+          zn.x += zb_e.x;
+          zn.y += zb_e.y;
+        }
+        reinterpret_cast<double2*>(a.z)[n] = zn;
+      }
+      if (store) {  // the warp's 32 rows: one tensor store
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        __syncwarp();
+        if (lane == 0) {
+          tma_store_rows(&tout, row0, smem_u32(sSt + (size_t)q * kWsStore));
+          asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
+        }
+      }
+    }
+    if (lane == 0) asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
+  } else if (warp == kWsOwnProd) {
+    // ---- own producer: the tiles' own rows, one tensor copy each
+    int kt = 0;
+    if (lane == 0) {
+      asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(&tin)) : "memory");
+      for (int tile = blockIdx.x; tile * kTile < N; tile += gridDim.x, ++kt) {
+        const int os = kt % kWsOwnStages;
+        if (kt >= kWsOwnStages &&
+            !ws_wait(oempty0 + 8u * os, (uint32_t)(kt / kWsOwnStages - 1) & 1u, lim, abort_v, a.err, tile, false))
+          break;
+        const uint32_t fb = ofull0 + 8u * os;
+        // the epilogue's generic reads of this stage are ordered before the copy's writes
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(fb), "r"((uint32_t)kWsOwn)
+                     : "memory");
+        tma_load_rows(smem_u32(sOwn + (size_t)os * kWsOwn), &tin, tile * kTile, fb);  // (past N: zeros)
+      }
+      // the copies issued land before the CTA leaves (bounded)
+      for (int j = max(0, kt - kWsOwnStages); j < kt; ++j)
+        mbar_wait(ofull0 + 8u * (j % kWsOwnStages), (uint32_t)(j / kWsOwnStages) & 1u, kMbarSpinLimit);
+    }
+  } else if (warp == kWsUnionProd) {
+    // ---- union producer: each tile's union and its node slots
+    int kt = 0;
+    for (int tile = blockIdx.x; tile * kTile < N; tile += gridDim.x, ++kt) {
+      const int us = kt & 1;
+      if (kt >= kWsUStages && !ws_wait(uempty0 + 8u * us, (uint32_t)((kt >> 1) - 1) & 1u, lim, abort_v, a.err, tile))
+        break;
+      const int4 ph = __ldg(&a.plan.hdr[tile]);
+      const bool planned = plan_takes(ph);
+      const int cnt = min(kTile, N - tile * kTile);
+      const int2 rn = planned && lane < ph.x ? __ldg(&a.plan.runs[(size_t)tile * kPlanMaxRuns + lane])
+                                             : make_int2(0, 0);  // lane j: run j (first node, rows)
+      int off = rn.y;  // inclusive prefix of the run lengths over the lanes
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, off, d);
+        if (lane >= d) off += v;
+      }
+      off -= rn.y;
+      const uint32_t stg = smem_u32(sU + (size_t)us * kWsUStage);
+      const uint32_t fb = ufull0 + 8u * us;
+      if (lane == 0) {
+        // the gathers' generic reads of this stage are ordered before the copies' writes
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(fb),
+                     "r"(planned ? (uint32_t)ph.y * 128u + (uint32_t)cnt * 16u : 0u)
+                     : "memory");
+        if (planned)
+          asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                           stg + kWsSlots),
+                       "l"(a.plan.local + (size_t)tile * kTile), "r"((uint32_t)cnt * 16u), "r"(fb)
+                       : "memory");
+      }
+      __syncwarp();
+      if (rn.y > 0)  // run j lands after the earlier runs
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                         stg + (uint32_t)off * 128u),
+                     "l"(a.Hin + (size_t)rn.x * F), "r"((uint32_t)rn.y * 128u), "r"(fb)
+                     : "memory");
+    }
+    // the copies issued land before the CTA leaves (bounded)
+    if (lane == 0)
+      for (int j = max(0, kt - kWsUStages); j < kt; ++j)
+        mbar_wait(ufull0 + 8u * (j & 1), (uint32_t)(j >> 1) & 1u, kMbarSpinLimit);
+  } else if (lane == 0) {
+    // ---- MMA: one thread
+    const uint32_t b_addr = smem_u32(sB);
+    int kt = 0;
+    for (int tile = blockIdx.x; tile * kTile < N; tile += gridDim.x, ++kt) {
+      const int os = kt % kWsOwnStages, hs = kt & 1;
+      const uint32_t opar = (uint32_t)(kt / kWsOwnStages) & 1u, hpar = (uint32_t)(kt >> 1) & 1u;
+      if (!ws_wait(mfull0 + 8u * hs, hpar, lim, abort_v, a.err, tile, false) ||
+          !ws_wait(ofull0 + 8u * os, opar, lim, abort_v, a.err, tile, false) ||
+          (kt >= 2 && !ws_wait(aempty0 + 8u * hs, hpar ^ 1u, lim, abort_v, a.err, tile, false)))
+        break;
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+      const uint32_t d = tmem + (uint32_t)(hs * F);
+      const uint32_t own = smem_u32(sOwn + (size_t)os * kWsOwn), mean = smem_u32(sMean + (size_t)hs * kTile * 128);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {  // K = 128 in slices of 16: four of the own rows, four of the means
+        const uint64_t ad = umma_desc_sw128((j < 4 ? own : mean) + (uint32_t)(j & 3) * 32u, 1024u);
+        const uint64_t bd = umma_desc(b_addr + (uint32_t)(2 * j) * 1024u, 1024u, 128u);
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d),
+            "l"(ad), "l"(bd), "r"(kIdesc), "r"(j > 0 ? 1u : 0u), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+      }
+      {  // + ones x bias parts
+        const uint64_t ad = umma_desc(smem_u32(sOnes), 2048u, 128u);
+        const uint64_t bd = umma_desc(smem_u32(sBias), 1024u, 128u);
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d),
+            "l"(ad), "l"(bd), "r"(kIdesc), "r"(1u), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(mdone0 + 8u * hs)
+                   : "memory");
+    }
+    // the MMAs issued complete before their shared and tensor memory are released (bounded)
+    for (int j = max(0, kt - 2); j < kt; ++j) mbar_wait(mdone0 + 8u * (j & 1), (uint32_t)(j >> 1) & 1u, kMbarSpinLimit);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  if (warp == kWsMma) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(2 * F));
 }
 
 // ---- training: loss and dL/dY ------------------------------------------------------------------
@@ -1454,7 +1772,7 @@ int grid_nodes(long long work, int per_block) {
 }
 
 int g_sms[64] = {};          // SM count per device (set by mpnn_prepare_device)
-bool g_tc_attr[8][64] = {};  // the layer kernel's attributes set: [TRAIN * 4 + LAST * 2 + PLAN][device]
+bool g_tc_attr[8][64] = {};  // the layer kernels' attributes set: [TRAIN * 4 + LAST * 2 + WS][device]
 
 int dev_slot() {
   int dev = 0;
@@ -1462,19 +1780,53 @@ int dev_slot() {
   return dev >= 0 && dev < 64 ? dev : 0;
 }
 
-template <bool TRAIN, bool LAST, bool PLAN>
+template <bool TRAIN, bool LAST, bool WS>
 cudaError_t set_tc_attr() {
-  bool& done = g_tc_attr[(TRAIN ? 4 : 0) + (LAST ? 2 : 0) + (PLAN ? 1 : 0)][dev_slot()];
+  bool& done = g_tc_attr[(TRAIN ? 4 : 0) + (LAST ? 2 : 0) + (WS ? 1 : 0)][dev_slot()];
   if (done) return cudaSuccess;
-  cudaError_t e = cudaFuncSetAttribute(k_mp_layer_tc<TRAIN, LAST, PLAN>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, PLAN ? kTcSmemPlan : kTcSmem);
+  const void* fn = WS ? reinterpret_cast<const void*>(k_mp_layer_ws<TRAIN, LAST>)
+                      : reinterpret_cast<const void*>(k_mp_layer_tc<TRAIN, LAST>);
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, WS ? kWsSmem : kTcSmem);
   if (e != cudaSuccess) return e;
-  // the whole unified L1 / shared array as shared memory: four CTAs of ~54 KB per SM (rows), two
-  // of ~110 KB (plan)
-  e = cudaFuncSetAttribute(k_mp_layer_tc<TRAIN, LAST, PLAN>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  // the whole unified L1 / shared array as shared memory: three CTAs of ~54 KB per SM (rows), one
+  // of ~203 KB (warp-specialised)
+  e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
   if (e != cudaSuccess) return e;
   done = true;
   return cudaSuccess;
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link against the driver
+// library); null when the driver does not provide it.
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+  static const EncodeTiledFn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return reinterpret_cast<EncodeTiledFn>(p);
+  }();
+  return fn;
+}
+
+// Tensor map of an activation array H [N][64] BF16 (rows of 128 bytes) with boxes of `box_rows`
+// rows x 64 features, written to / read from shared memory in the 128-byte swizzle.
+cudaError_t rows_map(CUtensorMap* map, const __nv_bfloat16* H, int N, int box_rows) {
+  const EncodeTiledFn enc = encode_tiled();
+  if (!enc) return cudaErrorNotSupported;
+  if (reinterpret_cast<uintptr_t>(H) & 15u) return cudaErrorInvalidValue;
+  const cuuint64_t dim[2] = {(cuuint64_t)F, (cuuint64_t)N};
+  const cuuint64_t stride[1] = {(cuuint64_t)F * 2};
+  const cuuint32_t box[2] = {(cuuint32_t)F, (cuuint32_t)box_rows};
+  const cuuint32_t elem[2] = {1, 1};
+  const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16*>(H), dim, stride, box,
+                         elem, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
 int enc_grid(int N) {  // one wave of kEncCtasPerSm CTAs per SM at most
@@ -1484,31 +1836,33 @@ int enc_grid(int N) {  // one wave of kEncCtasPerSm CTAs per SM at most
 }
 
 // One wave of the layer kernel: kLayerCtasPerSm CTAs on every SM (rows; the register cap of
-// __launch_bounds__ and the shared memory per CTA are sized for it), kPlanCtasPerSm (plan).
-int tc_grid(int N, bool plan) {
+// __launch_bounds__ and the shared memory per CTA are sized for it), one (warp-specialised).
+int tc_grid(int N, bool ws) {
   const int sms = g_sms[dev_slot()] > 0 ? g_sms[dev_slot()] : kSMs;
   const int tiles = (N + kTile - 1) / kTile;
-  return std::max(1, std::min(tiles, (plan ? kPlanCtasPerSm : kLayerCtasPerSm) * sms));
+  return std::max(1, std::min(tiles, (ws ? 1 : kLayerCtasPerSm) * sms));
 }
 
 template <bool TRAIN, bool LAST>
-void launch_layer_t(const MpLayerArgs& a, bool plan, cudaStream_t s) {
-  if (plan)
-    k_mp_layer_tc<TRAIN, LAST, true><<<tc_grid(a.N, true), kLTPlan, kTcSmemPlan, s>>>(a);
-  else
-    k_mp_layer_tc<TRAIN, LAST, false><<<tc_grid(a.N, false), kLT, kTcSmem, s>>>(a);
+cudaError_t launch_layer_t(const MpLayerArgs& a, bool plan, cudaStream_t s) {
+  if (!plan) {
+    k_mp_layer_tc<TRAIN, LAST><<<tc_grid(a.N, false), kLT, kTcSmem, s>>>(a);
+    return cudaSuccess;
+  }
+  CUtensorMap tin, tout;
+  cudaError_t e = rows_map(&tin, a.Hin, a.N, kTile);
+  if (e == cudaSuccess) e = rows_map(&tout, a.Hout ? a.Hout : a.Hin, a.N, 32);
+  if (e != cudaSuccess) return e;
+  k_mp_layer_ws<TRAIN, LAST><<<tc_grid(a.N, true), kWsT, kWsSmem, s>>>(a, tin, tout);
+  return cudaSuccess;
 }
 
-void launch_layer(const MpLayerArgs& a, bool train, bool last, cudaStream_t s) {
+cudaError_t launch_layer(const MpLayerArgs& a, bool train, bool last, cudaStream_t s) {
   const bool plan = a.plan.hdr != nullptr;
-  if (train && last)
-    launch_layer_t<true, true>(a, plan, s);
-  else if (train)
-    launch_layer_t<true, false>(a, plan, s);
-  else if (last)
-    launch_layer_t<false, true>(a, plan, s);
-  else
-    launch_layer_t<false, false>(a, plan, s);
+  if (train && last) return launch_layer_t<true, true>(a, plan, s);
+  if (train) return launch_layer_t<true, false>(a, plan, s);
+  if (last) return launch_layer_t<false, true>(a, plan, s);
+  return launch_layer_t<false, false>(a, plan, s);
 }
 
 }  // namespace
@@ -1614,7 +1968,8 @@ cudaError_t launch_mp_forward(const MpnnGraph& g, const MpnnParams& P, const dou
     a.Hout = train ? w.H[l + 1] : (last ? nullptr : w.H[(l + 1) & 1]);
     a.Gout = train ? w.G[l] : nullptr;
     a.Aout = train ? w.A[l] : nullptr;
-    launch_layer(a, train, last, s);
+    const cudaError_t e = launch_layer(a, train, last, s);
+    if (e != cudaSuccess) return e;
   }
   count_launches(1 + kMpL);
   return cudaGetLastError();
@@ -1648,7 +2003,8 @@ cudaError_t launch_mp_stage(const MpnnGraph& g, const MpnnParams& P, int stage, 
     const bool last = stage == kMpL;
     a.Hin = w.H[(stage - 1) & 1];
     a.Hout = last ? nullptr : w.H[stage & 1];
-    launch_layer(a, false, last, s);
+    const cudaError_t e = launch_layer(a, false, last, s);
+    if (e != cudaSuccess) return e;
   }
   count_launches(1);
   return cudaGetLastError();
