@@ -689,9 +689,10 @@ def rooflines(a, pkg, K, ctx, stream, ev_start, ev_stop, N, n, mat, weights, pre
     layer_bytes = N * 2 * 128 + graph_bytes
     last_bytes = N * 128 + graph_bytes + n * 8 * 3  # H in; r, D^-1 in, z out
     enc_bytes = N * (16 + 24 + 128)
-    lay = roof("k_mp_layer_tc (message-passing layer, tcgen05 BF16, layer 2 of 3, "
-               + ("gather plan" if planned else "row gather") + ")", layer_bytes, tm["layer_s"][1],
-               profile_traffic("mp_layer_tc_plate2m.md") if full else None,
+    lay = roof(("k_mp_layer_ws (message-passing layer, warp-specialised, tcgen05 BF16, layer 2 of 3, gather plan)"
+                if planned else "k_mp_layer_tc (message-passing layer, tcgen05 BF16, layer 2 of 3, row gather)"),
+               layer_bytes, tm["layer_s"][1],
+               profile_traffic("mp_layer_ws_plate2m.md") if full and planned else None,
                layers_us=[t * 1e6 for t in tm["layer_s"]], encoder_us=tm["encoder_s"] * 1e6,
                last_layer_gbs=last_bytes / tm["layer_s"][2] / 1e9, encoder_gbs=enc_bytes / tm["encoder_s"] / 1e9,
                network_apply_us=(tm["encoder_s"] + sum(tm["layer_s"])) * 1e6)

@@ -179,16 +179,17 @@ struct MpnnParams {  // device copies of the packed parameters
 // Per-tile gather plan of the message-passing layers (built on the GPU from the pattern, once
 // per matrix): for each tile of 128 consecutive nodes, the rows its nodes read (their own and
 // their neighbours') as at most kPlanMaxRuns runs of consecutive nodes holding at most
-// kPlanMaxUnion rows, and per node the positions of its own row and of its neighbours' rows
-// (ascending pattern order) in that union; an unused position holds kPlanNone, the row after the
-// union (which the layers keep at -0.0, so a padded sum needs no branch). A tile that does not
-// fit is marked and its neighbours are gathered from global memory instead.
+// kPlanMaxUnion rows, and per node its degree (neighbours without itself) and the positions of
+// its neighbours' rows (ascending pattern order) in that union; an unused position holds
+// kPlanNone, the row after the union (which the layers keep at -0.0, so a padded sum needs no
+// branch). A tile that does not fit is marked and its neighbours are gathered from global memory
+// instead.
 constexpr int kPlanMaxRuns = 8, kPlanMaxUnion = 400, kPlanMaxLocal = 7, kPlanSpan = 4096;
 constexpr int kPlanNone = kPlanMaxUnion;
 struct MpTilePlan {
   const int4* hdr = nullptr;    // [tiles]: (runs, union rows, fallback, 0)
   const int2* runs = nullptr;   // [tiles][kPlanMaxRuns]: (first node, rows)
-  const uint4* local = nullptr; // [nodes]: 8 uint16: [0] own row, [1..deg] neighbours, kPlanNone unused
+  const uint4* local = nullptr; // [nodes]: 8 uint16: [0] degree, [1..deg] neighbours, kPlanNone unused
 };
 struct MpnnGraph {  // the node-block pattern (self included; the network skips self)
   int n_nodes = 0;

@@ -294,12 +294,12 @@ __global__ void __launch_bounds__(256) k_mp_tile_plan(int N, const int* __restri
     uint16_t slot[8];
 #pragma unroll
     for (int j = 0; j < 8; ++j) slot[j] = (uint16_t)kPlanNone;
-    slot[0] = (uint16_t)rank(n);
     int k = 1;
     for (int e = node_ptr[n]; e < node_ptr[n + 1]; ++e) {
       const int v = nbr[e];
       if (v != n) slot[k++] = (uint16_t)rank(v);
     }
+    slot[0] = (uint16_t)(k - 1);  // the degree (the layers read their own rows elsewhere)
     local[n] = make_uint4((uint32_t)slot[0] | ((uint32_t)slot[1] << 16), (uint32_t)slot[2] | ((uint32_t)slot[3] << 16),
                           (uint32_t)slot[4] | ((uint32_t)slot[5] << 16), (uint32_t)slot[6] | ((uint32_t)slot[7] << 16));
   }
@@ -591,6 +591,18 @@ __device__ __forceinline__ void add_chunk_bf(float (&acc)[8], const uint4 v) {
         "add.rn.f32.bf16 %1, hi, %1;\n\t}\n"
         : "+f"(acc[2 * q]), "+f"(acc[2 * q + 1])
         : "r"(w[q]));
+}
+// g + the low / high BF16 of w, widened exactly: one IEEE round-to-nearest add (the bits of
+// bf_lo(w) + g, in one instruction).
+__device__ __forceinline__ float add_bf_lo(uint32_t w, float g) {
+  float d;
+  asm("{\n\t.reg .b16 lo, hi;\n\tmov.b32 {lo, hi}, %1;\n\tadd.rn.f32.bf16 %0, lo, %2;\n\t}\n" : "=f"(d) : "r"(w), "f"(g));
+  return d;
+}
+__device__ __forceinline__ float add_bf_hi(uint32_t w, float g) {
+  float d;
+  asm("{\n\t.reg .b16 lo, hi;\n\tmov.b32 {lo, hi}, %1;\n\tadd.rn.f32.bf16 %0, hi, %2;\n\t}\n" : "=f"(d) : "r"(w), "f"(g));
+  return d;
 }
 // Eight BF16 -0.0: the chunk a missing neighbour contributes. x + (-0) = x exactly for every x
 // (both zeros included), so a sum padded with it has the bits of the sum without it, and the
@@ -1052,6 +1064,7 @@ __global__ void __launch_bounds__(kWsT, 1)
   __shared__ uint32_t tmem_slot;
   __shared__ int abort_flag;
   __shared__ float wout[2 * F], bout[2];
+  __shared__ float s_inv[kPlanMaxLocal + 1];  // 1/deg (IEEE quotients), 0 for no neighbour
   uint8_t* base = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
   uint8_t* sB = base;  // element (n, k): (k/8)*1024 + (n/8)*128 + (n%8)*16 + (k%8)*2
   uint8_t* sOnes = base + kBSmem;
@@ -1090,6 +1103,7 @@ __global__ void __launch_bounds__(kWsT, 1)
     for (int i = t; i < 2 * F; i += blockDim.x) wout[i] = bf(a.P.pb[kMpOffWout + i]);
     if (t < 2) bout[t] = a.P.pf[kMpOffBout + t];
   }
+  if (t <= kPlanMaxLocal) s_inv[t] = inv_deg(t);
   // B, the ones and the bias parts (generic writes) are read by the tensor core (async proxy)
   asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
   if (warp == kWsMma) {
@@ -1130,12 +1144,15 @@ __global__ void __launch_bounds__(kWsT, 1)
     // ---- gather: the mean half of the A operand
     const int g = lane >> 3, c = lane & 7;
     int kt = 0;
+    int4 ph = (int)blockIdx.x * kTile < N ? __ldg(&a.plan.hdr[blockIdx.x]) : make_int4(0, 0, 1, 0);
     for (int tile = blockIdx.x; tile * kTile < N; tile += gridDim.x, ++kt) {
       const int hs = kt & 1;
       const uint32_t hpar = (uint32_t)(kt >> 1) & 1u;
+      const bool planned = plan_takes(ph);
+      const int next = tile + (int)gridDim.x;  // its header arrives during this tile
+      ph = next * kTile < N ? __ldg(&a.plan.hdr[next]) : make_int4(0, 0, 1, 0);
       if (!ws_wait(ufull0 + 8u * hs, hpar, lim, abort_v, a.err, tile)) break;
       if (kt >= 2 && !ws_wait(mdone0 + 8u * hs, hpar ^ 1u, lim, abort_v, a.err, tile)) break;  // mean half free
-      const bool planned = plan_takes(__ldg(&a.plan.hdr[tile]));
       const uint32_t row_a = smem_u32(sU + (size_t)hs * kWsUStage) + ((uint32_t)c << 4);  // chunk c of slot 0
       const uint32_t slot_a = smem_u32(sU + (size_t)hs * kWsUStage + kWsSlots);
       const uint32_t mean_a = smem_u32(sMean + (size_t)hs * kTile * 128);
@@ -1143,8 +1160,9 @@ __global__ void __launch_bounds__(kWsT, 1)
 #pragma unroll
       for (int u = 0; u < 2; ++u) {
         const int m = warp * 8 + u * 4 + g;
+        constexpr uint32_t kNone2 = (uint32_t)kPlanNone * 0x10001u;
         lp[u] = planned && tile * kTile + m < N ? lds128(slot_a + (uint32_t)m * 16u)
-                                                : make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu);
+                                                : make_uint4((uint32_t)kPlanNone << 16, kNone2, kNone2, kNone2);
       }
 #pragma unroll
       for (int u = 0; u < 2; ++u) {
@@ -1157,11 +1175,8 @@ __global__ void __launch_bounds__(kWsT, 1)
                                   lp[u].z >> 16, lp[u].w & 0xFFFFu, lp[u].w >> 16};
           uint4 v[7];
 #pragma unroll
-          for (int j = 0; j < 7; ++j) {  // (a node past N reads the -0.0 row too: slots 0xFFFF masked)
-            const uint32_t q = n < N ? sl[j] : (uint32_t)kPlanNone;
-            v[j] = lds128(row_a + q * 128u);
-            deg += q != (uint32_t)kPlanNone ? 1 : 0;
-          }
+          for (int j = 0; j < 7; ++j) v[j] = lds128(row_a + sl[j] * 128u);  // (unused: the -0.0 row)
+          deg = (int)(lp[u].x & 0xFFFFu);
 #pragma unroll
           for (int j = 0; j < 7; ++j) add_chunk_bf(acc, v[j]);
         } else if (n < N) {  // neighbours from global memory, in pattern order
@@ -1182,7 +1197,7 @@ __global__ void __launch_bounds__(kWsT, 1)
             }
           }
         }
-        const uint4 av = mean_chunk(acc, inv_deg(deg));
+        const uint4 av = mean_chunk(acc, deg <= kPlanMaxLocal ? s_inv[deg] : inv_deg(deg));
         sts128(mean_a + (uint32_t)m * 128u + ((uint32_t)(c ^ (m & 7)) << 4), av);
         if (TRAIN && n < N) reinterpret_cast<uint4*>(a.Aout + (size_t)n * F)[c] = av;
       }
@@ -1215,27 +1230,34 @@ __global__ void __launch_bounds__(kWsT, 1)
         if (a.zbase) zb_e = reinterpret_cast<const double2*>(a.zbase)[n];
       }
       if (store && lane == 0) asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory");  // staging free
-      if (!ws_wait(mdone0 + 8u * hs, hpar, lim, abort_v, a.err, tile)) break;
-      if (!ws_wait(ofull0 + 8u * os, opar, lim, abort_v, a.err, tile)) break;  // (complete: the MMA read it)
-      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+      if (!ws_wait(ofull0 + 8u * os, opar, lim, abort_v, a.err, tile)) break;
+      // the residual (the node's own row): the first half read while the MMA runs, the second
+      // while the accumulator's second half is read
       const uint32_t own_a = smem_u32(sOwn + (size_t)os * kWsOwn) + (uint32_t)m * 128u;
+      uint4 res[4];
+#pragma unroll
+      for (int cc = 0; cc < 4; ++cc) res[cc] = lds128(own_a + ((uint32_t)(cc ^ (m & 7)) << 4));
+      if (!ws_wait(mdone0 + 8u * hs, hpar, lim, abort_v, a.err, tile)) break;
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
       float y0 = LAST ? bout[0] : 0.f, y1 = LAST ? bout[1] : 0.f;
 #pragma unroll
       for (int hh = 0; hh < 2; ++hh) {
         uint32_t v[32];
         tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(hs * F + hh * 32), v);
+        if (hh == 1)
+#pragma unroll
+          for (int cc = 0; cc < 4; ++cc) res[cc] = lds128(own_a + ((uint32_t)((4 + cc) ^ (m & 7)) << 4));
         asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 #pragma unroll
         for (int cc = 0; cc < 4; ++cc) {
           const int ch = 4 * hh + cc;
-          const uint4 o = lds128(own_a + ((uint32_t)(ch ^ (m & 7)) << 4));  // the residual's chunk
-          const uint32_t ow[4] = {o.x, o.y, o.z, o.w};
+          const uint32_t ow[4] = {res[cc].x, res[cc].y, res[cc].z, res[cc].w};
           uint32_t hw[4], gw[4];
 #pragma unroll
           for (int j = 0; j < 4; ++j) {  // (the accumulator holds the bias already)
             const float g0 = fmaxf(__uint_as_float(v[cc * 8 + 2 * j]), 0.f);
             const float g1 = fmaxf(__uint_as_float(v[cc * 8 + 2 * j + 1]), 0.f);
-            hw[j] = pack_bf2(bf_lo(ow[j]) + g0, bf_hi(ow[j]) + g1);
+            hw[j] = pack_bf2(add_bf_lo(ow[j], g0), add_bf_hi(ow[j], g1));
             gw[j] = pack_bf2(g0, g1);
           }
           if (TRAIN && n < N)
@@ -1302,15 +1324,24 @@ __global__ void __launch_bounds__(kWsT, 1)
   } else if (warp == kWsUnionProd) {
     // ---- union producer: each tile's union and its node slots
     int kt = 0;
+    // lane j: run j (first node, rows) of the tile; the next tile's header and runs are loaded
+    // while this tile waits for its stage
+    auto tile_runs = [&](int tl, int4& h, int2& r) {
+      h = tl * kTile < N ? __ldg(&a.plan.hdr[tl]) : make_int4(0, 0, 1, 0);
+      r = plan_takes(h) && lane < h.x ? __ldg(&a.plan.runs[(size_t)tl * kPlanMaxRuns + lane]) : make_int2(0, 0);
+    };
+    int4 ph_next;
+    int2 rn_next;
+    tile_runs(blockIdx.x, ph_next, rn_next);
     for (int tile = blockIdx.x; tile * kTile < N; tile += gridDim.x, ++kt) {
       const int us = kt & 1;
+      const int4 ph = ph_next;
+      const int2 rn = rn_next;
+      tile_runs(tile + (int)gridDim.x, ph_next, rn_next);
       if (kt >= kWsUStages && !ws_wait(uempty0 + 8u * us, (uint32_t)((kt >> 1) - 1) & 1u, lim, abort_v, a.err, tile))
         break;
-      const int4 ph = __ldg(&a.plan.hdr[tile]);
       const bool planned = plan_takes(ph);
       const int cnt = min(kTile, N - tile * kTile);
-      const int2 rn = planned && lane < ph.x ? __ldg(&a.plan.runs[(size_t)tile * kPlanMaxRuns + lane])
-                                             : make_int2(0, 0);  // lane j: run j (first node, rows)
       int off = rn.y;  // inclusive prefix of the run lengths over the lanes
 #pragma unroll
       for (int d = 1; d < 32; d <<= 1) {
