@@ -956,7 +956,7 @@ __global__ void __launch_bounds__(kLT, kLayerCtasPerSm) k_mp_layer_tc(const MpLa
 //            staging buffer, releases the accumulator and the own stage, and stores the warp's 32
 //            rows with one 2-D tensor store. The last layer runs the decoder per thread (features
 //            0..63 in order) and writes z.
-// Waits suspend in the hardware between polls (a 500 ns hint), so the waiting warps take few
+// Waits suspend in the hardware between polls (a 2 us hint), so the waiting warps take few
 // issue slots; each is bounded (spin_limit polls). A role that gives up records the timeout and
 // raises the CTA's abort flag, which every other wait polls. Before the CTA leaves, the copies and
 // MMAs already issued have completed (bounded waits) and the tensor stores have read their staging.
@@ -984,7 +984,7 @@ static_assert(kWsOffOwn % 1024 == 0 && kWsOffMean % 1024 == 0 && kWsOffSt % 1024
               "the 128-byte swizzle's atoms start on 1024-byte boundaries");
 static_assert(kWsOffU % 16 == 0 && kWsUStage % 16 == 0, "bulk copies land on 16-byte boundaries");
 static_assert(kWsSmem + 1024 <= 227 * 1024, "one CTA per SM");
-constexpr uint32_t kWsSuspendNs = 500;  // suspend hint of a wait's poll
+constexpr uint32_t kWsSuspendNs = 2000;  // suspend hint of a wait's poll
 
 // 2-D tensor copy of a box of rows into shared memory, completing on an mbarrier (no multicast).
 __device__ __forceinline__ void tma_load_rows(uint32_t dst, const CUtensorMap* map, int row, uint32_t bar) {
@@ -1063,7 +1063,8 @@ __global__ void __launch_bounds__(kWsT, 1)
   __shared__ uint64_t m_full[2], mma_done[2], acc_empty[2];
   __shared__ uint32_t tmem_slot;
   __shared__ int abort_flag;
-  __shared__ float wout[2 * F], bout[2];
+  __shared__ __align__(16) float wout[2 * F];
+  __shared__ float bout[2];
   __shared__ float s_inv[kPlanMaxLocal + 1];  // 1/deg (IEEE quotients), 0 for no neighbour
   uint8_t* base = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
   uint8_t* sB = base;  // element (n, k): (k/8)*1024 + (n/8)*128 + (n%8)*16 + (k%8)*2
@@ -1263,13 +1264,18 @@ __global__ void __launch_bounds__(kWsT, 1)
           if (TRAIN && n < N)
             reinterpret_cast<uint4*>(a.Gout + (size_t)n * F)[ch] = make_uint4(gw[0], gw[1], gw[2], gw[3]);
           if (LAST) {  // decoder: y = b_out + sum over features 0..63 in order of W_out[:, f] H3[f]
+            const float4* w4 = reinterpret_cast<const float4*>(wout);
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-              const int f = 8 * ch + 2 * j;
-              y0 = fmaf(wout[f], bf_lo(hw[j]), y0);
-              y0 = fmaf(wout[f + 1], bf_hi(hw[j]), y0);
-              y1 = fmaf(wout[F + f], bf_lo(hw[j]), y1);
-              y1 = fmaf(wout[F + f + 1], bf_hi(hw[j]), y1);
+            for (int o = 0; o < 2; ++o) {  // output o's chain over the chunk's 8 features, in order
+              const float4 p0 = w4[o * (F >> 2) + 2 * ch], p1 = w4[o * (F >> 2) + 2 * ch + 1];
+              const float w[8] = {p0.x, p0.y, p0.z, p0.w, p1.x, p1.y, p1.z, p1.w};
+              float y = o ? y1 : y0;
+#pragma unroll
+              for (int j = 0; j < 4; ++j) {
+                y = fmaf(w[2 * j], bf_lo(hw[j]), y);
+                y = fmaf(w[2 * j + 1], bf_hi(hw[j]), y);
+              }
+              if (o) y1 = y; else y0 = y;
             }
           }
           if (store) sts128(st + ((uint32_t)(ch ^ (lane & 7)) << 4), make_uint4(hw[0], hw[1], hw[2], hw[3]));
