@@ -10,20 +10,21 @@
 // runs on the tensor cores too (one K=16 MMA per 128 nodes, the FP32 bias entering as three exact
 // BF16 parts against constant ones in the A operand).
 //
-// The three message-passing layers run on the 5th-generation tensor cores: a CTA owns a tile of
-// 128 nodes at a time, builds each node's own row and the mean of its neighbours' rows in shared
-// memory as the A operand ([128 nodes] x [128 = own 64 | mean 64], K-major, no swizzle), holds
-// W_l as the B operand, and one thread issues eight tcgen05.mma.kind::f16 (M=128, N=64, K=16)
-// into a 64-column FP32 accumulator in tensor memory. tcgen05.commit signals an mbarrier; each
-// warp then reads its 32 accumulator lanes (tcgen05.ld.32x32b) and applies bias, ReLU and the
-// residual add in the epilogue. On patterns with a gather plan a producer warp brings each
-// tile's rows into shared memory with bulk copies ahead of the tile warps.
+// The three message-passing layers run on the 5th-generation tensor cores: per tile of 128 nodes
+// the A operand is [own row 64 | mean of the neighbours' rows 64] (BF16, K-major, 128-byte
+// swizzle), W_l is the B operand, and one thread issues eight tcgen05.mma.kind::f16 (M=128, N=64,
+// K=16) plus one for the bias into a 64-column FP32 accumulator in tensor memory; tcgen05.commit
+// signals an mbarrier and the epilogue reads the accumulator (tcgen05.ld.32x32b), applies ReLU and
+// the residual add. Two kernels give the same bits: k_mp_layer_ws on patterns with a gather plan
+// (one warp-specialised CTA per SM: tensor and bulk copies, gathers, MMAs and epilogues of
+// consecutive tiles overlap) and k_mp_layer_tc row by row from global memory.
 //
 // Training: the forward pass also stores the inputs X, the aggregates A_l and the ReLU outputs
-// G_l; the backward pass (CUDA cores, FP32 accumulation of BF16 operands) produces weight
-// gradients as per-block partial sums added in block order (deterministic). The loss of a
-// (residual r, error e = A^-1 r) pair is 1 - (z'r)^2 / ((z'Az)(e'r)), the squared sine of the
-// energy-norm angle between z and e.
+// G_l. The backward pass runs the per-node parts (ReLU masks, the mean aggregation's transpose as
+// a gather over the symmetric pattern) on CUDA cores and the layers' weight gradients on the
+// tensor cores (k_mp_wgrad_tc: FP32 accumulation in tensor memory), each as per-block partial sums
+// added in block order (deterministic). The loss of a (residual r, error e = A^-1 r) pair is
+// 1 - (z'r)^2 / ((z'Az)(e'r)), the squared sine of the energy-norm angle between z and e.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
