@@ -2,7 +2,7 @@
 scalars, FP64 true-residual reliable updates) against the reference's FP64 solution.
 
 Bar: converged on the FP64 TRUE residual (< rtol), displacements within relative 1e-8 of the
-reference's serial FP64 CG at rtol 1e-10 (the north star's bar), iterations at most 1.35x the
+reference's serial FP64 CG at rtol 1e-10 (the correctness bar), iterations at most 1.35x the
 FP64 count (the difference form keeps the FP32 penalty small)."""
 import numpy as np
 import pytest
