@@ -952,10 +952,10 @@ __global__ void __launch_bounds__(kLT, kLayerCtasPerSm) k_mp_layer_tc(const MpLa
 //            parts) into the accumulator; tcgen05.commit arrives on the accumulator's barrier,
 //            which frees the mean half and starts the epilogue.
 //  epilogue (warps 16..19, warp 16+q on TMEM lanes 32q..32q+31, one thread per node): reads the
-//            accumulator (2 x tcgen05.ld.32x32b.x32) and the node's own row (the residual) chunk by
-//            chunk, applies ReLU and the residual, writes each chunk into a 128-byte swizzled
-//            staging buffer, releases the accumulator and the own stage, and stores the warp's 32
-//            rows with one 2-D tensor store. The last layer runs the decoder per thread (features
+//            node's own row (the residual; its first half while the MMA runs) and the accumulator
+//            (2 x tcgen05.ld.32x32b.x32), applies ReLU and the residual, writes each chunk into a
+//            128-byte swizzled staging buffer, releases the accumulator and the own stage, and
+//            stores the warp's 32 rows with one 2-D tensor store. The last layer runs the decoder per thread (features
 //            0..63 in order) and writes z.
 // Waits suspend in the hardware between polls (a 2 us hint), so the waiting warps take few
 // issue slots; each is bounded (spin_limit polls). A role that gives up records the timeout and
@@ -964,13 +964,16 @@ __global__ void __launch_bounds__(kLT, kLayerCtasPerSm) k_mp_layer_tc(const MpLa
 // Measured on the 2M-DOF plate (120.8 us for the previous two-CTA kernel whose tile warps gathered,
 // issued and ran the epilogue in turn): 8 gather warps and a union in swizzled 8-row boxes 186 us,
 // one own box and bulk runs 154 us; the gather was the limit, two warps per scheduler with a
-// swizzled-or-plain address per neighbour and a branch around each neighbour's adds.
+// swizzled-or-plain address per neighbour and a branch around each neighbour's adds. This layout
+// (16 gather warps, plain union addressing, no branches) ran at 106 us, and at 88 us (0.47 of the
+// measured HBM bandwidth) once the tile headers and runs were loaded a tile ahead; it is then
+// bound by instruction issue and shared-memory latency, not by HBM.
 constexpr int kWsGatherWarps = 16, kWsEpiWarps = 4;
 constexpr int kWsEpi0 = kWsGatherWarps;                    // warps 16..19 (TMEM lane quarters 0..3)
 constexpr int kWsOwnProd = kWsEpi0 + kWsEpiWarps;          // warp 20
 constexpr int kWsMma = kWsOwnProd + 1;                     // warp 21
 constexpr int kWsUnionProd = kWsMma + 1;                   // warp 22
-constexpr int kWsT = (kWsUnionProd + 1) * 32;              // 736 threads (88 registers each)
+constexpr int kWsT = (kWsUnionProd + 1) * 32;              // 736 threads (at most 88 registers each)
 constexpr int kWsOwnStages = 3, kWsUStages = 2;
 constexpr int kWsOwn = kTile * 128;                        // own stage: 128 rows
 constexpr int kWsSlots = (kPlanMaxUnion + 1) * 128;        // union stage: the rows, the -0.0 row,
