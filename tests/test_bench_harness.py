@@ -62,3 +62,35 @@ def test_clock_parsing():
            "1900, 1965, 995.0, Not Active, Not Active, Not Active, Active\n")
     c = bench.parse_clock_csv(txt)
     assert c["sm_mhz"] == 1900 and c["sm_max_mhz"] == 1965 and c["reasons"] == ["sw_power_cap"]
+
+
+def test_reference_arm_line():
+    """`bench.py --impl reference` (the reference's serial core on the host, one bounded sample of
+    the 2M-DOF workload per step) prints one JSON line with the contract's keys, flags the
+    extrapolation to the iteration count of the reference's own full run, and its figures agree
+    with one another: value = DOFs / time-to-solve, ms_per_step = the sample that ran, no
+    host-device bytes."""
+    import pytest
+    import oracle
+    if not oracle.RefCore.available():
+        pytest.skip("the reference core (oracle/_ref) is not built")
+    r = subprocess.run([sys.executable, os.path.join(REPO, "bench.py"), "--impl", "reference", "--steps", "1",
+                        "--warmup", "3"], capture_output=True, text=True, timeout=600, cwd=REPO)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1, r.stdout
+    d = json.loads(lines[0])
+    if "unavailable" in d:
+        pytest.skip(d["unavailable"])
+    for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
+              "scaling", "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"):
+        assert k in d, k
+    assert d["impl"] == "reference" and d["steps"] == 1 and d["warmup"] == 3 and d["higher_is_better"] is True
+    assert d["extrapolated"] is True and d["sample_iters"] > 0
+    cb = d["cpu_baseline"]
+    assert cb["kind"] in ("reference", "port") and cb["cores"] == 1 and cb["value"] == d["value"]
+    n_dofs = 2_000_244
+    assert abs(d["value"] * d["time_to_solve_s"] - n_dofs) < 1e-6 * n_dofs
+    assert d["e2e"]["value"] == d["value"] and d["e2e"]["h2d_bytes_per_step"] == 0 == d["e2e"]["d2h_bytes_per_step"]
+    # the sample that ran (setup + sample_iters iterations) is far shorter than the extrapolated solve
+    assert 0 < d["ms_per_step"] < 0.1 * d["time_to_solve_s"] * 1e3
