@@ -22,11 +22,11 @@ output_dir       = {out}
 bc.dirichlet     = left_sym:ux=0 ; bottom_sym:uy=0
 bc.traction      = {traction}
 kirsch.sigma_inf = 1
-kirsch.a         = 1
+kirsch.a         = {a}
 """
 
 
-def _run(pkg, tmp_path, mesh, solver="cg_jacobi", traction="right:tx=100e6,ty=0"):
+def _run(pkg, tmp_path, mesh, solver="cg_jacobi", traction="right:tx=100e6,ty=0", a=1.0):
     from importlib import import_module
     import io
     case = import_module("mpi-cst-fem-solver_b200.case")
@@ -34,7 +34,7 @@ def _run(pkg, tmp_path, mesh, solver="cg_jacobi", traction="right:tx=100e6,ty=0"
     pkg.write_gmsh(mesh, mp)
     out_dir = str(tmp_path / "out")
     cp = str(tmp_path / "k.case")
-    open(cp, "w").write(CASE.format(mesh=mp, out=out_dir, solver=solver, traction=traction))
+    open(cp, "w").write(CASE.format(mesh=mp, out=out_dir, solver=solver, traction=traction, a=repr(a)))
     out, err = io.StringIO(), io.StringIO()
     rc = case.run_case(cp, out, err)
     return rc, out.getvalue(), err.getvalue(), out_dir
@@ -97,3 +97,20 @@ def test_case_kirsch_exact_scf(pkg, gpu_lib, tmp_path, solver):
     k = t["kirsch"]
     assert 2.8 < k["scf"]["numerical"] < 3.2 and k["l2_rel_stress_error"] < 0.1
     assert t["solver"]["true_rel_residual"] <= 1e-10
+
+
+def test_case_kirsch_refinement_lowers_the_error(pkg, gpu_lib, golden, tmp_path):
+    """The reference's end-to-end check (its tests/check_e2e.cmake) on the GPU path: its committed
+    Kirsch meshes L0 and L1 (L = 1, hole radius 0.1) under the exact Kirsch traction, solved
+    through the case-file front end: converged, true residual below 1e-9, and the relative L2
+    error of the element stresses against the analytical field lower on L1 than on L0."""
+    errs = []
+    for name in ("kirsch_L0", "kirsch_L1"):
+        (tmp_path / name).mkdir()
+        rc, out, err, d = _run(pkg, tmp_path / name, golden(name).mesh(pkg), solver="gpu_cg",
+                               traction="kirsch_exact", a=0.1)
+        assert rc == 0, out + err
+        t = json.load(open(os.path.join(d, "timings.json")))
+        assert t["solver"]["converged"] and t["solver"]["true_rel_residual"] < 1e-9, t["solver"]
+        errs.append(t["kirsch"]["l2_rel_stress_error"])
+    assert 0.0 < errs[1] < errs[0], errs
