@@ -137,6 +137,28 @@ def test_empty_and_isolated(pkg, gpu_lib):
     K.ctx.close()
 
 
+def test_reference_triangle_known_answer(pkg, gpu_lib):
+    """The reference's element known answer (its tests/test_element.cpp:60-84) through the GPU
+    pattern and assembly: one triangle (0,0), (1,0), (0,1), E = 1, nu = 0, t = 1, plane stress;
+    the assembled 6 x 6 matrix equals the closed-form Ke within 1e-14."""
+    expected = np.array([[0.75, 0.25, -0.5, -0.25, -0.25, 0.0],
+                         [0.25, 0.75, 0.0, -0.25, -0.25, -0.5],
+                         [-0.5, 0.0, 0.5, 0.0, 0.0, 0.0],
+                         [-0.25, -0.25, 0.0, 0.25, 0.25, 0.0],
+                         [-0.25, -0.25, 0.0, 0.25, 0.25, 0.0],
+                         [0.0, -0.5, 0.0, 0.0, 0.0, 0.5]])
+    m = pkg.plate.Mesh(xy=np.array([0, 0, 1, 0, 0, 1.0]), triangles=np.array([0, 1, 2], np.int32),
+                       boundary_edges={})
+    K = pkg.build_stiffness_pattern(m)
+    pkg.assemble_stiffness(m, pkg.constitutive_matrix(1.0, 0.0), 1.0, K)
+    rp, cols, vals = K.download()
+    Kd = np.zeros((6, 6))
+    for i in range(6):
+        Kd[i, cols[rp[i]:rp[i + 1]]] = vals[rp[i]:rp[i + 1]]
+    assert np.max(np.abs(Kd - expected)) <= 1e-14
+    K.ctx.close()
+
+
 @pytest.fixture(scope="module")
 def big_plate(pkg):
     return pkg.plate.quarter_plate(565, 1766)  # 2,000,244 DOFs
